@@ -1,0 +1,203 @@
+/*
+ * jfem_gpu.h -- C ABI of the B200 (sm_100a) linear-solve library for JFEM.
+ *
+ * The library replaces the Java/JNI layer under JFEM's solver API.  Every
+ * entry point below names the reference interface it stands in for
+ * (paths relative to the JFEM project root).  Conventions:
+ *   - plain C types only; opaque handles; every call returns a jfg_status;
+ *   - host pointers ("h_") are copied in/out inside the call; device pointers
+ *     ("d_") must be device memory of the context's GPU;
+ *   - the caller owns host buffers, the library owns device buffers;
+ *   - a context owns one CUDA stream; one context per host thread.
+ * Index arrays follow JFEM's COO naming: `rows` are the row indices
+ * (SparseMatrix.sparseYs) and `cols` the column indices (sparseXs).
+ */
+#ifndef JFEM_GPU_H
+#define JFEM_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    JFG_OK = 0,
+    JFG_NOT_CONVERGED = 1,   /* iteration cap hit; x holds the last iterate */
+    JFG_BREAKDOWN = 2,       /* BiCGStab rho ~ 0 (after the GMRES fallback converged, see jfg_solve) */
+    JFG_NONFINITE = 3,       /* NaN/Inf met in a reduction */
+    JFG_ERR_BAD_ARG = 4,
+    JFG_ERR_SINGULAR = 5,
+    JFG_ERR_CUDA = 6,
+    JFG_ERR_NO_DEVICE = 7,
+    JFG_ERR_UNSUPPORTED = 8
+} jfg_status;
+
+typedef struct jfg_ctx jfg_ctx;
+typedef struct jfg_mat jfg_mat;
+typedef struct jfg_mg jfg_mg;
+
+/* ---- context --------------------------------------------------------- */
+/* Creates a context (one CUDA stream) on `device`. */
+int jfg_create(int device, jfg_ctx** out);
+int jfg_destroy(jfg_ctx* ctx);
+/* Message of the last failing call on this context ("" if none). */
+const char* jfg_last_error(jfg_ctx* ctx);
+/* Waits for all work queued on the context's stream. */
+int jfg_synchronize(jfg_ctx* ctx);
+/* The context's CUDA stream (cudaStream_t) for callers that time or order work. */
+void* jfg_stream(jfg_ctx* ctx);
+/* Library version string. */
+const char* jfg_version(void);
+/* Kernels this process has launched through the library, counting each
+ * executed kernel node of a replayed CUDA graph.  Measurement helper with no
+ * counterpart in the reference. */
+int jfg_kernel_launches(uint64_t* count);
+
+/* ---- sparse matrices ------------------------------------------------- */
+/* Builds a device matrix from COO triples in any order with duplicates,
+ * summing duplicates (the merge of SparseMatrix.getCoordinateEntryList,
+ * Core/src/main/java/linalg/SparseMatrix.java:196-225) and dropping entries
+ * that are exactly zero (e.g. Dirichlet rows zeroed in place,
+ * Core/src/main/java/basic/AcceptsMatrixBoundaryValues.java:39-40).
+ * Replaces: new SparseMatrix(rows, cols) + add(...) (SparseMatrix.java:274-294). */
+int jfg_matrix_from_coo(jfg_ctx* ctx, int n_rows, int n_cols, int64_t nnz, const int* h_rows,
+                        const int* h_cols, const double* h_vals, jfg_mat** out);
+int jfg_matrix_free(jfg_mat* m);
+/* Dimensions and merged nonzero count. */
+int jfg_matrix_info(jfg_mat* m, int* n_rows, int* n_cols, int64_t* nnz);
+/* y = A x.  Replaces SparseMatrix.mvMul (SparseMatrix.java:480-489) and
+ * SparseMvMul.mvMul (Core/src/main/java/linalg/SparseMvMul.java:73-94). */
+int jfg_spmv(jfg_mat* m, const double* h_x, double* h_y);
+/* y = A^T x.  Replaces SparseMatrix.tvMul (SparseMatrix.java:492-501) and
+ * SparseMvMul.tvMul (SparseMvMul.java:96-116). */
+int jfg_spmv_t(jfg_mat* m, const double* h_x, double* h_y);
+/* Device-pointer forms of the two products (no copies, queued on the stream). */
+int jfg_spmv_dev(jfg_mat* m, const double* d_x, double* d_y);
+int jfg_spmv_t_dev(jfg_mat* m, const double* d_x, double* d_y);
+/* FP32 product on FP32 device vectors (values rounded to FP32 once). */
+int jfg_spmv_f32_dev(jfg_mat* m, const float* d_x, float* d_y);
+/* Diagonal with duplicates summed.  Replaces Matrix.diag (Core/src/main/java/linalg/Matrix.java:157-175). */
+int jfg_matrix_diag(jfg_mat* m, double* h_diag);
+/* Times `iters` back-to-back FP64 (precision 0) or FP32 (precision 1)
+ * products y = A x on the context stream with CUDA events; returns the mean
+ * milliseconds per product.  x and y are library-owned device vectors
+ * (x = 1).  Measurement helper, not part of the reference surface. */
+int jfg_spmv_time(jfg_mat* m, int precision, int iters, double* ms_per_spmv);
+
+/* ---- smoothers ------------------------------------------------------- */
+typedef enum { JFG_SMOOTH_JACOBI = 0, JFG_SMOOTH_RICHARDSON = 1 } jfg_smoother_kind;
+typedef struct {
+    int kind;      /* jfg_smoother_kind */
+    int runs;      /* sweeps */
+    double omega;  /* damping */
+} jfg_smoother_desc;
+/* x <- smooth(A, rhs, x).  Replaces Smoother.smooth
+ * (Core/src/main/java/multigrid/Smoother.java:15) as implemented by
+ * JacobiSmoother.smooth (multigrid/JacobiSmoother.java:28-50) and
+ * RichardsonSmoother.smooth (multigrid/RichardsonSmoother.java:31-50). */
+int jfg_smooth(jfg_mat* A, const jfg_smoother_desc* sm, const double* h_rhs, double* h_x);
+
+/* ---- geometric multigrid -------------------------------------------- */
+typedef struct {
+    int cycles;        /* V-cycles per application (MGPreconditionerSpace.cycles, default 3) */
+    int use_fmg;       /* 1: FMG correction first (MGPreconditionerInterface.mvMul, :353-379);
+                          0: start the V-cycles from the boundary copy only */
+    int precision;     /* 0: FP64 hierarchy; 1: FP32 hierarchy (for mixed-precision solves) */
+} jfg_mg_desc;
+/* Builds a hierarchy from per-level systems A[0..levels) (0 = coarsest),
+ * prolongations P[l] (n_{l+1} x n_l, l < levels-1), Dirichlet node lists and
+ * smoothers (sm[l] for l >= 1; sm[0] ignored: level 0 is solved by dense LU).
+ * Replaces the MGPreconditionerSpace constructor's products
+ * (Core/src/main/java/multigrid/MGPreconditionerSpace.java:28-57). */
+int jfg_mg_create(jfg_ctx* ctx, int levels, jfg_mat* const* A, jfg_mat* const* P,
+                  const int* const* h_bdry, const int* n_bdry, const jfg_smoother_desc* sm,
+                  const jfg_mg_desc* desc, jfg_mg** out);
+int jfg_mg_free(jfg_mg* mg);
+/* out = M v, the preconditioner application.  Replaces
+ * MGPreconditionerInterface.mvMul (multigrid/MGPreconditionerInterface.java:352-379). */
+int jfg_mg_apply(jfg_mg* mg, const double* h_v, double* h_out);
+/* out = vCycle(x0, rhs).  Replaces MGPreconditionerInterface.vCycle (:293-298). */
+int jfg_mg_vcycle(jfg_mg* mg, const double* h_x0, const double* h_rhs, double* h_out);
+/* out = fullVCycleCorrection(defect).  Replaces MGPreconditionerInterface.fullVCycleCorrection (:307-326). */
+int jfg_mg_fmg(jfg_mg* mg, const double* h_defect, double* h_out);
+
+/* ---- iterative solvers ----------------------------------------------- */
+typedef enum {
+    JFG_CG = 0,          /* IterativeSolver.solveCG        (linalg/IterativeSolver.java:48-100) */
+    JFG_PCG = 1,         /* IterativeSolver.solvePCG       (:102-162) */
+    JFG_BICGSTAB = 2,    /* IterativeSolver.solveBiCGStab  (:256-323) */
+    JFG_PBICGSTAB = 3,   /* IterativeSolver.solvePBiCGStab (:325-402) */
+    JFG_GMRES = 4,       /* IterativeSolver.solveGMRES / GMRES.solve (linalg/GMRES.java:103-134) */
+    JFG_PGMRES = 5,      /* IterativeSolver.solvePGMRES / GMRES.solve with preconditioner (GMRES.java:64-101) */
+    JFG_GMRES2 = 6       /* GMRES2.solve (linalg/GMRES2.java:34-104) */
+} jfg_solver_kind;
+
+typedef enum {
+    JFG_PREC_NONE = 0,
+    JFG_PREC_MG = 1,       /* handle = jfg_mg* */
+    JFG_PREC_JACOBI = 2,   /* diagonal of A */
+    JFG_PREC_MATRIX = 3    /* handle = jfg_mat* applied as y = M x (e.g. an identity or an inverse) */
+} jfg_precond_kind;
+
+typedef enum {
+    JFG_FP64 = 0,          /* every operation in FP64 */
+    JFG_MIXED = 1          /* FP64 defect-correction outer loop around an FP32 inner solve */
+} jfg_precision;
+
+typedef struct {
+    double tol;            /* absolute residual tolerance, as the reference's `tol` */
+    int maxit;             /* 0: reference default (n for CG/BiCGStab, 10 n for PBiCGStab) */
+    int restart;           /* GMRES: GMRES.ITERATIONS_BEFORE_RESTART (default 150) */
+    int max_restarts;      /* GMRES: GMRES.MAX_RESTARTS (default 200) */
+    int precision;         /* jfg_precision */
+    double inner_rtol;     /* JFG_MIXED: relative tolerance of each inner solve (default 1e-4) */
+    int use_graph;         /* 1: replay the Krylov iteration as a CUDA graph */
+    int graph_chunk;       /* iterations per graph launch between convergence polls (default 8) */
+    double* h_history;     /* optional: residual norm per iteration */
+    int history_cap;
+} jfg_solver_opts;
+
+typedef struct {
+    int iterations;        /* IterativeSolver.iterations */
+    int restarts;
+    int status;            /* jfg_status */
+    int outer_iterations;  /* JFG_MIXED: defect-correction steps */
+    double final_residual; /* FP64 true residual ||b - A x|| at exit */
+    double final_norm;     /* last residual norm published by the iteration */
+    int history_len;
+    int not_pd;            /* CG met p.Ap <= 0 ("CG warning: Matrix not PD") */
+} jfg_solve_info;
+
+/* Fills opts with the reference defaults (tol 1e-10 absolute, restart 150,
+ * 200 restarts, FP64, CUDA graph on). */
+void jfg_solver_opts_default(jfg_solver_opts* opts);
+
+/* Solves A x = b.  x holds the start iterate on entry (the reference starts
+ * from e0, or from the previous solution when an IterativeSolver is reused,
+ * IterativeSolver.java:69-72) and the solution on exit.  `precond` is a
+ * jfg_mg* for JFG_PREC_MG, a jfg_mat* for JFG_PREC_MATRIX, NULL otherwise.
+ * Replaces the IterativeSolver.solve* methods listed in jfg_solver_kind. */
+int jfg_solve(jfg_ctx* ctx, int kind, jfg_mat* A, int precond_kind, void* precond, const double* h_b,
+              double* h_x, const jfg_solver_opts* opts, jfg_solve_info* info);
+/* Same on device vectors (no host copies; synchronises at exit). */
+int jfg_solve_dev(jfg_ctx* ctx, int kind, jfg_mat* A, int precond_kind, void* precond, const double* d_b,
+                  double* d_x, const jfg_solver_opts* opts, jfg_solve_info* info);
+
+/* ---- dense direct solves --------------------------------------------- */
+/* x = A^-1 b for a dense row-major n x n A (partial-pivot LU on the GPU).
+ * Replaces DenseMatrix.solve (linalg/DenseMatrix.java:516-519) and the JNI
+ * iSolve (JSparse/src/native/sparseSolver.cpp:10-60). */
+int jfg_dense_solve(jfg_ctx* ctx, int n, const double* h_A, const double* h_b, double* h_x);
+/* Ainv = A^-1.  Replaces DenseMatrix.inverse and the JNI iInverse (sparseSolver.cpp:63-113). */
+int jfg_dense_inverse(jfg_ctx* ctx, int n, const double* h_A, double* h_Ainv);
+/* Drop-in for SparseMatrix.solve(rhs) (linalg/SparseMatrix.java:142-150): COO in, x out.
+ * n <= 4096: dense LU of the merged matrix on the GPU (the reference's method);
+ * larger: FP64 GMRES with a Jacobi preconditioner to ||b - A x|| <= 1e-12 ||b||. */
+int jfg_sparse_solve(jfg_ctx* ctx, int n, int64_t nnz, const int* h_rows, const int* h_cols,
+                     const double* h_vals, const double* h_b, double* h_x);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* JFEM_GPU_H */

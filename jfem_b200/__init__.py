@@ -1,0 +1,15 @@
+"""jfem_b200 -- B200 (sm_100a) implementation of JFEM's linear-solve path.
+
+The compute lives in ``libjfem_gpu.so`` (hand-written CUDA behind the C ABI of
+``include/jfem_gpu.h``); this package is the host-side mirror of the
+reference's Java solver API (``linalg``, ``multigrid``) plus the structured
+grid assembler that produces the systems (``assembly``, ``problems``).
+"""
+from . import _native
+from .linalg import (DenseMatrix, DeviceMatrix, GMRES, IllegalArgumentException, IterativeSolver,
+                     SingularMatrixException, SparseMatrix, VectorMultiplyable)
+from .multigrid import JacobiSmoother, MGPreconditioner, RichardsonSmoother
+
+__all__ = ["DenseMatrix", "DeviceMatrix", "GMRES", "IllegalArgumentException", "IterativeSolver",
+           "SingularMatrixException", "SparseMatrix", "VectorMultiplyable", "JacobiSmoother",
+           "MGPreconditioner", "RichardsonSmoother"]

@@ -1,0 +1,724 @@
+// The extern "C" surface (include/jfem_gpu.h): argument checks, host<->device
+// staging and error translation.  No entry point lets a C++ exception escape.
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "jfg_krylov.cuh"
+
+struct jfg_ctx {
+    jfg::Context c;
+    jfg::SolverWork work;
+    jfg::DevBuf<double> stage_a, stage_b;   // staging vectors for host-pointer calls
+    jfg::DevBuf<double> stage_c;
+};
+
+struct jfg_mat {
+    jfg_ctx* ctx = nullptr;
+    jfg::Matrix* m = nullptr;
+};
+
+namespace {
+
+using jfg::DevBuf;
+using jfg::Error;
+
+template <class F>
+int guard(jfg_ctx* ctx, F&& f)
+{
+    try {
+        if (ctx) {
+            cudaError_t e = cudaSetDevice(ctx->c.device);
+            if (e != cudaSuccess) throw Error{JFG_ERR_CUDA, cudaGetErrorString(e)};
+        }
+        int st = f();
+        if (ctx && st != JFG_OK && ctx->c.last_error.empty()) ctx->c.last_error = "status " + std::to_string(st);
+        return st;
+    } catch (const Error& e) {
+        if (ctx) ctx->c.last_error = e.msg;
+        return e.status;
+    } catch (const std::exception& e) {
+        if (ctx) ctx->c.last_error = e.what();
+        return JFG_ERR_CUDA;
+    } catch (...) {
+        if (ctx) ctx->c.last_error = "unknown error";
+        return JFG_ERR_CUDA;
+    }
+}
+
+void stage_in(jfg_ctx* ctx, DevBuf<double>& buf, const double* h, size_t n)
+{
+    buf.alloc(n);
+    if (n) JFG_CUDA(cudaMemcpyAsync(buf.p, h, n * sizeof(double), cudaMemcpyHostToDevice, ctx->c.stream));
+}
+void stage_out(jfg_ctx* ctx, const double* d, double* h, size_t n)
+{
+    if (n) JFG_CUDA(cudaMemcpyAsync(h, d, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->c.stream));
+    JFG_CUDA(cudaStreamSynchronize(ctx->c.stream));
+}
+
+jfg::Scratch ctx_scratch(jfg_ctx* ctx, int max_blocks)
+{
+    ctx->work.c = &ctx->c;
+    ctx->work.ensure(0, max_blocks, 1);
+    return ctx->work.sc;
+}
+
+struct FinStoreD {
+    double* dst;
+    __device__ void operator()(const double* t) const { *dst = t[0]; }
+};
+
+struct SpmvStore64 {
+    static void run(cudaStream_t st, jfg::Matrix* M, const double* x, double* y, const jfg::Scratch& sc)
+    {
+        jfg::spmv_launch<double, double, 0>(st, M, M->val.p, x, jfg::EpiStore<double>{y}, sc, nullptr);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+const char* jfg_version(void) { return "jfem_b200 0.1 (sm_100a)"; }
+
+int jfg_create(int device, jfg_ctx** out)
+{
+    if (!out) return JFG_ERR_BAD_ARG;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return JFG_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= count) return JFG_ERR_BAD_ARG;
+    auto* ctx = new jfg_ctx();
+    ctx->c.device = device;
+    int st = guard(ctx, [&]() -> int {
+        JFG_CUDA(cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking));
+        ctx->work.c = &ctx->c;
+        return JFG_OK;
+    });
+    if (st != JFG_OK) {
+        delete ctx;
+        return st;
+    }
+    *out = ctx;
+    return JFG_OK;
+}
+
+int jfg_destroy(jfg_ctx* ctx)
+{
+    if (!ctx) return JFG_ERR_BAD_ARG;
+    cudaSetDevice(ctx->c.device);
+    cudaStreamSynchronize(ctx->c.stream);
+    cudaStream_t s = ctx->c.stream;
+    delete ctx;
+    if (s) cudaStreamDestroy(s);
+    return JFG_OK;
+}
+
+const char* jfg_last_error(jfg_ctx* ctx) { return ctx ? ctx->c.last_error.c_str() : "null context"; }
+
+int jfg_synchronize(jfg_ctx* ctx)
+{
+    if (!ctx) return JFG_ERR_BAD_ARG;
+    return guard(ctx, [&]() -> int {
+        JFG_CUDA(cudaStreamSynchronize(ctx->c.stream));
+        return JFG_OK;
+    });
+}
+
+void* jfg_stream(jfg_ctx* ctx) { return ctx ? (void*)ctx->c.stream : nullptr; }
+
+int jfg_kernel_launches(uint64_t* count)
+{
+    if (!count) return JFG_ERR_BAD_ARG;
+    *count = jfg::g_launches.load();
+    return JFG_OK;
+}
+
+// ---------------------------------------------------------------------------
+int jfg_matrix_from_coo(jfg_ctx* ctx, int n_rows, int n_cols, int64_t nnz, const int* rows, const int* cols,
+                        const double* vals, jfg_mat** out)
+{
+    if (!ctx || !out) return JFG_ERR_BAD_ARG;
+    *out = nullptr;
+    return guard(ctx, [&]() -> int {
+        jfg::Matrix* m = jfg::matrix_from_coo(&ctx->c, n_rows, n_cols, nnz, rows, cols, vals, false);
+        auto* h = new jfg_mat();
+        h->ctx = ctx;
+        h->m = m;
+        *out = h;
+        return JFG_OK;
+    });
+}
+
+int jfg_matrix_free(jfg_mat* m)
+{
+    if (!m) return JFG_ERR_BAD_ARG;
+    cudaSetDevice(m->ctx->c.device);
+    cudaStreamSynchronize(m->ctx->c.stream);
+    delete m->m;
+    delete m;
+    return JFG_OK;
+}
+
+int jfg_matrix_info(jfg_mat* m, int* n_rows, int* n_cols, int64_t* nnz)
+{
+    if (!m) return JFG_ERR_BAD_ARG;
+    if (n_rows) *n_rows = m->m->rows;
+    if (n_cols) *n_cols = m->m->cols;
+    if (nnz) *nnz = m->m->nnz;
+    return JFG_OK;
+}
+
+int jfg_spmv_dev(jfg_mat* m, const double* x, double* y)
+{
+    if (!m || (!x && m->m->cols) || (!y && m->m->rows)) return JFG_ERR_BAD_ARG;
+    jfg_ctx* ctx = m->ctx;
+    return guard(ctx, [&]() -> int {
+        jfg::Scratch sc = ctx_scratch(ctx, m->m->nblocks);
+        SpmvStore64::run(ctx->c.stream, m->m, x, y, sc);
+        return JFG_OK;
+    });
+}
+
+int jfg_spmv_t_dev(jfg_mat* m, const double* x, double* y)
+{
+    if (!m || (!x && m->m->rows) || (!y && m->m->cols)) return JFG_ERR_BAD_ARG;
+    jfg_ctx* ctx = m->ctx;
+    return guard(ctx, [&]() -> int {
+        jfg::Matrix* T = jfg::matrix_transpose(m->m);
+        jfg::Scratch sc = ctx_scratch(ctx, T->nblocks);
+        SpmvStore64::run(ctx->c.stream, T, x, y, sc);
+        return JFG_OK;
+    });
+}
+
+int jfg_spmv_f32_dev(jfg_mat* m, const float* x, float* y)
+{
+    if (!m || (!x && m->m->cols) || (!y && m->m->rows)) return JFG_ERR_BAD_ARG;
+    jfg_ctx* ctx = m->ctx;
+    return guard(ctx, [&]() -> int {
+        jfg::matrix_ensure_fp32(m->m);
+        jfg::Scratch sc = ctx_scratch(ctx, m->m->nblocks);
+        jfg::spmv_launch<float, float, 0>(ctx->c.stream, m->m, m->m->val32.p, x, jfg::EpiStore<float>{y}, sc, nullptr);
+        return JFG_OK;
+    });
+}
+
+int jfg_spmv(jfg_mat* m, const double* x, double* y)
+{
+    if (!m || (!x && m->m->cols) || (!y && m->m->rows)) return JFG_ERR_BAD_ARG;
+    jfg_ctx* ctx = m->ctx;
+    return guard(ctx, [&]() -> int {
+        stage_in(ctx, ctx->stage_a, x, m->m->cols);
+        ctx->stage_b.alloc(m->m->rows);
+        jfg::Scratch sc = ctx_scratch(ctx, m->m->nblocks);
+        SpmvStore64::run(ctx->c.stream, m->m, ctx->stage_a.p, ctx->stage_b.p, sc);
+        stage_out(ctx, ctx->stage_b.p, y, m->m->rows);
+        return JFG_OK;
+    });
+}
+
+int jfg_spmv_t(jfg_mat* m, const double* x, double* y)
+{
+    if (!m || (!x && m->m->rows) || (!y && m->m->cols)) return JFG_ERR_BAD_ARG;
+    jfg_ctx* ctx = m->ctx;
+    return guard(ctx, [&]() -> int {
+        jfg::Matrix* T = jfg::matrix_transpose(m->m);
+        stage_in(ctx, ctx->stage_a, x, m->m->rows);
+        ctx->stage_b.alloc(m->m->cols);
+        jfg::Scratch sc = ctx_scratch(ctx, T->nblocks);
+        SpmvStore64::run(ctx->c.stream, T, ctx->stage_a.p, ctx->stage_b.p, sc);
+        stage_out(ctx, ctx->stage_b.p, y, m->m->cols);
+        return JFG_OK;
+    });
+}
+
+int jfg_matrix_diag(jfg_mat* m, double* h_diag)
+{
+    if (!m || (!h_diag && m->m->rows)) return JFG_ERR_BAD_ARG;
+    jfg_ctx* ctx = m->ctx;
+    return guard(ctx, [&]() -> int {
+        int n = std::min(m->m->rows, m->m->cols);
+        stage_out(ctx, m->m->diag.p, h_diag, n);
+        return JFG_OK;
+    });
+}
+
+int jfg_spmv_time(jfg_mat* m, int precision, int iters, double* ms)
+{
+    if (!m || !ms || iters <= 0) return JFG_ERR_BAD_ARG;
+    jfg_ctx* ctx = m->ctx;
+    return guard(ctx, [&]() -> int {
+        cudaStream_t st = ctx->c.stream;
+        jfg::Matrix* M = m->m;
+        jfg::Scratch sc = ctx_scratch(ctx, M->nblocks);
+        cudaEvent_t e0, e1;
+        JFG_CUDA(cudaEventCreate(&e0));
+        JFG_CUDA(cudaEventCreate(&e1));
+        float t = 0;
+        if (precision == 0) {
+            DevBuf<double> x, y;
+            x.alloc(M->cols);
+            y.alloc(M->rows);
+            std::vector<double> ones(M->cols, 1.0);
+            JFG_CUDA(cudaMemcpyAsync(x.p, ones.data(), sizeof(double) * M->cols, cudaMemcpyHostToDevice, st));
+            for (int i = 0; i < 3; i++) SpmvStore64::run(st, M, x.p, y.p, sc);
+            JFG_CUDA(cudaEventRecord(e0, st));
+            for (int i = 0; i < iters; i++) SpmvStore64::run(st, M, x.p, y.p, sc);
+            JFG_CUDA(cudaEventRecord(e1, st));
+        } else {
+            jfg::matrix_ensure_fp32(M);
+            DevBuf<float> x, y;
+            x.alloc(M->cols);
+            y.alloc(M->rows);
+            std::vector<float> ones(M->cols, 1.0f);
+            JFG_CUDA(cudaMemcpyAsync(x.p, ones.data(), sizeof(float) * M->cols, cudaMemcpyHostToDevice, st));
+            for (int i = 0; i < 3; i++)
+                jfg::spmv_launch<float, float, 0>(st, M, M->val32.p, x.p, jfg::EpiStore<float>{y.p}, sc, nullptr);
+            JFG_CUDA(cudaEventRecord(e0, st));
+            for (int i = 0; i < iters; i++)
+                jfg::spmv_launch<float, float, 0>(st, M, M->val32.p, x.p, jfg::EpiStore<float>{y.p}, sc, nullptr);
+            JFG_CUDA(cudaEventRecord(e1, st));
+        }
+        JFG_CUDA(cudaEventSynchronize(e1));
+        JFG_CUDA(cudaEventElapsedTime(&t, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *ms = t / iters;
+        return JFG_OK;
+    });
+}
+
+// ---------------------------------------------------------------------------
+int jfg_smooth(jfg_mat* A, const jfg_smoother_desc* sm, const double* rhs, double* x)
+{
+    if (!A || !sm || A->m->rows != A->m->cols || sm->runs < 0) return JFG_ERR_BAD_ARG;
+    if (sm->kind != JFG_SMOOTH_JACOBI && sm->kind != JFG_SMOOTH_RICHARDSON) return JFG_ERR_BAD_ARG;
+    jfg_ctx* ctx = A->ctx;
+    return guard(ctx, [&]() -> int {
+        int n = A->m->rows;
+        stage_in(ctx, ctx->stage_a, rhs, n);
+        stage_in(ctx, ctx->stage_b, x, n);
+        jfg::SmootherDesc d;
+        d.kind = sm->kind;
+        d.runs = sm->runs;
+        d.omega = sm->omega;
+        jfg::Scratch sc = ctx_scratch(ctx, A->m->nblocks);
+        jfg::smooth_standalone(&ctx->c, A->m, d, ctx->stage_a.p, ctx->stage_b.p, sc);
+        stage_out(ctx, ctx->stage_b.p, x, n);
+        return JFG_OK;
+    });
+}
+
+// ---------------------------------------------------------------------------
+int jfg_mg_create(jfg_ctx* ctx, int levels, jfg_mat* const* A, jfg_mat* const* P, const int* const* bdry,
+                  const int* n_bdry, const jfg_smoother_desc* sm, const jfg_mg_desc* desc, jfg_mg** out)
+{
+    if (!ctx || !out || levels < 1 || !A || !n_bdry || !bdry || (levels > 1 && (!P || !sm))) return JFG_ERR_BAD_ARG;
+    *out = nullptr;
+    return guard(ctx, [&]() -> int {
+        auto* g = new jfg_mg();
+        try {
+            g->ctx = &ctx->c;
+            g->levels = levels;
+            g->cycles = desc ? desc->cycles : 3;
+            g->use_fmg = desc ? desc->use_fmg : 1;
+            g->precision = desc ? desc->precision : 0;
+            JFG_CHECK(g->cycles >= 0, JFG_ERR_BAD_ARG, "negative cycle count");
+            for (int l = 0; l < levels; l++) {
+                JFG_CHECK(A[l] && A[l]->ctx == ctx, JFG_ERR_BAD_ARG, "level matrix from another context");
+                g->A.push_back(A[l]->m);
+                if (l < levels - 1) {
+                    JFG_CHECK(P[l] && P[l]->ctx == ctx, JFG_ERR_BAD_ARG, "prolongation from another context");
+                    g->P.push_back(P[l]->m);
+                } else {
+                    g->P.push_back(nullptr);
+                }
+                g->bdry.emplace_back(bdry[l] ? std::vector<int>(bdry[l], bdry[l] + n_bdry[l]) : std::vector<int>());
+                jfg::SmootherDesc d;
+                if (l >= 1) {
+                    JFG_CHECK(sm[l].kind == JFG_SMOOTH_JACOBI || sm[l].kind == JFG_SMOOTH_RICHARDSON, JFG_ERR_BAD_ARG,
+                              "unknown smoother kind");
+                    JFG_CHECK(sm[l].runs >= 0, JFG_ERR_BAD_ARG, "negative smoother runs");
+                    d.kind = sm[l].kind;
+                    d.runs = sm[l].runs;
+                    d.omega = sm[l].omega;
+                }
+                g->sm.push_back(d);
+            }
+            std::vector<const int*> bp(levels);
+            std::vector<int> nbp(levels);
+            for (int l = 0; l < levels; l++) {
+                bp[l] = g->bdry[l].data();
+                nbp[l] = (int)g->bdry[l].size();
+            }
+            g->d64.reset(new jfg::MGImpl<double>());
+            g->d64->init(&ctx->c, levels, g->A.data(), g->P.data(), bp.data(), nbp.data(), g->sm.data(), g->cycles,
+                         g->use_fmg);
+            if (g->d64->coarse_status != JFG_OK) throw Error{JFG_ERR_SINGULAR, "coarsest-level matrix is singular"};
+            if (g->precision == 1) g->fp32();
+        } catch (...) {
+            delete g;
+            throw;
+        }
+        *out = g;
+        return JFG_OK;
+    });
+}
+
+int jfg_mg_free(jfg_mg* g)
+{
+    if (!g) return JFG_ERR_BAD_ARG;
+    cudaStreamSynchronize(g->ctx->stream);
+    delete g;
+    return JFG_OK;
+}
+
+static jfg_ctx* ctx_of(jfg_mg* g)
+{
+    // the Context is the first member of jfg_ctx
+    return reinterpret_cast<jfg_ctx*>(g->ctx);
+}
+
+int jfg_mg_apply(jfg_mg* g, const double* v, double* out)
+{
+    if (!g || !v || !out) return JFG_ERR_BAD_ARG;
+    jfg_ctx* ctx = ctx_of(g);
+    return guard(ctx, [&]() -> int {
+        int n = g->d64->n[g->levels - 1];
+        stage_in(ctx, ctx->stage_a, v, n);
+        ctx->stage_b.alloc(n);
+        jfg::Scratch sc = ctx_scratch(ctx, g->d64->max_blocks());
+        g->d64->apply(ctx->stage_a.p, ctx->stage_b.p, sc, nullptr, ctx->c.stream);
+        stage_out(ctx, ctx->stage_b.p, out, n);
+        return JFG_OK;
+    });
+}
+
+int jfg_mg_vcycle(jfg_mg* g, const double* x0, const double* rhs, double* out)
+{
+    if (!g || !x0 || !rhs || !out) return JFG_ERR_BAD_ARG;
+    jfg_ctx* ctx = ctx_of(g);
+    return guard(ctx, [&]() -> int {
+        int n = g->d64->n[g->levels - 1];
+        stage_in(ctx, ctx->stage_a, x0, n);
+        stage_in(ctx, ctx->stage_b, rhs, n);
+        ctx->stage_c.alloc(n);
+        jfg::Scratch sc = ctx_scratch(ctx, g->d64->max_blocks());
+        g->d64->vcycle(ctx->stage_a.p, ctx->stage_b.p, ctx->stage_c.p, sc, nullptr, ctx->c.stream);
+        stage_out(ctx, ctx->stage_c.p, out, n);
+        return JFG_OK;
+    });
+}
+
+int jfg_mg_fmg(jfg_mg* g, const double* defect, double* out)
+{
+    if (!g || !defect || !out) return JFG_ERR_BAD_ARG;
+    jfg_ctx* ctx = ctx_of(g);
+    return guard(ctx, [&]() -> int {
+        int n = g->d64->n[g->levels - 1];
+        stage_in(ctx, ctx->stage_a, defect, n);
+        ctx->stage_b.alloc(n);
+        jfg::Scratch sc = ctx_scratch(ctx, g->d64->max_blocks());
+        g->d64->fmg(ctx->stage_a.p, ctx->stage_b.p, sc, nullptr, ctx->c.stream);
+        stage_out(ctx, ctx->stage_b.p, out, n);
+        return JFG_OK;
+    });
+}
+
+// ---------------------------------------------------------------------------
+void jfg_solver_opts_default(jfg_solver_opts* o)
+{
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->tol = 1e-10;
+    o->maxit = 0;
+    o->restart = 150;
+    o->max_restarts = 200;
+    o->precision = JFG_FP64;
+    o->inner_rtol = 1e-4;
+    o->use_graph = 1;
+    o->graph_chunk = 8;
+}
+
+static int solve_impl(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, const double* d_b, double* d_x,
+                      const jfg_solver_opts* o, jfg_solve_info* info)
+{
+    using namespace jfg;
+    JFG_CHECK(A && A->ctx == ctx, JFG_ERR_BAD_ARG, "matrix from another context");
+    Matrix* M = A->m;
+    JFG_CHECK(M->rows == M->cols, JFG_ERR_BAD_ARG, "matrix is not square");
+    JFG_CHECK(kind >= JFG_CG && kind <= JFG_GMRES2, JFG_ERR_BAD_ARG, "unknown solver kind");
+    JFG_CHECK(pk >= JFG_PREC_NONE && pk <= JFG_PREC_MATRIX, JFG_ERR_BAD_ARG, "unknown preconditioner kind");
+    bool needs_prec = kind == JFG_PCG || kind == JFG_PBICGSTAB || kind == JFG_PGMRES;
+    JFG_CHECK(!needs_prec || pk != JFG_PREC_NONE, JFG_ERR_BAD_ARG, "solver kind needs a preconditioner");
+    JFG_CHECK(needs_prec || kind == JFG_GMRES2 || pk == JFG_PREC_NONE, JFG_ERR_BAD_ARG,
+              "solver kind takes no preconditioner");
+    JFG_CHECK(kind != JFG_GMRES2, JFG_ERR_UNSUPPORTED, "GMRES2 is not implemented on the GPU yet");
+    JFG_CHECK(o->tol >= 0 && std::isfinite(o->tol), JFG_ERR_BAD_ARG, "bad tolerance");
+    int n = M->rows;
+    jfg_mg* mg = pk == JFG_PREC_MG ? static_cast<jfg_mg*>(ph) : nullptr;
+    jfg_mat* pm = pk == JFG_PREC_MATRIX ? static_cast<jfg_mat*>(ph) : nullptr;
+    JFG_CHECK(pk != JFG_PREC_MG || (mg && mg->d64 && mg->d64->n[mg->levels - 1] == n), JFG_ERR_BAD_ARG,
+              "multigrid preconditioner does not match the system size");
+    JFG_CHECK(pk != JFG_PREC_MATRIX || (pm && pm->m->rows == n && pm->m->cols == n), JFG_ERR_BAD_ARG,
+              "preconditioner matrix does not match the system size");
+    bool mixed = o->precision == JFG_MIXED;
+    JFG_CHECK(!mixed || kind == JFG_CG || kind == JFG_PCG, JFG_ERR_UNSUPPORTED,
+              "mixed precision is implemented for CG/PCG");
+    SolverWork& w = ctx->work;
+    w.c = &ctx->c;
+    int mb = M->nblocks;
+    if (mg) mb = std::max(mb, mg->d64->max_blocks());
+    if (pm) mb = std::max(mb, pm->m->nblocks);
+    int hcap = o->h_history ? std::max(o->history_cap, 1) : 1;
+    w.ensure(n, mb, hcap);
+    cudaStream_t st = ctx->c.stream;
+    for (int i = 0; i < 12; i++) w.v64[i].alloc(n);
+    Precond<double> P64;
+    P64.kind = pk;
+    P64.n = n;
+    if (mg) P64.mg = mg->d64.get();
+    if (pm) P64.M = pm->m;
+    if (pk == JFG_PREC_JACOBI) {
+        w.dinv64.alloc(n);
+        // 1 / diag with zero diagonals replaced by 1
+        std::vector<double> d(n);
+        JFG_CUDA(cudaMemcpyAsync(d.data(), M->diag.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+        JFG_CUDA(cudaStreamSynchronize(st));
+        for (auto& v : d) v = (std::fabs(v) < 1e-300) ? 1.0 : 1.0 / v;
+        JFG_CUDA(cudaMemcpyAsync(w.dinv64.p, d.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
+        P64.dinv = w.dinv64.p;
+    }
+    int use_graph = o->use_graph;
+    int chunk = o->graph_chunk > 0 ? o->graph_chunk : 8;
+    double* hist = o->h_history ? w.hist.p : nullptr;
+    int maxit = o->maxit;
+    Ctl res{};
+    int restarts = 0, outer = 0, inner = 0;
+    if (kind == JFG_CG || kind == JFG_PCG) {
+        if (maxit <= 0) maxit = n;
+        if (mixed) {
+            for (int i = 0; i < 8; i++) w.v32[i].alloc(n);
+            Precond<float> P32;
+            P32.kind = pk;
+            P32.n = n;
+            if (mg) P32.mg = mg->fp32();
+            if (pm) {
+                matrix_ensure_fp32(pm->m);
+                P32.M = pm->m;
+            }
+            if (pk == JFG_PREC_JACOBI) {
+                w.dinv32.alloc(n);
+                std::vector<double> d(n);
+                std::vector<float> f(n);
+                JFG_CUDA(cudaMemcpyAsync(d.data(), w.dinv64.p, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+                JFG_CUDA(cudaStreamSynchronize(st));
+                for (int i = 0; i < n; i++) f[i] = (float)d[i];
+                JFG_CUDA(cudaMemcpyAsync(w.dinv32.p, f.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st));
+                P32.dinv = w.dinv32.p;
+            }
+            double rt = o->inner_rtol > 0 ? o->inner_rtol : 1e-4;
+            outer = run_mixed_cg(w, M, P32, d_b, d_x, o->tol, maxit, rt, use_graph, chunk, &inner, hist, hcap);
+            res = [&] {
+                Ctl h;
+                JFG_CUDA(cudaMemcpy(&h, w.ctl.p, sizeof(Ctl), cudaMemcpyDeviceToHost));
+                return h;
+            }();
+            res.iter = inner;
+        } else {
+            Ctl h{};
+            h.tol = o->tol;
+            h.maxit = maxit;
+            h.alpha = h.omega = h.rho = h.rho_last = h.beta = 1;
+            h.hist = hist;
+            h.hist_cap = hcap;
+            h.n = n;
+            h.status = JFG_NOT_CONVERGED;
+            JFG_CUDA(cudaMemcpyAsync(w.ctl.p, &h, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+            int nodes = run_cg<double>(w, 0, M, P64, d_b, d_x, w.v64[0].p, w.v64[1].p, w.v64[2].p, w.v64[3].p,
+                                       false, use_graph, chunk);
+            JFG_CUDA(cudaMemcpyAsync(&res, w.ctl.p, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+            JFG_CUDA(cudaStreamSynchronize(st));
+            note_launch((unsigned long long)nodes * (unsigned long long)(res.iter > 0 ? res.iter : 1));
+        }
+    } else if (kind == JFG_BICGSTAB || kind == JFG_PBICGSTAB) {
+        if (maxit <= 0) maxit = kind == JFG_BICGSTAB ? n : 10 * n;
+        // keep the start iterate for the GMRES fallback
+        JFG_CUDA(cudaMemcpyAsync(w.v64[11].p, d_x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        Ctl h{};
+        h.tol = o->tol;
+        h.maxit = maxit;
+        h.alpha = h.omega = h.rho = h.rho_last = h.beta = 1;
+        h.hist = hist;
+        h.hist_cap = hcap;
+        h.n = n;
+        h.status = JFG_NOT_CONVERGED;
+        JFG_CUDA(cudaMemcpyAsync(w.ctl.p, &h, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+        double* v[9] = {w.v64[0].p, w.v64[1].p, w.v64[2].p, w.v64[3].p, w.v64[4].p,
+                        w.v64[5].p, w.v64[6].p, w.v64[7].p, w.v64[8].p};
+        int nodes = run_bicgstab<double>(w, 0, M, P64, d_b, d_x, v, use_graph, chunk);
+        JFG_CUDA(cudaMemcpyAsync(&res, w.ctl.p, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+        JFG_CUDA(cudaStreamSynchronize(st));
+        note_launch((unsigned long long)nodes * (unsigned long long)(res.iter > 0 ? res.iter : 1));
+        if (res.status == JFG_BREAKDOWN) {
+            // IterativeSolver.java:293-294 / 369-370: fall back to (P)GMRES from
+            // the start iterate (unpreconditioned) or from zero (preconditioned)
+            int it0 = res.iter;
+            if (kind == JFG_BICGSTAB)
+                JFG_CUDA(cudaMemcpyAsync(d_x, w.v64[11].p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+            else
+                JFG_CUDA(cudaMemsetAsync(d_x, 0, sizeof(double) * n, st));
+            h.status = JFG_NOT_CONVERGED;
+            JFG_CUDA(cudaMemcpyAsync(w.ctl.p, &h, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+            restarts = run_gmres(w, M, P64, d_b, d_x, o->restart > 0 ? o->restart : 150,
+                                 o->max_restarts >= 0 ? o->max_restarts : 200, use_graph, chunk);
+            JFG_CUDA(cudaMemcpyAsync(&res, w.ctl.p, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+            JFG_CUDA(cudaStreamSynchronize(st));
+            res.iter += it0;
+            if (res.status == JFG_OK) res.status = JFG_BREAKDOWN;
+        }
+    } else {  // GMRES / PGMRES
+        Ctl h{};
+        h.tol = o->tol;
+        h.maxit = 1 << 30;
+        h.hist = hist;
+        h.hist_cap = hcap;
+        h.n = n;
+        h.restart_len = o->restart > 0 ? o->restart : 150;
+        h.status = JFG_NOT_CONVERGED;
+        JFG_CUDA(cudaMemcpyAsync(w.ctl.p, &h, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+        restarts = run_gmres(w, M, P64, d_b, d_x, h.restart_len, o->max_restarts >= 0 ? o->max_restarts : 200,
+                             use_graph, chunk);
+        JFG_CUDA(cudaMemcpyAsync(&res, w.ctl.p, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+        JFG_CUDA(cudaStreamSynchronize(st));
+    }
+    // FP64 true residual ||b - A x||
+    double* r = w.v64[10].p;
+    spmv_launch<double, double, 1>(st, M, M->val.p, d_x, EpiResid<double>{d_b, r}, w.sc, nullptr,
+                                   FinStoreD{&w.ctl.p[1].true_res});
+    double ss = 0;
+    JFG_CUDA(cudaMemcpyAsync(&ss, &w.ctl.p[1].true_res, sizeof(double), cudaMemcpyDeviceToHost, st));
+    JFG_CUDA(cudaStreamSynchronize(st));
+    if (info) {
+        std::memset(info, 0, sizeof(*info));
+        info->iterations = res.iter;
+        info->restarts = restarts;
+        info->status = res.status;
+        info->outer_iterations = outer;
+        info->final_residual = std::sqrt(ss);
+        info->final_norm = res.res_norm;
+        info->not_pd = res.not_pd;
+        int hl = mixed ? outer : res.iter;
+        info->history_len = std::min(hl, hcap);
+    }
+    if (o->h_history && o->history_cap > 0) {
+        int hl = std::min(mixed ? outer : res.iter, o->history_cap);
+        if (hl > 0) {
+            JFG_CUDA(cudaMemcpyAsync(o->h_history, w.hist.p, sizeof(double) * hl, cudaMemcpyDeviceToHost, st));
+            JFG_CUDA(cudaStreamSynchronize(st));
+        }
+    }
+    (void)inner;
+    return res.status == JFG_BREAKDOWN ? JFG_OK : (res.status == JFG_OK ? JFG_OK : res.status);
+}
+
+int jfg_solve_dev(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, const double* d_b, double* d_x,
+                  const jfg_solver_opts* opts, jfg_solve_info* info)
+{
+    if (!ctx || !A || !d_b || !d_x) return JFG_ERR_BAD_ARG;
+    jfg_solver_opts o;
+    if (opts)
+        o = *opts;
+    else
+        jfg_solver_opts_default(&o);
+    return guard(ctx, [&]() -> int { return solve_impl(ctx, kind, A, pk, ph, d_b, d_x, &o, info); });
+}
+
+int jfg_solve(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, const double* h_b, double* h_x,
+              const jfg_solver_opts* opts, jfg_solve_info* info)
+{
+    if (!ctx || !A || !h_b || !h_x) return JFG_ERR_BAD_ARG;
+    jfg_solver_opts o;
+    if (opts)
+        o = *opts;
+    else
+        jfg_solver_opts_default(&o);
+    return guard(ctx, [&]() -> int {
+        int n = A->m->rows;
+        stage_in(ctx, ctx->stage_a, h_b, n);
+        stage_in(ctx, ctx->stage_b, h_x, n);
+        int st = solve_impl(ctx, kind, A, pk, ph, ctx->stage_a.p, ctx->stage_b.p, &o, info);
+        stage_out(ctx, ctx->stage_b.p, h_x, n);
+        return st;
+    });
+}
+
+// ---------------------------------------------------------------------------
+int jfg_dense_solve(jfg_ctx* ctx, int n, const double* A, const double* b, double* x)
+{
+    if (!ctx || n < 0 || (n > 0 && (!A || !b || !x))) return JFG_ERR_BAD_ARG;
+    return guard(ctx, [&]() -> int {
+        DevBuf<double> dA;
+        dA.alloc((size_t)n * n);
+        JFG_CUDA(cudaMemcpyAsync(dA.p, A, sizeof(double) * n * n, cudaMemcpyHostToDevice, ctx->c.stream));
+        stage_in(ctx, ctx->stage_a, b, n);
+        ctx->stage_b.alloc(n);
+        int st = jfg::dense_solve_device(&ctx->c, n, dA.p, ctx->stage_a.p, ctx->stage_b.p);
+        if (st != JFG_OK) throw Error{st, "matrix is singular"};
+        stage_out(ctx, ctx->stage_b.p, x, n);
+        return JFG_OK;
+    });
+}
+
+int jfg_dense_inverse(jfg_ctx* ctx, int n, const double* A, double* Ainv)
+{
+    if (!ctx || n < 0 || (n > 0 && (!A || !Ainv))) return JFG_ERR_BAD_ARG;
+    return guard(ctx, [&]() -> int {
+        DevBuf<double> dA, dI;
+        dA.alloc((size_t)n * n);
+        dI.alloc((size_t)n * n);
+        JFG_CUDA(cudaMemcpyAsync(dA.p, A, sizeof(double) * n * n, cudaMemcpyHostToDevice, ctx->c.stream));
+        int st = jfg::dense_inverse_device(&ctx->c, n, dA.p, dI.p);
+        if (st != JFG_OK) throw Error{st, "matrix is singular"};
+        stage_out(ctx, dI.p, Ainv, (size_t)n * n);
+        return JFG_OK;
+    });
+}
+
+int jfg_sparse_solve(jfg_ctx* ctx, int n, int64_t nnz, const int* rows, const int* cols, const double* vals,
+                     const double* b, double* x)
+{
+    if (!ctx || n < 0 || nnz < 0 || (n > 0 && (!b || !x))) return JFG_ERR_BAD_ARG;
+    return guard(ctx, [&]() -> int {
+        jfg_mat* A = nullptr;
+        int st = jfg_matrix_from_coo(ctx, n, n, nnz, rows, cols, vals, &A);
+        if (st != JFG_OK) throw Error{st, ctx->c.last_error};
+        std::unique_ptr<jfg_mat, int (*)(jfg_mat*)> holder(A, jfg_matrix_free);
+        if (n <= 4096) {
+            // dense LU of the merged matrix (the reference's SparseMatrix.solve)
+            std::vector<double> dense((size_t)n * n, 0.0);
+            std::vector<int> ri(rows, rows + nnz), ci(cols, cols + nnz);
+            for (int64_t k = 0; k < nnz; k++) dense[(size_t)ri[k] * n + ci[k]] += vals[k];
+            return jfg_dense_solve(ctx, n, dense.data(), b, x);
+        }
+        jfg_solver_opts o;
+        jfg_solver_opts_default(&o);
+        double bn = 0;
+        for (int i = 0; i < n; i++) bn += b[i] * b[i];
+        o.tol = 1e-12 * std::sqrt(bn);
+        o.restart = 50;
+        o.max_restarts = 1000;
+        std::memset(x, 0, sizeof(double) * n);
+        jfg_solve_info info;
+        st = jfg_solve(ctx, JFG_PGMRES, A, JFG_PREC_JACOBI, nullptr, b, x, &o, &info);
+        if (st != JFG_OK) throw Error{st, ctx->c.last_error};
+        return (int)JFG_OK;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,146 @@
+// Shared definitions of the JFEM linear-solve library for sm_100a.
+//
+// Layout decisions (all device memory is owned by the library):
+//   * matrices live as a padded CSR whose row blocks start on 16-byte
+//     boundaries ("row-block CSR"): block b covers rows [rb[b], rb[b+1]) and
+//     its nonzeros [rowptr[rb[b]], rowptr[rb[b+1]]) with rowptr[rb[b]] a
+//     multiple of 4.  One CTA streams one row block with 128-bit loads into
+//     shared memory and reduces rows with LPR lanes per row;
+//   * values exist in FP64 and, on demand, FP32 (mixed-precision inner
+//     solves) -- both copies share the index arrays;
+//   * all scalars of an iterative solve (alpha, beta, <r,r>, flags, the
+//     iteration counter and the residual history) live in a device control
+//     block, so a whole Krylov iteration is a fixed kernel sequence that can be
+//     captured into a CUDA graph and replayed without host round trips.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+#include <atomic>
+#include <stdio.h>
+#include <string>
+#include <vector>
+
+#include "../../include/jfem_gpu.h"
+
+namespace jfg {
+
+constexpr int kThreads = 256;          // threads per CTA in streaming kernels
+constexpr int kBlockNnz = 2048;        // nonzeros staged per row block
+constexpr int kBlockRows = 256;        // rows per row block (<= kThreads)
+constexpr int kVecGrid = 148 * 8;      // fixed grid of the vector kernels (SM count x 8)
+
+struct Error {
+    int status;
+    std::string msg;
+};
+
+#define JFG_CUDA(call)                                                                     \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            throw ::jfg::Error{JFG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+    } while (0)
+
+#define JFG_CHECK(cond, code, text)                                                        \
+    do {                                                                                   \
+        if (!(cond)) throw ::jfg::Error{(code), (text)};                                   \
+    } while (0)
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count)
+    {
+        if (count <= n && p) return;
+        release();
+        JFG_CUDA(cudaMalloc(&p, (count ? count : 1) * sizeof(T)));
+        n = count;
+    }
+};
+
+// The control block of one iterative solve (device resident).
+struct Ctl {
+    double alpha, beta, omega, rho, rho_last;
+    double rr, rz, pAp;
+    double tol;             // absolute residual tolerance (the reference's `tol`)
+    double res_norm;        // latest published residual norm
+    double s_norm;          // BiCGStab: ||s||
+    double true_res;        // GMRES: ||A x - b|| after a cycle
+    int iter;               // iterations done (IterativeSolver.iterations)
+    int maxit;
+    int done;               // 1 = stop iterating
+    int status;             // jfg_status of the solve
+    int not_pd;             // CG met p.Ap <= 0
+    int sdone;              // BiCGStab: ||s|| < tol branch taken
+    int skip;               // BiCGStab: skip the second half of the iteration
+    int j;                  // GMRES: current Arnoldi index
+    int jfin;               // GMRES: index of the last column used
+    int cycle_done;         // GMRES: inner loop finished
+    int restart_len;        // GMRES: ITERATIONS_BEFORE_RESTART
+    int n;                  // problem size
+    int hist_cap;
+    double* hist;           // residual history (device)
+};
+
+struct Context;
+
+// Row-block CSR matrix on the device.
+struct Matrix {
+    Context* ctx = nullptr;
+    int rows = 0, cols = 0;
+    int64_t nnz = 0;              // stored nonzeros after merging (excl. padding)
+    int64_t nnz_padded = 0;       // length of col/val arrays
+    int nblocks = 0;
+    int lpr = 4;                  // lanes per row used in the reduction phase
+    DevBuf<int> rb;               // nblocks + 1 row-block starts
+    DevBuf<int> rowptr;           // rows + 1 (padded offsets)
+    DevBuf<int> col;              // nnz_padded
+    DevBuf<double> val;           // nnz_padded
+    DevBuf<float> val32;          // optional FP32 copy
+    DevBuf<__nv_bfloat16> val16;  // optional BF16 copy
+    DevBuf<double> diag;          // merged diagonal
+    int has32 = 0, has16 = 0;
+    Matrix* transposed = nullptr; // lazily built for tvMul
+    uint64_t uid = 0;             // unique id (keys of cached CUDA graphs)
+    Matrix();
+    ~Matrix();
+};
+
+struct Context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    // reduction scratch shared by the vector kernels of this context
+    DevBuf<double> partials;      // kVecGrid * 4 or nblocks * 4 doubles
+    DevBuf<unsigned> counters;    // last-block counters
+    DevBuf<double> scal;          // small scalar results
+};
+
+// host-side helpers implemented in jfg_matrix.cu
+Matrix* matrix_from_coo(Context* c, int rows, int cols, int64_t nnz, const int* ri, const int* ci,
+                        const double* v, bool keep_zeros);
+Matrix* matrix_from_csr_host(Context* c, int rows, int cols, const std::vector<int64_t>& rp,
+                             const std::vector<int>& ci, const std::vector<double>& v);
+Matrix* matrix_transpose(Matrix* m);
+void matrix_ensure_fp32(Matrix* m);
+void matrix_ensure_bf16(Matrix* m);
+uint64_t next_uid();
+
+// Kernels launched by this process (graph replays are added per executed
+// body); read through jfg_kernel_launches.
+extern std::atomic<unsigned long long> g_launches;
+inline void note_launch(unsigned long long k = 1) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+
+}  // namespace jfg

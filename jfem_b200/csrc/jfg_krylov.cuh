@@ -1,0 +1,63 @@
+// Krylov solvers on the device: shared declarations.
+#pragma once
+#include <functional>
+#include <map>
+#include <tuple>
+
+#include "jfg_mg.cuh"
+
+namespace jfg {
+
+template <typename T>
+struct Precond {
+    int kind = JFG_PREC_NONE;
+    MGImpl<T>* mg = nullptr;
+    Matrix* M = nullptr;
+    const T* dinv = nullptr;
+    int n = 0;
+    void apply(const T* r, T* z, const Scratch& sc, const int* done, cudaStream_t st) const;
+};
+
+// Runs `iter()` (which enqueues one iteration) until ctl->done is set,
+// either as a CUDA graph with a conditional WHILE node, as replayed graphs of
+// `chunk` iterations with a convergence poll in between, or as plain launches.
+struct GraphCache {
+    std::map<std::vector<uintptr_t>, cudaGraphExec_t> execs;
+    std::map<std::vector<uintptr_t>, int> nodes;     // kernel nodes per body
+    ~GraphCache();
+};
+
+struct SolverWork {
+    Context* c = nullptr;
+    DevBuf<Ctl> ctl;                // [0] outer / plain solve, [1] inner solve
+    DevBuf<double> hist;
+    DevBuf<double> partials;
+    DevBuf<unsigned> counter;
+    Scratch sc;
+    DevBuf<double> v64[12];         // FP64 work vectors
+    DevBuf<float> v32[8];           // FP32 work vectors
+    DevBuf<double> dinv64;
+    DevBuf<float> dinv32;
+    // GMRES
+    DevBuf<double> V, H, gam, cs, sn, fac, alpha, mdot_part;
+    int gm_m = 0;
+    GraphCache graphs;
+    void ensure(int n, int max_blocks, int hist_cap);
+};
+
+int run_loop(SolverWork& w, const int* flag, const std::vector<uintptr_t>& key, const std::function<void()>& iter,
+              int use_graph, int chunk);
+
+template <typename T>
+int run_cg(SolverWork& w, int ci, Matrix* A, const Precond<T>& M, const T* b, T* x, T* r, T* p, T* Ap, T* z,
+            bool xzero, int use_graph, int chunk);
+template <typename T>
+int run_bicgstab(SolverWork& w, int ci, Matrix* A, const Precond<T>& M, const T* b, T* x, T* const* v,
+                  int use_graph, int chunk);
+int run_gmres(SolverWork& w, Matrix* A, const Precond<double>& M, const double* b, double* x, int IBR,
+              int max_restarts, int use_graph, int chunk);
+int run_mixed_cg(SolverWork& w, Matrix* A, const Precond<float>& M, const double* b, double* x, double tol,
+                 int maxit, double inner_rtol, int use_graph, int chunk, int* inner_iters, double* hist, int hist_cap);
+uint64_t next_uid();
+
+}  // namespace jfg

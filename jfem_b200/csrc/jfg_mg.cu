@@ -1,0 +1,439 @@
+// Multigrid V-cycle, FMG and smoothers on the device.
+#include <algorithm>
+
+#include "jfg_mg.cuh"
+
+namespace jfg {
+
+namespace {
+
+template <typename T>
+__global__ void k_dinv(int n, const double* diag, T* dinv)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double d = diag[i];
+    if (fabs(d) < 1e-10) d = 1;          // JacobiSmoother.java:21-22
+    dinv[i] = (T)(1.0 / d);
+}
+
+__global__ void k_mask(int nb, const int* bd, unsigned char* mask)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nb) mask[bd[i]] = 1;
+}
+
+template <typename T>
+__global__ void k_cast(int64_t n, const double* a, T* b)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (T)a[i];
+}
+
+// x = Ainv * rhs with FP64 arithmetic; one warp per row.
+template <typename T>
+__global__ void k_coarse_gemv(int n, const double* __restrict__ ainv, const T* __restrict__ rhs, T* __restrict__ x,
+                              const int* __restrict__ done)
+{
+    if (done && *done) return;
+    int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    double s = 0;
+    for (int j = lane; j < n; j += 32) s += ainv[(size_t)row * n + j] * (double)rhs[j];
+    s = warp_sum(s);
+    if (lane == 0) x[row] = (T)s;
+}
+
+// defect rows touched by boundary columns: d[r] = v[r] - sum_j A[r, j] v[j]
+template <typename T>
+__global__ void k_bc_defect(int naff, const int* __restrict__ row, const int* __restrict__ ptr,
+                            const int* __restrict__ col, const T* __restrict__ val, const T* __restrict__ v,
+                            T* __restrict__ d, const int* __restrict__ done)
+{
+    if (done && *done) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= naff) return;
+    int r = row[i];
+    T s = 0;
+    for (int k = ptr[i]; k < ptr[i + 1]; k++) s += val[k] * v[col[k]];
+    d[r] = v[r] - s;
+}
+
+// out[bd] += v[bd]   (initial.add(iterate), initial = boundary copy of v)
+template <typename T>
+__global__ void k_bc_add(int nb, const int* __restrict__ bd, const T* __restrict__ v, T* __restrict__ out,
+                         const int* __restrict__ done)
+{
+    if (done && *done) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nb) out[bd[i]] = v[bd[i]] + out[bd[i]];
+}
+
+// Richardson update x += omega * r unless the level flag says "smooth"
+template <typename T>
+struct VRichardson {
+    const T* r;
+    T* x;
+    T omega;
+    const int* flag;
+    template <int K> __device__ void operator()(int i, double (&)[K]) const
+    {
+        if (*flag) return;
+        x[i] = x[i] + r[i] * omega;
+    }
+};
+
+struct FinSmoothFlag {  // RichardsonSmoother.java:33-38: stop when ||r|| < 1e-10
+    int* flag;
+    __device__ void operator()(const double* t) const { *flag = sqrt(t[0]) < 1e-10 ? 1 : 0; }
+};
+
+inline unsigned nb(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+template <typename T>
+void MGImpl<T>::init(Context* ctx, int levels, Matrix* const* As, Matrix* const* Ps, const int* const* bdry,
+                     const int* nbdry, const SmootherDesc* sms, int cycles_, int use_fmg_)
+{
+    c = ctx;
+    L = levels;
+    cycles = cycles_;
+    use_fmg = use_fmg_;
+    cudaStream_t st = c->stream;
+    A.assign(As, As + L);
+    P.assign(L, nullptr);
+    R.assign(L, nullptr);
+    n.resize(L);
+    sm.assign(sms, sms + L);
+    x = std::vector<DevBuf<T>>(L);
+    t = std::vector<DevBuf<T>>(L);
+    b = std::vector<DevBuf<T>>(L);
+    r = std::vector<DevBuf<T>>(L);
+    fr = std::vector<DevBuf<T>>(L);
+    dinv = std::vector<DevBuf<T>>(L);
+    mask = std::vector<DevBuf<unsigned char>>(L);
+    for (int l = 0; l < L; l++) {
+        JFG_CHECK(A[l] && A[l]->rows == A[l]->cols, JFG_ERR_BAD_ARG, "level matrix missing or not square");
+        n[l] = A[l]->rows;
+        if (l < L - 1) {
+            P[l] = Ps[l];
+            JFG_CHECK(P[l], JFG_ERR_BAD_ARG, "prolongation missing");
+            JFG_CHECK(P[l]->rows == As[l + 1]->rows && P[l]->cols == As[l]->rows, JFG_ERR_BAD_ARG,
+                      "prolongation shape does not match the level sizes");
+            R[l] = matrix_transpose(P[l]);
+        }
+        if (std::is_same<T, float>::value) {
+            matrix_ensure_fp32(A[l]);
+            if (l < L - 1) {
+                matrix_ensure_fp32(P[l]);
+                matrix_ensure_fp32(R[l]);
+            }
+        }
+        size_t m = (size_t)n[l];
+        x[l].alloc(m);
+        t[l].alloc(m);
+        b[l].alloc(m);
+        r[l].alloc(m);
+        fr[l].alloc(m);
+        dinv[l].alloc(m);
+        mask[l].alloc(m);
+        if (m) {
+            k_dinv<T><<<nb(m), 256, 0, st>>>((int)m, A[l]->diag.p, dinv[l].p);
+            JFG_CUDA(cudaMemsetAsync(mask[l].p, 0, m, st));
+            JFG_CUDA(cudaMemsetAsync(x[l].p, 0, m * sizeof(T), st));
+        }
+        JFG_CHECK(nbdry[l] >= 0 && (nbdry[l] == 0 || bdry[l]), JFG_ERR_BAD_ARG, "bad boundary list");
+        for (int i = 0; i < nbdry[l]; i++)
+            JFG_CHECK(bdry[l][i] >= 0 && bdry[l][i] < n[l], JFG_ERR_BAD_ARG, "boundary node out of range");
+        if (nbdry[l]) {
+            DevBuf<int> d_bd;
+            d_bd.alloc(nbdry[l]);
+            JFG_CUDA(cudaMemcpyAsync(d_bd.p, bdry[l], sizeof(int) * nbdry[l], cudaMemcpyHostToDevice, st));
+            k_mask<<<nb(nbdry[l]), 256, 0, st>>>(nbdry[l], d_bd.p, mask[l].p);
+            JFG_CUDA(cudaStreamSynchronize(st));
+        }
+        JFG_CUDA(cudaGetLastError());
+    }
+    // finest boundary list and the rows with entries in boundary columns
+    int Lf = L - 1;
+    nbd_fine = nbdry[Lf];
+    bd_fine.alloc(nbd_fine ? nbd_fine : 1);
+    if (nbd_fine)
+        JFG_CUDA(cudaMemcpyAsync(bd_fine.p, bdry[Lf], sizeof(int) * nbd_fine, cudaMemcpyHostToDevice, st));
+    {
+        Matrix* Af = A[Lf];
+        std::vector<int> hp(Af->rows + 1);
+        std::vector<int> hc((size_t)Af->nnz_padded);
+        std::vector<double> hv((size_t)Af->nnz_padded);
+        JFG_CUDA(cudaMemcpyAsync(hp.data(), Af->rowptr.p, sizeof(int) * (Af->rows + 1), cudaMemcpyDeviceToHost, st));
+        JFG_CUDA(cudaMemcpyAsync(hc.data(), Af->col.p, sizeof(int) * Af->nnz_padded, cudaMemcpyDeviceToHost, st));
+        JFG_CUDA(cudaMemcpyAsync(hv.data(), Af->val.p, sizeof(double) * Af->nnz_padded, cudaMemcpyDeviceToHost, st));
+        JFG_CUDA(cudaStreamSynchronize(st));
+        std::vector<char> isbd(Af->rows, 0);
+        for (int i = 0; i < nbd_fine; i++) isbd[bdry[Lf][i]] = 1;
+        std::vector<int> arow, aptr{0}, acol;
+        std::vector<T> aval;
+        for (int rr = 0; rr < Af->rows; rr++) {
+            bool any = false;
+            for (int k = hp[rr]; k < hp[rr + 1]; k++)
+                if (hv[k] != 0.0 && isbd[hc[k]]) {
+                    acol.push_back(hc[k]);
+                    aval.push_back((T)hv[k]);
+                    any = true;
+                }
+            if (any) {
+                arow.push_back(rr);
+                aptr.push_back((int)acol.size());
+            }
+        }
+        naff = (int)arow.size();
+        aff_row.alloc(naff ? naff : 1);
+        aff_ptr.alloc(naff + 1);
+        aff_col.alloc(acol.size() ? acol.size() : 1);
+        aff_val.alloc(aval.size() ? aval.size() : 1);
+        if (naff) {
+            JFG_CUDA(cudaMemcpyAsync(aff_row.p, arow.data(), sizeof(int) * naff, cudaMemcpyHostToDevice, st));
+            JFG_CUDA(cudaMemcpyAsync(aff_ptr.p, aptr.data(), sizeof(int) * (naff + 1), cudaMemcpyHostToDevice, st));
+            JFG_CUDA(cudaMemcpyAsync(aff_col.p, acol.data(), sizeof(int) * acol.size(), cudaMemcpyHostToDevice, st));
+            JFG_CUDA(cudaMemcpyAsync(aff_val.p, aval.data(), sizeof(T) * aval.size(), cudaMemcpyHostToDevice, st));
+        }
+        JFG_CUDA(cudaStreamSynchronize(st));
+    }
+    // coarsest level: dense inverse computed on the device in FP64
+    int n0 = n[0];
+    ainv0.alloc((size_t)n0 * n0);
+    {
+        DevBuf<double> dense;
+        dense.alloc((size_t)n0 * n0);
+        JFG_CUDA(cudaMemsetAsync(dense.p, 0, sizeof(double) * n0 * n0, st));
+        // scatter the level-0 CSR into the dense array
+        std::vector<int> hp(n0 + 1);
+        std::vector<int> hc((size_t)A[0]->nnz_padded);
+        std::vector<double> hv((size_t)A[0]->nnz_padded);
+        JFG_CUDA(cudaMemcpyAsync(hp.data(), A[0]->rowptr.p, sizeof(int) * (n0 + 1), cudaMemcpyDeviceToHost, st));
+        JFG_CUDA(cudaMemcpyAsync(hc.data(), A[0]->col.p, sizeof(int) * A[0]->nnz_padded, cudaMemcpyDeviceToHost, st));
+        JFG_CUDA(cudaMemcpyAsync(hv.data(), A[0]->val.p, sizeof(double) * A[0]->nnz_padded, cudaMemcpyDeviceToHost, st));
+        JFG_CUDA(cudaStreamSynchronize(st));
+        std::vector<double> hd((size_t)n0 * n0, 0.0);
+        for (int rr = 0; rr < n0; rr++)
+            for (int k = hp[rr]; k < hp[rr + 1]; k++) hd[(size_t)rr * n0 + hc[k]] += hv[k];
+        JFG_CUDA(cudaMemcpyAsync(dense.p, hd.data(), sizeof(double) * hd.size(), cudaMemcpyHostToDevice, st));
+        coarse_status = dense_inverse_device(c, n0, dense.p, ainv0.p);
+    }
+    flags.alloc(L);
+    zero_flag.alloc(1);
+    JFG_CUDA(cudaMemsetAsync(flags.p, 0, sizeof(int) * L, st));
+    JFG_CUDA(cudaMemsetAsync(zero_flag.p, 0, sizeof(int), st));
+    JFG_CUDA(cudaStreamSynchronize(st));
+}
+
+template <typename T>
+int MGImpl<T>::max_blocks() const
+{
+    int m = kVecGrid;
+    for (int l = 0; l < L; l++) {
+        m = std::max(m, A[l]->nblocks);
+        if (P[l]) m = std::max(m, P[l]->nblocks);
+        if (R[l]) m = std::max(m, R[l]->nblocks);
+    }
+    return m;
+}
+
+template <typename T>
+void MGImpl<T>::coarse(const T* rhs, T* out, const int* done, cudaStream_t st)
+{
+    int n0 = n[0];
+    k_coarse_gemv<T><<<(n0 + 7) / 8, 256, 0, st>>>(n0, ainv0.p, rhs, out, done);
+    JFG_CUDA(cudaGetLastError());
+    note_launch();
+}
+
+// Smoother.smooth on level l with rhs; the result ends in x[l].
+template <typename T>
+void MGImpl<T>::smooth(int l, const T* rhs, bool xzero, const Scratch& sc, const int* done, cudaStream_t st)
+{
+    const SmootherDesc& d = sm[l];
+    Matrix* M = A[l];
+    const T* val = vals_of<T>(M);
+    int m = n[l];
+    if (d.runs <= 0) {
+        if (xzero) vec_launch<0>(st, m, VZero<T>{x[l].p}, sc, done);
+        return;
+    }
+    if (d.kind == JFG_SMOOTH_JACOBI) {
+        T om = (T)d.omega;
+        int k = 0;
+        T* cur = x[l].p;
+        T* alt = t[l].p;
+        if (xzero) {
+            // first sweep from zero: x = (dinv * b) * omega; choose its target so
+            // that the last sweep lands in x[l]
+            T* dst = (d.runs % 2 == 1) ? x[l].p : t[l].p;
+            vec_launch<0>(st, m, VScaleMul<T>{dinv[l].p, rhs, dst, om}, sc, done);
+            cur = dst;
+            alt = (dst == x[l].p) ? t[l].p : x[l].p;
+            k = 1;
+        }
+        for (; k < d.runs; k++) {
+            spmv_launch<T, T, 0>(st, M, val, cur, EpiJacobi<T>{cur, rhs, dinv[l].p, alt, om}, sc, done);
+            std::swap(cur, alt);
+        }
+        if (cur != x[l].p) vec_launch<0>(st, m, VCopy<T>{cur, x[l].p}, sc, done);
+    } else {
+        if (xzero) vec_launch<0>(st, m, VZero<T>{x[l].p}, sc, done);
+        for (int k = 0; k < d.runs; k++) {
+            spmv_launch<T, T, 1>(st, M, val, x[l].p, EpiResid<T>{rhs, r[l].p}, sc, done,
+                                 FinSmoothFlag{flags.p + l});
+            vec_launch<0>(st, m, VRichardson<T>{r[l].p, x[l].p, (T)d.omega, flags.p + l}, sc, done);
+        }
+    }
+}
+
+// mgStepV (MGPreconditionerInterface.java:125-198): guess in x[l] (or zero),
+// rhs given; result in x[l].
+template <typename T>
+void MGImpl<T>::vstep(int l, const T* rhs, bool xzero, const Scratch& sc, const int* done, cudaStream_t st)
+{
+    if (l == 0) {
+        coarse(rhs, x[0].p, done, st);
+        return;
+    }
+    smooth(l, rhs, xzero, sc, done, st);
+    spmv_launch<T, T, 0>(st, A[l], vals_of<T>(A[l]), x[l].p, EpiResid<T>{rhs, r[l].p}, sc, done);
+    spmv_launch<T, T, 0>(st, R[l - 1], vals_of<T>(R[l - 1]), r[l].p, EpiMasked<T>{mask[l - 1].p, b[l - 1].p}, sc,
+                         done);
+    vstep(l - 1, b[l - 1].p, true, sc, done, st);
+    spmv_launch<T, T, 0>(st, P[l - 1], vals_of<T>(P[l - 1]), x[l - 1].p, EpiMaskedAdd<T>{mask[l].p, x[l].p}, sc,
+                         done);
+    smooth(l, rhs, false, sc, done, st);
+}
+
+// fullVCycleCorrection (MGPreconditionerInterface.java:307-326); result in x[L-1].
+template <typename T>
+void MGImpl<T>::fmg_into_top(const T* defect, const Scratch& sc, const int* done, cudaStream_t st)
+{
+    std::vector<const T*> rh(L);
+    rh[L - 1] = defect;
+    for (int l = L - 2; l >= 0; l--) {
+        spmv_launch<T, T, 0>(st, R[l], vals_of<T>(R[l]), rh[l + 1], EpiMasked<T>{mask[l].p, fr[l].p}, sc, done);
+        rh[l] = fr[l].p;
+    }
+    for (int l = 0; l < L - 1; l++) {
+        vstep(l, rh[l], false, sc, done, st);
+        // raw prolongation without boundary zeroing (getProlongationMatrix, line 323)
+        spmv_launch<T, T, 0>(st, P[l], vals_of<T>(P[l]), x[l].p, EpiStore<T>{x[l + 1].p}, sc, done);
+    }
+}
+
+template <typename T>
+void MGImpl<T>::apply(const T* v, T* out, const Scratch& sc, const int* done, cudaStream_t st)
+{
+    int Lf = L - 1, m = n[Lf];
+    T* defect = b[Lf].p;
+    vec_launch<0>(st, m, VCopy<T>{v, defect}, sc, done);
+    if (naff) {
+        k_bc_defect<T><<<nb(naff), 256, 0, st>>>(naff, aff_row.p, aff_ptr.p, aff_col.p, aff_val.p, v, defect, done);
+        JFG_CUDA(cudaGetLastError());
+        note_launch();
+    }
+    bool xzero = true;
+    if (use_fmg && L > 1) {
+        fmg_into_top(defect, sc, done, st);
+        xzero = false;
+    } else if (use_fmg && L == 1) {
+        coarse(defect, x[0].p, done, st);
+        xzero = false;
+    }
+    if (L == 1) {
+        for (int cyc = 0; cyc < cycles; cyc++) coarse(defect, x[0].p, done, st);
+        if (cycles == 0 && xzero) vec_launch<0>(st, m, VZero<T>{x[0].p}, sc, done);
+    } else {
+        for (int cyc = 0; cyc < cycles; cyc++) {
+            vstep(Lf, defect, xzero, sc, done, st);
+            xzero = false;
+        }
+        if (xzero) vec_launch<0>(st, m, VZero<T>{x[Lf].p}, sc, done);
+    }
+    vec_launch<0>(st, m, VCopy<T>{x[Lf].p, out}, sc, done);
+    if (nbd_fine) {
+        k_bc_add<T><<<nb(nbd_fine), 256, 0, st>>>(nbd_fine, bd_fine.p, v, out, done);
+        JFG_CUDA(cudaGetLastError());
+        note_launch();
+    }
+}
+
+template <typename T>
+void MGImpl<T>::vcycle(const T* x0, const T* rhs, T* out, const Scratch& sc, const int* done, cudaStream_t st)
+{
+    int Lf = L - 1, m = n[Lf];
+    vec_launch<0>(st, m, VCopy<T>{rhs, b[Lf].p}, sc, done);
+    vec_launch<0>(st, m, VCopy<T>{x0, x[Lf].p}, sc, done);
+    vstep(Lf, b[Lf].p, false, sc, done, st);
+    vec_launch<0>(st, m, VCopy<T>{x[Lf].p, out}, sc, done);
+}
+
+template <typename T>
+void MGImpl<T>::fmg(const T* defect, T* out, const Scratch& sc, const int* done, cudaStream_t st)
+{
+    int Lf = L - 1, m = n[Lf];
+    vec_launch<0>(st, m, VCopy<T>{defect, b[Lf].p}, sc, done);
+    if (L == 1) {
+        coarse(b[0].p, x[0].p, done, st);
+    } else {
+        fmg_into_top(b[Lf].p, sc, done, st);
+    }
+    vec_launch<0>(st, m, VCopy<T>{x[Lf].p, out}, sc, done);
+}
+
+template struct MGImpl<double>;
+template struct MGImpl<float>;
+
+void smooth_standalone(Context* c, Matrix* A, const SmootherDesc& d, const double* rhs, double* xv, const Scratch& sc)
+{
+    cudaStream_t st = c->stream;
+    int m = A->rows;
+    DevBuf<double> dinv, t, r;
+    DevBuf<int> flag;
+    dinv.alloc(m);
+    t.alloc(m);
+    r.alloc(m);
+    flag.alloc(1);
+    if (m) k_dinv<double><<<nb(m), 256, 0, st>>>(m, A->diag.p, dinv.p);
+    JFG_CUDA(cudaGetLastError());
+    if (d.kind == JFG_SMOOTH_JACOBI) {
+        double* cur = xv;
+        double* alt = t.p;
+        for (int k = 0; k < d.runs; k++) {
+            spmv_launch<double, double, 0>(st, A, A->val.p, cur, EpiJacobi<double>{cur, rhs, dinv.p, alt, d.omega},
+                                           sc, nullptr);
+            std::swap(cur, alt);
+        }
+        if (cur != xv) vec_launch<0>(st, m, VCopy<double>{cur, xv}, sc, nullptr);
+    } else {
+        for (int k = 0; k < d.runs; k++) {
+            spmv_launch<double, double, 1>(st, A, A->val.p, xv, EpiResid<double>{rhs, r.p}, sc, nullptr,
+                                           FinSmoothFlag{flag.p});
+            vec_launch<0>(st, m, VRichardson<double>{r.p, xv, d.omega, flag.p}, sc, nullptr);
+        }
+    }
+    JFG_CUDA(cudaStreamSynchronize(st));
+}
+
+}  // namespace jfg
+
+jfg::MGImpl<float>* jfg_mg::fp32()
+{
+    if (!d32) {
+        std::vector<const int*> bp(levels);
+        std::vector<int> nbp(levels);
+        for (int l = 0; l < levels; l++) {
+            bp[l] = bdry[l].data();
+            nbp[l] = (int)bdry[l].size();
+        }
+        d32.reset(new jfg::MGImpl<float>());
+        d32->init(ctx, levels, A.data(), P.data(), bp.data(), nbp.data(), sm.data(), cycles, use_fmg);
+    }
+    return d32.get();
+}

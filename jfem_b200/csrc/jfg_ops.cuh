@@ -1,0 +1,167 @@
+// Epilogue functors for the row-block SpMV, vector functors, and the launch
+// helpers shared by the multigrid and Krylov code.
+#pragma once
+#include "jfg_kernels.cuh"
+
+namespace jfg {
+
+// Reduction scratch of one solve / one context: partial sums and a counter.
+struct Scratch {
+    double* partials = nullptr;   // >= 4 * max(grid) doubles
+    unsigned* counter = nullptr;
+};
+
+inline int ilog2(int v)
+{
+    int l = 0;
+    while ((1 << (l + 1)) <= v) l++;
+    return l;
+}
+
+template <typename T> const T* vals_of(const Matrix* M);
+template <> inline const double* vals_of<double>(const Matrix* M) { return M->val.p; }
+template <> inline const float* vals_of<float>(const Matrix* M) { return M->val32.p; }
+
+// ---------------------------------------------------------------------------
+// SpMV epilogues (row r, row sum s)
+// ---------------------------------------------------------------------------
+template <typename T>
+struct EpiStore {  // y = A x
+    T* y;
+    template <typename AT, int K>
+    __device__ void operator()(int r, AT s, double (&)[K]) const { y[r] = (T)s; }
+};
+
+template <typename T>
+struct EpiStoreDot {  // y = A p, acc += p . y
+    T* y;
+    const T* p;
+    template <typename AT, int K>
+    __device__ void operator()(int r, AT s, double (&acc)[K]) const
+    {
+        y[r] = (T)s;
+        acc[0] += (double)p[r] * (double)s;
+    }
+};
+
+template <typename T>
+struct EpiResid {  // y = b - A x, acc += y^2
+    const T* b;
+    T* y;
+    template <typename AT, int K>
+    __device__ void operator()(int r, AT s, double (&acc)[K]) const
+    {
+        T v = b[r] - (T)s;
+        y[r] = v;
+        acc[0] += (double)v * (double)v;
+    }
+};
+
+template <typename T>
+struct EpiJacobi {  // xn = x + (dinv * (b - A x)) * omega   (JacobiSmoother.java:38-42)
+    const T* x;
+    const T* b;
+    const T* dinv;
+    T* xn;
+    T omega;
+    template <typename AT, int K>
+    __device__ void operator()(int r, AT s, double (&)[K]) const
+    {
+        xn[r] = x[r] + (dinv[r] * (b[r] - (T)s)) * omega;
+    }
+};
+
+template <typename T>
+struct EpiMasked {  // y = mask ? 0 : A x  (transfer followed by zero boundary values)
+    const unsigned char* mask;
+    T* y;
+    template <typename AT, int K>
+    __device__ void operator()(int r, AT s, double (&)[K]) const { y[r] = mask[r] ? (T)0 : (T)s; }
+};
+
+template <typename T>
+struct EpiMaskedAdd {  // x += mask ? 0 : A e   (prolongation + correction, MGPreconditionerInterface.java:171-174)
+    const unsigned char* mask;
+    T* x;
+    template <typename AT, int K>
+    __device__ void operator()(int r, AT s, double (&)[K]) const
+    {
+        x[r] = x[r] + (mask[r] ? (T)0 : (T)s);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// launch helpers
+// ---------------------------------------------------------------------------
+template <typename VT, typename XT, int NR, class Epi, class Fin = NoFin>
+void spmv_launch(cudaStream_t st, const Matrix* M, const VT* val, const XT* x, Epi epi, const Scratch& sc,
+                 const int* done, Fin fin = Fin())
+{
+    if (M->rows == 0) return;
+    GridRed<NR, Fin> red{sc.partials, sc.counter, fin};
+    SpmvArgs a{M->rb.p, M->rowptr.p, M->col.p};
+    k_spmv<VT, XT, NR, Epi, Fin><<<M->nblocks, kThreads, 0, st>>>(a, val, x, ilog2(M->lpr), epi, red, done);
+    JFG_CUDA(cudaGetLastError());
+    note_launch();
+}
+
+inline int vec_grid(int n)
+{
+    int g = (n + kThreads - 1) / kThreads;
+    return g < 1 ? 1 : (g > kVecGrid ? kVecGrid : g);
+}
+
+template <int NR, class F, class Fin = NoFin>
+void vec_launch(cudaStream_t st, int n, F f, const Scratch& sc, const int* done, Fin fin = Fin())
+{
+    GridRed<NR, Fin> red{sc.partials, sc.counter, fin};
+    k_vec<NR, F, Fin><<<vec_grid(n), kThreads, 0, st>>>(n, f, red, done);
+    JFG_CUDA(cudaGetLastError());
+    note_launch();
+}
+
+template <class F>
+void scalar_launch(cudaStream_t st, F f, const int* done)
+{
+    k_scalar<F><<<1, 1, 0, st>>>(f, done);
+    JFG_CUDA(cudaGetLastError());
+    note_launch();
+}
+
+// ---------------------------------------------------------------------------
+// vector functors
+// ---------------------------------------------------------------------------
+template <typename T>
+struct VCopy {
+    const T* a;
+    T* b;
+    template <int K> __device__ void operator()(int i, double (&)[K]) const { b[i] = a[i]; }
+};
+template <typename T>
+struct VZero {
+    T* a;
+    template <int K> __device__ void operator()(int i, double (&)[K]) const { a[i] = (T)0; }
+};
+template <typename T>
+struct VDot {
+    const T* a;
+    const T* b;
+    template <int K> __device__ void operator()(int i, double (&acc)[K]) const { acc[0] += (double)a[i] * (double)b[i]; }
+};
+template <typename T>
+struct VScaleMul {  // y = (dinv * b) * omega      (first Jacobi sweep from a zero guess)
+    const T* dinv;
+    const T* b;
+    T* y;
+    T omega;
+    template <int K> __device__ void operator()(int i, double (&)[K]) const { y[i] = (T)0 + (dinv[i] * b[i]) * omega; }
+};
+template <typename T>
+struct VMul {  // y = d * x
+    const T* d;
+    const T* x;
+    T* y;
+    template <int K> __device__ void operator()(int i, double (&)[K]) const { y[i] = d[i] * x[i]; }
+};
+
+}  // namespace jfg

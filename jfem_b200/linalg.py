@@ -1,0 +1,380 @@
+"""Host-side mirror of JFEM's linalg API over the CUDA library.
+
+Names, argument meaning and error behaviour follow the Java classes
+(Core/src/main/java/linalg/...): ``SparseMatrix`` (COO triples with
+duplicates, ``add``/``set``/``mvMul``/``tvMul``/``solve``), ``DenseMatrix``
+(``solve``/``inverse``), ``IterativeSolver`` (``solveCG``, ``solvePCG``,
+``solveGMRES``, ``solvePGMRES``, ``solveBiCGStab``, ``solvePBiCGStab`` with the
+public fields ``iterations``, ``showProgress`` and the warm start
+``lastSolution``) and ``GMRES`` (``ITERATIONS_BEFORE_RESTART``,
+``MAX_RESTARTS``).  Vectors are numpy float64 arrays.  Every product and solve
+runs in libjfem_gpu.so; nothing here computes on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+
+
+class IllegalArgumentException(ValueError):
+    """Raised where the Java code throws IllegalArgumentException."""
+
+
+class SingularMatrixException(ArithmeticError):
+    """The dense solve failed (the JNI layer returns null, sparseSolver.cpp:43-52)."""
+
+
+class VectorMultiplyable:
+    """linalg/VectorMultiplyable.java:8-17."""
+
+    def getVectorSize(self) -> int:
+        raise NotImplementedError
+
+    def getTVectorSize(self) -> int:
+        raise NotImplementedError
+
+    def mvMul(self, vector):
+        raise NotImplementedError
+
+    def tvMul(self, vector):
+        raise NotImplementedError
+
+
+class SparseMatrix(VectorMultiplyable):
+    """COO matrix (linalg/SparseMatrix.java).  Triples are kept in storage
+    order on the host as the reference keeps them; the device copy (merged,
+    row-block CSR) is built on first use and rebuilt after a modification."""
+
+    def __init__(self, rows: int, cols: int, ctx: N.Context | None = None):
+        self.rows, self.cols = int(rows), int(cols)
+        self._ri: list = []
+        self._ci: list = []
+        self._v: list = []
+        self._arrays = None
+        self._dev = None
+        self._ctx = ctx
+
+    # -- construction ------------------------------------------------------
+    @classmethod
+    def from_coo(cls, rows, cols, row_idx, col_idx, vals, ctx=None):
+        m = cls(rows, cols, ctx)
+        ri, ci, v = N.i32(row_idx), N.i32(col_idx), N.f64(vals)
+        if not (ri.size == ci.size == v.size):
+            raise IllegalArgumentException("COO arrays differ in length")
+        if ri.size and (ri.min() < 0 or ri.max() >= rows or ci.min() < 0 or ci.max() >= cols):
+            raise IllegalArgumentException("coordinate out of bounds")
+        m._arrays = (ri, ci, v)
+        return m
+
+    @classmethod
+    def identity(cls, n, ctx=None):
+        i = np.arange(n, dtype=np.int32)
+        return cls.from_coo(n, n, i, i, np.ones(n), ctx)
+
+    def _flush(self):
+        if self._ri:
+            add = (np.array(self._ri, np.int32), np.array(self._ci, np.int32), np.array(self._v, np.float64))
+            if self._arrays is None:
+                self._arrays = add
+            else:
+                self._arrays = tuple(np.concatenate([a, b]) for a, b in zip(self._arrays, add))
+            self._ri, self._ci, self._v = [], [], []
+        if self._arrays is None:
+            self._arrays = (np.zeros(0, np.int32), np.zeros(0, np.int32), np.zeros(0))
+
+    def coo(self):
+        self._flush()
+        return self._arrays
+
+    def add(self, value, row, col):
+        """SparseMatrix.add (SparseMatrix.java:274-294): appends a triple; zero values are skipped."""
+        if not (0 <= row < self.rows):
+            raise IllegalArgumentException(f"y coordinate out of bounds{row} with rows: {self.rows}")
+        if not (0 <= col < self.cols):
+            raise IllegalArgumentException("x coordinate out of bounds")
+        if value == 0:
+            return
+        self._ri.append(row)
+        self._ci.append(col)
+        self._v.append(float(value))
+        self._dev = None
+
+    def at(self, row, col):
+        ri, ci, v = self.coo()
+        return float(v[(ri == row) & (ci == col)].sum())
+
+    def set(self, value, row, col):
+        """SparseMatrix.set (:260-271): appends value - at(row, col)."""
+        d = value - self.at(row, col)
+        self._ri.append(row)
+        self._ci.append(col)
+        self._v.append(float(d))
+        self._dev = None
+
+    def getRows(self):
+        return self.rows
+
+    def getCols(self):
+        return self.cols
+
+    def getVectorSize(self):
+        return self.cols
+
+    def getTVectorSize(self):
+        return self.rows
+
+    def getSparseEntryCount(self):
+        return int(self.coo()[0].size)
+
+    # -- device side ---------------------------------------------------------
+    def device(self) -> "DeviceMatrix":
+        if self._dev is None:
+            ri, ci, v = self.coo()
+            self._dev = DeviceMatrix(self.rows, self.cols, ri, ci, v, self._ctx)
+        return self._dev
+
+    def mvMul(self, vector):
+        """SparseMatrix.mvMul (:480-489) -- IllegalArgumentException on size mismatch."""
+        x = N.f64(vector)
+        if x.shape != (self.cols,):
+            raise IllegalArgumentException("Incompatible sizes")
+        return self.device().spmv(x)
+
+    def tvMul(self, vector):
+        x = N.f64(vector)
+        if x.shape != (self.rows,):
+            raise IllegalArgumentException("Incompatible sizes")
+        return self.device().spmv_t(x)
+
+    def diag(self):
+        return self.device().diag()
+
+    def solve(self, rhs):
+        """SparseMatrix.solve (:142-145): the drop-in direct solve.  n <= 4096:
+        dense LU on the GPU (the reference densifies and factorises too);
+        larger: GPU GMRES to a 1e-12 relative residual."""
+        if self.rows != self.cols:
+            raise IllegalArgumentException("matrix is not square")
+        b = N.f64(rhs)
+        if b.shape != (self.rows,):
+            raise IllegalArgumentException("Incompatible sizes")
+        ctx = self._ctx or N.default_context()
+        ri, ci, v = self.coo()
+        x = np.zeros(self.rows)
+        st = N.load().jfg_sparse_solve(ctx.handle, self.rows, v.size, N.iptr(ri), N.iptr(ci), N.dptr(v),
+                                       N.dptr(b), N.dptr(x))
+        if st == N.ERR_SINGULAR:
+            raise SingularMatrixException(N.load().jfg_last_error(ctx.handle).decode())
+        ctx.check(st)
+        return x
+
+
+class DeviceMatrix:
+    """A matrix resident on the GPU (jfg_mat)."""
+
+    def __init__(self, rows, cols, ri, ci, v, ctx=None):
+        self.ctx = ctx or N.default_context()
+        self.rows, self.cols = int(rows), int(cols)
+        ri, ci, v = N.i32(ri), N.i32(ci), N.f64(v)
+        h = C.c_void_p()
+        st = N.load().jfg_matrix_from_coo(self.ctx.handle, self.rows, self.cols, v.size, N.iptr(ri), N.iptr(ci),
+                                          N.dptr(v), C.byref(h))
+        if st == N.ERR_BAD_ARG:
+            raise IllegalArgumentException(N.load().jfg_last_error(self.ctx.handle).decode())
+        self.ctx.check(st)
+        self._h = h
+        r, c, nz = C.c_int(), C.c_int(), C.c_int64()
+        N.load().jfg_matrix_info(h, C.byref(r), C.byref(c), C.byref(nz))
+        self.nnz = nz.value
+
+    @property
+    def handle(self):
+        return self._h
+
+    def spmv(self, x):
+        x = N.f64(x)
+        y = np.empty(self.rows)
+        self.ctx.check(N.load().jfg_spmv(self._h, N.dptr(x), N.dptr(y)))
+        return y
+
+    def spmv_t(self, x):
+        x = N.f64(x)
+        y = np.empty(self.cols)
+        self.ctx.check(N.load().jfg_spmv_t(self._h, N.dptr(x), N.dptr(y)))
+        return y
+
+    def diag(self):
+        d = np.empty(min(self.rows, self.cols))
+        self.ctx.check(N.load().jfg_matrix_diag(self._h, N.dptr(d)))
+        return d
+
+    def time_spmv(self, precision=0, iters=50):
+        ms = C.c_double()
+        self.ctx.check(N.load().jfg_spmv_time(self._h, precision, iters, C.byref(ms)))
+        return ms.value
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                N.load().jfg_matrix_free(self._h)
+        except Exception:
+            pass
+
+
+class DenseMatrix:
+    """linalg/DenseMatrix.java: dense solve and inverse (UJMP there, GPU LU here)."""
+
+    def __init__(self, a, ctx=None):
+        self.a = np.array(a, dtype=np.float64)
+        if self.a.ndim != 2:
+            raise IllegalArgumentException("not a matrix")
+        self.ctx = ctx or N.default_context()
+
+    @classmethod
+    def squareMatrixFromValues(cls, *values):
+        n = int(round(len(values) ** 0.5))
+        if n * n != len(values):
+            raise IllegalArgumentException("nope")
+        return cls(np.array(values, dtype=np.float64).reshape(n, n))
+
+    def mvMul(self, v):
+        return self.a @ N.f64(v)
+
+    def solve(self, rhs):
+        n = self.a.shape[0]
+        if self.a.shape != (n, n):
+            raise IllegalArgumentException("matrix is not square")
+        b = N.f64(rhs)
+        x = np.empty(n)
+        st = N.load().jfg_dense_solve(self.ctx.handle, n, N.dptr(N.f64(self.a)), N.dptr(b), N.dptr(x))
+        if st == N.ERR_SINGULAR:
+            raise SingularMatrixException("singular matrix")
+        self.ctx.check(st)
+        return x
+
+    def inverse(self):
+        n = self.a.shape[0]
+        out = np.empty((n, n))
+        st = N.load().jfg_dense_inverse(self.ctx.handle, n, N.dptr(N.f64(self.a)), N.dptr(out))
+        if st == N.ERR_SINGULAR:
+            raise SingularMatrixException("singular matrix")
+        self.ctx.check(st)
+        return out
+
+
+class GMRES:
+    """Public knobs of linalg/GMRES.java:16-19."""
+
+    def __init__(self):
+        self.MAX_RESTARTS = 200
+        self.ITERATIONS_BEFORE_RESTART = 150
+
+
+class SolveResult:
+    def __init__(self, info: N.SolveInfo, history: np.ndarray):
+        self.iterations = info.iterations
+        self.restarts = info.restarts
+        self.status = info.status
+        self.outer_iterations = info.outer_iterations
+        self.final_residual = info.final_residual
+        self.final_norm = info.final_norm
+        self.not_pd = bool(info.not_pd)
+        self.history = history[: info.history_len].copy()
+
+
+def _as_device(op) -> DeviceMatrix:
+    if isinstance(op, SparseMatrix):
+        return op.device()
+    if isinstance(op, DeviceMatrix):
+        return op
+    raise IllegalArgumentException(f"operator of type {type(op).__name__} is not a GPU matrix")
+
+
+class IterativeSolver:
+    """linalg/IterativeSolver.java.  ``precision`` ('fp64' or 'mixed'),
+    ``use_graph`` and ``history_cap`` select the GPU execution; the defaults
+    reproduce the reference's FP64 semantics."""
+
+    def __init__(self, showProgress: bool = False, ctx: N.Context | None = None):
+        self.showProgress = showProgress
+        self.iterations = 0
+        self.lastSolution = None
+        self.gm = GMRES()
+        self.ctx = ctx
+        self.precision = "fp64"
+        self.inner_rtol = 1e-4
+        self.use_graph = True
+        self.history_cap = 4096
+        self.last = None          # SolveResult of the last call
+
+    def _run(self, kind, op, prec, rhs, tol, x0, maxit=0):
+        A = _as_device(op)
+        ctx = A.ctx
+        b = N.f64(rhs)
+        if b.shape != (A.rows,):
+            raise IllegalArgumentException("Vectors are of different size")
+        x = N.f64(x0).copy()
+        pk, ph = N.PREC_NONE, None
+        if prec is not None:
+            from .multigrid import MGPreconditioner
+            if isinstance(prec, MGPreconditioner):
+                pk, ph = N.PREC_MG, prec.handle
+            elif isinstance(prec, (SparseMatrix, DeviceMatrix)):
+                pk, ph = N.PREC_MATRIX, _as_device(prec).handle
+            elif prec == "jacobi":
+                pk = N.PREC_JACOBI
+            else:
+                raise IllegalArgumentException(f"unsupported preconditioner {type(prec).__name__}")
+        opts = N.SolverOpts()
+        N.load().jfg_solver_opts_default(C.byref(opts))
+        opts.tol = tol
+        opts.maxit = maxit
+        opts.restart = self.gm.ITERATIONS_BEFORE_RESTART
+        opts.max_restarts = self.gm.MAX_RESTARTS
+        opts.precision = N.MIXED if self.precision == "mixed" else N.FP64
+        opts.inner_rtol = self.inner_rtol
+        opts.use_graph = 1 if self.use_graph else 0
+        hist = np.zeros(max(self.history_cap, 1))
+        opts.h_history = N.dptr(hist)
+        opts.history_cap = self.history_cap
+        info = N.SolveInfo()
+        st = N.load().jfg_solve(ctx.handle, kind, A.handle, pk, ph, N.dptr(b), N.dptr(x), C.byref(opts),
+                                C.byref(info))
+        ctx.check(st, allow=(N.OK, N.NOT_CONVERGED, N.NONFINITE))
+        self.last = SolveResult(info, hist)
+        self.iterations = info.iterations
+        if self.showProgress:
+            for i, r in enumerate(self.last.history):
+                print(f"residuum norm {i}: {r}")
+        self.lastSolution = x
+        return x
+
+    def _start(self, n, zero=False):
+        if self.lastSolution is not None:
+            return self.lastSolution
+        x = np.zeros(n)
+        if not zero:
+            x[0] = 1.0      # iterate.set(1, 0)  (IterativeSolver.java:69-70)
+        return x
+
+    def solveCG(self, operator, rhs, tol):
+        return self._run(N.CG, operator, None, rhs, tol, self._start(len(rhs)))
+
+    def solvePCG(self, operator, preconditioner, rhs, tol):
+        return self._run(N.PCG, operator, preconditioner, rhs, tol, self._start(len(rhs)))
+
+    def solveGMRES(self, operator, rhs, tol):
+        return self._run(N.GMRES, operator, None, rhs, tol, self._start(len(rhs)))
+
+    def solvePGMRES(self, operator, preconditioner, rhs, tol):
+        # GMRES.solve with a preconditioner starts from zero (GMRES.java:59-60)
+        return self._run(N.PGMRES, operator, preconditioner, rhs, tol, self._start(len(rhs), zero=True))
+
+    def solveBiCGStab(self, operator, rhs, tol):
+        return self._run(N.BICGSTAB, operator, None, rhs, tol, self._start(len(rhs)))
+
+    def solvePBiCGStab(self, operator, preconditioner, rhs, tol):
+        return self._run(N.PBICGSTAB, operator, preconditioner, rhs, tol, self._start(len(rhs)))

@@ -1,0 +1,130 @@
+"""Host-side mirror of JFEM's multigrid API over the CUDA library.
+
+``JacobiSmoother`` / ``RichardsonSmoother`` (multigrid/JacobiSmoother.java,
+multigrid/RichardsonSmoother.java) expose ``smooth(operator, rhs, iterate)``;
+``MGPreconditioner`` is the preconditioner of
+multigrid/MGPreconditionerInterface.java (``mvMul``, ``vCycle``,
+``fullVCycleCorrection``, ``cycles``) over explicit level systems,
+prolongation matrices and Dirichlet node lists, the data that
+MGPreconditionerSpace builds (multigrid/MGPreconditionerSpace.java:28-57).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from .linalg import DeviceMatrix, IllegalArgumentException, SparseMatrix, VectorMultiplyable, _as_device
+
+
+class JacobiSmoother:
+    def __init__(self, runs: int, omega: float, A=None):
+        self.runs, self.omega = int(runs), float(omega)
+        self.kind = N.SMOOTH_JACOBI
+
+    def desc(self):
+        return N.SmootherDesc(self.kind, self.runs, self.omega)
+
+    def smooth(self, operator, rhs, iterate, verbose=False, prefix=""):
+        A = _as_device(operator)
+        x = N.f64(iterate).copy()
+        b = N.f64(rhs)
+        if b.shape != (A.rows,) or x.shape != (A.rows,):
+            raise IllegalArgumentException("Incompatible sizes")
+        d = self.desc()
+        A.ctx.check(N.load().jfg_smooth(A.handle, C.byref(d), N.dptr(b), N.dptr(x)))
+        return x
+
+
+class RichardsonSmoother(JacobiSmoother):
+    def __init__(self, omega: float, runs: int):
+        self.runs, self.omega = int(runs), float(omega)
+        self.kind = N.SMOOTH_RICHARDSON
+
+
+class MGPreconditioner(VectorMultiplyable):
+    """Geometric multigrid preconditioner on the GPU.
+
+    systems[l]: level matrices (0 = coarsest); prolongations[l]: n_{l+1} x n_l;
+    boundary[l]: Dirichlet node lists; smoothers[l] for l >= 1 (entry 0 may be
+    None).  cycles / use_fmg follow MGPreconditionerInterface.mvMul; the plain
+    one-V-cycle preconditioner is cycles=1, use_fmg=False.
+    precision="mixed" also builds the FP32 hierarchy used by mixed solves.
+    """
+
+    def __init__(self, systems, prolongations, boundary, smoothers, cycles=3, use_fmg=True, precision="fp64",
+                 ctx=None):
+        L = len(systems)
+        if len(prolongations) != L - 1 or len(boundary) != L:
+            raise IllegalArgumentException("level data of inconsistent length")
+        self._A = [_as_device(s) for s in systems]
+        self._P = [_as_device(p) for p in prolongations]
+        self.ctx = ctx or self._A[0].ctx
+        self._bd = [N.i32(b) for b in boundary]
+        sm = list(smoothers)
+        if len(sm) == L - 1:
+            sm = [None] + sm
+        if len(sm) != L:
+            raise IllegalArgumentException("one smoother per level above the coarsest")
+        descs = (N.SmootherDesc * L)()
+        for l, s in enumerate(sm):
+            if s is not None:
+                descs[l] = s.desc()
+        Ah = (C.c_void_p * L)(*[a.handle for a in self._A])
+        Ph = (C.c_void_p * max(L, 1))(*([p.handle for p in self._P] + [None]))
+        Bh = (C.POINTER(C.c_int) * L)(*[N.iptr(b) for b in self._bd])
+        nb = np.array([b.size for b in self._bd], dtype=np.int32)
+        desc = N.MGDesc(int(cycles), 1 if use_fmg else 0, 1 if precision == "mixed" else 0)
+        h = C.c_void_p()
+        st = N.load().jfg_mg_create(self.ctx.handle, L, Ah, Ph, Bh, N.iptr(nb), descs, C.byref(desc), C.byref(h))
+        if st == N.ERR_BAD_ARG:
+            raise IllegalArgumentException(N.load().jfg_last_error(self.ctx.handle).decode())
+        self.ctx.check(st)
+        self._h = h
+        self.n = self._A[-1].rows
+        self.cycles = cycles
+
+    @property
+    def handle(self):
+        return self._h
+
+    def getVectorSize(self):
+        return self.n
+
+    def getTVectorSize(self):
+        return self.n
+
+    def mvMul(self, vector):
+        v = N.f64(vector)
+        if v.shape != (self.n,):
+            raise IllegalArgumentException("wrong size")
+        out = np.empty(self.n)
+        self.ctx.check(N.load().jfg_mg_apply(self._h, N.dptr(v), N.dptr(out)))
+        return out
+
+    def tvMul(self, vector):
+        raise NotImplementedError("not implemented yet")   # MGPreconditionerInterface.java:381-385
+
+    def vCycle(self, initialIterate, rhs):
+        x0, b = N.f64(initialIterate), N.f64(rhs)
+        if x0.shape != (self.n,) or b.shape != (self.n,):
+            raise IllegalArgumentException("wrong size")
+        out = np.empty(self.n)
+        self.ctx.check(N.load().jfg_mg_vcycle(self._h, N.dptr(x0), N.dptr(b), N.dptr(out)))
+        return out
+
+    def fullVCycleCorrection(self, defect):
+        d = N.f64(defect)
+        if d.shape != (self.n,):
+            raise IllegalArgumentException("wrong size")
+        out = np.empty(self.n)
+        self.ctx.check(N.load().jfg_mg_fmg(self._h, N.dptr(d), N.dptr(out)))
+        return out
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                N.load().jfg_mg_free(self._h)
+        except Exception:
+            pass

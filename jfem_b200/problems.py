@@ -1,0 +1,65 @@
+"""Seeded synthetic systems of the benchmark configurations.
+
+* ``poisson``: -Laplace u + c u = f on the unit square, zero Dirichlet data,
+  Q_p elements (ContinuousTPFESpace), f = sum_{k,l=1..K} a_kl sin(k pi x)
+  sin(l pi y) with a_kl ~ N(0, 1) from a seeded numpy Philox stream;
+  GRAD_GRAD + c VALUE_VALUE.  Q1 64x64 with K=4 is the small CG case, Q2
+  512x512 with K=16 the multigrid-PCG case.
+* ``hierarchy``: the nested spaces, per-level systems, prolongations and
+  Dirichlet lists of a geometric multigrid hierarchy (what
+  MGPreconditionerSpace builds, multigrid/MGPreconditionerSpace.java:28-57).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from .assembly import Space, System, assemble, prolongation
+
+
+def modes_source(K: int, seed: int):
+    rng = np.random.Generator(np.random.Philox(seed))
+    a = rng.standard_normal((K, K))
+    k = np.arange(1, K + 1)
+
+    def f(X, Y):
+        sx = np.sin(np.pi * X[..., None] * k)           # (..., K)
+        sy = np.sin(np.pi * Y[..., None] * k)
+        return np.einsum("...k,kl,...l->...", sx, a, sy)
+
+    return f, a
+
+
+def poisson(p: int, cells: int, mass: float = 5.0, modes: int = 4, seed: int = 0) -> tuple[Space, System]:
+    sp = Space(p, cells, cells)
+    f, _ = modes_source(modes, seed)
+    return sp, assemble(sp, 1.0, mass, source=f)
+
+
+@dataclass
+class Hierarchy:
+    spaces: list
+    systems: list            # System per level (0 = coarsest)
+    prolong: list            # (rows, cols, vals) per level l -> l+1
+    boundary: list
+
+    @property
+    def finest(self) -> System:
+        return self.systems[-1]
+
+
+def hierarchy(p: int, coarse_cells: int, levels: int, mass: float = 5.0, modes: int = 4, seed: int = 0,
+              grad_coef_cells=None) -> Hierarchy:
+    """Levels 0..levels-1 with coarse_cells * 2^l cells per direction; the
+    rhs of the finest level carries the seeded source."""
+    spaces = [Space(p, coarse_cells << l, coarse_cells << l) for l in range(levels)]
+    f, _ = modes_source(modes, seed)
+    systems = []
+    for l, sp in enumerate(spaces):
+        kc = None
+        if grad_coef_cells is not None:
+            kc = grad_coef_cells(sp)
+        systems.append(assemble(sp, 1.0, mass, source=f if l == levels - 1 else None, grad_coef_cells=kc))
+    prol = [prolongation(spaces[l], spaces[l + 1]) for l in range(levels - 1)]
+    return Hierarchy(spaces, systems, prol, [s.boundary for s in systems])

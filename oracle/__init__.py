@@ -1,0 +1,316 @@
+"""CPU oracle for JFEM's linear-solve path (test infrastructure only).
+
+This package wraps ``jfem_oracle.c`` -- a plain-C FP64 restatement of the
+reference's Java solver routines (each C function cites the Java file:line it
+follows).  It is the parity checker for the CUDA library and the timed CPU
+baseline.  Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU
+baseline leg import it; the product package ``jfem_b200`` never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SRC = os.path.join(_HERE, "jfem_oracle.c")
+_LIB = os.path.join(_HERE, "libjfem_oracle.so")
+
+OK, MAXITER, BREAKDOWN, NONFINITE, BADARG, SINGULAR = range(6)
+SMOOTH_JACOBI, SMOOTH_RICHARDSON = 0, 1
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with gcc (recipe also in oracle/Makefile)."""
+    if force or not os.path.exists(_LIB) or os.path.getmtime(_LIB) < os.path.getmtime(_SRC):
+        subprocess.check_call(["gcc", "-O2", "-fPIC", "-shared", "-o", _LIB, _SRC, "-lm"])
+    return _LIB
+
+
+class _Info(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("restarts", C.c_int), ("status", C.c_int),
+                ("final_norm", C.c_double), ("hist_len", C.c_int)]
+
+
+_lib = None
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(build())
+        L.or_mat_new.restype = _P
+        L.or_mat_new.argtypes = [C.c_int, C.c_int, C.c_longlong, _I, _I, _D]
+        L.or_mat_free.argtypes = [_P]
+        for f in ("or_mat_mvmul", "or_mat_tvmul", "or_mat_mvmul_rows", "or_mat_tvmul_cols"):
+            getattr(L, f).argtypes = [_P, _D, _D]
+        L.or_mat_diag.argtypes = [_P, _D]
+        L.or_mat_dense.argtypes = [_P, _D]
+        L.or_jrandom_doubles.argtypes = [C.c_longlong, C.c_longlong, _D]
+        L.or_dense_solve.argtypes = [C.c_int, _D, _D, _D]
+        L.or_dense_inverse.argtypes = [C.c_int, _D, _D]
+        L.or_op_matrix.restype = _P
+        L.or_op_matrix.argtypes = [_P]
+        L.or_op_identity.restype = _P
+        L.or_op_identity.argtypes = [C.c_int]
+        L.or_op_free.argtypes = [_P]
+        L.or_op_apply.argtypes = [_P, _D, _D]
+        L.or_solve_cg.argtypes = [_P, _D, _D, C.c_double, C.c_int, C.POINTER(_Info), _D, C.c_int]
+        L.or_solve_pcg.argtypes = [_P, _P, _D, _D, C.c_double, C.c_int, C.POINTER(_Info), _D, C.c_int]
+        L.or_solve_bicgstab.argtypes = [_P, _D, _D, C.c_double, C.c_int, C.POINTER(_Info), _D, C.c_int]
+        L.or_solve_pbicgstab.argtypes = [_P, _P, _D, _D, C.c_double, C.c_int, C.POINTER(_Info), _D, C.c_int]
+        L.or_solve_gmres.argtypes = [_P, _P, _D, _D, C.c_double, C.c_int, C.c_int, C.POINTER(_Info), _D, C.c_int]
+        L.or_solve_gmres2.argtypes = [_P, _P, _D, _D, C.c_double, C.c_int, C.c_int, C.POINTER(_Info), _D, C.c_int]
+        L.or_smooth.argtypes = [_P, C.c_int, C.c_int, C.c_double, _D, _D]
+        L.or_mg_new.restype = _P
+        L.or_mg_new.argtypes = [C.c_int, C.POINTER(_P), C.POINTER(_P), C.POINTER(_I), _I, _I, _I, _D, C.c_int]
+        L.or_mg_free.argtypes = [_P]
+        L.or_mg_vcycle.argtypes = [_P, _D, _D, _D]
+        L.or_mg_fmg.argtypes = [_P, _D, _D]
+        L.or_mg_apply.argtypes = [_P, _D, _D]
+        L.or_mg_apply_ex.argtypes = [_P, C.c_int, C.c_int, _D, _D]
+        L.or_op_mg.restype = _P
+        L.or_op_mg.argtypes = [_P, C.c_int, C.c_int]
+        L.or_op_mg_free.argtypes = [_P]
+        L.or_mg_coarse_status.argtypes = [_P]
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_D)
+
+
+def _i(a):
+    return a.ctypes.data_as(_I)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def java_random_doubles(seed: int, count: int) -> np.ndarray:
+    """``new java.util.Random(seed).nextDouble()`` repeated ``count`` times."""
+    out = np.empty(count, dtype=np.float64)
+    lib().or_jrandom_doubles(seed, count, _d(out))
+    return out
+
+
+class CooMatrix:
+    """COO triples in storage order, SparseMatrix.java semantics."""
+
+    def __init__(self, rows, cols, ri, ci, v):
+        self.rows, self.cols = int(rows), int(cols)
+        self.ri, self.ci, self.v = _i32(ri), _i32(ci), _f64(v)
+        h = lib().or_mat_new(self.rows, self.cols, len(self.v), _i(self.ri), _i(self.ci), _d(self.v))
+        if not h:
+            raise ValueError("invalid COO triples")
+        self._h = h
+        self._op = lib().or_op_matrix(h)
+
+    def __del__(self):
+        try:
+            lib().or_op_free(self._op)
+            lib().or_mat_free(self._h)
+        except Exception:
+            pass
+
+    def mvmul(self, x):
+        x = _f64(x)
+        y = np.empty(self.rows)
+        lib().or_mat_mvmul(self._h, _d(x), _d(y))
+        return y
+
+    def tvmul(self, x):
+        x = _f64(x)
+        y = np.empty(self.cols)
+        lib().or_mat_tvmul(self._h, _d(x), _d(y))
+        return y
+
+    def mvmul_rows(self, x):
+        x = _f64(x)
+        y = np.empty(self.rows)
+        lib().or_mat_mvmul_rows(self._h, _d(x), _d(y))
+        return y
+
+    def tvmul_cols(self, x):
+        x = _f64(x)
+        y = np.empty(self.cols)
+        lib().or_mat_tvmul_cols(self._h, _d(x), _d(y))
+        return y
+
+    def diag(self):
+        d = np.empty(min(self.rows, self.cols))
+        lib().or_mat_diag(self._h, _d(d))
+        return d
+
+    def dense(self):
+        a = np.empty((self.rows, self.cols))
+        lib().or_mat_dense(self._h, _d(a))
+        return a
+
+
+def dense_solve(a, b):
+    a = _f64(a)
+    b = _f64(b)
+    x = np.empty(len(b))
+    st = lib().or_dense_solve(a.shape[0], _d(a), _d(b), _d(x))
+    if st != OK:
+        raise np.linalg.LinAlgError("singular")
+    return x
+
+
+def dense_inverse(a):
+    a = _f64(a)
+    out = np.empty_like(a)
+    st = lib().or_dense_inverse(a.shape[0], _d(a), _d(out))
+    if st != OK:
+        raise np.linalg.LinAlgError("singular")
+    return out
+
+
+class Result:
+    def __init__(self, x, info, hist):
+        self.x = x
+        self.iterations = info.iterations
+        self.restarts = info.restarts
+        self.status = info.status
+        self.final_norm = info.final_norm
+        self.history = hist[: min(info.hist_len, len(hist))].copy()
+
+
+def _op(M):
+    if M is None:
+        return None
+    if isinstance(M, CooMatrix):
+        return M._op
+    if isinstance(M, MGPreconditioner):
+        return M._op
+    raise TypeError(type(M))
+
+
+def _run(fn, *args, x0, hist_cap=100000):
+    x = _f64(x0).copy()
+    info = _Info()
+    hist = np.zeros(hist_cap)
+    fn(*args[:-1], _d(x), *args[-1], C.byref(info), _d(hist), hist_cap)
+    return Result(x, info, hist)
+
+
+def start_iterate(n):
+    """The reference's default start vector e0 (IterativeSolver.java:69-70)."""
+    x = np.zeros(n)
+    x[0] = 1.0
+    return x
+
+
+def solve_cg(A: CooMatrix, b, tol, x0=None, maxit=0):
+    b = _f64(b)
+    x0 = start_iterate(len(b)) if x0 is None else x0
+    return _run(lib().or_solve_cg, A._op, _d(b), (C.c_double(tol), maxit), x0=x0)
+
+
+def solve_pcg(A, M, b, tol, x0=None, maxit=0):
+    b = _f64(b)
+    x0 = start_iterate(len(b)) if x0 is None else x0
+    return _run(lib().or_solve_pcg, A._op, _op(M), _d(b), (C.c_double(tol), maxit), x0=x0)
+
+
+def solve_bicgstab(A, b, tol, x0=None, maxit=0):
+    b = _f64(b)
+    x0 = start_iterate(len(b)) if x0 is None else x0
+    return _run(lib().or_solve_bicgstab, A._op, _d(b), (C.c_double(tol), maxit), x0=x0)
+
+
+def solve_pbicgstab(A, M, b, tol, x0=None, maxit=0):
+    b = _f64(b)
+    x0 = start_iterate(len(b)) if x0 is None else x0
+    return _run(lib().or_solve_pbicgstab, A._op, _op(M), _d(b), (C.c_double(tol), maxit), x0=x0)
+
+
+def solve_gmres(A, b, tol, M=None, x0=None, restart=150, max_restarts=200):
+    """GMRES.solve: e0 start without a preconditioner, zero start with one
+    (GMRES.java:40-62)."""
+    b = _f64(b)
+    if x0 is None:
+        x0 = start_iterate(len(b)) if M is None else np.zeros(len(b))
+    return _run(lib().or_solve_gmres, A._op, _op(M), _d(b), (C.c_double(tol), restart, max_restarts), x0=x0)
+
+
+def solve_gmres2(A, b, tol, M=None, x0=None, maxit=0, max_restarts=200):
+    b = _f64(b)
+    x0 = start_iterate(len(b)) if x0 is None else x0
+    return _run(lib().or_solve_gmres2, A._op, _op(M), _d(b), (C.c_double(tol), maxit, max_restarts), x0=x0)
+
+
+def smooth(A: CooMatrix, kind, runs, omega, rhs, x):
+    x = _f64(x).copy()
+    rhs = _f64(rhs)
+    lib().or_smooth(A._h, kind, runs, omega, _d(rhs), _d(x))
+    return x
+
+
+class MGPreconditioner:
+    """MGPreconditionerInterface over explicit level data.
+
+    ``mats[l]`` is the system on level l (0 = coarsest), ``prolong[l]`` the
+    n_{l+1} x n_l prolongation, ``bdry[l]`` the Dirichlet node list,
+    ``smoothers[l]`` a (kind, runs, omega) triple for l >= 1.
+    use_fmg/cycles select the reference mvMul (FMG + cycles V-cycles) or a
+    single V-cycle (use_fmg=False, cycles=1).
+    """
+
+    def __init__(self, mats, prolong, bdry, smoothers, cycles=3, use_fmg=True):
+        L = len(mats)
+        self.mats, self.prolong = mats, prolong
+        self._bd = [_i32(b) for b in bdry]
+        A = (_P * L)(*[m._h for m in mats])
+        P = (_P * L)(*([p._h for p in prolong] + [None]))
+        BD = (_I * L)(*[_i(b) for b in self._bd])
+        NBD = np.array([len(b) for b in self._bd], dtype=np.int32)
+        sm = list(smoothers) if len(smoothers) == L else [None] + list(smoothers)
+        kind = np.array([0 if s is None else s[0] for s in sm], dtype=np.int32)
+        runs = np.array([0 if s is None else s[1] for s in sm], dtype=np.int32)
+        omg = np.array([0.0 if s is None else s[2] for s in sm], dtype=np.float64)
+        self._h = lib().or_mg_new(L, A, P, BD, _i(NBD), _i(kind), _i(runs), _d(omg), cycles)
+        if lib().or_mg_coarse_status(self._h) != OK:
+            raise np.linalg.LinAlgError("coarsest matrix singular")
+        self._op = lib().or_op_mg(self._h, 1 if use_fmg else 0, cycles)
+        self.n = mats[-1].rows
+
+    def __del__(self):
+        try:
+            lib().or_op_mg_free(self._op)
+            lib().or_mg_free(self._h)
+        except Exception:
+            pass
+
+    def vcycle(self, x0, rhs):
+        out = np.empty(self.n)
+        lib().or_mg_vcycle(self._h, _d(_f64(x0)), _d(_f64(rhs)), _d(out))
+        return out
+
+    def fmg(self, defect):
+        out = np.empty(self.n)
+        lib().or_mg_fmg(self._h, _d(_f64(defect)), _d(out))
+        return out
+
+    def apply(self, v, use_fmg=True, cycles=None):
+        out = np.empty(self.n)
+        lib().or_mg_apply_ex(self._h, 1 if use_fmg else 0, 3 if cycles is None else cycles,
+                             _d(_f64(v)), _d(out))
+        return out
+
+    def mvmul(self, v):
+        out = np.empty(self.n)
+        lib().or_op_apply(self._op, _d(_f64(v)), _d(out))
+        return out

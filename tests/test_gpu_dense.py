@@ -1,0 +1,50 @@
+"""GPU dense LU (DenseMatrix.solve / inverse, JNI iSolve / iInverse) and the
+SparseMatrix.solve drop-in."""
+import numpy as np
+import pytest
+
+import oracle as O
+from fixtures import fe_system, kat
+from jfem_b200 import SingularMatrixException, SparseMatrix
+from jfem_b200.linalg import DenseMatrix
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", ["symm", "nonsymm", "good_nonsymm"])
+def test_kat(ctx, name):
+    k = kat()["systems"][name]
+    D = DenseMatrix(k["A"], ctx)
+    np.testing.assert_allclose(D.solve(k["b"]), k["x"], atol=1e-13)
+    np.testing.assert_allclose(D.inverse() @ np.array(k["A"], float), np.eye(3), atol=1e-13)
+
+
+@pytest.mark.parametrize("n", [1, 7, 81, 300])
+def test_random_dense(ctx, n):
+    rng = np.random.default_rng(n)
+    a = rng.standard_normal((n, n)) + n * np.eye(n)
+    b = rng.standard_normal(n)
+    D = DenseMatrix(a, ctx)
+    np.testing.assert_allclose(D.solve(b), O.dense_solve(a, b), rtol=1e-11, atol=1e-12)
+    np.testing.assert_allclose(D.inverse(), O.dense_inverse(a), rtol=1e-10, atol=1e-12)
+
+
+def test_singular(ctx):
+    with pytest.raises(SingularMatrixException):
+        DenseMatrix(np.array([[1.0, 2.0], [2.0, 4.0]]), ctx).solve([1.0, 1.0])
+
+
+def test_sparse_solve_dropin(ctx):
+    sp, sy = fe_system(1, 24)
+    A = SparseMatrix.from_coo(sy.n, sy.n, sy.rows, sy.cols, sy.vals, ctx)
+    ref = O.dense_solve(O.CooMatrix(sy.n, sy.n, sy.rows, sy.cols, sy.vals).dense(), sy.rhs)
+    x = A.solve(sy.rhs)
+    assert np.linalg.norm(x - ref) / np.linalg.norm(ref) < 1e-8
+
+
+def test_sparse_solve_dropin_large(ctx):
+    sp, sy = fe_system(1, 96)          # n = 9409 > 4096: iterative path
+    A = SparseMatrix.from_coo(sy.n, sy.n, sy.rows, sy.cols, sy.vals, ctx)
+    x = A.solve(sy.rhs)
+    r = sy.rhs - O.CooMatrix(sy.n, sy.n, sy.rows, sy.cols, sy.vals).mvmul(x)
+    assert np.linalg.norm(r) <= 1e-11 * np.linalg.norm(sy.rhs)

@@ -1,0 +1,61 @@
+"""GPU multigrid pieces (smoothers, V-cycle, FMG, preconditioner) against the oracle."""
+import numpy as np
+import pytest
+
+import oracle as O
+from fixtures import coo_oracle, fe_system, mg_levels
+from jfem_b200 import JacobiSmoother, MGPreconditioner, RichardsonSmoother
+from jfem_b200.linalg import DeviceMatrix
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(sy, ctx):
+    return DeviceMatrix(sy.n, sy.n, sy.rows, sy.cols, sy.vals, ctx)
+
+
+@pytest.mark.parametrize("kind,runs,omega", [(O.SMOOTH_JACOBI, 3, 2 / 3), (O.SMOOTH_RICHARDSON, 4, 0.1)])
+def test_smoother(ctx, kind, runs, omega):
+    sp, sy = fe_system(2, 16)
+    A = dev(sy, ctx)
+    x0 = np.random.default_rng(0).standard_normal(sy.n)
+    ref = O.smooth(coo_oracle(sy), kind, runs, omega, sy.rhs, x0)
+    sm = JacobiSmoother(runs, omega) if kind == O.SMOOTH_JACOBI else RichardsonSmoother(omega, runs)
+    got = sm.smooth(A, sy.rhs, x0)
+    np.testing.assert_allclose(got, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
+
+
+def build(h, ctx, sm_tuple, cycles, use_fmg):
+    mats_o = [coo_oracle(s) for s in h.systems]
+    prol_o = [O.CooMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l]) for l in range(len(h.systems) - 1)]
+    mg_o = O.MGPreconditioner(mats_o, prol_o, h.boundary, [None] + [sm_tuple] * (len(mats_o) - 1), cycles=cycles,
+                              use_fmg=use_fmg)
+    mats = [dev(s, ctx) for s in h.systems]
+    prol = [DeviceMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l], ctx) for l in range(len(h.systems) - 1)]
+    kind, runs, om = sm_tuple
+    sm = JacobiSmoother(runs, om) if kind == O.SMOOTH_JACOBI else RichardsonSmoother(om, runs)
+    mg = MGPreconditioner(mats, prol, h.boundary, [None] + [sm] * (len(mats) - 1), cycles=cycles, use_fmg=use_fmg,
+                          ctx=ctx)
+    return mg_o, mg, mats
+
+
+@pytest.mark.parametrize("p,coarse,L", [(1, 4, 5), (2, 2, 5)])
+@pytest.mark.parametrize("sm", [(O.SMOOTH_JACOBI, 2, 2 / 3), (O.SMOOTH_RICHARDSON, 8, 0.1)])
+def test_vcycle_fmg_apply(ctx, p, coarse, L, sm):
+    h = mg_levels(p, coarse, L, modes=6, seed=4)
+    mg_o, mg, mats = build(h, ctx, sm, 3, True)
+    b = h.finest.rhs
+    x0 = np.random.default_rng(1).standard_normal(b.size) * 0.1
+    for got, ref in ((mg.vCycle(x0, b), mg_o.vcycle(x0, b)),
+                     (mg.fullVCycleCorrection(b), mg_o.fmg(b)),
+                     (mg.mvMul(b), mg_o.mvmul(b))):
+        np.testing.assert_allclose(got, ref, rtol=1e-10, atol=1e-10 * np.abs(ref).max())
+
+
+def test_mg_single_level(ctx):
+    """levels = 1: the preconditioner is the dense coarse solve."""
+    sp, sy = fe_system(1, 4)
+    A = dev(sy, ctx)
+    mg = MGPreconditioner([A], [], [sy.boundary], [None], cycles=1, use_fmg=False, ctx=ctx)
+    D = coo_oracle(sy).dense()
+    np.testing.assert_allclose(mg.mvMul(sy.rhs), np.linalg.solve(D, sy.rhs), rtol=1e-12, atol=1e-14)

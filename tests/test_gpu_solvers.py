@@ -1,0 +1,205 @@
+"""GPU Krylov solvers through the C ABI against the oracle (same seeded inputs)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from fixtures import coo_oracle, fe_system, kat, mg_levels
+from jfem_b200 import IterativeSolver, MGPreconditioner, JacobiSmoother, RichardsonSmoother, SparseMatrix
+from jfem_b200 import _native as N
+from jfem_b200.linalg import DeviceMatrix
+
+pytestmark = pytest.mark.gpu
+
+REL = 1e-8   # FP64 path: relative solution error against the oracle's solve
+
+
+def dev(sy, ctx):
+    return DeviceMatrix(sy.n, sy.n, sy.rows, sy.cols, sy.vals, ctx)
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_cg_cfg0(ctx, graph):
+    """Q1 64x64 (4,225 dofs), -Lap u + 5u = f, CG to 1e-10 ||b|| from e0."""
+    sp, sy = fe_system(1, 64, modes=4, seed=0)
+    tol = 1e-10 * np.linalg.norm(sy.rhs)
+    ref = O.solve_cg(coo_oracle(sy), sy.rhs, tol)
+    s = IterativeSolver(ctx=ctx)
+    s.use_graph = graph
+    x = s.solveCG(dev(sy, ctx), sy.rhs, tol)
+    assert s.last.status == N.OK
+    assert rel(x, ref.x) < REL
+    assert abs(s.iterations - ref.iterations) <= 2
+    assert s.last.final_residual <= tol * 1.01
+    np.testing.assert_allclose(s.last.history[:10], ref.history[:10], rtol=1e-9)
+
+
+def test_cg_warm_start_and_reuse(ctx):
+    sp, sy = fe_system(1, 32)
+    tol = 1e-10 * np.linalg.norm(sy.rhs)
+    s = IterativeSolver(ctx=ctx)
+    A = dev(sy, ctx)
+    x1 = s.solveCG(A, sy.rhs, tol)
+    it1 = s.iterations
+    x2 = s.solveCG(A, sy.rhs, tol)          # lastSolution warm start: converged already
+    assert s.iterations == 0 and it1 > 0
+    assert np.array_equal(x1, x2)
+
+
+def _mg_pair(h, ctx, smoother, cycles, use_fmg, precision="fp64"):
+    mats_o = [coo_oracle(s) for s in h.systems]
+    prol_o = [O.CooMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l]) for l in range(len(h.systems) - 1)]
+    kind, runs, om = smoother
+    mg_o = O.MGPreconditioner(mats_o, prol_o, h.boundary, [None] + [smoother] * (len(mats_o) - 1), cycles=cycles,
+                              use_fmg=use_fmg)
+    mats = [dev(s, ctx) for s in h.systems]
+    prol = [DeviceMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l], ctx) for l in range(len(h.systems) - 1)]
+    sm = JacobiSmoother(runs, om) if kind == O.SMOOTH_JACOBI else RichardsonSmoother(om, runs)
+    mg = MGPreconditioner(mats, prol, h.boundary, [None] + [sm] * (len(mats) - 1), cycles=cycles, use_fmg=use_fmg,
+                          precision=precision, ctx=ctx)
+    return mats_o, mg_o, mats, mg
+
+
+@pytest.mark.parametrize("cycles,use_fmg", [(3, True), (1, False)])
+def test_pcg_mg_matches_oracle(ctx, cycles, use_fmg):
+    h = mg_levels(2, 4, 4, modes=8, seed=1)     # Q2 32x32 finest
+    mats_o, mg_o, mats, mg = _mg_pair(h, ctx, (O.SMOOTH_JACOBI, 2, 2.0 / 3.0), cycles, use_fmg)
+    b = h.finest.rhs
+    tol = 1e-8 * np.linalg.norm(b)
+    ref = O.solve_pcg(mats_o[-1], mg_o, b, tol)
+    s = IterativeSolver(ctx=ctx)
+    x = s.solvePCG(mats[-1], mg, b, tol)
+    assert s.last.status == N.OK
+    assert s.iterations == ref.iterations
+    assert rel(x, ref.x) < REL
+    np.testing.assert_allclose(s.last.history, ref.history, rtol=1e-7)
+
+
+def test_mixed_precision_pcg(ctx):
+    h = mg_levels(2, 4, 5, modes=16, seed=2)    # Q2 64x64
+    mats_o, mg_o, mats, mg = _mg_pair(h, ctx, (O.SMOOTH_JACOBI, 2, 2.0 / 3.0), 1, False, precision="mixed")
+    b = h.finest.rhs
+    tol = 1e-8 * np.linalg.norm(b)
+    ref = O.solve_pcg(mats_o[-1], mg_o, b, tol)
+    s = IterativeSolver(ctx=ctx)
+    s.precision = "mixed"
+    x = s.solvePCG(mats[-1], mg, b, tol)
+    assert s.last.status == N.OK
+    assert s.last.final_residual <= tol
+    assert rel(x, ref.x) < 1e-7
+    assert s.last.outer_iterations >= 2
+
+
+@pytest.mark.parametrize("name", ["symm", "nonsymm", "good_nonsymm"])
+def test_kat_gmres_bicgstab(ctx, name):
+    k = kat()["systems"][name]
+    a = np.array(k["A"], float)
+    r, c = np.nonzero(a)
+    A = SparseMatrix.from_coo(3, 3, r, c, a[r, c], ctx)
+    b = np.array(k["b"], float)
+    x = np.array(k["x"])
+    for solve in ("solveGMRES", "solveBiCGStab"):
+        s = IterativeSolver(ctx=ctx)
+        got = getattr(s, solve)(A, b, 1e-12)
+        np.testing.assert_allclose(got, x, atol=1e-9), solve
+    s = IterativeSolver(ctx=ctx)
+    got = s.solvePGMRES(A, SparseMatrix.identity(3, ctx), b, 1e-12)
+    np.testing.assert_allclose(got, x, atol=1e-9)
+
+
+def test_gmres_fe_matches_oracle(ctx):
+    sp, sy = fe_system(1, 24)
+    tol = 1e-10 * np.linalg.norm(sy.rhs)
+    ref = O.solve_gmres(coo_oracle(sy), sy.rhs, tol, restart=30)
+    s = IterativeSolver(ctx=ctx)
+    s.gm.ITERATIONS_BEFORE_RESTART = 30
+    x = s.solveGMRES(dev(sy, ctx), sy.rhs, tol)
+    assert s.last.status == N.OK
+    assert rel(x, ref.x) < REL
+    assert abs(s.iterations - ref.iterations) <= 2
+
+
+def test_pgmres_mg(ctx):
+    h = mg_levels(1, 4, 4, mass=0.0)
+    mats_o, mg_o, mats, mg = _mg_pair(h, ctx, (O.SMOOTH_RICHARDSON, 8, 0.1), 3, True)
+    b = h.finest.rhs
+    ref = O.solve_gmres(mats_o[-1], b, 1e-8, M=mg_o)
+    s = IterativeSolver(ctx=ctx)
+    x = s.solvePGMRES(mats[-1], mg, b, 1e-8)
+    assert s.last.status == N.OK
+    assert s.iterations < 10 and s.iterations == ref.iterations
+    assert rel(x, ref.x) < REL
+
+
+def test_bicgstab_fe_matches_oracle(ctx):
+    sp, sy = fe_system(1, 20)
+    tol = 1e-10 * np.linalg.norm(sy.rhs)
+    ref = O.solve_bicgstab(coo_oracle(sy), sy.rhs, tol)
+    s = IterativeSolver(ctx=ctx)
+    x = s.solveBiCGStab(dev(sy, ctx), sy.rhs, tol)
+    assert rel(x, ref.x) < REL
+    assert abs(s.iterations - ref.iterations) <= 2
+
+
+def test_pbicgstab_mg(ctx):
+    h = mg_levels(2, 4, 3)
+    mats_o, mg_o, mats, mg = _mg_pair(h, ctx, (O.SMOOTH_JACOBI, 2, 2.0 / 3.0), 1, False)
+    b = h.finest.rhs
+    tol = 1e-9 * np.linalg.norm(b)
+    ref = O.solve_pbicgstab(mats_o[-1], mg_o, b, tol)
+    s = IterativeSolver(ctx=ctx)
+    x = s.solvePBiCGStab(mats[-1], mg, b, tol)
+    assert rel(x, ref.x) < 1e-7
+    assert abs(s.iterations - ref.iterations) <= 1
+
+
+def test_nonfinite_rhs_status(ctx):
+    sp, sy = fe_system(1, 8)
+    b = sy.rhs.copy()
+    b[5] = np.nan
+    s = IterativeSolver(ctx=ctx)
+    s.solveCG(dev(sy, ctx), b, 1e-10)
+    assert s.last.status == N.NONFINITE
+
+
+def test_not_pd_flag(ctx):
+    a = np.diag([1.0, -2.0, 3.0])
+    r, c = np.nonzero(a)
+    A = SparseMatrix.from_coo(3, 3, r, c, a[r, c], ctx)
+    s = IterativeSolver(ctx=ctx)
+    s.solveCG(A, np.array([1.0, 1.0, 1.0]), 1e-12)
+    assert s.last.not_pd
+
+
+def test_iteration_cap(ctx):
+    sp, sy = fe_system(1, 32)
+    s = IterativeSolver(ctx=ctx)
+    A = dev(sy, ctx)
+    s._run(N.CG, A, None, sy.rhs, 1e-30, s._start(sy.n), maxit=7)
+    assert s.last.status == N.NOT_CONVERGED and s.iterations == 7
+
+
+def test_pcg_mg_full_size(ctx):
+    """Q2 512x512 (1,050,625 dofs), 8 levels, Jacobi 2/2 omega=2/3: FP64 and
+    mixed PCG reach the 1e-8 relative FP64 true residual and agree."""
+    h = mg_levels(2, 4, 8, modes=16, seed=0)
+    mats = [dev(s, ctx) for s in h.systems]
+    prol = [DeviceMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l], ctx) for l in range(7)]
+    sm = JacobiSmoother(2, 2.0 / 3.0)
+    mg = MGPreconditioner(mats, prol, h.boundary, [None] + [sm] * 7, cycles=1, use_fmg=False, precision="mixed",
+                          ctx=ctx)
+    b = h.finest.rhs
+    tol = 1e-8 * np.linalg.norm(b)
+    s = IterativeSolver(ctx=ctx)
+    x64 = s.solvePCG(mats[-1], mg, b, tol)
+    assert s.last.status == N.OK and s.last.final_residual <= tol
+    it64 = s.iterations
+    s2 = IterativeSolver(ctx=ctx)
+    s2.precision = "mixed"
+    x32 = s2.solvePCG(mats[-1], mg, b, tol)
+    assert s2.last.status == N.OK and s2.last.final_residual <= tol
+    assert rel(x32, x64) < 1e-7
+    assert it64 <= 20
