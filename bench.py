@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cells", type=int, default=CELLS)
     ap.add_argument("--levels", type=int, default=LEVELS)
+    ap.add_argument("--profile", default=None, choices=["solve-fp64", "solve-mixed", "spmv64", "spmv32"],
+                    help="set up, run the named operation --warmup + 1 times and exit (for ncu captures)")
     return ap.parse_args()
 
 
@@ -192,6 +194,18 @@ def run_ours(args):
         torch.cuda.synchronize()
         barrier()
         return max_over_ranks(ev0.elapsed_time(ev1) / steps)
+
+    if args.profile:
+        for _ in range(args.warmup + 1):
+            if args.profile == "solve-fp64":
+                solve_dev(N.FP64)
+            elif args.profile == "solve-mixed":
+                solve_dev(N.MIXED)
+            else:
+                A.time_spmv(precision=1 if args.profile == "spmv32" else 0, iters=1)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": args.profile, "iterations": info.iterations}))
+        return
 
     # FP64 judge (the plain drop-in) and the mixed-precision headline
     ms64 = timed(lambda: solve_dev(N.FP64), max(2, args.steps // 2), max(3, args.warmup))

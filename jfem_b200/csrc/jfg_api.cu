@@ -574,6 +574,8 @@ static int solve_impl(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, cons
             else
                 JFG_CUDA(cudaMemsetAsync(d_x, 0, sizeof(double) * n, st));
             h.status = JFG_NOT_CONVERGED;
+            h.restart_len = o->restart > 0 ? o->restart : 150;
+            h.maxit = 1 << 30;
             JFG_CUDA(cudaMemcpyAsync(w.ctl.p, &h, sizeof(Ctl), cudaMemcpyHostToDevice, st));
             restarts = run_gmres(w, M, P64, d_b, d_x, o->restart > 0 ? o->restart : 150,
                                  o->max_restarts >= 0 ? o->max_restarts : 200, use_graph, chunk);

@@ -117,6 +117,17 @@ struct VJacobiPre {  // z = dinv * r
 };
 
 template <typename T>
+struct VCopyNorm {   // b = a, acc += a^2
+    const T* a;
+    T* b;
+    template <int K> __device__ void operator()(int i, double (&acc)[K]) const
+    {
+        T v = a[i];
+        b[i] = v;
+        acc[0] += (double)v * (double)v;
+    }
+};
+template <typename T>
 struct VNorm2 {
     const T* a;
     template <int K> __device__ void operator()(int i, double (&acc)[K]) const { acc[0] += (double)a[i] * (double)a[i]; }
@@ -628,8 +639,7 @@ int run_cg(SolverWork& w, int ci, Matrix* A, const Precond<T>& M, const T* b, T*
     const T* val = vals_of<T>(A);
     bool pcg = M.kind != JFG_PREC_NONE;
     if (xzero) {
-        vec_launch<1>(st, n, VCopy<T>{b, r}, sc, nullptr, NoFin());
-        vec_launch<1>(st, n, VNorm2<T>{r}, sc, nullptr, FinInit{c});
+        vec_launch<1>(st, n, VCopyNorm<T>{b, r}, sc, nullptr, FinInit{c});
     } else {
         spmv_launch<T, T, 1>(st, A, val, x, EpiResid<T>{b, r}, sc, nullptr, FinInit{c});
     }
