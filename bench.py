@@ -126,6 +126,7 @@ def run_ours(args):
     import ctypes as C
 
     ctx = N.Context(local)
+    HEADLINE = N.MIXED_PRECOND
     t0 = time.time()
     h = build_problem(args.cells, args.levels)
     mats = [DeviceMatrix(s.n, s.n, s.rows, s.cols, s.vals, ctx) for s in h.systems]
@@ -200,7 +201,7 @@ def run_ours(args):
             if args.profile == "solve-fp64":
                 solve_dev(N.FP64)
             elif args.profile == "solve-mixed":
-                solve_dev(N.MIXED)
+                solve_dev(HEADLINE)
             else:
                 A.time_spmv(precision=1 if args.profile == "spmv32" else 0, iters=1)
         torch.cuda.synchronize()
@@ -211,11 +212,14 @@ def run_ours(args):
     ms64 = timed(lambda: solve_dev(N.FP64), max(2, args.steps // 2), max(3, args.warmup))
     it64, res64, _ = solve_dev(N.FP64)
     x64 = dx.cpu().numpy().copy()
+    # the other mixed mode (defect correction around FP32 inner PCG), reported beside
+    ms_dc = timed(lambda: solve_dev(N.MIXED), max(2, args.steps // 2), max(3, args.warmup))
+    it_dc, res_dc, outer_dc = solve_dev(N.MIXED)
     l0 = N.kernel_launches()
     with ClockSampler(local) as clk:
-        ms = timed(lambda: solve_dev(N.MIXED), args.steps, args.warmup)
+        ms = timed(lambda: solve_dev(HEADLINE), args.steps, args.warmup)
     launches = (N.kernel_launches() - l0) / (args.steps + args.warmup)
-    itm, resm, outer = solve_dev(N.MIXED)
+    itm, resm, outer = solve_dev(HEADLINE)
     xm = dx.cpu().numpy().copy()
     rel_err = float(np.linalg.norm(xm - x64) / np.linalg.norm(x64))
 
@@ -227,7 +231,7 @@ def run_ours(args):
 
     def solve_host():
         hx.numpy()[:] = e0h
-        o = opts(N.MIXED)
+        o = opts(HEADLINE)
         st = N.load().jfg_solve(ctx.handle, N.PCG, A.handle, N.PREC_MG, mg.handle,
                                 C.cast(hb.data_ptr(), C.POINTER(C.c_double)),
                                 C.cast(hx.data_ptr(), C.POINTER(C.c_double)), C.byref(o), C.byref(info))
@@ -288,6 +292,9 @@ def run_ours(args):
             "fp64_iterations": it64,
             "fp64_final_rel_residual": res64 / bnorm,
             "speedup_vs_fp64": ms64 / ms,
+            "mode": "FP64 PCG + FP32 V-cycle preconditioner",
+            "defect_correction": {"time_s": ms_dc / 1e3, "inner_iterations": it_dc, "outer_iterations": outer_dc,
+                                  "final_rel_residual": res_dc / bnorm},
             "spmv_gbs": {"fp64": gbs64, "fp32": gbs32},
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 2 * 8 * n, "d2h_bytes_per_step": 8 * n},
             "gpu_launches": int(round(launches)),

@@ -142,7 +142,8 @@ typedef enum {
 
 typedef enum {
     JFG_FP64 = 0,          /* every operation in FP64 */
-    JFG_MIXED = 1          /* FP64 defect-correction outer loop around an FP32 inner solve */
+    JFG_MIXED = 1,         /* FP64 defect-correction outer loop around an FP32 inner solve */
+    JFG_MIXED_PRECOND = 2  /* FP64 Krylov iteration (true residual, dots) with an FP32 preconditioner */
 } jfg_precision;
 
 typedef struct {

@@ -21,7 +21,7 @@ CG, PCG, BICGSTAB, PBICGSTAB, GMRES, PGMRES, GMRES2 = range(7)
 # jfg_precond_kind
 PREC_NONE, PREC_MG, PREC_JACOBI, PREC_MATRIX = range(4)
 # jfg_precision
-FP64, MIXED = 0, 1
+FP64, MIXED, MIXED_PRECOND = 0, 1, 2
 SMOOTH_JACOBI, SMOOTH_RICHARDSON = 0, 1
 
 # Every symbol include/jfem_gpu.h declares.

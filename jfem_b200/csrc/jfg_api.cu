@@ -467,6 +467,7 @@ static int solve_impl(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, cons
               "multigrid preconditioner does not match the system size");
     JFG_CHECK(pk != JFG_PREC_MATRIX || (pm && pm->m->rows == n && pm->m->cols == n), JFG_ERR_BAD_ARG,
               "preconditioner matrix does not match the system size");
+    JFG_CHECK(o->precision >= JFG_FP64 && o->precision <= JFG_MIXED_PRECOND, JFG_ERR_BAD_ARG, "unknown precision");
     bool mixed = o->precision == JFG_MIXED;
     JFG_CHECK(!mixed || kind == JFG_CG || kind == JFG_PCG, JFG_ERR_UNSUPPORTED,
               "mixed precision is implemented for CG/PCG");
@@ -483,6 +484,13 @@ static int solve_impl(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, cons
     P64.kind = pk;
     P64.n = n;
     if (mg) P64.mg = mg->d64.get();
+    if (mg && o->precision == JFG_MIXED_PRECOND) {
+        P64.mg32 = mg->fp32();
+        w.v32[6].alloc(n);
+        w.v32[7].alloc(n);
+        P64.r32 = w.v32[6].p;
+        P64.z32 = w.v32[7].p;
+    }
     if (pm) P64.M = pm->m;
     if (pk == JFG_PREC_JACOBI) {
         w.dinv64.alloc(n);

@@ -256,6 +256,7 @@ template <typename T>
 __global__ void k_mdot(int n, const T* __restrict__ V, const T* __restrict__ q, const Ctl* __restrict__ c,
                        double* __restrict__ part, const int* __restrict__ flag)
 {
+    pdl_wait();
     if (*flag) return;
     int i = blockIdx.y;
     if (i > c->j) return;
@@ -269,6 +270,7 @@ __global__ void k_mdot(int n, const T* __restrict__ V, const T* __restrict__ q, 
 __global__ void k_mdot_fin(int gx, const double* __restrict__ part, const Ctl* __restrict__ c, double* __restrict__ fac,
                            const int* __restrict__ flag)
 {
+    pdl_wait();
     if (*flag) return;
     int i = blockIdx.x;
     if (i > c->j) return;
@@ -435,6 +437,7 @@ struct FinTrueRes {
 
 __global__ void k_set_cond(cudaGraphConditionalHandle h, const int* flag)
 {
+    pdl_wait();
     cudaGraphSetConditional(h, *flag ? 0u : 1u);
 }
 
@@ -473,7 +476,13 @@ void Precond<T>::apply(const T* r, T* z, const Scratch& sc, const int* done, cud
 {
     switch (kind) {
     case JFG_PREC_MG:
-        mg->apply(r, z, sc, done, st);
+        if (mg32) {
+            vec_launch<0>(st, n, VCast<T, float>{r, r32}, sc, done);
+            mg32->apply(r32, z32, sc, done, st);
+            vec_launch<0>(st, n, VCast<float, T>{z32, z}, sc, done);
+        } else {
+            mg->apply(r, z, sc, done, st);
+        }
         break;
     case JFG_PREC_JACOBI:
         vec_launch<0>(st, n, VMul<T>{dinv, r, z}, sc, done);
@@ -547,8 +556,7 @@ int run_loop(SolverWork& w, const int* flag, const std::vector<uintptr_t>& key, 
                         unsigned long long before = g_launches.load();
                         try {
                             iter();
-                            k_set_cond<<<1, 1, 0, st>>>(h, flag);
-                            note_launch();
+                            launch_ex(k_set_cond, dim3(1), dim3(1), 0, st, h, flag);
                             nodes = (int)(g_launches.load() - before);
                             g_launches.fetch_sub(nodes);
                         } catch (...) {
@@ -661,7 +669,7 @@ int run_cg(SolverWork& w, int ci, Matrix* A, const Precond<T>& M, const T* b, T*
             vec_launch<0>(st, n, VXpby<T>{r, p, c}, sc, done);
         }
     };
-    std::vector<uintptr_t> key{1, (uintptr_t)A->uid, (uintptr_t)(M.mg ? M.mg->uid : 0), (uintptr_t)(M.M ? M.M->uid : 0), (uintptr_t)M.dinv, (uintptr_t)b,
+    std::vector<uintptr_t> key{1, (uintptr_t)A->uid, (uintptr_t)(M.mg ? M.mg->uid : 0), (uintptr_t)(M.M ? M.M->uid : 0), (uintptr_t)(M.mg32 ? M.mg32->uid : 0), (uintptr_t)M.r32, (uintptr_t)M.dinv, (uintptr_t)b,
                                (uintptr_t)x, (uintptr_t)r, (uintptr_t)p, (uintptr_t)z, (uintptr_t)Ap, (uintptr_t)sizeof(T),
                                (uintptr_t)M.kind, (uintptr_t)done};
     return run_loop(w, done, key, iter, use_graph, chunk);
@@ -706,7 +714,7 @@ int run_bicgstab(SolverWork& w, int ci, Matrix* A, const Precond<T>& M, const T*
             vec_launch<1>(st, n, VBicgEnd<T>{x, p, s, s, t, r, c}, sc, done, FinBicgEnd{c});
         }
     };
-    std::vector<uintptr_t> key{2, (uintptr_t)A->uid, (uintptr_t)(M.mg ? M.mg->uid : 0), (uintptr_t)(M.M ? M.M->uid : 0), (uintptr_t)M.dinv, (uintptr_t)b,
+    std::vector<uintptr_t> key{2, (uintptr_t)A->uid, (uintptr_t)(M.mg ? M.mg->uid : 0), (uintptr_t)(M.M ? M.M->uid : 0), (uintptr_t)(M.mg32 ? M.mg32->uid : 0), (uintptr_t)M.r32, (uintptr_t)M.dinv, (uintptr_t)b,
                                (uintptr_t)x, (uintptr_t)r0, (uintptr_t)r, (uintptr_t)p, (uintptr_t)vv, (uintptr_t)s,
                                (uintptr_t)t, (uintptr_t)y, (uintptr_t)z, (uintptr_t)pt, (uintptr_t)sizeof(T),
                                (uintptr_t)M.kind, (uintptr_t)done};
@@ -754,16 +762,16 @@ int run_gmres(SolverWork& w, Matrix* A, const Precond<double>& M, const double* 
             spmv_launch<double, double, 0>(st, A, val, vcur, EpiStore<double>{t}, sc, cdone);
             if (pre) M.apply(t, q, sc, cdone, st);
             dim3 g1(gx, m);
-            k_mdot<double><<<g1, kThreads, 0, st>>>(n, V, qq, c, w.mdot_part.p, cdone);
-            k_mdot_fin<<<m, kThreads, 0, st>>>(gx, w.mdot_part.p, c, w.fac.p, cdone);
-            JFG_CUDA(cudaGetLastError());
-            note_launch(2);
+            launch_ex(k_mdot<double>, g1, dim3(kThreads), 0, st, n, (const double*)V, qq, (const Ctl*)c,
+                      w.mdot_part.p, cdone);
+            launch_ex(k_mdot_fin, dim3(m), dim3(kThreads), 0, st, gx, (const double*)w.mdot_part.p, (const Ctl*)c,
+                      w.fac.p, cdone);
             vec_launch<1>(st, n, VGmresW<double>{V, qq, wv, w.fac.p, c, n}, sc, cdone,
                           FinGivens{c, w.H.p, w.gam.p, w.cs.p, w.sn.p, w.fac.p, ldh});
             vec_launch<0>(st, n, VGmresNext<double>{V, vcur, wv, w.H.p, c, n, ldh}, sc, cdone);
             scalar_launch(st, GmresAdvance{c}, cdone);
         };
-        std::vector<uintptr_t> key{3, (uintptr_t)A->uid, (uintptr_t)(M.mg ? M.mg->uid : 0), (uintptr_t)(M.M ? M.M->uid : 0), (uintptr_t)M.dinv,
+        std::vector<uintptr_t> key{3, (uintptr_t)A->uid, (uintptr_t)(M.mg ? M.mg->uid : 0), (uintptr_t)(M.M ? M.M->uid : 0), (uintptr_t)(M.mg32 ? M.mg32->uid : 0), (uintptr_t)M.r32, (uintptr_t)M.dinv,
                                    (uintptr_t)x, (uintptr_t)V, (uintptr_t)M.kind, (uintptr_t)m, (uintptr_t)t,
                                    (uintptr_t)q, (uintptr_t)wv, (uintptr_t)vcur, (uintptr_t)w.H.p,
                                    (uintptr_t)w.fac.p, (uintptr_t)w.mdot_part.p, (uintptr_t)cdone};

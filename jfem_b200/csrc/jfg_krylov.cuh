@@ -15,6 +15,11 @@ struct Precond {
     Matrix* M = nullptr;
     const T* dinv = nullptr;
     int n = 0;
+    // FP64 iteration with an FP32 multigrid preconditioner: r is rounded to
+    // FP32 into r32, the FP32 hierarchy computes z32, z is z32 widened.
+    MGImpl<float>* mg32 = nullptr;
+    float* r32 = nullptr;
+    float* z32 = nullptr;
     void apply(const T* r, T* z, const Scratch& sc, const int* done, cudaStream_t st) const;
 };
 

@@ -107,6 +107,28 @@ int choose_lpr_log2(double avg)
 
 std::atomic<unsigned long long> g_launches{0};
 
+bool use_pdl()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("JFEM_PDL");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v == 1;
+}
+
+int sm_count()
+{
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
 uint64_t next_uid()
 {
     static std::atomic<uint64_t> ctr{1};
@@ -144,21 +166,21 @@ static Matrix* build_from_sorted(Context* c, int rows, int cols, int64_t m, cons
     int r = 0;
     rb.push_back(0);
     // Greedy partition into row blocks of <= kBlockRows rows and
-    // <= kBlockNnz - 4 nonzeros (a longer row forms a block of its own).  Each
-    // block starts on a 4-element boundary; the <= 3 padding slots before it
-    // hold column 0 / value 0 and are summed into the previous block's last
-    // row as exact zeros.
+    // <= kBlockNnz - 8 nonzeros (a longer row forms a block of its own).  Each
+    // block starts on an 8-element boundary (16-byte aligned bulk copies for
+    // every value type); the <= 7 padding slots before it hold column 0 /
+    // value 0 and are summed into the previous block's last row as exact zeros.
     while (r < rows) {
-        off = (off + 3) & ~int64_t(3);
+        off = (off + 7) & ~int64_t(7);
         int start = r;
         int64_t bnnz = 0;
         while (r < rows && r - start < kBlockRows) {
             int len = h_cnt[r];
-            if (r > start && bnnz + len > kBlockNnz - 4) break;
+            if (r > start && bnnz + len > kBlockNnz - 8) break;
             newptr[r] = (int)(off + bnnz);
             bnnz += len;
             r++;
-            if (bnnz > kBlockNnz - 4) break;
+            if (bnnz > kBlockNnz - 8) break;
         }
         off += bnnz;
         rb.push_back(r);
@@ -167,7 +189,7 @@ static Matrix* build_from_sorted(Context* c, int rows, int cols, int64_t m, cons
     newptr[rows] = (int)off;
     JFG_CHECK(off < (int64_t)INT32_MAX - 64, JFG_ERR_UNSUPPORTED, "matrix has more than 2^31 nonzeros");
     M->nblocks = (int)rb.size() - 1;
-    M->nnz_padded = off + 8;
+    M->nnz_padded = off + 16;   // slack: bulk copies round the last block up to 8 elements
     M->rb.alloc(rb.size());
     M->rowptr.alloc((size_t)rows + 1);
     M->col.alloc((size_t)M->nnz_padded);

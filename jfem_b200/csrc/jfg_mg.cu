@@ -35,6 +35,7 @@ template <typename T>
 __global__ void k_coarse_gemv(int n, const double* __restrict__ ainv, const T* __restrict__ rhs, T* __restrict__ x,
                               const int* __restrict__ done)
 {
+    pdl_wait();
     if (done && *done) return;
     int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
@@ -51,6 +52,7 @@ __global__ void k_bc_defect(int naff, const int* __restrict__ row, const int* __
                             const int* __restrict__ col, const T* __restrict__ val, const T* __restrict__ v,
                             T* __restrict__ d, const int* __restrict__ done)
 {
+    pdl_wait();
     if (done && *done) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= naff) return;
@@ -65,6 +67,7 @@ template <typename T>
 __global__ void k_bc_add(int nb, const int* __restrict__ bd, const T* __restrict__ v, T* __restrict__ out,
                          const int* __restrict__ done)
 {
+    pdl_wait();
     if (done && *done) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < nb) out[bd[i]] = v[bd[i]] + out[bd[i]];
@@ -245,9 +248,7 @@ template <typename T>
 void MGImpl<T>::coarse(const T* rhs, T* out, const int* done, cudaStream_t st)
 {
     int n0 = n[0];
-    k_coarse_gemv<T><<<(n0 + 7) / 8, 256, 0, st>>>(n0, ainv0.p, rhs, out, done);
-    JFG_CUDA(cudaGetLastError());
-    note_launch();
+    launch_ex(k_coarse_gemv<T>, dim3((n0 + 7) / 8), dim3(256), 0, st, n0, (const double*)ainv0.p, rhs, out, done);
 }
 
 // Smoother.smooth on level l with rhs; the result ends in x[l].
@@ -334,9 +335,8 @@ void MGImpl<T>::apply(const T* v, T* out, const Scratch& sc, const int* done, cu
     T* defect = b[Lf].p;
     vec_launch<0>(st, m, VCopy<T>{v, defect}, sc, done);
     if (naff) {
-        k_bc_defect<T><<<nb(naff), 256, 0, st>>>(naff, aff_row.p, aff_ptr.p, aff_col.p, aff_val.p, v, defect, done);
-        JFG_CUDA(cudaGetLastError());
-        note_launch();
+        launch_ex(k_bc_defect<T>, dim3(nb(naff)), dim3(256), 0, st, naff, (const int*)aff_row.p,
+                  (const int*)aff_ptr.p, (const int*)aff_col.p, (const T*)aff_val.p, v, defect, done);
     }
     bool xzero = true;
     if (use_fmg && L > 1) {
@@ -358,9 +358,7 @@ void MGImpl<T>::apply(const T* v, T* out, const Scratch& sc, const int* done, cu
     }
     vec_launch<0>(st, m, VCopy<T>{x[Lf].p, out}, sc, done);
     if (nbd_fine) {
-        k_bc_add<T><<<nb(nbd_fine), 256, 0, st>>>(nbd_fine, bd_fine.p, v, out, done);
-        JFG_CUDA(cudaGetLastError());
-        note_launch();
+        launch_ex(k_bc_add<T>, dim3(nb(nbd_fine)), dim3(256), 0, st, nbd_fine, (const int*)bd_fine.p, v, out, done);
     }
 }
 

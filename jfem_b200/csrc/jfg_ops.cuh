@@ -93,16 +93,61 @@ struct EpiMaskedAdd {  // x += mask ? 0 : A e   (prolongation + correction, MGPr
 // ---------------------------------------------------------------------------
 // launch helpers
 // ---------------------------------------------------------------------------
+// Kernel launch with the programmatic-stream-serialization attribute (PDL):
+// the next kernel may be scheduled while this one drains; every solve-path
+// kernel starts with griddepcontrol.wait.  JFEM_PDL=0 disables it.
+bool use_pdl();
+
+template <typename... KArgs, typename... Args>
+void launch_ex(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = use_pdl() ? 1 : 0;
+    JFG_CUDA(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
+    note_launch();
+}
+
+template <typename VT> struct StagesOf { static constexpr int S = sizeof(VT) == 8 ? 3 : 4; };
+
+int sm_count();
+
+// Persistent grid of the pipelined SpMV for one kernel instance: resident
+// CTAs per SM (from the occupancy calculator) x SM count, capped by the
+// number of row blocks.
+template <typename K>
+int persistent_ctas(K kern, int smem)
+{
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        JFG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        int b = 0;
+        JFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kThreads, smem));
+        per_sm = b > 0 ? b : 1;
+    }
+    return per_sm * sm_count();
+}
+
 template <typename VT, typename XT, int NR, class Epi, class Fin = NoFin>
 void spmv_launch(cudaStream_t st, const Matrix* M, const VT* val, const XT* x, Epi epi, const Scratch& sc,
                  const int* done, Fin fin = Fin())
 {
     if (M->rows == 0) return;
+    constexpr int S = StagesOf<VT>::S;
+    constexpr int smem = spmv_smem_bytes<VT, S>();
     GridRed<NR, Fin> red{sc.partials, sc.counter, fin};
-    SpmvArgs a{M->rb.p, M->rowptr.p, M->col.p};
-    k_spmv<VT, XT, NR, Epi, Fin><<<M->nblocks, kThreads, 0, st>>>(a, val, x, ilog2(M->lpr), epi, red, done);
-    JFG_CUDA(cudaGetLastError());
-    note_launch();
+    SpmvArgs a{M->rb.p, M->rowptr.p, M->col.p, M->nblocks};
+    auto kern = k_spmv<VT, XT, NR, S, Epi, Fin>;
+    int grid = persistent_ctas(kern, smem);
+    if (grid > M->nblocks) grid = M->nblocks;
+    launch_ex(kern, dim3(grid), dim3(kThreads), smem, st, a, val, x, ilog2(M->lpr), epi, red, done);
 }
 
 inline int vec_grid(int n)
@@ -115,17 +160,13 @@ template <int NR, class F, class Fin = NoFin>
 void vec_launch(cudaStream_t st, int n, F f, const Scratch& sc, const int* done, Fin fin = Fin())
 {
     GridRed<NR, Fin> red{sc.partials, sc.counter, fin};
-    k_vec<NR, F, Fin><<<vec_grid(n), kThreads, 0, st>>>(n, f, red, done);
-    JFG_CUDA(cudaGetLastError());
-    note_launch();
+    launch_ex(k_vec<NR, F, Fin>, dim3(vec_grid(n)), dim3(kThreads), 0, st, n, f, red, done);
 }
 
 template <class F>
 void scalar_launch(cudaStream_t st, F f, const int* done)
 {
-    k_scalar<F><<<1, 1, 0, st>>>(f, done);
-    JFG_CUDA(cudaGetLastError());
-    note_launch();
+    launch_ex(k_scalar<F>, dim3(1), dim3(1), 0, st, f, done);
 }
 
 // ---------------------------------------------------------------------------
@@ -155,6 +196,12 @@ struct VScaleMul {  // y = (dinv * b) * omega      (first Jacobi sweep from a ze
     T* y;
     T omega;
     template <int K> __device__ void operator()(int i, double (&)[K]) const { y[i] = (T)0 + (dinv[i] * b[i]) * omega; }
+};
+template <typename A, typename B>
+struct VCast {  // b = (B) a
+    const A* a;
+    B* b;
+    template <int K> __device__ void operator()(int i, double (&)[K]) const { b[i] = (B)a[i]; }
 };
 template <typename T>
 struct VMul {  // y = d * x

@@ -294,7 +294,9 @@ def _as_device(op) -> DeviceMatrix:
 
 
 class IterativeSolver:
-    """linalg/IterativeSolver.java.  ``precision`` ('fp64' or 'mixed'),
+    """linalg/IterativeSolver.java.  ``precision`` ('fp64', 'mixed' = FP64
+    defect correction around FP32 inner solves, or 'mixed-precond' = FP64
+    iteration with an FP32 multigrid preconditioner),
     ``use_graph`` and ``history_cap`` select the GPU execution; the defaults
     reproduce the reference's FP64 semantics."""
 
@@ -334,7 +336,10 @@ class IterativeSolver:
         opts.maxit = maxit
         opts.restart = self.gm.ITERATIONS_BEFORE_RESTART
         opts.max_restarts = self.gm.MAX_RESTARTS
-        opts.precision = N.MIXED if self.precision == "mixed" else N.FP64
+        modes = {"fp64": N.FP64, "mixed": N.MIXED, "mixed-precond": N.MIXED_PRECOND}
+        if self.precision not in modes:
+            raise IllegalArgumentException(f"unknown precision {self.precision!r}")
+        opts.precision = modes[self.precision]
         opts.inner_rtol = self.inner_rtol
         opts.use_graph = 1 if self.use_graph else 0
         hist = np.zeros(max(self.history_cap, 1))

@@ -93,6 +93,12 @@ def test_mixed_precision_pcg(ctx):
     assert s.last.final_residual <= tol
     assert rel(x, ref.x) < 1e-7
     assert s.last.outer_iterations >= 2
+    s = IterativeSolver(ctx=ctx)
+    s.precision = "mixed-precond"
+    x = s.solvePCG(mats[-1], mg, b, tol)
+    assert s.last.status == N.OK and s.last.final_residual <= tol
+    assert rel(x, ref.x) < 1e-7
+    assert abs(s.iterations - ref.iterations) <= 1
 
 
 @pytest.mark.parametrize("name", ["symm", "nonsymm", "good_nonsymm"])
@@ -201,9 +207,10 @@ def test_pcg_mg_full_size(ctx):
     x64 = s.solvePCG(mats[-1], mg, b, tol)
     assert s.last.status == N.OK and s.last.final_residual <= tol
     it64 = s.iterations
-    s2 = IterativeSolver(ctx=ctx)
-    s2.precision = "mixed"
-    x32 = s2.solvePCG(mats[-1], mg, b, tol)
-    assert s2.last.status == N.OK and s2.last.final_residual <= tol
-    assert rel(x32, x64) < 1e-7
+    for mode in ("mixed", "mixed-precond"):
+        s2 = IterativeSolver(ctx=ctx)
+        s2.precision = mode
+        x32 = s2.solvePCG(mats[-1], mg, b, tol)
+        assert s2.last.status == N.OK and s2.last.final_residual <= tol, mode
+        assert rel(x32, x64) < 1e-7, mode
     assert it64 <= 20
