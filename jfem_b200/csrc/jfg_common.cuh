@@ -1,13 +1,10 @@
 // Shared definitions of the JFEM linear-solve library for sm_100a.
 //
 // Layout decisions (all device memory is owned by the library):
-//   * matrices live as a padded CSR whose row blocks start on 16-byte
-//     boundaries ("row-block CSR"): block b covers rows [rb[b], rb[b+1]) and
-//     its nonzeros [rowptr[rb[b]], rowptr[rb[b+1]]) with rowptr[rb[b]] a
-//     multiple of 4.  One CTA streams one row block with 128-bit loads into
-//     shared memory and reduces rows with LPR lanes per row;
-//   * values exist in FP64 and, on demand, FP32 (mixed-precision inner
-//     solves) -- both copies share the index arrays;
+//   * matrices live in SELL-32-sigma for the products (see Matrix) plus a
+//     plain CSR copy for set-up work;
+//   * values exist in FP64 and, on demand, FP32 / BF16 (mixed-precision
+//     hierarchies) -- all copies share the index arrays;
 //   * all scalars of an iterative solve (alpha, beta, <r,r>, flags, the
 //     iteration counter and the residual history) live in a device control
 //     block, so a whole Krylov iteration is a fixed kernel sequence that can be
@@ -26,8 +23,6 @@
 namespace jfg {
 
 constexpr int kThreads = 256;          // threads per CTA in streaming kernels
-constexpr int kBlockNnz = 2048;        // nonzeros staged per row block
-constexpr int kBlockRows = 256;        // rows per row block (<= kThreads)
 constexpr int kVecGrid = 148 * 8;      // fixed grid of the vector kernels (SM count x 8)
 
 struct Error {
@@ -97,17 +92,31 @@ struct Ctl {
 struct Context;
 
 // Row-block CSR matrix on the device.
+// Two layouts on the device:
+//   * CSR (csr_*): merged, sorted by row then column; used by set-up code
+//     (transposes, diagonal, dense extraction);
+//   * SELL-32-sigma (the SpMV layout): rows are sorted by length inside
+//     windows of kSellSigma rows, cut into slices of 32 rows, and each slice
+//     is stored column-major padded to its longest row: entry k of slice lane
+//     l lives at off[s] + 32 k + l.  perm[32 s + l] is the original row (-1
+//     for the padding rows of the last slice).  One thread owns one row.
+constexpr int kSliceRows = 32;
+constexpr int kSellSigma = 256;
+
 struct Matrix {
     Context* ctx = nullptr;
     int rows = 0, cols = 0;
-    int64_t nnz = 0;              // stored nonzeros after merging (excl. padding)
-    int64_t nnz_padded = 0;       // length of col/val arrays
-    int nblocks = 0;
-    int lpr = 4;                  // lanes per row used in the reduction phase
-    DevBuf<int> rb;               // nblocks + 1 row-block starts
-    DevBuf<int> rowptr;           // rows + 1 (padded offsets)
-    DevBuf<int> col;              // nnz_padded
-    DevBuf<double> val;           // nnz_padded
+    int64_t nnz = 0;              // stored nonzeros after merging
+    DevBuf<int> csr_ptr;          // rows + 1
+    DevBuf<int> csr_col;          // nnz
+    DevBuf<double> csr_val;       // nnz
+    int nslices = 0;
+    int64_t sell_len = 0;         // length of the SELL col/val arrays
+    int nblocks = 0;              // CTAs of one SpMV launch (kThreads rows each)
+    DevBuf<int> off;              // nslices + 1 slice offsets
+    DevBuf<int> perm;             // nslices * 32 original row of each slot
+    DevBuf<int> col;              // sell_len
+    DevBuf<double> val;           // sell_len
     DevBuf<float> val32;          // optional FP32 copy
     DevBuf<__nv_bfloat16> val16;  // optional BF16 copy
     DevBuf<double> diag;          // merged diagonal

@@ -118,176 +118,58 @@ __device__ __forceinline__ float to_acc(__nv_bfloat16 v) { return __bfloat162flo
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;"); }
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait: gives up after ~2^32 SM cycles (about 2 s) and reports false.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity)
-{
-    long long t0 = clock64();
-    while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > (1LL << 32)) return false;
-    }
-    return true;
-}
-// 1-D bulk copy global -> shared completing on an mbarrier (both addresses
-// 16-byte aligned, size a multiple of 16; no multicast).
-__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-
-// Device-side error word (set when a bounded wait gives up); read by the host.
-__device__ int g_device_error;
 
 // ---------------------------------------------------------------------------
-// row-block CSR SpMV: y-row sums handed to an epilogue
+// SELL-32-sigma SpMV: row sums handed to an epilogue
 // ---------------------------------------------------------------------------
 // Epilogue concept:  __device__ void operator()(int row, AT sum, double (&acc)[NR]) const
 // It writes its outputs for `row` and may add to the NR reduction values.
 struct SpmvArgs {
-    const int* rb;
-    const int* rowptr;
-    const int* col;
-    int nblocks;
+    const int* off;     // nslices + 1
+    const int* perm;    // nslices * 32
+    const int* col;     // SELL column indices
+    int nslots;         // nslices * 32
 };
 
-// Shared-memory layout of the pipelined SpMV: S stages of (columns, values),
-// then the product buffer, then S mbarriers.
-constexpr int kStageCap = kBlockNnz + 8;
-template <typename VT>
-__host__ __device__ constexpr int stage_bytes() { return kStageCap * (4 + (int)sizeof(VT)); }
-template <typename VT, int S>
-__host__ __device__ constexpr int spmv_smem_bytes()
-{
-    return S * stage_bytes<VT>() + kStageCap * (int)sizeof(typename AccOf<VT>::T) + S * 8 + 16;
-}
-
-// Persistent, TMA-pipelined SpMV.  CTA c handles row blocks c, c+G, c+2G, ...
-// Thread 0 keeps S blocks in flight: one bulk copy each for the block's
-// column indices and values into a shared-memory stage, completing on the
-// stage's mbarrier.  For the current block all threads gather x[col] and form
-// the products (8 independent gathers per thread), the stage is handed back
-// to the producer, and groups of 2^lpr_log2 lanes reduce rows from the
-// product buffer and call the epilogue.  Blocks longer than the stage (one
-// long row) are read directly from global memory.
-template <typename VT, typename XT, int NR, int S, class Epi, class Fin>
+// One thread per slot (row) of a 32-row slice.  A warp reads one slice
+// column per step: 32 consecutive column indices and 32 consecutive values
+// (fully coalesced), gathers x, and accumulates its row in a fixed order.
+// No shared memory, no barriers: occupancy and the unrolled independent loads
+// hide the gather latency.
+template <typename VT, typename XT, int NR, class Epi, class Fin>
 __global__ void __launch_bounds__(kThreads)
-k_spmv(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, int lpr_log2, Epi epi,
-       GridRed<NR, Fin> red, const int* __restrict__ done)
+k_spmv(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi, GridRed<NR, Fin> red,
+       const int* __restrict__ done)
 {
     using AT = typename AccOf<VT>::T;
     pdl_wait();
     if (done && *done) return;
-    extern __shared__ __align__(128) unsigned char smem[];
-    AT* prod = reinterpret_cast<AT*>(smem + S * stage_bytes<VT>());
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S * stage_bytes<VT>() + kStageCap * sizeof(AT));
-    __shared__ int ok_sh;
-    const int tid = threadIdx.x;
-    const int first = blockIdx.x, G = gridDim.x;
-    const int nmine = first < m.nblocks ? (m.nblocks - 1 - first) / G + 1 : 0;
-    if (tid == 0) {
-        for (int s = 0; s < S; s++) mbar_init(&bars[s], 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-    auto stage_col = [&](int s) { return reinterpret_cast<int*>(smem + s * stage_bytes<VT>()); };
-    auto stage_val = [&](int s) { return reinterpret_cast<VT*>(smem + s * stage_bytes<VT>() + kStageCap * 4); };
-    auto issue = [&](int it) {   // thread 0 only
-        const int b = first + it * G;
-        const int s = it % S;
-        const int k0 = m.rowptr[m.rb[b]], k1 = m.rowptr[m.rb[b + 1]];
-        const int nk = k1 - k0;
-        if (nk > 0 && nk <= kBlockNnz) {
-            const int nkp = (nk + 7) & ~7;
-            const uint32_t bc = nkp * 4u, bv = nkp * (uint32_t)sizeof(VT);
-            mbar_arrive_expect_tx(&bars[s], bc + bv);
-            tma_load_1d(stage_col(s), m.col + k0, bc, &bars[s]);
-            tma_load_1d(stage_val(s), val + k0, bv, &bars[s]);
-        } else {
-            mbar_arrive(&bars[s]);
-        }
-    };
-    if (tid == 0)
-        for (int it = 0; it < S && it < nmine; it++) issue(it);
     double acc[NR > 0 ? NR : 1];
 #pragma unroll
     for (int i = 0; i < (NR > 0 ? NR : 1); i++) acc[i] = 0;
-    const int lpr = 1 << lpr_log2;
-    const int g = tid >> lpr_log2;
-    const int lane = tid & (lpr - 1);
-    const int ngroups = kThreads >> lpr_log2;
-    int it = 0;
-    for (; it < nmine; it++) {
-        const int b = first + it * G;
-        const int s = it % S;
-        const int r0 = m.rb[b], r1 = m.rb[b + 1];
-        const int k0 = m.rowptr[r0], k1 = m.rowptr[r1];
-        const int nk = k1 - k0;
-        if (tid == 0) ok_sh = mbar_wait_bounded(&bars[s], (it / S) & 1) ? 1 : 0;
-        __syncthreads();
-        if (!ok_sh) {
-            if (tid == 0) atomicExch(&g_device_error, 1);
-            break;
+    const int slot = blockIdx.x * kThreads + threadIdx.x;
+    if (slot < m.nslots) {
+        const int s = slot >> 5, lane = slot & 31;
+        const int o = __ldg(m.off + s);
+        const int len = (__ldg(m.off + s + 1) - o) >> 5;
+        const int r = __ldg(m.perm + slot);
+        const int* cp = m.col + o + lane;
+        const VT* vp = val + o + lane;
+        AT sum = 0;
+        int k = 0;
+        for (; k + 4 <= len; k += 4) {
+            const int c0 = __ldg(cp + 32 * k), c1 = __ldg(cp + 32 * (k + 1));
+            const int c2 = __ldg(cp + 32 * (k + 2)), c3 = __ldg(cp + 32 * (k + 3));
+            const AT v0 = to_acc(__ldg(vp + 32 * k)), v1 = to_acc(__ldg(vp + 32 * (k + 1)));
+            const AT v2 = to_acc(__ldg(vp + 32 * (k + 2))), v3 = to_acc(__ldg(vp + 32 * (k + 3)));
+            const AT x0 = (AT)__ldg(x + c0), x1 = (AT)__ldg(x + c1), x2 = (AT)__ldg(x + c2), x3 = (AT)__ldg(x + c3);
+            sum += v0 * x0;
+            sum += v1 * x1;
+            sum += v2 * x2;
+            sum += v3 * x3;
         }
-        if (nk <= kBlockNnz) {
-            const int* sc = stage_col(s);
-            const VT* sv = stage_val(s);
-#pragma unroll
-            for (int j = 0; j < kBlockNnz / kThreads; j++) {
-                const int k = tid + j * kThreads;
-                if (k < nk) prod[k] = to_acc(sv[k]) * (AT)__ldg(x + sc[k]);
-            }
-            __syncthreads();
-            if (tid == 0 && it + S < nmine) issue(it + S);
-            for (int base = r0; base < r1; base += ngroups) {
-                const int r = base + g;
-                AT sum = 0;
-                if (r < r1) {
-                    const int a = m.rowptr[r] - k0, e = m.rowptr[r + 1] - k0;
-                    for (int k = a + lane; k < e; k += lpr) sum += prod[k];
-                }
-                for (int o = lpr >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-                if (r < r1 && lane == 0) epi(r, sum, acc);
-            }
-            __syncthreads();
-        } else {
-            double part[1] = {0};
-            for (int k = k0 + tid; k < k1; k += kThreads)
-                part[0] += (double)(to_acc(val[k]) * (AT)__ldg(x + m.col[k]));
-            block_sum<1>(part);
-            if (tid == 0) epi(r0, (AT)part[0], acc);
-            if (tid == 0 && it + S < nmine) issue(it + S);
-            __syncthreads();
-        }
-    }
-    if (it < nmine && tid == 0) {
-        // a wait gave up: let the copies already issued land (bounded) before exit
-        for (int j = it + 1; j < nmine && j < it + S; j++) mbar_wait_bounded(&bars[j % S], (j / S) & 1);
+        for (; k < len; k++) sum += to_acc(__ldg(vp + 32 * k)) * (AT)__ldg(x + __ldg(cp + 32 * k));
+        if (r >= 0) epi(r, sum, acc);
     }
     pdl_launch_dependents();
     if constexpr (NR > 0) red.reduce(acc);

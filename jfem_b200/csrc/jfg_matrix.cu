@@ -1,109 +1,14 @@
-// COO -> row-block CSR conversion on the device, transposes, precision
-// copies and the plain SpMV entry points.
+// COO -> CSR -> SELL-32-sigma conversion on the device, transposes and
+// precision copies.
 #include <cub/cub.cuh>
 
 #include <algorithm>
 #include <atomic>
+#include <numeric>
 
 #include "jfg_kernels.cuh"
 
 namespace jfg {
-
-namespace {
-
-__global__ void k_make_keys(int64_t nnz, const int* ri, const int* ci, int rows, int cols, uint64_t* key,
-                            int* bad)
-{
-    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nnz) return;
-    int r = ri[k], c = ci[k];
-    if (r < 0 || r >= rows || c < 0 || c >= cols) {
-        atomicExch(bad, 1);
-        r = 0;
-        c = 0;
-    }
-    key[k] = (uint64_t)r * (uint64_t)cols + (uint64_t)c;
-}
-
-__global__ void k_nonzero_flags(int64_t m, const double* v, char* f)
-{
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < m) f[i] = v[i] != 0.0;
-}
-
-__global__ void k_row_counts(int64_t m, const uint64_t* key, int cols, int* cnt)
-{
-    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= m) return;
-    atomicAdd(cnt + (int)(key[k] / (uint64_t)cols), 1);
-}
-
-__global__ void k_scatter_padded(int64_t m, const uint64_t* key, const double* v, int cols, const int64_t* oldptr,
-                                 const int* newptr, int* col, double* val)
-{
-    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= m) return;
-    int r = (int)(key[k] / (uint64_t)cols);
-    int c = (int)(key[k] % (uint64_t)cols);
-    int64_t pos = newptr[r] + (k - oldptr[r]);
-    col[pos] = c;
-    val[pos] = v[k];
-}
-
-__global__ void k_diag(int rows, int cols, const int* rowptr, const int* col, const double* val, double* d)
-{
-    int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= rows) return;
-    double s = 0;
-    if (r < cols)
-        for (int k = rowptr[r]; k < rowptr[r + 1]; k++)
-            if (col[k] == r) s += val[k];
-    d[r] = s;
-}
-
-__global__ void k_expand_rows(int rows, const int* rowptr, int* ri_out, const int64_t* dense_off)
-{
-    int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= rows) return;
-    int64_t o = dense_off[r];
-    for (int k = rowptr[r]; k < rowptr[r + 1]; k++) ri_out[o + (k - rowptr[r])] = r;
-}
-
-__global__ void k_compact(int rows, const int* rowptr, const int* col, const double* val, const int64_t* dense_off,
-                          int* ci_out, double* v_out)
-{
-    int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= rows) return;
-    int64_t o = dense_off[r];
-    for (int k = rowptr[r]; k < rowptr[r + 1]; k++) {
-        ci_out[o + (k - rowptr[r])] = col[k];
-        v_out[o + (k - rowptr[r])] = val[k];
-    }
-}
-
-__global__ void k_to_f32(int64_t n, const double* a, float* b)
-{
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) b[i] = (float)a[i];
-}
-__global__ void k_to_bf16(int64_t n, const double* a, __nv_bfloat16* b)
-{
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) b[i] = __float2bfloat16_rn((float)a[i]);
-}
-
-inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
-
-int choose_lpr_log2(double avg)
-{
-    if (avg <= 3) return 1;
-    if (avg <= 12) return 2;
-    if (avg <= 24) return 3;
-    if (avg <= 48) return 4;
-    return 5;
-}
-
-}  // namespace
 
 std::atomic<unsigned long long> g_launches{0};
 
@@ -138,82 +43,182 @@ uint64_t next_uid()
 Matrix::Matrix() : uid(next_uid()) {}
 Matrix::~Matrix() { delete transposed; }
 
-// Builds the padded row-block layout from merged, sorted, zero-free COO that
-// is already on the device (keys = row*cols+col, ascending).
+namespace {
+
+inline unsigned nblk(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+__global__ void k_make_keys(int64_t nnz, const int* ri, const int* ci, int rows, int cols, uint64_t* key, int* bad)
+{
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nnz) return;
+    int r = ri[k], c = ci[k];
+    if (r < 0 || r >= rows || c < 0 || c >= cols) {
+        atomicExch(bad, 1);
+        r = 0;
+        c = 0;
+    }
+    key[k] = (uint64_t)r * (uint64_t)cols + (uint64_t)c;
+}
+
+__global__ void k_nonzero_flags(int64_t m, const double* v, char* f)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) f[i] = v[i] != 0.0;
+}
+
+__global__ void k_row_counts(int64_t m, const uint64_t* key, int cols, int* cnt)
+{
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    atomicAdd(cnt + (int)(key[k] / (uint64_t)cols), 1);
+}
+
+// merged sorted keys -> CSR column indices (values are already in CSR order)
+__global__ void k_key_cols(int64_t m, const uint64_t* key, int cols, int* col)
+{
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < m) col[k] = (int)(key[k] % (uint64_t)cols);
+}
+
+__global__ void k_diag(int rows, int cols, const int* ptr, const int* col, const double* val, double* d)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    double s = 0;
+    if (r < cols)
+        for (int k = ptr[r]; k < ptr[r + 1]; k++)
+            if (col[k] == r) s += val[k];
+    d[r] = s;
+}
+
+// one thread per SELL slot: copies its row into the slice column-major and
+// pads with (last column of the row, 0.0)
+__global__ void k_fill_sell(int nslots, const int* perm, const int* off, const int* ptr, const int* ccol,
+                            const double* cval, int* col, double* val)
+{
+    int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= nslots) return;
+    int s = slot >> 5, lane = slot & 31;
+    int o = off[s];
+    int len = (off[s + 1] - o) >> 5;
+    int r = perm[slot];
+    int a = 0, e = 0;
+    if (r >= 0) {
+        a = ptr[r];
+        e = ptr[r + 1];
+    }
+    int pad_col = e > a ? ccol[e - 1] : 0;
+    for (int k = 0; k < len; k++) {
+        int64_t dst = (int64_t)o + (int64_t)k * 32 + lane;
+        if (a + k < e) {
+            col[dst] = ccol[a + k];
+            val[dst] = cval[a + k];
+        } else {
+            col[dst] = pad_col;
+            val[dst] = 0.0;
+        }
+    }
+}
+
+__global__ void k_expand_rows(int rows, const int* ptr, int* ri)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    for (int k = ptr[r]; k < ptr[r + 1]; k++) ri[k] = r;
+}
+
+__global__ void k_to_f32(int64_t n, const double* a, float* b)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (float)a[i];
+}
+__global__ void k_to_bf16(int64_t n, const double* a, __nv_bfloat16* b)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = __float2bfloat16_rn((float)a[i]);
+}
+
+}  // namespace
+
+// Builds CSR and SELL-32-sigma from merged, sorted, zero-free COO that is
+// already on the device (keys = row*cols+col ascending, values alongside).
 static Matrix* build_from_sorted(Context* c, int rows, int cols, int64_t m, const uint64_t* d_key,
                                  const double* d_val)
 {
     cudaStream_t s = c->stream;
+    JFG_CHECK(m < (int64_t)INT32_MAX - 64, JFG_ERR_UNSUPPORTED, "matrix has more than 2^31 nonzeros");
     auto* M = new Matrix();
     M->ctx = c;
     M->rows = rows;
     M->cols = cols;
     M->nnz = m;
+    // row counts -> CSR row pointers
     DevBuf<int> cnt;
     cnt.alloc((size_t)rows + 1);
     JFG_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * ((size_t)rows + 1), s));
     if (m) k_row_counts<<<nblk(m), 256, 0, s>>>(m, d_key, cols, cnt.p);
     JFG_CUDA(cudaGetLastError());
-    std::vector<int> h_cnt(rows + 1);
-    JFG_CUDA(cudaMemcpyAsync(h_cnt.data(), cnt.p, sizeof(int) * rows, cudaMemcpyDeviceToHost, s));
+    std::vector<int> len(rows + 1, 0);
+    JFG_CUDA(cudaMemcpyAsync(len.data(), cnt.p, sizeof(int) * rows, cudaMemcpyDeviceToHost, s));
     JFG_CUDA(cudaStreamSynchronize(s));
-    // merged offsets and the padded row-block layout
-    std::vector<int64_t> oldptr(rows + 1, 0);
-    for (int r = 0; r < rows; r++) oldptr[r + 1] = oldptr[r] + h_cnt[r];
-    std::vector<int> rb;
-    std::vector<int> newptr(rows + 1, 0);
-    int64_t off = 0;
-    int r = 0;
-    rb.push_back(0);
-    // Greedy partition into row blocks of <= kBlockRows rows and
-    // <= kBlockNnz - 8 nonzeros (a longer row forms a block of its own).  Each
-    // block starts on an 8-element boundary (16-byte aligned bulk copies for
-    // every value type); the <= 7 padding slots before it hold column 0 /
-    // value 0 and are summed into the previous block's last row as exact zeros.
-    while (r < rows) {
-        off = (off + 7) & ~int64_t(7);
-        int start = r;
-        int64_t bnnz = 0;
-        while (r < rows && r - start < kBlockRows) {
-            int len = h_cnt[r];
-            if (r > start && bnnz + len > kBlockNnz - 8) break;
-            newptr[r] = (int)(off + bnnz);
-            bnnz += len;
-            r++;
-            if (bnnz > kBlockNnz - 8) break;
-        }
-        off += bnnz;
-        rb.push_back(r);
+    std::vector<int> ptr(rows + 1, 0);
+    for (int r = 0; r < rows; r++) ptr[r + 1] = ptr[r] + len[r];
+    M->csr_ptr.alloc((size_t)rows + 1);
+    M->csr_col.alloc(m ? (size_t)m : 1);
+    M->csr_val.alloc(m ? (size_t)m : 1);
+    JFG_CUDA(cudaMemcpyAsync(M->csr_ptr.p, ptr.data(), sizeof(int) * (rows + 1), cudaMemcpyHostToDevice, s));
+    if (m) {
+        k_key_cols<<<nblk(m), 256, 0, s>>>(m, d_key, cols, M->csr_col.p);
+        JFG_CUDA(cudaMemcpyAsync(M->csr_val.p, d_val, sizeof(double) * m, cudaMemcpyDeviceToDevice, s));
     }
-    if (rows == 0) rb.push_back(0);
-    newptr[rows] = (int)off;
-    JFG_CHECK(off < (int64_t)INT32_MAX - 64, JFG_ERR_UNSUPPORTED, "matrix has more than 2^31 nonzeros");
-    M->nblocks = (int)rb.size() - 1;
-    M->nnz_padded = off + 16;   // slack: bulk copies round the last block up to 8 elements
-    M->rb.alloc(rb.size());
-    M->rowptr.alloc((size_t)rows + 1);
-    M->col.alloc((size_t)M->nnz_padded);
-    M->val.alloc((size_t)M->nnz_padded);
-    JFG_CUDA(cudaMemcpyAsync(M->rb.p, rb.data(), sizeof(int) * rb.size(), cudaMemcpyHostToDevice, s));
-    JFG_CUDA(cudaMemcpyAsync(M->rowptr.p, newptr.data(), sizeof(int) * (rows + 1), cudaMemcpyHostToDevice, s));
-    JFG_CUDA(cudaMemsetAsync(M->col.p, 0, sizeof(int) * M->nnz_padded, s));
-    JFG_CUDA(cudaMemsetAsync(M->val.p, 0, sizeof(double) * M->nnz_padded, s));
-    DevBuf<int64_t> d_old;
-    d_old.alloc((size_t)rows + 1);
-    JFG_CUDA(cudaMemcpyAsync(d_old.p, oldptr.data(), sizeof(int64_t) * (rows + 1), cudaMemcpyHostToDevice, s));
-    if (m) k_scatter_padded<<<nblk(m), 256, 0, s>>>(m, d_key, d_val, cols, d_old.p, M->rowptr.p, M->col.p, M->val.p);
-    JFG_CUDA(cudaGetLastError());
     M->diag.alloc((size_t)rows);
-    if (rows) k_diag<<<nblk(rows), 256, 0, s>>>(rows, cols, M->rowptr.p, M->col.p, M->val.p, M->diag.p);
+    if (rows) k_diag<<<nblk(rows), 256, 0, s>>>(rows, cols, M->csr_ptr.p, M->csr_col.p, M->csr_val.p, M->diag.p);
     JFG_CUDA(cudaGetLastError());
-    M->lpr = 1 << choose_lpr_log2(rows ? (double)m / rows : 1.0);
+    // SELL-32-sigma: sort rows by length (descending, stable) inside windows
+    int nslices = (rows + kSliceRows - 1) / kSliceRows;
+    std::vector<int> perm((size_t)nslices * kSliceRows, -1);
+    std::vector<int> idx(rows);
+    std::iota(idx.begin(), idx.end(), 0);
+    for (int w0 = 0; w0 < rows; w0 += kSellSigma) {
+        int w1 = std::min(rows, w0 + kSellSigma);
+        std::stable_sort(idx.begin() + w0, idx.begin() + w1, [&](int a, int b) { return len[a] > len[b]; });
+    }
+    std::copy(idx.begin(), idx.end(), perm.begin());
+    std::vector<int> off(nslices + 1, 0);
+    int64_t total = 0;
+    for (int sl = 0; sl < nslices; sl++) {
+        int mx = 0;
+        for (int l = 0; l < kSliceRows; l++) {
+            int r = perm[(size_t)sl * kSliceRows + l];
+            if (r >= 0) mx = std::max(mx, len[r]);
+        }
+        off[sl] = (int)total;
+        total += (int64_t)mx * kSliceRows;
+        JFG_CHECK(total < (int64_t)INT32_MAX - 64, JFG_ERR_UNSUPPORTED, "padded matrix exceeds 2^31 entries");
+    }
+    off[nslices] = (int)total;
+    M->nslices = nslices;
+    M->sell_len = total;
+    M->nblocks = std::max(1, (nslices * kSliceRows + kThreads - 1) / kThreads);
+    M->off.alloc((size_t)nslices + 1);
+    M->perm.alloc(perm.size() ? perm.size() : 1);
+    M->col.alloc(total ? (size_t)total : 1);
+    M->val.alloc(total ? (size_t)total : 1);
+    JFG_CUDA(cudaMemcpyAsync(M->off.p, off.data(), sizeof(int) * (nslices + 1), cudaMemcpyHostToDevice, s));
+    if (!perm.empty())
+        JFG_CUDA(cudaMemcpyAsync(M->perm.p, perm.data(), sizeof(int) * perm.size(), cudaMemcpyHostToDevice, s));
+    if (nslices)
+        k_fill_sell<<<nblk((int64_t)nslices * kSliceRows), 256, 0, s>>>(nslices * kSliceRows, M->perm.p, M->off.p,
+                                                                         M->csr_ptr.p, M->csr_col.p, M->csr_val.p,
+                                                                         M->col.p, M->val.p);
+    JFG_CUDA(cudaGetLastError());
     JFG_CUDA(cudaStreamSynchronize(s));
     return M;
 }
 
 // COO on the device -> Matrix (sort, merge duplicates, drop zeros).
 static Matrix* from_device_coo(Context* c, int rows, int cols, int64_t nnz, const int* d_ri, const int* d_ci,
-                               const double* d_v, bool keep_zeros)
+                               const double* d_v)
 {
     cudaStream_t s = c->stream;
     DevBuf<uint64_t> key, key2, ukey;
@@ -235,48 +240,44 @@ static Matrix* from_device_coo(Context* c, int rows, int cols, int64_t nnz, cons
     JFG_CUDA(cudaMemcpyAsync(&h_bad, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     JFG_CUDA(cudaStreamSynchronize(s));
     JFG_CHECK(!h_bad, JFG_ERR_BAD_ARG, "COO index out of bounds");
+    if (!nnz) return build_from_sorted(c, rows, cols, 0, ukey.p, uval.p);
     int end_bit = 1;
     uint64_t maxkey = (uint64_t)rows * (uint64_t)cols;
     while (end_bit < 64 && (1ULL << end_bit) < maxkey) end_bit++;
+    size_t tmp_bytes = 0, tmp2 = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, key.p, key2.p, d_v, v2.p, (int64_t)nnz, 0, end_bit, s);
+    cub::DeviceReduce::ReduceByKey(nullptr, tmp2, key2.p, ukey.p, v2.p, uval.p, nrun.p, cub::Sum(), (int64_t)nnz, s);
+    DevBuf<char> tmp;
+    tmp.alloc(std::max(tmp_bytes, tmp2) + 64);
+    JFG_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, key.p, key2.p, d_v, v2.p, (int64_t)nnz, 0, end_bit, s));
+    JFG_CUDA(cub::DeviceReduce::ReduceByKey(tmp.p, tmp2, key2.p, ukey.p, v2.p, uval.p, nrun.p, cub::Sum(),
+                                            (int64_t)nnz, s));
     int64_t m = 0;
-    if (nnz) {
-        size_t tmp_bytes = 0, tmp2 = 0;
-        cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, key.p, key2.p, d_v, v2.p, (int64_t)nnz, 0, end_bit, s);
-        cub::DeviceReduce::ReduceByKey(nullptr, tmp2, key2.p, ukey.p, v2.p, uval.p, nrun.p, cub::Sum(), (int64_t)nnz, s);
-        DevBuf<char> tmp;
-        tmp.alloc(std::max(tmp_bytes, tmp2) + 64);
-        JFG_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, tmp_bytes, key.p, key2.p, d_v, v2.p, (int64_t)nnz, 0, end_bit, s));
-        JFG_CUDA(cub::DeviceReduce::ReduceByKey(tmp.p, tmp2, key2.p, ukey.p, v2.p, uval.p, nrun.p, cub::Sum(),
-                                                (int64_t)nnz, s));
-        int64_t h_runs = 0;
-        JFG_CUDA(cudaMemcpyAsync(&h_runs, nrun.p, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-        JFG_CUDA(cudaStreamSynchronize(s));
-        m = h_runs;
-        if (!keep_zeros && m) {
-            // keep the merged entries whose value is nonzero
-            DevBuf<char> flags;
-            flags.alloc((size_t)m);
-            k_nonzero_flags<<<nblk(m), 256, 0, s>>>(m, uval.p, flags.p);
-            JFG_CUDA(cudaGetLastError());
-            size_t t1 = 0, t2 = 0;
-            cub::DeviceSelect::Flagged(nullptr, t1, ukey.p, flags.p, key.p, nrun.p + 1, m, s);
-            cub::DeviceSelect::Flagged(nullptr, t2, uval.p, flags.p, v2.p, nrun.p + 1, m, s);
-            DevBuf<char> tmp4;
-            tmp4.alloc(std::max(t1, t2) + 64);
-            JFG_CUDA(cub::DeviceSelect::Flagged(tmp4.p, t1, ukey.p, flags.p, key.p, nrun.p + 1, m, s));
-            JFG_CUDA(cub::DeviceSelect::Flagged(tmp4.p, t2, uval.p, flags.p, v2.p, nrun.p + 1, m, s));
-            int64_t h_sel = 0;
-            JFG_CUDA(cudaMemcpyAsync(&h_sel, nrun.p + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-            JFG_CUDA(cudaStreamSynchronize(s));
-            return build_from_sorted(c, rows, cols, h_sel, key.p, v2.p);
-        }
-    }
-    return build_from_sorted(c, rows, cols, m, ukey.p, uval.p);
+    JFG_CUDA(cudaMemcpyAsync(&m, nrun.p, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    JFG_CUDA(cudaStreamSynchronize(s));
+    if (!m) return build_from_sorted(c, rows, cols, 0, ukey.p, uval.p);
+    // keep the merged entries whose value is nonzero
+    DevBuf<char> flags;
+    flags.alloc((size_t)m);
+    k_nonzero_flags<<<nblk(m), 256, 0, s>>>(m, uval.p, flags.p);
+    JFG_CUDA(cudaGetLastError());
+    size_t t1 = 0, t2 = 0;
+    cub::DeviceSelect::Flagged(nullptr, t1, ukey.p, flags.p, key.p, nrun.p + 1, m, s);
+    cub::DeviceSelect::Flagged(nullptr, t2, uval.p, flags.p, v2.p, nrun.p + 1, m, s);
+    DevBuf<char> tmp4;
+    tmp4.alloc(std::max(t1, t2) + 64);
+    JFG_CUDA(cub::DeviceSelect::Flagged(tmp4.p, t1, ukey.p, flags.p, key.p, nrun.p + 1, m, s));
+    JFG_CUDA(cub::DeviceSelect::Flagged(tmp4.p, t2, uval.p, flags.p, v2.p, nrun.p + 1, m, s));
+    int64_t h_sel = 0;
+    JFG_CUDA(cudaMemcpyAsync(&h_sel, nrun.p + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    JFG_CUDA(cudaStreamSynchronize(s));
+    return build_from_sorted(c, rows, cols, h_sel, key.p, v2.p);
 }
 
 Matrix* matrix_from_coo(Context* c, int rows, int cols, int64_t nnz, const int* ri, const int* ci, const double* v,
                         bool keep_zeros)
 {
+    (void)keep_zeros;
     JFG_CHECK(rows >= 0 && cols >= 0 && nnz >= 0, JFG_ERR_BAD_ARG, "negative matrix dimension or nnz");
     JFG_CHECK(nnz == 0 || (ri && ci && v), JFG_ERR_BAD_ARG, "null COO array");
     cudaStream_t s = c->stream;
@@ -291,7 +292,7 @@ Matrix* matrix_from_coo(Context* c, int rows, int cols, int64_t nnz, const int* 
         JFG_CUDA(cudaMemcpyAsync(d_ci.p, ci, sizeof(int) * nnz, cudaMemcpyHostToDevice, s));
         JFG_CUDA(cudaMemcpyAsync(d_v.p, v, sizeof(double) * nnz, cudaMemcpyHostToDevice, s));
     }
-    return from_device_coo(c, rows, cols, nnz, d_ri.p, d_ci.p, d_v.p, keep_zeros);
+    return from_device_coo(c, rows, cols, nnz, d_ri.p, d_ci.p, d_v.p);
 }
 
 Matrix* matrix_from_csr_host(Context* c, int rows, int cols, const std::vector<int64_t>& rp,
@@ -303,41 +304,26 @@ Matrix* matrix_from_csr_host(Context* c, int rows, int cols, const std::vector<i
     return matrix_from_coo(c, rows, cols, (int64_t)ci.size(), ri.data(), ci.data(), v.data(), false);
 }
 
-// Expands the padded layout back to COO on the device and rebuilds with rows
-// and columns exchanged.
+// CSR -> COO with rows and columns exchanged -> Matrix.
 Matrix* matrix_transpose(Matrix* M)
 {
     if (M->transposed) return M->transposed;
     Context* c = M->ctx;
     cudaStream_t s = c->stream;
-    std::vector<int> hptr(M->rows + 1);
-    JFG_CUDA(cudaMemcpyAsync(hptr.data(), M->rowptr.p, sizeof(int) * (M->rows + 1), cudaMemcpyDeviceToHost, s));
-    JFG_CUDA(cudaStreamSynchronize(s));
-    std::vector<int64_t> doff(M->rows + 1, 0);
-    for (int r = 0; r < M->rows; r++) doff[r + 1] = doff[r] + (hptr[r + 1] - hptr[r]);
-    int64_t m = doff[M->rows];
-    DevBuf<int64_t> d_off;
-    DevBuf<int> ri, ci;
-    DevBuf<double> v;
-    d_off.alloc((size_t)M->rows + 1);
+    int64_t m = M->nnz;
+    DevBuf<int> ri;
     ri.alloc(m ? (size_t)m : 1);
-    ci.alloc(m ? (size_t)m : 1);
-    v.alloc(m ? (size_t)m : 1);
-    JFG_CUDA(cudaMemcpyAsync(d_off.p, doff.data(), sizeof(int64_t) * (M->rows + 1), cudaMemcpyHostToDevice, s));
-    if (M->rows) {
-        k_expand_rows<<<nblk(M->rows), 256, 0, s>>>(M->rows, M->rowptr.p, ri.p, d_off.p);
-        k_compact<<<nblk(M->rows), 256, 0, s>>>(M->rows, M->rowptr.p, M->col.p, M->val.p, d_off.p, ci.p, v.p);
-    }
+    if (M->rows) k_expand_rows<<<nblk(M->rows), 256, 0, s>>>(M->rows, M->csr_ptr.p, ri.p);
     JFG_CUDA(cudaGetLastError());
-    M->transposed = from_device_coo(c, M->cols, M->rows, m, ci.p, ri.p, v.p, false);
+    M->transposed = from_device_coo(c, M->cols, M->rows, m, M->csr_col.p, ri.p, M->csr_val.p);
     return M->transposed;
 }
 
 void matrix_ensure_fp32(Matrix* M)
 {
     if (M->has32) return;
-    M->val32.alloc((size_t)M->nnz_padded);
-    k_to_f32<<<nblk(M->nnz_padded), 256, 0, M->ctx->stream>>>(M->nnz_padded, M->val.p, M->val32.p);
+    M->val32.alloc(M->sell_len ? (size_t)M->sell_len : 1);
+    if (M->sell_len) k_to_f32<<<nblk(M->sell_len), 256, 0, M->ctx->stream>>>(M->sell_len, M->val.p, M->val32.p);
     JFG_CUDA(cudaGetLastError());
     M->has32 = 1;
 }
@@ -345,8 +331,8 @@ void matrix_ensure_fp32(Matrix* M)
 void matrix_ensure_bf16(Matrix* M)
 {
     if (M->has16) return;
-    M->val16.alloc((size_t)M->nnz_padded);
-    k_to_bf16<<<nblk(M->nnz_padded), 256, 0, M->ctx->stream>>>(M->nnz_padded, M->val.p, M->val16.p);
+    M->val16.alloc(M->sell_len ? (size_t)M->sell_len : 1);
+    if (M->sell_len) k_to_bf16<<<nblk(M->sell_len), 256, 0, M->ctx->stream>>>(M->sell_len, M->val.p, M->val16.p);
     JFG_CUDA(cudaGetLastError());
     M->has16 = 1;
 }

@@ -168,11 +168,11 @@ void MGImpl<T>::init(Context* ctx, int levels, Matrix* const* As, Matrix* const*
     {
         Matrix* Af = A[Lf];
         std::vector<int> hp(Af->rows + 1);
-        std::vector<int> hc((size_t)Af->nnz_padded);
-        std::vector<double> hv((size_t)Af->nnz_padded);
-        JFG_CUDA(cudaMemcpyAsync(hp.data(), Af->rowptr.p, sizeof(int) * (Af->rows + 1), cudaMemcpyDeviceToHost, st));
-        JFG_CUDA(cudaMemcpyAsync(hc.data(), Af->col.p, sizeof(int) * Af->nnz_padded, cudaMemcpyDeviceToHost, st));
-        JFG_CUDA(cudaMemcpyAsync(hv.data(), Af->val.p, sizeof(double) * Af->nnz_padded, cudaMemcpyDeviceToHost, st));
+        std::vector<int> hc((size_t)Af->nnz + 1);
+        std::vector<double> hv((size_t)Af->nnz + 1);
+        JFG_CUDA(cudaMemcpyAsync(hp.data(), Af->csr_ptr.p, sizeof(int) * (Af->rows + 1), cudaMemcpyDeviceToHost, st));
+        JFG_CUDA(cudaMemcpyAsync(hc.data(), Af->csr_col.p, sizeof(int) * Af->nnz, cudaMemcpyDeviceToHost, st));
+        JFG_CUDA(cudaMemcpyAsync(hv.data(), Af->csr_val.p, sizeof(double) * Af->nnz, cudaMemcpyDeviceToHost, st));
         JFG_CUDA(cudaStreamSynchronize(st));
         std::vector<char> isbd(Af->rows, 0);
         for (int i = 0; i < nbd_fine; i++) isbd[bdry[Lf][i]] = 1;
@@ -213,11 +213,11 @@ void MGImpl<T>::init(Context* ctx, int levels, Matrix* const* As, Matrix* const*
         JFG_CUDA(cudaMemsetAsync(dense.p, 0, sizeof(double) * n0 * n0, st));
         // scatter the level-0 CSR into the dense array
         std::vector<int> hp(n0 + 1);
-        std::vector<int> hc((size_t)A[0]->nnz_padded);
-        std::vector<double> hv((size_t)A[0]->nnz_padded);
-        JFG_CUDA(cudaMemcpyAsync(hp.data(), A[0]->rowptr.p, sizeof(int) * (n0 + 1), cudaMemcpyDeviceToHost, st));
-        JFG_CUDA(cudaMemcpyAsync(hc.data(), A[0]->col.p, sizeof(int) * A[0]->nnz_padded, cudaMemcpyDeviceToHost, st));
-        JFG_CUDA(cudaMemcpyAsync(hv.data(), A[0]->val.p, sizeof(double) * A[0]->nnz_padded, cudaMemcpyDeviceToHost, st));
+        std::vector<int> hc((size_t)A[0]->nnz + 1);
+        std::vector<double> hv((size_t)A[0]->nnz + 1);
+        JFG_CUDA(cudaMemcpyAsync(hp.data(), A[0]->csr_ptr.p, sizeof(int) * (n0 + 1), cudaMemcpyDeviceToHost, st));
+        JFG_CUDA(cudaMemcpyAsync(hc.data(), A[0]->csr_col.p, sizeof(int) * A[0]->nnz, cudaMemcpyDeviceToHost, st));
+        JFG_CUDA(cudaMemcpyAsync(hv.data(), A[0]->csr_val.p, sizeof(double) * A[0]->nnz, cudaMemcpyDeviceToHost, st));
         JFG_CUDA(cudaStreamSynchronize(st));
         std::vector<double> hd((size_t)n0 * n0, 0.0);
         for (int rr = 0; rr < n0; rr++)

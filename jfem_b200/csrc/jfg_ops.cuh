@@ -115,39 +115,16 @@ void launch_ex(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaS
     note_launch();
 }
 
-template <typename VT> struct StagesOf { static constexpr int S = sizeof(VT) == 8 ? 3 : 4; };
-
 int sm_count();
-
-// Persistent grid of the pipelined SpMV for one kernel instance: resident
-// CTAs per SM (from the occupancy calculator) x SM count, capped by the
-// number of row blocks.
-template <typename K>
-int persistent_ctas(K kern, int smem)
-{
-    static int per_sm = 0;
-    if (per_sm == 0) {
-        JFG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        int b = 0;
-        JFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, kThreads, smem));
-        per_sm = b > 0 ? b : 1;
-    }
-    return per_sm * sm_count();
-}
 
 template <typename VT, typename XT, int NR, class Epi, class Fin = NoFin>
 void spmv_launch(cudaStream_t st, const Matrix* M, const VT* val, const XT* x, Epi epi, const Scratch& sc,
                  const int* done, Fin fin = Fin())
 {
     if (M->rows == 0) return;
-    constexpr int S = StagesOf<VT>::S;
-    constexpr int smem = spmv_smem_bytes<VT, S>();
     GridRed<NR, Fin> red{sc.partials, sc.counter, fin};
-    SpmvArgs a{M->rb.p, M->rowptr.p, M->col.p, M->nblocks};
-    auto kern = k_spmv<VT, XT, NR, S, Epi, Fin>;
-    int grid = persistent_ctas(kern, smem);
-    if (grid > M->nblocks) grid = M->nblocks;
-    launch_ex(kern, dim3(grid), dim3(kThreads), smem, st, a, val, x, ilog2(M->lpr), epi, red, done);
+    SpmvArgs a{M->off.p, M->perm.p, M->col.p, M->nslices * kSliceRows};
+    launch_ex(k_spmv<VT, XT, NR, Epi, Fin>, dim3(M->nblocks), dim3(kThreads), 0, st, a, val, x, epi, red, done);
 }
 
 inline int vec_grid(int n)
