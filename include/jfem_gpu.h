@@ -192,6 +192,23 @@ int jfg_solve_dev(jfg_ctx* ctx, int kind, jfg_mat* A, int precond_kind, void* pr
 int jfg_dense_solve(jfg_ctx* ctx, int n, const double* h_A, const double* h_b, double* h_x);
 /* Ainv = A^-1.  Replaces DenseMatrix.inverse and the JNI iInverse (sparseSolver.cpp:63-113). */
 int jfg_dense_inverse(jfg_ctx* ctx, int n, const double* h_A, double* h_Ainv);
+/* CG on a system the caller already holds on the device as CSR (row
+ * pointers, column indices, values; no duplicates), for callers that must not
+ * allocate device memory while they solve -- e.g. code running under CUDA
+ * stream capture or inside a framework that owns the device heap.  No
+ * counterpart in the reference: it is the allocation-free twin of
+ * jfg_solve_dev(JFG_CG, ...), with the same iteration and semantics (x holds
+ * the start iterate on entry, the solution on exit; absolute tolerance;
+ * maxit <= 0 means n).  All work memory (three vectors of n doubles, the
+ * reduction partials, the control block) is one fixed __device__ array of
+ * about 6.3 MB per GPU: n is limited to 262,144 unknowns (larger n is
+ * rejected with JFG_ERR_BAD_ARG).  The array is shared by every call and
+ * keeps the last call's contents; calls that overlap on the GPU race on it.
+ * The first call on a device looks up the array's address and should come
+ * before any stream capture.  Calls no cudaMalloc/cudaFree. */
+int jfg_cg_noalloc(jfg_ctx* ctx, int n, const int* d_rowptr, const int* d_col, const double* d_val,
+                   const double* d_b, double* d_x, double tol, int maxit, int* iterations, double* final_norm);
+
 /* Drop-in for SparseMatrix.solve(rhs) (linalg/SparseMatrix.java:142-150): COO in, x out.
  * n <= 4096: dense LU of the merged matrix on the GPU (the reference's method);
  * larger: FP64 GMRES with a Jacobi preconditioner to ||b - A x|| <= 1e-12 ||b||. */

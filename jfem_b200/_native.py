@@ -32,7 +32,7 @@ EXPORTED = [
     "jfg_spmv_t_dev", "jfg_spmv_f32_dev", "jfg_matrix_diag", "jfg_spmv_time", "jfg_smooth",
     "jfg_mg_create", "jfg_mg_free", "jfg_mg_apply", "jfg_mg_vcycle", "jfg_mg_fmg",
     "jfg_solver_opts_default", "jfg_solve", "jfg_solve_dev",
-    "jfg_dense_solve", "jfg_dense_inverse", "jfg_sparse_solve",
+    "jfg_dense_solve", "jfg_dense_inverse", "jfg_sparse_solve", "jfg_cg_noalloc",
 ]
 
 
@@ -110,6 +110,7 @@ def load():
     L.jfg_dense_solve.argtypes = [_P, C.c_int, _D, _D, _D]
     L.jfg_dense_inverse.argtypes = [_P, C.c_int, _D, _D]
     L.jfg_sparse_solve.argtypes = [_P, C.c_int, C.c_int64, _I, _I, _D, _D, _D]
+    L.jfg_cg_noalloc.argtypes = [_P, C.c_int, _P, _P, _P, _P, _P, C.c_double, C.c_int, _I, _D]
     _lib = L
     return L
 

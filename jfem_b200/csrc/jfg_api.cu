@@ -18,6 +18,12 @@ struct jfg_mat {
     jfg::Matrix* m = nullptr;
 };
 
+namespace jfg {
+cudaStream_t ctx_stream(jfg_ctx* ctx) { return ctx->c.stream; }
+int ctx_device(jfg_ctx* ctx) { return ctx->c.device; }
+void ctx_set_error(jfg_ctx* ctx, const std::string& msg) { ctx->c.last_error = msg; }
+}  // namespace jfg
+
 namespace {
 
 using jfg::DevBuf;
