@@ -112,7 +112,8 @@ struct Matrix {
     DevBuf<double> csr_val;       // nnz
     int nslices = 0;
     int64_t sell_len = 0;         // length of the SELL col/val arrays
-    int nblocks = 0;              // CTAs of one SpMV launch (kThreads rows each)
+    int nblocks = 0;              // CTAs of one SpMV launch
+    int tpr_log2 = 0;             // log2 of the threads per row in the SpMV
     DevBuf<int> off;              // nslices + 1 slice offsets
     DevBuf<int> perm;             // nslices * 32 original row of each slot
     DevBuf<int> col;              // sell_len

@@ -129,13 +129,17 @@ struct SpmvArgs {
     const int* perm;    // nslices * 32
     const int* col;     // SELL column indices
     int nslots;         // nslices * 32
+    int tpr_log2;       // log2 of the threads that share one row (0..3)
 };
 
-// One thread per slot (row) of a 32-row slice.  A warp reads one slice
-// column per step: 32 consecutive column indices and 32 consecutive values
-// (fully coalesced), gathers x, and accumulates its row in a fixed order.
-// No shared memory, no barriers: occupancy and the unrolled independent loads
-// hide the gather latency.
+// 2^tpr_log2 adjacent threads per slot (row) of a 32-row slice; thread `sub`
+// of a row takes the row's entries sub, sub + TPR, ...  For a fixed k the
+// threads of a warp read consecutive slots of one slice column, so every
+// 32-byte sector they touch is used in full.  Partial sums are combined with
+// shuffles in a fixed order.  TPR = 1 on large levels (occupancy hides the
+// gather latency); TPR = 4..8 on small levels, where the row loop would
+// otherwise be a chain of dependent gathers per thread.  No shared memory,
+// no barriers.
 template <typename VT, typename XT, int NR, class Epi, class Fin>
 __global__ void __launch_bounds__(kThreads)
 k_spmv(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi, GridRed<NR, Fin> red,
@@ -147,30 +151,36 @@ k_spmv(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi
     double acc[NR > 0 ? NR : 1];
 #pragma unroll
     for (int i = 0; i < (NR > 0 ? NR : 1); i++) acc[i] = 0;
-    const int slot = blockIdx.x * kThreads + threadIdx.x;
+    const int gid = blockIdx.x * kThreads + threadIdx.x;
+    const int tpr = 1 << m.tpr_log2;
+    const int slot = gid >> m.tpr_log2;
+    const int sub = gid & (tpr - 1);
+    AT sum = 0;
+    int r = -1;
     if (slot < m.nslots) {
         const int s = slot >> 5, lane = slot & 31;
         const int o = __ldg(m.off + s);
         const int len = (__ldg(m.off + s + 1) - o) >> 5;
-        const int r = __ldg(m.perm + slot);
+        r = __ldg(m.perm + slot);
         const int* cp = m.col + o + lane;
         const VT* vp = val + o + lane;
-        AT sum = 0;
-        int k = 0;
-        for (; k + 4 <= len; k += 4) {
-            const int c0 = __ldg(cp + 32 * k), c1 = __ldg(cp + 32 * (k + 1));
-            const int c2 = __ldg(cp + 32 * (k + 2)), c3 = __ldg(cp + 32 * (k + 3));
-            const AT v0 = to_acc(__ldg(vp + 32 * k)), v1 = to_acc(__ldg(vp + 32 * (k + 1)));
-            const AT v2 = to_acc(__ldg(vp + 32 * (k + 2))), v3 = to_acc(__ldg(vp + 32 * (k + 3)));
+        const int st = 32 * tpr;
+        int k = sub;
+        for (; k + 3 * tpr < len; k += 4 * tpr) {
+            const int c0 = __ldg(cp + 32 * k), c1 = __ldg(cp + 32 * k + st);
+            const int c2 = __ldg(cp + 32 * k + 2 * st), c3 = __ldg(cp + 32 * k + 3 * st);
+            const AT v0 = to_acc(__ldg(vp + 32 * k)), v1 = to_acc(__ldg(vp + 32 * k + st));
+            const AT v2 = to_acc(__ldg(vp + 32 * k + 2 * st)), v3 = to_acc(__ldg(vp + 32 * k + 3 * st));
             const AT x0 = (AT)__ldg(x + c0), x1 = (AT)__ldg(x + c1), x2 = (AT)__ldg(x + c2), x3 = (AT)__ldg(x + c3);
             sum += v0 * x0;
             sum += v1 * x1;
             sum += v2 * x2;
             sum += v3 * x3;
         }
-        for (; k < len; k++) sum += to_acc(__ldg(vp + 32 * k)) * (AT)__ldg(x + __ldg(cp + 32 * k));
-        if (r >= 0) epi(r, sum, acc);
+        for (; k < len; k += tpr) sum += to_acc(__ldg(vp + 32 * k)) * (AT)__ldg(x + __ldg(cp + 32 * k));
     }
+    for (int o = tpr >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (sub == 0 && r >= 0) epi(r, sum, acc);
     pdl_launch_dependents();
     if constexpr (NR > 0) red.reduce(acc);
 }

@@ -199,7 +199,12 @@ static Matrix* build_from_sorted(Context* c, int rows, int cols, int64_t m, cons
     off[nslices] = (int)total;
     M->nslices = nslices;
     M->sell_len = total;
-    M->nblocks = std::max(1, (nslices * kSliceRows + kThreads - 1) / kThreads);
+    // threads per row: 1 on large matrices, 4 or 8 on small ones (JFEM_TPR overrides)
+    double avg = rows ? (double)m / rows : 0.0;
+    int tl = rows >= 262144 ? 0 : (avg >= 10.0 ? 3 : 2);
+    if (const char* e = getenv("JFEM_TPR")) tl = std::max(0, std::min(3, atoi(e)));
+    M->tpr_log2 = tl;
+    M->nblocks = std::max(1, (int)((((int64_t)nslices * kSliceRows << tl) + kThreads - 1) / kThreads));
     M->off.alloc((size_t)nslices + 1);
     M->perm.alloc(perm.size() ? perm.size() : 1);
     M->col.alloc(total ? (size_t)total : 1);

@@ -112,213 +112,7 @@ struct EpiRestrictSweep {
     }
 };
 
-// ---------------------------------------------------------------------------
-// the bottom of the V-cycle in one CTA
-// ---------------------------------------------------------------------------
-constexpr int kCoarseMaxLevels = 8;
-constexpr int kCoarseThreads = 1024;
-
-template <typename T>
-struct SellRef {
-    const int* off;
-    const int* perm;
-    const int* col;
-    const T* val;
-    int nslots;
-};
-
-template <typename T>
-struct CoarseLevel {
-    SellRef<T> A, P, R;      // P: prolongation into this level, R: restriction out of it
-    const T* dinv;
-    const unsigned char* mask;
-    T *x, *t, *b, *r;
-    int n, kind, runs;
-    T omega;
-};
-
-template <typename T>
-struct CoarseArgs {
-    CoarseLevel<T> lv[kCoarseMaxLevels];
-    int top;
-    const double* ainv0;
-    int n0;
-};
-
-// x is written earlier in the same kernel, so it is read with coherent loads
-// (no __restrict__ / read-only path); the matrix arrays are read-only.
-template <typename T, class Epi>
-__device__ __forceinline__ void cta_spmv(const SellRef<T>& m, const T* x, Epi epi)
-{
-    double acc[1] = {0};
-    for (int slot = threadIdx.x; slot < m.nslots; slot += blockDim.x) {
-        const int s = slot >> 5, lane = slot & 31;
-        const int o = m.off[s];
-        const int len = (m.off[s + 1] - o) >> 5;
-        const int r = m.perm[slot];
-        T sum = 0;
-        for (int k = 0; k < len; k++) sum += m.val[o + 32 * k + lane] * x[m.col[o + 32 * k + lane]];
-        if (r >= 0) epi(r, sum, acc);
-    }
-}
-
-template <typename T, class Epi>
-__device__ __forceinline__ double cta_spmv_norm(const SellRef<T>& m, const T* x, Epi epi)
-{
-    double acc[1] = {0};
-    for (int slot = threadIdx.x; slot < m.nslots; slot += blockDim.x) {
-        const int s = slot >> 5, lane = slot & 31;
-        const int o = m.off[s];
-        const int len = (m.off[s + 1] - o) >> 5;
-        const int r = m.perm[slot];
-        T sum = 0;
-        for (int k = 0; k < len; k++) sum += m.val[o + 32 * k + lane] * x[m.col[o + 32 * k + lane]];
-        if (r >= 0) epi(r, sum, acc);
-    }
-    __shared__ double sh[kCoarseThreads / 32];
-    double v = warp_sum(acc[0]);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
-    __syncthreads();
-    double tot = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) tot += sh[w];
-    __syncthreads();
-    return tot;
-}
-
-// Smoother.smooth on one level inside the CTA; result in L.x.
-template <typename T>
-__device__ void cta_smooth(const CoarseLevel<T>& L, const T* rhs, bool xzero)
-{
-    const int n = L.n;
-    if (L.runs <= 0) {
-        if (xzero)
-            for (int i = threadIdx.x; i < n; i += blockDim.x) L.x[i] = (T)0;
-        __syncthreads();
-        return;
-    }
-    if (L.kind == JFG_SMOOTH_JACOBI) {
-        T* cur = L.x;
-        T* alt = L.t;
-        int k = 0;
-        if (xzero) {
-            T* dst = (L.runs % 2 == 1) ? L.x : L.t;
-            for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = (T)0 + (L.dinv[i] * rhs[i]) * L.omega;
-            __syncthreads();
-            cur = dst;
-            alt = (dst == L.x) ? L.t : L.x;
-            k = 1;
-        }
-        for (; k < L.runs; k++) {
-            cta_spmv(L.A, cur, EpiJacobi<T>{cur, rhs, L.dinv, alt, L.omega});
-            __syncthreads();
-            T* tmp = cur;
-            cur = alt;
-            alt = tmp;
-        }
-        if (cur != L.x) {
-            for (int i = threadIdx.x; i < n; i += blockDim.x) L.x[i] = cur[i];
-            __syncthreads();
-        }
-    } else {
-        if (xzero) {
-            for (int i = threadIdx.x; i < n; i += blockDim.x) L.x[i] = (T)0;
-            __syncthreads();
-        }
-        for (int k = 0; k < L.runs; k++) {
-            double rr = cta_spmv_norm(L.A, L.x, EpiResid<T>{rhs, L.r});
-            if (sqrt(rr) < 1e-10) break;     // RichardsonSmoother.java:33-38 (uniform across the CTA)
-            for (int i = threadIdx.x; i < n; i += blockDim.x) L.x[i] = L.x[i] + L.r[i] * L.omega;
-            __syncthreads();
-        }
-    }
-}
-
-// mgStepV for levels top..0 (MGPreconditionerInterface.java:125-198), the
-// recursion unrolled into a down and an up sweep, one CTA, __syncthreads()
-// between phases.  The vectors and matrices of these levels fit in L2.
-template <typename T>
-__global__ void __launch_bounds__(kCoarseThreads)
-k_coarse_vcycle(CoarseArgs<T> a, const T* rhs_top, int xzero_top, const int* __restrict__ done)
-{
-    pdl_wait();
-    if (done && *done) return;
-    const int top = a.top;
-    for (int l = top; l >= 1; l--) {
-        const CoarseLevel<T>& L = a.lv[l];
-        const T* rhs = (l == top) ? rhs_top : L.b;
-        cta_smooth(L, rhs, l == top ? (xzero_top != 0) : true);
-        cta_spmv(L.A, L.x, EpiResid<T>{rhs, L.r});
-        __syncthreads();
-        cta_spmv(L.R, L.r, EpiMasked<T>{a.lv[l - 1].mask, a.lv[l - 1].b});
-        __syncthreads();
-    }
-    {
-        const CoarseLevel<T>& L0 = a.lv[0];
-        const T* rhs0 = (top == 0) ? rhs_top : L0.b;
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        for (int row = warp; row < a.n0; row += (int)(blockDim.x >> 5)) {
-            double s = 0;
-            for (int j = lane; j < a.n0; j += 32) s += a.ainv0[(size_t)row * a.n0 + j] * (double)rhs0[j];
-            s = warp_sum(s);
-            if (lane == 0) L0.x[row] = (T)s;
-        }
-        __syncthreads();
-    }
-    for (int l = 1; l <= top; l++) {
-        const CoarseLevel<T>& L = a.lv[l];
-        const T* rhs = (l == top) ? rhs_top : L.b;
-        cta_spmv(L.P, a.lv[l - 1].x, EpiMaskedAdd<T>{L.mask, L.x});
-        __syncthreads();
-        cta_smooth(L, rhs, false);
-    }
-    pdl_launch_dependents();
-}
-
-template <typename T>
-SellRef<T> sell_ref(const Matrix* M)
-{
-    return SellRef<T>{M->off.p, M->perm.p, M->col.p, vals_of<T>(M), M->nslices * kSliceRows};
-}
-
-int coarse_fuse_rows()
-{
-    static int v = -1;
-    if (v < 0) {
-        const char* e = getenv("JFEM_COARSE_FUSE_ROWS");
-        v = e ? atoi(e) : 4500;
-    }
-    return v;
-}
-
 }  // namespace
-
-template <typename T>
-void MGImpl<T>::fused_bottom(int top, const T* rhs, bool xzero, const int* done, cudaStream_t st)
-{
-    CoarseArgs<T> a{};
-    a.top = top;
-    a.ainv0 = ainv0.p;
-    a.n0 = n[0];
-    for (int l = 0; l <= top; l++) {
-        CoarseLevel<T>& L = a.lv[l];
-        L.A = sell_ref<T>(A[l]);
-        if (l >= 1) {
-            L.P = sell_ref<T>(P[l - 1]);
-            L.R = sell_ref<T>(R[l - 1]);
-        }
-        L.dinv = dinv[l].p;
-        L.mask = mask[l].p;
-        L.x = x[l].p;
-        L.t = t[l].p;
-        L.b = b[l].p;
-        L.r = r[l].p;
-        L.n = n[l];
-        L.kind = sm[l].kind;
-        L.runs = sm[l].runs;
-        L.omega = (T)sm[l].omega;
-    }
-    launch_ex(k_coarse_vcycle<T>, dim3(1), dim3(kCoarseThreads), 0, st, a, rhs, xzero ? 1 : 0, done);
-}
 
 template <typename T>
 void MGImpl<T>::init(Context* ctx, int levels, Matrix* const* As, Matrix* const* Ps, const int* const* bdry,
@@ -449,10 +243,6 @@ void MGImpl<T>::init(Context* ctx, int levels, Matrix* const* As, Matrix* const*
         JFG_CUDA(cudaMemcpyAsync(dense.p, hd.data(), sizeof(double) * hd.size(), cudaMemcpyHostToDevice, st));
         coarse_status = dense_inverse_device(c, n0, dense.p, ainv0.p);
     }
-    fuse_top = -1;
-    for (int l = 0; l < L && l < kCoarseMaxLevels; l++)
-        if (n[l] <= coarse_fuse_rows()) fuse_top = l;
-        else break;
     flags.alloc(L);
     zero_flag.alloc(1);
     JFG_CUDA(cudaMemsetAsync(flags.p, 0, sizeof(int) * L, st));
@@ -528,10 +318,6 @@ template <typename T>
 void MGImpl<T>::vstep(int l, const T* rhs, bool xzero, const Scratch& sc, const int* done, cudaStream_t st,
                       bool first_sweep_done)
 {
-    if (l <= fuse_top) {
-        fused_bottom(l, rhs, xzero, done, st);
-        return;
-    }
     if (l == 0) {
         coarse(rhs, x[0].p, done, st);
         return;
@@ -539,7 +325,7 @@ void MGImpl<T>::vstep(int l, const T* rhs, bool xzero, const Scratch& sc, const 
     smooth(l, rhs, xzero, sc, done, st, first_sweep_done);
     spmv_launch<T, T, 0>(st, A[l], vals_of<T>(A[l]), x[l].p, EpiResid<T>{rhs, r[l].p}, sc, done);
     const int lc = l - 1;
-    const bool fuse_sweep = lc >= 1 && lc > fuse_top && sm[lc].kind == JFG_SMOOTH_JACOBI && sm[lc].runs > 0;
+    const bool fuse_sweep = lc >= 1 && sm[lc].kind == JFG_SMOOTH_JACOBI && sm[lc].runs > 0;
     if (fuse_sweep) {
         T* dst = (sm[lc].runs % 2 == 1) ? x[lc].p : t[lc].p;
         spmv_launch<T, T, 0>(st, R[lc], vals_of<T>(R[lc]), r[l].p,

@@ -42,9 +42,6 @@ struct MGImpl {
     int naff = 0;
     DevBuf<int> flags;                      // per-level smoother flags
     DevBuf<int> zero_flag;                  // a flag that stays 0
-    // levels 0..fuse_top run as one single-CTA launch (k_coarse_vcycle);
-    // -1 disables the fused bottom
-    int fuse_top = -1;
 
     // Builds all level data; A/P are borrowed (must outlive the hierarchy).
     void init(Context* ctx, int levels, Matrix* const* As, Matrix* const* Ps, const int* const* bdry,
@@ -63,7 +60,6 @@ struct MGImpl {
                bool first_sweep_done = false);
     void smooth(int l, const T* rhs, bool xzero, const Scratch& sc, const int* done, cudaStream_t st,
                 bool first_sweep_done = false);
-    void fused_bottom(int top, const T* rhs, bool xzero, const int* done, cudaStream_t st);
     void coarse(const T* rhs, T* out, const int* done, cudaStream_t st);
     void fmg_into_top(const T* defect, const Scratch& sc, const int* done, cudaStream_t st);
     int max_blocks() const;

@@ -123,7 +123,7 @@ void spmv_launch(cudaStream_t st, const Matrix* M, const VT* val, const XT* x, E
 {
     if (M->rows == 0) return;
     GridRed<NR, Fin> red{sc.partials, sc.counter, fin};
-    SpmvArgs a{M->off.p, M->perm.p, M->col.p, M->nslices * kSliceRows};
+    SpmvArgs a{M->off.p, M->perm.p, M->col.p, M->nslices * kSliceRows, M->tpr_log2};
     launch_ex(k_spmv<VT, XT, NR, Epi, Fin>, dim3(M->nblocks), dim3(kThreads), 0, st, a, val, x, epi, red, done);
 }
 
