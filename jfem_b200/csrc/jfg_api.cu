@@ -464,7 +464,6 @@ static int solve_impl(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, cons
     JFG_CHECK(!needs_prec || pk != JFG_PREC_NONE, JFG_ERR_BAD_ARG, "solver kind needs a preconditioner");
     JFG_CHECK(needs_prec || kind == JFG_GMRES2 || pk == JFG_PREC_NONE, JFG_ERR_BAD_ARG,
               "solver kind takes no preconditioner");
-    JFG_CHECK(kind != JFG_GMRES2, JFG_ERR_UNSUPPORTED, "GMRES2 is not implemented on the GPU yet");
     JFG_CHECK(o->tol >= 0 && std::isfinite(o->tol), JFG_ERR_BAD_ARG, "bad tolerance");
     int n = M->rows;
     jfg_mg* mg = pk == JFG_PREC_MG ? static_cast<jfg_mg*>(ph) : nullptr;
@@ -598,6 +597,17 @@ static int solve_impl(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, cons
             res.iter += it0;
             if (res.status == JFG_OK) res.status = JFG_BREAKDOWN;
         }
+    } else if (kind == JFG_GMRES2) {
+        int it = 0;
+        double fn = 0;
+        int cap = o->restart > 0 ? o->restart + 2 : 152;
+        int mx = maxit > 0 ? maxit : 10 * n + 10;
+        int stt = run_gmres2(w, M, P64, d_b, d_x, o->tol, mx, o->max_restarts >= 0 ? o->max_restarts : 200, cap, &it,
+                             &restarts, &fn, hist, hcap);
+        res = Ctl{};
+        res.iter = it;
+        res.status = stt;
+        res.res_norm = fn;
     } else {  // GMRES / PGMRES
         Ctl h{};
         h.tol = o->tol;

@@ -140,7 +140,7 @@ struct SpmvArgs {
 // gather latency); TPR = 4..8 on small levels, where the row loop would
 // otherwise be a chain of dependent gathers per thread.  No shared memory,
 // no barriers.
-template <typename VT, typename XT, int NR, class Epi, class Fin>
+template <typename VT, typename XT, int NR, int TPR, class Epi, class Fin>
 __global__ void __launch_bounds__(kThreads)
 k_spmv(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi, GridRed<NR, Fin> red,
        const int* __restrict__ done)
@@ -152,9 +152,9 @@ k_spmv(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi
 #pragma unroll
     for (int i = 0; i < (NR > 0 ? NR : 1); i++) acc[i] = 0;
     const int gid = blockIdx.x * kThreads + threadIdx.x;
-    const int tpr = 1 << m.tpr_log2;
-    const int slot = gid >> m.tpr_log2;
-    const int sub = gid & (tpr - 1);
+    constexpr int tpr = TPR;
+    const int slot = gid / TPR;
+    const int sub = gid % TPR;
     AT sum = 0;
     int r = -1;
     if (slot < m.nslots) {

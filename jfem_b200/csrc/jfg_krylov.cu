@@ -862,6 +862,192 @@ int run_mixed_cg(SolverWork& w, Matrix* A, const Precond<float>& M, const double
     return outer;
 }
 
+// ---------------------------------------------------------------------------
+// GMRES2 (GMRES2.java:60-104) with its Arnoldi helper (Arnoldi.java:13-83)
+// ---------------------------------------------------------------------------
+namespace {
+// device scalars of GMRES2 (w.g2): [0] t, [1] ||res||, [2] ||q_last||, [3] proj, [4] nn
+struct FinG2T {       // t = Mres.Av / Av.Av
+    double* g;
+    __device__ void operator()(const double* s) const { g[0] = s[0] / s[1]; }
+};
+struct FinG2Store {   // g[idx] = sqrt(s) or s
+    double* g;
+    int idx;
+    int root;
+    __device__ void operator()(const double* s) const { g[idx] = root ? sqrt(s[0]) : s[0]; }
+};
+struct EpiG2Res {     // res -= t * (A v); acc += res^2
+    double* res;
+    const double* g;
+    template <typename AT, int K>
+    __device__ void operator()(int r, AT s, double (&acc)[K]) const
+    {
+        double v = res[r] - (double)s * g[0];
+        res[r] = v;
+        acc[0] += v * v;
+    }
+};
+struct VG2Step {      // x += v t; Mres -= Av t
+    double* x;
+    const double* v;
+    double* mres;
+    const double* av;
+    const double* g;
+    template <int K> __device__ void operator()(int i, double (&)[K]) const
+    {
+        x[i] = x[i] + v[i] * g[0];
+        mres[i] = mres[i] - av[i] * g[0];
+    }
+};
+struct VG2Scale {     // y = a * (1 / g[idx])
+    const double* a;
+    double* y;
+    const double* g;
+    int idx;
+    template <int K> __device__ void operator()(int i, double (&)[K]) const { y[i] = a[i] * (1.0 / g[idx]); }
+};
+struct VG2Mgs {       // apply the previous projection (if any), then acc += newAw . Av_i
+    double* w;
+    double* naw;
+    const double* vprev;
+    const double* avprev;
+    const double* avi;      // null on the closing pass (then acc += naw^2)
+    const double* g;
+    template <int K> __device__ void operator()(int r, double (&acc)[K]) const
+    {
+        double nv = naw[r];
+        if (vprev) {
+            double p = g[3];
+            w[r] = w[r] - vprev[r] * p;
+            nv = nv - avprev[r] * p;
+            naw[r] = nv;
+        }
+        acc[0] += avi ? nv * avi[r] : nv * nv;
+    }
+};
+struct VG2New {       // V = w / nn, AV = newAw / nn
+    double* v;
+    double* av;
+    const double* wv;
+    const double* naw;
+    const double* g;
+    template <int K> __device__ void operator()(int i, double (&)[K]) const
+    {
+        v[i] = wv[i] * (1.0 / g[4]);
+        av[i] = naw[i] * (1.0 / g[4]);
+    }
+};
+}  // namespace
+
+int run_gmres2(SolverWork& w, Matrix* A, const Precond<double>& M, const double* b, double* x, double tol, int maxit,
+               int max_restarts, int basis_cap, int* iters, int* restarts_out, double* final_norm, double* hist,
+               int hist_cap)
+{
+    cudaStream_t st = w.c->stream;
+    const Scratch& sc = w.sc;
+    int n = A->rows;
+    const double* val = A->val.p;
+    if (basis_cap < 2) basis_cap = 2;
+    if (w.g2_cap < basis_cap || w.V2.n < (size_t)basis_cap * n) {
+        w.V2.alloc((size_t)basis_cap * n);
+        w.AV2.alloc((size_t)basis_cap * n);
+        w.g2_cap = basis_cap;
+    }
+    w.g2.alloc(8);
+    double* g = w.g2.p;
+    double *res = w.v64[0].p, *mres = w.v64[1].p, *ql = w.v64[2].p, *wv = w.v64[3].p, *naw = w.v64[4].p,
+           *t1 = w.v64[5].p;
+    auto V = [&](int i) { return w.V2.p + (size_t)i * n; };
+    auto AV = [&](int i) { return w.AV2.p + (size_t)i * n; };
+    auto norm_into = [&](const double* a, int idx) {
+        vec_launch<1>(st, n, VDot<double>{a, a}, sc, nullptr, FinG2Store{g, idx, 1});
+    };
+    auto MA = [&](const double* in, double* out) {  // out = M (A in)
+        spmv_launch<double, double, 0>(st, A, val, in, EpiStore<double>{t1}, sc, nullptr);
+        M.apply(t1, out, sc, nullptr, st);
+    };
+    auto read = [&](int idx) {
+        double h = 0;
+        JFG_CUDA(cudaMemcpyAsync(&h, g + idx, sizeof(double), cudaMemcpyDeviceToHost, st));
+        JFG_CUDA(cudaStreamSynchronize(st));
+        return h;
+    };
+    int it = 0, restarts = 0, status = JFG_NOT_CONVERGED;
+    double rn = 0;
+    for (;;) {
+        // solveInternal: res = b - A x; Mres = M res; Arnoldi(Mres, MA)
+        spmv_launch<double, double, 1>(st, A, val, x, EpiResid<double>{b, res}, sc, nullptr, FinG2Store{g, 1, 1});
+        M.apply(res, mres, sc, nullptr, st);
+        norm_into(mres, 2);
+        vec_launch<0>(st, n, VG2Scale{mres, wv, g, 2}, sc, nullptr);          // w0 = Mres / |Mres|
+        MA(wv, ql);                                                            // q1 = MA w0 = Aw0
+        norm_into(ql, 4);
+        vec_launch<0>(st, n, VG2New{V(0), AV(0), wv, ql, g}, sc, nullptr);   // v0, Av0
+        norm_into(ql, 2);
+        vec_launch<0>(st, n, VG2Scale{ql, wv, g, 2}, sc, nullptr);
+        MA(wv, naw);                                                           // q2 = MA(q1 / |q1|)
+        vec_launch<0>(st, n, VCopy<double>{naw, ql}, sc, nullptr);
+        norm_into(ql, 2);
+        int nv = 1;
+        rn = read(1);
+        bool restart = false;
+        while (rn > tol) {
+            if (it >= maxit) break;
+            const double* v = V(nv - 1);
+            const double* av = AV(nv - 1);
+            vec_launch<2>(st, n, VDot2<double>{av, mres}, sc, nullptr, FinG2T{g});
+            spmv_launch<double, double, 1>(st, A, val, v, EpiG2Res{res, g}, sc, nullptr, FinG2Store{g, 1, 1});
+            vec_launch<0>(st, n, VG2Step{x, v, mres, av, g}, sc, nullptr);
+            rn = read(1);
+            if (hist && it < hist_cap) JFG_CUDA(cudaMemcpyAsync(hist + it, g + 1, sizeof(double),
+                                                                cudaMemcpyDeviceToDevice, st));
+            it++;
+            if (!std::isfinite(rn)) {
+                status = JFG_NONFINITE;
+                break;
+            }
+            // arnoldiStep
+            vec_launch<0>(st, n, VG2Scale{ql, wv, g, 2}, sc, nullptr);       // w = q_last / |q_last|
+            MA(wv, naw);                                                     // newAw = MA w
+            vec_launch<0>(st, n, VCopy<double>{naw, ql}, sc, nullptr);     // q_last = newAw
+            norm_into(ql, 2);
+            for (int i = 0; i <= nv; i++) {
+                const double* vprev = i > 0 ? V(i - 1) : nullptr;
+                const double* avprev = i > 0 ? AV(i - 1) : nullptr;
+                const double* avi = i < nv ? AV(i) : nullptr;
+                vec_launch<1>(st, n, VG2Mgs{wv, naw, vprev, avprev, avi, g}, sc, nullptr,
+                              FinG2Store{g, i < nv ? 3 : 4, i < nv ? 0 : 1});
+            }
+            if (nv >= basis_cap) {   // basis full: restart from the current iterate
+                restart = true;
+                break;
+            }
+            vec_launch<0>(st, n, VG2New{V(nv), AV(nv), wv, naw, g}, sc, nullptr);
+            nv++;
+            if (read(4) < 1e-13) {
+                restart = true;
+                break;
+            }
+        }
+        if (status == JFG_NONFINITE) break;
+        if (!(rn > tol)) {
+            status = JFG_OK;
+            break;
+        }
+        if (restart && restarts < max_restarts && it < maxit) {
+            restarts++;
+            continue;
+        }
+        break;
+    }
+    JFG_CUDA(cudaStreamSynchronize(st));
+    *iters = it;
+    *restarts_out = restarts;
+    *final_norm = rn;
+    return status;
+}
+
 // Jacobi preconditioner vectors
 template <typename T>
 void jacobi_apply(cudaStream_t st, int n, const T* d, const T* r, T* z, const Scratch& sc, const int* done)

@@ -45,6 +45,9 @@ struct SolverWork {
     DevBuf<float> dinv32;
     // GMRES
     DevBuf<double> V, H, gam, cs, sn, fac, alpha, mdot_part;
+    // GMRES2: the v and A v bases and a few device scalars
+    DevBuf<double> V2, AV2, g2;
+    int g2_cap = 0;
     int gm_m = 0;
     GraphCache graphs;
     void ensure(int n, int max_blocks, int hist_cap);
@@ -63,6 +66,9 @@ int run_gmres(SolverWork& w, Matrix* A, const Precond<double>& M, const double* 
               int max_restarts, int use_graph, int chunk);
 int run_mixed_cg(SolverWork& w, Matrix* A, const Precond<float>& M, const double* b, double* x, double tol,
                  int maxit, double inner_rtol, int use_graph, int chunk, int* inner_iters, double* hist, int hist_cap);
+int run_gmres2(SolverWork& w, Matrix* A, const Precond<double>& M, const double* b, double* x, double tol,
+               int maxit, int max_restarts, int basis_cap, int* iters, int* restarts, double* final_norm,
+               double* hist, int hist_cap);
 uint64_t next_uid();
 
 }  // namespace jfg

@@ -202,7 +202,10 @@ static Matrix* build_from_sorted(Context* c, int rows, int cols, int64_t m, cons
     // threads per row: 1 on large matrices, 4 or 8 on small ones (JFEM_TPR overrides)
     double avg = rows ? (double)m / rows : 0.0;
     int tl = rows >= 262144 ? 0 : (avg >= 10.0 ? 3 : 2);
-    if (const char* e = getenv("JFEM_TPR")) tl = std::max(0, std::min(3, atoi(e)));
+    if (const char* e = getenv("JFEM_TPR")) {
+        int v = atoi(e);
+        tl = v <= 0 ? 0 : (v <= 2 ? 2 : 3);   // the SpMV is instantiated for 1, 4 and 8 threads per row
+    }
     M->tpr_log2 = tl;
     M->nblocks = std::max(1, (int)((((int64_t)nslices * kSliceRows << tl) + kThreads - 1) / kThreads));
     M->off.alloc((size_t)nslices + 1);

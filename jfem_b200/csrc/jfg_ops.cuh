@@ -124,7 +124,20 @@ void spmv_launch(cudaStream_t st, const Matrix* M, const VT* val, const XT* x, E
     if (M->rows == 0) return;
     GridRed<NR, Fin> red{sc.partials, sc.counter, fin};
     SpmvArgs a{M->off.p, M->perm.p, M->col.p, M->nslices * kSliceRows, M->tpr_log2};
-    launch_ex(k_spmv<VT, XT, NR, Epi, Fin>, dim3(M->nblocks), dim3(kThreads), 0, st, a, val, x, epi, red, done);
+    switch (M->tpr_log2) {
+    case 0:
+        launch_ex(k_spmv<VT, XT, NR, 1, Epi, Fin>, dim3(M->nblocks), dim3(kThreads), 0, st, a, val, x, epi, red,
+                  done);
+        break;
+    case 2:
+        launch_ex(k_spmv<VT, XT, NR, 4, Epi, Fin>, dim3(M->nblocks), dim3(kThreads), 0, st, a, val, x, epi, red,
+                  done);
+        break;
+    default:
+        launch_ex(k_spmv<VT, XT, NR, 8, Epi, Fin>, dim3(M->nblocks), dim3(kThreads), 0, st, a, val, x, epi, red,
+                  done);
+        break;
+    }
 }
 
 inline int vec_grid(int n)

@@ -273,6 +273,36 @@ class GMRES:
         self.ITERATIONS_BEFORE_RESTART = 150
 
 
+class GMRES2:
+    """linalg/GMRES2.java: minimal residual along A-orthonormalised Krylov
+    directions (Arnoldi.java).  As in the Java class, the iterate persists
+    between calls (field ``iterate``, starting at e0)."""
+
+    def __init__(self, tol: float, ctx: N.Context | None = None):
+        self.tol = float(tol)
+        self.iterate = None
+        self.ctx = ctx
+        self.last = None
+        self.iterations = 0
+
+    def solve(self, A, b_or_preconditioner, b=None):
+        """solve(A, b) or solve(A, M, b) (GMRES2.java:34-58)."""
+        if b is None:
+            M, rhs = None, b_or_preconditioner
+        else:
+            M, rhs = b_or_preconditioner, b
+        s = IterativeSolver(ctx=self.ctx)
+        n = len(rhs)
+        if self.iterate is None:
+            self.iterate = np.zeros(n)
+            self.iterate[0] = 1.0
+        x = s._run(N.GMRES2, A, M, rhs, self.tol, self.iterate)
+        self.iterate = x
+        self.last = s.last
+        self.iterations = s.iterations
+        return x
+
+
 class SolveResult:
     def __init__(self, info: N.SolveInfo, history: np.ndarray):
         self.iterations = info.iterations

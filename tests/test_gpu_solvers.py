@@ -118,6 +118,37 @@ def test_kat_gmres_bicgstab(ctx, name):
     np.testing.assert_allclose(got, x, atol=1e-9)
 
 
+@pytest.mark.parametrize("name", ["symm", "nonsymm", "good_nonsymm"])
+def test_kat_gmres2(ctx, name):
+    """GMResTest.java: GMRES2(1e-12).solve(A, b) and solve(A, I, b) equal solve(b)."""
+    from jfem_b200.linalg import GMRES2, DenseMatrix
+    k = kat()["systems"][name]
+    a = np.array(k["A"], float)
+    r, c = np.nonzero(a)
+    A = SparseMatrix.from_coo(3, 3, r, c, a[r, c], ctx)
+    b = np.array(k["b"], float)
+    x = np.array(k["x"])
+    np.testing.assert_allclose(GMRES2(1e-12, ctx).solve(A, b), x, atol=1e-9)
+    np.testing.assert_allclose(GMRES2(1e-12, ctx).solve(A, SparseMatrix.identity(3, ctx), b), x, atol=1e-9)
+    if name == "good_nonsymm":
+        inv = DenseMatrix(a, ctx).inverse()
+        ri, ci = np.nonzero(inv)
+        Minv = SparseMatrix.from_coo(3, 3, ri, ci, inv[ri, ci], ctx)
+        np.testing.assert_allclose(GMRES2(1e-12, ctx).solve(A, Minv, b), x, atol=1e-9)
+
+
+def test_gmres2_fe_matches_oracle(ctx):
+    from jfem_b200.linalg import GMRES2
+    sp, sy = fe_system(1, 12)
+    tol = 1e-9 * np.linalg.norm(sy.rhs)
+    ref = O.solve_gmres2(coo_oracle(sy), sy.rhs, tol)
+    g = GMRES2(tol, ctx)
+    x = g.solve(dev(sy, ctx), sy.rhs)
+    assert g.last.status == N.OK
+    assert rel(x, ref.x) < 1e-7
+    assert abs(g.iterations - ref.iterations) <= 2
+
+
 def test_gmres_fe_matches_oracle(ctx):
     sp, sy = fe_system(1, 24)
     tol = 1e-10 * np.linalg.norm(sy.rhs)
