@@ -185,6 +185,46 @@ int jfg_solve(jfg_ctx* ctx, int kind, jfg_mat* A, int precond_kind, void* precon
 int jfg_solve_dev(jfg_ctx* ctx, int kind, jfg_mat* A, int precond_kind, void* precond, const double* d_b,
                   double* d_x, const jfg_solver_opts* opts, jfg_solve_info* info);
 
+/* ---- batched implicit time stepping ----------------------------------- */
+/* Many independent systems of uneven size advanced together by implicit
+ * Euler: K_s u_s^{k+1} = M_s u_s^k + f_s with K_s = M_s + dt A_s, for every
+ * system s and step k, each solve an FP32 Jacobi-PCG inside an FP64
+ * refinement loop accepted on the FP64 relative true residual.  Replaces the
+ * time loop of Examples/src/HeatEquation.java:81-94 (solveCG(M + dt A,
+ * source + M u, 1e-10) per step) and FullyImplicitParabolicIntegrator.timeStep
+ * (Core/src/main/java/basic/FullyImplicitParabolicIntegrator.java:41-53) for a
+ * whole batch.  All systems' iterations run in one persistent launch:
+ * thread-block clusters take systems from a work queue (largest first) and
+ * reduce across the cluster through distributed shared memory. */
+typedef struct jfg_batch jfg_batch;
+typedef struct {
+    int cluster;        /* CTAs per system (1, 2, 4, 8); 0 = autotuned */
+    int threads;        /* threads per CTA (256, 512); 0 = autotuned */
+    double rtol;        /* relative FP64 residual per step (default 1e-10) */
+    double inner_rtol;  /* FP32 inner PCG relative tolerance (default 1e-5) */
+    int inner_max;      /* inner iteration cap (default 500) */
+    int max_refine;     /* refinement steps per time step (default 6) */
+} jfg_batch_opts;
+typedef struct {
+    int total_inner_iterations;
+    int max_refine_used;
+    double max_rel_residual;   /* worst FP64 relative residual over systems (last step) */
+    int failed;                /* systems that missed rtol within max_refine */
+    int cluster, threads;      /* configuration used */
+    double ms;                 /* device time of the persistent launch */
+} jfg_batch_info;
+void jfg_batch_opts_default(jfg_batch_opts* o);
+/* K[s], M[s]: square matrices of the same size n_s; f (optional) packed
+ * sum_s n_s right-hand-side increments added every step. */
+int jfg_batch_create(jfg_ctx* ctx, int nsys, jfg_mat* const* K, jfg_mat* const* M, jfg_batch** out);
+int jfg_batch_free(jfg_batch* b);
+/* Total unknowns (sum of n_s) and the offset of system s in packed vectors. */
+int jfg_batch_layout(jfg_batch* b, int64_t* total, int64_t* offsets);
+/* Advances every system `steps` implicit-Euler steps.  h_u: packed FP64
+ * states (in: u0, out: u after the last step); h_f: packed increments or NULL. */
+int jfg_batch_heat(jfg_batch* b, int steps, const double* h_f, double* h_u, const jfg_batch_opts* opts,
+                   jfg_batch_info* info);
+
 /* ---- dense direct solves --------------------------------------------- */
 /* x = A^-1 b for a dense row-major n x n A (partial-pivot LU on the GPU).
  * Replaces DenseMatrix.solve (linalg/DenseMatrix.java:516-519) and the JNI

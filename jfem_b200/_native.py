@@ -33,6 +33,7 @@ EXPORTED = [
     "jfg_mg_create", "jfg_mg_free", "jfg_mg_apply", "jfg_mg_vcycle", "jfg_mg_fmg",
     "jfg_solver_opts_default", "jfg_solve", "jfg_solve_dev",
     "jfg_dense_solve", "jfg_dense_inverse", "jfg_sparse_solve", "jfg_cg_noalloc",
+    "jfg_batch_opts_default", "jfg_batch_create", "jfg_batch_free", "jfg_batch_layout", "jfg_batch_heat",
 ]
 
 
@@ -54,6 +55,17 @@ class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("restarts", C.c_int), ("status", C.c_int),
                 ("outer_iterations", C.c_int), ("final_residual", C.c_double), ("final_norm", C.c_double),
                 ("history_len", C.c_int), ("not_pd", C.c_int)]
+
+
+class BatchOpts(C.Structure):
+    _fields_ = [("cluster", C.c_int), ("threads", C.c_int), ("rtol", C.c_double), ("inner_rtol", C.c_double),
+                ("inner_max", C.c_int), ("max_refine", C.c_int)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("total_inner_iterations", C.c_int), ("max_refine_used", C.c_int),
+                ("max_rel_residual", C.c_double), ("failed", C.c_int), ("cluster", C.c_int),
+                ("threads", C.c_int), ("ms", C.c_double)]
 
 
 class JfgError(RuntimeError):
@@ -111,6 +123,12 @@ def load():
     L.jfg_dense_inverse.argtypes = [_P, C.c_int, _D, _D]
     L.jfg_sparse_solve.argtypes = [_P, C.c_int, C.c_int64, _I, _I, _D, _D, _D]
     L.jfg_cg_noalloc.argtypes = [_P, C.c_int, _P, _P, _P, _P, _P, C.c_double, C.c_int, _I, _D]
+    L.jfg_batch_opts_default.restype = None
+    L.jfg_batch_opts_default.argtypes = [C.POINTER(BatchOpts)]
+    L.jfg_batch_create.argtypes = [_P, C.c_int, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]
+    L.jfg_batch_free.argtypes = [_P]
+    L.jfg_batch_layout.argtypes = [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.jfg_batch_heat.argtypes = [_P, C.c_int, _D, _D, C.POINTER(BatchOpts), C.POINTER(BatchInfo)]
     _lib = L
     return L
 

@@ -171,13 +171,15 @@ class System:
 
 
 def assemble(space: Space, grad_coef=1.0, mass_coef=0.0, source=None, boundary_value=None,
-             grad_coef_cells=None) -> System:
+             grad_coef_cells=None, dirichlet=True) -> System:
     """GRAD_GRAD * grad_coef + VALUE_VALUE * mass_coef with a VALUE right-hand
     side ``source(x, y)`` and Dirichlet data ``boundary_value(x, y)`` (zero
     when None) on the whole boundary.
 
     ``grad_coef_cells`` (length = number of cells) multiplies the GRAD_GRAD
     integral cell by cell (a piecewise-constant coefficient kappa).
+    ``dirichlet=False`` leaves the natural (Neumann) boundary: no row or
+    column is overwritten.
     """
     p = space.p
     gg, vv, bw = _ref_tables(p, space.hx, space.hy)
@@ -204,6 +206,8 @@ def assemble(space: Space, grad_coef=1.0, mass_coef=0.0, source=None, boundary_v
         cell_rhs = f @ bw                                    # (cells, nl)
         np.add.at(rhs, dofs.reshape(-1), cell_rhs.reshape(-1))
     bd = space.boundary_nodes()
+    if not dirichlet:
+        return System(space.n, R, Cc, V, rhs, np.zeros(0, dtype=np.int32))
     # Dirichlet (AcceptsMatrixBoundaryValues.overWriteValue)
     is_bd = np.zeros(space.n, dtype=bool)
     is_bd[bd] = True

@@ -22,6 +22,8 @@ namespace jfg {
 cudaStream_t ctx_stream(jfg_ctx* ctx) { return ctx->c.stream; }
 int ctx_device(jfg_ctx* ctx) { return ctx->c.device; }
 void ctx_set_error(jfg_ctx* ctx, const std::string& msg) { ctx->c.last_error = msg; }
+Matrix* mat_of(jfg_mat* m) { return m->m; }
+jfg_ctx* mat_ctx(jfg_mat* m) { return m->ctx; }
 }  // namespace jfg
 
 namespace {

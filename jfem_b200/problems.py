@@ -63,3 +63,37 @@ def hierarchy(p: int, coarse_cells: int, levels: int, mass: float = 5.0, modes: 
         systems.append(assemble(sp, 1.0, mass, source=f if l == levels - 1 else None, grad_coef_cells=kc))
     prol = [prolongation(spaces[l], spaces[l + 1]) for l in range(levels - 1)]
     return Hierarchy(spaces, systems, prol, [s.boundary for s in systems])
+
+
+@dataclass
+class HeatSystem:
+    space: Space
+    K: System        # M + dt A (COO)
+    M: System        # mass matrix (COO)
+    u0: np.ndarray
+
+
+def heat_batch(nsys: int = 256, sizes=tuple(range(32, 257, 16)), dt: float = 1e-3, bumps: int = 8,
+               seed: int = 0) -> list:
+    """The batched heat workload: `nsys` Q1 systems on the unit square with
+    cell grids drawn uniformly from `sizes` (square), implicit Euler
+    K = M + dt A with the natural boundary condition, and u0 = a seeded sum
+    of `bumps` Gaussian bumps with sigma ~ U(0.02, 0.1) (numpy Philox stream).
+    """
+    rng = np.random.Generator(np.random.Philox(seed))
+    out = []
+    for s in range(nsys):
+        c = int(rng.choice(np.asarray(sizes)))
+        sp = Space(1, c, c)
+        Mm = assemble(sp, 0.0, 1.0, dirichlet=False)
+        Ka = assemble(sp, dt, 1.0, dirichlet=False)
+        cx = rng.uniform(0.15, 0.85, bumps)
+        cy = rng.uniform(0.15, 0.85, bumps)
+        sg = rng.uniform(0.02, 0.1, bumps)
+        am = rng.standard_normal(bumps)
+        px, py = sp.node_points()
+        u0 = np.zeros(sp.n)
+        for j in range(bumps):
+            u0 += am[j] * np.exp(-((px - cx[j]) ** 2 + (py - cy[j]) ** 2) / (2 * sg[j] ** 2))
+        out.append(HeatSystem(sp, Ka, Mm, u0))
+    return out

@@ -1,0 +1,68 @@
+"""Batched implicit-Euler heat stepping in one persistent launch, against the
+oracle's per-step FP64 CG (HeatEquation.java:81-94 for every system)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from jfem_b200 import problems
+from jfem_b200.batch import BatchedParabolicIntegrator
+from jfem_b200.linalg import DeviceMatrix
+
+pytestmark = pytest.mark.gpu
+
+
+def build(ctx, batch):
+    K = [DeviceMatrix(s.K.n, s.K.n, s.K.rows, s.K.cols, s.K.vals, ctx) for s in batch]
+    M = [DeviceMatrix(s.M.n, s.M.n, s.M.rows, s.M.cols, s.M.vals, ctx) for s in batch]
+    return BatchedParabolicIntegrator(K, M, ctx)
+
+
+def oracle_steps(s, steps):
+    K = O.CooMatrix(s.K.n, s.K.n, s.K.rows, s.K.cols, s.K.vals)
+    M = O.CooMatrix(s.M.n, s.M.n, s.M.rows, s.M.cols, s.M.vals)
+    u = s.u0.copy()
+    for _ in range(steps):
+        rhs = M.mvmul(u)
+        r = O.solve_cg(K, rhs, 1e-13 * np.linalg.norm(rhs), x0=u)
+        u = r.x
+    return u
+
+
+@pytest.mark.parametrize("cluster,threads", [(1, 256), (2, 512), (4, 256), (8, 512)])
+def test_batch_matches_oracle(ctx, cluster, threads):
+    batch = problems.heat_batch(nsys=7, sizes=(4, 8, 12, 16, 24), dt=1e-3, seed=5)
+    B = build(ctx, batch)
+    steps = 4
+    u = B.timeSteps([s.u0 for s in batch], steps, cluster=cluster, threads=threads)
+    assert B.last.status == 0 and B.last.failed == 0
+    assert B.last.max_rel_residual <= 1e-10
+    assert (B.last.cluster, B.last.threads) == (cluster, threads)
+    for s, us in zip(batch, B.unpack(u)):
+        ref = oracle_steps(s, steps)
+        assert np.linalg.norm(us - ref) / np.linalg.norm(ref) < 1e-8
+
+
+def test_batch_autotune_and_uneven_sizes(ctx):
+    batch = problems.heat_batch(nsys=20, sizes=(8, 16, 32, 48), dt=1e-3, seed=11)
+    B = build(ctx, batch)
+    u = B.timeSteps([s.u0 for s in batch], 3)
+    assert B.last.failed == 0 and B.last.cluster in (1, 2, 4, 8) and B.last.threads in (256, 512)
+    for s, us in zip(batch[:4], B.unpack(u)[:4]):
+        ref = oracle_steps(s, 3)
+        assert np.linalg.norm(us - ref) / np.linalg.norm(ref) < 1e-8
+
+
+def test_batch_full_size_conservation(ctx):
+    """256 Q1 systems, cells from {32, 48, ..., 256}^2, dt = 1e-3,
+    50 steps.  With the natural boundary the mass 1^T M u is conserved by
+    implicit Euler and the M-energy decays; both hold per system."""
+    batch = problems.heat_batch(nsys=256, dt=1e-3, seed=0)
+    B = build(ctx, batch)
+    u = B.timeSteps([s.u0 for s in batch], 50)
+    assert B.last.failed == 0 and B.last.max_rel_residual <= 1e-10
+    for s, us in zip(batch, B.unpack(u)):
+        M = O.CooMatrix(s.M.n, s.M.n, s.M.rows, s.M.cols, s.M.vals)
+        m0 = M.mvmul(s.u0).sum()
+        m1 = M.mvmul(us).sum()
+        assert abs(m1 - m0) <= 1e-9 * max(1.0, abs(m0)) + 1e-9 * np.abs(M.mvmul(s.u0)).sum()
+        assert us @ M.mvmul(us) <= s.u0 @ M.mvmul(s.u0) * (1 + 1e-12)
