@@ -225,6 +225,30 @@ int jfg_batch_layout(jfg_batch* b, int64_t* total, int64_t* offsets);
 int jfg_batch_heat(jfg_batch* b, int steps, const double* h_f, double* h_u, const jfg_batch_opts* opts,
                    jfg_batch_info* info);
 
+/* ---- learned smoother network ------------------------------------------ */
+/* No counterpart in the reference (JFEM has no neural-network code): a 6-layer
+ * 3x3 convolutional residual network on the node grid (32 channels, no
+ * biases), BF16 tensor-core forward and backward kernels with FP32
+ * accumulation, FP32 Adam master weights.  Images are (B, H, W) FP32 device
+ * arrays.  Weights: 37,440 FP32 values, layer by layer in (Cout, Cin, 3, 3)
+ * order (conv1 32x1, conv2..5 32x32, conv6 1x32). */
+typedef struct jfg_cnn jfg_cnn;
+int jfg_cnn_num_params(int* count);
+int jfg_cnn_create(jfg_ctx* ctx, jfg_cnn** out);
+int jfg_cnn_free(jfg_cnn* n);
+int jfg_cnn_set_weights(jfg_cnn* n, const float* h_w);
+int jfg_cnn_get_weights(jfg_cnn* n, float* h_w);
+/* y = net(x) on device images. */
+int jfg_cnn_forward_dev(jfg_cnn* n, int B, int H, int W, const float* d_x, float* d_y);
+/* loss = mean (net(x) - t)^2 and its weight gradient (kept for the next
+ * Adam step; copied to h_grad when non-NULL). */
+int jfg_cnn_loss_grad_dev(jfg_cnn* n, int B, int H, int W, const float* d_x, const float* d_t, double* loss,
+                          float* h_grad);
+/* One Adam step with the last computed gradient. */
+int jfg_cnn_adam_step(jfg_cnn* n, double lr, double beta1, double beta2, double eps);
+/* Times the forward pass (ms per pass) and one 32 -> 32 tensor-core layer. */
+int jfg_cnn_time_forward(jfg_cnn* n, int B, int H, int W, int iters, double* ms_total, double* ms_mid);
+
 /* ---- dense direct solves --------------------------------------------- */
 /* x = A^-1 b for a dense row-major n x n A (partial-pivot LU on the GPU).
  * Replaces DenseMatrix.solve (linalg/DenseMatrix.java:516-519) and the JNI

@@ -34,6 +34,8 @@ EXPORTED = [
     "jfg_solver_opts_default", "jfg_solve", "jfg_solve_dev",
     "jfg_dense_solve", "jfg_dense_inverse", "jfg_sparse_solve", "jfg_cg_noalloc",
     "jfg_batch_opts_default", "jfg_batch_create", "jfg_batch_free", "jfg_batch_layout", "jfg_batch_heat",
+    "jfg_cnn_num_params", "jfg_cnn_create", "jfg_cnn_free", "jfg_cnn_set_weights", "jfg_cnn_get_weights",
+    "jfg_cnn_forward_dev", "jfg_cnn_loss_grad_dev", "jfg_cnn_adam_step", "jfg_cnn_time_forward",
 ]
 
 
@@ -129,6 +131,15 @@ def load():
     L.jfg_batch_free.argtypes = [_P]
     L.jfg_batch_layout.argtypes = [_P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.jfg_batch_heat.argtypes = [_P, C.c_int, _D, _D, C.POINTER(BatchOpts), C.POINTER(BatchInfo)]
+    L.jfg_cnn_num_params.argtypes = [_I]
+    L.jfg_cnn_create.argtypes = [_P, C.POINTER(_P)]
+    L.jfg_cnn_free.argtypes = [_P]
+    L.jfg_cnn_set_weights.argtypes = [_P, _F]
+    L.jfg_cnn_get_weights.argtypes = [_P, _F]
+    L.jfg_cnn_forward_dev.argtypes = [_P, C.c_int, C.c_int, C.c_int, _P, _P]
+    L.jfg_cnn_loss_grad_dev.argtypes = [_P, C.c_int, C.c_int, C.c_int, _P, _P, _D, _F]
+    L.jfg_cnn_adam_step.argtypes = [_P, C.c_double, C.c_double, C.c_double, C.c_double]
+    L.jfg_cnn_time_forward.argtypes = [_P, C.c_int, C.c_int, C.c_int, C.c_int, _D, _D]
     _lib = L
     return L
 

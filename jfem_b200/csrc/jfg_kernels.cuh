@@ -118,6 +118,8 @@ __device__ __forceinline__ float to_acc(__nv_bfloat16 v) { return __bfloat162flo
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;"); }
 
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
 
 // ---------------------------------------------------------------------------
 // SELL-32-sigma SpMV: row sums handed to an epilogue

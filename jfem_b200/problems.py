@@ -97,3 +97,47 @@ def heat_batch(nsys: int = 256, sizes=tuple(range(32, 257, 16)), dt: float = 1e-
             u0 += am[j] * np.exp(-((px - cx[j]) ** 2 + (py - cy[j]) ** 2) / (2 * sg[j] ** 2))
         out.append(HeatSystem(sp, Ka, Mm, u0))
     return out
+
+
+def grf_cells(cells: int, length: float = 0.05, variance: float = 1.0, seed: int = 0) -> np.ndarray:
+    """A stationary Gaussian random field with squared-exponential covariance
+    sigma^2 exp(-d^2 / (2 l^2)) sampled at the cell centres of a cells x cells
+    grid on the unit square, by circulant embedding on a periodic grid of
+    twice the size (exact covariance, FFT sampling, seeded Philox stream)."""
+    N = 2 * cells
+    h = 1.0 / cells
+    idx = np.arange(N)
+    d = np.minimum(idx, N - idx) * h
+    cov = variance * np.exp(-(d[:, None] ** 2 + d[None, :] ** 2) / (2 * length ** 2))
+    lam = np.maximum(np.fft.fft2(cov).real, 0.0)
+    rng = np.random.Generator(np.random.Philox(seed))
+    w = rng.standard_normal((N, N))
+    g = np.fft.ifft2(np.sqrt(lam) * np.fft.fft2(w)).real
+    return g[:cells, :cells]
+
+
+def coarsen_cells(k: np.ndarray) -> np.ndarray:
+    """Arithmetic mean over 2x2 blocks of cells."""
+    return 0.25 * (k[0::2, 0::2] + k[1::2, 0::2] + k[0::2, 1::2] + k[1::2, 1::2])
+
+
+def kappa_hierarchy(p: int, coarse_cells: int, levels: int, length=0.05, variance=1.0, kseed=0, modes=4,
+                    fseed=0) -> tuple:
+    """-div(kappa grad u) = f with kappa = exp(g), g a GRF on the finest cells;
+    coarse levels rediscretise with 2x2-averaged kappa.  Returns the hierarchy
+    and the finest kappa (cells x cells, index [ix, iy])."""
+    fine = coarse_cells << (levels - 1)
+    kf = np.exp(grf_cells(fine, length, variance, kseed))
+    ks = [kf]
+    for _ in range(levels - 1):
+        ks.append(coarsen_cells(ks[-1]))
+    ks = ks[::-1]
+    spaces = [Space(p, coarse_cells << l, coarse_cells << l) for l in range(levels)]
+    f, _ = modes_source(modes, fseed)
+    systems = []
+    for l, sp in enumerate(spaces):
+        # Space orders cells with the y index fastest (ix-major)
+        systems.append(assemble(sp, 1.0, 0.0, source=f if l == levels - 1 else None,
+                                grad_coef_cells=ks[l].reshape(-1)))
+    prol = [prolongation(spaces[l], spaces[l + 1]) for l in range(levels - 1)]
+    return Hierarchy(spaces, systems, prol, [s.boundary for s in systems]), kf

@@ -1,0 +1,34 @@
+"""The float64 numpy oracle of the learned smoother: analytic gradients
+against central finite differences (no GPU)."""
+import numpy as np
+
+import oracle.cnn_oracle as CO
+
+
+def test_oracle_gradients_finite_differences():
+    rng = np.random.default_rng(0)
+    w = CO.init_weights(C=4, seed=1)
+    x = rng.standard_normal((2, 5, 6))
+    t = rng.standard_normal((2, 5, 6))
+    _, g = CO.loss_and_grads(w, x, t)
+    for li in range(6):
+        for _ in range(3):
+            idx = tuple(int(rng.integers(0, s)) for s in w[li].shape)
+            e = 1e-6
+            wp = [a.copy() for a in w]
+            wp[li][idx] += e
+            wm = [a.copy() for a in w]
+            wm[li][idx] -= e
+            fd = (CO.loss_and_grads(wp, x, t)[0] - CO.loss_and_grads(wm, x, t)[0]) / (2 * e)
+            assert abs(fd - g[li][idx]) <= 1e-6 * max(1.0, abs(fd)), (li, idx)
+
+
+def test_conv_adjoint():
+    """<conv(x, w), g> = <x, conv_grad_input(g, w)>."""
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal((2, 7, 5, 3))
+    w = rng.standard_normal((4, 3, 3, 3))
+    g = rng.standard_normal((2, 7, 5, 4))
+    lhs = np.sum(CO.conv(x, w) * g)
+    rhs = np.sum(x * CO.conv_grad_input(g, w))
+    assert abs(lhs - rhs) <= 1e-10 * abs(lhs)

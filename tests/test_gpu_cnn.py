@@ -1,0 +1,70 @@
+"""The learned smoother network: GPU forward and backward kernels against the
+float64 numpy oracle (oracle/cnn_oracle.py), and GPU training."""
+import numpy as np
+import pytest
+import torch
+
+import oracle.cnn_oracle as CO
+from jfem_b200.cnn import LearnedSmoother, he_init, num_params, unpack
+
+pytestmark = pytest.mark.gpu
+
+
+def bf16_round(a):
+    t = torch.from_numpy(np.asarray(a, dtype=np.float32)).to(torch.bfloat16).to(torch.float32)
+    return t.numpy().astype(np.float64)
+
+
+@pytest.mark.parametrize("shape", [(1, 16, 16), (2, 19, 37), (3, 33, 8)])
+def test_forward_matches_oracle(ctx, shape):
+    rng = np.random.default_rng(1)
+    w = he_init(seed=2, gain_last=1.0)
+    x = rng.standard_normal(shape).astype(np.float32)
+    net = LearnedSmoother(ctx, w)
+    y = net.forward(torch.from_numpy(x).cuda()).cpu().numpy()
+    # the GPU rounds weights and activations to BF16: compare with the oracle on
+    # BF16-rounded weights, tolerance of a few BF16 ulps accumulated over 6 layers
+    yr, _ = CO.forward([bf16_round(a) for a in unpack(w)], x.astype(np.float64))
+    err = np.linalg.norm(y - yr) / np.linalg.norm(yr)
+    assert err < 3e-2, err
+
+
+@pytest.mark.parametrize("shape", [(2, 16, 16), (1, 21, 18)])
+def test_gradient_matches_oracle(ctx, shape):
+    rng = np.random.default_rng(3)
+    w = he_init(seed=4, gain_last=1.0)
+    x = rng.standard_normal(shape).astype(np.float32)
+    t = rng.standard_normal(shape).astype(np.float32)
+    net = LearnedSmoother(ctx, w)
+    loss, g = net.loss_and_grad(torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda())
+    L, gr = CO.loss_and_grads([bf16_round(a) for a in unpack(w)], x.astype(np.float64), t.astype(np.float64))
+    assert abs(loss - L) / L < 2e-2
+    for l, (gg, rr) in enumerate(zip(unpack(g), gr)):
+        err = np.linalg.norm(gg - rr) / np.linalg.norm(rr)
+        assert err < 6e-2, (l, err)
+
+
+def test_training_reduces_loss(ctx):
+    """A few hundred Adam steps fit a fixed linear target operator (a 3x3
+    smoothing stencil) on random inputs."""
+    rng = np.random.default_rng(5)
+    net = LearnedSmoother(ctx, he_init(seed=6))
+    k = np.array([[1, 2, 1], [2, 4, 2], [1, 2, 1]], dtype=np.float64) / 16.0
+
+    def target(x):
+        xp = np.pad(x, ((0, 0), (1, 1), (1, 1)))
+        out = np.zeros_like(x)
+        for dy in range(3):
+            for dx in range(3):
+                out += k[dy, dx] * xp[:, dy:dy + x.shape[1], dx:dx + x.shape[2]]
+        return out
+
+    losses = []
+    for it in range(300):
+        x = rng.standard_normal((8, 32, 32))
+        t = target(x)
+        losses.append(net.train_step(torch.from_numpy(x.astype(np.float32)).cuda(),
+                                     torch.from_numpy(t.astype(np.float32)).cuda(), lr=2e-3))
+    assert np.mean(losses[-20:]) < 0.2 * np.mean(losses[:5])
+    w = net.get_weights()
+    assert w.size == num_params() == 37440 and np.all(np.isfinite(w))
