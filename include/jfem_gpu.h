@@ -130,14 +130,17 @@ typedef enum {
     JFG_PBICGSTAB = 3,   /* IterativeSolver.solvePBiCGStab (:325-402) */
     JFG_GMRES = 4,       /* IterativeSolver.solveGMRES / GMRES.solve (linalg/GMRES.java:103-134) */
     JFG_PGMRES = 5,      /* IterativeSolver.solvePGMRES / GMRES.solve with preconditioner (GMRES.java:64-101) */
-    JFG_GMRES2 = 6       /* GMRES2.solve (linalg/GMRES2.java:34-104) */
+    JFG_GMRES2 = 6,      /* GMRES2.solve (linalg/GMRES2.java:34-104) */
+    JFG_FGMRES = 7       /* flexible right-preconditioned GMRES(restart); no counterpart in the reference
+                            (needed for a preconditioner that changes between iterations) */
 } jfg_solver_kind;
 
 typedef enum {
     JFG_PREC_NONE = 0,
     JFG_PREC_MG = 1,       /* handle = jfg_mg* */
     JFG_PREC_JACOBI = 2,   /* diagonal of A */
-    JFG_PREC_MATRIX = 3    /* handle = jfg_mat* applied as y = M x (e.g. an identity or an inverse) */
+    JFG_PREC_MATRIX = 3,   /* handle = jfg_mat* applied as y = M x (e.g. an identity or an inverse) */
+    JFG_PREC_MG_CNN = 4    /* handle = jfg_mgcnn*: FP32 V-cycle followed by the learned smoother */
 } jfg_precond_kind;
 
 typedef enum {
@@ -248,6 +251,24 @@ int jfg_cnn_loss_grad_dev(jfg_cnn* n, int B, int H, int W, const float* d_x, con
 int jfg_cnn_adam_step(jfg_cnn* n, double lr, double beta1, double beta2, double eps);
 /* Times the forward pass (ms per pass) and one 32 -> 32 tensor-core layer. */
 int jfg_cnn_time_forward(jfg_cnn* n, int B, int H, int W, int iters, double* ms_total, double* ms_mid);
+
+/* The preconditioner "FP32 V-cycle, then the learned smoother" for FGMRES:
+ *   z = V(v);  r' = v - A z;  s = rms(r');
+ *   z += out_scale * s * scatter(net(gather(r') / s))   (zero on Dirichlet nodes)
+ * where the node grid is H x W and h_dof_of_pixel[i] is the unknown at pixel
+ * i (row-major).  The V-cycle runs on mg's FP32 copy of the hierarchy
+ * (built on first use); A is the system matrix.  use_net = 0 applies the
+ * V-cycle only (the method without the network, for comparison).  The
+ * network's current weights are used at every application.  Pass the handle
+ * to jfg_solve with JFG_PREC_MG_CNN and JFG_FGMRES. */
+typedef struct jfg_mgcnn jfg_mgcnn;
+int jfg_mgcnn_create(jfg_ctx* ctx, jfg_mg* mg, jfg_cnn* net, jfg_mat* A, int H, int W, const int* h_dof_of_pixel,
+                     const int* h_bdry, int n_bdry, double out_scale, int use_net, jfg_mgcnn** out);
+/* Changes out_scale and use_net of an existing handle. */
+int jfg_mgcnn_set(jfg_mgcnn* p, double out_scale, int use_net);
+/* z = the preconditioner applied to v (FP64 device vectors of the system size). */
+int jfg_mgcnn_apply_dev(jfg_mgcnn* p, const double* d_v, double* d_z);
+int jfg_mgcnn_free(jfg_mgcnn* p);
 
 /* ---- dense direct solves --------------------------------------------- */
 /* x = A^-1 b for a dense row-major n x n A (partial-pivot LU on the GPU).

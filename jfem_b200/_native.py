@@ -17,9 +17,9 @@ OK, NOT_CONVERGED, BREAKDOWN, NONFINITE, ERR_BAD_ARG, ERR_SINGULAR, ERR_CUDA, ER
 STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "BREAKDOWN", 3: "NONFINITE", 4: "BAD_ARG", 5: "SINGULAR",
                 6: "CUDA", 7: "NO_DEVICE", 8: "UNSUPPORTED"}
 # jfg_solver_kind
-CG, PCG, BICGSTAB, PBICGSTAB, GMRES, PGMRES, GMRES2 = range(7)
+CG, PCG, BICGSTAB, PBICGSTAB, GMRES, PGMRES, GMRES2, FGMRES = range(8)
 # jfg_precond_kind
-PREC_NONE, PREC_MG, PREC_JACOBI, PREC_MATRIX = range(4)
+PREC_NONE, PREC_MG, PREC_JACOBI, PREC_MATRIX, PREC_MG_CNN = range(5)
 # jfg_precision
 FP64, MIXED, MIXED_PRECOND = 0, 1, 2
 SMOOTH_JACOBI, SMOOTH_RICHARDSON = 0, 1
@@ -36,6 +36,7 @@ EXPORTED = [
     "jfg_batch_opts_default", "jfg_batch_create", "jfg_batch_free", "jfg_batch_layout", "jfg_batch_heat",
     "jfg_cnn_num_params", "jfg_cnn_create", "jfg_cnn_free", "jfg_cnn_set_weights", "jfg_cnn_get_weights",
     "jfg_cnn_forward_dev", "jfg_cnn_loss_grad_dev", "jfg_cnn_adam_step", "jfg_cnn_time_forward",
+    "jfg_mgcnn_create", "jfg_mgcnn_set", "jfg_mgcnn_apply_dev", "jfg_mgcnn_free",
 ]
 
 
@@ -140,6 +141,11 @@ def load():
     L.jfg_cnn_loss_grad_dev.argtypes = [_P, C.c_int, C.c_int, C.c_int, _P, _P, _D, _F]
     L.jfg_cnn_adam_step.argtypes = [_P, C.c_double, C.c_double, C.c_double, C.c_double]
     L.jfg_cnn_time_forward.argtypes = [_P, C.c_int, C.c_int, C.c_int, C.c_int, _D, _D]
+    L.jfg_mgcnn_create.argtypes = [_P, _P, _P, _P, C.c_int, C.c_int, _I, _I, C.c_int, C.c_double, C.c_int,
+                                   C.POINTER(_P)]
+    L.jfg_mgcnn_set.argtypes = [_P, C.c_double, C.c_int]
+    L.jfg_mgcnn_apply_dev.argtypes = [_P, _P, _P]
+    L.jfg_mgcnn_free.argtypes = [_P]
     _lib = L
     return L
 

@@ -112,3 +112,59 @@ class LearnedSmoother:
                 N.load().jfg_cnn_free(self._h)
         except Exception:
             pass
+
+
+class MGCNNPreconditioner:
+    """The nonlinear preconditioner "FP32 V-cycle of `mg`, then the learned
+    smoother" for FGMRES (libjfem_gpu.so's jfg_mgcnn):
+
+        z = V(v);  r' = v - A z;  s = rms(r');  z += out_scale * s * net(r' / s)
+
+    on the H x W node grid (``dof_of_pixel[i]`` is the unknown at row-major
+    pixel i), with the correction zeroed on the Dirichlet nodes ``boundary``.
+    ``use_net=False`` keeps only the V-cycle (the same preconditioner without
+    the network, for comparisons)."""
+
+    def __init__(self, mg, net: LearnedSmoother, A, H: int, W: int, dof_of_pixel, boundary, out_scale: float = 1.0,
+                 use_net: bool = True):
+        from .linalg import _as_device
+        self.mg, self.net = mg, net
+        self.A = _as_device(A)
+        self.ctx = self.A.ctx
+        self.n = self.A.rows
+        dof = np.ascontiguousarray(dof_of_pixel, dtype=np.int32)
+        bd = np.ascontiguousarray(boundary, dtype=np.int32)
+        h = C.c_void_p()
+        self.ctx.check(N.load().jfg_mgcnn_create(
+            self.ctx.handle, mg.handle, net.handle, self.A.handle, H, W, dof.ctypes.data_as(C.POINTER(C.c_int)),
+            bd.ctypes.data_as(C.POINTER(C.c_int)), int(bd.size), float(out_scale), 1 if use_net else 0,
+            C.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set(self, out_scale: float, use_net: bool = True):
+        self.ctx.check(N.load().jfg_mgcnn_set(self._h, float(out_scale), 1 if use_net else 0))
+
+    def apply_dev(self, v: torch.Tensor) -> torch.Tensor:
+        """z = M(v) for an FP64 CUDA vector."""
+        v = v.contiguous()
+        z = torch.empty_like(v)
+        torch.cuda.synchronize()
+        self.ctx.check(N.load().jfg_mgcnn_apply_dev(self._h, C.c_void_p(v.data_ptr()), C.c_void_p(z.data_ptr())))
+        return z
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                N.load().jfg_mgcnn_free(self._h)
+        except Exception:
+            pass
+
+
+def pixel_map(space):
+    """(H, W, dof_of_pixel) of a Q_p space's node grid: pixel (gx, gy) at
+    row-major index gx * W + gy holds unknown node_of_grid[gx * W + gy]."""
+    return space.nx, space.ny, np.ascontiguousarray(space.node_of_grid, dtype=np.int32)

@@ -460,11 +460,13 @@ static int solve_impl(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, cons
     JFG_CHECK(A && A->ctx == ctx, JFG_ERR_BAD_ARG, "matrix from another context");
     Matrix* M = A->m;
     JFG_CHECK(M->rows == M->cols, JFG_ERR_BAD_ARG, "matrix is not square");
-    JFG_CHECK(kind >= JFG_CG && kind <= JFG_GMRES2, JFG_ERR_BAD_ARG, "unknown solver kind");
-    JFG_CHECK(pk >= JFG_PREC_NONE && pk <= JFG_PREC_MATRIX, JFG_ERR_BAD_ARG, "unknown preconditioner kind");
+    JFG_CHECK(kind >= JFG_CG && kind <= JFG_FGMRES, JFG_ERR_BAD_ARG, "unknown solver kind");
+    JFG_CHECK(pk >= JFG_PREC_NONE && pk <= JFG_PREC_MG_CNN, JFG_ERR_BAD_ARG, "unknown preconditioner kind");
+    JFG_CHECK(pk != JFG_PREC_MG_CNN || kind == JFG_FGMRES, JFG_ERR_UNSUPPORTED,
+              "the multigrid + network preconditioner is nonlinear: use FGMRES");
     bool needs_prec = kind == JFG_PCG || kind == JFG_PBICGSTAB || kind == JFG_PGMRES;
     JFG_CHECK(!needs_prec || pk != JFG_PREC_NONE, JFG_ERR_BAD_ARG, "solver kind needs a preconditioner");
-    JFG_CHECK(needs_prec || kind == JFG_GMRES2 || pk == JFG_PREC_NONE, JFG_ERR_BAD_ARG,
+    JFG_CHECK(needs_prec || kind == JFG_GMRES2 || kind == JFG_FGMRES || pk == JFG_PREC_NONE, JFG_ERR_BAD_ARG,
               "solver kind takes no preconditioner");
     JFG_CHECK(o->tol >= 0 && std::isfinite(o->tol), JFG_ERR_BAD_ARG, "bad tolerance");
     int n = M->rows;
@@ -483,11 +485,12 @@ static int solve_impl(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, cons
     int mb = M->nblocks;
     if (mg) mb = std::max(mb, mg->d64->max_blocks());
     if (pm) mb = std::max(mb, pm->m->nblocks);
+    Precond<double> P64;
+    if (pk == JFG_PREC_MG_CNN) mb = std::max(mb, mgcnn_precond(ph, P64, n));
     int hcap = o->h_history ? std::max(o->history_cap, 1) : 1;
     w.ensure(n, mb, hcap);
     cudaStream_t st = ctx->c.stream;
     for (int i = 0; i < 12; i++) w.v64[i].alloc(n);
-    Precond<double> P64;
     P64.kind = pk;
     P64.n = n;
     if (mg) P64.mg = mg->d64.get();
@@ -610,6 +613,20 @@ static int solve_impl(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, cons
         res.iter = it;
         res.status = stt;
         res.res_norm = fn;
+    } else if (kind == JFG_FGMRES) {
+        Ctl h{};
+        h.tol = o->tol;
+        h.maxit = 1 << 30;
+        h.hist = hist;
+        h.hist_cap = hcap;
+        h.n = n;
+        h.restart_len = o->restart > 0 ? o->restart : 30;
+        h.status = JFG_NOT_CONVERGED;
+        JFG_CUDA(cudaMemcpyAsync(w.ctl.p, &h, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+        restarts = run_fgmres(w, M, P64, d_b, d_x, h.restart_len, o->max_restarts >= 0 ? o->max_restarts : 200,
+                              use_graph, chunk);
+        JFG_CUDA(cudaMemcpyAsync(&res, w.ctl.p, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+        JFG_CUDA(cudaStreamSynchronize(st));
     } else {  // GMRES / PGMRES
         Ctl h{};
         h.tol = o->tol;

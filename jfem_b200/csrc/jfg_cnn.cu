@@ -20,7 +20,7 @@
 #include <cmath>
 #include <cstring>
 
-#include "jfg_ops.cuh"
+#include "jfg_krylov.cuh"
 
 namespace jfg {
 
@@ -794,6 +794,201 @@ int jfg_cnn_time_forward(jfg_cnn* n, int B, int H, int W, int iters, double* ms_
         jfg::ctx_set_error(n->ctx, e.msg);
         return e.status;
     }
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// FP32 V-cycle followed by the learned smoother (a preconditioner for FGMRES)
+// ---------------------------------------------------------------------------
+struct jfg_mat;
+namespace jfg {
+Matrix* mat_of(jfg_mat* m);
+jfg_ctx* mat_ctx(jfg_mat* m);
+}  // namespace jfg
+
+struct jfg_mgcnn {
+    jfg_ctx* ctx = nullptr;
+    jfg_mg* mg = nullptr;
+    jfg_cnn* net = nullptr;
+    jfg::Matrix* A = nullptr;
+    int H = 0, W = 0, n = 0, use_net = 1;
+    double out_scale = 1.0;
+    uint64_t uid = jfg::next_uid();
+    jfg::DevBuf<int> dof;
+    jfg::DevBuf<unsigned char> bd;
+    jfg::DevBuf<float> r32, z32, img_in, img_out;
+    jfg::DevBuf<double> rp, scale;
+    jfg::DevBuf<double> partials;     // scratch of jfg_mgcnn_apply_dev
+    jfg::DevBuf<unsigned> counter;
+};
+
+namespace jfg {
+namespace {
+
+struct FinRms {   // scale = rms of the vector (1 when it is zero)
+    double* scale;
+    double invn;
+    __device__ void operator()(const double* s) const
+    {
+        double r = sqrt(s[0] * invn);
+        *scale = r > 0 ? r : 1.0;
+    }
+};
+
+__global__ void k_gather_img(int npix, const int* __restrict__ dof, const double* __restrict__ r,
+                             const double* __restrict__ scale, float* __restrict__ img)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < npix) img[i] = (float)(r[dof[i]] / *scale);
+}
+
+__global__ void k_scatter_img(int npix, const int* __restrict__ dof, const unsigned char* __restrict__ bd,
+                              const float* __restrict__ img, const double* __restrict__ scale, double out_scale,
+                              double* __restrict__ z)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npix) return;
+    int d = dof[i];
+    if (bd[d]) return;
+    z[d] += (double)img[i] * (*scale) * out_scale;
+}
+
+void mgcnn_apply(void* self, const double* v, double* z, const Scratch& sc, const int* done, cudaStream_t st)
+{
+    auto* p = static_cast<jfg_mgcnn*>(self);
+    const int n = p->n;
+    vec_launch<0>(st, n, VCast<double, float>{v, p->r32.p}, sc, done);
+    p->mg->fp32()->apply(p->r32.p, p->z32.p, sc, done, st);
+    vec_launch<0>(st, n, VCast<float, double>{p->z32.p, z}, sc, done);
+    if (!p->use_net) return;
+    spmv_launch<double, double, 1>(st, p->A, p->A->val.p, z, EpiResid<double>{v, p->rp.p}, sc, done,
+                                   FinRms{p->scale.p, 1.0 / n});
+    const int npix = p->H * p->W;
+    k_gather_img<<<(npix + 255) / 256, 256, 0, st>>>(npix, p->dof.p, p->rp.p, p->scale.p, p->img_in.p);
+    // repack the BF16 weights every application: a replayed graph then always
+    // sees the current master weights
+    k_pack_weights<<<(4 * kMidParams + 255) / 256, 256, 0, st>>>(p->net->w32.p, p->net->wk.p, p->net->wt.p);
+    p->net->packed = true;
+    JFG_CUDA(cudaGetLastError());
+    note_launch(2);
+    cnn_forward(p->net, st, 1, p->H, p->W, p->img_in.p, p->img_out.p);
+    k_scatter_img<<<(npix + 255) / 256, 256, 0, st>>>(npix, p->dof.p, p->bd.p, p->img_out.p, p->scale.p,
+                                                       p->out_scale, z);
+    JFG_CUDA(cudaGetLastError());
+    note_launch();
+}
+
+}  // namespace
+
+// Fills a Precond<double> with the mgcnn hook; returns the largest SpMV grid.
+int mgcnn_precond(void* h, Precond<double>& P, int n)
+{
+    auto* p = static_cast<jfg_mgcnn*>(h);
+    JFG_CHECK(p && p->n == n, JFG_ERR_BAD_ARG, "multigrid + network preconditioner does not match the system size");
+    P.kind = JFG_PREC_MG_CNN;
+    P.hook = mgcnn_apply;
+    P.hook_self = p;
+    P.hook_uid = p->uid;
+    P.mg = nullptr;
+    P.n = n;
+    return std::max(p->mg->fp32()->max_blocks(), p->A->nblocks);
+}
+
+}  // namespace jfg
+
+extern "C" {
+
+int jfg_mgcnn_create(jfg_ctx* ctx, jfg_mg* mg, jfg_cnn* net, jfg_mat* A, int H, int W, const int* h_dof_of_pixel,
+                     const int* h_bdry, int n_bdry, double out_scale, int use_net, jfg_mgcnn** out)
+{
+    if (!ctx || !mg || !net || !A || !out || H < 1 || W < 1 || !h_dof_of_pixel || n_bdry < 0 ||
+        (n_bdry > 0 && !h_bdry))
+        return JFG_ERR_BAD_ARG;
+    *out = nullptr;
+    auto* p = new jfg_mgcnn();
+    try {
+        JFG_CUDA(cudaSetDevice(jfg::ctx_device(ctx)));
+        cudaStream_t st = jfg::ctx_stream(ctx);
+        jfg::Matrix* M = jfg::mat_of(A);
+        JFG_CHECK(jfg::mat_ctx(A) == ctx, JFG_ERR_BAD_ARG, "matrix from another context");
+        JFG_CHECK(M->rows == M->cols, JFG_ERR_BAD_ARG, "matrix is not square");
+        int n = M->rows;
+        JFG_CHECK((int64_t)H * W == n, JFG_ERR_BAD_ARG, "H * W must equal the number of unknowns");
+        JFG_CHECK(mg->d64 && mg->d64->n[mg->levels - 1] == n, JFG_ERR_BAD_ARG,
+                  "multigrid hierarchy does not match the matrix");
+        for (int i = 0; i < n; i++)
+            JFG_CHECK(h_dof_of_pixel[i] >= 0 && h_dof_of_pixel[i] < n, JFG_ERR_BAD_ARG, "pixel map out of range");
+        for (int i = 0; i < n_bdry; i++)
+            JFG_CHECK(h_bdry[i] >= 0 && h_bdry[i] < n, JFG_ERR_BAD_ARG, "boundary node out of range");
+        p->ctx = ctx;
+        p->mg = mg;
+        p->net = net;
+        p->A = M;
+        p->H = H;
+        p->W = W;
+        p->n = n;
+        p->use_net = use_net ? 1 : 0;
+        p->out_scale = out_scale;
+        mg->fp32();
+        p->dof.alloc(n);
+        p->bd.alloc(n);
+        p->r32.alloc(n);
+        p->z32.alloc(n);
+        p->img_in.alloc(n);
+        p->img_out.alloc(n);
+        p->rp.alloc(n);
+        p->scale.alloc(1);
+        std::vector<unsigned char> hb(n, 0);
+        for (int i = 0; i < n_bdry; i++) hb[h_bdry[i]] = 1;
+        JFG_CUDA(cudaMemcpyAsync(p->dof.p, h_dof_of_pixel, sizeof(int) * n, cudaMemcpyHostToDevice, st));
+        JFG_CUDA(cudaMemcpyAsync(p->bd.p, hb.data(), n, cudaMemcpyHostToDevice, st));
+        jfg::cnn_reserve(net, (size_t)n);
+        int mb = std::max(std::max(mg->fp32()->max_blocks(), M->nblocks), jfg::kVecGrid);
+        p->partials.alloc((size_t)4 * mb);
+        p->counter.alloc(4);
+        JFG_CUDA(cudaMemsetAsync(p->counter.p, 0, 4 * sizeof(unsigned), st));
+        JFG_CUDA(cudaStreamSynchronize(st));
+    } catch (const jfg::Error& e) {
+        jfg::ctx_set_error(ctx, e.msg);
+        delete p;
+        return e.status;
+    }
+    *out = p;
+    return JFG_OK;
+}
+
+int jfg_mgcnn_set(jfg_mgcnn* p, double out_scale, int use_net)
+{
+    if (!p || !std::isfinite(out_scale)) return JFG_ERR_BAD_ARG;
+    p->out_scale = out_scale;
+    p->use_net = use_net ? 1 : 0;
+    p->uid = jfg::next_uid();     // graphs captured with the old settings are not reused
+    return JFG_OK;
+}
+
+int jfg_mgcnn_apply_dev(jfg_mgcnn* p, const double* d_v, double* d_z)
+{
+    if (!p || !d_v || !d_z) return JFG_ERR_BAD_ARG;
+    try {
+        JFG_CUDA(cudaSetDevice(jfg::ctx_device(p->ctx)));
+        cudaStream_t st = jfg::ctx_stream(p->ctx);
+        jfg::Scratch sc{p->partials.p, p->counter.p};
+        jfg::mgcnn_apply(p, d_v, d_z, sc, nullptr, st);
+        JFG_CUDA(cudaStreamSynchronize(st));
+        return JFG_OK;
+    } catch (const jfg::Error& e) {
+        jfg::ctx_set_error(p->ctx, e.msg);
+        return e.status;
+    }
+}
+
+int jfg_mgcnn_free(jfg_mgcnn* p)
+{
+    if (!p) return JFG_ERR_BAD_ARG;
+    cudaStreamSynchronize(jfg::ctx_stream(p->ctx));
+    delete p;
+    return JFG_OK;
 }
 
 }  // extern "C"

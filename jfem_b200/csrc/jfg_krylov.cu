@@ -490,6 +490,9 @@ void Precond<T>::apply(const T* r, T* z, const Scratch& sc, const int* done, cud
     case JFG_PREC_MATRIX:
         spmv_launch<T, T, 0>(st, M, vals_of<T>(M), r, EpiStore<T>{z}, sc, done);
         break;
+    case JFG_PREC_MG_CNN:
+        hook(hook_self, r, z, sc, done, st);
+        break;
     default:
         vec_launch<0>(st, n, VCopy<T>{r, z}, sc, done);
         break;
@@ -807,6 +810,148 @@ int run_gmres(SolverWork& w, Matrix* A, const Precond<double>& M, const double* 
         Ctl hc = h;
         hc.status = JFG_OK;
         hc.done = 1;
+        JFG_CUDA(cudaMemcpyAsync(w.ctl.p, &hc, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+        break;
+    }
+    JFG_CUDA(cudaStreamSynchronize(st));
+    return restarts;
+}
+
+// ---------------------------------------------------------------------------
+// Flexible GMRES(m) with right preconditioning (Saad 1993): the
+// preconditioner may change between iterations (the learned smoother is
+// nonlinear), so z_j = M_j v_j is stored and x = x0 + Z y.  Classical
+// Gram-Schmidt with one re-orthogonalisation pass.  No counterpart in the
+// reference (its GMRES is left-preconditioned, GMRES.java:64-101).
+// ---------------------------------------------------------------------------
+namespace {
+template <typename T>
+struct VGmresW0 {    // w = q - sum_i V_i fac_i (no norm)
+    const T* V;
+    const T* q;
+    T* w;
+    const double* fac;
+    const Ctl* c;
+    int n;
+    template <int K> __device__ void operator()(int r, double (&)[K]) const
+    {
+        int j = c->j;
+        T lc = 0;
+        for (int i = 0; i <= j; i++) lc = lc + V[(size_t)i * n + r] * (T)fac[i];
+        w[r] = q[r] - lc;
+    }
+};
+struct FinGivensSum {   // h column = fac + fac2, then the rotations of FinGivens
+    FinGivens g;
+    const double* fac2;
+    double* facsum;
+    __device__ void operator()(const double* t) const
+    {
+        int j = g.c->j;
+        for (int i = 0; i <= j; i++) facsum[i] = g.fac[i] + fac2[i];
+        FinGivens g2 = g;
+        g2.fac = facsum;
+        g2(t);
+    }
+};
+struct VStoreCol {      // Z[:, j] = z
+    double* Z;
+    const double* z;
+    const Ctl* c;
+    int n;
+    template <int K> __device__ void operator()(int r, double (&)[K]) const { Z[(size_t)c->j * n + r] = z[r]; }
+};
+}  // namespace
+
+int run_fgmres(SolverWork& w, Matrix* A, const Precond<double>& M, const double* b, double* x, int m_restart,
+               int max_restarts, int use_graph, int chunk)
+{
+    cudaStream_t st = w.c->stream;
+    Ctl* c = w.ctl.p;
+    const int* cdone = &c->cycle_done;
+    int n = A->rows;
+    const Scratch& sc = w.sc;
+    const double* val = A->val.p;
+    int IBR = m_restart;
+    int m = IBR + 3;
+    int ldh = IBR + 10;
+    if (w.gm_m < m || w.V.n < (size_t)m * n) {
+        w.V.alloc((size_t)m * n);
+        w.gm_m = m;
+    }
+    w.Z.alloc((size_t)m * n);
+    w.H.alloc((size_t)ldh * ldh);
+    w.gam.alloc(ldh);
+    w.cs.alloc(ldh);
+    w.sn.alloc(ldh);
+    w.fac.alloc(ldh);
+    w.fac2.alloc(ldh);
+    w.facsum.alloc(ldh);
+    w.alpha.alloc(ldh);
+    int gx = vec_grid_n(n) < 296 ? vec_grid_n(n) : 296;
+    w.mdot_part.alloc((size_t)gx * m);
+    double *t = w.v64[2].p, *wv = w.v64[4].p, *vcur = w.v64[5].p, *rr = w.v64[6].p, *zcur = w.v64[7].p;
+    double* V = w.V.p;
+    double* Z = w.Z.p;
+    int restarts = 0;
+    int iter_before = read_ctl(w, 0).iter;
+    for (;;) {
+        JFG_CUDA(cudaMemsetAsync(w.H.p, 0, sizeof(double) * ldh * ldh, st));
+        JFG_CUDA(cudaMemsetAsync(w.gam.p, 0, sizeof(double) * ldh, st));
+        spmv_launch<double, double, 0>(st, A, val, x, EpiResid<double>{b, rr}, sc, nullptr);
+        vec_launch<1>(st, n, VNorm2<double>{rr}, sc, nullptr, FinGamma0{c, w.gam.p});
+        vec_launch<0>(st, n, VScaleInto2<double>{V, vcur, rr, w.gam.p}, sc, cdone);
+        auto iter = [&]() {
+            M.apply(vcur, zcur, sc, cdone, st);
+            vec_launch<0>(st, n, VStoreCol{Z, zcur, c, n}, sc, cdone);
+            spmv_launch<double, double, 0>(st, A, val, zcur, EpiStore<double>{t}, sc, cdone);
+            dim3 g1(gx, m);
+            // pass 1: fac = V^T t ; w = t - V fac
+            launch_ex(k_mdot<double>, g1, dim3(kThreads), 0, st, n, (const double*)V, (const double*)t,
+                      (const Ctl*)c, w.mdot_part.p, cdone);
+            launch_ex(k_mdot_fin, dim3(m), dim3(kThreads), 0, st, gx, (const double*)w.mdot_part.p, (const Ctl*)c,
+                      w.fac.p, cdone);
+            vec_launch<0>(st, n, VGmresW0<double>{V, t, wv, w.fac.p, c, n}, sc, cdone);
+            // pass 2: fac2 = V^T w ; w = w - V fac2 ; ||w|| ; Givens on fac + fac2
+            launch_ex(k_mdot<double>, g1, dim3(kThreads), 0, st, n, (const double*)V, (const double*)wv,
+                      (const Ctl*)c, w.mdot_part.p, cdone);
+            launch_ex(k_mdot_fin, dim3(m), dim3(kThreads), 0, st, gx, (const double*)w.mdot_part.p, (const Ctl*)c,
+                      w.fac2.p, cdone);
+            vec_launch<1>(st, n, VGmresW<double>{V, wv, wv, w.fac2.p, c, n}, sc, cdone,
+                          FinGivensSum{FinGivens{c, w.H.p, w.gam.p, w.cs.p, w.sn.p, w.fac.p, ldh}, w.fac2.p,
+                                       w.facsum.p});
+            vec_launch<0>(st, n, VGmresNext<double>{V, vcur, wv, w.H.p, c, n, ldh}, sc, cdone);
+            scalar_launch(st, GmresAdvance{c}, cdone);
+        };
+        std::vector<uintptr_t> key{7, (uintptr_t)A->uid, (uintptr_t)(M.mg ? M.mg->uid : 0),
+                                   (uintptr_t)(M.hook_uid), (uintptr_t)(M.mg32 ? M.mg32->uid : 0),
+                                   (uintptr_t)M.r32, (uintptr_t)M.kind, (uintptr_t)x, (uintptr_t)V, (uintptr_t)Z,
+                                   (uintptr_t)m, (uintptr_t)t, (uintptr_t)wv, (uintptr_t)vcur, (uintptr_t)zcur,
+                                   (uintptr_t)w.H.p, (uintptr_t)w.fac.p, (uintptr_t)w.fac2.p,
+                                   (uintptr_t)w.mdot_part.p, (uintptr_t)cdone};
+        int nodes = run_loop(w, cdone, key, iter, use_graph, chunk);
+        Ctl h = read_ctl(w, 0);
+        note_launch((unsigned long long)nodes * (unsigned long long)(h.iter - iter_before + 1));
+        iter_before = h.iter;
+        if (h.done) break;
+        scalar_launch(st, GmresAlpha{c, w.H.p, w.gam.p, w.alpha.p, ldh}, nullptr);
+        vec_launch<0>(st, n, VGmresX<double>{x, Z, w.alpha.p, c, n}, sc, nullptr);
+        spmv_launch<double, double, 1>(st, A, val, x, EpiResid<double>{b, t}, sc, nullptr, FinTrueRes{c});
+        h = read_ctl(w, 0);
+        Ctl hc = h;
+        hc.done = 1;
+        if (!std::isfinite(h.true_res) || h.status == JFG_NONFINITE) {
+            hc.status = JFG_NONFINITE;
+        } else if ((h.jfin > IBR && restarts < max_restarts) || h.true_res > h.tol) {
+            // the restart rule of GMRES.java:92, bounded by max_restarts
+            if (restarts < max_restarts) {
+                restarts++;
+                continue;
+            }
+            hc.status = JFG_NOT_CONVERGED;
+        } else {
+            hc.status = JFG_OK;
+        }
         JFG_CUDA(cudaMemcpyAsync(w.ctl.p, &hc, sizeof(Ctl), cudaMemcpyHostToDevice, st));
         break;
     }

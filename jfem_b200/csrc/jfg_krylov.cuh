@@ -20,6 +20,10 @@ struct Precond {
     MGImpl<float>* mg32 = nullptr;
     float* r32 = nullptr;
     float* z32 = nullptr;
+    // an external preconditioner (the multigrid + learned smoother of jfg_cnn.cu)
+    void (*hook)(void* self, const T* r, T* z, const Scratch& sc, const int* done, cudaStream_t st) = nullptr;
+    void* hook_self = nullptr;
+    uint64_t hook_uid = 0;
     void apply(const T* r, T* z, const Scratch& sc, const int* done, cudaStream_t st) const;
 };
 
@@ -48,6 +52,8 @@ struct SolverWork {
     // GMRES2: the v and A v bases and a few device scalars
     DevBuf<double> V2, AV2, g2;
     int g2_cap = 0;
+    // FGMRES: preconditioned directions and the second Gram-Schmidt pass
+    DevBuf<double> Z, fac2, facsum;
     int gm_m = 0;
     GraphCache graphs;
     void ensure(int n, int max_blocks, int hist_cap);
@@ -66,9 +72,14 @@ int run_gmres(SolverWork& w, Matrix* A, const Precond<double>& M, const double* 
               int max_restarts, int use_graph, int chunk);
 int run_mixed_cg(SolverWork& w, Matrix* A, const Precond<float>& M, const double* b, double* x, double tol,
                  int maxit, double inner_rtol, int use_graph, int chunk, int* inner_iters, double* hist, int hist_cap);
+int run_fgmres(SolverWork& w, Matrix* A, const Precond<double>& M, const double* b, double* x, int m_restart,
+               int max_restarts, int use_graph, int chunk);
 int run_gmres2(SolverWork& w, Matrix* A, const Precond<double>& M, const double* b, double* x, double tol,
                int maxit, int max_restarts, int basis_cap, int* iters, int* restarts, double* final_norm,
                double* hist, int hist_cap);
 uint64_t next_uid();
+// Fills P with the multigrid + learned-smoother hook of a jfg_mgcnn handle
+// (defined with the network kernels); returns its largest grid.
+int mgcnn_precond(void* handle, Precond<double>& P, int n);
 
 }  // namespace jfg

@@ -342,7 +342,7 @@ class IterativeSolver:
         self.history_cap = 4096
         self.last = None          # SolveResult of the last call
 
-    def _run(self, kind, op, prec, rhs, tol, x0, maxit=0):
+    def _run(self, kind, op, prec, rhs, tol, x0, maxit=0, restart=None):
         A = _as_device(op)
         ctx = A.ctx
         b = N.f64(rhs)
@@ -352,8 +352,11 @@ class IterativeSolver:
         pk, ph = N.PREC_NONE, None
         if prec is not None:
             from .multigrid import MGPreconditioner
+            from .cnn import MGCNNPreconditioner
             if isinstance(prec, MGPreconditioner):
                 pk, ph = N.PREC_MG, prec.handle
+            elif isinstance(prec, MGCNNPreconditioner):
+                pk, ph = N.PREC_MG_CNN, prec.handle
             elif isinstance(prec, (SparseMatrix, DeviceMatrix)):
                 pk, ph = N.PREC_MATRIX, _as_device(prec).handle
             elif prec == "jacobi":
@@ -364,7 +367,7 @@ class IterativeSolver:
         N.load().jfg_solver_opts_default(C.byref(opts))
         opts.tol = tol
         opts.maxit = maxit
-        opts.restart = self.gm.ITERATIONS_BEFORE_RESTART
+        opts.restart = self.gm.ITERATIONS_BEFORE_RESTART if restart is None else restart
         opts.max_restarts = self.gm.MAX_RESTARTS
         modes = {"fp64": N.FP64, "mixed": N.MIXED, "mixed-precond": N.MIXED_PRECOND}
         if self.precision not in modes:
@@ -407,6 +410,14 @@ class IterativeSolver:
     def solvePGMRES(self, operator, preconditioner, rhs, tol):
         # GMRES.solve with a preconditioner starts from zero (GMRES.java:59-60)
         return self._run(N.PGMRES, operator, preconditioner, rhs, tol, self._start(len(rhs), zero=True))
+
+    def solveFGMRES(self, operator, preconditioner, rhs, tol, restart: int = 30):
+        """Flexible right-preconditioned GMRES(restart) from zero; no
+        counterpart in the reference.  The preconditioner may change from one
+        application to the next (the multigrid + learned smoother).  Same
+        absolute tolerance and restart semantics as solveGMRES."""
+        return self._run(N.FGMRES, operator, preconditioner, rhs, tol, self._start(len(rhs), zero=True),
+                         restart=restart)
 
     def solveBiCGStab(self, operator, rhs, tol):
         return self._run(N.BICGSTAB, operator, None, rhs, tol, self._start(len(rhs)))
