@@ -253,8 +253,8 @@ int jfg_cnn_adam_step(jfg_cnn* n, double lr, double beta1, double beta2, double 
 int jfg_cnn_time_forward(jfg_cnn* n, int B, int H, int W, int iters, double* ms_total, double* ms_mid);
 
 /* The preconditioner "FP32 V-cycle, then the learned smoother" for FGMRES:
- *   z = V(v);  r' = v - A z;  s = rms(r');
- *   z += out_scale * s * scatter(net(gather(r') / s))   (zero on Dirichlet nodes)
+ *   z = V(v);  r' = v - A z;  q = D^-1 r' (D = diag A);  s = rms(q);
+ *   z += out_scale * s * scatter(net(gather(q) / s))   (zero on Dirichlet nodes)
  * where the node grid is H x W and h_dof_of_pixel[i] is the unknown at pixel
  * i (row-major).  The V-cycle runs on mg's FP32 copy of the hierarchy
  * (built on first use); A is the system matrix.  use_net = 0 applies the

@@ -118,7 +118,7 @@ class MGCNNPreconditioner:
     """The nonlinear preconditioner "FP32 V-cycle of `mg`, then the learned
     smoother" for FGMRES (libjfem_gpu.so's jfg_mgcnn):
 
-        z = V(v);  r' = v - A z;  s = rms(r');  z += out_scale * s * net(r' / s)
+        z = V(v);  r' = v - A z;  q = D^-1 r';  s = rms(q);  z += out_scale * s * net(q / s)
 
     on the H x W node grid (``dof_of_pixel[i]`` is the unknown at row-major
     pixel i), with the correction zeroed on the Dirichlet nodes ``boundary``.

@@ -836,11 +836,30 @@ struct FinRms {   // scale = rms of the vector (1 when it is zero)
     }
 };
 
+struct EpiResidJac {   // y = b - A x, acc += (y / diag)^2 (zero diagonals count as 1)
+    const double* b;
+    const double* diag;
+    double* y;
+    template <typename AT, int K>
+    __device__ void operator()(int r, AT s, double (&acc)[K]) const
+    {
+        double v = b[r] - (double)s;
+        y[r] = v;
+        double d = diag[r];
+        double q = v / (d != 0.0 ? d : 1.0);
+        acc[0] += q * q;
+    }
+};
+
 __global__ void k_gather_img(int npix, const int* __restrict__ dof, const double* __restrict__ r,
-                             const double* __restrict__ scale, float* __restrict__ img)
+                             const double* __restrict__ diag, const double* __restrict__ scale,
+                             float* __restrict__ img)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < npix) img[i] = (float)(r[dof[i]] / *scale);
+    if (i >= npix) return;
+    int d = dof[i];
+    double dg = diag[d];
+    img[i] = (float)(r[d] / (dg != 0.0 ? dg : 1.0) / *scale);
 }
 
 __global__ void k_scatter_img(int npix, const int* __restrict__ dof, const unsigned char* __restrict__ bd,
@@ -862,10 +881,11 @@ void mgcnn_apply(void* self, const double* v, double* z, const Scratch& sc, cons
     p->mg->fp32()->apply(p->r32.p, p->z32.p, sc, done, st);
     vec_launch<0>(st, n, VCast<float, double>{p->z32.p, z}, sc, done);
     if (!p->use_net) return;
-    spmv_launch<double, double, 1>(st, p->A, p->A->val.p, z, EpiResid<double>{v, p->rp.p}, sc, done,
+    spmv_launch<double, double, 1>(st, p->A, p->A->val.p, z, EpiResidJac{v, p->A->diag.p, p->rp.p}, sc, done,
                                    FinRms{p->scale.p, 1.0 / n});
     const int npix = p->H * p->W;
-    k_gather_img<<<(npix + 255) / 256, 256, 0, st>>>(npix, p->dof.p, p->rp.p, p->scale.p, p->img_in.p);
+    k_gather_img<<<(npix + 255) / 256, 256, 0, st>>>(npix, p->dof.p, p->rp.p, p->A->diag.p, p->scale.p,
+                                                      p->img_in.p);
     // repack the BF16 weights every application: a replayed graph then always
     // sees the current master weights
     k_pack_weights<<<(4 * kMidParams + 255) / 256, 256, 0, st>>>(p->net->w32.p, p->net->wk.p, p->net->wt.p);

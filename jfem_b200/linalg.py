@@ -200,6 +200,16 @@ class DeviceMatrix:
         self.ctx.check(N.load().jfg_spmv(self._h, N.dptr(x), N.dptr(y)))
         return y
 
+    def spmv_dev(self, x, y=None):
+        """y = A x for contiguous FP64 CUDA tensors (returns when y is written)."""
+        import torch
+        if y is None:
+            y = torch.empty(self.rows, dtype=torch.float64, device=x.device)
+        torch.cuda.synchronize()
+        self.ctx.check(N.load().jfg_spmv_dev(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())))
+        self.ctx.check(N.load().jfg_synchronize(self.ctx.handle))
+        return y
+
     def spmv_t(self, x):
         x = N.f64(x)
         y = np.empty(self.cols)
@@ -342,13 +352,18 @@ class IterativeSolver:
         self.history_cap = 4096
         self.last = None          # SolveResult of the last call
 
-    def _run(self, kind, op, prec, rhs, tol, x0, maxit=0, restart=None):
+    def _run(self, kind, op, prec, rhs, tol, x0, maxit=0, restart=None, device=False):
         A = _as_device(op)
         ctx = A.ctx
-        b = N.f64(rhs)
-        if b.shape != (A.rows,):
-            raise IllegalArgumentException("Vectors are of different size")
-        x = N.f64(x0).copy()
+        if device:      # FP64 CUDA tensors, x0 is updated in place
+            b, x = rhs, x0
+            if tuple(b.shape) != (A.rows,) or tuple(x.shape) != (A.rows,):
+                raise IllegalArgumentException("Vectors are of different size")
+        else:
+            b = N.f64(rhs)
+            if b.shape != (A.rows,):
+                raise IllegalArgumentException("Vectors are of different size")
+            x = N.f64(x0).copy()
         pk, ph = N.PREC_NONE, None
         if prec is not None:
             from .multigrid import MGPreconditioner
@@ -379,8 +394,14 @@ class IterativeSolver:
         opts.h_history = N.dptr(hist)
         opts.history_cap = self.history_cap
         info = N.SolveInfo()
-        st = N.load().jfg_solve(ctx.handle, kind, A.handle, pk, ph, N.dptr(b), N.dptr(x), C.byref(opts),
-                                C.byref(info))
+        if device:
+            import torch
+            torch.cuda.synchronize()
+            st = N.load().jfg_solve_dev(ctx.handle, kind, A.handle, pk, ph, C.c_void_p(b.data_ptr()),
+                                        C.c_void_p(x.data_ptr()), C.byref(opts), C.byref(info))
+        else:
+            st = N.load().jfg_solve(ctx.handle, kind, A.handle, pk, ph, N.dptr(b), N.dptr(x), C.byref(opts),
+                                    C.byref(info))
         ctx.check(st, allow=(N.OK, N.NOT_CONVERGED, N.NONFINITE))
         self.last = SolveResult(info, hist)
         self.iterations = info.iterations
@@ -418,6 +439,11 @@ class IterativeSolver:
         absolute tolerance and restart semantics as solveGMRES."""
         return self._run(N.FGMRES, operator, preconditioner, rhs, tol, self._start(len(rhs), zero=True),
                          restart=restart)
+
+    def solve_device(self, kind: int, operator, preconditioner, b, x, tol, maxit=0, restart=None):
+        """Any solver kind (``_native.CG`` ... ``_native.FGMRES``) on FP64 CUDA
+        tensors; x holds the start iterate and receives the solution."""
+        return self._run(kind, operator, preconditioner, b, tol, x, maxit=maxit, restart=restart, device=True)
 
     def solveBiCGStab(self, operator, rhs, tol):
         return self._run(N.BICGSTAB, operator, None, rhs, tol, self._start(len(rhs)))

@@ -70,7 +70,7 @@ def _mgcnn(ctx, h, mg, mats, weights, use_net=True, out_scale=1.0):
 
 
 def test_mgcnn_apply_matches_oracles(ctx):
-    """z = V32(v) + s * net(r'/s): the V-cycle part against the FP64
+    """z = V32(v) + s * net(D^-1 r' / s): the V-cycle part against the FP64
     multigrid oracle (FP32 tolerance), the network part against the float64
     network oracle run on the GPU's own r' (BF16 tolerance)."""
     h, mg_o, mg, mats = setup(ctx, L=4)
@@ -85,9 +85,9 @@ def test_mgcnn_apply_matches_oracles(ctx):
     pc.set(0.75, use_net=True)
     z1 = pc.apply_dev(vt).cpu().numpy()
     A_o = coo_oracle(h.finest)
-    rp = v - A_o.mvmul(z0)
-    sc = np.sqrt(np.mean(rp ** 2))
-    img = (rp[dof] / sc).reshape(1, H, W)
+    q = (v - A_o.mvmul(z0)) / A_o.diag()
+    sc = np.sqrt(np.mean(q ** 2))
+    img = (q[dof] / sc).reshape(1, H, W)
     y = CO.forward(unpack(w), img)[0].reshape(-1)
     corr = np.zeros(n)
     corr[dof] = y * sc * 0.75
