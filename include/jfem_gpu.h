@@ -86,17 +86,54 @@ int jfg_matrix_diag(jfg_mat* m, double* h_diag);
 int jfg_spmv_time(jfg_mat* m, int precision, int iters, double* ms_per_spmv);
 
 /* ---- smoothers ------------------------------------------------------- */
-typedef enum { JFG_SMOOTH_JACOBI = 0, JFG_SMOOTH_RICHARDSON = 1 } jfg_smoother_kind;
+typedef struct jfg_schwarz jfg_schwarz;
+typedef enum { JFG_SMOOTH_JACOBI = 0, JFG_SMOOTH_RICHARDSON = 1, JFG_SMOOTH_SCHWARZ = 2 } jfg_smoother_kind;
 typedef struct {
     int kind;      /* jfg_smoother_kind */
-    int runs;      /* sweeps */
-    double omega;  /* damping */
+    int runs;      /* sweeps (Schwarz: SubspaceCorrection.apply calls) */
+    double omega;  /* damping (Jacobi / Richardson; a Schwarz handle keeps its own) */
+    jfg_schwarz* schwarz;  /* JFG_SMOOTH_SCHWARZ: the decomposition of this level's matrix */
 } jfg_smoother_desc;
 /* x <- smooth(A, rhs, x).  Replaces Smoother.smooth
  * (Core/src/main/java/multigrid/Smoother.java:15) as implemented by
  * JacobiSmoother.smooth (multigrid/JacobiSmoother.java:28-50) and
- * RichardsonSmoother.smooth (multigrid/RichardsonSmoother.java:31-50). */
+ * RichardsonSmoother.smooth (multigrid/RichardsonSmoother.java:31-50) and
+ * SchwarzSmoother.smooth (schwarz/SchwarzSmoother.java:21-43). */
 int jfg_smooth(jfg_mat* A, const jfg_smoother_desc* sm, const double* h_rhs, double* h_x);
+
+/* ---- overlapping Schwarz decompositions -------------------------------- */
+/* Subspace corrections over patches of DOFs with cached dense patch inverses.
+ * Replaces UpFrontSchwarz (schwarz/UpFrontSchwarz.java:11-81) with its
+ * DirectSolver (schwarz/DirectSolver.java:12-38, inverse of R A R^T per
+ * patch, RestrictionMatrix.selectFrom, schwarz/RestrictionMatrix.java:22-43)
+ * and the subspace corrections
+ *   JFG_SCHWARZ_MULTIPLICATIVE  MultiplicativeSubspaceCorrection (schwarz/MultiplicativeSubspaceCorrection.java:29-81)
+ *   JFG_SCHWARZ_COLORED         ColoredMultiplicativeSubspaceCorrection (schwarz/ColoredMultiplicativeSubspaceCorrection.java:33-123)
+ *   JFG_SCHWARZ_ADDITIVE        AdditiveSubspaceCorrection (schwarz/AdditiveSubspaceCorrection.java:22-46)
+ * Patches: patch_dofs[patch_ptr[p] .. patch_ptr[p+1]) (any order; sorted
+ * internally, at most 1024 DOFs).  Colours (JFG_SCHWARZ_COLORED only):
+ * color_patches[color_ptr[c] .. color_ptr[c+1]).  The patch builders
+ * (CartesianUpFrontSchwarz, ColoredCartesianSchwarz, VankaSchwarz) live in the
+ * host package and produce these lists.  JFG_ERR_SINGULAR: a patch matrix is
+ * singular. */
+typedef enum { JFG_SCHWARZ_MULTIPLICATIVE = 0, JFG_SCHWARZ_COLORED = 1, JFG_SCHWARZ_ADDITIVE = 2 } jfg_schwarz_kind;
+int jfg_schwarz_create(jfg_ctx* ctx, jfg_mat* A, int kind, double omega, int npatches, const int64_t* patch_ptr,
+                       const int* patch_dofs, int ncolors, const int* color_ptr, const int* color_patches,
+                       jfg_schwarz** out);
+int jfg_schwarz_free(jfg_schwarz* s);
+/* Largest patch, number of stored inverse entries, colours run as one fused launch. */
+int jfg_schwarz_info(jfg_schwarz* s, int* max_patch, int64_t* inverse_entries, int* independent_colors);
+/* x <- SubspaceCorrection.apply(schwarz, x, rhs) (SubspaceCorrection.java:11-18 and overrides). */
+int jfg_schwarz_apply(jfg_schwarz* s, const double* h_rhs, double* h_x);
+/* out = SubspaceCorrection.solve(schwarz, rhs) = AbstractSchwarz.mvMul (AbstractSchwarz.java:62-66). */
+int jfg_schwarz_solve(jfg_schwarz* s, const double* h_rhs, double* h_out);
+/* x <- SchwarzSmoother.smooth: runs x apply. */
+int jfg_schwarz_smooth(jfg_schwarz* s, int runs, const double* h_rhs, double* h_x);
+int jfg_schwarz_smooth_dev(jfg_schwarz* s, int runs, const double* d_rhs, double* d_x);
+/* Patch p's size, sorted DOFs and row-major inverse (each output may be NULL). */
+int jfg_schwarz_local_inverse(jfg_schwarz* s, int patch, int* m, int* h_dofs, double* h_inv);
+/* Mean milliseconds of one apply (CUDA events). */
+int jfg_schwarz_time(jfg_schwarz* s, int iters, double* ms_apply);
 
 /* ---- geometric multigrid -------------------------------------------- */
 typedef struct {
@@ -140,7 +177,8 @@ typedef enum {
     JFG_PREC_MG = 1,       /* handle = jfg_mg* */
     JFG_PREC_JACOBI = 2,   /* diagonal of A */
     JFG_PREC_MATRIX = 3,   /* handle = jfg_mat* applied as y = M x (e.g. an identity or an inverse) */
-    JFG_PREC_MG_CNN = 4    /* handle = jfg_mgcnn*: FP32 V-cycle followed by the learned smoother */
+    JFG_PREC_MG_CNN = 4,   /* handle = jfg_mgcnn*: FP32 V-cycle followed by the learned smoother */
+    JFG_PREC_SCHWARZ = 5   /* handle = jfg_schwarz*: AbstractSchwarz.mvMul (FP64 solves) */
 } jfg_precond_kind;
 
 typedef enum {

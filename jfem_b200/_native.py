@@ -19,10 +19,11 @@ STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "BREAKDOWN", 3: "NONFINITE", 4: 
 # jfg_solver_kind
 CG, PCG, BICGSTAB, PBICGSTAB, GMRES, PGMRES, GMRES2, FGMRES = range(8)
 # jfg_precond_kind
-PREC_NONE, PREC_MG, PREC_JACOBI, PREC_MATRIX, PREC_MG_CNN = range(5)
+PREC_NONE, PREC_MG, PREC_JACOBI, PREC_MATRIX, PREC_MG_CNN, PREC_SCHWARZ = range(6)
 # jfg_precision
 FP64, MIXED, MIXED_PRECOND = 0, 1, 2
-SMOOTH_JACOBI, SMOOTH_RICHARDSON = 0, 1
+SMOOTH_JACOBI, SMOOTH_RICHARDSON, SMOOTH_SCHWARZ = 0, 1, 2
+SCHWARZ_MULTIPLICATIVE, SCHWARZ_COLORED, SCHWARZ_ADDITIVE = 0, 1, 2
 
 # Every symbol include/jfem_gpu.h declares.
 EXPORTED = [
@@ -37,11 +38,13 @@ EXPORTED = [
     "jfg_cnn_num_params", "jfg_cnn_create", "jfg_cnn_free", "jfg_cnn_set_weights", "jfg_cnn_get_weights",
     "jfg_cnn_forward_dev", "jfg_cnn_loss_grad_dev", "jfg_cnn_adam_step", "jfg_cnn_time_forward",
     "jfg_mgcnn_create", "jfg_mgcnn_set", "jfg_mgcnn_apply_dev", "jfg_mgcnn_free",
+    "jfg_schwarz_create", "jfg_schwarz_free", "jfg_schwarz_info", "jfg_schwarz_apply", "jfg_schwarz_solve",
+    "jfg_schwarz_smooth", "jfg_schwarz_smooth_dev", "jfg_schwarz_local_inverse", "jfg_schwarz_time",
 ]
 
 
 class SmootherDesc(C.Structure):
-    _fields_ = [("kind", C.c_int), ("runs", C.c_int), ("omega", C.c_double)]
+    _fields_ = [("kind", C.c_int), ("runs", C.c_int), ("omega", C.c_double), ("schwarz", C.c_void_p)]
 
 
 class MGDesc(C.Structure):
@@ -146,6 +149,16 @@ def load():
     L.jfg_mgcnn_set.argtypes = [_P, C.c_double, C.c_int]
     L.jfg_mgcnn_apply_dev.argtypes = [_P, _P, _P]
     L.jfg_mgcnn_free.argtypes = [_P]
+    L.jfg_schwarz_create.argtypes = [_P, _P, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_int64), _I, C.c_int, _I,
+                                     _I, C.POINTER(_P)]
+    L.jfg_schwarz_free.argtypes = [_P]
+    L.jfg_schwarz_info.argtypes = [_P, _I, C.POINTER(C.c_int64), _I]
+    L.jfg_schwarz_apply.argtypes = [_P, _D, _D]
+    L.jfg_schwarz_solve.argtypes = [_P, _D, _D]
+    L.jfg_schwarz_smooth.argtypes = [_P, C.c_int, _D, _D]
+    L.jfg_schwarz_smooth_dev.argtypes = [_P, C.c_int, _P, _P]
+    L.jfg_schwarz_local_inverse.argtypes = [_P, C.c_int, _I, _I, _D]
+    L.jfg_schwarz_time.argtypes = [_P, C.c_int, _D]
     _lib = L
     return L
 

@@ -5,6 +5,7 @@
 #include <memory>
 
 #include "jfg_krylov.cuh"
+#include "jfg_schwarz.cuh"
 
 struct jfg_ctx {
     jfg::Context c;
@@ -22,6 +23,7 @@ namespace jfg {
 cudaStream_t ctx_stream(jfg_ctx* ctx) { return ctx->c.stream; }
 int ctx_device(jfg_ctx* ctx) { return ctx->c.device; }
 void ctx_set_error(jfg_ctx* ctx, const std::string& msg) { ctx->c.last_error = msg; }
+Context* ctx_context(jfg_ctx* ctx) { return &ctx->c; }
 Matrix* mat_of(jfg_mat* m) { return m->m; }
 jfg_ctx* mat_ctx(jfg_mat* m) { return m->ctx; }
 }  // namespace jfg
@@ -305,7 +307,10 @@ int jfg_spmv_time(jfg_mat* m, int precision, int iters, double* ms)
 int jfg_smooth(jfg_mat* A, const jfg_smoother_desc* sm, const double* rhs, double* x)
 {
     if (!A || !sm || A->m->rows != A->m->cols || sm->runs < 0) return JFG_ERR_BAD_ARG;
-    if (sm->kind != JFG_SMOOTH_JACOBI && sm->kind != JFG_SMOOTH_RICHARDSON) return JFG_ERR_BAD_ARG;
+    if (sm->kind != JFG_SMOOTH_JACOBI && sm->kind != JFG_SMOOTH_RICHARDSON && sm->kind != JFG_SMOOTH_SCHWARZ)
+        return JFG_ERR_BAD_ARG;
+    if (sm->kind == JFG_SMOOTH_SCHWARZ && (!sm->schwarz || jfg::schwarz_of(sm->schwarz)->n != A->m->rows))
+        return JFG_ERR_BAD_ARG;
     jfg_ctx* ctx = A->ctx;
     return guard(ctx, [&]() -> int {
         int n = A->m->rows;
@@ -315,6 +320,7 @@ int jfg_smooth(jfg_mat* A, const jfg_smoother_desc* sm, const double* rhs, doubl
         d.kind = sm->kind;
         d.runs = sm->runs;
         d.omega = sm->omega;
+        d.schwarz = jfg::schwarz_of(sm->schwarz);
         jfg::Scratch sc = ctx_scratch(ctx, A->m->nblocks);
         jfg::smooth_standalone(&ctx->c, A->m, d, ctx->stage_a.p, ctx->stage_b.p, sc);
         stage_out(ctx, ctx->stage_b.p, x, n);
@@ -349,12 +355,18 @@ int jfg_mg_create(jfg_ctx* ctx, int levels, jfg_mat* const* A, jfg_mat* const* P
                 g->bdry.emplace_back(bdry[l] ? std::vector<int>(bdry[l], bdry[l] + n_bdry[l]) : std::vector<int>());
                 jfg::SmootherDesc d;
                 if (l >= 1) {
-                    JFG_CHECK(sm[l].kind == JFG_SMOOTH_JACOBI || sm[l].kind == JFG_SMOOTH_RICHARDSON, JFG_ERR_BAD_ARG,
-                              "unknown smoother kind");
+                    JFG_CHECK(sm[l].kind == JFG_SMOOTH_JACOBI || sm[l].kind == JFG_SMOOTH_RICHARDSON ||
+                                  sm[l].kind == JFG_SMOOTH_SCHWARZ,
+                              JFG_ERR_BAD_ARG, "unknown smoother kind");
                     JFG_CHECK(sm[l].runs >= 0, JFG_ERR_BAD_ARG, "negative smoother runs");
                     d.kind = sm[l].kind;
                     d.runs = sm[l].runs;
                     d.omega = sm[l].omega;
+                    if (d.kind == JFG_SMOOTH_SCHWARZ) {
+                        d.schwarz = jfg::schwarz_of(sm[l].schwarz);
+                        JFG_CHECK(d.schwarz && d.schwarz->A == A[l]->m, JFG_ERR_BAD_ARG,
+                                  "Schwarz smoother built on another matrix than its level");
+                    }
                 }
                 g->sm.push_back(d);
             }
@@ -461,7 +473,9 @@ static int solve_impl(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, cons
     Matrix* M = A->m;
     JFG_CHECK(M->rows == M->cols, JFG_ERR_BAD_ARG, "matrix is not square");
     JFG_CHECK(kind >= JFG_CG && kind <= JFG_FGMRES, JFG_ERR_BAD_ARG, "unknown solver kind");
-    JFG_CHECK(pk >= JFG_PREC_NONE && pk <= JFG_PREC_MG_CNN, JFG_ERR_BAD_ARG, "unknown preconditioner kind");
+    JFG_CHECK(pk >= JFG_PREC_NONE && pk <= JFG_PREC_SCHWARZ, JFG_ERR_BAD_ARG, "unknown preconditioner kind");
+    JFG_CHECK(pk != JFG_PREC_SCHWARZ || o->precision == JFG_FP64, JFG_ERR_UNSUPPORTED,
+              "the Schwarz preconditioner runs in FP64");
     JFG_CHECK(pk != JFG_PREC_MG_CNN || kind == JFG_FGMRES, JFG_ERR_UNSUPPORTED,
               "the multigrid + network preconditioner is nonlinear: use FGMRES");
     bool needs_prec = kind == JFG_PCG || kind == JFG_PBICGSTAB || kind == JFG_PGMRES;
@@ -487,6 +501,7 @@ static int solve_impl(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, cons
     if (pm) mb = std::max(mb, pm->m->nblocks);
     Precond<double> P64;
     if (pk == JFG_PREC_MG_CNN) mb = std::max(mb, mgcnn_precond(ph, P64, n));
+    if (pk == JFG_PREC_SCHWARZ) mb = std::max(mb, schwarz_precond(ph, P64, n));
     int hcap = o->h_history ? std::max(o->history_cap, 1) : 1;
     w.ensure(n, mb, hcap);
     cudaStream_t st = ctx->c.stream;

@@ -81,5 +81,7 @@ uint64_t next_uid();
 // Fills P with the multigrid + learned-smoother hook of a jfg_mgcnn handle
 // (defined with the network kernels); returns its largest grid.
 int mgcnn_precond(void* handle, Precond<double>& P, int n);
+// The same for a jfg_schwarz handle (AbstractSchwarz.mvMul); defined with the Schwarz kernels.
+int schwarz_precond(void* handle, Precond<double>& P, int n);
 
 }  // namespace jfg

@@ -2,6 +2,7 @@
 #include <algorithm>
 
 #include "jfg_mg.cuh"
+#include "jfg_schwarz.cuh"
 
 namespace jfg {
 
@@ -302,6 +303,10 @@ void MGImpl<T>::smooth(int l, const T* rhs, bool xzero, const Scratch& sc, const
             std::swap(cur, alt);
         }
         if (cur != x[l].p) vec_launch<0>(st, m, VCopy<T>{cur, x[l].p}, sc, done);
+    } else if (d.kind == JFG_SMOOTH_SCHWARZ) {
+        // SchwarzSmoother.smooth (schwarz/SchwarzSmoother.java:21-43)
+        if (xzero) vec_launch<0>(st, m, VZero<T>{x[l].p}, sc, done);
+        d.schwarz->smooth<T>(d.runs, rhs, x[l].p, sc, done, st);
     } else {
         if (xzero) vec_launch<0>(st, m, VZero<T>{x[l].p}, sc, done);
         for (int k = 0; k < d.runs; k++) {
@@ -419,6 +424,11 @@ void smooth_standalone(Context* c, Matrix* A, const SmootherDesc& d, const doubl
 {
     cudaStream_t st = c->stream;
     int m = A->rows;
+    if (d.kind == JFG_SMOOTH_SCHWARZ) {
+        d.schwarz->smooth<double>(d.runs, rhs, xv, sc, nullptr, st);
+        JFG_CUDA(cudaStreamSynchronize(st));
+        return;
+    }
     DevBuf<double> dinv, t, r;
     DevBuf<int> flag;
     dinv.alloc(m);

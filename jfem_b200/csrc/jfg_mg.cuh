@@ -6,10 +6,13 @@
 
 namespace jfg {
 
+struct SchwarzImpl;
+
 struct SmootherDesc {
     int kind = JFG_SMOOTH_JACOBI;
     int runs = 2;
     double omega = 2.0 / 3.0;
+    SchwarzImpl* schwarz = nullptr;   // JFG_SMOOTH_SCHWARZ
 };
 
 // The hierarchy of MGPreconditionerSpace / MGPreconditionerInterface

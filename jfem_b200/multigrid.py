@@ -67,6 +67,7 @@ class MGPreconditioner(VectorMultiplyable):
             sm = [None] + sm
         if len(sm) != L:
             raise IllegalArgumentException("one smoother per level above the coarsest")
+        self._smoothers = sm        # Schwarz smoothers own device data the hierarchy points to
         descs = (N.SmootherDesc * L)()
         for l, s in enumerate(sm):
             if s is not None:

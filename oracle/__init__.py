@@ -78,6 +78,17 @@ def lib():
         L.or_op_mg.argtypes = [_P, C.c_int, C.c_int]
         L.or_op_mg_free.argtypes = [_P]
         L.or_mg_coarse_status.argtypes = [_P]
+        L.or_mg_set_schwarz.argtypes = [_P, C.c_int, _P, C.c_int]
+        L.or_schwarz_new.restype = _P
+        L.or_schwarz_new.argtypes = [_P, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_longlong), _I, C.c_int, _I,
+                                     _I]
+        L.or_schwarz_status.argtypes = [_P]
+        L.or_schwarz_free.argtypes = [_P]
+        L.or_schwarz_apply.argtypes = [_P, _D, _D]
+        L.or_schwarz_solve.argtypes = [_P, _D, _D]
+        L.or_schwarz_smooth.argtypes = [_P, C.c_int, _D, _D]
+        L.or_schwarz_inverse.restype = _D
+        L.or_schwarz_inverse.argtypes = [_P, C.c_int, _I]
         _lib = L
     return _lib
 
@@ -314,3 +325,63 @@ class MGPreconditioner:
         out = np.empty(self.n)
         lib().or_op_apply(self._op, _d(_f64(v)), _d(out))
         return out
+
+    def set_schwarz(self, level: int, schwarz: "Schwarz", runs: int):
+        """Level ``level`` smooths with SchwarzSmoother(runs, schwarz)."""
+        self._keep = getattr(self, "_keep", []) + [schwarz]
+        lib().or_mg_set_schwarz(self._h, level, schwarz._h, runs)
+
+
+SCHWARZ_MULTIPLICATIVE, SCHWARZ_COLORED, SCHWARZ_ADDITIVE = 0, 1, 2
+
+
+class Schwarz:
+    """UpFrontSchwarz + DirectSolver + one SubspaceCorrection over explicit
+    patch DOF lists (and colours for the coloured correction)."""
+
+    def __init__(self, A: CooMatrix, kind: int, patches, omega: float = 1.0, colours=None):
+        self.A = A
+        self.n = A.rows
+        ptr = np.zeros(len(patches) + 1, dtype=np.int64)
+        ptr[1:] = np.cumsum([len(p) for p in patches])
+        dofs = np.ascontiguousarray(np.concatenate([np.asarray(p, dtype=np.int32) for p in patches]),
+                                    dtype=np.int32)
+        if colours is None:
+            colours = []
+        cptr = np.zeros(len(colours) + 1, dtype=np.int32)
+        cptr[1:] = np.cumsum([len(c) for c in colours]) if colours else []
+        cpat = np.ascontiguousarray(np.concatenate([np.asarray(c, dtype=np.int32) for c in colours])
+                                    if colours else np.zeros(1, dtype=np.int32), dtype=np.int32)
+        self._h = lib().or_schwarz_new(A._h, kind, omega, len(patches), ptr.ctypes.data_as(C.POINTER(C.c_longlong)),
+                                       _i(dofs), len(colours), _i(cptr), _i(cpat))
+        if lib().or_schwarz_status(self._h) != OK:
+            lib().or_schwarz_free(self._h)
+            self._h = None
+            raise np.linalg.LinAlgError("singular patch matrix")
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().or_schwarz_free(self._h)
+        except Exception:
+            pass
+
+    def apply(self, x, rhs):
+        x = _f64(x).copy()
+        lib().or_schwarz_apply(self._h, _d(x), _d(_f64(rhs)))
+        return x
+
+    def solve(self, rhs):
+        out = np.empty(self.n)
+        lib().or_schwarz_solve(self._h, _d(_f64(rhs)), _d(out))
+        return out
+
+    def smooth(self, runs, rhs, x):
+        x = _f64(x).copy()
+        lib().or_schwarz_smooth(self._h, runs, _d(_f64(rhs)), _d(x))
+        return x
+
+    def inverse(self, p):
+        m = C.c_int()
+        ptr = lib().or_schwarz_inverse(self._h, p, C.byref(m))
+        return np.ctypeslib.as_array(ptr, shape=(m.value * m.value,)).reshape(m.value, m.value).copy()

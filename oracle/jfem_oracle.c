@@ -801,15 +801,216 @@ int or_solve_gmres2(const or_op* A, const or_op* M, const double* b, double* x, 
 }
 
 /* ------------------------------------------------------------------ */
+/* Schwarz subspace corrections (schwarz/*.java)                        */
+/* ------------------------------------------------------------------ */
+#define OR_SCHWARZ_MULT 0
+#define OR_SCHWARZ_COLORED 1
+#define OR_SCHWARZ_ADDITIVE 2
+
+typedef struct or_schwarz {
+    const or_mat* A;
+    int n, kind, np, nc;
+    double omega;
+    long long* pptr; int* dofs;       /* patch DOF lists, ascending (TreeSet by global index) */
+    int* cptr; int* cpat;             /* colours: ascending patch lists (IntRBTreeSet) */
+    double** inv;                     /* DirectSolver cache: dense inverse of R A R^T per patch */
+    int status;
+} or_schwarz;
+
+static int cmp_int(const void* a, const void* b)
+{
+    int x = *(const int*)a, y = *(const int*)b;
+    return (x > y) - (x < y);
+}
+
+/* UpFrontSchwarz.build (UpFrontSchwarz.java:25-59) with
+ * RestrictionMatrix.selectFrom (RestrictionMatrix.java:22-43): the local
+ * operator keeps the merged entries whose row and column both lie in the
+ * patch; DirectSolver.solve (DirectSolver.java:22-38) caches its inverse. */
+or_schwarz* or_schwarz_new(const or_mat* A, int kind, double omega, int np, const long long* pptr,
+                           const int* dofs, int nc, const int* cptr, const int* cpat)
+{
+    or_schwarz* S = (or_schwarz*)calloc(1, sizeof(or_schwarz));
+    S->A = A; S->n = A->rows; S->kind = kind; S->omega = omega; S->np = np; S->nc = nc;
+    S->pptr = (long long*)malloc(sizeof(long long) * (np + 1));
+    memcpy(S->pptr, pptr, sizeof(long long) * (np + 1));
+    S->dofs = (int*)malloc(sizeof(int) * (pptr[np] ? pptr[np] : 1));
+    memcpy(S->dofs, dofs, sizeof(int) * pptr[np]);
+    for (int p = 0; p < np; p++)
+        qsort(S->dofs + pptr[p], (size_t)(pptr[p + 1] - pptr[p]), sizeof(int), cmp_int);
+    if (kind == OR_SCHWARZ_COLORED) {
+        S->cptr = (int*)malloc(sizeof(int) * (nc + 1));
+        memcpy(S->cptr, cptr, sizeof(int) * (nc + 1));
+        S->cpat = (int*)malloc(sizeof(int) * (cptr[nc] ? cptr[nc] : 1));
+        memcpy(S->cpat, cpat, sizeof(int) * cptr[nc]);
+        for (int c = 0; c < nc; c++) qsort(S->cpat + cptr[c], (size_t)(cptr[c + 1] - cptr[c]), sizeof(int), cmp_int);
+    }
+    S->inv = (double**)calloc(np, sizeof(double*));
+    int* loc = (int*)malloc(sizeof(int) * (S->n ? S->n : 1));
+    for (int i = 0; i < S->n; i++) loc[i] = -1;
+    for (int p = 0; p < np && S->status == OR_OK; p++) {
+        int m = (int)(pptr[p + 1] - pptr[p]);
+        const int* d = S->dofs + pptr[p];
+        for (int i = 0; i < m; i++) loc[d[i]] = i;
+        double* a = (double*)calloc((size_t)m * m, sizeof(double));
+        for (int i = 0; i < m; i++) {
+            int g = d[i];
+            for (long long k = A->rp[g]; k < A->rp[g + 1]; k++) {
+                int j = loc[A->rc[k]];
+                if (j >= 0) a[(size_t)i * m + j] += A->rv[k];
+            }
+        }
+        S->inv[p] = (double*)malloc(sizeof(double) * (size_t)m * m);
+        if (or_dense_inverse(m, a, S->inv[p]) != OR_OK) S->status = OR_SINGULAR;
+        free(a);
+        for (int i = 0; i < m; i++) loc[d[i]] = -1;
+    }
+    free(loc);
+    return S;
+}
+
+int or_schwarz_status(const or_schwarz* S) { return S->status; }
+
+void or_schwarz_free(or_schwarz* S)
+{
+    if (!S) return;
+    for (int p = 0; p < S->np; p++) free(S->inv[p]);
+    free(S->inv); free(S->pptr); free(S->dofs); free(S->cptr); free(S->cpat);
+    free(S);
+}
+
+/* getGlobalVector(p, solveLocalSystem(p, getLocalVector(p, r))) as a dense
+ * global vector comp (zero outside the patch). */
+static void patch_component(const or_schwarz* S, int p, const double* r, double* comp)
+{
+    int m = (int)(S->pptr[p + 1] - S->pptr[p]);
+    const int* d = S->dofs + S->pptr[p];
+    double* loc = vnew(m);
+    for (int i = 0; i < m; i++) loc[i] = r[d[i]];
+    memset(comp, 0, sizeof(double) * S->n);
+    const double* iv = S->inv[p];
+    for (int i = 0; i < m; i++) {
+        double acc = 0;
+        for (int j = 0; j < m; j++) acc += iv[(size_t)i * m + j] * loc[j];
+        comp[d[i]] = acc;
+    }
+    free(loc);
+}
+
+static void residual(const or_schwarz* S, const double* rhs, const double* x, double* r)
+{
+    or_mat_mvmul(S->A, x, r);
+    for (int i = 0; i < S->n; i++) r[i] = rhs[i] - r[i];
+}
+
+/* MultiplicativeSubspaceCorrection.upgradePatch (:61-81) and
+ * ColoredMultiplicativeSubspaceCorrection.colorSetUpgrade (:84-123). */
+static void colour_upgrade(const or_schwarz* S, const int* patches, int count, double om, const double* rhs,
+                           double* x, double* r, double* comp)
+{
+    residual(S, rhs, x, r);
+    double** comps = (double**)malloc(sizeof(double*) * (count ? count : 1));
+    for (int q = 0; q < count; q++) {
+        comps[q] = vnew(S->n);
+        patch_component(S, patches[q], r, comps[q]);
+    }
+    for (int q = 0; q < count; q++) {
+        for (int i = 0; i < S->n; i++) x[i] = x[i] + comps[q][i] * om;
+        free(comps[q]);
+    }
+    free(comps);
+    (void)comp;
+}
+
+/* SubspaceCorrection.apply: x <- new iterate. */
+void or_schwarz_apply(const or_schwarz* S, double* x, const double* rhs)
+{
+    int n = S->n;
+    double* r = vnew(n);
+    double* comp = vnew(n);
+    if (S->kind == OR_SCHWARZ_MULT) {           /* MultiplicativeSubspaceCorrection.apply (:46-59) */
+        for (int p = 0; p < S->np; p++) {
+            residual(S, rhs, x, r);
+            patch_component(S, p, r, comp);
+            for (int i = 0; i < n; i++) x[i] = x[i] + comp[i];
+        }
+        for (int p = S->np - 1; p >= 0; p--) {
+            residual(S, rhs, x, r);
+            patch_component(S, p, r, comp);
+            for (int i = 0; i < n; i++) x[i] = x[i] + comp[i];
+        }
+    } else if (S->kind == OR_SCHWARZ_COLORED) { /* ColoredMultiplicativeSubspaceCorrection.apply (:68-82) */
+        for (int c = 0; c < S->nc; c++)
+            colour_upgrade(S, S->cpat + S->cptr[c], S->cptr[c + 1] - S->cptr[c], S->omega, rhs, x, r, comp);
+        for (int c = S->nc - 1; c >= 0; c--)
+            colour_upgrade(S, S->cpat + S->cptr[c], S->cptr[c + 1] - S->cptr[c], S->omega, rhs, x, r, comp);
+    } else {                                    /* SubspaceCorrection.apply default (:11-18) */
+        residual(S, rhs, x, r);
+        double* sol = vnew(n);
+        for (int p = 0; p < S->np; p++) {       /* AdditiveSubspaceCorrection.solve (:22-46) */
+            patch_component(S, p, r, comp);
+            for (int i = 0; i < n; i++) sol[i] = sol[i] + comp[i] * S->omega;
+        }
+        for (int i = 0; i < n; i++) x[i] = x[i] + sol[i];
+        free(sol);
+    }
+    free(r); free(comp);
+}
+
+/* SubspaceCorrection.solve = AbstractSchwarz.mvMul. */
+void or_schwarz_solve(const or_schwarz* S, const double* rhs, double* out)
+{
+    int n = S->n;
+    double* r = vnew(n);
+    double* comp = vnew(n);
+    memset(out, 0, sizeof(double) * n);
+    if (S->kind == OR_SCHWARZ_ADDITIVE) {
+        for (int p = 0; p < S->np; p++) {
+            patch_component(S, p, rhs, comp);
+            for (int i = 0; i < n; i++) out[i] = out[i] + comp[i] * S->omega;
+        }
+    } else {
+        patch_component(S, 0, rhs, out);        /* the first patch alone (:32-35 of both) */
+        if (S->kind == OR_SCHWARZ_MULT) {
+            for (int p = 1; p < S->np; p++) {
+                residual(S, rhs, out, r);
+                patch_component(S, p, r, comp);
+                for (int i = 0; i < n; i++) out[i] = out[i] + comp[i];
+            }
+        } else {
+            for (int c = 0; c < S->nc; c++)
+                colour_upgrade(S, S->cpat + S->cptr[c], S->cptr[c + 1] - S->cptr[c], S->omega, rhs, out, r, comp);
+        }
+    }
+    free(r); free(comp);
+}
+
+/* SchwarzSmoother.smooth (SchwarzSmoother.java:21-43). */
+void or_schwarz_smooth(const or_schwarz* S, int runs, const double* rhs, double* x)
+{
+    for (int i = 0; i < runs; i++) or_schwarz_apply(S, x, rhs);
+}
+
+/* the cached inverse of patch p (m*m, row-major) */
+const double* or_schwarz_inverse(const or_schwarz* S, int p, int* m)
+{
+    *m = (int)(S->pptr[p + 1] - S->pptr[p]);
+    return S->inv[p];
+}
+
+/* ------------------------------------------------------------------ */
 /* smoothers                                                            */
 /* ------------------------------------------------------------------ */
 #define OR_SMOOTH_JACOBI 0
 #define OR_SMOOTH_RICHARDSON 1
 
+#define OR_SMOOTH_SCHWARZ 2
+
 typedef struct {
     int kind, runs;
     double omega;
     double* dinv;      /* Jacobi: 1/diag with |d| < 1e-10 -> 1 (JacobiSmoother.java:16-24) */
+    const or_schwarz* schwarz;   /* SchwarzSmoother: its own decomposition and global operator */
 } or_smoother;
 
 /* JacobiSmoother.smooth (JacobiSmoother.java:28-50) and RichardsonSmoother.smooth
@@ -817,6 +1018,10 @@ typedef struct {
 static void smooth(const or_smoother* s, const or_mat* A, const double* rhs, double* x, double* r)
 {
     int n = A->rows;
+    if (s->kind == OR_SMOOTH_SCHWARZ) {
+        or_schwarz_smooth(s->schwarz, s->runs, rhs, x);
+        return;
+    }
     for (int it = 0; it < s->runs; it++) {
         or_mat_mvmul(A, x, r);
         for (int i = 0; i < n; i++) r[i] = rhs[i] - r[i];
@@ -831,7 +1036,7 @@ static void smooth(const or_smoother* s, const or_mat* A, const double* rhs, dou
 
 static void smoother_init(or_smoother* s, int kind, int runs, double omega, const or_mat* A)
 {
-    s->kind = kind; s->runs = runs; s->omega = omega; s->dinv = NULL;
+    s->kind = kind; s->runs = runs; s->omega = omega; s->dinv = NULL; s->schwarz = NULL;
     if (kind == OR_SMOOTH_JACOBI) {
         s->dinv = vnew(A->rows);
         or_mat_diag(A, s->dinv);
@@ -913,6 +1118,16 @@ or_mg* or_mg_new(int L, const or_mat** A, const or_mat** P, const int** bd, cons
     g->coarse_status = lu_factor(&g->coarse, n0, dense);
     free(dense);
     return g;
+}
+
+/* Level l smooths with SchwarzSmoother(runs, S). */
+void or_mg_set_schwarz(or_mg* g, int l, const or_schwarz* S, int runs)
+{
+    free(g->sm[l].dinv);
+    g->sm[l].dinv = NULL;
+    g->sm[l].kind = OR_SMOOTH_SCHWARZ;
+    g->sm[l].runs = runs;
+    g->sm[l].schwarz = S;
 }
 
 void or_mg_free(or_mg* g)

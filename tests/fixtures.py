@@ -57,3 +57,22 @@ def coo_oracle(sy):
 
 def mg_levels(p, coarse, L, mass=5.0, modes=4, seed=0):
     return problems.hierarchy(p, coarse, L, mass, modes, seed)
+
+
+def schwarz_test_matrix(n):
+    """CartesianSchwarzTest.createSparseMatrix (CartesianSchwarzTest.java:20-33):
+    over the n x n shape range a draw < 0.4 adds (int)(10 u - 5), every
+    diagonal entry gets 15, and the result is A + A^T (dense float64)."""
+    u = O.java_random_doubles(14239078, 2 * n * n)
+    a = np.zeros((n, n))
+    k = 0
+    for r in range(n):
+        for c in range(n):
+            d = u[k]
+            k += 1
+            if d < 0.4:
+                a[r, c] += float(int(10 * u[k] - 5))
+                k += 1
+            if r == c:
+                a[r, c] += 15.0
+    return a + a.T
