@@ -2,16 +2,17 @@
 (Q1, kappa = exp(g), g a Gaussian random field).  No counterpart in the
 reference (JFEM has no neural-network code).
 
-Training pairs are made on the GPU from independently seeded kappa fields:
+Training data are made on the GPU from independently seeded kappa fields:
 
     v        a random vector of mixed spectrum (zero on Dirichlet nodes, unit norm)
     r'       = v - A V(v)                 the residual left by one FP32 V-cycle
     q        = D^-1 r',  s = rms(q)       the network input is q / s
-    e'       = A^-1 r'                    (FP64 PCG with the same hierarchy)
-    target   = e' / s
 
-so that V(v) + s * net(q / s) approximates A^-1 v; random square crops of the
-node grid form the training images.  The trained network is used by
+The default loss is the residual left after the network's correction,
+||r' - A s net(q / s)||^2 on the full node grid, so the network learns a
+local smoother for what the V-cycle leaves behind.  The alternative loss
+fits e' / s with e' = A^-1 r' (FP64 PCG with the same hierarchy) on random
+square crops.  The trained network is used by
 MGCNNPreconditioner inside FGMRES(30) and compared with plain FP64 GMG-PCG.
 
 Command line:
@@ -126,9 +127,59 @@ def make_pairs(ks: KappaSystem, count: int, crops: int, crop: int, gen: torch.Ge
     return X, T
 
 
+def make_residuals(ks: KappaSystem, count: int, gen: torch.Generator, net):
+    """count (network input, residual, scale) triples on the full node grid:
+    q / s as (count, H, W) float32, r' as (count, n) float64, s as (count,)."""
+    pc = ks.preconditioner(net, use_net=False)
+    X = torch.empty(count, ks.H, ks.W, dtype=torch.float32, device="cuda")
+    RP = torch.empty(count, ks.n, dtype=torch.float64, device="cuda")
+    S = torch.empty(count, dtype=torch.float64, device="cuda")
+    vs = random_vectors(ks, count, gen)
+    for i in range(count):
+        v = vs[i].contiguous()
+        rp = v - ks.A.spmv_dev(pc.apply_dev(v))
+        q = rp / ks.diag_t
+        s = torch.sqrt(torch.mean(q * q))
+        X[i] = (q[ks.dof_t] / s).reshape(ks.H, ks.W).float()
+        RP[i] = rp
+        S[i] = s
+    return X, RP, S
+
+
+def residual_step(net, A, dof_t, bd_t, X, RP, S, lr):
+    """One Adam step on L = sum_b ||r'_b - A z_b||^2 / (B n) with
+    z_b = s_b * scatter(net(x_b)) (zero on Dirichlet nodes).  The network
+    kernels train on mean((y - t)^2); the pseudo-target
+    t = y - dL/dy * (B H W) / 2 gives them exactly dL/dy.  Returns
+    sum ||r' - A z||^2 / sum ||r'||^2."""
+    B, H, W = X.shape
+    n = RP.shape[1]
+    y = net.forward(X)
+    z = torch.zeros(B, n, dtype=torch.float64, device="cuda")
+    z[:, dof_t] = y.reshape(B, -1).double() * S[:, None]
+    z[:, bd_t] = 0.0
+    g = torch.empty_like(z)
+    num = den = 0.0
+    for b in range(B):
+        res = RP[b] - A.spmv_dev(z[b].contiguous())
+        num += float((res * res).sum())
+        den += float((RP[b] * RP[b]).sum())
+        g[b] = A.spmv_t_dev(res.contiguous()) * (-2.0 / (B * n))
+    g[:, bd_t] = 0.0
+    gy = (g[:, dof_t] * S[:, None]).reshape(B, H, W)
+    t = (y.double() - gy * (B * H * W / 2.0)).float().contiguous()
+    net.train_step(X, t, lr=lr)
+    return num / den
+
+
 def train(ctx, cells=1024, fields=16, pairs=125, crops=4, crop=128, steps=4000, batch=16, lr=1e-3, seed=0,
-          log=print):
-    """Trains from scratch; returns (weights, report)."""
+          log=print, loss="residual"):
+    """Trains from scratch; returns (weights, report).  loss="residual"
+    minimises the residual left after the network's correction on full node
+    grids (batch images of one field per step); loss="error" fits the
+    normalised error e'/s on random crops."""
+    if loss == "residual":
+        return _train_residual(ctx, cells, fields, pairs, steps, min(batch, 4), lr, seed, log)
     gen = torch.Generator(device="cuda")
     gen.manual_seed(seed)
     t0 = time.time()
@@ -159,6 +210,37 @@ def train(ctx, cells=1024, fields=16, pairs=125, crops=4, crop=128, steps=4000, 
     report = {"pairs": fields * pairs, "fields": fields, "crops": int(m), "crop": crop, "steps": steps,
               "batch": batch, "data_s": round(t_data, 1), "train_s": round(t_train, 1),
               "final_loss": float(np.mean(losses[-100:])), "first_loss": float(np.mean(losses[:100]))}
+    return net.get_weights(), report
+
+
+def _train_residual(ctx, cells, fields, pairs, steps, batch, lr, seed, log):
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    t0 = time.time()
+    net = LearnedSmoother(ctx, weights=he_init(seed, gain_last=0.1))
+    sets = []
+    for f in range(fields):
+        ks = KappaSystem(ctx, cells, kseed=1000 + f)
+        X, RP, S = make_residuals(ks, pairs, gen, net)
+        sets.append((ks.A, ks.dof_t, ks.bd_t, X, RP, S))
+        log(f"field {f}: {pairs} residuals, {time.time() - t0:.1f} s")
+        del ks
+    t_data = time.time() - t0
+    t1 = time.time()
+    ratios = []
+    for it in range(steps):
+        f = int(torch.randint(0, fields, (1,), generator=gen, device="cuda").item())
+        A, dof_t, bd_t, X, RP, S = sets[f]
+        idx = torch.randint(0, X.shape[0], (batch,), generator=gen, device="cuda")
+        cur = lr * 0.5 * (1 + math.cos(math.pi * it / steps))
+        ratios.append(residual_step(net, A, dof_t, bd_t, X[idx].contiguous(), RP[idx].contiguous(),
+                                    S[idx].contiguous(), cur))
+        if it % 250 == 0 or it == steps - 1:
+            log(f"step {it}: residual ratio {np.mean(ratios[-50:]):.4f}")
+    t_train = time.time() - t1
+    report = {"loss": "residual", "pairs": fields * pairs, "fields": fields, "grid": [cells + 1, cells + 1],
+              "steps": steps, "batch": batch, "data_s": round(t_data, 1), "train_s": round(t_train, 1),
+              "first_ratio": float(np.mean(ratios[:50])), "final_ratio": float(np.mean(ratios[-50:]))}
     return net.get_weights(), report
 
 
@@ -215,6 +297,7 @@ def main(argv=None):
     t.add_argument("--lr", type=float, default=1e-3)
     t.add_argument("--seed", type=int, default=0)
     t.add_argument("--report", default=None)
+    t.add_argument("--loss", choices=("residual", "error"), default="residual")
     e = sub.add_parser("eval")
     e.add_argument("--weights", default=WEIGHTS)
     e.add_argument("--cells", type=int, default=1024)
@@ -223,7 +306,7 @@ def main(argv=None):
     a = ap.parse_args(argv)
     ctx = N.default_context()
     if a.cmd == "train":
-        w, rep = train(ctx, a.cells, a.fields, a.pairs, a.crops, a.crop, a.steps, a.batch, a.lr, a.seed)
+        w, rep = train(ctx, a.cells, a.fields, a.pairs, a.crops, a.crop, a.steps, a.batch, a.lr, a.seed, loss=a.loss)
         os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
         np.save(a.out, w)
         print(json.dumps(rep))

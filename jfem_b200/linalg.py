@@ -210,6 +210,16 @@ class DeviceMatrix:
         self.ctx.check(N.load().jfg_synchronize(self.ctx.handle))
         return y
 
+    def spmv_t_dev(self, x, y=None):
+        """y = A^T x for contiguous FP64 CUDA tensors (returns when y is written)."""
+        import torch
+        if y is None:
+            y = torch.empty(self.cols, dtype=torch.float64, device=x.device)
+        torch.cuda.synchronize()
+        self.ctx.check(N.load().jfg_spmv_t_dev(self._h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())))
+        self.ctx.check(N.load().jfg_synchronize(self.ctx.handle))
+        return y
+
     def spmv_t(self, x):
         x = N.f64(x)
         y = np.empty(self.cols)

@@ -175,8 +175,8 @@ def test_mg_with_schwarz_smoother(ctx):
 
 
 def test_schwarz_preconditioned_krylov(ctx):
-    sp, sy = fe_system(1, 16)
-    _, patches = cartesian_patch_dofs(sp, (8, 8), 1)
+    sp, sy = fe_system(1, 32, mass=0.0)
+    _, patches = cartesian_patch_dofs(sp, (16, 16), 1)
     S = UpFrontSchwarz(dev(sy, ctx), patches, AdditiveSubspaceCorrection(0.25))
     A = dev(sy, ctx)
     b = sy.rhs
@@ -188,7 +188,7 @@ def test_schwarz_preconditioned_krylov(ctx):
     s2.solveCG(A, b, tol)
     assert s.last.status == N.OK and it_pcg < s2.iterations
     assert np.linalg.norm(b - coo_oracle(sy).mvmul(x)) <= tol * 1.0001
-    Sc = UpFrontSchwarz(A, patches, ColoredMultiplicativeSubspaceCorrection(1.0), colours=nine_colours((8, 8)))
+    Sc = UpFrontSchwarz(A, patches, ColoredMultiplicativeSubspaceCorrection(1.0), colours=nine_colours((16, 16)))
     s3 = IterativeSolver(ctx=ctx)
     x3 = s3.solvePGMRES(A, Sc, b, tol)
     assert s3.last.status == N.OK
