@@ -178,7 +178,8 @@ typedef enum {
     JFG_PREC_JACOBI = 2,   /* diagonal of A */
     JFG_PREC_MATRIX = 3,   /* handle = jfg_mat* applied as y = M x (e.g. an identity or an inverse) */
     JFG_PREC_MG_CNN = 4,   /* handle = jfg_mgcnn*: FP32 V-cycle followed by the learned smoother */
-    JFG_PREC_SCHWARZ = 5   /* handle = jfg_schwarz*: AbstractSchwarz.mvMul (FP64 solves) */
+    JFG_PREC_SCHWARZ = 5,  /* handle = jfg_schwarz*: AbstractSchwarz.mvMul (FP64 solves) */
+    JFG_PREC_BLOCKDIAG = 6 /* handle = jfg_blockdiag*: velocity multigrid + diagonal pressure block */
 } jfg_precond_kind;
 
 typedef enum {
@@ -307,6 +308,19 @@ int jfg_mgcnn_set(jfg_mgcnn* p, double out_scale, int use_net);
 /* z = the preconditioner applied to v (FP64 device vectors of the system size). */
 int jfg_mgcnn_apply_dev(jfg_mgcnn* p, const double* d_v, double* d_z);
 int jfg_mgcnn_free(jfg_mgcnn* p);
+
+/* ---- block-diagonal saddle-point preconditioner ------------------------ */
+/* For systems ordered velocity first (TaylorHoodSpace numbering): z_v = mg
+ * applied to r_v (mg built on the velocity block, nv unknowns; FP32 V-cycle
+ * when fp32_vcycle), z_p = pinv * r_p (np unknowns, e.g. the inverse lumped
+ * pressure mass).  The block-diagonal preconditioner of the Stokes
+ * examples (examples StokesMG / StokesMGBS*: velocity multigrid, pressure
+ * mass scaling).  Pass to jfg_solve with JFG_PREC_BLOCKDIAG. */
+typedef struct jfg_blockdiag jfg_blockdiag;
+int jfg_blockdiag_create(jfg_ctx* ctx, jfg_mg* mg, int nv, int np, const double* h_pinv, int fp32_vcycle,
+                         jfg_blockdiag** out);
+int jfg_blockdiag_apply(jfg_blockdiag* b, const double* h_v, double* h_out);
+int jfg_blockdiag_free(jfg_blockdiag* b);
 
 /* ---- dense direct solves --------------------------------------------- */
 /* x = A^-1 b for a dense row-major n x n A (partial-pivot LU on the GPU).

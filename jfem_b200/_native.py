@@ -19,7 +19,7 @@ STATUS_NAMES = {0: "OK", 1: "NOT_CONVERGED", 2: "BREAKDOWN", 3: "NONFINITE", 4: 
 # jfg_solver_kind
 CG, PCG, BICGSTAB, PBICGSTAB, GMRES, PGMRES, GMRES2, FGMRES = range(8)
 # jfg_precond_kind
-PREC_NONE, PREC_MG, PREC_JACOBI, PREC_MATRIX, PREC_MG_CNN, PREC_SCHWARZ = range(6)
+PREC_NONE, PREC_MG, PREC_JACOBI, PREC_MATRIX, PREC_MG_CNN, PREC_SCHWARZ, PREC_BLOCKDIAG = range(7)
 # jfg_precision
 FP64, MIXED, MIXED_PRECOND = 0, 1, 2
 SMOOTH_JACOBI, SMOOTH_RICHARDSON, SMOOTH_SCHWARZ = 0, 1, 2
@@ -40,6 +40,7 @@ EXPORTED = [
     "jfg_mgcnn_create", "jfg_mgcnn_set", "jfg_mgcnn_apply_dev", "jfg_mgcnn_free",
     "jfg_schwarz_create", "jfg_schwarz_free", "jfg_schwarz_info", "jfg_schwarz_apply", "jfg_schwarz_solve",
     "jfg_schwarz_smooth", "jfg_schwarz_smooth_dev", "jfg_schwarz_local_inverse", "jfg_schwarz_time",
+    "jfg_blockdiag_create", "jfg_blockdiag_apply", "jfg_blockdiag_free",
 ]
 
 
@@ -159,6 +160,9 @@ def load():
     L.jfg_schwarz_smooth_dev.argtypes = [_P, C.c_int, _P, _P]
     L.jfg_schwarz_local_inverse.argtypes = [_P, C.c_int, _I, _I, _D]
     L.jfg_schwarz_time.argtypes = [_P, C.c_int, _D]
+    L.jfg_blockdiag_create.argtypes = [_P, _P, C.c_int, C.c_int, _D, C.c_int, C.POINTER(_P)]
+    L.jfg_blockdiag_apply.argtypes = [_P, _D, _D]
+    L.jfg_blockdiag_free.argtypes = [_P]
     _lib = L
     return L
 

@@ -9,7 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libjfem_gpu.so")
 SOURCES = ["jfg_matrix.cu", "jfg_mg.cu", "jfg_dense.cu", "jfg_krylov.cu", "jfg_api.cu", "jfg_noalloc.cu",
-           "jfg_batch.cu", "jfg_cnn.cu", "jfg_schwarz.cu"]
+           "jfg_batch.cu", "jfg_cnn.cu", "jfg_schwarz.cu", "jfg_block.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-lineinfo",
          "-Xcompiler", "-fPIC", "-shared"]

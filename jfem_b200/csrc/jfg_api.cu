@@ -473,9 +473,9 @@ static int solve_impl(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, cons
     Matrix* M = A->m;
     JFG_CHECK(M->rows == M->cols, JFG_ERR_BAD_ARG, "matrix is not square");
     JFG_CHECK(kind >= JFG_CG && kind <= JFG_FGMRES, JFG_ERR_BAD_ARG, "unknown solver kind");
-    JFG_CHECK(pk >= JFG_PREC_NONE && pk <= JFG_PREC_SCHWARZ, JFG_ERR_BAD_ARG, "unknown preconditioner kind");
-    JFG_CHECK(pk != JFG_PREC_SCHWARZ || o->precision == JFG_FP64, JFG_ERR_UNSUPPORTED,
-              "the Schwarz preconditioner runs in FP64");
+    JFG_CHECK(pk >= JFG_PREC_NONE && pk <= JFG_PREC_BLOCKDIAG, JFG_ERR_BAD_ARG, "unknown preconditioner kind");
+    JFG_CHECK((pk != JFG_PREC_SCHWARZ && pk != JFG_PREC_BLOCKDIAG) || o->precision == JFG_FP64, JFG_ERR_UNSUPPORTED,
+              "this preconditioner takes its own precision: solve with precision FP64");
     JFG_CHECK(pk != JFG_PREC_MG_CNN || kind == JFG_FGMRES, JFG_ERR_UNSUPPORTED,
               "the multigrid + network preconditioner is nonlinear: use FGMRES");
     bool needs_prec = kind == JFG_PCG || kind == JFG_PBICGSTAB || kind == JFG_PGMRES;
@@ -502,6 +502,7 @@ static int solve_impl(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, cons
     Precond<double> P64;
     if (pk == JFG_PREC_MG_CNN) mb = std::max(mb, mgcnn_precond(ph, P64, n));
     if (pk == JFG_PREC_SCHWARZ) mb = std::max(mb, schwarz_precond(ph, P64, n));
+    if (pk == JFG_PREC_BLOCKDIAG) mb = std::max(mb, blockdiag_precond(ph, P64, n));
     int hcap = o->h_history ? std::max(o->history_cap, 1) : 1;
     w.ensure(n, mb, hcap);
     cudaStream_t st = ctx->c.stream;

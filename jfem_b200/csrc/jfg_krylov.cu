@@ -474,6 +474,10 @@ inline int vec_grid_n(int n) { return vec_grid(n); }
 template <typename T>
 void Precond<T>::apply(const T* r, T* z, const Scratch& sc, const int* done, cudaStream_t st) const
 {
+    if (hook) {     // multigrid + network, Schwarz, block-diagonal
+        hook(hook_self, r, z, sc, done, st);
+        return;
+    }
     switch (kind) {
     case JFG_PREC_MG:
         if (mg32) {
@@ -489,9 +493,6 @@ void Precond<T>::apply(const T* r, T* z, const Scratch& sc, const int* done, cud
         break;
     case JFG_PREC_MATRIX:
         spmv_launch<T, T, 0>(st, M, vals_of<T>(M), r, EpiStore<T>{z}, sc, done);
-        break;
-    case JFG_PREC_MG_CNN:
-        hook(hook_self, r, z, sc, done, st);
         break;
     default:
         vec_launch<0>(st, n, VCopy<T>{r, z}, sc, done);
@@ -672,7 +673,7 @@ int run_cg(SolverWork& w, int ci, Matrix* A, const Precond<T>& M, const T* b, T*
             vec_launch<0>(st, n, VXpby<T>{r, p, c}, sc, done);
         }
     };
-    std::vector<uintptr_t> key{1, (uintptr_t)A->uid, (uintptr_t)(M.mg ? M.mg->uid : 0), (uintptr_t)(M.M ? M.M->uid : 0), (uintptr_t)(M.mg32 ? M.mg32->uid : 0), (uintptr_t)M.r32, (uintptr_t)M.dinv, (uintptr_t)b,
+    std::vector<uintptr_t> key{1, (uintptr_t)A->uid, (uintptr_t)(M.mg ? M.mg->uid : 0), (uintptr_t)M.hook_uid, (uintptr_t)(M.M ? M.M->uid : 0), (uintptr_t)(M.mg32 ? M.mg32->uid : 0), (uintptr_t)M.r32, (uintptr_t)M.dinv, (uintptr_t)b,
                                (uintptr_t)x, (uintptr_t)r, (uintptr_t)p, (uintptr_t)z, (uintptr_t)Ap, (uintptr_t)sizeof(T),
                                (uintptr_t)M.kind, (uintptr_t)done};
     return run_loop(w, done, key, iter, use_graph, chunk);
@@ -717,7 +718,7 @@ int run_bicgstab(SolverWork& w, int ci, Matrix* A, const Precond<T>& M, const T*
             vec_launch<1>(st, n, VBicgEnd<T>{x, p, s, s, t, r, c}, sc, done, FinBicgEnd{c});
         }
     };
-    std::vector<uintptr_t> key{2, (uintptr_t)A->uid, (uintptr_t)(M.mg ? M.mg->uid : 0), (uintptr_t)(M.M ? M.M->uid : 0), (uintptr_t)(M.mg32 ? M.mg32->uid : 0), (uintptr_t)M.r32, (uintptr_t)M.dinv, (uintptr_t)b,
+    std::vector<uintptr_t> key{2, (uintptr_t)A->uid, (uintptr_t)(M.mg ? M.mg->uid : 0), (uintptr_t)M.hook_uid, (uintptr_t)(M.M ? M.M->uid : 0), (uintptr_t)(M.mg32 ? M.mg32->uid : 0), (uintptr_t)M.r32, (uintptr_t)M.dinv, (uintptr_t)b,
                                (uintptr_t)x, (uintptr_t)r0, (uintptr_t)r, (uintptr_t)p, (uintptr_t)vv, (uintptr_t)s,
                                (uintptr_t)t, (uintptr_t)y, (uintptr_t)z, (uintptr_t)pt, (uintptr_t)sizeof(T),
                                (uintptr_t)M.kind, (uintptr_t)done};
@@ -774,7 +775,7 @@ int run_gmres(SolverWork& w, Matrix* A, const Precond<double>& M, const double* 
             vec_launch<0>(st, n, VGmresNext<double>{V, vcur, wv, w.H.p, c, n, ldh}, sc, cdone);
             scalar_launch(st, GmresAdvance{c}, cdone);
         };
-        std::vector<uintptr_t> key{3, (uintptr_t)A->uid, (uintptr_t)(M.mg ? M.mg->uid : 0), (uintptr_t)(M.M ? M.M->uid : 0), (uintptr_t)(M.mg32 ? M.mg32->uid : 0), (uintptr_t)M.r32, (uintptr_t)M.dinv,
+        std::vector<uintptr_t> key{3, (uintptr_t)A->uid, (uintptr_t)(M.mg ? M.mg->uid : 0), (uintptr_t)M.hook_uid, (uintptr_t)(M.M ? M.M->uid : 0), (uintptr_t)(M.mg32 ? M.mg32->uid : 0), (uintptr_t)M.r32, (uintptr_t)M.dinv,
                                    (uintptr_t)x, (uintptr_t)V, (uintptr_t)M.kind, (uintptr_t)m, (uintptr_t)t,
                                    (uintptr_t)q, (uintptr_t)wv, (uintptr_t)vcur, (uintptr_t)w.H.p,
                                    (uintptr_t)w.fac.p, (uintptr_t)w.mdot_part.p, (uintptr_t)cdone};

@@ -83,5 +83,7 @@ uint64_t next_uid();
 int mgcnn_precond(void* handle, Precond<double>& P, int n);
 // The same for a jfg_schwarz handle (AbstractSchwarz.mvMul); defined with the Schwarz kernels.
 int schwarz_precond(void* handle, Precond<double>& P, int n);
+// The same for a jfg_blockdiag handle (velocity multigrid + diagonal pressure block).
+int blockdiag_precond(void* handle, Precond<double>& P, int n);
 
 }  // namespace jfg

@@ -384,6 +384,8 @@ class IterativeSolver:
                 pk, ph = N.PREC_MG_CNN, prec.handle
             elif hasattr(prec, "correction") and hasattr(prec, "patches"):     # a Schwarz decomposition
                 pk, ph = N.PREC_SCHWARZ, prec.handle
+            elif type(prec).__name__ == "BlockDiagonalPreconditioner":
+                pk, ph = N.PREC_BLOCKDIAG, prec.handle
             elif isinstance(prec, (SparseMatrix, DeviceMatrix)):
                 pk, ph = N.PREC_MATRIX, _as_device(prec).handle
             elif prec == "jacobi":

@@ -79,6 +79,8 @@ def lib():
         L.or_op_mg_free.argtypes = [_P]
         L.or_mg_coarse_status.argtypes = [_P]
         L.or_mg_set_schwarz.argtypes = [_P, C.c_int, _P, C.c_int]
+        L.or_op_blockdiag.restype = _P
+        L.or_op_blockdiag.argtypes = [_P, C.c_int, _D]
         L.or_schwarz_new.restype = _P
         L.or_schwarz_new.argtypes = [_P, C.c_int, C.c_double, C.c_int, C.POINTER(C.c_longlong), _I, C.c_int, _I,
                                      _I]
@@ -202,11 +204,30 @@ class Result:
 def _op(M):
     if M is None:
         return None
-    if isinstance(M, CooMatrix):
-        return M._op
-    if isinstance(M, MGPreconditioner):
+    if isinstance(M, (CooMatrix, MGPreconditioner, BlockDiagonal)):
         return M._op
     raise TypeError(type(M))
+
+
+class BlockDiagonal:
+    """diag(velocity multigrid, pressure scaling) over velocity-first unknowns."""
+
+    def __init__(self, mg: "MGPreconditioner", pinv):
+        self.mg = mg
+        self._pinv = _f64(pinv)
+        self._op = lib().or_op_blockdiag(mg._op, self._pinv.size, _d(self._pinv))
+        self.n = mg.n + self._pinv.size
+
+    def mvmul(self, v):
+        out = np.empty(self.n)
+        lib().or_op_apply(self._op, _d(_f64(v)), _d(out))
+        return out
+
+    def __del__(self):
+        try:
+            lib().or_op_free(self._op)
+        except Exception:
+            pass
 
 
 def _run(fn, *args, x0, hist_cap=100000):

@@ -370,6 +370,23 @@ void or_op_free(or_op* o)
     free(o->tmp);
     free(o);
 }
+
+/* Block-diagonal saddle-point preconditioner: y[0, nv) = vel(x[0, nv)),
+ * y[nv, n) = pinv * x[nv, n) (tmp holds pinv, inner1 the velocity operator). */
+static void op_blockdiag_mv(const or_op* o, const double* x, double* y)
+{
+    int nv = o->inner1->n;
+    o->inner1->mv(o->inner1, x, y);
+    for (int i = nv; i < o->n; i++) y[i] = o->tmp[i - nv] * x[i];
+}
+or_op* or_op_blockdiag(const or_op* vel, int np, const double* pinv)
+{
+    or_op* o = (or_op*)calloc(1, sizeof(or_op));
+    o->n = vel->n + np; o->mv = op_blockdiag_mv; o->inner1 = vel;
+    o->tmp = vnew(np);
+    memcpy(o->tmp, pinv, sizeof(double) * np);
+    return o;
+}
 void or_op_apply(const or_op* o, const double* x, double* y) { o->mv(o, x, y); }
 
 /* ------------------------------------------------------------------ */

@@ -58,7 +58,7 @@ def test_large_patch_global_memory_inverse(ctx):
     sp, sy = fe_system(2, 12)
     _, patches = cartesian_patch_dofs(sp, (4, 4), 2)
     S = UpFrontSchwarz(dev(sy, ctx), patches, AdditiveSubspaceCorrection(0.1))
-    assert S.info()["max_patch"] > 160
+    assert S.info()["max_patch"] > 168
     So = O.Schwarz(coo_oracle(sy), O.SCHWARZ_ADDITIVE, patches, 0.1)
     b = sy.rhs
     x0 = np.random.default_rng(3).standard_normal(sy.n)
