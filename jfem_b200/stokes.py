@@ -139,7 +139,10 @@ def _eliminate(R, Cc, V, rhs, bd, g):
             np.concatenate([V, np.ones(bd.size)]), rhs)
 
 
-def assemble_stokes(th: TaylorHoodSpace, nu: float = 1.0, force=None, lid: bool = True) -> StokesSystem:
+def assemble_stokes(th: TaylorHoodSpace, nu: float = 1.0, force=None, lid: bool = True,
+                    pin_pressure: bool = True) -> StokesSystem:
+    """pin_pressure=False leaves the pressure determined up to a constant
+    (a consistent singular system; pressure_fixed = -1)."""
     K, B0, B1, _, rw = _tables(th.hx, th.hy)
     nc = th.cx * th.cy
     vn, pn = th.cell_vnodes, th.cell_pnodes
@@ -178,9 +181,9 @@ def assemble_stokes(th: TaylorHoodSpace, nu: float = 1.0, force=None, lid: bool 
         top = np.nonzero(np.isclose(py, 1.0))[0]
         g[top] = 1.0                                       # u0 = 1 on y = 1, u1 = 0
     # velocity Dirichlet data and the first pressure unknown fixed to zero
-    fixed = np.concatenate([bd, np.array([th.nv], dtype=np.int32)])
+    fixed = np.concatenate([bd, np.array([th.nv], dtype=np.int32)]) if pin_pressure else bd
     R, Cc, V, rhs = _eliminate(R, Cc, V, rhs, fixed, g)
-    return StokesSystem(th.n, th.nv, R, Cc, V, rhs, bd, th.nv)
+    return StokesSystem(th.n, th.nv, R, Cc, V, rhs, bd, th.nv if pin_pressure else -1)
 
 
 def velocity_block(th: TaylorHoodSpace, nu: float = 1.0):
@@ -272,12 +275,20 @@ class StokesProblem:
     nu: float
 
 
-def stokes_problem(cells: int = 256, coarse_cells: int = 4, nu: float = 1.0, seed: int = 0) -> StokesProblem:
+def stokes_problem(cells: int = 256, coarse_cells: int = 4, nu: float = 1.0, seed: int = 0,
+                   pin_pressure: bool = True) -> StokesProblem:
+    """pin_pressure=True is the reference's system (first pressure unknown
+    overwritten by 0).  Pinning one unknown turns the constant pressure into a
+    near-null mode of the preconditioned operator (eigenvalue ~ h^2), which
+    restarted GMRES resolves only slowly; pin_pressure=False keeps the
+    consistent singular system, whose constant-pressure null space never
+    enters the Krylov space, and StokesSolver.solve shifts the pressure so that
+    the first unknown is 0 -- a solution of the pinned system."""
     levels = int(round(np.log2(cells // coarse_cells))) + 1
     if coarse_cells << (levels - 1) != cells:
         raise IllegalArgumentException("cells must be coarse_cells * 2^k")
     ths = [TaylorHoodSpace(coarse_cells << l, coarse_cells << l) for l in range(levels)]
-    system = assemble_stokes(ths[-1], nu, fourier_force(seed=seed))
+    system = assemble_stokes(ths[-1], nu, fourier_force(seed=seed), pin_pressure=pin_pressure)
     vb, vbd = [], []
     for t in ths:
         R, Cc, V, bd = velocity_block(t, nu)
@@ -285,7 +296,8 @@ def stokes_problem(cells: int = 256, coarse_cells: int = 4, nu: float = 1.0, see
         vbd.append(bd)
     prol = [velocity_prolongation(ths[l], ths[l + 1]) for l in range(levels - 1)]
     pinv = nu / lumped_pressure_mass(ths[-1])
-    pinv[0] = 1.0
+    if pin_pressure:
+        pinv[0] = 1.0
     return StokesProblem(ths, system, vb, vbd, prol, pinv, nu)
 
 
@@ -328,4 +340,7 @@ class StokesSolver:
         it.gm.ITERATIONS_BEFORE_RESTART = restart
         it.gm.MAX_RESTARTS = max_restarts
         x = it.solvePGMRES(self.A, self.P, self.prob.system.rhs, tol)
+        s = self.prob.system
+        if s.pressure_fixed < 0:
+            x[s.nv:] -= x[s.nv]          # the pinned system's pressure gauge
         return x, it

@@ -30,7 +30,7 @@ def oracle_setup(prob, solver):
 
 @pytest.fixture(scope="module")
 def small(ctx):
-    prob = stokes_problem(16, 4, nu=1.0, seed=2)
+    prob = stokes_problem(16, 4, nu=1.0, seed=2, pin_pressure=False)
     return prob, StokesSolver(ctx, prob)
 
 
@@ -54,7 +54,24 @@ def test_gmres50_matches_oracle(small):
     assert abs(it.iterations - ref.iterations) <= 1
     k = min(5, ref.iterations)
     np.testing.assert_allclose(it.last.history[:k], ref.history[:k], rtol=1e-7)
-    np.testing.assert_allclose(x, ref.x, rtol=1e-6, atol=1e-7 * np.abs(ref.x).max())
+    xr = ref.x.copy()
+    nv = prob.spaces[-1].nv
+    xr[nv:] -= xr[nv]
+    np.testing.assert_allclose(x, xr, rtol=1e-6, atol=1e-7 * np.abs(xr).max())
+
+
+def test_pinned_system_solves(ctx):
+    """The reference's own system (first pressure unknown pinned) converges to
+    the same solution as the consistent singular system shifted to p0 = 0."""
+    prob_p = stokes_problem(16, 4, seed=2, pin_pressure=True)
+    prob_s = stokes_problem(16, 4, seed=2, pin_pressure=False)
+    b = prob_p.system.rhs
+    tol = 1e-10 * np.linalg.norm(b)
+    xp, itp = StokesSolver(ctx, prob_p).solve(tol)
+    xs, its = StokesSolver(ctx, prob_s).solve(tol)
+    assert itp.last.status == N.OK and its.last.status == N.OK
+    assert its.iterations < itp.iterations
+    np.testing.assert_allclose(xp, xs, rtol=1e-6, atol=1e-6 * np.abs(xs).max())
 
 
 def test_solution_is_discretely_divergence_free(small):
@@ -70,7 +87,7 @@ def test_solution_is_discretely_divergence_free(small):
 
 
 def test_jacobi_and_fp32_variants_converge(ctx):
-    prob = stokes_problem(16, 4, seed=5)
+    prob = stokes_problem(16, 4, seed=5, pin_pressure=False)
     b = prob.system.rhs
     tol = 1e-8 * np.linalg.norm(b)
     for kw in ({"smoother": "jacobi", "runs": 2, "omega": 0.6}, {"fp32_vcycle": True}):
