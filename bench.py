@@ -13,6 +13,13 @@ than L2, so no flush is needed between steps.
 
 Under torchrun every rank solves its own replica (no data-path collective;
 "replicas only"); the step time is the max over ranks.
+
+The other configurations are measured with --workload (one JSON line each,
+1 GPU, no reference arm): batch-heat (256 uneven Q1 heat systems, 50
+implicit-Euler steps in one persistent launch), stokes (Taylor-Hood Q2/Q1
+on 256x256 cells, GMRES(50) with the block-diagonal preconditioner) and
+learned (-div(kappa grad u) = f on Q1 1024x1024: FGMRES(30) with the
+V-cycle + learned smoother against FP64 GMG-PCG).
 """
 from __future__ import annotations
 
@@ -43,6 +50,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cells", type=int, default=CELLS)
     ap.add_argument("--levels", type=int, default=LEVELS)
+    ap.add_argument("--workload", default="gmg-pcg", choices=["gmg-pcg", "batch-heat", "stokes", "learned"])
     ap.add_argument("--profile", default=None, choices=["solve-fp64", "solve-mixed", "spmv64", "spmv32"],
                     help="set up, run the named operation --warmup + 1 times and exit (for ncu captures)")
     return ap.parse_args()
@@ -366,10 +374,146 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def run_batch_heat(args):
+    """256 Q1 heat systems, cells drawn from {32, 48, ..., 256}^2,
+    dt = 1e-3, 50 implicit-Euler steps, FP32 PCG + FP64 refinement to 1e-10."""
+    import torch
+    from jfem_b200 import _native as N
+    from jfem_b200 import problems
+    from jfem_b200.batch import BatchedParabolicIntegrator
+    from jfem_b200.linalg import DeviceMatrix
+    ctx = N.default_context()
+    batch = problems.heat_batch(nsys=256, dt=1e-3, seed=0)
+    K = [DeviceMatrix(s.K.n, s.K.n, s.K.rows, s.K.cols, s.K.vals, ctx) for s in batch]
+    M = [DeviceMatrix(s.M.n, s.M.n, s.M.rows, s.M.cols, s.M.vals, ctx) for s in batch]
+    B = BatchedParabolicIntegrator(K, M, ctx)
+    u0 = B.pack([s.u0 for s in batch])
+    steps = 50
+    for _ in range(max(3, args.warmup)):
+        B.timeSteps(u0, steps)
+    ms = []
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            B.timeSteps(u0, steps)
+            ms.append((time.perf_counter() - t0) * 1e3)
+    last = B.last
+    dofs = int(sum(s.K.n for s in batch))
+    nnz = int(sum(s.K.nnz for s in batch))
+    cpu = None
+    if os.environ.get("JFEM_BENCH_NO_CPU") != "1":
+        import oracle as O
+        pick = list(range(0, 256, 32))
+        t0 = time.perf_counter()
+        n_s = 0
+        for i in pick:
+            s = batch[i]
+            Ko = O.CooMatrix(s.K.n, s.K.n, s.K.rows, s.K.cols, s.K.vals)
+            Mo = O.CooMatrix(s.M.n, s.M.n, s.M.rows, s.M.cols, s.M.vals)
+            rhs = Mo.mvmul(s.u0)
+            O.solve_cg(Ko, rhs, 1e-10 * np.linalg.norm(rhs), x0=s.u0)
+            n_s += s.K.n
+        t = time.perf_counter() - t0
+        cpu = {"value": t / n_s * dofs * steps, "unit": "s", "cores": 1, "kind": "port",
+               "sample": f"one CG step (1e-10) of {len(pick)} systems, scaled by unknowns to 256 systems x 50 steps"}
+    line = {"metric": "time for 50 implicit-Euler steps of 256 uneven Q1 heat systems (s)",
+            "value": statistics.median(ms) / 1e3, "unit": "s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": statistics.median(ms), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded bumps)",
+            "config": {"workload": "batch-heat: 256 Q1 systems, cells {32..256 step 16}^2, dt=1e-3, 50 steps "
+                                   "(configs[2])", "systems": 256, "dofs": dofs, "nnz": nnz},
+            "kernel_ms": last.ms, "total_inner_iterations": last.total_inner_iterations,
+            "max_rel_residual": last.max_rel_residual, "failed": last.failed,
+            "cluster": last.cluster, "threads": last.threads, "clocks": clk.summary(), "cpu_baseline": cpu}
+    print(json.dumps(line))
+
+
+def run_stokes(args):
+    """Taylor-Hood Stokes on 256x256 cells, GMRES(50) + block-diagonal
+    preconditioner to 1e-8, variants of the velocity smoother and precision."""
+    import torch
+    from jfem_b200 import _native as N
+    from jfem_b200.stokes import StokesSolver, stokes_problem
+    ctx = N.default_context()
+    t0 = time.time()
+    prob = stokes_problem(args.cells if args.cells != CELLS else 256, 4, seed=0, pin_pressure=False)
+    assemble_s = time.time() - t0
+    b = prob.system.rhs
+    tol = RTOL * float(np.linalg.norm(b))
+    out = {}
+    for name, kw in (("schwarz_fp64", {}), ("schwarz_fp32_vcycle", {"fp32_vcycle": True}),
+                     ("jacobi_fp64", {"smoother": "jacobi", "runs": 2, "omega": 0.6})):
+        t1 = time.time()
+        sol = StokesSolver(ctx, prob, **kw)
+        setup = time.time() - t1
+        for _ in range(max(1, args.warmup)):
+            x, it = sol.solve(tol)
+        ts = []
+        for _ in range(max(1, args.steps // 3)):
+            t2 = time.perf_counter()
+            x, it = sol.solve(tol)
+            ts.append(time.perf_counter() - t2)
+        A = sol.A
+        r = b - A.spmv(x)
+        out[name] = {"time_s": min(ts), "iterations": it.iterations, "restarts": it.last.restarts,
+                     "status": N.STATUS_NAMES[it.last.status],
+                     "true_rel_residual": float(np.linalg.norm(r) / np.linalg.norm(b)), "setup_s": setup}
+        del sol
+    s = prob.system
+    line = {"metric": "time-to-1e-8 residual (s), Stokes GMRES(50) + block-diagonal preconditioner",
+            "value": out["schwarz_fp64"]["time_s"], "unit": "s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (lid-driven cavity + seeded Fourier body force)",
+            "config": {"workload": "stokes: Taylor-Hood Q2/Q1 256x256 cells (configs[3])", "dofs": s.n,
+                       "velocity_dofs": s.nv, "nnz": int(s.vals.size), "levels": len(prob.spaces),
+                       "preconditioner": "velocity V-cycle (coloured Schwarz, 2x2-cell partitions + 1 cell "
+                                         "overlap, 9 colours) | nu / lumped pressure mass",
+                       "pressure": "consistent singular system, gauge p0 = 0 after the solve"},
+            "variants": out, "assemble_s": assemble_s}
+    print(json.dumps(line))
+
+
+def run_learned(args):
+    """FGMRES(30) + FP32 V-cycle + learned smoother vs FP64 GMG-PCG."""
+    from jfem_b200 import _native as N
+    from jfem_b200.learned import WEIGHTS, evaluate
+    ctx = N.default_context()
+    w = np.load(WEIGHTS)
+    out = evaluate(ctx, w, cells=1024, kseed=0, out_scales=(1.0, 0.5), repeats=max(3, args.steps))
+    with open(WEIGHTS.replace(".npy", ".train.json")) as f:
+        train = json.load(f)
+    best = min(v["time_s"] for v in out["fgmres_vcycle_net"].values())
+    line = {"metric": "time-to-1e-8 residual (s): FGMRES(30)+V-cycle+learned smoother vs FP64 GMG-PCG",
+            "value": best, "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32+f64",
+            "data": "synthetic (GRF kappa, seeded)",
+            "config": {"workload": "learned: -div(kappa grad u) = f, Q1 1024x1024, kappa = exp(GRF l=0.05 s2=1) "
+                                   "(configs[4])", "training": train},
+            "speedup_vs_fp64_gmg_pcg": out["gmg_pcg_fp64"]["time_s"] / best, "arms": out}
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
+        if args.workload != "gmg-pcg":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference arm covers the gmg-pcg workload"}))
+            return
         run_reference(args)
+    elif args.workload == "batch-heat":
+        run_batch_heat(args)
+    elif args.workload == "stokes":
+        run_stokes(args)
+    elif args.workload == "learned":
+        run_learned(args)
     else:
         run_ours(args)
 
