@@ -117,6 +117,8 @@ struct Matrix {
     DevBuf<int> off;              // nslices + 1 slice offsets
     DevBuf<int> perm;             // nslices * 32 original row of each slot
     DevBuf<int> col;              // sell_len
+    DevBuf<int16_t> col16;        // sell_len: col - max(row, 0) when every entry fits 16 bits
+    int idx16 = 0;                // the SpMV reads col16 instead of col
     DevBuf<double> val;           // sell_len
     DevBuf<float> val32;          // optional FP32 copy
     DevBuf<__nv_bfloat16> val16;  // optional BF16 copy

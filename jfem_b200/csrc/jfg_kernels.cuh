@@ -132,6 +132,7 @@ struct SpmvArgs {
     const int* col;     // SELL column indices
     int nslots;         // nslices * 32
     int tpr_log2;       // log2 of the threads that share one row (0..3)
+    const int16_t* col16;  // SELL column offsets from the slot's row (IDX16 kernels)
 };
 
 // 2^tpr_log2 adjacent threads per slot (row) of a 32-row slice; thread `sub`
@@ -142,7 +143,7 @@ struct SpmvArgs {
 // gather latency); TPR = 4..8 on small levels, where the row loop would
 // otherwise be a chain of dependent gathers per thread.  No shared memory,
 // no barriers.
-template <typename VT, typename XT, int NR, int TPR, class Epi, class Fin>
+template <typename VT, typename XT, int NR, int TPR, class Epi, class Fin, bool IDX16 = false>
 __global__ void __launch_bounds__(kThreads)
 k_spmv(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi, GridRed<NR, Fin> red,
        const int* __restrict__ done)
@@ -164,22 +165,42 @@ k_spmv(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi
         const int o = __ldg(m.off + s);
         const int len = (__ldg(m.off + s + 1) - o) >> 5;
         r = __ldg(m.perm + slot);
-        const int* cp = m.col + o + lane;
         const VT* vp = val + o + lane;
         const int st = 32 * tpr;
         int k = sub;
-        for (; k + 3 * tpr < len; k += 4 * tpr) {
-            const int c0 = __ldg(cp + 32 * k), c1 = __ldg(cp + 32 * k + st);
-            const int c2 = __ldg(cp + 32 * k + 2 * st), c3 = __ldg(cp + 32 * k + 3 * st);
-            const AT v0 = to_acc(__ldg(vp + 32 * k)), v1 = to_acc(__ldg(vp + 32 * k + st));
-            const AT v2 = to_acc(__ldg(vp + 32 * k + 2 * st)), v3 = to_acc(__ldg(vp + 32 * k + 3 * st));
-            const AT x0 = (AT)__ldg(x + c0), x1 = (AT)__ldg(x + c1), x2 = (AT)__ldg(x + c2), x3 = (AT)__ldg(x + c3);
-            sum += v0 * x0;
-            sum += v1 * x1;
-            sum += v2 * x2;
-            sum += v3 * x3;
+        if constexpr (IDX16) {
+            // columns stored as 16-bit offsets from the row: 2 bytes less per entry
+            const int base = r < 0 ? 0 : r;
+            const int16_t* cp = m.col16 + o + lane;
+            for (; k + 3 * tpr < len; k += 4 * tpr) {
+                const int c0 = base + __ldg(cp + 32 * k), c1 = base + __ldg(cp + 32 * k + st);
+                const int c2 = base + __ldg(cp + 32 * k + 2 * st), c3 = base + __ldg(cp + 32 * k + 3 * st);
+                const AT v0 = to_acc(__ldg(vp + 32 * k)), v1 = to_acc(__ldg(vp + 32 * k + st));
+                const AT v2 = to_acc(__ldg(vp + 32 * k + 2 * st)), v3 = to_acc(__ldg(vp + 32 * k + 3 * st));
+                const AT x0 = (AT)__ldg(x + c0), x1 = (AT)__ldg(x + c1), x2 = (AT)__ldg(x + c2),
+                         x3 = (AT)__ldg(x + c3);
+                sum += v0 * x0;
+                sum += v1 * x1;
+                sum += v2 * x2;
+                sum += v3 * x3;
+            }
+            for (; k < len; k += tpr) sum += to_acc(__ldg(vp + 32 * k)) * (AT)__ldg(x + base + __ldg(cp + 32 * k));
+        } else {
+            const int* cp = m.col + o + lane;
+            for (; k + 3 * tpr < len; k += 4 * tpr) {
+                const int c0 = __ldg(cp + 32 * k), c1 = __ldg(cp + 32 * k + st);
+                const int c2 = __ldg(cp + 32 * k + 2 * st), c3 = __ldg(cp + 32 * k + 3 * st);
+                const AT v0 = to_acc(__ldg(vp + 32 * k)), v1 = to_acc(__ldg(vp + 32 * k + st));
+                const AT v2 = to_acc(__ldg(vp + 32 * k + 2 * st)), v3 = to_acc(__ldg(vp + 32 * k + 3 * st));
+                const AT x0 = (AT)__ldg(x + c0), x1 = (AT)__ldg(x + c1), x2 = (AT)__ldg(x + c2),
+                         x3 = (AT)__ldg(x + c3);
+                sum += v0 * x0;
+                sum += v1 * x1;
+                sum += v2 * x2;
+                sum += v3 * x3;
+            }
+            for (; k < len; k += tpr) sum += to_acc(__ldg(vp + 32 * k)) * (AT)__ldg(x + __ldg(cp + 32 * k));
         }
-        for (; k < len; k += tpr) sum += to_acc(__ldg(vp + 32 * k)) * (AT)__ldg(x + __ldg(cp + 32 * k));
     }
     for (int o = tpr >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
     if (sub == 0 && r >= 0) epi(r, sum, acc);

@@ -120,6 +120,27 @@ __global__ void k_fill_sell(int nslots, const int* perm, const int* off, const i
     }
 }
 
+// 16-bit column offsets relative to the slot's row (FE matrices couple rows
+// to nearby columns); flags an entry that does not fit
+__global__ void k_make_col16(int nslots, const int* perm, const int* off, const int* col, int16_t* col16, int* bad)
+{
+    int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= nslots) return;
+    int s = slot >> 5, lane = slot & 31;
+    int o = off[s];
+    int len = (off[s + 1] - o) >> 5;
+    int base = max(perm[slot], 0);
+    for (int k = 0; k < len; k++) {
+        int64_t at = (int64_t)o + (int64_t)k * 32 + lane;
+        int d = col[at] - base;
+        if (d < -32768 || d > 32767) {
+            atomicOr(bad, 1);
+            return;
+        }
+        col16[at] = (int16_t)d;
+    }
+}
+
 __global__ void k_expand_rows(int rows, const int* ptr, int* ri)
 {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -220,6 +241,21 @@ static Matrix* build_from_sorted(Context* c, int rows, int cols, int64_t m, cons
                                                                          M->csr_ptr.p, M->csr_col.p, M->csr_val.p,
                                                                          M->col.p, M->val.p);
     JFG_CUDA(cudaGetLastError());
+    const char* e16 = getenv("JFEM_IDX16");
+    if (nslices && !(e16 && e16[0] == '0')) {
+        DevBuf<int> bad;
+        bad.alloc(1);
+        JFG_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
+        M->col16.alloc((size_t)total);
+        k_make_col16<<<nblk((int64_t)nslices * kSliceRows), 256, 0, s>>>(nslices * kSliceRows, M->perm.p, M->off.p,
+                                                                          M->col.p, M->col16.p, bad.p);
+        JFG_CUDA(cudaGetLastError());
+        int hb = 0;
+        JFG_CUDA(cudaMemcpyAsync(&hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+        JFG_CUDA(cudaStreamSynchronize(s));
+        M->idx16 = hb ? 0 : 1;
+        if (hb) M->col16.release();
+    }
     JFG_CUDA(cudaStreamSynchronize(s));
     return M;
 }

@@ -123,20 +123,20 @@ void spmv_launch(cudaStream_t st, const Matrix* M, const VT* val, const XT* x, E
 {
     if (M->rows == 0) return;
     GridRed<NR, Fin> red{sc.partials, sc.counter, fin};
-    SpmvArgs a{M->off.p, M->perm.p, M->col.p, M->nslices * kSliceRows, M->tpr_log2};
+    SpmvArgs a{M->off.p, M->perm.p, M->col.p, M->nslices * kSliceRows, M->tpr_log2, M->col16.p};
+    const dim3 g(M->nblocks), b(kThreads);
+    if (M->idx16) {
+        switch (M->tpr_log2) {
+        case 0: launch_ex(k_spmv<VT, XT, NR, 1, Epi, Fin, true>, g, b, 0, st, a, val, x, epi, red, done); break;
+        case 2: launch_ex(k_spmv<VT, XT, NR, 4, Epi, Fin, true>, g, b, 0, st, a, val, x, epi, red, done); break;
+        default: launch_ex(k_spmv<VT, XT, NR, 8, Epi, Fin, true>, g, b, 0, st, a, val, x, epi, red, done); break;
+        }
+        return;
+    }
     switch (M->tpr_log2) {
-    case 0:
-        launch_ex(k_spmv<VT, XT, NR, 1, Epi, Fin>, dim3(M->nblocks), dim3(kThreads), 0, st, a, val, x, epi, red,
-                  done);
-        break;
-    case 2:
-        launch_ex(k_spmv<VT, XT, NR, 4, Epi, Fin>, dim3(M->nblocks), dim3(kThreads), 0, st, a, val, x, epi, red,
-                  done);
-        break;
-    default:
-        launch_ex(k_spmv<VT, XT, NR, 8, Epi, Fin>, dim3(M->nblocks), dim3(kThreads), 0, st, a, val, x, epi, red,
-                  done);
-        break;
+    case 0: launch_ex(k_spmv<VT, XT, NR, 1, Epi, Fin>, g, b, 0, st, a, val, x, epi, red, done); break;
+    case 2: launch_ex(k_spmv<VT, XT, NR, 4, Epi, Fin>, g, b, 0, st, a, val, x, epi, red, done); break;
+    default: launch_ex(k_spmv<VT, XT, NR, 8, Epi, Fin>, g, b, 0, st, a, val, x, epi, red, done); break;
     }
 }
 

@@ -3,7 +3,8 @@
 // subspace corrections (schwarz/*.java).
 //
 // Layout in HBM: patch p's sorted DOF list is dofs[pptr[p] .. pptr[p+1]) and
-// its m_p x m_p row-major inverse of R_p A R_p^T sits at inv + inv_off[p].
+// the transpose of the m_p x m_p inverse of R_p A R_p^T sits at inv + inv_off[p]
+// (column-major inverse).
 // One sweep step over a colour is one launch with a CTA per patch: the CTA
 // gathers the patch rows of b - A x straight from A's CSR rows (no global
 // residual vector), multiplies by the patch inverse (warp per row, coalesced
@@ -160,47 +161,73 @@ __global__ void __launch_bounds__(kSchThreads)
         }
     }
     __syncthreads();
+    // stored transposed (the apply kernels read it column by column)
     if (SMEM) {
         double* out = inv + inv_off[p];
-        for (int64_t e = tid; e < (int64_t)m * m; e += blockDim.x) out[e] = Ms[e];
+        for (int64_t e = tid; e < (int64_t)m * m; e += blockDim.x) {
+            const int j = (int)(e / m), i = (int)(e - (int64_t)j * m);
+            out[e] = Ms[(size_t)i * m + j];
+        }
+    } else {
+        for (int64_t e = tid; e < (int64_t)m * m; e += blockDim.x) {
+            const int i = (int)(e / m), j = (int)(e - (int64_t)i * m);
+            if (i < j) {
+                const double a = M[(size_t)i * m + j];
+                M[(size_t)i * m + j] = M[(size_t)j * m + i];
+                M[(size_t)j * m + i] = a;
+            }
+        }
     }
     if (tid == 0) status[p] = s_sing;
 }
 
 // One patch: local residual rows of b - A x, times the patch inverse; either
 // x += omega * correction (direct) or the correction into lsol[pptr[p] + i].
+// Built for memory-level parallelism: the row ranges of all patch rows are
+// fetched in one pass, the residual rows are summed by groups of 8 lanes (32
+// rows in flight per CTA), and the inverse is stored transposed so that
+// thread i walks column j of row i with every warp reading 32 consecutive
+// entries per j (coalesced, many independent loads in flight per thread).
+constexpr int kRowLanes = 8;
+
 template <typename T, typename IT>
 __device__ __forceinline__ void patch_correct(const CsrView& A, int p, const int64_t* __restrict__ pptr,
                                               const int* __restrict__ dofs, const int64_t* __restrict__ inv_off,
                                               const IT* __restrict__ inv, const T* b, T* x, double om,
-                                              double* lsol, bool direct, int* sdof, double* sr)
+                                              double* lsol, bool direct, int* sdof, int* srs, int* sre, double* sr)
 {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+    const int tid = threadIdx.x;
     const int64_t off = pptr[p];
     const int m = (int)(pptr[p + 1] - off);
-    for (int i = tid; i < m; i += blockDim.x) sdof[i] = dofs[off + i];
-    __syncthreads();
-    for (int i = warp; i < m; i += nw) {
-        const int g = sdof[i];
-        double acc = 0.0;
-        for (int k = A.rp[g] + lane; k < A.rp[g + 1]; k += 32) acc += A.val[k] * (double)x[A.col[k]];
-        acc = warp_sum(acc);
-        if (lane == 0) sr[i] = (double)b[g] - acc;
+    for (int i = tid; i < m; i += blockDim.x) {
+        const int g = dofs[off + i];
+        sdof[i] = g;
+        srs[i] = A.rp[g];
+        sre[i] = A.rp[g + 1];
     }
     __syncthreads();
-    const IT* Ai = inv + inv_off[p];
-    for (int i = warp; i < m; i += nw) {
+    const int sub = tid & (kRowLanes - 1);
+    const int per_pass = blockDim.x / kRowLanes;
+    for (int i0 = 0; i0 < m; i0 += per_pass) {          // uniform trip count: the shuffles see full warps
+        const int i = i0 + tid / kRowLanes;
         double acc = 0.0;
-        const IT* row = Ai + (size_t)i * m;
-        for (int j = lane; j < m; j += 32) acc += (double)row[j] * sr[j];
-        acc = warp_sum(acc);
-        if (lane == 0) {
-            if (direct) {
-                const int g = sdof[i];
-                x[g] = (T)((double)x[g] + acc * om);
-            } else {
-                lsol[off + i] = acc;
-            }
+        if (i < m)
+            for (int k = srs[i] + sub; k < sre[i]; k += kRowLanes) acc += A.val[k] * (double)x[A.col[k]];
+#pragma unroll
+        for (int o = 1; o < kRowLanes; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (i < m && sub == 0) sr[i] = (double)b[sdof[i]] - acc;
+    }
+    __syncthreads();
+    const IT* At = inv + inv_off[p];                    // transposed: At[j * m + i] = inverse(i, j)
+    for (int i = tid; i < m; i += blockDim.x) {
+        double acc = 0.0;
+#pragma unroll 8
+        for (int j = 0; j < m; j++) acc += (double)At[(size_t)j * m + i] * sr[j];
+        if (direct) {
+            const int g = sdof[i];
+            x[g] = (T)((double)x[g] + acc * om);
+        } else {
+            lsol[off + i] = acc;
         }
     }
     __syncthreads();
@@ -213,9 +240,10 @@ __global__ void __launch_bounds__(kSchThreads)
                       const T* b, T* x, double om, double* lsol, int direct, const int* done)
 {
     if (done && *done) return;
-    __shared__ int sdof[kMaxPatch];
+    __shared__ int sdof[kMaxPatch], srs[kMaxPatch], sre[kMaxPatch];
     __shared__ double sr[kMaxPatch];
-    patch_correct<T, IT>(A, plist[blockIdx.x], pptr, dofs, inv_off, inv, b, x, om, lsol, direct != 0, sdof, sr);
+    patch_correct<T, IT>(A, plist[blockIdx.x], pptr, dofs, inv_off, inv, b, x, om, lsol, direct != 0, sdof, srs, sre,
+                         sr);
 }
 
 // MultiplicativeSubspaceCorrection: the patches of plist one after another
@@ -227,10 +255,10 @@ __global__ void __launch_bounds__(kSchThreads)
                   const T* b, T* x, const int* done)
 {
     if (done && *done) return;
-    __shared__ int sdof[kMaxPatch];
+    __shared__ int sdof[kMaxPatch], srs[kMaxPatch], sre[kMaxPatch];
     __shared__ double sr[kMaxPatch];
     for (int q = 0; q < count; q++)
-        patch_correct<T, IT>(A, plist[q], pptr, dofs, inv_off, inv, b, x, 1.0, nullptr, true, sdof, sr);
+        patch_correct<T, IT>(A, plist[q], pptr, dofs, inv_off, inv, b, x, 1.0, nullptr, true, sdof, srs, sre, sr);
 }
 
 // x[d] = x[d] + omega * c_1 + omega * c_2 + ... (coloured) or
@@ -722,9 +750,15 @@ int jfg_schwarz_local_inverse(jfg_schwarz* s, int patch, int* m, int* h_dofs, do
         int mm = (int)(se[1] - se[0]);
         if (m) *m = mm;
         if (h_dofs) JFG_CUDA(cudaMemcpyAsync(h_dofs, S.dofs.p + se[0], sizeof(int) * mm, cudaMemcpyDeviceToHost, st));
-        if (h_inv)
-            JFG_CUDA(cudaMemcpyAsync(h_inv, S.inv.p + off, sizeof(double) * mm * mm, cudaMemcpyDeviceToHost, st));
+        std::vector<double> t;
+        if (h_inv) {
+            t.resize((size_t)mm * mm);
+            JFG_CUDA(cudaMemcpyAsync(t.data(), S.inv.p + off, sizeof(double) * mm * mm, cudaMemcpyDeviceToHost, st));
+        }
         JFG_CUDA(cudaStreamSynchronize(st));
+        if (h_inv)   // stored transposed on the device
+            for (int i = 0; i < mm; i++)
+                for (int j = 0; j < mm; j++) h_inv[(size_t)i * mm + j] = t[(size_t)j * mm + i];
         return JFG_OK;
     });
 }

@@ -23,7 +23,7 @@ struct SchwarzImpl {
     uint64_t uid = next_uid();
     DevBuf<int64_t> pptr, inv_off;      // patch p: dofs[pptr[p], pptr[p+1]), inverse at inv + inv_off[p]
     DevBuf<int> dofs;
-    DevBuf<double> inv;                 // row-major m_p x m_p inverses
+    DevBuf<double> inv;                 // m_p x m_p inverses, column-major (transposed)
     DevBuf<float> inv32;                // FP32 copy for FP32 hierarchies (built on first use)
     DevBuf<int> seq;                    // multiplicative: patches forward then backward (2 np)
     DevBuf<int> cpat;                   // colour patch lists, concatenated
