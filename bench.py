@@ -62,9 +62,12 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 20 ms; summary()
+    keeps the samples taken between mark_start() and mark_end().  When the
+    timed region is shorter than a few sampling periods, extend() keeps the
+    same work running (untimed) until three samples exist after mark_start."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -72,13 +75,15 @@ class ClockSampler:
         self.device = device
         self.proc = None
         self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device}.csv")
+        self.t0 = self.t1 = None
+        self.extended = False
 
     def __enter__(self):
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                          "--format=csv,noheader,nounits", "-lms", "20"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -90,23 +95,61 @@ class ClockSampler:
             self.proc.wait()
             self.f.close()
 
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
+
+    def _rows(self):
+        import datetime
+        rows = []
+        try:
+            self.f.flush()
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) < 10:
+                        continue
+                    try:
+                        ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                    except ValueError:
+                        continue
+                    rows.append((ts, parts[1:]))
+        except Exception:
+            pass
+        return rows
+
+    def extend(self, fn, min_samples=3, max_s=5.0):
+        if not self.proc or self.t0 is None:
+            return
+        t_stop = time.time() + max_s
+        while time.time() < t_stop:
+            if len([r for r in self._rows() if r[0] >= self.t0 - 0.005]) >= min_samples:
+                break
+            fn()
+            self.extended = True
+        self.t1 = max(self.t1 or 0.0, time.time())
+
     def summary(self):
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        rows = []
-        with open(self.path) as f:
-            for line in f:
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
+        rows = self._rows()
+        if self.t0 is not None:
+            inside = [r for r in rows if self.t0 - 0.005 <= r[0] <= (self.t1 or time.time()) + 0.005]
+            rows = inside
+        rows = [r[1] for r in rows]
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+               "reasons": reasons, "samples": len(rows)}
+        if self.extended:
+            out["note"] = "timed region shorter than the sampling period: the same solve kept running untimed"
+        return out
 
 
 def build_problem(cells, levels):
@@ -188,19 +231,23 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    def timed(fn, steps, warmup):
+    def timed(fn, steps, warmup, clk=None):
         for _ in range(warmup):
             fn()
         barrier()
         torch.cuda.synchronize()
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
+        if clk:
+            clk.mark_start()
         ev0.record(stream)
         for _ in range(steps):
             fn()
         ev1.record(stream)
         ev1.synchronize()
         torch.cuda.synchronize()
+        if clk:
+            clk.mark_end()
         barrier()
         return max_over_ranks(ev0.elapsed_time(ev1) / steps)
 
@@ -225,8 +272,9 @@ def run_ours(args):
     it_dc, res_dc, outer_dc = solve_dev(N.MIXED)
     l0 = N.kernel_launches()
     with ClockSampler(local) as clk:
-        ms = timed(lambda: solve_dev(HEADLINE), args.steps, args.warmup)
-    launches = (N.kernel_launches() - l0) / (args.steps + args.warmup)
+        ms = timed(lambda: solve_dev(HEADLINE), args.steps, args.warmup, clk)
+        launches = (N.kernel_launches() - l0) / (args.steps + args.warmup)
+        clk.extend(lambda: solve_dev(HEADLINE))
     itm, resm, outer = solve_dev(HEADLINE)
     xm = dx.cpu().numpy().copy()
     rel_err = float(np.linalg.norm(xm - x64) / np.linalg.norm(x64))
@@ -401,10 +449,12 @@ def run_batch_heat(args):
         B.timeSteps(u0, steps)
     ms = []
     with ClockSampler(0) as clk:
+        clk.mark_start()
         for _ in range(args.steps):
             t0 = time.perf_counter()
             B.timeSteps(u0, steps)
             ms.append((time.perf_counter() - t0) * 1e3)
+        clk.mark_end()
     last = B.last
     dofs = int(sum(s.K.n for s in batch))
     nnz = int(sum(s.K.nnz for s in batch))

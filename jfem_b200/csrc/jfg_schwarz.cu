@@ -188,7 +188,8 @@ __global__ void __launch_bounds__(kSchThreads)
 // rows in flight per CTA), and the inverse is stored transposed so that
 // thread i walks column j of row i with every warp reading 32 consecutive
 // entries per j (coalesced, many independent loads in flight per thread).
-constexpr int kRowLanes = 8;
+constexpr int kRowLanes = 4;     // lanes per residual row: 64 rows in flight per CTA
+constexpr int kRowUnroll = 8;    // entries per lane fetched before any product (rows <= 32 entries in one shot)
 
 template <typename T, typename IT>
 __device__ __forceinline__ void patch_correct(const CsrView& A, int p, const int64_t* __restrict__ pptr,
@@ -211,8 +212,21 @@ __device__ __forceinline__ void patch_correct(const CsrView& A, int p, const int
     for (int i0 = 0; i0 < m; i0 += per_pass) {          // uniform trip count: the shuffles see full warps
         const int i = i0 + tid / kRowLanes;
         double acc = 0.0;
-        if (i < m)
-            for (int k = srs[i] + sub; k < sre[i]; k += kRowLanes) acc += A.val[k] * (double)x[A.col[k]];
+        if (i < m) {
+            const int k0 = srs[i] + sub, k1 = sre[i];
+            int c[kRowUnroll];
+            double v[kRowUnroll];
+#pragma unroll
+            for (int u = 0; u < kRowUnroll; u++) {      // all index/value loads first
+                const int k = k0 + u * kRowLanes;
+                c[u] = k < k1 ? __ldg(A.col + k) : -1;
+                v[u] = k < k1 ? __ldg(A.val + k) : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < kRowUnroll; u++)
+                if (c[u] >= 0) acc += v[u] * (double)x[c[u]];
+            for (int k = k0 + kRowUnroll * kRowLanes; k < k1; k += kRowLanes) acc += A.val[k] * (double)x[A.col[k]];
+        }
 #pragma unroll
         for (int o = 1; o < kRowLanes; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if (i < m && sub == 0) sr[i] = (double)b[sdof[i]] - acc;
@@ -221,8 +235,8 @@ __device__ __forceinline__ void patch_correct(const CsrView& A, int p, const int
     const IT* At = inv + inv_off[p];                    // transposed: At[j * m + i] = inverse(i, j)
     for (int i = tid; i < m; i += blockDim.x) {
         double acc = 0.0;
-#pragma unroll 8
-        for (int j = 0; j < m; j++) acc += (double)At[(size_t)j * m + i] * sr[j];
+#pragma unroll 16
+        for (int j = 0; j < m; j++) acc += (double)__ldg(At + (size_t)j * m + i) * sr[j];
         if (direct) {
             const int g = sdof[i];
             x[g] = (T)((double)x[g] + acc * om);
@@ -234,7 +248,7 @@ __device__ __forceinline__ void patch_correct(const CsrView& A, int p, const int
 }
 
 template <typename T, typename IT>
-__global__ void __launch_bounds__(kSchThreads)
+__global__ void __launch_bounds__(kSchThreads, 5)
     k_schwarz_patches(CsrView A, const int* __restrict__ plist, const int64_t* __restrict__ pptr,
                       const int* __restrict__ dofs, const int64_t* __restrict__ inv_off, const IT* __restrict__ inv,
                       const T* b, T* x, double om, double* lsol, int direct, const int* done)
