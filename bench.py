@@ -62,38 +62,66 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 20 ms; summary()
-    keeps the samples taken between mark_start() and mark_end().  When the
-    timed region is shorter than a few sampling periods, extend() keeps the
-    same work running (untimed) until three samples exist after mark_start."""
+    """SM clocks and throttle reasons of the benchmarked GPU sampled every
+    10 ms by NVML (the library behind nvidia-smi; read-only queries) on a
+    background thread; summary() keeps the samples taken between
+    mark_start() and mark_end().  When the timed region is shorter than a
+    few sampling periods, extend() keeps the same work running (untimed)
+    until three samples exist after mark_start().  Without NVML the clocks
+    are reported as unavailable."""
 
-    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
     def __init__(self, device):
         self.device = device
-        self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{device}.csv")
+        self.samples = []          # (time, sm_mhz, max_mhz, power_w, reasons_mask)
         self.t0 = self.t1 = None
         self.extended = False
+        self.source = None
+        self._stop = None
+        self._thread = None
+
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.device)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
 
     def __enter__(self):
+        import threading
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "20"], stdout=self.f,
-                                         stderr=subprocess.DEVNULL)
+            nv, h = self._handle()
+            reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            self._stop = threading.Event()
+
+            def run():
+                while not self._stop.is_set():
+                    try:
+                        self.samples.append((time.time(), nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), mx,
+                                             nv.nvmlDeviceGetPowerUsage(h) / 1000.0, int(reasons(h))))
+                    except Exception:
+                        pass
+                    self._stop.wait(0.01)
+
+            self._thread = threading.Thread(target=run, daemon=True)
+            self._thread.start()
+            self.source = "nvml"
         except Exception:
-            self.proc = None
+            self.source = None
         return self
 
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
-            self.proc.wait()
-            self.f.close()
+        if self._thread:
+            self._stop.set()
+            self._thread.join()
 
     def mark_start(self):
         self.t0 = time.time()
@@ -101,52 +129,31 @@ class ClockSampler:
     def mark_end(self):
         self.t1 = time.time()
 
-    def _rows(self):
-        import datetime
-        rows = []
-        try:
-            self.f.flush()
-            with open(self.path) as f:
-                for line in f:
-                    parts = [p.strip() for p in line.split(",")]
-                    if len(parts) < 10:
-                        continue
-                    try:
-                        ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
-                    except ValueError:
-                        continue
-                    rows.append((ts, parts[1:]))
-        except Exception:
-            pass
-        return rows
+    def _inside(self):
+        t0 = self.t0 if self.t0 is not None else 0.0
+        t1 = self.t1 if self.t1 is not None else time.time()
+        return [r for r in list(self.samples) if t0 - 0.005 <= r[0] <= t1 + 0.005]
 
     def extend(self, fn, min_samples=3, max_s=5.0):
-        if not self.proc or self.t0 is None:
+        if not self.source or self.t0 is None:
             return
         t_stop = time.time() + max_s
-        while time.time() < t_stop:
-            if len([r for r in self._rows() if r[0] >= self.t0 - 0.005]) >= min_samples:
-                break
+        self.t1 = None
+        while time.time() < t_stop and len(self._inside()) < min_samples:
             fn()
             self.extended = True
-        self.t1 = max(self.t1 or 0.0, time.time())
+        self.t1 = time.time()
 
     def summary(self):
-        if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        rows = self._rows()
-        if self.t0 is not None:
-            inside = [r for r in rows if self.t0 - 0.005 <= r[0] <= (self.t1 or time.time()) + 0.005]
-            rows = inside
-        rows = [r[1] for r in rows]
+        if not self.source:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        rows = self._inside()
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
-        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-               "reasons": reasons, "samples": len(rows)}
+        reasons = sorted({name for r in rows for name, bit in self.REASONS if r[4] & bit})
+        out = {"sm_mhz": statistics.median(r[1] for r in rows), "sm_max_mhz": max(r[2] for r in rows),
+               "reasons": reasons, "samples": len(rows), "power_w_median": statistics.median(r[3] for r in rows),
+               "source": self.source}
         if self.extended:
             out["note"] = "timed region shorter than the sampling period: the same solve kept running untimed"
         return out

@@ -140,7 +140,8 @@ typedef struct {
     int cycles;        /* V-cycles per application (MGPreconditionerSpace.cycles, default 3) */
     int use_fmg;       /* 1: FMG correction first (MGPreconditionerInterface.mvMul, :353-379);
                           0: start the V-cycles from the boundary copy only */
-    int precision;     /* 0: FP64 hierarchy; 1: FP32 hierarchy (for mixed-precision solves) */
+    int precision;     /* 0: FP64 hierarchy; 1: FP32 hierarchy (for mixed-precision solves);
+                          2: FP32 hierarchy whose SpMVs read BF16 matrix values (FP32 vectors and sums) */
 } jfg_mg_desc;
 /* Builds a hierarchy from per-level systems A[0..levels) (0 = coarsest),
  * prolongations P[l] (n_{l+1} x n_l, l < levels-1), Dirichlet node lists and

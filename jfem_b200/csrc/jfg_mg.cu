@@ -117,7 +117,7 @@ struct EpiRestrictSweep {
 
 template <typename T>
 void MGImpl<T>::init(Context* ctx, int levels, Matrix* const* As, Matrix* const* Ps, const int* const* bdry,
-                     const int* nbdry, const SmootherDesc* sms, int cycles_, int use_fmg_)
+                     const int* nbdry, const SmootherDesc* sms, int cycles_, int use_fmg_, int bf16)
 {
     c = ctx;
     L = levels;
@@ -147,10 +147,12 @@ void MGImpl<T>::init(Context* ctx, int levels, Matrix* const* As, Matrix* const*
             R[l] = matrix_transpose(P[l]);
         }
         if (std::is_same<T, float>::value) {
-            matrix_ensure_fp32(A[l]);
+            vbf16 = bf16 ? 1 : 0;
+            auto ensure = vbf16 ? matrix_ensure_bf16 : matrix_ensure_fp32;
+            ensure(A[l]);
             if (l < L - 1) {
-                matrix_ensure_fp32(P[l]);
-                matrix_ensure_fp32(R[l]);
+                ensure(P[l]);
+                ensure(R[l]);
             }
         }
         size_t m = (size_t)n[l];
@@ -263,6 +265,21 @@ int MGImpl<T>::max_blocks() const
     return m;
 }
 
+// y-epilogue SpMV on a level matrix in the hierarchy's value type (FP64,
+// FP32, or BF16 values with FP32 vectors)
+template <typename T, int NR, class Epi, class Fin = NoFin>
+static void mg_spmv(const MGImpl<T>& g, cudaStream_t st, const Matrix* M, const T* x, Epi epi, const Scratch& sc,
+                    const int* done, Fin fin = Fin())
+{
+    if constexpr (std::is_same<T, float>::value) {
+        if (g.vbf16) {
+            spmv_launch<__nv_bfloat16, float, NR>(st, M, M->val16.p, x, epi, sc, done, fin);
+            return;
+        }
+    }
+    spmv_launch<T, T, NR>(st, M, vals_of<T>(M), x, epi, sc, done, fin);
+}
+
 template <typename T>
 void MGImpl<T>::coarse(const T* rhs, T* out, const int* done, cudaStream_t st)
 {
@@ -277,7 +294,6 @@ void MGImpl<T>::smooth(int l, const T* rhs, bool xzero, const Scratch& sc, const
 {
     const SmootherDesc& d = sm[l];
     Matrix* M = A[l];
-    const T* val = vals_of<T>(M);
     int m = n[l];
     if (d.runs <= 0) {
         if (xzero) vec_launch<0>(st, m, VZero<T>{x[l].p}, sc, done);
@@ -299,7 +315,7 @@ void MGImpl<T>::smooth(int l, const T* rhs, bool xzero, const Scratch& sc, const
             k = 1;
         }
         for (; k < d.runs; k++) {
-            spmv_launch<T, T, 0>(st, M, val, cur, EpiJacobi<T>{cur, rhs, dinv[l].p, alt, om}, sc, done);
+            mg_spmv<T, 0>(*this, st, M, cur, EpiJacobi<T>{cur, rhs, dinv[l].p, alt, om}, sc, done);
             std::swap(cur, alt);
         }
         if (cur != x[l].p) vec_launch<0>(st, m, VCopy<T>{cur, x[l].p}, sc, done);
@@ -310,7 +326,7 @@ void MGImpl<T>::smooth(int l, const T* rhs, bool xzero, const Scratch& sc, const
     } else {
         if (xzero) vec_launch<0>(st, m, VZero<T>{x[l].p}, sc, done);
         for (int k = 0; k < d.runs; k++) {
-            spmv_launch<T, T, 1>(st, M, val, x[l].p, EpiResid<T>{rhs, r[l].p}, sc, done,
+            mg_spmv<T, 1>(*this, st, M, x[l].p, EpiResid<T>{rhs, r[l].p}, sc, done,
                                  FinSmoothFlag{flags.p + l});
             vec_launch<0>(st, m, VRichardson<T>{r[l].p, x[l].p, (T)d.omega, flags.p + l}, sc, done);
         }
@@ -328,18 +344,18 @@ void MGImpl<T>::vstep(int l, const T* rhs, bool xzero, const Scratch& sc, const 
         return;
     }
     smooth(l, rhs, xzero, sc, done, st, first_sweep_done);
-    spmv_launch<T, T, 0>(st, A[l], vals_of<T>(A[l]), x[l].p, EpiResid<T>{rhs, r[l].p}, sc, done);
+    mg_spmv<T, 0>(*this, st, A[l], x[l].p, EpiResid<T>{rhs, r[l].p}, sc, done);
     const int lc = l - 1;
     const bool fuse_sweep = lc >= 1 && sm[lc].kind == JFG_SMOOTH_JACOBI && sm[lc].runs > 0;
     if (fuse_sweep) {
         T* dst = (sm[lc].runs % 2 == 1) ? x[lc].p : t[lc].p;
-        spmv_launch<T, T, 0>(st, R[lc], vals_of<T>(R[lc]), r[l].p,
+        mg_spmv<T, 0>(*this, st, R[lc], r[l].p,
                              EpiRestrictSweep<T>{mask[lc].p, b[lc].p, dinv[lc].p, dst, (T)sm[lc].omega}, sc, done);
     } else {
-        spmv_launch<T, T, 0>(st, R[lc], vals_of<T>(R[lc]), r[l].p, EpiMasked<T>{mask[lc].p, b[lc].p}, sc, done);
+        mg_spmv<T, 0>(*this, st, R[lc], r[l].p, EpiMasked<T>{mask[lc].p, b[lc].p}, sc, done);
     }
     vstep(lc, b[lc].p, true, sc, done, st, fuse_sweep);
-    spmv_launch<T, T, 0>(st, P[lc], vals_of<T>(P[lc]), x[lc].p, EpiMaskedAdd<T>{mask[l].p, x[l].p}, sc, done);
+    mg_spmv<T, 0>(*this, st, P[lc], x[lc].p, EpiMaskedAdd<T>{mask[l].p, x[l].p}, sc, done);
     smooth(l, rhs, false, sc, done, st);
 }
 
@@ -350,13 +366,13 @@ void MGImpl<T>::fmg_into_top(const T* defect, const Scratch& sc, const int* done
     std::vector<const T*> rh(L);
     rh[L - 1] = defect;
     for (int l = L - 2; l >= 0; l--) {
-        spmv_launch<T, T, 0>(st, R[l], vals_of<T>(R[l]), rh[l + 1], EpiMasked<T>{mask[l].p, fr[l].p}, sc, done);
+        mg_spmv<T, 0>(*this, st, R[l], rh[l + 1], EpiMasked<T>{mask[l].p, fr[l].p}, sc, done);
         rh[l] = fr[l].p;
     }
     for (int l = 0; l < L - 1; l++) {
         vstep(l, rh[l], false, sc, done, st);
         // raw prolongation without boundary zeroing (getProlongationMatrix, line 323)
-        spmv_launch<T, T, 0>(st, P[l], vals_of<T>(P[l]), x[l].p, EpiStore<T>{x[l + 1].p}, sc, done);
+        mg_spmv<T, 0>(*this, st, P[l], x[l].p, EpiStore<T>{x[l + 1].p}, sc, done);
     }
 }
 
@@ -468,7 +484,9 @@ jfg::MGImpl<float>* jfg_mg::fp32()
             nbp[l] = (int)bdry[l].size();
         }
         d32.reset(new jfg::MGImpl<float>());
-        d32->init(ctx, levels, A.data(), P.data(), bp.data(), nbp.data(), sm.data(), cycles, use_fmg);
+        const char* e = getenv("JFEM_MG_BF16");
+        const int bf16 = precision == 2 || (e && e[0] == '1');
+        d32->init(ctx, levels, A.data(), P.data(), bp.data(), nbp.data(), sm.data(), cycles, use_fmg, bf16);
     }
     return d32.get();
 }

@@ -27,6 +27,7 @@ struct MGImpl {
     int L = 0;
     int cycles = 3;
     int use_fmg = 1;
+    int vbf16 = 0;                          // float hierarchy: matrices read as BF16 (FP32 vectors, FP32 sums)
     std::vector<Matrix*> A, P, R;          // A[l], P[l] : n_{l+1} x n_l, R[l] = P[l]^T
     std::vector<int> n;
     std::vector<DevBuf<T>> x, t, b, r, fr;
@@ -47,8 +48,9 @@ struct MGImpl {
     DevBuf<int> zero_flag;                  // a flag that stays 0
 
     // Builds all level data; A/P are borrowed (must outlive the hierarchy).
+    // bf16: (float hierarchy only) SpMVs read BF16 copies of the matrices.
     void init(Context* ctx, int levels, Matrix* const* As, Matrix* const* Ps, const int* const* bdry,
-              const int* nbdry, const SmootherDesc* sms, int cycles_, int use_fmg_);
+              const int* nbdry, const SmootherDesc* sms, int cycles_, int use_fmg_, int bf16 = 0);
 
     // out = M v (the preconditioner application).  v and out are device
     // vectors of the finest size; `done` is an optional skip flag.

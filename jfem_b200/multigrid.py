@@ -50,7 +50,8 @@ class MGPreconditioner(VectorMultiplyable):
     boundary[l]: Dirichlet node lists; smoothers[l] for l >= 1 (entry 0 may be
     None).  cycles / use_fmg follow MGPreconditionerInterface.mvMul; the plain
     one-V-cycle preconditioner is cycles=1, use_fmg=False.
-    precision="mixed" also builds the FP32 hierarchy used by mixed solves.
+    precision="mixed" also builds the FP32 hierarchy used by mixed solves;
+    "mixed-bf16" builds it with BF16 matrix values (FP32 vectors and sums).
     """
 
     def __init__(self, systems, prolongations, boundary, smoothers, cycles=3, use_fmg=True, precision="fp64",
@@ -76,7 +77,10 @@ class MGPreconditioner(VectorMultiplyable):
         Ph = (C.c_void_p * max(L, 1))(*([p.handle for p in self._P] + [None]))
         Bh = (C.POINTER(C.c_int) * L)(*[N.iptr(b) for b in self._bd])
         nb = np.array([b.size for b in self._bd], dtype=np.int32)
-        desc = N.MGDesc(int(cycles), 1 if use_fmg else 0, 1 if precision == "mixed" else 0)
+        levels = {"fp64": 0, "mixed": 1, "mixed-bf16": 2}
+        if precision not in levels:
+            raise IllegalArgumentException(f"unknown hierarchy precision {precision!r}")
+        desc = N.MGDesc(int(cycles), 1 if use_fmg else 0, levels[precision])
         h = C.c_void_p()
         st = N.load().jfg_mg_create(self.ctx.handle, L, Ah, Ph, Bh, N.iptr(nb), descs, C.byref(desc), C.byref(h))
         if st == N.ERR_BAD_ARG:

@@ -245,3 +245,20 @@ def test_pcg_mg_full_size(ctx):
         assert s2.last.status == N.OK and s2.last.final_residual <= tol, mode
         assert rel(x32, x64) < 1e-7, mode
     assert it64 <= 20
+
+
+def test_pcg_bf16_vcycle(ctx):
+    """FP64 PCG with the FP32 V-cycle reading BF16 matrices (hierarchy
+    precision "mixed-bf16"): same FP64 true residual, at most one extra
+    iteration over the FP64 preconditioner."""
+    h = mg_levels(2, 4, 6, modes=16, seed=3)    # Q2 128x128
+    mats_o, mg_o, mats, mg = _mg_pair(h, ctx, (O.SMOOTH_JACOBI, 2, 2.0 / 3.0), 1, False, precision="mixed-bf16")
+    b = h.finest.rhs
+    tol = 1e-8 * np.linalg.norm(b)
+    ref = O.solve_pcg(mats_o[-1], mg_o, b, tol)
+    s = IterativeSolver(ctx=ctx)
+    s.precision = "mixed-precond"
+    x = s.solvePCG(mats[-1], mg, b, tol)
+    assert s.last.status == N.OK and s.last.final_residual <= tol
+    assert rel(x, ref.x) < 1e-7
+    assert s.iterations <= ref.iterations + 1
