@@ -4,7 +4,9 @@
 //
 // Layout in HBM: patch p's sorted DOF list is dofs[pptr[p] .. pptr[p+1]) and
 // the transpose of the m_p x m_p inverse of R_p A R_p^T sits at inv + inv_off[p]
-// (column-major inverse).
+// (column-major inverse).  Patches whose local operators are identical (the
+// interior patches of a structured grid) share one inverse, found by hashing
+// the local matrices, so the inverses the sweeps stream stay in L2.
 // One sweep step over a colour is one launch with a CTA per patch: the CTA
 // gathers the patch rows of b - A x straight from A's CSR rows (no global
 // residual vector), multiplies by the patch inverse (warp per row, coalesced
@@ -16,7 +18,9 @@
 // keeps the reference's order of additions.
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <numeric>
+#include <tuple>
 
 #include "jfg_krylov.cuh"
 #include "jfg_schwarz.cuh"
@@ -41,8 +45,9 @@ struct CsrView {
 // the column interchanges undone in reverse order at the end.
 template <bool SMEM>
 __global__ void __launch_bounds__(kSchThreads)
-    k_patch_inverse(int mcap, CsrView A, const int64_t* __restrict__ pptr, const int* __restrict__ dofs,
-                    const int64_t* __restrict__ inv_off, double* __restrict__ inv, int* __restrict__ status)
+    k_patch_inverse(int mcap, CsrView A, const int* __restrict__ plist, const int64_t* __restrict__ pptr,
+                    const int* __restrict__ dofs, const int64_t* __restrict__ inv_off, double* __restrict__ inv,
+                    int* __restrict__ status)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     double* Ms = reinterpret_cast<double*>(smraw);
@@ -53,7 +58,7 @@ __global__ void __launch_bounds__(kSchThreads)
     __shared__ double wv[kSchThreads / 32];
     __shared__ int wi[kSchThreads / 32];
     __shared__ int s_sing;
-    const int p = blockIdx.x;
+    const int p = plist[blockIdx.x];
     const int64_t off = pptr[p];
     const int m = (int)(pptr[p + 1] - off);
     double* M = SMEM ? Ms : inv + inv_off[p];
@@ -178,7 +183,70 @@ __global__ void __launch_bounds__(kSchThreads)
             }
         }
     }
-    if (tid == 0) status[p] = s_sing;
+    if (tid == 0) status[blockIdx.x] = s_sing;
+}
+
+// Two 64-bit hashes of R A R^T per patch (entries in row order, columns
+// ascending), so that patches with identical local operators share one
+// inverse: on structured grids every interior patch has the same matrix.
+__device__ __forceinline__ uint64_t mix64(uint64_t h, uint64_t v, uint64_t k1, uint64_t k2)
+{
+    h ^= v + 0x9e3779b97f4a7c15ULL + (h << 6) + (h >> 2);
+    h ^= h >> 31;
+    h *= k1;
+    h ^= h >> 29;
+    h *= k2;
+    h ^= h >> 32;
+    return h;
+}
+
+__global__ void __launch_bounds__(kSchThreads)
+    k_patch_hash(CsrView A, const int64_t* __restrict__ pptr, const int* __restrict__ dofs, uint64_t* __restrict__ out)
+{
+    __shared__ int sdof[kMaxPatch];
+    __shared__ uint64_t rh[2][kMaxPatch];
+    const int p = blockIdx.x;
+    const int64_t off = pptr[p];
+    const int m = (int)(pptr[p + 1] - off);
+    for (int i = threadIdx.x; i < m; i += blockDim.x) sdof[i] = dofs[off + i];
+    __syncthreads();
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        uint64_t h1 = 0x1234567ULL + (uint64_t)i, h2 = 0x89abcdefULL ^ ((uint64_t)i << 20);
+        const int g = sdof[i];
+        for (int k = A.rp[g]; k < A.rp[g + 1]; k++) {
+            const int c = A.col[k];
+            int lo = 0, hi = m - 1, j = -1;
+            while (lo <= hi) {
+                const int mid = (lo + hi) >> 1;
+                const int v = sdof[mid];
+                if (v == c) {
+                    j = mid;
+                    break;
+                }
+                if (v < c)
+                    lo = mid + 1;
+                else
+                    hi = mid - 1;
+            }
+            if (j < 0) continue;
+            const uint64_t bits = (uint64_t)__double_as_longlong(A.val[k]);
+            const uint64_t key = ((uint64_t)(uint32_t)j << 32) ^ (uint64_t)(uint32_t)i;
+            h1 = mix64(mix64(h1, key, 0xbf58476d1ce4e5b9ULL, 0x94d049bb133111ebULL), bits, 0xbf58476d1ce4e5b9ULL,
+                       0x94d049bb133111ebULL);
+            h2 = mix64(mix64(h2, bits, 0x7fb5d329728ea185ULL, 0x81dadef4bc2dd44dULL), key, 0x7fb5d329728ea185ULL,
+                       0x81dadef4bc2dd44dULL);
+        }
+        rh[0][i] = h1;
+        rh[1][i] = h2;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        const uint64_t k1 = threadIdx.x ? 0x7fb5d329728ea185ULL : 0xbf58476d1ce4e5b9ULL;
+        const uint64_t k2 = threadIdx.x ? 0x81dadef4bc2dd44dULL : 0x94d049bb133111ebULL;
+        uint64_t h = (uint64_t)m * 0x100000001b3ULL;
+        for (int i = 0; i < m; i++) h = mix64(h, rh[threadIdx.x][i], k1, k2);
+        out[2 * (size_t)p + threadIdx.x] = h;
+    }
 }
 
 // One patch: local residual rows of b - A x, times the patch inverse; either
@@ -393,38 +461,76 @@ void SchwarzImpl::init(Context* ctx, Matrix* Am, int kind_, double omega_, int n
         hoff[p + 1] = hoff[p] + m * m;
     }
     total_m = hp[np];
-    total_inv = hoff[np];
     pptr.alloc(np + 1);
     inv_off.alloc(np);
     dofs.alloc(total_m);
-    inv.alloc(total_inv);
     flag.alloc(1);
     JFG_CUDA(cudaMemcpyAsync(pptr.p, hp.data(), sizeof(int64_t) * (np + 1), cudaMemcpyHostToDevice, st));
-    JFG_CUDA(cudaMemcpyAsync(inv_off.p, hoff.data(), sizeof(int64_t) * np, cudaMemcpyHostToDevice, st));
     JFG_CUDA(cudaMemcpyAsync(dofs.p, hd.data(), sizeof(int) * total_m, cudaMemcpyHostToDevice, st));
-    // DirectSolver: every patch inverse up front
-    DevBuf<int> pstat;
-    pstat.alloc(np);
+    // DirectSolver: every distinct patch operator is inverted once, up front
+    std::vector<int> reps;                     // patches whose inverse is computed
+    std::vector<int64_t> hoff2(np);
+    const char* ed = getenv("JFEM_SCHWARZ_DEDUP");
+    if (!(ed && ed[0] == '0')) {
+        DevBuf<uint64_t> hh;
+        hh.alloc(2 * (size_t)np);
+        k_patch_hash<<<np, kSchThreads, 0, st>>>(csr_of(A), pptr.p, dofs.p, hh.p);
+        JFG_CUDA(cudaGetLastError());
+        note_launch();
+        std::vector<uint64_t> h(2 * (size_t)np);
+        JFG_CUDA(cudaMemcpyAsync(h.data(), hh.p, sizeof(uint64_t) * h.size(), cudaMemcpyDeviceToHost, st));
+        JFG_CUDA(cudaStreamSynchronize(st));
+        std::map<std::tuple<int64_t, uint64_t, uint64_t>, int64_t> seen;
+        int64_t tot = 0;
+        for (int p = 0; p < np; p++) {
+            const int64_t m = hp[p + 1] - hp[p];
+            auto key = std::make_tuple(m, h[2 * (size_t)p], h[2 * (size_t)p + 1]);
+            auto it = seen.find(key);
+            if (it == seen.end()) {
+                seen.emplace(key, tot);
+                hoff2[p] = tot;
+                reps.push_back(p);
+                tot += m * m;
+            } else {
+                hoff2[p] = it->second;
+            }
+        }
+        total_inv = tot;
+    } else {
+        for (int p = 0; p < np; p++) {
+            hoff2[p] = hoff[p];
+            reps.push_back(p);
+        }
+        total_inv = hoff[np];
+    }
+    nunique = (int)reps.size();
+    inv.alloc(total_inv);
+    JFG_CUDA(cudaMemcpyAsync(inv_off.p, hoff2.data(), sizeof(int64_t) * np, cudaMemcpyHostToDevice, st));
+    DevBuf<int> pstat, d_reps;
+    pstat.alloc(reps.size());
+    d_reps.alloc(reps.size());
+    JFG_CUDA(cudaMemcpyAsync(d_reps.p, reps.data(), sizeof(int) * reps.size(), cudaMemcpyHostToDevice, st));
     const bool smem = max_m <= kSmemInvMax;
     const int mcap = max_m;
+    const unsigned nr = (unsigned)reps.size();
     size_t dyn = (smem ? (size_t)mcap * mcap * sizeof(double) : 0) + 2 * (size_t)mcap * sizeof(double) +
                  2 * (size_t)mcap * sizeof(int);
     if (smem) {
         JFG_CUDA(cudaFuncSetAttribute(k_patch_inverse<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-        k_patch_inverse<true><<<np, kSchThreads, dyn, st>>>(mcap, csr_of(A), pptr.p, dofs.p, inv_off.p, inv.p,
-                                                            pstat.p);
+        k_patch_inverse<true><<<nr, kSchThreads, dyn, st>>>(mcap, csr_of(A), d_reps.p, pptr.p, dofs.p, inv_off.p,
+                                                            inv.p, pstat.p);
     } else {
         JFG_CUDA(cudaFuncSetAttribute(k_patch_inverse<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
-        k_patch_inverse<false><<<np, kSchThreads, dyn, st>>>(mcap, csr_of(A), pptr.p, dofs.p, inv_off.p, inv.p,
-                                                             pstat.p);
+        k_patch_inverse<false><<<nr, kSchThreads, dyn, st>>>(mcap, csr_of(A), d_reps.p, pptr.p, dofs.p, inv_off.p,
+                                                             inv.p, pstat.p);
     }
     JFG_CUDA(cudaGetLastError());
     note_launch();
-    std::vector<int> hs(np);
-    JFG_CUDA(cudaMemcpyAsync(hs.data(), pstat.p, sizeof(int) * np, cudaMemcpyDeviceToHost, st));
+    std::vector<int> hs(reps.size());
+    JFG_CUDA(cudaMemcpyAsync(hs.data(), pstat.p, sizeof(int) * hs.size(), cudaMemcpyDeviceToHost, st));
     JFG_CUDA(cudaStreamSynchronize(st));
-    for (int p = 0; p < np; p++)
-        JFG_CHECK(hs[p] == 0, JFG_ERR_SINGULAR, "a patch matrix is singular (patch " + std::to_string(p) + ")");
+    for (size_t q = 0; q < reps.size(); q++)
+        JFG_CHECK(hs[q] == 0, JFG_ERR_SINGULAR, "a patch matrix is singular (patch " + std::to_string(reps[q]) + ")");
 
     std::vector<int> h_touched;
     std::vector<int64_t> h_tptr, h_slots;

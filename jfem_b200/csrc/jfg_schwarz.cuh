@@ -20,6 +20,7 @@ struct SchwarzImpl {
     int np = 0;
     int max_m = 0;
     int64_t total_m = 0, total_inv = 0;
+    int nunique = 0;                    // distinct patch operators (inverses stored)
     uint64_t uid = next_uid();
     DevBuf<int64_t> pptr, inv_off;      // patch p: dofs[pptr[p], pptr[p+1]), inverse at inv + inv_off[p]
     DevBuf<int> dofs;

@@ -195,3 +195,20 @@ def test_schwarz_preconditioned_krylov(ctx):
     assert s3.last.status == N.OK
     # left preconditioning: the tolerance applies to the preconditioned residual
     assert np.linalg.norm(b - coo_oracle(sy).mvmul(x3)) <= 1e-6 * np.linalg.norm(b)
+
+
+def test_shared_inverses_for_identical_patches(ctx, monkeypatch):
+    """Interior patches of a uniform grid have identical local operators and
+    share one inverse; the result is bit-identical to one inverse per patch."""
+    sp, sy = fe_system(2, 16)
+    _, patches = cartesian_patch_dofs(sp, (8, 8), 1)
+    cols = nine_colours((8, 8))
+    S1 = UpFrontSchwarz(dev(sy, ctx), patches, ColoredMultiplicativeSubspaceCorrection(1.0), colours=cols)
+    monkeypatch.setenv("JFEM_SCHWARZ_DEDUP", "0")
+    S2 = UpFrontSchwarz(dev(sy, ctx), patches, ColoredMultiplicativeSubspaceCorrection(1.0), colours=cols)
+    e1, e2 = S1.info()["inverse_entries"], S2.info()["inverse_entries"]
+    assert e1 < e2 / 4
+    x0 = np.random.default_rng(9).standard_normal(sy.n)
+    assert np.array_equal(S1.apply(x0, sy.rhs), S2.apply(x0, sy.rhs))
+    for i in (0, 9, 27, 63):
+        assert np.array_equal(S1.localInverse(i), S2.localInverse(i))
