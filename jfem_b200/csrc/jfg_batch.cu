@@ -141,7 +141,7 @@ __device__ __forceinline__ float sell_row32(const int* off, const int* col, cons
     return sum;
 }
 
-__global__ void __launch_bounds__(512) k_batch_heat(BatchParams P)
+__global__ void __launch_bounds__(512, 2) k_batch_heat(BatchParams P)
 {
     cg::cluster_group cl = cg::this_cluster();
     __shared__ double sh[64];
@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(512) k_batch_heat(BatchParams P)
         const int si = *cl.map_shared_rank(&sys_sh, 0);
         cl.sync();   // everyone has read the leader's slot before it is reused
         if (si < 0) break;
-        const SysDesc S = P.sys[si];
+        const SysDesc& S = P.sys[si];   // fields re-read from L1 rather than pinned in registers
         // this CTA's slots
         const int chunk = ((S.nslots / 32 + C - 1) / C) * 32;
         const int s0 = min(S.nslots, (int)rank * chunk), s1 = min(S.nslots, s0 + chunk);
