@@ -51,7 +51,8 @@ def parse():
     ap.add_argument("--cells", type=int, default=CELLS)
     ap.add_argument("--levels", type=int, default=LEVELS)
     ap.add_argument("--workload", default="gmg-pcg", choices=["gmg-pcg", "batch-heat", "stokes", "learned"])
-    ap.add_argument("--profile", default=None, choices=["solve-fp64", "solve-mixed", "spmv64", "spmv32"],
+    ap.add_argument("--profile", default=None,
+                    choices=["solve-fp64", "solve-mixed", "solve-mixed-nograph", "spmv64", "spmv32"],
                     help="set up, run the named operation --warmup + 1 times and exit (for ncu captures)")
     return ap.parse_args()
 
@@ -220,6 +221,8 @@ def run_ours(args):
         with torch.cuda.stream(stream):
             dx.copy_(e0)           # the reference's start vector e0
         o = opts(precision)
+        if args.profile == "solve-mixed-nograph":
+            o.use_graph = 0        # plain launches: every kernel of the solve is visible to a profiler
         st = N.load().jfg_solve_dev(ctx.handle, N.PCG, A.handle, N.PREC_MG, mg.handle, C.c_void_p(db.data_ptr()),
                                     C.c_void_p(dx.data_ptr()), C.byref(o), C.byref(info))
         ctx.check(st)
@@ -262,7 +265,7 @@ def run_ours(args):
         for _ in range(args.warmup + 1):
             if args.profile == "solve-fp64":
                 solve_dev(N.FP64)
-            elif args.profile == "solve-mixed":
+            elif args.profile in ("solve-mixed", "solve-mixed-nograph"):
                 solve_dev(HEADLINE)
             else:
                 A.time_spmv(precision=1 if args.profile == "spmv32" else 0, iters=1)

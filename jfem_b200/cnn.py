@@ -168,3 +168,23 @@ def pixel_map(space):
     """(H, W, dof_of_pixel) of a Q_p space's node grid: pixel (gx, gy) at
     row-major index gx * W + gy holds unknown node_of_grid[gx * W + gy]."""
     return space.nx, space.ny, np.ascontiguousarray(space.node_of_grid, dtype=np.int32)
+
+
+def main(argv=None):
+    """python -m jfem_b200.cnn B H W [iters]: times the forward pass on random
+    input (CUDA events inside the library) and prints ms and TFLOP/s."""
+    import json
+    import sys
+    a = [int(v) for v in (argv if argv is not None else sys.argv[1:])]
+    B, H, W = a[:3]
+    iters = a[3] if len(a) > 3 else 20
+    net = LearnedSmoother(N.default_context(), weights=he_init(0))
+    tot, mid = net.time_forward(B, H, W, iters)
+    flops = 2.0 * sum(int(np.prod(s)) for s in SHAPES) * B * H * W
+    mid_flops = 2.0 * 9 * 32 * 32 * B * H * W
+    print(json.dumps({"pixels": B * H * W, "forward_ms": tot, "forward_tflops": flops / (tot * 1e-3) / 1e12,
+                      "mid_layer_ms": mid, "mid_layer_tflops": mid_flops / (mid * 1e-3) / 1e12}))
+
+
+if __name__ == "__main__":
+    main()

@@ -44,6 +44,7 @@ using namespace jfg;
 struct SysDesc {
     int n, nslots;
     const int *k_off, *k_perm, *k_col;
+    const int16_t* k_col16;      // 16-bit column offsets from the row, or null
     const double* k_v64;
     const float* k_v32;
     const int *m_off, *m_perm, *m_col;
@@ -123,21 +124,41 @@ __device__ __forceinline__ double sell_row(const int* off, const int* col, const
     for (int k = 0; k < len; k++) sum += (double)val[o + 32 * k + lane] * (double)x[col[o + 32 * k + lane]];
     return sum;
 }
-__device__ __forceinline__ float sell_row32(const int* off, const int* col, const float* val, const float* x, int slot)
+__device__ __forceinline__ float sell_row32(const int* off, const int* col, const int16_t* col16, const float* val,
+                                            const float* x, int slot, int row)
 {
     const int s = slot >> 5, lane = slot & 31;
     const int o = off[s];
     const int len = (off[s + 1] - o) >> 5;
+    const float* vp = val + o + lane;
     float sum = 0;
     int k = 0;
-    for (; k + 2 <= len; k += 2) {
-        const int c0 = col[o + 32 * k + lane], c1 = col[o + 32 * (k + 1) + lane];
-        const float v0 = val[o + 32 * k + lane], v1 = val[o + 32 * (k + 1) + lane];
-        const float x0 = x[c0], x1 = x[c1];
+    if (col16) {            // 2 bytes per entry instead of 4
+        const int16_t* cp = col16 + o + lane;
+        for (; k + 4 <= len; k += 4) {
+            const int c0 = row + cp[32 * k], c1 = row + cp[32 * (k + 1)];
+            const int c2 = row + cp[32 * (k + 2)], c3 = row + cp[32 * (k + 3)];
+            const float v0 = vp[32 * k], v1 = vp[32 * (k + 1)], v2 = vp[32 * (k + 2)], v3 = vp[32 * (k + 3)];
+            const float x0 = x[c0], x1 = x[c1], x2 = x[c2], x3 = x[c3];
+            sum += v0 * x0;
+            sum += v1 * x1;
+            sum += v2 * x2;
+            sum += v3 * x3;
+        }
+        for (; k < len; k++) sum += vp[32 * k] * x[row + cp[32 * k]];
+        return sum;
+    }
+    const int* cp = col + o + lane;
+    for (; k + 4 <= len; k += 4) {
+        const int c0 = cp[32 * k], c1 = cp[32 * (k + 1)], c2 = cp[32 * (k + 2)], c3 = cp[32 * (k + 3)];
+        const float v0 = vp[32 * k], v1 = vp[32 * (k + 1)], v2 = vp[32 * (k + 2)], v3 = vp[32 * (k + 3)];
+        const float x0 = x[c0], x1 = x[c1], x2 = x[c2], x3 = x[c3];
         sum += v0 * x0;
         sum += v1 * x1;
+        sum += v2 * x2;
+        sum += v3 * x3;
     }
-    for (; k < len; k++) sum += val[o + 32 * k + lane] * x[col[o + 32 * k + lane]];
+    for (; k < len; k++) sum += vp[32 * k] * x[cp[32 * k]];
     return sum;
 }
 
@@ -227,7 +248,7 @@ __global__ void __launch_bounds__(512, 2) k_batch_heat(BatchParams P)
                     for (int slot_i = s0 + threadIdx.x; slot_i < s1; slot_i += blockDim.x) {
                         const int row = S.k_perm[slot_i];
                         if (row < 0) continue;
-                        const float q = sell_row32(S.k_off, S.k_col, S.k_v32, S.z, slot_i);
+                        const float q = sell_row32(S.k_off, S.k_col, S.k_col16, S.k_v32, S.z, slot_i, row);
                         const float pn = S.z[row] + bf * S.p[row];
                         const float apn = q + bf * S.Ap[row];
                         S.p[row] = pn;
@@ -320,6 +341,7 @@ void build_desc(jfg_batch* b, bool with_f)
         d.k_off = K->off.p;
         d.k_perm = K->perm.p;
         d.k_col = K->col.p;
+        d.k_col16 = K->idx16 ? K->col16.p : nullptr;
         d.k_v64 = K->val.p;
         d.k_v32 = K->val32.p;
         d.m_off = M->off.p;
