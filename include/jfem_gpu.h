@@ -200,6 +200,9 @@ typedef struct {
     int graph_chunk;       /* iterations per graph launch between convergence polls (default 8) */
     double* h_history;     /* optional: residual norm per iteration */
     int history_cap;
+    int start;             /* jfg_solve: 0 = x holds the start iterate (copied in, e.g. lastSolution);
+                              1 = start from e0 (IterativeSolver.java:69-70) and 2 = from zero, without
+                              reading x (one host-to-device copy fewer) */
 } jfg_solver_opts;
 
 typedef struct {

@@ -55,7 +55,8 @@ class MGDesc(C.Structure):
 class SolverOpts(C.Structure):
     _fields_ = [("tol", C.c_double), ("maxit", C.c_int), ("restart", C.c_int), ("max_restarts", C.c_int),
                 ("precision", C.c_int), ("inner_rtol", C.c_double), ("use_graph", C.c_int),
-                ("graph_chunk", C.c_int), ("h_history", C.POINTER(C.c_double)), ("history_cap", C.c_int)]
+                ("graph_chunk", C.c_int), ("h_history", C.POINTER(C.c_double)), ("history_cap", C.c_int),
+                ("start", C.c_int)]
 
 
 class SolveInfo(C.Structure):

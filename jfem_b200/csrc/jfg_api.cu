@@ -67,6 +67,20 @@ void stage_out(jfg_ctx* ctx, const double* d, double* h, size_t n)
     JFG_CUDA(cudaStreamSynchronize(ctx->c.stream));
 }
 
+__global__ void k_start_vector(int n, double* x, int e0)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        x[i] = (e0 && i == 0) ? 1.0 : 0.0;
+}
+// x = e0 (start 1) or 0 (start 2) on the device
+void set_start(jfg_ctx* ctx, double* x, int n, int start)
+{
+    if (n <= 0) return;
+    k_start_vector<<<std::min((n + 255) / 256, jfg::kVecGrid), 256, 0, ctx->c.stream>>>(n, x, start == 1);
+    JFG_CUDA(cudaGetLastError());
+    jfg::note_launch();
+}
+
 jfg::Scratch ctx_scratch(jfg_ctx* ctx, int max_blocks)
 {
     ctx->work.c = &ctx->c;
@@ -698,7 +712,11 @@ int jfg_solve_dev(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, const do
         o = *opts;
     else
         jfg_solver_opts_default(&o);
-    return guard(ctx, [&]() -> int { return solve_impl(ctx, kind, A, pk, ph, d_b, d_x, &o, info); });
+    if (o.start < 0 || o.start > 2) return JFG_ERR_BAD_ARG;
+    return guard(ctx, [&]() -> int {
+        if (o.start != 0) set_start(ctx, d_x, A->m->rows, o.start);
+        return solve_impl(ctx, kind, A, pk, ph, d_b, d_x, &o, info);
+    });
 }
 
 int jfg_solve(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, const double* h_b, double* h_x,
@@ -710,10 +728,16 @@ int jfg_solve(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, const double
         o = *opts;
     else
         jfg_solver_opts_default(&o);
+    if (o.start < 0 || o.start > 2) return JFG_ERR_BAD_ARG;
     return guard(ctx, [&]() -> int {
         int n = A->m->rows;
         stage_in(ctx, ctx->stage_a, h_b, n);
-        stage_in(ctx, ctx->stage_b, h_x, n);
+        if (o.start == 0) {
+            stage_in(ctx, ctx->stage_b, h_x, n);
+        } else {       // e0 or zero, made on the device
+            ctx->stage_b.alloc(n);
+            set_start(ctx, ctx->stage_b.p, n, o.start);
+        }
         int st = solve_impl(ctx, kind, A, pk, ph, ctx->stage_a.p, ctx->stage_b.p, &o, info);
         stage_out(ctx, ctx->stage_b.p, h_x, n);
         return st;

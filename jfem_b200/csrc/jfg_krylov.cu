@@ -108,6 +108,39 @@ struct VXpby {       // p = z + p*beta
     const Ctl* c;
     template <int K> __device__ void operator()(int i, double (&)[K]) const { p[i] = z[i] + p[i] * (T)c->beta; }
 };
+// FP64 PCG with an FP32 multigrid preconditioner: the r -> FP32 copy is
+// written by the update kernel and z is consumed in FP32 (widened exactly
+// inside the dot and the direction update), which gives bit-identical
+// iterates without two cast kernels and the FP64 z vector per iteration.
+struct VCGUpdate32 {  // VCGUpdate<double> and r32 = (float) r
+    double* x;
+    const double* p;
+    double* r;
+    const double* Ap;
+    float* r32;
+    const Ctl* c;
+    template <int K> __device__ void operator()(int i, double (&acc)[K]) const
+    {
+        double a = c->alpha;
+        x[i] = x[i] + p[i] * a;
+        double rn = r[i] - Ap[i] * a;
+        r[i] = rn;
+        r32[i] = (float)rn;
+        acc[0] += rn * rn;
+    }
+};
+struct VDotMixed {    // acc += r . (double) z32
+    const double* r;
+    const float* z;
+    template <int K> __device__ void operator()(int i, double (&acc)[K]) const { acc[0] += r[i] * (double)z[i]; }
+};
+struct VXpby32 {      // p = (double) z32 + p * beta
+    const float* z;
+    double* p;
+    const Ctl* c;
+    template <int K> __device__ void operator()(int i, double (&)[K]) const { p[i] = (double)z[i] + p[i] * c->beta; }
+};
+
 template <typename T>
 struct VJacobiPre {  // z = dinv * r
     const T* d;
@@ -662,8 +695,18 @@ int run_cg(SolverWork& w, int ci, Matrix* A, const Precond<T>& M, const T* b, T*
     } else {
         vec_copy<T>(st, n, r, p, sc, done);
     }
+    const bool fused32 = std::is_same<T, double>::value && M.kind == JFG_PREC_MG && M.mg32 && !M.hook;
     auto iter = [&]() {
         spmv_launch<T, T, 1>(st, A, val, p, EpiStoreDot<T>{Ap, p}, sc, done, FinAlpha{c});
+        if constexpr (std::is_same<T, double>::value) {
+            if (fused32) {
+                vec_launch<1>(st, n, VCGUpdate32{x, p, r, Ap, M.r32, c}, sc, done, FinCGRes{c, 1});
+                M.mg32->apply(M.r32, M.z32, sc, done, st);
+                vec_launch<1>(st, n, VDotMixed{r, M.z32}, sc, done, FinBeta{c});
+                vec_launch<0>(st, n, VXpby32{M.z32, p, c}, sc, done);
+                return;
+            }
+        }
         vec_launch<1>(st, n, VCGUpdate<T>{x, p, r, Ap, c}, sc, done, FinCGRes{c, pcg ? 1 : 0});
         if (pcg) {
             M.apply(r, z, sc, done, st);

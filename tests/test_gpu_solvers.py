@@ -262,3 +262,27 @@ def test_pcg_bf16_vcycle(ctx):
     assert s.last.status == N.OK and s.last.final_residual <= tol
     assert rel(x, ref.x) < 1e-7
     assert s.iterations <= ref.iterations + 1
+
+
+def test_start_modes(ctx):
+    """opts.start = 1 (e0) and 2 (zero) give the same solve as passing that
+    start vector in x (start = 0)."""
+    import ctypes as C
+    sp, sy = fe_system(1, 24)
+    A = dev(sy, ctx)
+    b = sy.rhs
+    n = sy.n
+    for start, x0 in ((1, np.eye(1, n, 0)[0]), (2, np.zeros(n))):
+        outs = []
+        for mode in (0, start):
+            o = N.SolverOpts()
+            N.load().jfg_solver_opts_default(C.byref(o))
+            o.tol = 1e-10 * np.linalg.norm(b)
+            o.start = mode
+            x = x0.copy() if mode == 0 else np.full(n, np.nan)
+            info = N.SolveInfo()
+            ctx.check(N.load().jfg_solve(ctx.handle, N.CG, A.handle, N.PREC_NONE, None, N.dptr(N.f64(b)),
+                                         N.dptr(x), C.byref(o), C.byref(info)))
+            outs.append((x, info.iterations))
+        assert outs[0][1] == outs[1][1]
+        assert np.array_equal(outs[0][0], outs[1][0])
