@@ -58,8 +58,8 @@ def parse():
 
 
 def dist_env():
-    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
-        os.environ.get("LOCAL_RANK", "0"))
+    from jfem_b200.replicas import dist_env as de
+    return de()
 
 
 class ClockSampler:
@@ -172,11 +172,9 @@ def spmv_bytes(n, nnz, sval, sx):
 
 def run_ours(args):
     import torch
-    rank, world, local = dist_env()
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
-                                timeout=__import__("datetime").timedelta(seconds=600))
+    from jfem_b200.replicas import Replicas
+    reps = Replicas(timeout_s=120)
+    rank, world, local = reps.rank, reps.world, reps.local
     torch.cuda.set_device(local)
     os.environ["JFEM_DEVICE"] = str(local)
     from jfem_b200 import IterativeSolver, JacobiSmoother, MGPreconditioner
@@ -229,17 +227,10 @@ def run_ours(args):
         return info.iterations, info.final_residual, info.outer_iterations
 
     def barrier():
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
+        reps.barrier()
 
     def max_over_ranks(v):
-        if world == 1:
-            return v
-        import torch.distributed as dist
-        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reps.max(v)
 
     def timed(fn, steps, warmup, clk=None):
         for _ in range(warmup):
@@ -371,9 +362,7 @@ def run_ours(args):
             "setup_s": setup_s,
         }
         print(json.dumps(line))
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    reps.close()
 
 
 def cpu_baseline(h, tol, iters_hint):
