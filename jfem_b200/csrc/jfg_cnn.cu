@@ -8,7 +8,10 @@
 //   h5 = relu(h3 + conv5(a4))    32 -> 32
 //   y  = conv6(h5)               32 -> 1   (FP32 CUDA cores)
 //
-// The 32 -> 32 convolutions are implicit GEMMs (M = pixels, N = 32,
+// The forward 32 -> 32 convolutions run on tcgen05 with TMEM accumulators
+// (jfg_cnn_tc.cu).  The kernels below are the mma.sync versions: the input
+// gradients of the backward pass, and the forward when JFEM_CNN_TC=0.  They
+// are implicit GEMMs (M = pixels, N = 32,
 // K = 9 taps x 32 channels) on mma.sync m16n8k16 BF16 with FP32 accumulators:
 // a CTA stages an 18x18 halo of NHWC activations and the 32x288 weights in
 // shared memory (padded rows, conflict-free ldmatrix) and each warp computes
@@ -483,6 +486,9 @@ __global__ void k_adam(int n, float* __restrict__ w, const float* __restrict__ g
 }
 
 }  // namespace
+
+void conv_mid_tc(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* in, const __nv_bfloat16* wk,
+                 const __nv_bfloat16* skip, __nv_bfloat16* out, int* err);
 }  // namespace jfg
 
 // ---------------------------------------------------------------------------
@@ -503,6 +509,7 @@ struct jfg_cnn {
     jfg::DevBuf<double> loss;
     jfg::DevBuf<double> partials;
     jfg::DevBuf<unsigned> counter;
+    jfg::DevBuf<int> tc_err;        // set by the tensor-core convolution when an MMA wait timed out
     size_t cap = 0;
     int adam_t = 0;
     bool packed = false;
@@ -538,6 +545,15 @@ void cnn_pack(jfg_cnn* n, cudaStream_t st)
     n->packed = true;
 }
 
+// synchronises the stream; a timed-out tensor-core wait becomes an error
+void cnn_check_tc(jfg_cnn* n, cudaStream_t st)
+{
+    int h = 0;
+    JFG_CUDA(cudaMemcpyAsync(&h, n->tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    JFG_CUDA(cudaStreamSynchronize(st));
+    JFG_CHECK(h == 0, JFG_ERR_CUDA, "tensor-core convolution: an MMA wait timed out");
+}
+
 inline unsigned grid1d(size_t n) { return (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16); }
 
 template <typename InT, typename OutT, int SK, bool RELU, bool OMASK>
@@ -560,6 +576,14 @@ void wgrad_mid(jfg_cnn* n, cudaStream_t st, int B, int H, int W, const float* G,
     note_launch(2);
 }
 
+// The forward 32 -> 32 layers run on tcgen05 (jfg_cnn_tc.cu) unless
+// JFEM_CNN_TC=0 selects the mma.sync kernels.
+bool use_tc()
+{
+    const char* e = getenv("JFEM_CNN_TC");
+    return !(e && e[0] == '0');
+}
+
 void cnn_forward(jfg_cnn* n, cudaStream_t st, int B, int H, int W, const float* x, float* y)
 {
     size_t npx = (size_t)B * H * W;
@@ -567,10 +591,20 @@ void cnn_forward(jfg_cnn* n, cudaStream_t st, int B, int H, int W, const float* 
     const bf16* wk = n->wk.p;
     k_conv_in<<<grid1d(npx), 256, 0, st>>>(B, H, W, x, n->w32.p + kLayerOff[0], n->h1.p);
     JFG_CUDA(cudaGetLastError());
-    conv_mid<bf16, bf16, 0, true, false>(st, B, H, W, n->h1.p, wk + 0 * kMidParams, nullptr, nullptr, n->a2.p);
-    conv_mid<bf16, bf16, 1, true, false>(st, B, H, W, n->a2.p, wk + 1 * kMidParams, n->h1.p, nullptr, n->h3.p);
-    conv_mid<bf16, bf16, 0, true, false>(st, B, H, W, n->h3.p, wk + 2 * kMidParams, nullptr, nullptr, n->a4.p);
-    conv_mid<bf16, bf16, 1, true, false>(st, B, H, W, n->a4.p, wk + 3 * kMidParams, n->h3.p, nullptr, n->h5.p);
+    if (use_tc()) {
+        int* err = n->tc_err.p;
+        conv_mid_tc(st, B, H, W, n->h1.p, wk + 0 * kMidParams, nullptr, n->a2.p, err);
+        conv_mid_tc(st, B, H, W, n->a2.p, wk + 1 * kMidParams, n->h1.p, n->h3.p, err);
+        conv_mid_tc(st, B, H, W, n->h3.p, wk + 2 * kMidParams, nullptr, n->a4.p, err);
+        conv_mid_tc(st, B, H, W, n->a4.p, wk + 3 * kMidParams, n->h3.p, n->h5.p, err);
+    } else {
+        conv_mid<bf16, bf16, 0, true, false>(st, B, H, W, n->h1.p, wk + 0 * kMidParams, nullptr, nullptr, n->a2.p);
+        conv_mid<bf16, bf16, 1, true, false>(st, B, H, W, n->a2.p, wk + 1 * kMidParams, n->h1.p, nullptr,
+                                             n->h3.p);
+        conv_mid<bf16, bf16, 0, true, false>(st, B, H, W, n->h3.p, wk + 2 * kMidParams, nullptr, nullptr, n->a4.p);
+        conv_mid<bf16, bf16, 1, true, false>(st, B, H, W, n->a4.p, wk + 3 * kMidParams, n->h3.p, nullptr,
+                                             n->h5.p);
+    }
     k_conv_out<<<grid1d(npx), 256, 0, st>>>(B, H, W, n->h5.p, n->w32.p + kLayerOff[5], y);
     JFG_CUDA(cudaGetLastError());
     note_launch(2);
@@ -643,7 +677,9 @@ int jfg_cnn_create(jfg_ctx* ctx, jfg_cnn** out)
         n->loss.alloc(1);
         n->partials.alloc(4 * jfg::kVecGrid);
         n->counter.alloc(4);
+        n->tc_err.alloc(1);
         cudaStream_t st = jfg::ctx_stream(ctx);
+        JFG_CUDA(cudaMemsetAsync(n->tc_err.p, 0, sizeof(int), st));
         JFG_CUDA(cudaMemsetAsync(n->w32.p, 0, sizeof(float) * jfg::kNumParams, st));
         JFG_CUDA(cudaMemsetAsync(n->m.p, 0, sizeof(float) * jfg::kNumParams, st));
         JFG_CUDA(cudaMemsetAsync(n->v.p, 0, sizeof(float) * jfg::kNumParams, st));
@@ -707,7 +743,7 @@ int jfg_cnn_forward_dev(jfg_cnn* n, int B, int H, int W, const float* d_x, float
         cudaStream_t st = jfg::ctx_stream(n->ctx);
         jfg::cnn_reserve(n, (size_t)B * H * W);
         jfg::cnn_forward(n, st, B, H, W, d_x, d_y);
-        JFG_CUDA(cudaStreamSynchronize(st));
+        jfg::cnn_check_tc(n, st);
         return JFG_OK;
     } catch (const jfg::Error& e) {
         jfg::ctx_set_error(n->ctx, e.msg);
@@ -728,7 +764,7 @@ int jfg_cnn_loss_grad_dev(jfg_cnn* n, int B, int H, int W, const float* d_x, con
         if (loss) JFG_CUDA(cudaMemcpyAsync(loss, n->loss.p, sizeof(double), cudaMemcpyDeviceToHost, st));
         if (h_grad)
             JFG_CUDA(cudaMemcpyAsync(h_grad, n->g32.p, sizeof(float) * jfg::kNumParams, cudaMemcpyDeviceToHost, st));
-        JFG_CUDA(cudaStreamSynchronize(st));
+        jfg::cnn_check_tc(n, st);
         return JFG_OK;
     } catch (const jfg::Error& e) {
         jfg::ctx_set_error(n->ctx, e.msg);
@@ -776,11 +812,17 @@ int jfg_cnn_time_forward(jfg_cnn* n, int B, int H, int W, int iters, double* ms_
         JFG_CUDA(cudaEventRecord(e0, st));
         for (int i = 0; i < iters; i++) jfg::cnn_forward(n, st, B, H, W, x.p, n->y.p);
         JFG_CUDA(cudaEventRecord(e1, st));
-        for (int i = 0; i < iters; i++)
-            jfg::conv_mid<__nv_bfloat16, __nv_bfloat16, 0, true, false>(st, B, H, W, n->h1.p, n->wk.p, nullptr,
-                                                                         nullptr, n->a2.p);
+        const bool tc = jfg::use_tc();
+        for (int i = 0; i < iters; i++) {
+            if (tc)
+                jfg::conv_mid_tc(st, B, H, W, n->h1.p, n->wk.p, nullptr, n->a2.p, n->tc_err.p);
+            else
+                jfg::conv_mid<__nv_bfloat16, __nv_bfloat16, 0, true, false>(st, B, H, W, n->h1.p, n->wk.p, nullptr,
+                                                                             nullptr, n->a2.p);
+        }
         JFG_CUDA(cudaEventRecord(e2, st));
         JFG_CUDA(cudaEventSynchronize(e2));
+        jfg::cnn_check_tc(n, st);
         float t1 = 0, t2 = 0;
         JFG_CUDA(cudaEventElapsedTime(&t1, e0, e1));
         JFG_CUDA(cudaEventElapsedTime(&t2, e1, e2));

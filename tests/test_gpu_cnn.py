@@ -68,3 +68,20 @@ def test_training_reduces_loss(ctx):
     assert np.mean(losses[-20:]) < 0.2 * np.mean(losses[:5])
     w = net.get_weights()
     assert w.size == num_params() == 37440 and np.all(np.isfinite(w))
+
+
+@pytest.mark.parametrize("shape", [(2, 45, 27), (1, 257, 131)])
+def test_tcgen05_forward_matches_mma_sync(ctx, shape, monkeypatch):
+    """The tcgen05 forward (TMEM accumulators) and the mma.sync forward agree
+    to BF16 rounding of the activations (partial tiles and a batch included)."""
+    rng = np.random.default_rng(11)
+    w = he_init(seed=5, gain_last=1.0)
+    x = torch.from_numpy(rng.standard_normal(shape).astype(np.float32)).cuda()
+    net = LearnedSmoother(ctx, w)
+    monkeypatch.setenv("JFEM_CNN_TC", "1")
+    y_tc = net.forward(x).cpu().numpy()
+    monkeypatch.setenv("JFEM_CNN_TC", "0")
+    y_ms = net.forward(x).cpu().numpy()
+    assert np.all(np.isfinite(y_tc))
+    err = np.linalg.norm(y_tc - y_ms) / np.linalg.norm(y_ms)
+    assert err < 1e-2, err
