@@ -1,5 +1,6 @@
 // 32 -> 32 3x3 convolution of the learned smoother's forward pass on the
-// fifth-generation tensor cores (tcgen05.mma, accumulator in TMEM).
+// fifth-generation tensor cores (tcgen05.mma, accumulators in TMEM), fed by
+// TMA.
 //
 // Implicit GEMM per tile of 16 x 8 = 128 output pixels (the MMA's M):
 //   D[p][co] = sum_{tap, ci} X[p + tap][ci] * W[co][tap * 32 + ci]
@@ -7,20 +8,25 @@
 //
 // Shared-memory layout (canonical K-major, no swizzle: core matrices of 8
 // rows x 16 bytes):
-//  - the input halo (18 x 10 pixels) is stored as four planes of 8 channels,
-//    pixel (hy, hx) of plane q at q * 2880 + (hy * 10 + hx) * 16.  Because a
-//    tile is 8 pixels wide, the 8 rows of every core matrix of the A operand
-//    of any tap are 8 consecutive halo pixels of one halo row, the next core
-//    matrix (next tile row) is 160 bytes further, and the next 8 channels are
-//    one plane further: every tap's A operand is a descriptor view of the
-//    halo (start, LBO = plane, SBO = halo row), nothing is copied;
+//  - the input halo (18 x 10 pixels) arrives by four TMA box loads of 8
+//    channels each (box 8 x 10 x 18, zero fill outside the image), plane q of
+//    a stage at q * 2944, pixel (hy, hx) at (hy * 10 + hx) * 16 inside it.
+//    Because a tile is 8 pixels wide, the 8 rows of every core matrix of the A
+//    operand of any tap are 8 consecutive halo pixels of one halo row, the
+//    next core matrix (next tile row) is 160 bytes further and the next 8
+//    channels one plane further: every tap's A operand is a descriptor view of
+//    the halo (start, LBO = plane, SBO = halo row), nothing is copied;
 //  - the weights W[co][k] at (co / 8) * 4608 + (k / 8) * 128 + (co % 8) * 16
 //    + (k % 8) * 2 (LBO = 128, SBO = 4608).
-// One thread issues the 18 MMAs and commits them to an mbarrier; after the
-// (bounded) wait each warp reads its 32 TMEM lanes (one pixel per thread, 32
-// FP32 channels), adds the skip input, applies ReLU and stores BF16.
-// Persistent CTAs of 128 threads stride over the tiles; ~30 KB of shared
-// memory and 32 TMEM columns each (at most 16 CTAs per SM fit in 512 columns).
+// Two stages: while one tile's MMAs and epilogue run, the TMA loads of the
+// CTA's next tile land in the other halo buffer; each stage has its own TMEM
+// accumulator (2 x 32 columns).  One thread issues the TMA loads and the 18
+// MMAs (committed to an mbarrier); after the bounded wait each warp reads its
+// 32 TMEM lanes (one pixel per thread, 32 FP32 channels), adds the skip
+// input, applies ReLU and stores BF16.  Persistent CTAs of 128 threads stride
+// over the tiles (~42 KB of shared memory and 64 TMEM columns each).
+#include <cudaTypedefs.h>
+
 #include "jfg_ops.cuh"
 
 namespace jfg {
@@ -30,12 +36,14 @@ typedef __nv_bfloat16 bf16;
 
 constexpr int kTH = 16, kTW = 8;                 // tile rows x columns (128 pixels)
 constexpr int kHH = kTH + 2, kHW = kTW + 2;      // halo 18 x 10
-constexpr int kPlane = kHH * kHW * 16;           // bytes of one 8-channel plane
-constexpr int kHaloBytes = 4 * kPlane;           // 11,520
+constexpr int kPlaneData = kHH * kHW * 16;       // bytes one TMA box writes (2880)
+constexpr int kPlane = 2944;                     // plane stride: 2880 rounded up to 128
+constexpr int kHaloBytes = 4 * kPlane;           // 11,776 per stage
+constexpr int kStages = 2;
 constexpr int kWRowGroup = 36 * 128;             // bytes per 8 output channels (4608)
 constexpr int kWBytes = 4 * kWRowGroup;          // 18,432
 constexpr int kTcThreads = 128;
-constexpr int kTcCtasPerSm = 7;
+constexpr int kTcCtasPerSm = 5;
 // kind::f16 instruction descriptor: D FP32, A and B BF16, both K-major, N = 32, M = 128
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
 
@@ -66,15 +74,26 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
     return false;
 }
 
+__device__ __forceinline__ void tma_plane(uint32_t dst, const CUtensorMap* map, int c, int x, int y, int b,
+                                          uint32_t bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], "
+        "[%2];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(c), "r"(x), "r"(y), "r"(b)
+        : "memory");
+}
+
 template <int SK>
 __global__ void __launch_bounds__(kTcThreads)
-k_conv_mid_tc(int B, int H, int W, const bf16* __restrict__ in, const bf16* __restrict__ wk,
+k_conv_mid_tc(const __grid_constant__ CUtensorMap tin, int B, int H, int W, const bf16* __restrict__ wk,
               const bf16* __restrict__ skip, bf16* __restrict__ out, int* __restrict__ err)
 {
     __shared__ __align__(128) unsigned char wsm[kWBytes];
-    __shared__ __align__(128) unsigned char halo[kHaloBytes];
-    __shared__ __align__(8) uint64_t mbar;
+    __shared__ __align__(128) unsigned char halo[kStages][kHaloBytes];
+    __shared__ __align__(8) uint64_t full[kStages], mdone[kStages];
     __shared__ uint32_t tmem_sh;
+    __shared__ int s_stop;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     for (int i = tid; i < 32 * 36; i += kTcThreads) {
         const int co = i / 36, j = i % 36;
@@ -82,69 +101,92 @@ k_conv_mid_tc(int B, int H, int W, const bf16* __restrict__ in, const bf16* __re
         *reinterpret_cast<uint4*>(wsm + (co >> 3) * kWRowGroup + j * 128 + (co & 7) * 16) = v;
     }
     if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(smem_u32(&tmem_sh))
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(smem_u32(&tmem_sh))
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)) : "memory");
+        s_stop = 0;
+        for (int s = 0; s < kStages; s++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[s])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mdone[s])) : "memory");
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    // the weights written by threads are read by the tensor core (async proxy)
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_sh;
-    const uint32_t bar = smem_u32(&mbar);
-    const uint32_t hbase = smem_u32(halo), wbase = smem_u32(wsm);
+    const uint32_t wbase = smem_u32(wsm);
     const int tilesx = (W + kTW - 1) / kTW, tilesy = (H + kTH - 1) / kTH;
-    const int ntiles = tilesx * tilesy * B;
-    uint32_t parity = 0;
-    bool healthy = true;
-    for (int t = blockIdx.x; t < ntiles && healthy; t += gridDim.x) {
-        const int b = t / (tilesx * tilesy), rem = t - b * (tilesx * tilesy);
+    const int per_img = tilesx * tilesy;
+    const int ntiles = per_img * B;
+
+    auto issue_load = [&](int t, int s) {       // thread 0 only
+        const int b = t / per_img, rem = t - b * per_img;
         const int y0 = (rem / tilesx) * kTH, x0 = (rem % tilesx) * kTW;
-        for (int i = tid; i < kHH * kHW * 4; i += kTcThreads) {
-            const int q = i & 3, pix = i >> 2;
-            const int hy = pix / kHW, hx = pix - hy * kHW;
-            const int gy = y0 + hy - 1, gx = x0 + hx - 1;
-            uint4 v = make_uint4(0u, 0u, 0u, 0u);
-            if (gy >= 0 && gy < H && gx >= 0 && gx < W)
-                v = *reinterpret_cast<const uint4*>(in + (((size_t)b * H + gy) * W + gx) * 32 + q * 8);
-            *reinterpret_cast<uint4*>(halo + q * kPlane + (hy * kHW + hx) * 16) = v;
-        }
-        // generic-proxy writes -> visible to the tensor core's async proxy; the
-        // previous tile's TMEM reads finish before the MMAs overwrite D
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t bar = smem_u32(&full[s]);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(4 * kPlaneData)
+                     : "memory");
+        const uint32_t dst = smem_u32(halo[s]);
+#pragma unroll
+        for (int q = 0; q < 4; q++) tma_plane(dst + q * kPlane, &tin, 8 * q, x0 - 1, y0 - 1, b, bar);
+    };
+
+    if (tid == 0 && (int)blockIdx.x < ntiles) issue_load(blockIdx.x, 0);
+    bool pending_load = (int)blockIdx.x < ntiles;   // a load into the next stage that no one waited for yet
+    bool pending_mma = false, load_failed = false;
+    int it = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
+        const int s = it & 1;
+        const uint32_t par = (uint32_t)((it >> 1) & 1);
+        const int tn = t + (int)gridDim.x;
         if (tid == 0) {
+            // the other stage's buffer is free: the MMAs that read it (previous tile) are complete
+            if (tn < ntiles) issue_load(tn, s ^ 1);
+            if (mbar_wait(smem_u32(&full[s]), par)) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t hb = smem_u32(halo[s]);
 #pragma unroll
-            for (int tap = 0; tap < 9; tap++) {
-                const int dy = tap / 3, dx = tap % 3;
+                for (int tap = 0; tap < 9; tap++) {
+                    const int dy = tap / 3, dx = tap % 3;
 #pragma unroll
-                for (int s = 0; s < 2; s++) {
-                    const uint64_t da = umma_desc(hbase + 2 * s * kPlane + (dy * kHW + dx) * 16, kPlane, kHW * 16);
-                    const uint64_t db = umma_desc(wbase + (4 * tap + 2 * s) * 128, 128, kWRowGroup);
-                    const uint32_t accum = (tap | s) ? 1u : 0u;
-                    asm volatile(
-                        "{\n\t.reg .pred p;\n\t"
-                        "setp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-                        ::"r"(tmem), "l"(da), "l"(db), "r"(kIdesc), "r"(accum)
-                        : "memory");
+                    for (int k = 0; k < 2; k++) {
+                        const uint64_t da = umma_desc(hb + 2 * k * kPlane + (dy * kHW + dx) * 16, kPlane, kHW * 16);
+                        const uint64_t db = umma_desc(wbase + (4 * tap + 2 * k) * 128, 128, kWRowGroup);
+                        const uint32_t accum = (tap | k) ? 1u : 0u;
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                            ::"r"(tmem + (uint32_t)(s * 32)), "l"(da), "l"(db), "r"(kIdesc), "r"(accum)
+                            : "memory");
+                    }
                 }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&mdone[s]))
+                             : "memory");
+            } else {
+                s_stop = 1;
             }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-                         : "memory");
         }
-        const bool ok = mbar_wait(bar, parity);
-        parity ^= 1u;
-        if (__syncthreads_or(!ok)) {
+        __syncthreads();
+        pending_load = tn < ntiles;
+        if (s_stop) {                              // this tile's load timed out: nothing was issued for it
             if (tid == 0) atomicOr(err, 1);
-            healthy = false;
+            load_failed = true;
             break;
         }
+        pending_mma = true;
+        const bool ok = mbar_wait(smem_u32(&mdone[s]), par);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicOr(err, 1);
+            s_stop = 1;
+            break;
+        }
+        pending_mma = false;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         uint32_t r[32];
         asm volatile(
@@ -156,9 +198,11 @@ k_conv_mid_tc(int B, int H, int W, const bf16* __restrict__ in, const bf16* __re
               "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
               "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
               "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-            : "r"(tmem + ((uint32_t)(warp * 32) << 16))
+            : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * 32))
             : "memory");
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const int b = t / per_img, rem = t - b * per_img;
+        const int y0 = (rem / tilesx) * kTH, x0 = (rem % tilesx) * kTW;
         const int m = warp * 32 + lane;
         const int gy = y0 + (m >> 3), gx = x0 + (m & 7);
         if (gy < H && gx < W) {
@@ -180,32 +224,68 @@ k_conv_mid_tc(int B, int H, int W, const bf16* __restrict__ in, const bf16* __re
             for (int q = 0; q < 4; q++)
                 *reinterpret_cast<uint4*>(out + base + 8 * q) = *reinterpret_cast<const uint4*>(o + 8 * q);
         }
+        // every thread's TMEM reads are done before the MMAs two tiles on overwrite this stage
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
     }
-    if (!healthy) mbar_wait(bar, parity ^ 1u);   // MMAs in flight finish before their TMEM is released
+    if (s_stop) {
+        // error path: let the copies and MMAs still in flight finish (bounded) before releasing TMEM
+        const int s = it & 1;
+        const uint32_t par = (uint32_t)((it >> 1) & 1);
+        if (load_failed) mbar_wait(smem_u32(&full[s]), par);
+        if (pending_mma) mbar_wait(smem_u32(&mdone[s]), par);
+        if (pending_load) mbar_wait(smem_u32(&full[s ^ 1]), (uint32_t)(((it + 1) >> 1) & 1));
+    }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(tmem) : "memory");
     }
 }
 
 }  // namespace
 
+// The driver's tensor-map encoder, fetched once through the runtime (no link
+// against libcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        JFG_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        JFG_CHECK(q == cudaDriverEntryPointSuccess && p, JFG_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
 // out = relu(conv3x3(in, wk) [+ skip]) for BF16 (B, H, W, 32) images; wk is
-// BF16 [32 outputs][9 taps x 32 inputs].  err is set to 1 if an MMA wait
-// timed out (the output is then incomplete).
+// BF16 [32 outputs][9 taps x 32 inputs].  err is set to 1 if a TMA or MMA
+// wait timed out (the output is then incomplete).
 void conv_mid_tc(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* in, const __nv_bfloat16* wk,
                  const __nv_bfloat16* skip, __nv_bfloat16* out, int* err)
 {
     const long long ntiles = (long long)((W + kTW - 1) / kTW) * ((H + kTH - 1) / kTH) * B;
     JFG_CHECK(ntiles < (1LL << 31), JFG_ERR_UNSUPPORTED, "image too large for the tensor-core convolution");
+    JFG_CHECK(((uintptr_t)in & 15) == 0, JFG_ERR_BAD_ARG, "convolution input not 16-byte aligned");
     const int grid = (int)std::min<long long>(ntiles, (long long)sm_count() * kTcCtasPerSm);
     if (grid <= 0) return;
+    CUtensorMap map;
+    const cuuint64_t dims[4] = {32, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
+    const cuuint64_t strides[3] = {64, (cuuint64_t)W * 64, (cuuint64_t)W * H * 64};
+    const cuuint32_t box[4] = {8, (cuuint32_t)kHW, (cuuint32_t)kHH, 1};
+    const cuuint32_t estride[4] = {1, 1, 1, 1};
+    CUresult r = tensor_map_encoder()(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(in), dims,
+                                      strides, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    JFG_CHECK(r == CUDA_SUCCESS, JFG_ERR_CUDA, "cuTensorMapEncodeTiled failed");
     if (skip)
-        k_conv_mid_tc<1><<<grid, kTcThreads, 0, st>>>(B, H, W, in, wk, skip, out, err);
+        k_conv_mid_tc<1><<<grid, kTcThreads, 0, st>>>(map, B, H, W, wk, skip, out, err);
     else
-        k_conv_mid_tc<0><<<grid, kTcThreads, 0, st>>>(B, H, W, in, wk, nullptr, out, err);
+        k_conv_mid_tc<0><<<grid, kTcThreads, 0, st>>>(map, B, H, W, wk, nullptr, out, err);
     JFG_CUDA(cudaGetLastError());
     note_launch();
 }
