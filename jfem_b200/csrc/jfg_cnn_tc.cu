@@ -18,10 +18,10 @@
 //    the halo (start, LBO = plane, SBO = halo row), nothing is copied;
 //  - the weights W[co][k] at (co / 8) * 4608 + (k / 8) * 128 + (co % 8) * 16
 //    + (k % 8) * 2 (LBO = 128, SBO = 4608).
-// Two stages: while one tile's MMAs and epilogue run, the TMA loads of the
-// CTA's next tile land in the other halo buffer; each stage has its own TMEM
-// accumulator (2 x 32 columns).  One thread issues the TMA loads and the 18
-// MMAs (committed to an mbarrier); after the bounded wait each warp reads its
+// Two stages, software-pipelined: the TMA loads of a CTA's tiles run two
+// tiles ahead and the MMAs of tile i + 1 run while tile i's epilogue reads
+// its own TMEM accumulator (2 x 32 columns).  One thread issues the TMA loads
+// and the 18 MMAs (committed to an mbarrier); after the bounded wait each warp reads its
 // 32 TMEM lanes (one pixel per thread, 32 FP32 channels), adds the skip
 // input, applies ReLU and stores BF16.  Persistent CTAs of 128 threads stride
 // over the tiles (~42 KB of shared memory and 64 TMEM columns each).
@@ -135,58 +135,77 @@ k_conv_mid_tc(const __grid_constant__ CUtensorMap tin, int B, int H, int W, cons
         for (int q = 0; q < 4; q++) tma_plane(dst + q * kPlane, &tin, 8 * q, x0 - 1, y0 - 1, b, bar);
     };
 
-    if (tid == 0 && (int)blockIdx.x < ntiles) issue_load(blockIdx.x, 0);
-    bool pending_load = (int)blockIdx.x < ntiles;   // a load into the next stage that no one waited for yet
-    bool pending_mma = false, load_failed = false;
-    int it = 0;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
-        const int s = it & 1;
-        const uint32_t par = (uint32_t)((it >> 1) & 1);
-        const int tn = t + (int)gridDim.x;
-        if (tid == 0) {
-            // the other stage's buffer is free: the MMAs that read it (previous tile) are complete
-            if (tn < ntiles) issue_load(tn, s ^ 1);
-            if (mbar_wait(smem_u32(&full[s]), par)) {
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t hb = smem_u32(halo[s]);
+    // tiles of this CTA: t_i = blockIdx.x + i * gridDim.x, i < cnt
+    const int cnt = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    auto tile_of = [&](int i) { return (int)blockIdx.x + i * (int)gridDim.x; };
+    auto issue_mma = [&](int i) -> bool {     // thread 0: wait for tile i's halo, MMAs into TMEM stage i & 1
+        const int s = i & 1;
+        if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((i >> 1) & 1))) return false;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t hb = smem_u32(halo[s]);
 #pragma unroll
-                for (int tap = 0; tap < 9; tap++) {
-                    const int dy = tap / 3, dx = tap % 3;
+        for (int tap = 0; tap < 9; tap++) {
+            const int dy = tap / 3, dx = tap % 3;
 #pragma unroll
-                    for (int k = 0; k < 2; k++) {
-                        const uint64_t da = umma_desc(hb + 2 * k * kPlane + (dy * kHW + dx) * 16, kPlane, kHW * 16);
-                        const uint64_t db = umma_desc(wbase + (4 * tap + 2 * k) * 128, 128, kWRowGroup);
-                        const uint32_t accum = (tap | k) ? 1u : 0u;
-                        asm volatile(
-                            "{\n\t.reg .pred p;\n\t"
-                            "setp.ne.b32 p, %4, 0;\n\t"
-                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-                            ::"r"(tmem + (uint32_t)(s * 32)), "l"(da), "l"(db), "r"(kIdesc), "r"(accum)
-                            : "memory");
-                    }
-                }
-                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                 smem_u32(&mdone[s]))
-                             : "memory");
+            for (int k = 0; k < 2; k++) {
+                const uint64_t da = umma_desc(hb + 2 * k * kPlane + (dy * kHW + dx) * 16, kPlane, kHW * 16);
+                const uint64_t db = umma_desc(wbase + (4 * tap + 2 * k) * 128, 128, kWRowGroup);
+                const uint32_t accum = (tap | k) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                    ::"r"(tmem + (uint32_t)(s * 32)), "l"(da), "l"(db), "r"(kIdesc), "r"(accum)
+                    : "memory");
+            }
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(&mdone[s]))
+                     : "memory");
+        return true;
+    };
+
+    // Pipeline: loads run two tiles ahead, the MMAs of tile i + 1 run during
+    // the epilogue of tile i.  Outstanding async work is tracked by thread 0
+    // for the error path.
+    int loads_issued = 0, loads_done = 0, mmas_issued = 0;
+    if (tid == 0) {
+        for (int i = 0; i < 2 && i < cnt; i++) {
+            issue_load(tile_of(i), i);
+            loads_issued++;
+        }
+        if (cnt > 0) {
+            if (issue_mma(0)) {
+                loads_done = 1;
+                mmas_issued = 1;
             } else {
                 s_stop = 1;
             }
         }
-        __syncthreads();
-        pending_load = tn < ntiles;
-        if (s_stop) {                              // this tile's load timed out: nothing was issued for it
-            if (tid == 0) atomicOr(err, 1);
-            load_failed = true;
-            break;
-        }
-        pending_mma = true;
-        const bool ok = mbar_wait(smem_u32(&mdone[s]), par);
+    }
+    __syncthreads();
+    int i = 0;
+    for (; i < cnt && !s_stop; i++) {
+        const int s = i & 1;
+        const bool ok = mbar_wait(smem_u32(&mdone[s]), (uint32_t)((i >> 1) & 1));
         if (__syncthreads_or(!ok)) {
-            if (tid == 0) atomicOr(err, 1);
-            s_stop = 1;
+            if (tid == 0) s_stop = 1;
             break;
         }
-        pending_mma = false;
+        if (tid == 0) {
+            if (i + 2 < cnt) {                   // its buffer held tile i, whose MMAs are complete
+                issue_load(tile_of(i + 2), s);
+                loads_issued++;
+            }
+            if (i + 1 < cnt) {
+                if (issue_mma(i + 1)) {
+                    loads_done++;
+                    mmas_issued++;
+                } else {
+                    s_stop = 1;
+                }
+            }
+        }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         uint32_t r[32];
         asm volatile(
@@ -201,6 +220,7 @@ k_conv_mid_tc(const __grid_constant__ CUtensorMap tin, int B, int H, int W, cons
             : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * 32))
             : "memory");
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const int t = tile_of(i);
         const int b = t / per_img, rem = t - b * per_img;
         const int y0 = (rem / tilesx) * kTH, x0 = (rem % tilesx) * kTW;
         const int m = warp * 32 + lane;
@@ -212,7 +232,7 @@ k_conv_mid_tc(const __grid_constant__ CUtensorMap tin, int B, int H, int W, cons
             if (SK) {
 #pragma unroll
                 for (int q = 0; q < 4; q++)
-                    *reinterpret_cast<uint4*>(sv + 8 * q) = *reinterpret_cast<const uint4*>(skip + base + 8 * q);
+                    *reinterpret_cast<uint4*>(sv + 8 * q) = __ldg(reinterpret_cast<const uint4*>(skip + base + 8 * q));
             }
 #pragma unroll
             for (int c = 0; c < 32; c++) {
@@ -228,13 +248,11 @@ k_conv_mid_tc(const __grid_constant__ CUtensorMap tin, int B, int H, int W, cons
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
     }
-    if (s_stop) {
-        // error path: let the copies and MMAs still in flight finish (bounded) before releasing TMEM
-        const int s = it & 1;
-        const uint32_t par = (uint32_t)((it >> 1) & 1);
-        if (load_failed) mbar_wait(smem_u32(&full[s]), par);
-        if (pending_mma) mbar_wait(smem_u32(&mdone[s]), par);
-        if (pending_load) mbar_wait(smem_u32(&full[s ^ 1]), (uint32_t)(((it + 1) >> 1) & 1));
+    if (s_stop && tid == 0) {
+        // error path: report, then let the copies and MMAs still in flight finish (bounded) before TMEM is freed
+        atomicOr(err, 1);
+        for (int k = loads_done; k < loads_issued; k++) mbar_wait(smem_u32(&full[k & 1]), (uint32_t)((k >> 1) & 1));
+        for (int k = i; k < mmas_issued; k++) mbar_wait(smem_u32(&mdone[k & 1]), (uint32_t)((k >> 1) & 1));
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
