@@ -87,3 +87,28 @@ def test_linearity_full_size(ctx):
     lhs = A.spmv(2.0 * x - 0.5 * y)
     rhs = 2.0 * A.spmv(x) - 0.5 * A.spmv(y)
     np.testing.assert_allclose(lhs, rhs, rtol=1e-10, atol=1e-10 * np.abs(rhs).max())
+
+
+def test_wide_offsets_use_32bit_columns(ctx):
+    """Column offsets beyond 16 bits keep the 32-bit index stream (a column
+    150,000 away from its row); the product is unchanged."""
+    n = 200_000
+    rng = np.random.default_rng(8)
+    ri = np.array([0, 0, 1, 2, 2, 2], np.int32)
+    ci = np.array([0, 150_000, 1, 2, 199_999, 3], np.int32)
+    v = rng.standard_normal(ri.size)
+    A = DeviceMatrix(3, n, ri, ci, v, ctx)
+    x = rng.standard_normal(n)
+    ref = O.CooMatrix(3, n, ri, ci, v).mvmul(x)
+    np.testing.assert_allclose(A.spmv(x), ref, rtol=1e-14, atol=1e-14)
+
+
+def test_16bit_offsets_match_32bit(ctx, monkeypatch):
+    """The 16-bit column-offset stream gives bit-identical products."""
+    sp, sy = fe_system(2, 24)
+    x = np.sin(np.arange(sy.n))
+    A16 = DeviceMatrix(sy.n, sy.n, sy.rows, sy.cols, sy.vals, ctx)
+    monkeypatch.setenv("JFEM_IDX16", "0")
+    A32 = DeviceMatrix(sy.n, sy.n, sy.rows, sy.cols, sy.vals, ctx)
+    assert np.array_equal(A16.spmv(x), A32.spmv(x))
+    assert np.array_equal(A16.spmv_t(x), A32.spmv_t(x))
