@@ -1,8 +1,12 @@
 // Multigrid V-cycle, FMG and smoothers on the device.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 
 #include "jfg_mg.cuh"
 #include "jfg_schwarz.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace jfg {
 
@@ -112,6 +116,233 @@ struct EpiRestrictSweep {
         xd[r] = (T)0 + (dinv[r] * v) * omega;
     }
 };
+
+// ---------------------------------------------------------------------------
+// The bottom of the V-cycle in one launch.  Below a few thousand rows every
+// level's kernels are launch-latency bound (a few microseconds each whatever
+// their size), so the levels 0..bot run inside one thread-block cluster:
+// every phase (Jacobi sweep, residual, restriction with the fused first
+// sweep, coarse solve, prolongation + correction) is a cluster-wide loop over
+// the level's SELL slots followed by a cluster barrier.  Row sums use the
+// SpMV kernel's order (same lanes per row, same unrolling and shuffle tree),
+// so the result is bit-identical to the per-kernel V-cycle; vectors written
+// inside the kernel are read with coherent loads.
+constexpr int kBotMax = 6;                // levels handled by the cluster kernel, coarse level included
+constexpr int kBotRows = 4500;            // largest level taken into the cluster kernel
+constexpr int kBotCtas = 8;               // portable cluster size
+constexpr int kBotThreads = 1024;
+
+template <typename VT>
+struct BotMat {
+    const int* off;
+    const int* perm;
+    const int* col;
+    const int16_t* col16;
+    const VT* val;
+    int nslots, tpr_log2, idx16;
+};
+
+template <typename T, typename VT>
+struct BotLevel {
+    BotMat<VT> A, R, P;       // R: restriction to level l - 1, P: prolongation from level l - 1
+    T *x, *t, *b, *r;
+    const T* dinv;
+    const unsigned char* mask;
+    int n, runs;
+    T omega;
+};
+
+template <typename T, typename VT>
+struct BotParams {
+    BotLevel<T, VT> lv[kBotMax];
+    int top, n0, fsd;
+    const double* ainv0;
+    const int* done;
+};
+
+template <typename VT>
+BotMat<VT> bot_mat(const Matrix* M, const VT* val)
+{
+    return BotMat<VT>{M->off.p, M->perm.p, M->col.p, M->col16.p, val, M->nslices * kSliceRows, M->tpr_log2,
+                      M->idx16};
+}
+
+template <typename VT, typename XT, int TPR, bool I16>
+__device__ __forceinline__ typename AccOf<VT>::T bot_row(const BotMat<VT>& m, const XT* x, int slot, int sub, int& r)
+{
+    using AT = typename AccOf<VT>::T;
+    AT sum = 0;
+    r = -1;
+    if (slot < m.nslots) {
+        const int s = slot >> 5, lane = slot & 31;
+        const int o = __ldg(m.off + s);
+        const int len = (__ldg(m.off + s + 1) - o) >> 5;
+        r = __ldg(m.perm + slot);
+        const VT* vp = m.val + o + lane;
+        const int st = 32 * TPR;
+        int k = sub;
+        if constexpr (I16) {
+            const int base = r < 0 ? 0 : r;
+            const int16_t* cp = m.col16 + o + lane;
+            for (; k + 3 * TPR < len; k += 4 * TPR) {
+                const int c0 = base + __ldg(cp + 32 * k), c1 = base + __ldg(cp + 32 * k + st);
+                const int c2 = base + __ldg(cp + 32 * k + 2 * st), c3 = base + __ldg(cp + 32 * k + 3 * st);
+                const AT v0 = to_acc(__ldg(vp + 32 * k)), v1 = to_acc(__ldg(vp + 32 * k + st));
+                const AT v2 = to_acc(__ldg(vp + 32 * k + 2 * st)), v3 = to_acc(__ldg(vp + 32 * k + 3 * st));
+                const AT x0 = (AT)x[c0], x1 = (AT)x[c1], x2 = (AT)x[c2], x3 = (AT)x[c3];
+                sum += v0 * x0;
+                sum += v1 * x1;
+                sum += v2 * x2;
+                sum += v3 * x3;
+            }
+            for (; k < len; k += TPR) sum += to_acc(__ldg(vp + 32 * k)) * (AT)x[base + __ldg(cp + 32 * k)];
+        } else {
+            const int* cp = m.col + o + lane;
+            for (; k + 3 * TPR < len; k += 4 * TPR) {
+                const int c0 = __ldg(cp + 32 * k), c1 = __ldg(cp + 32 * k + st);
+                const int c2 = __ldg(cp + 32 * k + 2 * st), c3 = __ldg(cp + 32 * k + 3 * st);
+                const AT v0 = to_acc(__ldg(vp + 32 * k)), v1 = to_acc(__ldg(vp + 32 * k + st));
+                const AT v2 = to_acc(__ldg(vp + 32 * k + 2 * st)), v3 = to_acc(__ldg(vp + 32 * k + 3 * st));
+                const AT x0 = (AT)x[c0], x1 = (AT)x[c1], x2 = (AT)x[c2], x3 = (AT)x[c3];
+                sum += v0 * x0;
+                sum += v1 * x1;
+                sum += v2 * x2;
+                sum += v3 * x3;
+            }
+            for (; k < len; k += TPR) sum += to_acc(__ldg(vp + 32 * k)) * (AT)x[__ldg(cp + 32 * k)];
+        }
+    }
+    for (int o = TPR >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    return sum;
+}
+
+template <int TPR, bool I16, typename VT, typename XT, class Epi>
+__device__ __forceinline__ void bot_spmv_t(const BotMat<VT>& m, const XT* x, Epi epi, int gtid, int gthreads)
+{
+    const int total = m.nslots * TPR;
+    for (int base = 0; base < total; base += gthreads) {      // warp-uniform trip count
+        const int gid = base + gtid;
+        int r;
+        const auto sum = bot_row<VT, XT, TPR, I16>(m, x, gid / TPR, gid % TPR, r);
+        double acc[1] = {0.0};
+        if (gid % TPR == 0 && r >= 0) epi(r, sum, acc);
+    }
+}
+
+template <typename VT, typename XT, class Epi>
+__device__ void bot_spmv(const BotMat<VT>& m, const XT* x, Epi epi, int gtid, int gthreads)
+{
+    if (m.idx16) {
+        switch (m.tpr_log2) {
+        case 0: bot_spmv_t<1, true>(m, x, epi, gtid, gthreads); break;
+        case 2: bot_spmv_t<4, true>(m, x, epi, gtid, gthreads); break;
+        default: bot_spmv_t<8, true>(m, x, epi, gtid, gthreads); break;
+        }
+    } else {
+        switch (m.tpr_log2) {
+        case 0: bot_spmv_t<1, false>(m, x, epi, gtid, gthreads); break;
+        case 2: bot_spmv_t<4, false>(m, x, epi, gtid, gthreads); break;
+        default: bot_spmv_t<8, false>(m, x, epi, gtid, gthreads); break;
+        }
+    }
+}
+
+template <typename T, typename VT>
+__global__ void __launch_bounds__(kBotThreads, 1) k_mg_bottom(const __grid_constant__ BotParams<T, VT> P)
+{
+    pdl_wait();
+    if (P.done && *P.done) return;           // the same answer for every CTA of the cluster
+    cg::cluster_group cl = cg::this_cluster();
+    const int gthreads = (int)cl.num_blocks() * blockDim.x;
+    const int gtid = (int)cl.block_rank() * blockDim.x + threadIdx.x;
+    bool fsd = P.fsd != 0;
+    for (int l = P.top; l >= 1; l--) {
+        const BotLevel<T, VT>& L = P.lv[l];
+        const T* rhs = L.b;
+        T* dst = (L.runs % 2 == 1) ? L.x : L.t;
+        if (!fsd) {                           // first sweep from the zero guess
+            for (int i = gtid; i < L.n; i += gthreads) dst[i] = (T)0 + (L.dinv[i] * rhs[i]) * L.omega;
+            cl.sync();
+        }
+        T* cur = dst;
+        T* alt = (dst == L.x) ? L.t : L.x;
+        for (int k = 1; k < L.runs; k++) {
+            bot_spmv(L.A, cur, EpiJacobi<T>{cur, rhs, L.dinv, alt, L.omega}, gtid, gthreads);
+            cl.sync();
+            T* tmp = cur;
+            cur = alt;
+            alt = tmp;
+        }
+        if (cur != L.x) {
+            for (int i = gtid; i < L.n; i += gthreads) L.x[i] = cur[i];
+            cl.sync();
+        }
+        bot_spmv(L.A, L.x, EpiResid<T>{rhs, L.r}, gtid, gthreads);
+        cl.sync();
+        const BotLevel<T, VT>& Cl = P.lv[l - 1];
+        if (l - 1 >= 1) {
+            T* dc = (Cl.runs % 2 == 1) ? Cl.x : Cl.t;
+            bot_spmv(L.R, L.r, EpiRestrictSweep<T>{Cl.mask, Cl.b, Cl.dinv, dc, Cl.omega}, gtid, gthreads);
+            fsd = true;
+        } else {
+            bot_spmv(L.R, L.r, EpiMasked<T>{Cl.mask, Cl.b}, gtid, gthreads);
+        }
+        cl.sync();
+    }
+    {   // coarsest level: x0 = Ainv * b0 in FP64, one warp per row (the order of k_coarse_gemv)
+        const int lane = threadIdx.x & 31;
+        const int nw = gthreads >> 5;
+        for (int row = gtid >> 5; row < P.n0; row += nw) {
+            double s = 0;
+            for (int j = lane; j < P.n0; j += 32) s += P.ainv0[(size_t)row * P.n0 + j] * (double)P.lv[0].b[j];
+            s = warp_sum(s);
+            if (lane == 0) P.lv[0].x[row] = (T)s;
+        }
+        cl.sync();
+    }
+    for (int l = 1; l <= P.top; l++) {
+        const BotLevel<T, VT>& L = P.lv[l];
+        bot_spmv(L.P, P.lv[l - 1].x, EpiMaskedAdd<T>{L.mask, L.x}, gtid, gthreads);
+        cl.sync();
+        T* cur = L.x;
+        T* alt = L.t;
+        for (int k = 0; k < L.runs; k++) {
+            bot_spmv(L.A, cur, EpiJacobi<T>{cur, L.b, L.dinv, alt, L.omega}, gtid, gthreads);
+            cl.sync();
+            T* tmp = cur;
+            cur = alt;
+            alt = tmp;
+        }
+        if (cur != L.x) {
+            for (int i = gtid; i < L.n; i += gthreads) L.x[i] = cur[i];
+            cl.sync();
+        }
+    }
+}
+
+template <typename T, typename VT>
+void launch_bottom(const BotParams<T, VT>& p, cudaStream_t st)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kBotCtas);
+    cfg.blockDim = dim3(kBotThreads);
+    cfg.stream = st;
+    cudaLaunchAttribute at[2];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = kBotCtas;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    int na = 1;
+    if (use_pdl()) {
+        at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at[1].val.programmaticStreamSerializationAllowed = 1;
+        na = 2;
+    }
+    cfg.attrs = at;
+    cfg.numAttrs = na;
+    JFG_CUDA(cudaLaunchKernelEx(&cfg, k_mg_bottom<T, VT>, p));
+    note_launch();
+}
 
 }  // namespace
 
@@ -250,6 +481,16 @@ void MGImpl<T>::init(Context* ctx, int levels, Matrix* const* As, Matrix* const*
     zero_flag.alloc(1);
     JFG_CUDA(cudaMemsetAsync(flags.p, 0, sizeof(int) * L, st));
     JFG_CUDA(cudaMemsetAsync(zero_flag.p, 0, sizeof(int), st));
+    // levels 1..bot (all small, Jacobi-smoothed) and the coarse solve run as one
+    // cluster kernel; JFEM_MG_BOTTOM=0 keeps one launch per operation
+    bot = -1;
+    const char* eb = getenv("JFEM_MG_BOTTOM");
+    if (!(eb && eb[0] == '0')) {
+        for (int l = 1; l < L - 1 && l < kBotMax; l++) {
+            if (n[l] > kBotRows || sm[l].kind != JFG_SMOOTH_JACOBI || sm[l].runs < 1) break;
+            bot = l;
+        }
+    }
     JFG_CUDA(cudaStreamSynchronize(st));
 }
 
@@ -333,12 +574,56 @@ void MGImpl<T>::smooth(int l, const T* rhs, bool xzero, const Scratch& sc, const
     }
 }
 
+template <typename T>
+void MGImpl<T>::bottom(bool first_sweep_done, const int* done, cudaStream_t st)
+{
+    auto fill = [&](auto& p, auto vals) {
+        p.top = bot;
+        p.n0 = n[0];
+        p.fsd = first_sweep_done ? 1 : 0;
+        p.ainv0 = ainv0.p;
+        p.done = done;
+        for (int l = 0; l <= bot; l++) {
+            auto& L = p.lv[l];
+            L.A = bot_mat(A[l], vals(A[l]));
+            if (l >= 1) {
+                L.R = bot_mat(R[l - 1], vals(R[l - 1]));
+                L.P = bot_mat(P[l - 1], vals(P[l - 1]));
+            }
+            L.x = x[l].p;
+            L.t = t[l].p;
+            L.b = b[l].p;
+            L.r = r[l].p;
+            L.dinv = dinv[l].p;
+            L.mask = mask[l].p;
+            L.n = n[l];
+            L.runs = sm[l].runs;
+            L.omega = (T)sm[l].omega;
+        }
+    };
+    if constexpr (std::is_same<T, float>::value) {
+        if (vbf16) {
+            BotParams<float, __nv_bfloat16> p = {};
+            fill(p, [](const Matrix* M) { return (const __nv_bfloat16*)M->val16.p; });
+            launch_bottom(p, st);
+            return;
+        }
+    }
+    BotParams<T, T> p = {};
+    fill(p, [](const Matrix* M) { return vals_of<T>(M); });
+    launch_bottom(p, st);
+}
+
 // mgStepV (MGPreconditionerInterface.java:125-198): guess in x[l] (or zero),
 // rhs given; result in x[l].
 template <typename T>
 void MGImpl<T>::vstep(int l, const T* rhs, bool xzero, const Scratch& sc, const int* done, cudaStream_t st,
                       bool first_sweep_done)
 {
+    if (l == bot && xzero && rhs == b[l].p) {    // the whole bottom of the cycle in one cluster launch
+        bottom(first_sweep_done, done, st);
+        return;
+    }
     if (l == 0) {
         coarse(rhs, x[0].p, done, st);
         return;

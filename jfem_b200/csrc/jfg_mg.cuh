@@ -28,6 +28,7 @@ struct MGImpl {
     int cycles = 3;
     int use_fmg = 1;
     int vbf16 = 0;                          // float hierarchy: matrices read as BF16 (FP32 vectors, FP32 sums)
+    int bot = -1;                           // levels 0..bot run as one cluster kernel (-1: none)
     std::vector<Matrix*> A, P, R;          // A[l], P[l] : n_{l+1} x n_l, R[l] = P[l]^T
     std::vector<int> n;
     std::vector<DevBuf<T>> x, t, b, r, fr;
@@ -66,6 +67,8 @@ struct MGImpl {
     void smooth(int l, const T* rhs, bool xzero, const Scratch& sc, const int* done, cudaStream_t st,
                 bool first_sweep_done = false);
     void coarse(const T* rhs, T* out, const int* done, cudaStream_t st);
+    // the V-cycle below and including level `bot`, entered from the restriction above
+    void bottom(bool first_sweep_done, const int* done, cudaStream_t st);
     void fmg_into_top(const T* defect, const Scratch& sc, const int* done, cudaStream_t st);
     int max_blocks() const;
 };

@@ -59,3 +59,34 @@ def test_mg_single_level(ctx):
     mg = MGPreconditioner([A], [], [sy.boundary], [None], cycles=1, use_fmg=False, ctx=ctx)
     D = coo_oracle(sy).dense()
     np.testing.assert_allclose(mg.mvMul(sy.rhs), np.linalg.solve(D, sy.rhs), rtol=1e-12, atol=1e-14)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_cluster_bottom_is_bit_identical(ctx, monkeypatch, precision):
+    """The levels below 4,500 rows run as one cluster kernel; the V-cycle,
+    the preconditioner and a whole PCG solve equal the one-launch-per-
+    operation path bit for bit."""
+    from jfem_b200 import IterativeSolver
+    h = mg_levels(2, 2, 6, modes=8, seed=5)        # Q2 64x64: levels 81 ... 16,641 rows
+    sm = (O.SMOOTH_JACOBI, 2, 2.0 / 3.0)
+    b = h.finest.rhs
+    outs = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("JFEM_MG_BOTTOM", flag)
+        mg_o, mg, mats = build(h, ctx, sm, 1, False) if precision == "fp64" else (None, None, None)
+        if precision != "fp64":
+            mats = [dev(s, ctx) for s in h.systems]
+            prol = [DeviceMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l], ctx) for l in range(5)]
+            mg = MGPreconditioner(mats, prol, h.boundary, [None] + [JacobiSmoother(2, 2.0 / 3.0)] * 5, cycles=1,
+                                  use_fmg=False, precision="mixed", ctx=ctx)
+        s = IterativeSolver(ctx=ctx)
+        s.precision = "fp64" if precision == "fp64" else "mixed-precond"
+        x = s.solvePCG(mats[-1], mg, b, 1e-9 * np.linalg.norm(b))
+        outs.append((mg.vCycle(np.zeros(b.size), b) if precision == "fp64" else None, x, s.iterations,
+                     s.last.history.copy()))
+    (v1, x1, i1, h1), (v0, x0, i0, h0) = outs
+    if precision == "fp64":
+        assert np.array_equal(v1, v0)
+    assert i1 == i0
+    assert np.array_equal(h1, h0)
+    assert np.array_equal(x1, x0)
