@@ -481,11 +481,14 @@ void MGImpl<T>::init(Context* ctx, int levels, Matrix* const* As, Matrix* const*
     zero_flag.alloc(1);
     JFG_CUDA(cudaMemsetAsync(flags.p, 0, sizeof(int) * L, st));
     JFG_CUDA(cudaMemsetAsync(zero_flag.p, 0, sizeof(int), st));
-    // levels 1..bot (all small, Jacobi-smoothed) and the coarse solve run as one
-    // cluster kernel; JFEM_MG_BOTTOM=0 keeps one launch per operation
+    // JFEM_MG_BOTTOM=1: levels 1..bot (all small, Jacobi-smoothed) and the
+    // coarse solve run as one cluster kernel.  Off by default: on the Q2 512^2
+    // hierarchy it replaces ~19 launches per V-cycle but is ~26 us slower per
+    // V-cycle, because one 8-SM cluster hides far less load latency than the
+    // whole GPU does per launch.
     bot = -1;
     const char* eb = getenv("JFEM_MG_BOTTOM");
-    if (!(eb && eb[0] == '0')) {
+    if (eb && eb[0] == '1') {
         for (int l = 1; l < L - 1 && l < kBotMax; l++) {
             if (n[l] > kBotRows || sm[l].kind != JFG_SMOOTH_JACOBI || sm[l].runs < 1) break;
             bot = l;

@@ -63,9 +63,9 @@ def test_mg_single_level(ctx):
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_cluster_bottom_is_bit_identical(ctx, monkeypatch, precision):
-    """The levels below 4,500 rows run as one cluster kernel; the V-cycle,
-    the preconditioner and a whole PCG solve equal the one-launch-per-
-    operation path bit for bit."""
+    """With JFEM_MG_BOTTOM=1 the levels below 4,500 rows run as one cluster
+    kernel; the V-cycle, the preconditioner and a whole PCG solve equal the
+    one-launch-per-operation path bit for bit."""
     from jfem_b200 import IterativeSolver
     h = mg_levels(2, 2, 6, modes=8, seed=5)        # Q2 64x64: levels 81 ... 16,641 rows
     sm = (O.SMOOTH_JACOBI, 2, 2.0 / 3.0)
