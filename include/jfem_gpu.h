@@ -79,10 +79,11 @@ int jfg_spmv_t_dev(jfg_mat* m, const double* d_x, double* d_y);
 int jfg_spmv_f32_dev(jfg_mat* m, const float* d_x, float* d_y);
 /* Diagonal with duplicates summed.  Replaces Matrix.diag (Core/src/main/java/linalg/Matrix.java:157-175). */
 int jfg_matrix_diag(jfg_mat* m, double* h_diag);
-/* Times `iters` back-to-back FP64 (precision 0) or FP32 (precision 1)
- * products y = A x on the context stream with CUDA events; returns the mean
- * milliseconds per product.  x and y are library-owned device vectors
- * (x = 1).  Measurement helper, not part of the reference surface. */
+/* Times `iters` FP64 (precision 0) or FP32 (precision 1) products y = A x
+ * on the context stream, each with CUDA events around the launch and the L2
+ * flushed before it (a 256 MB write between products, not timed); returns
+ * the mean milliseconds per product.  x and y are library-owned device
+ * vectors (x = 1).  Measurement helper, not part of the reference surface. */
 int jfg_spmv_time(jfg_mat* m, int precision, int iters, double* ms_per_spmv);
 
 /* ---- smoothers ------------------------------------------------------- */

@@ -2,6 +2,7 @@
 // staging and error translation.  No entry point lets a C++ exception escape.
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <memory>
 
 #include "jfg_krylov.cuh"
@@ -280,20 +281,30 @@ int jfg_spmv_time(jfg_mat* m, int precision, int iters, double* ms)
         cudaStream_t st = ctx->c.stream;
         jfg::Matrix* M = m->m;
         jfg::Scratch sc = ctx_scratch(ctx, M->nblocks);
-        cudaEvent_t e0, e1;
-        JFG_CUDA(cudaEventCreate(&e0));
-        JFG_CUDA(cudaEventCreate(&e1));
-        float t = 0;
+        // every timed product starts with a cold L2: a 256 MB buffer (twice
+        // the L2) is written between the products, outside the timed events
+        DevBuf<unsigned char> flush;
+        const size_t fbytes = (size_t)256 << 20;
+        flush.alloc(fbytes);
+        std::vector<cudaEvent_t> ev(2 * (size_t)iters);
+        for (auto& e : ev) JFG_CUDA(cudaEventCreate(&e));
+        auto timed = [&](const std::function<void()>& launch) {
+            for (int i = 0; i < 3; i++) launch();
+            for (int i = 0; i < iters; i++) {
+                JFG_CUDA(cudaMemsetAsync(flush.p, i & 0xff, fbytes, st));
+                JFG_CUDA(cudaEventRecord(ev[2 * i], st));
+                launch();
+                JFG_CUDA(cudaEventRecord(ev[2 * i + 1], st));
+            }
+        };
         if (precision == 0) {
             DevBuf<double> x, y;
             x.alloc(M->cols);
             y.alloc(M->rows);
             std::vector<double> ones(M->cols, 1.0);
             JFG_CUDA(cudaMemcpyAsync(x.p, ones.data(), sizeof(double) * M->cols, cudaMemcpyHostToDevice, st));
-            for (int i = 0; i < 3; i++) SpmvStore64::run(st, M, x.p, y.p, sc);
-            JFG_CUDA(cudaEventRecord(e0, st));
-            for (int i = 0; i < iters; i++) SpmvStore64::run(st, M, x.p, y.p, sc);
-            JFG_CUDA(cudaEventRecord(e1, st));
+            timed([&]() { SpmvStore64::run(st, M, x.p, y.p, sc); });
+            JFG_CUDA(cudaStreamSynchronize(st));
         } else {
             jfg::matrix_ensure_fp32(M);
             DevBuf<float> x, y;
@@ -301,18 +312,19 @@ int jfg_spmv_time(jfg_mat* m, int precision, int iters, double* ms)
             y.alloc(M->rows);
             std::vector<float> ones(M->cols, 1.0f);
             JFG_CUDA(cudaMemcpyAsync(x.p, ones.data(), sizeof(float) * M->cols, cudaMemcpyHostToDevice, st));
-            for (int i = 0; i < 3; i++)
+            timed([&]() {
                 jfg::spmv_launch<float, float, 0>(st, M, M->val32.p, x.p, jfg::EpiStore<float>{y.p}, sc, nullptr);
-            JFG_CUDA(cudaEventRecord(e0, st));
-            for (int i = 0; i < iters; i++)
-                jfg::spmv_launch<float, float, 0>(st, M, M->val32.p, x.p, jfg::EpiStore<float>{y.p}, sc, nullptr);
-            JFG_CUDA(cudaEventRecord(e1, st));
+            });
+            JFG_CUDA(cudaStreamSynchronize(st));
         }
-        JFG_CUDA(cudaEventSynchronize(e1));
-        JFG_CUDA(cudaEventElapsedTime(&t, e0, e1));
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        *ms = t / iters;
+        double total = 0;
+        for (int i = 0; i < iters; i++) {
+            float t = 0;
+            JFG_CUDA(cudaEventElapsedTime(&t, ev[2 * i], ev[2 * i + 1]));
+            total += t;
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+        *ms = total / iters;
         return JFG_OK;
     });
 }
