@@ -37,7 +37,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "time-to-1e-8 residual (s) & SpMV GB/s: mixed+learned vs plain FP64 GMG-PCG, 1 B200"
-WORKLOAD = "Q2 512x512 -Lap u + 5u = f, GMG-PCG to 1e-8 relative FP64 residual (configs[1])"
+WORKLOAD = "Q2 512x512 -Lap u + 5u = f, GMG-PCG to 1e-8 relative FP64 residual"
 CELLS, P, LEVELS, MODES, SEED = 512, 2, 8, 16, 0
 RTOL = 1e-8
 
@@ -163,6 +163,13 @@ class ClockSampler:
 def build_problem(cells, levels):
     from jfem_b200 import problems
     return problems.hierarchy(P, cells >> (levels - 1), levels, mass=5.0, modes=MODES, seed=SEED)
+
+
+# DRAM bytes (read + write) of one cold launch of the FP32 finest-level SpMV of
+# Q2 512x512 (n = 1,050,625, nnz = 16,707,665), 16-bit column offsets, from one
+# ncu capture; it applies only to that matrix.
+SPMV32_TRAFFIC_CASE = (1050625, 16707665)
+SPMV32_TRAFFIC_BYTES = 109.12e6 + 5.16e6
 
 
 def spmv_bytes(n, nnz, sval, sx):
@@ -301,7 +308,8 @@ def run_ours(args):
     e2e_s = (time.perf_counter() - t_e2e) / args.steps
     e2e_s = max_over_ranks(e2e_s)
 
-    # dominant kernel: the finest-level row-block SpMV (FP32 in the mixed solve)
+    # dominant kernel: the finest-level SELL-32 SpMV (FP32 in the mixed solve),
+    # timed with the L2 flushed before every launch
     nnz = A.nnz
     ms_spmv32 = A.time_spmv(precision=1, iters=50)
     ms_spmv64 = A.time_spmv(precision=0, iters=50)
@@ -338,7 +346,8 @@ def run_ours(args):
             "data": "synthetic (seeded sine-mode source, assembled Q2 system)",
             "config": {"workload": WORKLOAD, "dofs": n, "nnz": int(nnz), "levels": args.levels,
                        "smoother": "Jacobi 2+2 omega=2/3", "coarse": "dense FP64 inverse 81x81",
-                       "l2": "inputs larger than L2 (finest matrix > 126 MB)", "parallelism": f"replicas{world}"},
+                       "l2": "solve working set larger than L2 (FP64 finest matrix 167 MB + FP32 hierarchy); "
+                             "roofline SpMV timed with the L2 flushed before each launch", "parallelism": f"replicas{world}"},
             "iterations": itm,
             "outer_iterations": outer,
             "final_rel_residual": resm / bnorm,
@@ -355,7 +364,9 @@ def run_ours(args):
                     "path": "jfg_solve (C ABI) with pinned host rhs in and solution out; start e0 (opts.start=1)"},
             "gpu_launches": int(round(launches)),
             "roofline": {"bound": "hbm", "achieved": gbs32, "peak": peak, "unit": "GB/s", "frac": gbs32 / peak,
-                         "traffic": None, "kernel": "k_spmv<float> finest level", "peak_source": peak_src,
+                         "traffic": SPMV32_TRAFFIC_BYTES if (n, nnz) == SPMV32_TRAFFIC_CASE else None, "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
+                         "one cold launch (profiles/k_spmv_sell_fp32_q2_512.md)",
+                         "kernel": "k_spmv<float> finest level", "peak_source": peak_src,
                          "bytes_per_launch": b32, "ms_per_launch": ms_spmv32},
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
@@ -429,7 +440,7 @@ def _peaks():
 
 
 def run_batch_heat(args):
-    """configs[2]: 256 Q1 heat systems, cells drawn from {32, 48, ..., 256}^2,
+    """256 Q1 heat systems, cells drawn from {32, 48, ..., 256}^2,
     dt = 1e-3, 50 implicit-Euler steps, FP32 PCG + FP64 refinement to 1e-10."""
     import torch
     from jfem_b200 import _native as N
@@ -476,8 +487,8 @@ def run_batch_heat(args):
             "value": statistics.median(ms) / 1e3, "unit": "s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": statistics.median(ms), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded bumps)",
-            "config": {"workload": "batch-heat: 256 Q1 systems, cells {32..256 step 16}^2, dt=1e-3, 50 steps "
-                                   "(configs[2])", "systems": 256, "dofs": dofs, "nnz": nnz},
+            "config": {"workload": "batch-heat: 256 Q1 systems, cells {32..256 step 16}^2, dt=1e-3, 50 steps",
+                                   "systems": 256, "dofs": dofs, "nnz": nnz},
             "kernel_ms": last.ms, "total_inner_iterations": last.total_inner_iterations,
             "max_rel_residual": last.max_rel_residual, "failed": last.failed,
             "cluster": last.cluster, "threads": last.threads, "clocks": clk.summary(), "cpu_baseline": cpu}
@@ -485,7 +496,7 @@ def run_batch_heat(args):
 
 
 def run_stokes(args):
-    """configs[3]: Taylor-Hood Stokes on 256x256 cells, GMRES(50) + block-diagonal
+    """Taylor-Hood Stokes on 256x256 cells, GMRES(50) + block-diagonal
     preconditioner to 1e-8, variants of the velocity smoother and precision."""
     import torch
     from jfem_b200 import _native as N
@@ -520,7 +531,7 @@ def run_stokes(args):
             "value": out["schwarz_fp64"]["time_s"], "unit": "s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (lid-driven cavity + seeded Fourier body force)",
-            "config": {"workload": "stokes: Taylor-Hood Q2/Q1 256x256 cells (configs[3])", "dofs": s.n,
+            "config": {"workload": "stokes: Taylor-Hood Q2/Q1 256x256 cells", "dofs": s.n,
                        "velocity_dofs": s.nv, "nnz": int(s.vals.size), "levels": len(prob.spaces),
                        "preconditioner": "velocity V-cycle (coloured Schwarz, 2x2-cell partitions + 1 cell "
                                          "overlap, 9 colours) | nu / lumped pressure mass",
@@ -530,7 +541,7 @@ def run_stokes(args):
 
 
 def run_learned(args):
-    """configs[4]: FGMRES(30) + FP32 V-cycle + learned smoother vs FP64 GMG-PCG."""
+    """FGMRES(30) + FP32 V-cycle + learned smoother vs FP64 GMG-PCG."""
     from jfem_b200 import _native as N
     from jfem_b200.learned import WEIGHTS, evaluate
     ctx = N.default_context()
@@ -543,8 +554,8 @@ def run_learned(args):
             "value": best, "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f32+f64",
             "data": "synthetic (GRF kappa, seeded)",
-            "config": {"workload": "learned: -div(kappa grad u) = f, Q1 1024x1024, kappa = exp(GRF l=0.05 s2=1) "
-                                   "(configs[4])", "training": train},
+            "config": {"workload": "learned: -div(kappa grad u) = f, Q1 1024x1024, kappa = exp(GRF l=0.05 s2=1)",
+                                   "training": train},
             "speedup_vs_fp64_gmg_pcg": out["gmg_pcg_fp64"]["time_s"] / best, "arms": out}
     print(json.dumps(line))
 

@@ -81,7 +81,7 @@ int jfg_spmv_f32_dev(jfg_mat* m, const float* d_x, float* d_y);
 int jfg_matrix_diag(jfg_mat* m, double* h_diag);
 /* Times `iters` FP64 (precision 0) or FP32 (precision 1) products y = A x
  * on the context stream, each with CUDA events around the launch and the L2
- * flushed before it (a 256 MB write between products, not timed); returns
+ * flushed before it (a 256 MB buffer read between products, not timed); returns
  * the mean milliseconds per product.  x and y are library-owned device
  * vectors (x = 1).  Measurement helper, not part of the reference surface. */
 int jfg_spmv_time(jfg_mat* m, int precision, int iters, double* ms_per_spmv);

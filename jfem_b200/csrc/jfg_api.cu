@@ -273,6 +273,18 @@ int jfg_matrix_diag(jfg_mat* m, double* h_diag)
     });
 }
 
+// Reads a buffer larger than the L2 (clean lines only, so the next kernel's
+// misses cause no write-backs of flush data).
+__global__ void k_l2_flush(const uint4* __restrict__ buf, size_t n, unsigned* sink)
+{
+    unsigned acc = 0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const uint4 v = buf[i];
+        acc ^= v.x ^ v.y ^ v.z ^ v.w;
+    }
+    if (acc == 0x9e3779b9u) *sink = acc;     // practically never: keeps the loads alive
+}
+
 int jfg_spmv_time(jfg_mat* m, int precision, int iters, double* ms)
 {
     if (!m || !ms || iters <= 0) return JFG_ERR_BAD_ARG;
@@ -282,16 +294,20 @@ int jfg_spmv_time(jfg_mat* m, int precision, int iters, double* ms)
         jfg::Matrix* M = m->m;
         jfg::Scratch sc = ctx_scratch(ctx, M->nblocks);
         // every timed product starts with a cold L2: a 256 MB buffer (twice
-        // the L2) is written between the products, outside the timed events
-        DevBuf<unsigned char> flush;
-        const size_t fbytes = (size_t)256 << 20;
-        flush.alloc(fbytes);
+        // the L2) is read between the products, outside the timed events
+        DevBuf<uint4> flush;
+        DevBuf<unsigned> sink;
+        const size_t fn = ((size_t)256 << 20) / sizeof(uint4);
+        flush.alloc(fn);
+        sink.alloc(1);
+        JFG_CUDA(cudaMemsetAsync(flush.p, 0, fn * sizeof(uint4), st));
         std::vector<cudaEvent_t> ev(2 * (size_t)iters);
         for (auto& e : ev) JFG_CUDA(cudaEventCreate(&e));
         auto timed = [&](const std::function<void()>& launch) {
             for (int i = 0; i < 3; i++) launch();
             for (int i = 0; i < iters; i++) {
-                JFG_CUDA(cudaMemsetAsync(flush.p, i & 0xff, fbytes, st));
+                k_l2_flush<<<jfg::sm_count() * 8, 256, 0, st>>>(flush.p, fn, sink.p);
+                JFG_CUDA(cudaGetLastError());
                 JFG_CUDA(cudaEventRecord(ev[2 * i], st));
                 launch();
                 JFG_CUDA(cudaEventRecord(ev[2 * i + 1], st));

@@ -53,7 +53,7 @@ def test_batch_autotune_and_uneven_sizes(ctx):
 
 
 def test_batch_full_size_conservation(ctx):
-    """configs[2]: 256 Q1 systems, cells from {32, 48, ..., 256}^2, dt = 1e-3,
+    """256 Q1 systems, cells from {32, 48, ..., 256}^2, dt = 1e-3,
     50 steps.  With the natural boundary the mass 1^T M u is conserved by
     implicit Euler and the M-energy decays; both hold per system."""
     batch = problems.heat_batch(nsys=256, dt=1e-3, seed=0)
