@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cells", type=int, default=CELLS)
     ap.add_argument("--levels", type=int, default=LEVELS)
-    ap.add_argument("--workload", default="gmg-pcg", choices=["gmg-pcg", "batch-heat", "stokes", "learned"])
+    ap.add_argument("--workload", default="gmg-pcg", choices=["gmg-pcg", "cg-small", "batch-heat", "stokes", "learned"])
     ap.add_argument("--profile", default=None,
                     choices=["solve-fp64", "solve-mixed", "solve-mixed-nograph", "spmv64", "spmv32"],
                     help="set up, run the named operation --warmup + 1 times and exit (for ncu captures)")
@@ -376,6 +376,19 @@ def run_ours(args):
     reps.close()
 
 
+def oracle_threads():
+    """All host threads this process may use, for the oracle loops the
+    reference runs as parallel streams (restriction, GMRES factors, Schwarz
+    patches of a colour); the COO SpMV and the vector updates stay serial as
+    in the reference."""
+    import oracle as O
+    try:
+        n = len(os.sched_getaffinity(0))
+    except Exception:
+        n = os.cpu_count() or 1
+    return O.set_threads(n)
+
+
 def cpu_baseline(h, tol, iters_hint):
     """The oracle (C restatement of the reference's FP64 PCG + GMG V-cycle),
     one host thread, on a bounded sample: 2 PCG iterations, scaled to the
@@ -387,11 +400,12 @@ def cpu_baseline(h, tol, iters_hint):
                             cycles=1, use_fmg=False)
     b = h.finest.rhs
     sample = 2
+    cores = oracle_threads()
     t0 = time.perf_counter()
     O.solve_pcg(mats[-1], mg, b, tol, maxit=sample)
     t = time.perf_counter() - t0
     per_it = t / sample
-    return {"value": per_it * max(iters_hint, 1), "unit": "s", "cores": 1, "kind": "port",
+    return {"value": per_it * max(iters_hint, 1), "unit": "s", "cores": cores, "kind": "port",
             "sample": f"{sample} PCG iterations (incl. setup residual) scaled to {iters_hint} iterations",
             "sample_s": t}
 
@@ -408,25 +422,24 @@ def run_reference(args):
                             cycles=1, use_fmg=False)
     b = h.finest.rhs
     tol = RTOL * float(np.linalg.norm(b))
-    # each step: 1 PCG iteration of the full-size solve; value = per-iteration
-    # time x the iterations the full solve takes (measured once below)
-    full = O.solve_pcg(mats[-1], mg, b, tol)
+    cores = oracle_threads()
+    # each step is one whole FP64 GMG-PCG solve from e0 (about 3 s on one
+    # host core for the SpMV, all cores for the restriction)
     times = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        O.solve_pcg(mats[-1], mg, b, tol, maxit=1)
+        full = O.solve_pcg(mats[-1], mg, b, tol)
         if i >= args.warmup:
             times.append(time.perf_counter() - t0)
-    per = statistics.mean(times)
-    val = per * full.iterations
+    val = statistics.mean(times)
     line = {"metric": METRIC, "value": val, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": val * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded sine-mode source, assembled Q2 system)",
             "config": {"workload": WORKLOAD, "dofs": int(h.finest.n), "parallelism": "cpu"},
             "impl": "reference",
             "iterations": full.iterations,
-            "cpu_baseline": {"value": val, "unit": "s", "cores": 1, "kind": "port",
-                             "sample": f"1 PCG iteration per step x {full.iterations} iterations of the full solve"},
+            "cpu_baseline": {"value": val, "unit": "s", "cores": cores, "kind": "port",
+                             "sample": f"one whole solve per step ({full.iterations} PCG iterations)"},
             "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -437,6 +450,65 @@ def _peaks():
             return json.load(f)
     except Exception:
         return {}
+
+
+def run_cg_small(args):
+    """-Lap u + 5u = f, Q1 on 64 x 64 cells (4,225 unknowns), 4 x 4 seeded sine
+    modes, unpreconditioned CG to 1e-10 * ||b|| from e0, FP64; the oracle CG
+    is timed on the whole solve beside it."""
+    import torch
+    from jfem_b200 import _native as N
+    from jfem_b200.linalg import DeviceMatrix, IterativeSolver
+    ctx = N.default_context()
+    h = problems_hierarchy(1, 64, 1, modes=4)
+    s = h.finest
+    A = DeviceMatrix(s.n, s.n, s.rows, s.cols, s.vals, ctx)
+    b = torch.tensor(s.rhs, device="cuda")
+    tol = 1e-10 * float(np.linalg.norm(s.rhs))
+    e0 = torch.zeros_like(b)
+    e0[0] = 1.0
+    solver = IterativeSolver(ctx=ctx)
+    ms = []
+    with ClockSampler(0) as clk:
+        for i in range(max(3, args.warmup) + args.steps):
+            x = e0.clone()
+            torch.cuda.synchronize()
+            if i == max(3, args.warmup):
+                clk.mark_start()
+            t0 = time.perf_counter()
+            solver.solve_device(N.CG, A, None, b, x, tol)
+            torch.cuda.synchronize()
+            if i >= max(3, args.warmup):
+                ms.append((time.perf_counter() - t0) * 1e3)
+        clk.mark_end()
+    it = solver.iterations
+    res = float(np.linalg.norm(s.rhs - A.spmv(x.cpu().numpy())))
+    cpu = None
+    if os.environ.get("JFEM_BENCH_NO_CPU") != "1":
+        import oracle as O
+        Ao = O.CooMatrix(s.n, s.n, s.rows, s.cols, s.vals)
+        ts = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            ref = O.solve_cg(Ao, s.rhs, tol)
+            ts.append(time.perf_counter() - t0)
+        cpu = {"value": statistics.median(ts), "unit": "s", "cores": 1, "kind": "port",
+               "sample": "the whole CG solve (median of 5); serial: the reference's CG has no parallel loop",
+               "iterations": ref.iterations}
+    line = {"metric": "time-to-1e-10 residual (s), unpreconditioned CG", "value": statistics.median(ms) / 1e3,
+            "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": statistics.median(ms), "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded 4x4 sine-mode source)",
+            "config": {"workload": "cg-small: -Lap u + 5u = f, Q1 64x64 cells, CG to 1e-10 ||b|| from e0",
+                       "dofs": s.n, "nnz": int(A.nnz)},
+            "iterations": it, "final_rel_residual": res / float(np.linalg.norm(s.rhs)),
+            "clocks": clk.summary(), "cpu_baseline": cpu}
+    print(json.dumps(line))
+
+
+def problems_hierarchy(p, cells, levels, modes):
+    from jfem_b200 import problems
+    return problems.hierarchy(p, cells >> (levels - 1), levels, mass=5.0, modes=modes, seed=SEED)
 
 
 def run_batch_heat(args):
@@ -482,7 +554,8 @@ def run_batch_heat(args):
             n_s += s.K.n
         t = time.perf_counter() - t0
         cpu = {"value": t / n_s * dofs * steps, "unit": "s", "cores": 1, "kind": "port",
-               "sample": f"one CG step (1e-10) of {len(pick)} systems, scaled by unknowns to 256 systems x 50 steps"}
+               "sample": f"one CG step (1e-10) of {len(pick)} systems, scaled by unknowns to 256 systems x 50 steps; "
+                         "serial: the reference's CG has no parallel loop"}
     line = {"metric": "time for 50 implicit-Euler steps of 256 uneven Q1 heat systems (s)",
             "value": statistics.median(ms) / 1e3, "unit": "s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": statistics.median(ms), "higher_is_better": False,
@@ -495,11 +568,47 @@ def run_batch_heat(args):
     print(json.dumps(line))
 
 
+def stokes_cpu_sample(cells=64):
+    """The oracle (GMRES(50) + block-diagonal preconditioner with the coloured
+    Schwarz-smoothed velocity V-cycle, one host thread) solved whole on a
+    smaller Taylor-Hood grid; the per-iteration time is scaled by unknowns to
+    the full grid.  The Schwarz patches and colours come from the GPU solver's
+    own decomposition of that grid."""
+    import oracle as O
+    from jfem_b200 import _native as N
+    from jfem_b200.stokes import StokesSolver, stokes_problem
+    prob = stokes_problem(cells, 4, seed=0, pin_pressure=False)
+    sol = StokesSolver(N.default_context(), prob)
+    L = len(prob.spaces)
+    t0 = time.perf_counter()
+    mats = [O.CooMatrix(t.nv, t.nv, *prob.velocity_blocks[l]) for l, t in enumerate(prob.spaces)]
+    prol = [O.CooMatrix(prob.spaces[l + 1].nv, prob.spaces[l].nv, *prob.prolongations[l]) for l in range(L - 1)]
+    mg = O.MGPreconditioner(mats, prol, prob.velocity_boundary, [None] + [(O.SMOOTH_JACOBI, 1, 1.0)] * (L - 1),
+                            cycles=1, use_fmg=False)
+    keep = []
+    for l in range(1, L):
+        sw = sol.schwarz[l - 1]
+        So = O.Schwarz(mats[l], O.SCHWARZ_COLORED, sw.patches, 1.0, colours=sw.colours)
+        keep.append(So)
+        mg.set_schwarz(l, So, 1)
+    s = prob.system
+    A = O.CooMatrix(s.n, s.n, s.rows, s.cols, s.vals)
+    P = O.BlockDiagonal(mg, prob.pressure_inverse)
+    setup = time.perf_counter() - t0
+    cores = oracle_threads()
+    b = s.rhs
+    t0 = time.perf_counter()
+    ref = O.solve_gmres(A, b, RTOL * float(np.linalg.norm(b)), M=P, restart=50)
+    t = time.perf_counter() - t0
+    return {"n": s.n, "iterations": ref.iterations, "solve_s": t, "setup_s": setup, "cells": cells, "cores": cores}
+
+
 def run_stokes(args):
     """Taylor-Hood Stokes on 256x256 cells, GMRES(50) + block-diagonal
     preconditioner to 1e-8, variants of the velocity smoother and precision."""
     import torch
     from jfem_b200 import _native as N
+    from jfem_b200.linalg import DeviceMatrix
     from jfem_b200.stokes import StokesSolver, stokes_problem
     ctx = N.default_context()
     t0 = time.time()
@@ -537,6 +646,19 @@ def run_stokes(args):
                                          "overlap, 9 colours) | nu / lumped pressure mass",
                        "pressure": "consistent singular system, gauge p0 = 0 after the solve"},
             "variants": out, "assemble_s": assemble_s}
+    A64 = DeviceMatrix(s.n, s.n, s.rows, s.cols, s.vals, ctx)
+    ms64 = A64.time_spmv(precision=0, iters=50)
+    line["spmv_gbs_fp64"] = spmv_bytes(s.n, A64.nnz, 8, 8) / (ms64 * 1e-3) / 1e9
+    del A64
+    if os.environ.get("JFEM_BENCH_NO_CPU") != "1":
+        c = stokes_cpu_sample()
+        it = out["schwarz_fp64"]["iterations"]
+        line["cpu_baseline"] = {"value": c["solve_s"] / c["iterations"] * (s.n / c["n"]) * it, "unit": "s",
+                                "cores": c["cores"], "kind": "port",
+                                "sample": f"whole oracle solve on {c['cells']}x{c['cells']} cells ({c['n']} unknowns, "
+                                          f"{c['iterations']} iterations, {c['solve_s']:.2f} s), per iteration "
+                                          f"scaled by unknowns to {s.n} and to {it} iterations",
+                                "sample_setup_s": c["setup_s"]}
     print(json.dumps(line))
 
 
@@ -544,9 +666,11 @@ def run_learned(args):
     """FGMRES(30) + FP32 V-cycle + learned smoother vs FP64 GMG-PCG."""
     from jfem_b200 import _native as N
     from jfem_b200.learned import WEIGHTS, evaluate
+    from jfem_b200.learned import KappaSystem
     ctx = N.default_context()
     w = np.load(WEIGHTS)
-    out = evaluate(ctx, w, cells=1024, kseed=0, out_scales=(1.0, 0.5), repeats=max(3, args.steps))
+    ks = KappaSystem(ctx, 1024, kseed=0)
+    out = evaluate(ctx, w, cells=1024, kseed=0, out_scales=(1.0, 0.5), repeats=max(3, args.steps), ks=ks)
     with open(WEIGHTS.replace(".npy", ".train.json")) as f:
         train = json.load(f)
     best = min(v["time_s"] for v in out["fgmres_vcycle_net"].values())
@@ -557,6 +681,12 @@ def run_learned(args):
             "config": {"workload": "learned: -div(kappa grad u) = f, Q1 1024x1024, kappa = exp(GRF l=0.05 s2=1)",
                                    "training": train},
             "speedup_vs_fp64_gmg_pcg": out["gmg_pcg_fp64"]["time_s"] / best, "arms": out}
+    ms64 = ks.A.time_spmv(precision=0, iters=50)
+    ms32 = ks.A.time_spmv(precision=1, iters=50)
+    line["spmv_gbs"] = {"fp64": spmv_bytes(ks.n, ks.A.nnz, 8, 8) / (ms64 * 1e-3) / 1e9,
+                        "fp32": spmv_bytes(ks.n, ks.A.nnz, 4, 4) / (ms32 * 1e-3) / 1e9}
+    if os.environ.get("JFEM_BENCH_NO_CPU") != "1":
+        line["cpu_baseline"] = cpu_baseline(ks.h, out["tol"], out["gmg_pcg_fp64"]["iterations"])
     print(json.dumps(line))
 
 
@@ -567,6 +697,8 @@ def main():
             print(json.dumps({"impl": "reference", "unavailable": "the reference arm covers the gmg-pcg workload"}))
             return
         run_reference(args)
+    elif args.workload == "cg-small":
+        run_cg_small(args)
     elif args.workload == "batch-heat":
         run_batch_heat(args)
     elif args.workload == "stokes":

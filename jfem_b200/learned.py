@@ -244,11 +244,13 @@ def _train_residual(ctx, cells, fields, pairs, steps, batch, lr, seed, log):
     return net.get_weights(), report
 
 
-def evaluate(ctx, weights, cells=1024, kseed=0, tol_rel=1e-8, restart=30, out_scales=(1.0,), repeats=3):
+def evaluate(ctx, weights, cells=1024, kseed=0, tol_rel=1e-8, restart=30, out_scales=(1.0,), repeats=3, ks=None):
     """Time-to-tolerance on one kappa field: FP64 GMG-PCG, FGMRES(restart)
     with the FP32 V-cycle alone, and with the V-cycle + network; the solve is
-    repeated and the best time kept (the first run also captures graphs)."""
-    ks = KappaSystem(ctx, cells, kseed=kseed)
+    repeated and the best time kept (the first run also captures graphs).
+    ks: an already built KappaSystem of that field (built here if None)."""
+    if ks is None:
+        ks = KappaSystem(ctx, cells, kseed=kseed)
     b = torch.tensor(ks.b, device="cuda")
     tol = tol_rel * float(np.linalg.norm(ks.b))
     net = LearnedSmoother(ctx, weights=weights)

@@ -25,8 +25,19 @@ SMOOTH_JACOBI, SMOOTH_RICHARDSON = 0, 1
 def build(force: bool = False) -> str:
     """Compile the oracle with gcc (recipe also in oracle/Makefile)."""
     if force or not os.path.exists(_LIB) or os.path.getmtime(_LIB) < os.path.getmtime(_SRC):
-        subprocess.check_call(["gcc", "-O2", "-fPIC", "-shared", "-o", _LIB, _SRC, "-lm"])
+        subprocess.check_call(["gcc", "-O2", "-fPIC", "-fopenmp", "-shared", "-o", _LIB, _SRC, "-lm"])
     return _LIB
+
+
+def set_threads(n: int) -> int:
+    """Threads of the loops the reference runs as parallel streams; returns
+    the count in effect."""
+    lib().or_set_threads(int(n))
+    return lib().or_threads()
+
+
+def threads() -> int:
+    return lib().or_threads()
 
 
 class _Info(C.Structure):
@@ -49,6 +60,8 @@ def lib():
         L.or_mat_free.argtypes = [_P]
         for f in ("or_mat_mvmul", "or_mat_tvmul", "or_mat_mvmul_rows", "or_mat_tvmul_cols"):
             getattr(L, f).argtypes = [_P, _D, _D]
+        L.or_set_threads.argtypes = [C.c_int]
+        L.or_threads.restype = C.c_int
         L.or_mat_diag.argtypes = [_P, _D]
         L.or_mat_dense.argtypes = [_P, _D]
         L.or_jrandom_doubles.argtypes = [C.c_longlong, C.c_longlong, _D]

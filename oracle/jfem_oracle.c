@@ -25,12 +25,23 @@
  *   - java.util.Random (48-bit LCG, nextDouble) for the seeded fixtures of the
  *     reference tests (linalg/SparseMvMulTest.java:12-113).
  *
+ * Threads: the loops the reference runs as Java parallel streams when
+ * PerformanceArguments.parallelizeThreads is set (PerformanceArguments.java:24)
+ * run as OpenMP loops here -- SparseMvMul.mvMul/tvMul rows/columns
+ * (SparseMvMul.java:81-84, 103-106), the GMRES orthogonality factors
+ * (GMRES.java:203-210) and the patches of one colour
+ * (ColoredMultiplicativeSubspaceCorrection.java:91-111).  Each output element
+ * is computed by one thread in the serial order, so the results do not depend
+ * on the thread count.  Everything else, the COO scatter SpMV included, is
+ * serial as in the reference.  or_set_threads() sets the count.
+ *
  * Deviations, all documented: solvers carry an iteration/restart cap so that no
  * call can run forever (the reference's GMRES restarts without bound while the
  * true residual exceeds tol, GMRES.java:92; GMRES2 loops without bound,
  * GMRES2.java:70).
  */
 #include <math.h>
+#include <omp.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -182,9 +193,13 @@ void or_mat_tvmul(const or_mat* m, const double* x, double* y)
     for (long long k = 0; k < m->nnz; k++) y[m->ci[k]] += m->v[k] * x[m->ri[k]];
 }
 
+void or_set_threads(int n) { omp_set_num_threads(n > 0 ? n : 1); }
+int or_threads(void) { return omp_get_max_threads(); }
+
 /* SparseMvMul.mvMul (SparseMvMul.java:73-94): row-bucketed dot per row. */
 void or_mat_mvmul_rows(const or_mat* m, const double* x, double* y)
 {
+#pragma omp parallel for schedule(static)
     for (int r = 0; r < m->rows; r++) {
         double s = 0;
         for (long long p = m->rp[r]; p < m->rp[r + 1]; p++) s += m->rv[p] * x[m->rc[p]];
@@ -195,6 +210,7 @@ void or_mat_mvmul_rows(const or_mat* m, const double* x, double* y)
 /* SparseMvMul.tvMul (SparseMvMul.java:96-116): column-bucketed dot per column. */
 void or_mat_tvmul_cols(const or_mat* m, const double* x, double* y)
 {
+#pragma omp parallel for schedule(static)
     for (int c = 0; c < m->cols; c++) {
         double s = 0;
         for (long long p = m->cp[c]; p < m->cp[c + 1]; p++) s += m->cv[p] * x[m->cr[p]];
@@ -540,6 +556,7 @@ int or_solve_gmres(const or_op* A, const or_op* M, const double* b, double* x, d
         for (j = 0; j < n; j++) {
             A->mv(A, V[j], t);
             if (M) M->mv(M, t, q); else memcpy(q, t, sizeof(double) * n);
+#pragma omp parallel for schedule(static)
             for (int i = 0; i < nv; i++) fac[i] = vdot(n, V[i], q);     /* calculateOrthogonalityFactors */
             memset(w, 0, sizeof(double) * n);                         /* linearCombination */
             for (int i = 0; i < nv; i++)
@@ -927,6 +944,7 @@ static void colour_upgrade(const or_schwarz* S, const int* patches, int count, d
 {
     residual(S, rhs, x, r);
     double** comps = (double**)malloc(sizeof(double*) * (count ? count : 1));
+#pragma omp parallel for schedule(dynamic, 4)
     for (int q = 0; q < count; q++) {
         comps[q] = vnew(S->n);
         patch_component(S, patches[q], r, comps[q]);
