@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cells", type=int, default=CELLS)
     ap.add_argument("--levels", type=int, default=LEVELS)
-    ap.add_argument("--workload", default="gmg-pcg", choices=["gmg-pcg", "cg-small", "batch-heat", "stokes", "learned"])
+    ap.add_argument("--workload", default="gmg-pcg", choices=["gmg-pcg", "cg-small", "batch-heat", "stokes", "learned", "galerkin"])
     ap.add_argument("--profile", default=None,
                     choices=["solve-fp64", "solve-mixed", "solve-mixed-nograph", "spmv64", "spmv32"],
                     help="set up, run the named operation --warmup + 1 times and exit (for ncu captures)")
@@ -506,6 +506,70 @@ def run_cg_small(args):
     print(json.dumps(line))
 
 
+def run_galerkin(args):
+    """Set-up of an AMG-from-matrix hierarchy: the Galerkin coarse systems
+    (P^T A) P of the Q2 512x512 finest matrix down 8 levels on the GPU
+    (AMGFromMatrix), timed per hierarchy; the oracle builds the same chain on
+    the host.  A check: on interior nodes the Galerkin operator of nested
+    conforming spaces equals the assembled coarse operator."""
+    import torch
+    from jfem_b200 import _native as N
+    from jfem_b200.linalg import DeviceMatrix
+    ctx = N.default_context()
+    h = build_problem(args.cells, args.levels)
+    L = len(h.systems)
+    fine = h.finest
+    A = DeviceMatrix(fine.n, fine.n, fine.rows, fine.cols, fine.vals, ctx)
+    P = [DeviceMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l], ctx) for l in range(L - 1)]
+
+    def chain():
+        out, M = [], A
+        for l in range(L - 2, -1, -1):
+            M = M.galerkin(P[l])
+            out.append(M)
+        return out
+
+    for _ in range(max(1, args.warmup)):
+        chain()
+    ts = []
+    for _ in range(max(1, args.steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        levels = chain()
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t0)
+    # interior rows and columns of the first coarse level against the assembled matrix
+    C = levels[0]
+    sc = h.systems[L - 2]
+    Ac = DeviceMatrix(sc.n, sc.n, sc.rows, sc.cols, sc.vals, ctx)
+    inner = np.ones(sc.n, bool)
+    inner[np.asarray(h.boundary[L - 2], dtype=np.int64)] = False
+    x = np.where(inner, np.random.default_rng(0).standard_normal(sc.n), 0.0)
+    d = np.where(inner, C.spmv(x) - Ac.spmv(x), 0.0)
+    rel = float(np.linalg.norm(d) / np.linalg.norm(np.where(inner, Ac.spmv(x), 0.0)))
+    cpu = None
+    if os.environ.get("JFEM_BENCH_NO_CPU") != "1":
+        import oracle as O
+        Ao = O.CooMatrix(fine.n, fine.n, *A.coo())
+        Po = [O.CooMatrix(p.rows, p.cols, *p.coo()) for p in P]
+        t0 = time.perf_counter()
+        M = Ao
+        for l in range(L - 2, -1, -1):
+            M = Po[l].tmmul(M).mmmul(Po[l])
+        t = time.perf_counter() - t0
+        cpu = {"value": t, "unit": "s", "cores": 1, "kind": "port",
+               "sample": "the whole chain, Gustavson restatement of SparseMatrix.mmMul (the reference's own "
+                         "mmMul loops over every column of B for every row of A)"}
+    line = {"metric": "time to build the Galerkin coarse systems (s)", "value": statistics.median(ts), "unit": "s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (assembled Q2 system)",
+            "config": {"workload": f"galerkin: (P^T A) P, Q2 {args.cells}x{args.cells}, {L} levels",
+                       "dofs": fine.n, "nnz": int(A.nnz)},
+            "coarse_nnz": [int(m.nnz) for m in levels],
+            "interior_rel_diff_vs_assembled": rel, "cpu_baseline": cpu}
+    print(json.dumps(line))
+
+
 def problems_hierarchy(p, cells, levels, modes):
     from jfem_b200 import problems
     return problems.hierarchy(p, cells >> (levels - 1), levels, mass=5.0, modes=modes, seed=SEED)
@@ -697,6 +761,8 @@ def main():
             print(json.dumps({"impl": "reference", "unavailable": "the reference arm covers the gmg-pcg workload"}))
             return
         run_reference(args)
+    elif args.workload == "galerkin":
+        run_galerkin(args)
     elif args.workload == "cg-small":
         run_cg_small(args)
     elif args.workload == "batch-heat":

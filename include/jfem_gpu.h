@@ -45,6 +45,10 @@ int jfg_destroy(jfg_ctx* ctx);
 const char* jfg_last_error(jfg_ctx* ctx);
 /* Waits for all work queued on the context's stream. */
 int jfg_synchronize(jfg_ctx* ctx);
+/* Frees the grow-only scratch the sparse products keep in the context (up to
+ * ~70 bytes per product of the largest row chunk, i.e. a few GB after a
+ * Galerkin product of a 1 M-row matrix).  Not part of the reference surface. */
+int jfg_release_scratch(jfg_ctx* ctx);
 /* The context's CUDA stream (cudaStream_t) for callers that time or order work. */
 void* jfg_stream(jfg_ctx* ctx);
 /* Library version string. */
@@ -79,6 +83,24 @@ int jfg_spmv_t_dev(jfg_mat* m, const double* d_x, double* d_y);
 int jfg_spmv_f32_dev(jfg_mat* m, const float* d_x, float* d_y);
 /* Diagonal with duplicates summed.  Replaces Matrix.diag (Core/src/main/java/linalg/Matrix.java:157-175). */
 int jfg_matrix_diag(jfg_mat* m, double* h_diag);
+/* The merged CSR of the matrix (rows sorted, columns ascending within a row):
+ * h_ptr[n_rows + 1], h_col[nnz], h_val[nnz] (sizes from jfg_matrix_info).
+ * Replaces reading SparseMatrix.getCoordinateEntryList (SparseMatrix.java:403-417). */
+int jfg_matrix_csr(jfg_mat* m, int* h_ptr, int* h_col, double* h_val);
+/* Sparse products on the device; *out is a new matrix owned by the caller
+ * (jfg_matrix_free).  Each entry is the sum over k of the rounded products
+ * a_ik * b_kj, added from 0 in ascending k without fused multiply-adds;
+ * entries whose sum is exactly zero are not stored (SparseMatrix.add skips
+ * zeros, SparseMatrix.java:289).  JFG_ERR_BAD_ARG on incompatible sizes.
+ *   jfg_matrix_mmmul:    C = A B    -- SparseMatrix.mmMul (SparseMatrix.java:549-593)
+ *   jfg_matrix_tmmul:    C = A^T B  -- Matrix.tmMul (Core/src/main/java/linalg/Matrix.java:142-148)
+ *   jfg_matrix_galerkin: C = (R A) P, or (P^T A) P when r is NULL -- the coarse
+ *     systems of AMGSpace.createSystems (Core/src/main/java/multigrid/AMGSpace.java:60-78)
+ *     and MGPreconditionerInterface.AMGFromMatrix
+ *     (Core/src/main/java/multigrid/MGPreconditionerInterface.java:387-402), same association. */
+int jfg_matrix_mmmul(jfg_mat* a, jfg_mat* b, jfg_mat** out);
+int jfg_matrix_tmmul(jfg_mat* a, jfg_mat* b, jfg_mat** out);
+int jfg_matrix_galerkin(jfg_mat* r, jfg_mat* a, jfg_mat* p, jfg_mat** out);
 /* Times `iters` FP64 (precision 0) or FP32 (precision 1) products y = A x
  * on the context stream, each with CUDA events around the launch and the L2
  * flushed before it (a 256 MB buffer read between products, not timed); returns

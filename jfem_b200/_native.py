@@ -27,10 +27,12 @@ SCHWARZ_MULTIPLICATIVE, SCHWARZ_COLORED, SCHWARZ_ADDITIVE = 0, 1, 2
 
 # Every symbol include/jfem_gpu.h declares.
 EXPORTED = [
-    "jfg_create", "jfg_destroy", "jfg_last_error", "jfg_synchronize", "jfg_stream", "jfg_version",
+    "jfg_create", "jfg_destroy", "jfg_last_error", "jfg_synchronize", "jfg_release_scratch", "jfg_stream",
+    "jfg_version",
     "jfg_kernel_launches",
     "jfg_matrix_from_coo", "jfg_matrix_free", "jfg_matrix_info", "jfg_spmv", "jfg_spmv_t", "jfg_spmv_dev",
     "jfg_spmv_t_dev", "jfg_spmv_f32_dev", "jfg_matrix_diag", "jfg_spmv_time", "jfg_smooth",
+    "jfg_matrix_csr", "jfg_matrix_mmmul", "jfg_matrix_tmmul", "jfg_matrix_galerkin",
     "jfg_mg_create", "jfg_mg_free", "jfg_mg_apply", "jfg_mg_vcycle", "jfg_mg_fmg",
     "jfg_solver_opts_default", "jfg_solve", "jfg_solve_dev",
     "jfg_dense_solve", "jfg_dense_inverse", "jfg_sparse_solve", "jfg_cg_noalloc",
@@ -102,6 +104,7 @@ def load():
     L.jfg_last_error.restype = C.c_char_p
     L.jfg_last_error.argtypes = [_P]
     L.jfg_synchronize.argtypes = [_P]
+    L.jfg_release_scratch.argtypes = [_P]
     L.jfg_stream.restype = _P
     L.jfg_stream.argtypes = [_P]
     L.jfg_version.restype = C.c_char_p
@@ -115,6 +118,10 @@ def load():
         getattr(L, f).argtypes = [_P, _P, _P]
     L.jfg_matrix_diag.argtypes = [_P, _D]
     L.jfg_spmv_time.argtypes = [_P, C.c_int, C.c_int, _D]
+    L.jfg_matrix_csr.argtypes = [_P, _I, _I, _D]
+    for f in ("jfg_matrix_mmmul", "jfg_matrix_tmmul"):
+        getattr(L, f).argtypes = [_P, _P, C.POINTER(_P)]
+    L.jfg_matrix_galerkin.argtypes = [_P, _P, _P, C.POINTER(_P)]
     L.jfg_smooth.argtypes = [_P, C.POINTER(SmootherDesc), _D, _D]
     L.jfg_mg_create.argtypes = [_P, C.c_int, C.POINTER(_P), C.POINTER(_P), C.POINTER(_I), _I,
                                 C.POINTER(SmootherDesc), C.POINTER(MGDesc), C.POINTER(_P)]

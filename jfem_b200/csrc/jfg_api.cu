@@ -154,6 +154,17 @@ int jfg_synchronize(jfg_ctx* ctx)
     });
 }
 
+int jfg_release_scratch(jfg_ctx* ctx)
+{
+    if (!ctx) return JFG_ERR_BAD_ARG;
+    return guard(ctx, [&]() -> int {
+        JFG_CUDA(cudaStreamSynchronize(ctx->c.stream));
+        ctx->c.gemm_rows.release();
+        ctx->c.gemm_ws.release();
+        return JFG_OK;
+    });
+}
+
 void* jfg_stream(jfg_ctx* ctx) { return ctx ? (void*)ctx->c.stream : nullptr; }
 
 int jfg_kernel_launches(uint64_t* count)
@@ -271,6 +282,54 @@ int jfg_matrix_diag(jfg_mat* m, double* h_diag)
         stage_out(ctx, m->m->diag.p, h_diag, n);
         return JFG_OK;
     });
+}
+
+int jfg_matrix_csr(jfg_mat* m, int* h_ptr, int* h_col, double* h_val)
+{
+    if (!m || !h_ptr || (m->m->nnz && (!h_col || !h_val))) return JFG_ERR_BAD_ARG;
+    jfg_ctx* ctx = m->ctx;
+    return guard(ctx, [&]() -> int {
+        cudaStream_t s = ctx->c.stream;
+        const jfg::Matrix* M = m->m;
+        JFG_CUDA(cudaMemcpyAsync(h_ptr, M->csr_ptr.p, sizeof(int) * ((size_t)M->rows + 1), cudaMemcpyDeviceToHost, s));
+        if (M->nnz) {
+            JFG_CUDA(cudaMemcpyAsync(h_col, M->csr_col.p, sizeof(int) * M->nnz, cudaMemcpyDeviceToHost, s));
+            JFG_CUDA(cudaMemcpyAsync(h_val, M->csr_val.p, sizeof(double) * M->nnz, cudaMemcpyDeviceToHost, s));
+        }
+        JFG_CUDA(cudaStreamSynchronize(s));
+        return JFG_OK;
+    });
+}
+
+static int wrap_product(jfg_ctx* ctx, jfg_mat** out, const std::function<jfg::Matrix*()>& f)
+{
+    *out = nullptr;
+    return guard(ctx, [&]() -> int {
+        jfg::Matrix* m = f();
+        auto* h = new jfg_mat();
+        h->ctx = ctx;
+        h->m = m;
+        *out = h;
+        return JFG_OK;
+    });
+}
+
+int jfg_matrix_mmmul(jfg_mat* a, jfg_mat* b, jfg_mat** out)
+{
+    if (!a || !b || !out || a->ctx != b->ctx) return JFG_ERR_BAD_ARG;
+    return wrap_product(a->ctx, out, [&] { return jfg::matrix_mmmul(a->m, b->m); });
+}
+
+int jfg_matrix_tmmul(jfg_mat* a, jfg_mat* b, jfg_mat** out)
+{
+    if (!a || !b || !out || a->ctx != b->ctx) return JFG_ERR_BAD_ARG;
+    return wrap_product(a->ctx, out, [&] { return jfg::matrix_tmmul(a->m, b->m); });
+}
+
+int jfg_matrix_galerkin(jfg_mat* r, jfg_mat* a, jfg_mat* p, jfg_mat** out)
+{
+    if (!a || !p || !out || a->ctx != p->ctx || (r && r->ctx != a->ctx)) return JFG_ERR_BAD_ARG;
+    return wrap_product(a->ctx, out, [&] { return jfg::matrix_galerkin(r ? r->m : nullptr, a->m, p->m); });
 }
 
 // Reads a buffer larger than the L2 (clean lines only, so the next kernel's

@@ -124,6 +124,7 @@ struct Matrix {
     DevBuf<__nv_bfloat16> val16;  // optional BF16 copy
     DevBuf<double> diag;          // merged diagonal
     int has32 = 0, has16 = 0;
+    int csr_only = 0;             // no SELL layout (an intermediate of a sparse product)
     Matrix* transposed = nullptr; // lazily built for tvMul
     uint64_t uid = 0;             // unique id (keys of cached CUDA graphs)
     Matrix();
@@ -138,6 +139,8 @@ struct Context {
     DevBuf<double> partials;      // kVecGrid * 4 or nblocks * 4 doubles
     DevBuf<unsigned> counters;    // last-block counters
     DevBuf<double> scal;          // small scalar results
+    // grow-only scratch of the sparse products (per-row counts; products and sort space)
+    DevBuf<char> gemm_rows, gemm_ws;
 };
 
 // host-side helpers implemented in jfg_matrix.cu
@@ -146,6 +149,14 @@ Matrix* matrix_from_coo(Context* c, int rows, int cols, int64_t nnz, const int* 
 Matrix* matrix_from_csr_host(Context* c, int rows, int cols, const std::vector<int64_t>& rp,
                              const std::vector<int>& ci, const std::vector<double>& v);
 Matrix* matrix_transpose(Matrix* m);
+// merged, sorted (key = row * cols + col ascending), zero-free entries on the device -> Matrix
+// (sell = false: CSR only, no SpMV layout -- for intermediates of products)
+Matrix* matrix_from_sorted_keys(Context* c, int rows, int cols, int64_t m, const uint64_t* d_key,
+                                const double* d_val, bool sell = true);
+// sparse products (jfg_spgemm.cu)
+Matrix* matrix_mmmul(Matrix* a, Matrix* b, bool sell = true);
+Matrix* matrix_tmmul(Matrix* a, Matrix* b, bool sell = true);
+Matrix* matrix_galerkin(Matrix* r, Matrix* a, Matrix* p);
 void matrix_ensure_fp32(Matrix* m);
 void matrix_ensure_bf16(Matrix* m);
 uint64_t next_uid();

@@ -164,7 +164,7 @@ __global__ void k_to_bf16(int64_t n, const double* a, __nv_bfloat16* b)
 // Builds CSR and SELL-32-sigma from merged, sorted, zero-free COO that is
 // already on the device (keys = row*cols+col ascending, values alongside).
 static Matrix* build_from_sorted(Context* c, int rows, int cols, int64_t m, const uint64_t* d_key,
-                                 const double* d_val)
+                                 const double* d_val, bool sell = true)
 {
     cudaStream_t s = c->stream;
     JFG_CHECK(m < (int64_t)INT32_MAX - 64, JFG_ERR_UNSUPPORTED, "matrix has more than 2^31 nonzeros");
@@ -195,6 +195,11 @@ static Matrix* build_from_sorted(Context* c, int rows, int cols, int64_t m, cons
     M->diag.alloc((size_t)rows);
     if (rows) k_diag<<<nblk(rows), 256, 0, s>>>(rows, cols, M->csr_ptr.p, M->csr_col.p, M->csr_val.p, M->diag.p);
     JFG_CUDA(cudaGetLastError());
+    if (!sell) {
+        M->csr_only = 1;
+        JFG_CUDA(cudaStreamSynchronize(s));
+        return M;
+    }
     // SELL-32-sigma: sort rows by length (descending, stable) inside windows
     int nslices = (rows + kSliceRows - 1) / kSliceRows;
     std::vector<int> perm((size_t)nslices * kSliceRows, -1);
@@ -258,6 +263,12 @@ static Matrix* build_from_sorted(Context* c, int rows, int cols, int64_t m, cons
     }
     JFG_CUDA(cudaStreamSynchronize(s));
     return M;
+}
+
+Matrix* matrix_from_sorted_keys(Context* c, int rows, int cols, int64_t m, const uint64_t* d_key,
+                                const double* d_val, bool sell)
+{
+    return build_from_sorted(c, rows, cols, m, d_key, d_val, sell);
 }
 
 // COO on the device -> Matrix (sort, merge duplicates, drop zeros).

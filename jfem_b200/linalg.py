@@ -152,6 +152,30 @@ class SparseMatrix(VectorMultiplyable):
     def diag(self):
         return self.device().diag()
 
+    def _from_device(self, d: "DeviceMatrix") -> "SparseMatrix":
+        ri, ci, v = d.coo()
+        out = SparseMatrix.from_coo(d.rows, d.cols, ri, ci, v, self._ctx)
+        out._dev = d
+        return out
+
+    def mmMul(self, matrix: "SparseMatrix") -> "SparseMatrix":
+        """SparseMatrix.mmMul (SparseMatrix.java:549-593): the product on the
+        GPU, returned as a new SparseMatrix (merged triples, zero sums not stored)."""
+        if self.cols != matrix.rows:
+            raise IllegalArgumentException("Incompatible sizes")
+        return self._from_device(self.device().mmMul(matrix.device()))
+
+    def tmMul(self, matrix: "SparseMatrix") -> "SparseMatrix":
+        """Matrix.tmMul (Matrix.java:142-148): self^T * matrix."""
+        if self.rows != matrix.rows:
+            raise IllegalArgumentException("Incompatible sizes")
+        return self._from_device(self.device().tmMul(matrix.device()))
+
+    def transpose(self) -> "SparseMatrix":
+        """SparseMatrix.transpose (SparseMatrix.java:469-478): triples with rows and columns exchanged."""
+        ri, ci, v = self.coo()
+        return SparseMatrix.from_coo(self.cols, self.rows, ci, ri, v, self._ctx)
+
     def solve(self, rhs):
         """SparseMatrix.solve (:142-145): the drop-in direct solve.  n <= 4096:
         dense LU on the GPU (the reference densifies and factorises too);
@@ -190,9 +214,60 @@ class DeviceMatrix:
         N.load().jfg_matrix_info(h, C.byref(r), C.byref(c), C.byref(nz))
         self.nnz = nz.value
 
+    @classmethod
+    def _adopt(cls, h, ctx):
+        """A DeviceMatrix owning the library matrix handle h."""
+        self = cls.__new__(cls)
+        self.ctx = ctx
+        self._h = h
+        r, c, nz = C.c_int(), C.c_int(), C.c_int64()
+        N.load().jfg_matrix_info(h, C.byref(r), C.byref(c), C.byref(nz))
+        self.rows, self.cols, self.nnz = r.value, c.value, nz.value
+        return self
+
     @property
     def handle(self):
         return self._h
+
+    def csr(self):
+        """(row pointers, columns, values) of the merged matrix, rows sorted
+        and columns ascending within a row."""
+        ptr = np.empty(self.rows + 1, dtype=np.int32)
+        col = np.empty(max(self.nnz, 1), dtype=np.int32)
+        val = np.empty(max(self.nnz, 1))
+        self.ctx.check(N.load().jfg_matrix_csr(self._h, N.iptr(ptr), N.iptr(col), N.dptr(val)))
+        return ptr, col[: self.nnz], val[: self.nnz]
+
+    def coo(self):
+        ptr, col, val = self.csr()
+        return np.repeat(np.arange(self.rows, dtype=np.int32), np.diff(ptr)), col, val
+
+    def _product(self, fn, *others):
+        h = C.c_void_p()
+        st = fn(*[o.handle if o is not None else None for o in (self, *others)], C.byref(h))
+        if st == N.ERR_BAD_ARG:
+            raise IllegalArgumentException(N.load().jfg_last_error(self.ctx.handle).decode())
+        self.ctx.check(st)
+        return DeviceMatrix._adopt(h, self.ctx)
+
+    def mmMul(self, other: "DeviceMatrix") -> "DeviceMatrix":
+        """SparseMatrix.mmMul (SparseMatrix.java:549-593) on the device."""
+        return self._product(N.load().jfg_matrix_mmmul, other)
+
+    def tmMul(self, other: "DeviceMatrix") -> "DeviceMatrix":
+        """Matrix.tmMul (Matrix.java:142-148): self^T * other on the device."""
+        return self._product(N.load().jfg_matrix_tmmul, other)
+
+    def galerkin(self, prolongation: "DeviceMatrix", restriction: "DeviceMatrix | None" = None) -> "DeviceMatrix":
+        """Coarse operator (R A) P, or (P^T A) P without R, with A = self
+        (AMGSpace.java:60-78, MGPreconditionerInterface.java:397-402)."""
+        h = C.c_void_p()
+        st = N.load().jfg_matrix_galerkin(restriction.handle if restriction is not None else None, self._h,
+                                          prolongation.handle, C.byref(h))
+        if st == N.ERR_BAD_ARG:
+            raise IllegalArgumentException(N.load().jfg_last_error(self.ctx.handle).decode())
+        self.ctx.check(st)
+        return DeviceMatrix._adopt(h, self.ctx)
 
     def spmv(self, x):
         x = N.f64(x)

@@ -89,6 +89,8 @@ class MGPreconditioner(VectorMultiplyable):
         self._h = h
         self.n = self._A[-1].rows
         self.cycles = cycles
+        self.use_fmg = use_fmg
+        self.precision = precision
 
     @property
     def handle(self):
@@ -110,6 +112,40 @@ class MGPreconditioner(VectorMultiplyable):
 
     def tvMul(self, vector):
         raise NotImplementedError("not implemented yet")   # MGPreconditionerInterface.java:381-385
+
+    def getSystem(self, level: int):
+        return self._A[level]
+
+    def getProlongationMatrix(self, level: int):
+        return self._P[level]
+
+    def maxLevel(self) -> int:
+        return len(self._A) - 1
+
+    def AMGFromMatrix(self, mat, levelToSmoother, isVerbose: bool = False, cycles: int | None = None,
+                      precision: str | None = None) -> "MGPreconditioner":
+        """MGPreconditionerInterface.AMGFromMatrix (MGPreconditionerInterface.java:387-471):
+        a hierarchy whose finest system is `mat` and whose coarser systems are
+        the Galerkin products P^T A P of the next finer one (P.tmMul(A).mmMul(P),
+        computed on the GPU), with this hierarchy's prolongations, boundary
+        handling of the transfers and level count up to the level of `mat`'s
+        size; levelToSmoother(l, A_l) gives the smoother of level l >= 1."""
+        A = _as_device(mat)
+        sizes = [a.rows for a in self._A]
+        if A.rows not in sizes:
+            raise IllegalArgumentException("Matrix needs to be of same shape as finest system")
+        level = max(l for l, n in enumerate(sizes) if n == A.rows)     # levelFromSize
+        if A.rows != self._A[level].rows or A.cols != self._A[level].cols:
+            raise IllegalArgumentException("Matrix needs to be of same shape as finest system")
+        systems = [A]
+        for i in range(1, level + 1):
+            systems.append(systems[-1].galerkin(self._P[level - i]))
+        systems.reverse()
+        self.ctx.check(N.load().jfg_release_scratch(self.ctx.handle))
+        smoothers = [None] + [levelToSmoother(l, systems[l]) for l in range(1, level + 1)]
+        return MGPreconditioner(systems, self._P[:level], self._bd[:level + 1], smoothers,
+                                cycles=self.cycles if cycles is None else cycles, use_fmg=self.use_fmg,
+                                precision=self.precision if precision is None else precision, ctx=self.ctx)
 
     def vCycle(self, initialIterate, rhs):
         x0, b = N.f64(initialIterate), N.f64(rhs)

@@ -25,7 +25,8 @@ SMOOTH_JACOBI, SMOOTH_RICHARDSON = 0, 1
 def build(force: bool = False) -> str:
     """Compile the oracle with gcc (recipe also in oracle/Makefile)."""
     if force or not os.path.exists(_LIB) or os.path.getmtime(_LIB) < os.path.getmtime(_SRC):
-        subprocess.check_call(["gcc", "-O2", "-fPIC", "-fopenmp", "-shared", "-o", _LIB, _SRC, "-lm"])
+        subprocess.check_call(["gcc", "-O2", "-fPIC", "-fopenmp", "-ffp-contract=off", "-shared", "-o", _LIB, _SRC,
+                               "-lm"])
     return _LIB
 
 
@@ -60,6 +61,11 @@ def lib():
         L.or_mat_free.argtypes = [_P]
         for f in ("or_mat_mvmul", "or_mat_tvmul", "or_mat_mvmul_rows", "or_mat_tvmul_cols"):
             getattr(L, f).argtypes = [_P, _D, _D]
+        L.or_mat_nnz.restype = C.c_longlong
+        L.or_mat_nnz.argtypes = [_P]
+        L.or_mat_coo.argtypes = [_P, _I, _I, _D]
+        L.or_mat_mmmul.restype = _P
+        L.or_mat_mmmul.argtypes = [_P, _P]
         L.or_set_threads.argtypes = [C.c_int]
         L.or_threads.restype = C.c_int
         L.or_mat_diag.argtypes = [_P, _D]
@@ -183,6 +189,29 @@ class CooMatrix:
         a = np.empty((self.rows, self.cols))
         lib().or_mat_dense(self._h, _d(a))
         return a
+
+    def mmmul(self, other: "CooMatrix") -> "CooMatrix":
+        """SparseMatrix.mmMul: self * other (row-major triples, zero sums dropped)."""
+        h = lib().or_mat_mmmul(self._h, other._h)
+        if not h:
+            raise ValueError("Incompatible sizes")
+        try:
+            m = lib().or_mat_nnz(h)
+            ri = np.empty(m, dtype=np.int32)
+            ci = np.empty(m, dtype=np.int32)
+            v = np.empty(m)
+            lib().or_mat_coo(h, _i(ri), _i(ci), _d(v))
+        finally:
+            lib().or_mat_free(h)
+        return CooMatrix(self.rows, other.cols, ri, ci, v)
+
+    def transpose(self) -> "CooMatrix":
+        """SparseMatrix.transpose (SparseMatrix.java:469-478): triples with rows and columns exchanged."""
+        return CooMatrix(self.cols, self.rows, self.ci, self.ri, self.v)
+
+    def tmmul(self, other: "CooMatrix") -> "CooMatrix":
+        """Matrix.tmMul (Matrix.java:142-148): transpose().mmMul(other)."""
+        return self.transpose().mmmul(other)
 
 
 def dense_solve(a, b):

@@ -179,11 +179,77 @@ void or_mat_free(or_mat* m)
 int or_mat_rows(const or_mat* m) { return m->rows; }
 int or_mat_cols(const or_mat* m) { return m->cols; }
 
+static int cmp_int_asc(const void* a, const void* b)
+{
+    int x = *(const int*)a, y = *(const int*)b;
+    return (x > y) - (x < y);
+}
+
 /* SparseMatrix.mvMul (SparseMatrix.java:480-489): COO scatter in storage order. */
 void or_mat_mvmul(const or_mat* m, const double* x, double* y)
 {
     memset(y, 0, sizeof(double) * m->rows);
     for (long long k = 0; k < m->nnz; k++) y[m->ri[k]] += m->v[k] * x[m->ci[k]];
+}
+
+long long or_mat_nnz(const or_mat* m) { return m->nnz; }
+
+/* The stored COO triples (for a product: row-major, columns ascending). */
+void or_mat_coo(const or_mat* m, int* ri, int* ci, double* v)
+{
+    if (!m->nnz) return;
+    memcpy(ri, m->ri, sizeof(int) * m->nnz);
+    memcpy(ci, m->ci, sizeof(int) * m->nnz);
+    memcpy(v, m->v, sizeof(double) * m->nnz);
+}
+
+/* SparseMatrix.mmMul (SparseMatrix.java:549-593): for every merged row i of A
+ * and every column j of B, contraction = sum over column j's entries (k, b_kj)
+ * of row_i[k] * b_kj, added with SparseMatrix.add (zero sums are not stored,
+ * SparseMatrix.java:289).  The reference visits a column's entries in HashMap
+ * order; here they are visited in ascending k, row by row with a dense
+ * accumulator (the sums of the touched columns are the column contractions;
+ * untouched columns contract to zero and are not stored). */
+or_mat* or_mat_mmmul(const or_mat* A, const or_mat* B)
+{
+    if (A->cols != B->rows) return NULL;
+    int n = B->cols;
+    double* acc = (double*)calloc(n > 0 ? n : 1, sizeof(double));
+    char* touched = (char*)calloc(n > 0 ? n : 1, 1);
+    int* list = (int*)malloc(sizeof(int) * (n > 0 ? n : 1));
+    long long cap = 1024, m = 0;
+    int* ri = (int*)malloc(sizeof(int) * cap);
+    int* ci = (int*)malloc(sizeof(int) * cap);
+    double* v = (double*)malloc(sizeof(double) * cap);
+    for (int i = 0; i < A->rows; i++) {
+        int cnt = 0;
+        for (long long p = A->rp[i]; p < A->rp[i + 1]; p++) {
+            int k = A->rc[p];
+            double a = A->rv[p];
+            for (long long q = B->rp[k]; q < B->rp[k + 1]; q++) {
+                int j = B->rc[q];
+                if (!touched[j]) { touched[j] = 1; list[cnt++] = j; acc[j] = 0.0; }
+                double prod = a * B->rv[q];
+                acc[j] = acc[j] + prod;
+            }
+        }
+        qsort(list, cnt, sizeof(int), cmp_int_asc);
+        for (int t = 0; t < cnt; t++) {
+            int j = list[t];
+            touched[j] = 0;
+            if (acc[j] == 0.0) continue;
+            if (m == cap) {
+                cap *= 2;
+                ri = (int*)realloc(ri, sizeof(int) * cap);
+                ci = (int*)realloc(ci, sizeof(int) * cap);
+                v = (double*)realloc(v, sizeof(double) * cap);
+            }
+            ri[m] = i; ci[m] = j; v[m] = acc[j]; m++;
+        }
+    }
+    or_mat* C = or_mat_new(A->rows, n, m, ri, ci, v);
+    free(acc); free(touched); free(list); free(ri); free(ci); free(v);
+    return C;
 }
 
 /* SparseMatrix.tvMul (SparseMatrix.java:492-501). */

@@ -131,3 +131,20 @@ def test_laplace_mg_gmres_pin():
         r = O.solve_gmres(mats[-1], b, 1e-8, M=mg)
         assert r.status == O.OK
         assert r.iterations < 10
+
+
+def test_oracle_mmmul_tmmul_dense():
+    """SparseMatrix.mmMul / Matrix.tmMul restatements against dense products;
+    exact-zero sums are not stored."""
+    rng = np.random.default_rng(11)
+    for (m, k, n) in ((30, 20, 25), (1, 7, 3)):
+        a = np.where(rng.random((m, k)) < 0.2, rng.integers(-3, 4, (m, k)), 0).astype(float)
+        b = np.where(rng.random((k, n)) < 0.2, rng.integers(-3, 4, (k, n)), 0).astype(float)
+        A = O.CooMatrix(m, k, *np.nonzero(a), a[np.nonzero(a)])
+        B = O.CooMatrix(k, n, *np.nonzero(b), b[np.nonzero(b)])
+        C = A.mmmul(B)
+        assert np.array_equal(C.dense(), a @ b)
+        assert C.v.size == np.count_nonzero(a @ b) and np.all(C.v != 0)
+        c = np.where(rng.random((m, n)) < 0.2, rng.standard_normal((m, n)), 0.0)
+        Cm = O.CooMatrix(m, n, *np.nonzero(c), c[np.nonzero(c)])
+        np.testing.assert_allclose(A.tmmul(Cm).dense(), a.T @ c, rtol=1e-14, atol=1e-14)
