@@ -110,19 +110,57 @@ int jfg_spmv_time(jfg_mat* m, int precision, int iters, double* ms_per_spmv);
 
 /* ---- smoothers ------------------------------------------------------- */
 typedef struct jfg_schwarz jfg_schwarz;
-typedef enum { JFG_SMOOTH_JACOBI = 0, JFG_SMOOTH_RICHARDSON = 1, JFG_SMOOTH_SCHWARZ = 2 } jfg_smoother_kind;
+typedef struct jfg_gs jfg_gs;
+typedef enum {
+    JFG_SMOOTH_JACOBI = 0,
+    JFG_SMOOTH_RICHARDSON = 1,
+    JFG_SMOOTH_SCHWARZ = 2,
+    JFG_SMOOTH_FBGS = 3,   /* ForwardBackwardGaussSeidelSmoother */
+    JFG_SMOOTH_GS = 4      /* GaussSeidelSmoother */
+} jfg_smoother_kind;
 typedef struct {
     int kind;      /* jfg_smoother_kind */
     int runs;      /* sweeps (Schwarz: SubspaceCorrection.apply calls) */
     double omega;  /* damping (Jacobi / Richardson; a Schwarz handle keeps its own) */
     jfg_schwarz* schwarz;  /* JFG_SMOOTH_SCHWARZ: the decomposition of this level's matrix */
+    jfg_gs* gs;            /* JFG_SMOOTH_FBGS / JFG_SMOOTH_GS: the triangular parts of this level's matrix */
 } jfg_smoother_desc;
 /* x <- smooth(A, rhs, x).  Replaces Smoother.smooth
  * (Core/src/main/java/multigrid/Smoother.java:15) as implemented by
- * JacobiSmoother.smooth (multigrid/JacobiSmoother.java:28-50) and
- * RichardsonSmoother.smooth (multigrid/RichardsonSmoother.java:31-50) and
- * SchwarzSmoother.smooth (schwarz/SchwarzSmoother.java:21-43). */
+ * JacobiSmoother.smooth (multigrid/JacobiSmoother.java:28-50),
+ * RichardsonSmoother.smooth (multigrid/RichardsonSmoother.java:31-50),
+ * SchwarzSmoother.smooth (schwarz/SchwarzSmoother.java:21-43),
+ * ForwardBackwardGaussSeidelSmoother.smooth (multigrid/ForwardBackwardGaussSeidelSmoother.java:23-44:
+ * runs x { x += L^-1 D U^-1 (b - A x) }, L / U the lower / upper triangles
+ * with the diagonal) and GaussSeidelSmoother.smooth
+ * (multigrid/GaussSeidelSmoother.java:24-32: runs x { x = (L + D)^-1 (b - R x) },
+ * R the strict upper triangle). */
 int jfg_smooth(jfg_mat* A, const jfg_smoother_desc* sm, const double* h_rhs, double* h_x);
+
+/* ---- Gauss-Seidel triangular parts ---------------------------------- */
+/* The lower and upper triangles of a square matrix in an ordering of its
+ * rows, with schedules of independent row sets for the two triangular
+ * solves.  Row i of a triangular solve computes, as
+ * LowerTriangularSparseMatrix / UpperTriangularSparseMatrix.solve do
+ * (linalg/LowerTriangularSparseMatrix.java:173-212,
+ * linalg/UpperTriangularSparseMatrix.java:185-221),
+ *     sol_i = rhs_i / d_i;  sol_i += (-sol_j / d_i) * a_ij  for its entries j
+ * (ascending column; the reference visits them in HashMap order).
+ *   JFG_GS_NATURAL     the matrix's own row order (the reference's algorithm);
+ *                      rows are grouped into dependency levels, so a solve
+ *                      takes as many steps as the longest dependency chain.
+ *   JFG_GS_MULTICOLOR  rows ordered colour by colour (greedy colouring of the
+ *                      graph of A + A^T in row order): the same smoothers
+ *                      applied to the symmetrically permuted system; one step
+ *                      per colour.
+ * JFG_ERR_SINGULAR when a diagonal entry is zero ("Singular Matrix"). */
+typedef enum { JFG_GS_NATURAL = 0, JFG_GS_MULTICOLOR = 1 } jfg_gs_ordering;
+int jfg_gs_create(jfg_ctx* ctx, jfg_mat* A, int ordering, jfg_gs** out);
+int jfg_gs_free(jfg_gs* g);
+/* Steps of the forward and backward solves, and colours (0 for natural). */
+int jfg_gs_info(jfg_gs* g, int* forward_levels, int* backward_levels, int* colours);
+/* Position of every row in the ordering (h_rank[n_rows]). */
+int jfg_gs_ranks(jfg_gs* g, int* h_rank);
 
 /* ---- overlapping Schwarz decompositions -------------------------------- */
 /* Subspace corrections over patches of DOFs with cached dense patch inverses.

@@ -8,8 +8,9 @@ grid assembler that produces the systems (``assembly``, ``problems``).
 from . import _native
 from .linalg import (DenseMatrix, DeviceMatrix, GMRES, IllegalArgumentException, IterativeSolver,
                      SingularMatrixException, SparseMatrix, VectorMultiplyable)
-from .multigrid import JacobiSmoother, MGPreconditioner, RichardsonSmoother
+from .multigrid import (ForwardBackwardGaussSeidelSmoother, GaussSeidelSmoother, JacobiSmoother,
+                        MGPreconditioner, RichardsonSmoother)
 
 __all__ = ["DenseMatrix", "DeviceMatrix", "GMRES", "IllegalArgumentException", "IterativeSolver",
            "SingularMatrixException", "SparseMatrix", "VectorMultiplyable", "JacobiSmoother",
-           "MGPreconditioner", "RichardsonSmoother"]
+           "MGPreconditioner", "RichardsonSmoother", "ForwardBackwardGaussSeidelSmoother", "GaussSeidelSmoother"]

@@ -22,7 +22,8 @@ CG, PCG, BICGSTAB, PBICGSTAB, GMRES, PGMRES, GMRES2, FGMRES = range(8)
 PREC_NONE, PREC_MG, PREC_JACOBI, PREC_MATRIX, PREC_MG_CNN, PREC_SCHWARZ, PREC_BLOCKDIAG = range(7)
 # jfg_precision
 FP64, MIXED, MIXED_PRECOND = 0, 1, 2
-SMOOTH_JACOBI, SMOOTH_RICHARDSON, SMOOTH_SCHWARZ = 0, 1, 2
+SMOOTH_JACOBI, SMOOTH_RICHARDSON, SMOOTH_SCHWARZ, SMOOTH_FBGS, SMOOTH_GS = 0, 1, 2, 3, 4
+GS_NATURAL, GS_MULTICOLOR = 0, 1
 SCHWARZ_MULTIPLICATIVE, SCHWARZ_COLORED, SCHWARZ_ADDITIVE = 0, 1, 2
 
 # Every symbol include/jfem_gpu.h declares.
@@ -33,6 +34,7 @@ EXPORTED = [
     "jfg_matrix_from_coo", "jfg_matrix_free", "jfg_matrix_info", "jfg_spmv", "jfg_spmv_t", "jfg_spmv_dev",
     "jfg_spmv_t_dev", "jfg_spmv_f32_dev", "jfg_matrix_diag", "jfg_spmv_time", "jfg_smooth",
     "jfg_matrix_csr", "jfg_matrix_mmmul", "jfg_matrix_tmmul", "jfg_matrix_galerkin",
+    "jfg_gs_create", "jfg_gs_free", "jfg_gs_info", "jfg_gs_ranks",
     "jfg_mg_create", "jfg_mg_free", "jfg_mg_apply", "jfg_mg_vcycle", "jfg_mg_fmg",
     "jfg_solver_opts_default", "jfg_solve", "jfg_solve_dev",
     "jfg_dense_solve", "jfg_dense_inverse", "jfg_sparse_solve", "jfg_cg_noalloc",
@@ -47,7 +49,8 @@ EXPORTED = [
 
 
 class SmootherDesc(C.Structure):
-    _fields_ = [("kind", C.c_int), ("runs", C.c_int), ("omega", C.c_double), ("schwarz", C.c_void_p)]
+    _fields_ = [("kind", C.c_int), ("runs", C.c_int), ("omega", C.c_double), ("schwarz", C.c_void_p),
+                ("gs", C.c_void_p)]
 
 
 class MGDesc(C.Structure):
@@ -122,6 +125,10 @@ def load():
     for f in ("jfg_matrix_mmmul", "jfg_matrix_tmmul"):
         getattr(L, f).argtypes = [_P, _P, C.POINTER(_P)]
     L.jfg_matrix_galerkin.argtypes = [_P, _P, _P, C.POINTER(_P)]
+    L.jfg_gs_create.argtypes = [_P, _P, C.c_int, C.POINTER(_P)]
+    L.jfg_gs_free.argtypes = [_P]
+    L.jfg_gs_info.argtypes = [_P, _I, _I, _I]
+    L.jfg_gs_ranks.argtypes = [_P, _I]
     L.jfg_smooth.argtypes = [_P, C.POINTER(SmootherDesc), _D, _D]
     L.jfg_mg_create.argtypes = [_P, C.c_int, C.POINTER(_P), C.POINTER(_P), C.POINTER(_I), _I,
                                 C.POINTER(SmootherDesc), C.POINTER(MGDesc), C.POINTER(_P)]

@@ -7,6 +7,7 @@
 
 #include "jfg_krylov.cuh"
 #include "jfg_schwarz.cuh"
+#include "jfg_gs.cuh"
 
 struct jfg_ctx {
     jfg::Context c;
@@ -408,9 +409,13 @@ int jfg_spmv_time(jfg_mat* m, int precision, int iters, double* ms)
 int jfg_smooth(jfg_mat* A, const jfg_smoother_desc* sm, const double* rhs, double* x)
 {
     if (!A || !sm || A->m->rows != A->m->cols || sm->runs < 0) return JFG_ERR_BAD_ARG;
-    if (sm->kind != JFG_SMOOTH_JACOBI && sm->kind != JFG_SMOOTH_RICHARDSON && sm->kind != JFG_SMOOTH_SCHWARZ)
+    if (sm->kind != JFG_SMOOTH_JACOBI && sm->kind != JFG_SMOOTH_RICHARDSON && sm->kind != JFG_SMOOTH_SCHWARZ &&
+        sm->kind != JFG_SMOOTH_FBGS && sm->kind != JFG_SMOOTH_GS)
         return JFG_ERR_BAD_ARG;
     if (sm->kind == JFG_SMOOTH_SCHWARZ && (!sm->schwarz || jfg::schwarz_of(sm->schwarz)->n != A->m->rows))
+        return JFG_ERR_BAD_ARG;
+    if ((sm->kind == JFG_SMOOTH_FBGS || sm->kind == JFG_SMOOTH_GS) &&
+        (!sm->gs || jfg::gs_of(sm->gs)->n != A->m->rows))
         return JFG_ERR_BAD_ARG;
     jfg_ctx* ctx = A->ctx;
     return guard(ctx, [&]() -> int {
@@ -422,6 +427,7 @@ int jfg_smooth(jfg_mat* A, const jfg_smoother_desc* sm, const double* rhs, doubl
         d.runs = sm->runs;
         d.omega = sm->omega;
         d.schwarz = jfg::schwarz_of(sm->schwarz);
+        d.gs = (sm->kind == JFG_SMOOTH_FBGS || sm->kind == JFG_SMOOTH_GS) ? jfg::gs_of(sm->gs) : nullptr;
         jfg::Scratch sc = ctx_scratch(ctx, A->m->nblocks);
         jfg::smooth_standalone(&ctx->c, A->m, d, ctx->stage_a.p, ctx->stage_b.p, sc);
         stage_out(ctx, ctx->stage_b.p, x, n);
@@ -457,7 +463,8 @@ int jfg_mg_create(jfg_ctx* ctx, int levels, jfg_mat* const* A, jfg_mat* const* P
                 jfg::SmootherDesc d;
                 if (l >= 1) {
                     JFG_CHECK(sm[l].kind == JFG_SMOOTH_JACOBI || sm[l].kind == JFG_SMOOTH_RICHARDSON ||
-                                  sm[l].kind == JFG_SMOOTH_SCHWARZ,
+                                  sm[l].kind == JFG_SMOOTH_SCHWARZ || sm[l].kind == JFG_SMOOTH_FBGS ||
+                                  sm[l].kind == JFG_SMOOTH_GS,
                               JFG_ERR_BAD_ARG, "unknown smoother kind");
                     JFG_CHECK(sm[l].runs >= 0, JFG_ERR_BAD_ARG, "negative smoother runs");
                     d.kind = sm[l].kind;
@@ -467,6 +474,11 @@ int jfg_mg_create(jfg_ctx* ctx, int levels, jfg_mat* const* A, jfg_mat* const* P
                         d.schwarz = jfg::schwarz_of(sm[l].schwarz);
                         JFG_CHECK(d.schwarz && d.schwarz->A == A[l]->m, JFG_ERR_BAD_ARG,
                                   "Schwarz smoother built on another matrix than its level");
+                    }
+                    if (d.kind == JFG_SMOOTH_FBGS || d.kind == JFG_SMOOTH_GS) {
+                        d.gs = jfg::gs_of(sm[l].gs);
+                        JFG_CHECK(d.gs && d.gs->n == A[l]->m->rows, JFG_ERR_BAD_ARG,
+                                  "Gauss-Seidel smoother of another size than its level");
                     }
                 }
                 g->sm.push_back(d);

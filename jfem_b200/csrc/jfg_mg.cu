@@ -4,6 +4,7 @@
 #include <algorithm>
 
 #include "jfg_mg.cuh"
+#include "jfg_gs.cuh"
 #include "jfg_schwarz.cuh"
 
 namespace cg = cooperative_groups;
@@ -567,6 +568,21 @@ void MGImpl<T>::smooth(int l, const T* rhs, bool xzero, const Scratch& sc, const
         // SchwarzSmoother.smooth (schwarz/SchwarzSmoother.java:21-43)
         if (xzero) vec_launch<0>(st, m, VZero<T>{x[l].p}, sc, done);
         d.schwarz->smooth<T>(d.runs, rhs, x[l].p, sc, done, st);
+    } else if (d.kind == JFG_SMOOTH_FBGS) {
+        // ForwardBackwardGaussSeidelSmoother.smooth: x += L^-1 D U^-1 (b - A x)
+        if (xzero) vec_launch<0>(st, m, VZero<T>{x[l].p}, sc, done);
+        for (int k = 0; k < d.runs; k++) {
+            mg_spmv<T, 0>(*this, st, M, x[l].p, EpiResid<T>{rhs, r[l].p}, sc, done);
+            d.gs->backward<T>(r[l].p, t[l].p, done, st);
+            d.gs->forward_fbgs<T>(t[l].p, r[l].p, x[l].p, done, st);
+        }
+    } else if (d.kind == JFG_SMOOTH_GS) {
+        // GaussSeidelSmoother.smooth: x = (L + D)^-1 (b - R x)
+        if (xzero) vec_launch<0>(st, m, VZero<T>{x[l].p}, sc, done);
+        for (int k = 0; k < d.runs; k++) {
+            d.gs->strict_upper<T>(rhs, x[l].p, t[l].p, done, st);
+            d.gs->forward<T>(t[l].p, x[l].p, done, st);
+        }
     } else {
         if (xzero) vec_launch<0>(st, m, VZero<T>{x[l].p}, sc, done);
         for (int k = 0; k < d.runs; k++) {
@@ -739,6 +755,20 @@ void smooth_standalone(Context* c, Matrix* A, const SmootherDesc& d, const doubl
     t.alloc(m);
     r.alloc(m);
     flag.alloc(1);
+    if (d.kind == JFG_SMOOTH_FBGS || d.kind == JFG_SMOOTH_GS) {
+        for (int k = 0; k < d.runs; k++) {
+            if (d.kind == JFG_SMOOTH_FBGS) {
+                spmv_launch<double, double, 0>(st, A, A->val.p, xv, EpiResid<double>{rhs, r.p}, sc, nullptr);
+                d.gs->backward<double>(r.p, t.p, nullptr, st);
+                d.gs->forward_fbgs<double>(t.p, r.p, xv, nullptr, st);
+            } else {
+                d.gs->strict_upper<double>(rhs, xv, t.p, nullptr, st);
+                d.gs->forward<double>(t.p, xv, nullptr, st);
+            }
+        }
+        JFG_CUDA(cudaStreamSynchronize(st));
+        return;
+    }
     if (m) k_dinv<double><<<nb(m), 256, 0, st>>>(m, A->diag.p, dinv.p);
     JFG_CUDA(cudaGetLastError());
     if (d.kind == JFG_SMOOTH_JACOBI) {

@@ -7,12 +7,14 @@
 namespace jfg {
 
 struct SchwarzImpl;
+struct GSImpl;
 
 struct SmootherDesc {
     int kind = JFG_SMOOTH_JACOBI;
     int runs = 2;
     double omega = 2.0 / 3.0;
     SchwarzImpl* schwarz = nullptr;   // JFG_SMOOTH_SCHWARZ
+    GSImpl* gs = nullptr;             // JFG_SMOOTH_FBGS / JFG_SMOOTH_GS
 };
 
 // The hierarchy of MGPreconditionerSpace / MGPreconditionerInterface

@@ -19,7 +19,7 @@ _SRC = os.path.join(_HERE, "jfem_oracle.c")
 _LIB = os.path.join(_HERE, "libjfem_oracle.so")
 
 OK, MAXITER, BREAKDOWN, NONFINITE, BADARG, SINGULAR = range(6)
-SMOOTH_JACOBI, SMOOTH_RICHARDSON = 0, 1
+SMOOTH_JACOBI, SMOOTH_RICHARDSON, SMOOTH_FBGS, SMOOTH_GS = 0, 1, 3, 4
 
 
 def build(force: bool = False) -> str:
@@ -66,6 +66,7 @@ def lib():
         L.or_mat_coo.argtypes = [_P, _I, _I, _D]
         L.or_mat_mmmul.restype = _P
         L.or_mat_mmmul.argtypes = [_P, _P]
+        L.or_gs_smooth.argtypes = [_P, C.c_int, C.c_int, _I, _D, _D]
         L.or_set_threads.argtypes = [C.c_int]
         L.or_threads.restype = C.c_int
         L.or_mat_diag.argtypes = [_P, _D]
@@ -324,6 +325,17 @@ def solve_gmres2(A, b, tol, M=None, x0=None, maxit=0, max_restarts=200):
     b = _f64(b)
     x0 = start_iterate(len(b)) if x0 is None else x0
     return _run(lib().or_solve_gmres2, A._op, _op(M), _d(b), (C.c_double(tol), maxit, max_restarts), x0=x0)
+
+
+def gs_smooth(A: CooMatrix, kind, runs, rhs, x, rank=None):
+    """ForwardBackwardGaussSeidelSmoother (kind SMOOTH_FBGS) / GaussSeidelSmoother
+    (SMOOTH_GS) in the ordering `rank` (natural when None)."""
+    x = _f64(x).copy()
+    rk = None if rank is None else _i32(rank)
+    st = lib().or_gs_smooth(A._h, kind, runs, _i(rk) if rk is not None else None, _d(_f64(rhs)), _d(x))
+    if st == SINGULAR:
+        raise np.linalg.LinAlgError("Singular Matrix")
+    return x
 
 
 def smooth(A: CooMatrix, kind, runs, omega, rhs, x):

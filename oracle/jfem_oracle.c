@@ -1106,13 +1106,89 @@ const double* or_schwarz_inverse(const or_schwarz* S, int p, int* m)
 #define OR_SMOOTH_RICHARDSON 1
 
 #define OR_SMOOTH_SCHWARZ 2
+#define OR_SMOOTH_FBGS 3
+#define OR_SMOOTH_GS 4
 
 typedef struct {
     int kind, runs;
     double omega;
     double* dinv;      /* Jacobi: 1/diag with |d| < 1e-10 -> 1 (JacobiSmoother.java:16-24) */
     const or_schwarz* schwarz;   /* SchwarzSmoother: its own decomposition and global operator */
+    const int* rank;   /* Gauss-Seidel: position of each row in the ordering (NULL: natural) */
 } or_smoother;
+
+/* Triangular solve of the lower (lower != 0) or upper triangle of A with the
+ * diagonal, rows visited in rank order (upper: reverse), each row as
+ * LowerTriangularSparseMatrix.backsubstituteRow / UpperTriangularSparseMatrix.
+ * forwardsubstituteRow do (LowerTriangularSparseMatrix.java:188-212,
+ * UpperTriangularSparseMatrix.java:197-221): sol_i = rhs_i / d, then
+ * sol_i += (-sol_j / d) * a_ij over the row's other triangle entries, here in
+ * ascending column order (the reference: HashMap order of its row bucket).
+ * scale != 0 uses d_i * rhs_i as the right-hand side (D.mvMul first). */
+static void gs_trsv(const or_mat* A, int lower, const int* rank, const int* order, const double* diag,
+                    const double* rhs, int scale, double* sol)
+{
+    int n = A->rows;
+    for (int p = 0; p < n; p++) {
+        int i = order[lower ? p : n - 1 - p];
+        double d = diag[i];
+        double r = scale ? d * rhs[i] : rhs[i];
+        double s = r / d;
+        for (long long q = A->rp[i]; q < A->rp[i + 1]; q++) {
+            int j = A->rc[q];
+            if (j == i) continue;
+            int in = lower ? rank[j] < rank[i] : rank[j] > rank[i];
+            if (!in) continue;
+            double t = -sol[j] / d;
+            s = s + t * A->rv[q];
+        }
+        sol[i] = s;
+    }
+}
+
+/* ForwardBackwardGaussSeidelSmoother.smooth (ForwardBackwardGaussSeidelSmoother.java:23-44):
+ * runs x { x += L^-1 D U^-1 (b - A x) };  GaussSeidelSmoother.smooth
+ * (GaussSeidelSmoother.java:24-32): runs x { x = (L + D)^-1 (b - R x) }, the
+ * dense inverse of L + D restated as a forward substitution.  rank == NULL:
+ * the natural row order.  Returns OR_SINGULAR for a zero diagonal entry. */
+int or_gs_smooth(const or_mat* A, int kind, int runs, const int* rank_in, const double* rhs, double* x)
+{
+    int n = A->rows;
+    if (A->rows != A->cols) return OR_BADARG;
+    int* rank = (int*)malloc(sizeof(int) * (n ? n : 1));
+    int* order = (int*)malloc(sizeof(int) * (n ? n : 1));
+    double* diag = vnew(n);
+    for (int i = 0; i < n; i++) rank[i] = rank_in ? rank_in[i] : i;
+    for (int i = 0; i < n; i++) order[rank[i]] = i;
+    or_mat_diag(A, diag);
+    int st = OR_OK;
+    for (int i = 0; i < n; i++)
+        if (diag[i] == 0.0) st = OR_SINGULAR;
+    double* r = vnew(n);
+    double* y = vnew(n);
+    double* w = vnew(n);
+    for (int it = 0; st == OR_OK && it < runs; it++) {
+        if (kind == OR_SMOOTH_FBGS) {
+            or_mat_mvmul(A, x, r);
+            for (int i = 0; i < n; i++) r[i] = rhs[i] - r[i];
+            gs_trsv(A, 0, rank, order, diag, r, 0, y);
+            gs_trsv(A, 1, rank, order, diag, y, 1, w);
+            for (int i = 0; i < n; i++) x[i] = x[i] + w[i];
+        } else {
+            for (int i = 0; i < n; i++) {
+                double s = 0;
+                for (long long q = A->rp[i]; q < A->rp[i + 1]; q++) {
+                    int j = A->rc[q];
+                    if (j != i && rank[j] > rank[i]) s = s + A->rv[q] * x[j];
+                }
+                r[i] = rhs[i] - s;
+            }
+            gs_trsv(A, 1, rank, order, diag, r, 0, x);
+        }
+    }
+    free(rank); free(order); free(diag); free(r); free(y); free(w);
+    return st;
+}
 
 /* JacobiSmoother.smooth (JacobiSmoother.java:28-50) and RichardsonSmoother.smooth
  * (RichardsonSmoother.java:31-50, unpreconditioned form).  x is updated in place. */
@@ -1121,6 +1197,10 @@ static void smooth(const or_smoother* s, const or_mat* A, const double* rhs, dou
     int n = A->rows;
     if (s->kind == OR_SMOOTH_SCHWARZ) {
         or_schwarz_smooth(s->schwarz, s->runs, rhs, x);
+        return;
+    }
+    if (s->kind == OR_SMOOTH_FBGS || s->kind == OR_SMOOTH_GS) {
+        or_gs_smooth(A, s->kind, s->runs, s->rank, rhs, x);
         return;
     }
     for (int it = 0; it < s->runs; it++) {
@@ -1137,7 +1217,7 @@ static void smooth(const or_smoother* s, const or_mat* A, const double* rhs, dou
 
 static void smoother_init(or_smoother* s, int kind, int runs, double omega, const or_mat* A)
 {
-    s->kind = kind; s->runs = runs; s->omega = omega; s->dinv = NULL; s->schwarz = NULL;
+    s->kind = kind; s->runs = runs; s->omega = omega; s->dinv = NULL; s->schwarz = NULL; s->rank = NULL;
     if (kind == OR_SMOOTH_JACOBI) {
         s->dinv = vnew(A->rows);
         or_mat_diag(A, s->dinv);

@@ -148,3 +148,26 @@ def test_oracle_mmmul_tmmul_dense():
         c = np.where(rng.random((m, n)) < 0.2, rng.standard_normal((m, n)), 0.0)
         Cm = O.CooMatrix(m, n, *np.nonzero(c), c[np.nonzero(c)])
         np.testing.assert_allclose(A.tmmul(Cm).dense(), a.T @ c, rtol=1e-14, atol=1e-14)
+
+
+def test_oracle_gauss_seidel_dense():
+    """ForwardBackwardGaussSeidelSmoother / GaussSeidelSmoother restatements
+    against dense triangular algebra, natural and permuted orderings."""
+    rng = np.random.default_rng(5)
+    n = 12
+    a = rng.standard_normal((n, n))
+    a = a + a.T + 12 * np.eye(n)
+    a[np.abs(a) < 0.6] = 0.0
+    A = O.CooMatrix(n, n, *np.nonzero(a), a[np.nonzero(a)])
+    b, x0 = rng.standard_normal(n), rng.standard_normal(n)
+    for rank in (None, rng.permutation(n).astype(np.int32)):
+        p = np.arange(n) if rank is None else np.argsort(rank)      # p[k] = row at position k
+        ap = a[np.ix_(p, p)]
+        L, U, D = np.tril(ap), np.triu(ap), np.diag(np.diag(ap))
+        bp, xp = b[p], x0[p]
+        ref = xp + np.linalg.solve(L, D @ np.linalg.solve(U, bp - ap @ xp))
+        got = O.gs_smooth(A, O.SMOOTH_FBGS, 1, b, x0, rank)
+        np.testing.assert_allclose(got[p], ref, rtol=1e-13, atol=1e-13)
+        ref = np.linalg.solve(L, bp - np.triu(ap, 1) @ xp)
+        got = O.gs_smooth(A, O.SMOOTH_GS, 1, b, x0, rank)
+        np.testing.assert_allclose(got[p], ref, rtol=1e-13, atol=1e-13)
