@@ -50,9 +50,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cells", type=int, default=CELLS)
     ap.add_argument("--levels", type=int, default=LEVELS)
-    ap.add_argument("--workload", default="gmg-pcg", choices=["gmg-pcg", "cg-small", "batch-heat", "stokes", "learned", "galerkin"])
+    ap.add_argument("--workload", default="gmg-pcg", choices=["gmg-pcg", "cg-small", "batch-heat", "stokes", "learned", "galerkin", "gs-pcg"])
     ap.add_argument("--profile", default=None,
-                    choices=["solve-fp64", "solve-mixed", "solve-mixed-nograph", "spmv64", "spmv32"],
+                    choices=["solve-fp64", "solve-mixed", "solve-mixed-nograph", "gs-mixed-nograph", "spmv64", "spmv32"],
                     help="set up, run the named operation --warmup + 1 times and exit (for ncu captures)")
     return ap.parse_args()
 
@@ -195,9 +195,12 @@ def run_ours(args):
     h = build_problem(args.cells, args.levels)
     mats = [DeviceMatrix(s.n, s.n, s.rows, s.cols, s.vals, ctx) for s in h.systems]
     prol = [DeviceMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l], ctx) for l in range(args.levels - 1)]
-    sm = JacobiSmoother(2, 2.0 / 3.0)
-    mg = MGPreconditioner(mats, prol, h.boundary, [None] + [sm] * (args.levels - 1), cycles=1, use_fmg=False,
-                          precision="mixed", ctx=ctx)
+    if args.profile == "gs-mixed-nograph":      # forward-backward Gauss-Seidel (1 run), multicolour
+        from jfem_b200 import ForwardBackwardGaussSeidelSmoother
+        sms = [None] + [ForwardBackwardGaussSeidelSmoother(1, mats[l], "multicolour") for l in range(1, args.levels)]
+    else:
+        sms = [None] + [JacobiSmoother(2, 2.0 / 3.0)] * (args.levels - 1)
+    mg = MGPreconditioner(mats, prol, h.boundary, sms, cycles=1, use_fmg=False, precision="mixed", ctx=ctx)
     A = mats[-1]
     n = A.rows
     b_host = h.finest.rhs.copy()
@@ -226,7 +229,7 @@ def run_ours(args):
         with torch.cuda.stream(stream):
             dx.copy_(e0)           # the reference's start vector e0
         o = opts(precision)
-        if args.profile == "solve-mixed-nograph":
+        if args.profile in ("solve-mixed-nograph", "gs-mixed-nograph"):
             o.use_graph = 0        # plain launches: every kernel of the solve is visible to a profiler
         st = N.load().jfg_solve_dev(ctx.handle, N.PCG, A.handle, N.PREC_MG, mg.handle, C.c_void_p(db.data_ptr()),
                                     C.c_void_p(dx.data_ptr()), C.byref(o), C.byref(info))
@@ -263,7 +266,7 @@ def run_ours(args):
         for _ in range(args.warmup + 1):
             if args.profile == "solve-fp64":
                 solve_dev(N.FP64)
-            elif args.profile in ("solve-mixed", "solve-mixed-nograph"):
+            elif args.profile in ("solve-mixed", "solve-mixed-nograph", "gs-mixed-nograph"):
                 solve_dev(HEADLINE)
             else:
                 A.time_spmv(precision=1 if args.profile == "spmv32" else 0, iters=1)
@@ -570,6 +573,58 @@ def run_galerkin(args):
     print(json.dumps(line))
 
 
+def run_gs_pcg(args):
+    """The GMG-PCG solve of the Q2 512x512 system with forward-backward
+    Gauss-Seidel smoothing (1 run pre and post) in the multicolour and the
+    natural ordering, against Jacobi 2 + 2; FP64 and mixed (FP32 V-cycle)."""
+    import torch
+    from jfem_b200 import _native as N
+    from jfem_b200.linalg import DeviceMatrix, IterativeSolver
+    from jfem_b200.multigrid import ForwardBackwardGaussSeidelSmoother, JacobiSmoother, MGPreconditioner
+    ctx = N.default_context()
+    h = build_problem(args.cells, args.levels)
+    L = len(h.systems)
+    mats = [DeviceMatrix(s.n, s.n, s.rows, s.cols, s.vals, ctx) for s in h.systems]
+    prol = [DeviceMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l], ctx) for l in range(L - 1)]
+    b = torch.tensor(h.finest.rhs, device="cuda")
+    tol = RTOL * float(np.linalg.norm(h.finest.rhs))
+    out = {}
+    variants = [("jacobi_2_2", lambda A: JacobiSmoother(2, 2 / 3)),
+                ("fbgs_1_multicolour", lambda A: ForwardBackwardGaussSeidelSmoother(1, A, "multicolour")),
+                ("fbgs_1_natural", lambda A: ForwardBackwardGaussSeidelSmoother(1, A, "natural"))]
+    for name, make in variants:
+        t0 = time.perf_counter()
+        sms = [None] + [make(mats[l]) for l in range(1, L)]
+        setup = time.perf_counter() - t0
+        mg = MGPreconditioner(mats, prol, h.boundary, sms, cycles=1, use_fmg=False, precision="mixed", ctx=ctx)
+        info = sms[-1].info() if hasattr(sms[-1], "info") else None
+        for prec in ("fp64", "mixed-precond"):
+            s = IterativeSolver(ctx=ctx)
+            s.precision = prec
+            best = None
+            for _ in range(max(1, args.warmup) + max(1, args.steps // 3)):
+                x = torch.zeros_like(b)
+                x[0] = 1.0
+                torch.cuda.synchronize()
+                t1 = time.perf_counter()
+                s.solve_device(N.PCG, mats[-1], mg, b, x, tol)
+                torch.cuda.synchronize()
+                dt = time.perf_counter() - t1
+                best = dt if best is None else min(best, dt)
+            r = float(torch.linalg.vector_norm(b - mats[-1].spmv_dev(x)).item())
+            out[f"{name}/{prec}"] = {"time_s": best, "iterations": s.iterations, "status": N.STATUS_NAMES[s.last.status],
+                                     "true_rel_residual": r / float(torch.linalg.vector_norm(b).item()),
+                                     "smoother_setup_s": setup, "finest_levels_fwd_bwd_colours": info}
+    line = {"metric": "time-to-1e-8 residual (s), GMG-PCG with Gauss-Seidel smoothing",
+            "value": out["fbgs_1_multicolour/mixed-precond"]["time_s"], "unit": "s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic (seeded sine-mode source, assembled Q2 system)",
+            "config": {"workload": f"gs-pcg: Q2 {args.cells}x{args.cells}, {L} levels, FBGS(1) vs Jacobi 2+2",
+                       "dofs": int(h.finest.n)},
+            "variants": out}
+    print(json.dumps(line))
+
+
 def problems_hierarchy(p, cells, levels, modes):
     from jfem_b200 import problems
     return problems.hierarchy(p, cells >> (levels - 1), levels, mass=5.0, modes=modes, seed=SEED)
@@ -761,6 +816,8 @@ def main():
             print(json.dumps({"impl": "reference", "unavailable": "the reference arm covers the gmg-pcg workload"}))
             return
         run_reference(args)
+    elif args.workload == "gs-pcg":
+        run_gs_pcg(args)
     elif args.workload == "galerkin":
         run_galerkin(args)
     elif args.workload == "cg-small":

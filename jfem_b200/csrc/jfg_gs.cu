@@ -14,11 +14,14 @@
 // :188-212), sol_i = rhs_i / d_i and then sol_i += (-sol_j / d_i) * a_ij for
 // its off-diagonal entries j in ascending column order, each operation
 // rounded on its own (no fused multiply-add).  Runs of small levels go to one
-// CTA that steps through them with a barrier between levels; a large level
-// is one grid launch.  The natural ordering reproduces the reference's
+// CTA (levels of at most 512 rows) or one 8-CTA cluster (at most 4,096) that
+// steps through them with a barrier between levels; a large level is one
+// grid launch.  The natural ordering reproduces the reference's
 // sequential algorithm (as many steps as the longest dependency chain); the
 // multicolour ordering (greedy colouring of the graph of A + A^T) is the same
 // algorithm on the symmetrically permuted system and has one step per colour.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <numeric>
 
@@ -30,8 +33,9 @@ namespace {
 
 inline unsigned nb(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
 
-constexpr int kCtaThreads = 1024;
-constexpr int kCtaMaxRows = 4096;     // levels up to this size run inside the single-CTA kernel
+constexpr int kCtaThreads = 512;
+constexpr int kClusterCtas = 8;
+constexpr int kCtaMaxRows = kCtaThreads * kClusterCtas;   // levels up to this size run inside the cluster kernel
 
 __device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
 __device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
@@ -41,8 +45,11 @@ __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
 
 // one row of a triangular solve; slot q of a level with cnt rows, its ELL
-// entries at col/val + k * cnt + q
-template <typename T, bool SCALE, bool ADDX>
+// entries at col/val + k * cnt + q.  Entries are taken in chunks of kChunk:
+// the chunk's column, value and solution loads are all issued before its
+// arithmetic, so a row costs one memory round trip per chunk rather than
+// one per entry; the arithmetic keeps the entry order.
+template <typename T, bool SCALE, bool ADDX, int kChunk>
 __device__ __forceinline__ void trsv_row(int q, int cnt, int width, const int* __restrict__ rows,
                                          const int* __restrict__ col, const T* __restrict__ val,
                                          const T* __restrict__ diag, const T* __restrict__ rhs, T* sol, T* x)
@@ -52,10 +59,20 @@ __device__ __forceinline__ void trsv_row(int q, int cnt, int width, const int* _
     T r = rhs[i];
     if (SCALE) r = mul_rn(d, r);     // D.mvMul(y)
     T s = div_rn(r, d);
-    for (int k = 0; k < width; k++) {
-        const int j = col[(int64_t)k * cnt + q];
-        if (j < 0) break;
-        s = add_rn(s, mul_rn(div_rn(-sol[j], d), val[(int64_t)k * cnt + q]));
+    for (int k0 = 0; k0 < width; k0 += kChunk) {
+        int js[kChunk];
+        T vs[kChunk], xs[kChunk];
+#pragma unroll
+        for (int u = 0; u < kChunk; u++) js[u] = k0 + u < width ? col[(int64_t)(k0 + u) * cnt + q] : -1;
+#pragma unroll
+        for (int u = 0; u < kChunk; u++) {
+            vs[u] = js[u] >= 0 ? val[(int64_t)(k0 + u) * cnt + q] : (T)0;
+            xs[u] = js[u] >= 0 ? sol[js[u]] : (T)0;
+        }
+#pragma unroll
+        for (int u = 0; u < kChunk; u++)
+            if (js[u] >= 0) s = add_rn(s, mul_rn(div_rn(-xs[u], d), vs[u]));
+        if (js[kChunk - 1] < 0) break;
     }
     sol[i] = s;
     if (ADDX) x[i] = add_rn(x[i], s);
@@ -70,11 +87,113 @@ __global__ void k_trsv_level(int cnt, int width, const int* __restrict__ rows, c
     if (done && *done) return;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= cnt) return;
-    trsv_row<T, SCALE, ADDX>(q, cnt, width, rows, col, val, diag, rhs, sol, x);
+    trsv_row<T, SCALE, ADDX, 8>(q, cnt, width, rows, col, val, diag, rhs, sol, x);
 }
 
-// levels [l0, l1) in one CTA; __syncthreads makes a level's solution entries
-// visible to the next level's threads
+// Levels [l0, l1) in one CTA or one cluster of kClusterCtas CTAs, one row per
+// thread (every level of the run fits the threads).  A thread loads the next
+// level's row data (row, diagonal, right-hand side, the first 8 entries)
+// before the barrier that ends the current level, so a level costs one round
+// trip for the solution entries it reads.  In a cluster the barrier
+// (release / acquire at cluster scope) orders the level's solution stores
+// before the next level's loads, which read through L2 (ld.global.cg) so that
+// no CTA sees a line its own L1 cached before another CTA wrote it.
+template <typename T>
+struct RowPre {
+    int i = -1;          // row, -1 when this thread has none in the level
+    int cnt = 0, w = 0, q = 0;
+    int64_t b = 0;
+    T d = 0, r = 0;
+    int js[8];
+    T vs[8];
+};
+
+template <typename T, bool SCALE>
+__device__ __forceinline__ void row_prefetch(RowPre<T>& p, int l, int tid, const int* __restrict__ lstart,
+                                             const int* __restrict__ lwidth, const int64_t* __restrict__ lbase,
+                                             const int* __restrict__ rows, const int* __restrict__ col,
+                                             const T* __restrict__ val, const T* __restrict__ diag,
+                                             const T* __restrict__ rhs)
+{
+    const int s0 = lstart[l];
+    p.cnt = lstart[l + 1] - s0;
+    p.w = lwidth[l];
+    p.b = lbase[l];
+    p.q = tid;
+    p.i = tid < p.cnt ? rows[s0 + tid] : -1;
+    if (p.i < 0) return;
+    p.d = diag[p.i];
+    p.r = rhs[p.i];
+    if (SCALE) p.r = mul_rn(p.d, p.r);
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+        p.js[u] = u < p.w ? col[p.b + (int64_t)u * p.cnt + tid] : -1;
+        p.vs[u] = p.js[u] >= 0 ? val[p.b + (int64_t)u * p.cnt + tid] : (T)0;
+    }
+}
+
+// the loop of the level-run kernels; CL = 1: one CTA, __syncthreads between
+// levels (same SM: block-scope visibility); CL = kClusterCtas: a cluster
+// barrier between levels and solution loads through L2
+template <typename T, bool SCALE, bool ADDX, int CL>
+__device__ __forceinline__ void level_run(int l0, int l1, int tid, const int* __restrict__ lstart,
+                                          const int* __restrict__ lwidth, const int64_t* __restrict__ lbase,
+                                          const int* __restrict__ rows, const int* __restrict__ col,
+                                          const T* __restrict__ val, const T* __restrict__ diag,
+                                          const T* __restrict__ rhs, T* sol, T* x)
+{
+    auto ld = [&](int j) -> T { return CL > 1 ? __ldcg(sol + j) : sol[j]; };
+    RowPre<T> p;
+    row_prefetch<T, SCALE>(p, l0, tid, lstart, lwidth, lbase, rows, col, val, diag, rhs);
+    for (int l = l0; l < l1; l++) {
+        if (p.i >= 0) {
+            T xs[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) xs[u] = p.js[u] >= 0 ? ld(p.js[u]) : (T)0;
+            T s = div_rn(p.r, p.d);
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+                if (p.js[u] >= 0) s = add_rn(s, mul_rn(div_rn(-xs[u], p.d), p.vs[u]));
+            for (int k0 = 8; k0 < p.w && p.js[7] >= 0; k0 += 8) {   // rows longer than the prefetched chunk
+                int js[8];
+                T vs[8], ys[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) js[u] = k0 + u < p.w ? col[p.b + (int64_t)(k0 + u) * p.cnt + p.q] : -1;
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    vs[u] = js[u] >= 0 ? val[p.b + (int64_t)(k0 + u) * p.cnt + p.q] : (T)0;
+                    ys[u] = js[u] >= 0 ? ld(js[u]) : (T)0;
+                }
+#pragma unroll
+                for (int u = 0; u < 8; u++)
+                    if (js[u] >= 0) s = add_rn(s, mul_rn(div_rn(-ys[u], p.d), vs[u]));
+                if (js[7] < 0) break;
+            }
+            sol[p.i] = s;
+            if (ADDX) x[p.i] = add_rn(x[p.i], s);
+        }
+        if (l + 1 < l1) row_prefetch<T, SCALE>(p, l + 1, tid, lstart, lwidth, lbase, rows, col, val, diag, rhs);
+        if (CL > 1) {
+            cooperative_groups::this_cluster().sync();
+        } else {
+            __syncthreads();
+        }
+    }
+}
+
+template <typename T, bool SCALE, bool ADDX>
+__global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kCtaThreads, 1)
+    k_trsv_levels_cluster(int l0, int l1, const int* __restrict__ lstart, const int* __restrict__ lwidth,
+                          const int64_t* __restrict__ lbase, const int* __restrict__ rows,
+                          const int* __restrict__ col, const T* __restrict__ val, const T* __restrict__ diag,
+                          const T* __restrict__ rhs, T* sol, T* x, const int* __restrict__ done)
+{
+    pdl_wait();
+    if (done && *done) return;      // uniform over the cluster: no barrier is left waiting
+    const int tid = (int)cooperative_groups::this_cluster().block_rank() * blockDim.x + threadIdx.x;
+    level_run<T, SCALE, ADDX, kClusterCtas>(l0, l1, tid, lstart, lwidth, lbase, rows, col, val, diag, rhs, sol, x);
+}
+
 template <typename T, bool SCALE, bool ADDX>
 __global__ void __launch_bounds__(kCtaThreads, 1)
     k_trsv_levels_cta(int l0, int l1, const int* __restrict__ lstart, const int* __restrict__ lwidth,
@@ -84,13 +203,7 @@ __global__ void __launch_bounds__(kCtaThreads, 1)
 {
     pdl_wait();
     if (done && *done) return;
-    for (int l = l0; l < l1; l++) {
-        const int s0 = lstart[l], cnt = lstart[l + 1] - s0, w = lwidth[l];
-        const int64_t b = lbase[l];
-        for (int q = threadIdx.x; q < cnt; q += blockDim.x)
-            trsv_row<T, SCALE, ADDX>(q, cnt, w, rows + s0, col + b, val + b, diag, rhs, sol, x);
-        __syncthreads();
-    }
+    level_run<T, SCALE, ADDX, 1>(l0, l1, threadIdx.x, lstart, lwidth, lbase, rows, col, val, diag, rhs, sol, x);
 }
 
 // t = b - R x over the strict upper triangle (CSR in row order, ascending columns)
@@ -186,10 +299,14 @@ static void build_tri(GSImpl::Tri& tri, int n, bool is_lower, const std::vector<
             sg.l1 = l + 1;
             sg.cta = false;
         } else {
-            int e = l + 1;
-            while (e < nl && tri.start[e + 1] - tri.start[e] <= kCtaMaxRows) e++;
+            int e = l + 1, mx = tri.start[l + 1] - tri.start[l];
+            while (e < nl && tri.start[e + 1] - tri.start[e] <= kCtaMaxRows) {
+                mx = std::max(mx, tri.start[e + 1] - tri.start[e]);
+                e++;
+            }
             sg.l1 = e;
             sg.cta = true;
+            sg.cluster = mx > kCtaThreads;
         }
         tri.segs.push_back(sg);
         l = sg.l1;
@@ -360,7 +477,8 @@ void GSImpl::solve(Tri& tri, const T* rhs, T* sol, T* x, const int* done, cudaSt
     const T* d = dvals<T>();
     for (const auto& sg : tri.segs) {
         if (sg.cta) {
-            launch_ex(k_trsv_levels_cta<T, SCALE, ADDX>, dim3(1), dim3(kCtaThreads), 0, st, sg.l0, sg.l1,
+            launch_ex(sg.cluster ? k_trsv_levels_cluster<T, SCALE, ADDX> : k_trsv_levels_cta<T, SCALE, ADDX>,
+                      dim3(sg.cluster ? kClusterCtas : 1), dim3(kCtaThreads), 0, st, sg.l0, sg.l1,
                       (const int*)tri.d_start.p, (const int*)tri.d_width.p, (const int64_t*)tri.d_base.p,
                       (const int*)tri.rows.p, (const int*)tri.col.p, v, d, rhs, sol, x, done);
         } else {

@@ -25,10 +25,11 @@ struct GSImpl {
         DevBuf<double> val;
         DevBuf<float> val32;                // FP32 copy for FP32 hierarchies (built on first use)
         // consecutive levels run by one launch: a run of small levels in one
-        // CTA (a barrier between levels), or one large level on a grid
+        // cluster (a cluster barrier between levels), or one large level on a grid
         struct Seg {
             int l0 = 0, l1 = 0;
             bool cta = false;
+            bool cluster = false;           // run of levels larger than one CTA's threads
         };
         std::vector<Seg> segs;
     };
