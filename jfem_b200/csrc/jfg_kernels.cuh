@@ -169,22 +169,29 @@ k_spmv(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi
         const int st = 32 * tpr;
         int k = sub;
         if constexpr (IDX16) {
-            // columns stored as 16-bit offsets from the row: 2 bytes less per entry
+            // columns stored as 16-bit offsets from the row: 2 bytes less per
+            // entry.  Chunks of U entries: all column and value loads of a
+            // chunk, then all its x gathers, then the sums in entry order
+            // (entries past the slice length are predicated off), so a
+            // thread has U entries of the matrix stream in flight.
+            constexpr int U = TPR == 1 ? 8 : 4;
             const int base = r < 0 ? 0 : r;
             const int16_t* cp = m.col16 + o + lane;
-            for (; k + 3 * tpr < len; k += 4 * tpr) {
-                const int c0 = base + __ldg(cp + 32 * k), c1 = base + __ldg(cp + 32 * k + st);
-                const int c2 = base + __ldg(cp + 32 * k + 2 * st), c3 = base + __ldg(cp + 32 * k + 3 * st);
-                const AT v0 = to_acc(__ldg(vp + 32 * k)), v1 = to_acc(__ldg(vp + 32 * k + st));
-                const AT v2 = to_acc(__ldg(vp + 32 * k + 2 * st)), v3 = to_acc(__ldg(vp + 32 * k + 3 * st));
-                const AT x0 = (AT)__ldg(x + c0), x1 = (AT)__ldg(x + c1), x2 = (AT)__ldg(x + c2),
-                         x3 = (AT)__ldg(x + c3);
-                sum += v0 * x0;
-                sum += v1 * x1;
-                sum += v2 * x2;
-                sum += v3 * x3;
+            for (; k < len; k += U * tpr) {
+                int c[U];
+                AT v[U], xv[U];
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const bool ok = k + u * tpr < len;
+                    c[u] = ok ? base + __ldg(cp + 32 * k + u * st) : base;
+                    v[u] = ok ? to_acc(__ldg(vp + 32 * k + u * st)) : (AT)0;
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++) xv[u] = k + u * tpr < len ? (AT)__ldg(x + c[u]) : (AT)0;
+#pragma unroll
+                for (int u = 0; u < U; u++)
+                    if (k + u * tpr < len) sum += v[u] * xv[u];
             }
-            for (; k < len; k += tpr) sum += to_acc(__ldg(vp + 32 * k)) * (AT)__ldg(x + base + __ldg(cp + 32 * k));
         } else {
             const int* cp = m.col + o + lane;
             for (; k + 3 * tpr < len; k += 4 * tpr) {
