@@ -50,7 +50,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cells", type=int, default=CELLS)
     ap.add_argument("--levels", type=int, default=LEVELS)
-    ap.add_argument("--workload", default="gmg-pcg", choices=["gmg-pcg", "cg-small", "batch-heat", "stokes", "learned", "galerkin", "gs-pcg"])
+    ap.add_argument("--workload", default="gmg-pcg", choices=["gmg-pcg", "cg-small", "batch-heat", "stokes", "learned", "galerkin", "gs-pcg",
+                                                        "assemble"])
     ap.add_argument("--profile", default=None,
                     choices=["solve-fp64", "solve-mixed", "solve-mixed-nograph", "gs-mixed-nograph", "spmv64", "spmv32"],
                     help="set up, run the named operation --warmup + 1 times and exit (for ncu captures)")
@@ -625,6 +626,57 @@ def run_gs_pcg(args):
     print(json.dumps(line))
 
 
+def run_assemble(args):
+    """Assembly of the Q2 512x512 system (GRAD_GRAD + 5 VALUE_VALUE, 16 x 16
+    sine-mode source, zero Dirichlet data) on the GPU (jfg_assemble_tp: host
+    source values at the Gauss points in, device matrix and host rhs out)
+    against the host numpy assembler of the same system."""
+    import ctypes as C
+    import torch
+    from jfem_b200 import _native as N
+    from jfem_b200.assembly import Space, assemble
+    from jfem_b200.problems import modes_source
+    ctx = N.default_context()
+    sp = Space(P, args.cells, args.cells)
+    f, _ = modes_source(MODES, SEED)
+    X, Y = sp.quadrature_points()
+    fq = np.ascontiguousarray(f(X, Y))
+    d = N.TPDesc(P, args.cells, args.cells, 0.0, 1.0, 0.0, 1.0, 1.0, 5.0, 1)
+    n = sp.nx * sp.ny
+    rhs = np.empty(n)
+
+    def once():
+        h = C.c_void_p()
+        ctx.check(N.load().jfg_assemble_tp(ctx.handle, C.byref(d), None, N.dptr(fq), C.byref(h), N.dptr(rhs),
+                                           None, None))
+        N.load().jfg_matrix_free(h)
+
+    for _ in range(max(1, args.warmup)):
+        once()
+    ts = []
+    for _ in range(max(1, args.steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        once()
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t0)
+    cpu = None
+    if os.environ.get("JFEM_BENCH_NO_CPU") != "1":
+        t0 = time.perf_counter()
+        assemble(sp, 1.0, 5.0, source=lambda X, Y: fq)
+        cpu = {"value": time.perf_counter() - t0, "unit": "s", "cores": 1, "kind": "port",
+               "sample": "the whole host numpy assembly of the same system, the same source values at the Gauss "
+                         "points given"}
+    line = {"metric": "time to assemble the system (s)", "value": statistics.median(ts), "unit": "s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (16 x 16 seeded sine modes)",
+            "config": {"workload": f"assemble: Q{P} {args.cells}x{args.cells}, GRAD_GRAD + 5 VALUE_VALUE",
+                       "dofs": n, "cell_triples": args.cells * args.cells * (P + 1) ** 4},
+            "note": "GPU time: source values at the Gauss points already on the host (52 MB copied in), the "
+                    "matrix merged on the device, the rhs copied out", "cpu_baseline": cpu}
+    print(json.dumps(line))
+
+
 def problems_hierarchy(p, cells, levels, modes):
     from jfem_b200 import problems
     return problems.hierarchy(p, cells >> (levels - 1), levels, mass=5.0, modes=modes, seed=SEED)
@@ -816,6 +868,8 @@ def main():
             print(json.dumps({"impl": "reference", "unavailable": "the reference arm covers the gmg-pcg workload"}))
             return
         run_reference(args)
+    elif args.workload == "assemble":
+        run_assemble(args)
     elif args.workload == "gs-pcg":
         run_gs_pcg(args)
     elif args.workload == "galerkin":

@@ -137,6 +137,33 @@ typedef struct {
  * R the strict upper triangle). */
 int jfg_smooth(jfg_mat* A, const jfg_smoother_desc* sm, const double* h_rhs, double* h_x);
 
+/* ---- finite-element assembly on the device ---------------------------- */
+/* Assembles grad_coef * GRAD_GRAD + mass_coef * VALUE_VALUE (+ a VALUE right-
+ * hand side) of a Q_p Lagrange space (ContinuousTPFESpace with equidistant
+ * nodes, tensorproduct/ContinuousTPFESpace.java:30-50) on a uniform cx x cy
+ * grid of [x0,x1] x [y0,y1], replacing MatrixFESpace.writeCellIntegralsToMatrix
+ * / writeCellIntegralsToRhs (basic/MatrixFESpace.java:29-131) with the cell
+ * integrals of TPCellIntegral (tensorproduct/TPCellIntegral.java:78-159, a 5x5
+ * Gauss rule) and, when dirichlet != 0, the zero-data Dirichlet treatment of
+ * AcceptsMatrixBoundaryValues (basic/AcceptsMatrixBoundaryValues.java:25-44):
+ * boundary rows and columns zeroed, a unit diagonal, rhs 0 on the boundary.
+ *   numbering: the reference's first-appearance numbering (cells with the
+ *     last coordinate fastest, local functions x-fastest);
+ *   h_kappa_cells: optional per-cell factor of GRAD_GRAD (cx * cy, same cell order);
+ *   h_source_qp: optional source values at the 25 Gauss points of every cell
+ *     (cells x 25, x index slowest), NULL for a zero rhs;
+ *   outputs: the merged matrix, h_rhs[n], h_node_of_grid[nx * ny] (dof of grid
+ *     node gx * ny + gy) when not NULL, h_boundary (ascending boundary dofs,
+ *     2 (nx + ny) - 4 of them) when not NULL;  n = (p cx + 1)(p cy + 1). */
+typedef struct {
+    int p, cx, cy;
+    double x0, x1, y0, y1;
+    double grad_coef, mass_coef;
+    int dirichlet;
+} jfg_tp_desc;
+int jfg_assemble_tp(jfg_ctx* ctx, const jfg_tp_desc* d, const double* h_kappa_cells, const double* h_source_qp,
+                    jfg_mat** A, double* h_rhs, int* h_node_of_grid, int* h_boundary);
+
 /* ---- Gauss-Seidel triangular parts ---------------------------------- */
 /* The lower and upper triangles of a square matrix in an ordering of its
  * rows, with schedules of independent row sets for the two triangular

@@ -20,7 +20,10 @@ grids so that the solver sees the same kind of system the reference builds:
 * nodal prolongation between nested grids, P[f, c] = phi_c(x_f) with zero
   values omitted (multigrid/MGPreconditionerSpace.java:59-75).
 
-Everything is vectorised numpy; nothing here runs on the GPU.
+``assemble`` is vectorised numpy on the host; ``assemble_device`` builds the
+same system on the GPU (``jfg_assemble_tp``: numbering, cell integrals,
+Dirichlet rows and the right-hand side in CUDA kernels) and leaves the matrix
+on the device.
 """
 from __future__ import annotations
 
@@ -258,3 +261,38 @@ def prolongation(coarse: Space, fine: Space):
     cols = coarse.node_of_grid[cxa * coarse.ny + cya]
     order = np.lexsort((cols, rows))
     return rows[order].astype(np.int32), cols[order].astype(np.int32), vals[order]
+
+
+def assemble_device(space: Space, grad_coef=1.0, mass_coef=0.0, source=None, grad_coef_cells=None, dirichlet=True,
+                    ctx=None):
+    """``assemble`` on the GPU for zero Dirichlet data: returns (DeviceMatrix,
+    rhs, boundary dofs, node_of_grid).  The source is evaluated on the host at
+    the cells' Gauss points; the matrix stays on the device.  The numbering,
+    the merged matrix and the rhs are those of ``assemble`` (matrix and rhs to
+    rounding: the element tables and the Gauss sums are added in a different
+    order)."""
+    import ctypes as C
+
+    from . import _native as N
+    from .linalg import DeviceMatrix
+    ctx = ctx or N.default_context()
+    d = N.TPDesc(space.p, space.cx, space.cy, space.x0, space.x1, space.y0, space.y1, float(grad_coef),
+                 float(mass_coef), 1 if dirichlet else 0)
+    kap = None
+    if grad_coef_cells is not None:
+        kap = np.ascontiguousarray(grad_coef_cells, dtype=np.float64).reshape(space.cx * space.cy)
+    f = None
+    if source is not None:
+        X, Y = space.quadrature_points()
+        f = np.ascontiguousarray(source(X, Y), dtype=np.float64)
+    n = space.nx * space.ny
+    rhs = np.empty(n)
+    nog = np.empty(n, dtype=np.int32)
+    bd = np.empty(2 * (space.nx + space.ny) - 4, dtype=np.int32)
+    h = C.c_void_p()
+    st = N.load().jfg_assemble_tp(ctx.handle, C.byref(d), N.dptr(kap) if kap is not None else None,
+                                  N.dptr(f) if f is not None else None, C.byref(h), N.dptr(rhs), N.iptr(nog),
+                                  N.iptr(bd))
+    ctx.check(st)
+    A = DeviceMatrix._adopt(h, ctx)
+    return A, rhs, (bd if dirichlet else np.zeros(0, dtype=np.int32)), nog

@@ -315,6 +315,15 @@ static int wrap_product(jfg_ctx* ctx, jfg_mat** out, const std::function<jfg::Ma
     });
 }
 
+int jfg_assemble_tp(jfg_ctx* ctx, const jfg_tp_desc* d, const double* h_kappa_cells, const double* h_source_qp,
+                    jfg_mat** A, double* h_rhs, int* h_node_of_grid, int* h_boundary)
+{
+    if (!ctx || !d || !A) return JFG_ERR_BAD_ARG;
+    return wrap_product(ctx, A, [&] {
+        return jfg::assemble_tp(&ctx->c, *d, h_kappa_cells, h_source_qp, h_rhs, h_node_of_grid, h_boundary);
+    });
+}
+
 int jfg_matrix_mmmul(jfg_mat* a, jfg_mat* b, jfg_mat** out)
 {
     if (!a || !b || !out || a->ctx != b->ctx) return JFG_ERR_BAD_ARG;

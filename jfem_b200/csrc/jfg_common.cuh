@@ -157,6 +157,9 @@ Matrix* matrix_from_sorted_keys(Context* c, int rows, int cols, int64_t m, const
 Matrix* matrix_mmmul(Matrix* a, Matrix* b, bool sell = true);
 Matrix* matrix_tmmul(Matrix* a, Matrix* b, bool sell = true);
 Matrix* matrix_galerkin(Matrix* r, Matrix* a, Matrix* p);
+// finite-element assembly (jfg_assembly.cu)
+Matrix* assemble_tp(Context* c, const jfg_tp_desc& d, const double* h_kappa, const double* h_f, double* h_rhs,
+                    int* h_node_of_grid, int* h_boundary);
 void matrix_ensure_fp32(Matrix* m);
 void matrix_ensure_bf16(Matrix* m);
 uint64_t next_uid();

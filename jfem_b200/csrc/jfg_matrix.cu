@@ -329,6 +329,12 @@ static Matrix* from_device_coo(Context* c, int rows, int cols, int64_t nnz, cons
     return build_from_sorted(c, rows, cols, h_sel, key.p, v2.p);
 }
 
+Matrix* matrix_from_device_coo(Context* c, int rows, int cols, int64_t nnz, const int* d_ri, const int* d_ci,
+                               const double* d_v)
+{
+    return from_device_coo(c, rows, cols, nnz, d_ri, d_ci, d_v);
+}
+
 Matrix* matrix_from_coo(Context* c, int rows, int cols, int64_t nnz, const int* ri, const int* ci, const double* v,
                         bool keep_zeros)
 {
