@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cells", type=int, default=CELLS)
     ap.add_argument("--levels", type=int, default=LEVELS)
+    ap.add_argument("--vcycle", default="fp32", choices=["fp32", "fp16", "bf16"],
+                    help="storage of the V-cycle matrices of the mixed solve (FP32 vectors and sums in every case)")
     ap.add_argument("--workload", default="gmg-pcg", choices=["gmg-pcg", "cg-small", "batch-heat", "stokes", "learned", "galerkin", "gs-pcg",
                                                         "assemble"])
     ap.add_argument("--profile", default=None,
@@ -201,7 +203,8 @@ def run_ours(args):
         sms = [None] + [ForwardBackwardGaussSeidelSmoother(1, mats[l], "multicolour") for l in range(1, args.levels)]
     else:
         sms = [None] + [JacobiSmoother(2, 2.0 / 3.0)] * (args.levels - 1)
-    mg = MGPreconditioner(mats, prol, h.boundary, sms, cycles=1, use_fmg=False, precision="mixed", ctx=ctx)
+    hier = {"fp32": "mixed", "fp16": "mixed-fp16", "bf16": "mixed-bf16"}[args.vcycle]
+    mg = MGPreconditioner(mats, prol, h.boundary, sms, cycles=1, use_fmg=False, precision=hier, ctx=ctx)
     A = mats[-1]
     n = A.rows
     b_host = h.finest.rhs.copy()
@@ -226,13 +229,14 @@ def run_ours(args):
 
     info = N.SolveInfo()
 
-    def solve_dev(precision):
+    def solve_dev(precision, hierarchy=None):
         with torch.cuda.stream(stream):
             dx.copy_(e0)           # the reference's start vector e0
         o = opts(precision)
         if args.profile in ("solve-mixed-nograph", "gs-mixed-nograph"):
             o.use_graph = 0        # plain launches: every kernel of the solve is visible to a profiler
-        st = N.load().jfg_solve_dev(ctx.handle, N.PCG, A.handle, N.PREC_MG, mg.handle, C.c_void_p(db.data_ptr()),
+        g = mg if hierarchy is None else hierarchy
+        st = N.load().jfg_solve_dev(ctx.handle, N.PCG, A.handle, N.PREC_MG, g.handle, C.c_void_p(db.data_ptr()),
                                     C.c_void_p(dx.data_ptr()), C.byref(o), C.byref(info))
         ctx.check(st)
         return info.iterations, info.final_residual, info.outer_iterations
@@ -290,6 +294,19 @@ def run_ours(args):
     itm, resm, outer = solve_dev(HEADLINE)
     xm = dx.cpu().numpy().copy()
     rel_err = float(np.linalg.norm(xm - x64) / np.linalg.norm(x64))
+    # the same mixed solve with the V-cycle matrices stored as scaled FP16
+    # (reported beside; FP32 vectors and sums, the same FP64 stopping test)
+    alt = None
+    if args.vcycle == "fp32":
+        mg16 = MGPreconditioner(mats, prol, h.boundary, sms, cycles=1, use_fmg=False, precision="mixed-fp16",
+                                ctx=ctx)
+        ms16 = timed(lambda: solve_dev(HEADLINE, mg16), args.steps, args.warmup)
+        it16, res16, _ = solve_dev(HEADLINE, mg16)
+        x16 = dx.cpu().numpy().copy()
+        alt = {"time_s": ms16 / 1e3, "iterations": it16, "final_rel_residual": res16 / bnorm,
+               "rel_error_vs_fp64": float(np.linalg.norm(x16 - x64) / np.linalg.norm(x64)),
+               "mode": "FP64 PCG + FP32 V-cycle reading scaled-FP16 matrices"}
+        del mg16
 
     # end to end through the C ABI with host buffers (pinned), copies timed
     hb = torch.from_numpy(b_host).pin_memory()
@@ -360,9 +377,11 @@ def run_ours(args):
             "fp64_iterations": it64,
             "fp64_final_rel_residual": res64 / bnorm,
             "speedup_vs_fp64": ms64 / ms,
-            "mode": "FP64 PCG + FP32 V-cycle preconditioner",
+            "mode": "FP64 PCG + FP32 V-cycle preconditioner" + {"fp32": "", "fp16": " (matrices stored as scaled FP16)",
+                                                                   "bf16": " (matrices stored as BF16)"}[args.vcycle],
             "defect_correction": {"time_s": ms_dc / 1e3, "inner_iterations": it_dc, "outer_iterations": outer_dc,
                                   "final_rel_residual": res_dc / bnorm},
+            "fp16_vcycle": alt,
             "spmv_gbs": {"fp64": gbs64, "fp32": gbs32},
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
                     "path": "jfg_solve (C ABI) with pinned host rhs in and solution out; start e0 (opts.start=1)"},

@@ -229,7 +229,9 @@ typedef struct {
     int use_fmg;       /* 1: FMG correction first (MGPreconditionerInterface.mvMul, :353-379);
                           0: start the V-cycles from the boundary copy only */
     int precision;     /* 0: FP64 hierarchy; 1: FP32 hierarchy (for mixed-precision solves);
-                          2: FP32 hierarchy whose SpMVs read BF16 matrix values (FP32 vectors and sums) */
+                          2: FP32 hierarchy whose SpMVs read BF16 matrix values (FP32 vectors and sums);
+                          3: FP32 hierarchy whose SpMVs read FP16 matrix values scaled by a power of two
+                             per matrix (max |a| * 2^k in [2^14, 2^15)), FP32 vectors and sums */
 } jfg_mg_desc;
 /* Builds a hierarchy from per-level systems A[0..levels) (0 = coarsest),
  * prolongations P[l] (n_{l+1} x n_l, l < levels-1), Dirichlet node lists and

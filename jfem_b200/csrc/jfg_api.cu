@@ -502,7 +502,7 @@ int jfg_mg_create(jfg_ctx* ctx, int levels, jfg_mat* const* A, jfg_mat* const* P
             g->d64->init(&ctx->c, levels, g->A.data(), g->P.data(), bp.data(), nbp.data(), g->sm.data(), g->cycles,
                          g->use_fmg);
             if (g->d64->coarse_status != JFG_OK) throw Error{JFG_ERR_SINGULAR, "coarsest-level matrix is singular"};
-            JFG_CHECK(g->precision >= 0 && g->precision <= 2, JFG_ERR_BAD_ARG, "unknown hierarchy precision");
+            JFG_CHECK(g->precision >= 0 && g->precision <= 3, JFG_ERR_BAD_ARG, "unknown hierarchy precision");
             if (g->precision >= 1) g->fp32();
         } catch (...) {
             delete g;

@@ -12,6 +12,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <stdint.h>
 #include <atomic>
 #include <stdio.h>
@@ -123,7 +124,9 @@ struct Matrix {
     DevBuf<float> val32;          // optional FP32 copy
     DevBuf<__nv_bfloat16> val16;  // optional BF16 copy
     DevBuf<double> diag;          // merged diagonal
-    int has32 = 0, has16 = 0;
+    DevBuf<__half> valh;          // optional FP16 copy of the values scaled by 2^k (fits the FP16 range)
+    float hscale_inv = 1.0f;      // 2^-k: row sums of valh times this are the sums of the values
+    int has32 = 0, has16 = 0, hash = 0;
     int csr_only = 0;             // no SELL layout (an intermediate of a sparse product)
     Matrix* transposed = nullptr; // lazily built for tvMul
     uint64_t uid = 0;             // unique id (keys of cached CUDA graphs)
@@ -162,6 +165,7 @@ Matrix* assemble_tp(Context* c, const jfg_tp_desc& d, const double* h_kappa, con
                     int* h_node_of_grid, int* h_boundary);
 void matrix_ensure_fp32(Matrix* m);
 void matrix_ensure_bf16(Matrix* m);
+void matrix_ensure_fp16(Matrix* m);
 uint64_t next_uid();
 
 // Kernels launched by this process (graph replays are added per executed

@@ -105,10 +105,12 @@ __device__ __forceinline__ void load4(const __nv_bfloat16* p, float (&o)[4])
 }
 template <typename VT> struct AccOf { using T = VT; };
 template <> struct AccOf<__nv_bfloat16> { using T = float; };
+template <> struct AccOf<__half> { using T = float; };
 
 __device__ __forceinline__ float to_acc(float v) { return v; }
 __device__ __forceinline__ double to_acc(double v) { return v; }
 __device__ __forceinline__ float to_acc(__nv_bfloat16 v) { return __bfloat162float(v); }
+__device__ __forceinline__ float to_acc(__half v) { return __half2float(v); }
 
 // ---------------------------------------------------------------------------
 // programmatic dependent launch (PDL) and TMA/mbarrier helpers
@@ -133,6 +135,7 @@ struct SpmvArgs {
     int nslots;         // nslices * 32
     int tpr_log2;       // log2 of the threads that share one row (0..3)
     const int16_t* col16;  // SELL column offsets from the slot's row (IDX16 kernels)
+    float vscale;          // FP16 values: factor of the row sums (2^-k of the value scaling)
 };
 
 // 2^tpr_log2 adjacent threads per slot (row) of a 32-row slice; thread `sub`
@@ -210,6 +213,7 @@ k_spmv(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi
         }
     }
     for (int o = tpr >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if constexpr (std::is_same<VT, __half>::value) sum *= m.vscale;
     if (sub == 0 && r >= 0) epi(r, sum, acc);
     pdl_launch_dependents();
     if constexpr (NR > 0) red.reduce(acc);

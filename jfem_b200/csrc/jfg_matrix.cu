@@ -3,6 +3,8 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cmath>
+#include <cstring>
 #include <atomic>
 #include <numeric>
 
@@ -387,6 +389,55 @@ void matrix_ensure_fp32(Matrix* M)
     if (M->sell_len) k_to_f32<<<nblk(M->sell_len), 256, 0, M->ctx->stream>>>(M->sell_len, M->val.p, M->val32.p);
     JFG_CUDA(cudaGetLastError());
     M->has32 = 1;
+}
+
+namespace {
+__global__ void k_absmax(int64_t n, const double* __restrict__ a, unsigned long long* __restrict__ out)
+{
+    // |a| of finite doubles orders like its bit pattern: one atomicMax on the bits
+    unsigned long long m = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(a[i]));
+        m = b > m ? b : m;
+    }
+    atomicMax(out, m);
+}
+__global__ void k_to_f16(int64_t n, const double* __restrict__ a, double s, __half* __restrict__ b)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = __double2half(a[i] * s);       // exact scaling by 2^k, one rounding
+}
+}  // namespace
+
+// FP16 copy of the SpMV values scaled by s = 2^k with max |a| * s in
+// [2^14, 2^15]: the small entries (mass terms ~h^2) stay out of the FP16
+// subnormal range; the SpMV multiplies its row sums by 1/s (exact).
+void matrix_ensure_fp16(Matrix* M)
+{
+    if (M->hash) return;
+    cudaStream_t st = M->ctx->stream;
+    DevBuf<unsigned long long> mx;
+    mx.alloc(1);
+    JFG_CUDA(cudaMemsetAsync(mx.p, 0, sizeof(unsigned long long), st));
+    if (M->nnz) k_absmax<<<std::min<int64_t>(nblk(M->nnz), 1184), 256, 0, st>>>(M->nnz, M->csr_val.p, mx.p);
+    JFG_CUDA(cudaGetLastError());
+    unsigned long long hb = 0;
+    JFG_CUDA(cudaMemcpyAsync(&hb, mx.p, sizeof(hb), cudaMemcpyDeviceToHost, st));
+    JFG_CUDA(cudaStreamSynchronize(st));
+    double amax;
+    memcpy(&amax, &hb, sizeof(amax));
+    int e = 0;
+    if (amax > 0 && std::isfinite(amax)) {
+        std::frexp(amax, &e);                       // amax in [2^(e-1), 2^e)
+        e = 15 - e;                                 // amax * 2^e in [2^14, 2^15)
+        e = std::max(-120, std::min(120, e));
+    }
+    const double s = std::ldexp(1.0, e);
+    M->hscale_inv = (float)std::ldexp(1.0, -e);
+    M->valh.alloc(M->sell_len ? (size_t)M->sell_len : 1);
+    if (M->sell_len) k_to_f16<<<nblk(M->sell_len), 256, 0, st>>>(M->sell_len, M->val.p, s, M->valh.p);
+    JFG_CUDA(cudaGetLastError());
+    M->hash = 1;
 }
 
 void matrix_ensure_bf16(Matrix* M)

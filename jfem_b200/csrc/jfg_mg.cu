@@ -349,7 +349,7 @@ void launch_bottom(const BotParams<T, VT>& p, cudaStream_t st)
 
 template <typename T>
 void MGImpl<T>::init(Context* ctx, int levels, Matrix* const* As, Matrix* const* Ps, const int* const* bdry,
-                     const int* nbdry, const SmootherDesc* sms, int cycles_, int use_fmg_, int bf16)
+                     const int* nbdry, const SmootherDesc* sms, int cycles_, int use_fmg_, int vfmt)
 {
     c = ctx;
     L = levels;
@@ -379,8 +379,9 @@ void MGImpl<T>::init(Context* ctx, int levels, Matrix* const* As, Matrix* const*
             R[l] = matrix_transpose(P[l]);
         }
         if (std::is_same<T, float>::value) {
-            vbf16 = bf16 ? 1 : 0;
-            auto ensure = vbf16 ? matrix_ensure_bf16 : matrix_ensure_fp32;
+            vbf16 = vfmt == 1 ? 1 : 0;
+            vfp16 = vfmt == 2 ? 1 : 0;
+            auto ensure = vbf16 ? matrix_ensure_bf16 : (vfp16 ? matrix_ensure_fp16 : matrix_ensure_fp32);
             ensure(A[l]);
             if (l < L - 1) {
                 ensure(P[l]);
@@ -489,7 +490,7 @@ void MGImpl<T>::init(Context* ctx, int levels, Matrix* const* As, Matrix* const*
     // whole GPU does per launch.
     bot = -1;
     const char* eb = getenv("JFEM_MG_BOTTOM");
-    if (eb && eb[0] == '1') {
+    if (eb && eb[0] == '1' && !vfp16) {
         for (int l = 1; l < L - 1 && l < kBotMax; l++) {
             if (n[l] > kBotRows || sm[l].kind != JFG_SMOOTH_JACOBI || sm[l].runs < 1) break;
             bot = l;
@@ -519,6 +520,10 @@ static void mg_spmv(const MGImpl<T>& g, cudaStream_t st, const Matrix* M, const 
     if constexpr (std::is_same<T, float>::value) {
         if (g.vbf16) {
             spmv_launch<__nv_bfloat16, float, NR>(st, M, M->val16.p, x, epi, sc, done, fin);
+            return;
+        }
+        if (g.vfp16) {
+            spmv_launch<__half, float, NR>(st, M, M->valh.p, x, epi, sc, done, fin);
             return;
         }
     }
@@ -803,8 +808,8 @@ jfg::MGImpl<float>* jfg_mg::fp32()
         }
         d32.reset(new jfg::MGImpl<float>());
         const char* e = getenv("JFEM_MG_BF16");
-        const int bf16 = precision == 2 || (e && e[0] == '1');
-        d32->init(ctx, levels, A.data(), P.data(), bp.data(), nbp.data(), sm.data(), cycles, use_fmg, bf16);
+        const int vfmt = precision == 3 ? 2 : ((precision == 2 || (e && e[0] == '1')) ? 1 : 0);
+        d32->init(ctx, levels, A.data(), P.data(), bp.data(), nbp.data(), sm.data(), cycles, use_fmg, vfmt);
     }
     return d32.get();
 }

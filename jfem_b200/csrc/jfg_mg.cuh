@@ -30,6 +30,7 @@ struct MGImpl {
     int cycles = 3;
     int use_fmg = 1;
     int vbf16 = 0;                          // float hierarchy: matrices read as BF16 (FP32 vectors, FP32 sums)
+    int vfp16 = 0;                          // float hierarchy: matrices read as scaled FP16 (FP32 vectors, sums)
     int bot = -1;                           // levels 0..bot run as one cluster kernel (-1: none)
     std::vector<Matrix*> A, P, R;          // A[l], P[l] : n_{l+1} x n_l, R[l] = P[l]^T
     std::vector<int> n;
@@ -53,7 +54,7 @@ struct MGImpl {
     // Builds all level data; A/P are borrowed (must outlive the hierarchy).
     // bf16: (float hierarchy only) SpMVs read BF16 copies of the matrices.
     void init(Context* ctx, int levels, Matrix* const* As, Matrix* const* Ps, const int* const* bdry,
-              const int* nbdry, const SmootherDesc* sms, int cycles_, int use_fmg_, int bf16 = 0);
+              const int* nbdry, const SmootherDesc* sms, int cycles_, int use_fmg_, int vfmt = 0);
 
     // out = M v (the preconditioner application).  v and out are device
     // vectors of the finest size; `done` is an optional skip flag.

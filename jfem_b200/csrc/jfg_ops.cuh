@@ -123,7 +123,8 @@ void spmv_launch(cudaStream_t st, const Matrix* M, const VT* val, const XT* x, E
 {
     if (M->rows == 0) return;
     GridRed<NR, Fin> red{sc.partials, sc.counter, fin};
-    SpmvArgs a{M->off.p, M->perm.p, M->col.p, M->nslices * kSliceRows, M->tpr_log2, M->col16.p};
+    SpmvArgs a{M->off.p, M->perm.p, M->col.p, M->nslices * kSliceRows, M->tpr_log2, M->col16.p,
+               std::is_same<VT, __half>::value ? M->hscale_inv : 1.0f};
     const dim3 g(M->nblocks), b(kThreads);
     if (M->idx16) {
         switch (M->tpr_log2) {

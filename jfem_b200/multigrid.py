@@ -112,7 +112,8 @@ class MGPreconditioner(VectorMultiplyable):
     None).  cycles / use_fmg follow MGPreconditionerInterface.mvMul; the plain
     one-V-cycle preconditioner is cycles=1, use_fmg=False.
     precision="mixed" also builds the FP32 hierarchy used by mixed solves;
-    "mixed-bf16" builds it with BF16 matrix values (FP32 vectors and sums).
+    "mixed-bf16" builds it with BF16 matrix values (FP32 vectors and sums);
+    "mixed-fp16" with FP16 matrix values scaled by a power of two per matrix.
     """
 
     def __init__(self, systems, prolongations, boundary, smoothers, cycles=3, use_fmg=True, precision="fp64",
@@ -138,7 +139,7 @@ class MGPreconditioner(VectorMultiplyable):
         Ph = (C.c_void_p * max(L, 1))(*([p.handle for p in self._P] + [None]))
         Bh = (C.POINTER(C.c_int) * L)(*[N.iptr(b) for b in self._bd])
         nb = np.array([b.size for b in self._bd], dtype=np.int32)
-        levels = {"fp64": 0, "mixed": 1, "mixed-bf16": 2}
+        levels = {"fp64": 0, "mixed": 1, "mixed-bf16": 2, "mixed-fp16": 3}
         if precision not in levels:
             raise IllegalArgumentException(f"unknown hierarchy precision {precision!r}")
         desc = N.MGDesc(int(cycles), 1 if use_fmg else 0, levels[precision])

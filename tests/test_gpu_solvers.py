@@ -247,12 +247,13 @@ def test_pcg_mg_full_size(ctx):
     assert it64 <= 20
 
 
-def test_pcg_bf16_vcycle(ctx):
-    """FP64 PCG with the FP32 V-cycle reading BF16 matrices (hierarchy
-    precision "mixed-bf16"): same FP64 true residual, at most one extra
-    iteration over the FP64 preconditioner."""
+@pytest.mark.parametrize("precision", ["mixed-bf16", "mixed-fp16"])
+def test_pcg_bf16_vcycle(ctx, precision):
+    """FP64 PCG with the FP32 V-cycle reading BF16 or scaled-FP16 matrices
+    (hierarchy precision "mixed-bf16" / "mixed-fp16"): same FP64 true
+    residual, at most one extra iteration over the FP64 preconditioner."""
     h = mg_levels(2, 4, 6, modes=16, seed=3)    # Q2 128x128
-    mats_o, mg_o, mats, mg = _mg_pair(h, ctx, (O.SMOOTH_JACOBI, 2, 2.0 / 3.0), 1, False, precision="mixed-bf16")
+    mats_o, mg_o, mats, mg = _mg_pair(h, ctx, (O.SMOOTH_JACOBI, 2, 2.0 / 3.0), 1, False, precision=precision)
     b = h.finest.rhs
     tol = 1e-8 * np.linalg.norm(b)
     ref = O.solve_pcg(mats_o[-1], mg_o, b, tol)
@@ -262,6 +263,40 @@ def test_pcg_bf16_vcycle(ctx):
     assert s.last.status == N.OK and s.last.final_residual <= tol
     assert rel(x, ref.x) < 1e-7
     assert s.iterations <= ref.iterations + 1
+    if precision == "mixed-fp16":
+        assert s.iterations == ref.iterations
+
+
+def _fp16_rounded(dev_matrix):
+    """The oracle matrix of the merged values rounded as the FP16 hierarchy
+    stores them: fp16(a 2^k) / 2^k with max |a| 2^k in [2^14, 2^15)."""
+    ri, ci, v = dev_matrix.coo()
+    k = 15 - int(np.frexp(np.abs(v).max())[1])
+    vh = (v * 2.0 ** k).astype(np.float16).astype(np.float64) / 2.0 ** k
+    assert np.count_nonzero(vh) == np.count_nonzero(v)          # no entry flushed to zero
+    return O.CooMatrix(dev_matrix.rows, dev_matrix.cols, ri, ci, vh)
+
+
+def test_fp16_vcycle_matches_rounded_oracle(ctx):
+    """Mixed PCG with the FP16 hierarchy against the oracle PCG whose V-cycle
+    runs in FP64 on the same FP16-rounded matrices: same iterations, residual
+    histories within 10 % (the GPU keeps the Jacobi diagonal and the coarsest
+    inverse in full precision, the oracle's V-cycle takes them from the
+    rounded matrices)."""
+    h = mg_levels(2, 4, 5, modes=8, seed=2)
+    mats_o, mg_o, mats, mg = _mg_pair(h, ctx, (O.SMOOTH_JACOBI, 2, 2.0 / 3.0), 1, False, precision="mixed-fp16")
+    prol = [DeviceMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l], ctx) for l in range(len(h.systems) - 1)]
+    mg_r = O.MGPreconditioner([_fp16_rounded(m) for m in mats], [_fp16_rounded(p) for p in prol], h.boundary,
+                              [None] + [(O.SMOOTH_JACOBI, 2, 2.0 / 3.0)] * (len(mats) - 1), cycles=1, use_fmg=False)
+    b = h.finest.rhs
+    tol = 1e-8 * np.linalg.norm(b)
+    ref = O.solve_pcg(mats_o[-1], mg_r, b, tol)
+    s = IterativeSolver(ctx=ctx)
+    s.precision = "mixed-precond"
+    s.solvePCG(mats[-1], mg, b, tol)
+    assert s.last.status == N.OK and s.iterations == ref.iterations
+    assert len(s.last.history) == len(ref.history)
+    np.testing.assert_allclose(s.last.history, ref.history, rtol=0.1)
 
 
 def test_start_modes(ctx):
