@@ -15,7 +15,8 @@ OBJ = os.path.join(HERE, "build")
 LIB = os.path.join(HERE, "libjfem_gpu.so")
 SOURCES = ["jfg_matrix.cu", "jfg_mg.cu", "jfg_dense.cu", "jfg_krylov.cu", "jfg_api.cu", "jfg_noalloc.cu",
            "jfg_batch.cu", "jfg_cnn.cu", "jfg_cnn_tc.cu", "jfg_schwarz.cu", "jfg_block.cu",
-           "jfg_spgemm.cu", "jfg_gs.cu", "jfg_assembly.cu"]
+           "jfg_spgemm.cu", "jfg_gs.cu", "jfg_assembly.cu",
+           "jfg_cg_small.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = [*ARCH, "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC"]

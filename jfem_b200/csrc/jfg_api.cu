@@ -697,11 +697,17 @@ static int solve_impl(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, cons
             h.n = n;
             h.status = JFG_NOT_CONVERGED;
             JFG_CUDA(cudaMemcpyAsync(w.ctl.p, &h, sizeof(Ctl), cudaMemcpyHostToDevice, st));
-            int nodes = run_cg<double>(w, 0, M, P64, d_b, d_x, w.v64[0].p, w.v64[1].p, w.v64[2].p, w.v64[3].p,
-                                       false, use_graph, chunk);
-            JFG_CUDA(cudaMemcpyAsync(&res, w.ctl.p, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
-            JFG_CUDA(cudaStreamSynchronize(st));
-            note_launch((unsigned long long)nodes * (unsigned long long)(res.iter > 0 ? res.iter : 1));
+            if (kind == JFG_CG && pk == JFG_PREC_NONE && cg_small_fits(M)) {
+                run_cg_small(w, M, d_b, d_x);       // the whole solve in one cluster launch
+                JFG_CUDA(cudaMemcpyAsync(&res, w.ctl.p, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+                JFG_CUDA(cudaStreamSynchronize(st));
+            } else {
+                int nodes = run_cg<double>(w, 0, M, P64, d_b, d_x, w.v64[0].p, w.v64[1].p, w.v64[2].p,
+                                           w.v64[3].p, false, use_graph, chunk);
+                JFG_CUDA(cudaMemcpyAsync(&res, w.ctl.p, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+                JFG_CUDA(cudaStreamSynchronize(st));
+                note_launch((unsigned long long)nodes * (unsigned long long)(res.iter > 0 ? res.iter : 1));
+            }
         }
     } else if (kind == JFG_BICGSTAB || kind == JFG_PBICGSTAB) {
         if (maxit <= 0) maxit = kind == JFG_BICGSTAB ? n : 10 * n;

@@ -65,6 +65,9 @@ int run_loop(SolverWork& w, const int* flag, const std::vector<uintptr_t>& key, 
 template <typename T>
 int run_cg(SolverWork& w, int ci, Matrix* A, const Precond<T>& M, const T* b, T* x, T* r, T* p, T* Ap, T* z,
             bool xzero, int use_graph, int chunk);
+// unpreconditioned FP64 CG of a small system in one cluster launch (jfg_cg_small.cu)
+bool cg_small_fits(const Matrix* A);
+void run_cg_small(SolverWork& w, Matrix* A, const double* b, double* x);
 template <typename T>
 int run_bicgstab(SolverWork& w, int ci, Matrix* A, const Precond<T>& M, const T* b, T* x, T* const* v,
                   int use_graph, int chunk);

@@ -321,3 +321,35 @@ def test_start_modes(ctx):
             outs.append((x, info.iterations))
         assert outs[0][1] == outs[1][1]
         assert np.array_equal(outs[0][0], outs[1][0])
+
+
+@pytest.mark.parametrize("p,cells", [(1, 64), (2, 40), (1, 127)])
+def test_cg_small_cluster_path(ctx, monkeypatch, p, cells):
+    """Unpreconditioned CG of systems up to 16,384 rows runs in one cluster
+    launch: same iterations as the oracle (+-2) and as the multi-kernel loop,
+    solutions equal to rounding, the first residuals equal; the maxit and
+    zero-iteration exits."""
+    sp, sy = fe_system(p, cells)
+    A = dev(sy, ctx)
+    b = sy.rhs
+    tol = 1e-10 * np.linalg.norm(b)
+    ref = O.solve_cg(coo_oracle(sy), b, tol)
+    out = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("JFEM_SMALL_CG", flag)
+        s = IterativeSolver(ctx=ctx)
+        x = s.solveCG(A, b, tol)
+        out[flag] = (x, s.iterations, s.last.status, s.last.history)
+    x1, it1, st1, h1 = out["1"]
+    x0, it0, st0, h0 = out["0"]
+    assert st1 == N.OK and st0 == N.OK
+    assert abs(it1 - ref.iterations) <= 2 and abs(it1 - it0) <= 2
+    assert rel(x1, ref.x) < 1e-8 and rel(x1, x0) < 1e-8
+    # histories agree until rounding differences are amplified (as for the oracle)
+    np.testing.assert_allclose(h1[:5], h0[:5], rtol=1e-8)
+    monkeypatch.setenv("JFEM_SMALL_CG", "1")
+    s = IterativeSolver(ctx=ctx)
+    s._run(N.CG, A, None, b, 1e-30, s._start(len(b)), maxit=5)
+    assert s.last.status == N.NOT_CONVERGED and s.iterations == 5
+    s._run(N.CG, A, None, b, 1e300, s._start(len(b)))
+    assert s.last.status == N.OK and s.iterations == 0
