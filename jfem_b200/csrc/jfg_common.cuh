@@ -128,6 +128,7 @@ struct Matrix {
     float hscale_inv = 1.0f;      // 2^-k: row sums of valh times this are the sums of the values
     int has32 = 0, has16 = 0, hash = 0;
     int csr_only = 0;             // no SELL layout (an intermediate of a sparse product)
+    int cg_small_nnz = -1;        // small-system CG: largest CSR slice of its 8 row blocks (-1: not computed)
     Matrix* transposed = nullptr; // lazily built for tvMul
     uint64_t uid = 0;             // unique id (keys of cached CUDA graphs)
     Matrix();

@@ -335,18 +335,22 @@ def test_cg_small_cluster_path(ctx, monkeypatch, p, cells):
     tol = 1e-10 * np.linalg.norm(b)
     ref = O.solve_cg(coo_oracle(sy), b, tol)
     out = {}
-    for flag in ("1", "0"):
+    for flag, smem in (("1", "1"), ("1", "0"), ("0", "1")):     # shared-memory variant, global variant, loop
         monkeypatch.setenv("JFEM_SMALL_CG", flag)
+        monkeypatch.setenv("JFEM_SMALL_CG_SMEM", smem)
         s = IterativeSolver(ctx=ctx)
         x = s.solveCG(A, b, tol)
-        out[flag] = (x, s.iterations, s.last.status, s.last.history)
-    x1, it1, st1, h1 = out["1"]
-    x0, it0, st0, h0 = out["0"]
-    assert st1 == N.OK and st0 == N.OK
-    assert abs(it1 - ref.iterations) <= 2 and abs(it1 - it0) <= 2
-    assert rel(x1, ref.x) < 1e-8 and rel(x1, x0) < 1e-8
-    # histories agree until rounding differences are amplified (as for the oracle)
-    np.testing.assert_allclose(h1[:5], h0[:5], rtol=1e-8)
+        out[flag + smem] = (x, s.iterations, s.last.status, s.last.history)
+    x0, it0, st0, h0 = out["01"]
+    assert st0 == N.OK
+    for key in ("11", "10"):
+        x1, it1, st1, h1 = out[key]
+        assert st1 == N.OK
+        assert abs(it1 - ref.iterations) <= 2 and abs(it1 - it0) <= 2
+        assert rel(x1, ref.x) < 1e-8 and rel(x1, x0) < 1e-8
+        # histories agree until rounding differences are amplified (as for the oracle)
+        np.testing.assert_allclose(h1[:5], h0[:5], rtol=1e-8)
+    monkeypatch.setenv("JFEM_SMALL_CG_SMEM", "1")
     monkeypatch.setenv("JFEM_SMALL_CG", "1")
     s = IterativeSolver(ctx=ctx)
     s._run(N.CG, A, None, b, 1e-30, s._start(len(b)), maxit=5)
