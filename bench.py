@@ -836,6 +836,18 @@ def run_stokes(args):
                                          "overlap, 9 colours) | nu / lumped pressure mass",
                        "pressure": "consistent singular system, gauge p0 = 0 after the solve"},
             "variants": out, "assemble_s": assemble_s}
+    # the same system assembled on the GPU (jfg_assemble_taylor_hood), timed
+    from jfem_b200.stokes import TaylorHoodSpace, assemble_stokes_device, fourier_force
+    th = TaylorHoodSpace(prob.spaces[-1].cx, prob.spaces[-1].cy)
+    fo = fourier_force(seed=0)
+    assemble_stokes_device(th, 1.0, fo, pin_pressure=False, ctx=ctx)
+    torch.cuda.synchronize()
+    t3 = time.perf_counter()
+    Ad, _, _ = assemble_stokes_device(th, 1.0, fo, pin_pressure=False, ctx=ctx)
+    torch.cuda.synchronize()
+    line["assemble_device_s"] = time.perf_counter() - t3
+    line["assemble_device_nnz_equal"] = bool(Ad.nnz == DeviceMatrix(s.n, s.n, s.rows, s.cols, s.vals, ctx).nnz)
+    del Ad
     A64 = DeviceMatrix(s.n, s.n, s.rows, s.cols, s.vals, ctx)
     ms64 = A64.time_spmv(precision=0, iters=50)
     line["spmv_gbs_fp64"] = spmv_bytes(s.n, A64.nnz, 8, 8) / (ms64 * 1e-3) / 1e9

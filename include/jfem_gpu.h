@@ -164,6 +164,21 @@ typedef struct {
 int jfg_assemble_tp(jfg_ctx* ctx, const jfg_tp_desc* d, const double* h_kappa_cells, const double* h_source_qp,
                     jfg_mat** A, double* h_rhs, int* h_node_of_grid, int* h_boundary);
 
+/* The Taylor-Hood Q2/Q1 Stokes system on the unit square with cx x cy cells
+ * (unknowns: u0 and u1 on the Q2 node grid, then p on the Q1 grid, each grid
+ * numbered x-major): nu * GRAD_GRAD per velocity component and the
+ * divergence blocks -B, -B^T (the lid-driven-cavity setup of the Stokes
+ * configuration); velocity Dirichlet data on the whole boundary, u0 = 1 on the
+ * top side when lid != 0, and the first pressure unknown fixed to 0 when
+ * pin_pressure != 0, eliminated as AcceptsMatrixBoundaryValues does
+ * (basic/AcceptsMatrixBoundaryValues.java:25-44: rows and columns zeroed, a
+ * unit diagonal, the boundary values lifted into the rhs).
+ * h_force_qp: optional body force at the 25 Gauss points of every cell
+ * (2 x cells x 25: component, cell, point); outputs the matrix, h_rhs[n] and
+ * the ascending velocity boundary dofs (2 (2 (vnx + vny) - 4) of them). */
+int jfg_assemble_taylor_hood(jfg_ctx* ctx, int cx, int cy, double nu, const double* h_force_qp, int lid,
+                             int pin_pressure, jfg_mat** A, double* h_rhs, int* h_velocity_boundary);
+
 /* ---- Gauss-Seidel triangular parts ---------------------------------- */
 /* The lower and upper triangles of a square matrix in an ordering of its
  * rows, with schedules of independent row sets for the two triangular

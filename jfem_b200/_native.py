@@ -35,6 +35,7 @@ EXPORTED = [
     "jfg_spmv_t_dev", "jfg_spmv_f32_dev", "jfg_matrix_diag", "jfg_spmv_time", "jfg_smooth",
     "jfg_matrix_csr", "jfg_matrix_mmmul", "jfg_matrix_tmmul", "jfg_matrix_galerkin",
     "jfg_gs_create", "jfg_gs_free", "jfg_gs_info", "jfg_gs_ranks", "jfg_assemble_tp",
+    "jfg_assemble_taylor_hood",
     "jfg_mg_create", "jfg_mg_free", "jfg_mg_apply", "jfg_mg_vcycle", "jfg_mg_fmg",
     "jfg_solver_opts_default", "jfg_solve", "jfg_solve_dev",
     "jfg_dense_solve", "jfg_dense_inverse", "jfg_sparse_solve", "jfg_cg_noalloc",
@@ -136,6 +137,8 @@ def load():
     L.jfg_gs_info.argtypes = [_P, _I, _I, _I]
     L.jfg_gs_ranks.argtypes = [_P, _I]
     L.jfg_assemble_tp.argtypes = [_P, C.POINTER(TPDesc), _D, _D, C.POINTER(_P), _D, _I, _I]
+    L.jfg_assemble_taylor_hood.argtypes = [_P, C.c_int, C.c_int, C.c_double, _D, C.c_int, C.c_int, C.POINTER(_P),
+                                           _D, _I]
     L.jfg_smooth.argtypes = [_P, C.POINTER(SmootherDesc), _D, _D]
     L.jfg_mg_create.argtypes = [_P, C.c_int, C.POINTER(_P), C.POINTER(_P), C.POINTER(_I), _I,
                                 C.POINTER(SmootherDesc), C.POINTER(MGDesc), C.POINTER(_P)]

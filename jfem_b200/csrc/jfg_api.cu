@@ -324,6 +324,15 @@ int jfg_assemble_tp(jfg_ctx* ctx, const jfg_tp_desc* d, const double* h_kappa_ce
     });
 }
 
+int jfg_assemble_taylor_hood(jfg_ctx* ctx, int cx, int cy, double nu, const double* h_force_qp, int lid,
+                             int pin_pressure, jfg_mat** A, double* h_rhs, int* h_velocity_boundary)
+{
+    if (!ctx || !A || !(nu > 0)) return JFG_ERR_BAD_ARG;
+    return wrap_product(ctx, A, [&] {
+        return jfg::assemble_th(&ctx->c, cx, cy, nu, h_force_qp, lid, pin_pressure, h_rhs, h_velocity_boundary);
+    });
+}
+
 int jfg_matrix_mmmul(jfg_mat* a, jfg_mat* b, jfg_mat** out)
 {
     if (!a || !b || !out || a->ctx != b->ctx) return JFG_ERR_BAD_ARG;

@@ -164,6 +164,8 @@ Matrix* matrix_galerkin(Matrix* r, Matrix* a, Matrix* p);
 // finite-element assembly (jfg_assembly.cu)
 Matrix* assemble_tp(Context* c, const jfg_tp_desc& d, const double* h_kappa, const double* h_f, double* h_rhs,
                     int* h_node_of_grid, int* h_boundary);
+Matrix* assemble_th(Context* c, int cx, int cy, double nu, const double* h_force_qp, int lid, int pin,
+                    double* h_rhs, int* h_boundary);
 void matrix_ensure_fp32(Matrix* m);
 void matrix_ensure_bf16(Matrix* m);
 void matrix_ensure_fp16(Matrix* m);

@@ -186,6 +186,31 @@ def assemble_stokes(th: TaylorHoodSpace, nu: float = 1.0, force=None, lid: bool 
     return StokesSystem(th.n, th.nv, R, Cc, V, rhs, bd, th.nv if pin_pressure else -1)
 
 
+def assemble_stokes_device(th: TaylorHoodSpace, nu: float = 1.0, force=None, lid: bool = True,
+                           pin_pressure: bool = True, ctx=None):
+    """``assemble_stokes`` on the GPU (jfg_assemble_taylor_hood): returns
+    (DeviceMatrix, rhs, velocity boundary).  The force is evaluated on the
+    host at the cells' Gauss points; the matrix stays on the device and
+    equals the host system's merged matrix to rounding."""
+    from . import _native as N
+    from .linalg import DeviceMatrix
+    ctx = ctx or N.default_context()
+    f = None
+    if force is not None:
+        qi, qj = np.repeat(np.arange(5), 5), np.tile(np.arange(5), 5)
+        ix, iy = np.meshgrid(np.arange(th.cx), np.arange(th.cy), indexing="ij")
+        X = (ix.ravel()[:, None] + QUAD_T[qi][None, :]) * th.hx
+        Y = (iy.ravel()[:, None] + QUAD_T[qj][None, :]) * th.hy
+        f = np.ascontiguousarray(np.stack([force(X, Y, 0), force(X, Y, 1)]), dtype=np.float64)
+    rhs = np.empty(th.n)
+    bd = np.empty(2 * (2 * (th.vnx + th.vny) - 4), dtype=np.int32)
+    h = C.c_void_p()
+    ctx.check(N.load().jfg_assemble_taylor_hood(ctx.handle, th.cx, th.cy, float(nu),
+                                                N.dptr(f) if f is not None else None, 1 if lid else 0,
+                                                1 if pin_pressure else 0, C.byref(h), N.dptr(rhs), N.iptr(bd)))
+    return DeviceMatrix._adopt(h, ctx), rhs, bd
+
+
 def velocity_block(th: TaylorHoodSpace, nu: float = 1.0):
     """The velocity-velocity block with zero Dirichlet rows eliminated (COO)."""
     K, *_ = _tables(th.hx, th.hy)

@@ -62,3 +62,19 @@ def test_full_size_q2_512(ctx):
     s = IterativeSolver(ctx=ctx)
     x = s._run(N.CG, A, None, rhs, 1e-30, s._start(len(rhs)), maxit=20)
     assert s.last.status == N.NOT_CONVERGED and np.isfinite(x).all()
+
+
+@pytest.mark.parametrize("cx,cy,lid,pin", [(8, 8, True, True), (6, 10, True, False), (4, 4, False, True)])
+def test_taylor_hood_matches_host(ctx, cx, cy, lid, pin):
+    from jfem_b200.stokes import TaylorHoodSpace, assemble_stokes, assemble_stokes_device, fourier_force
+    th = TaylorHoodSpace(cx, cy)
+    f = fourier_force(seed=1)
+    sy = assemble_stokes(th, 0.7, f, lid=lid, pin_pressure=pin)
+    Ah = DeviceMatrix(sy.n, sy.n, sy.rows, sy.cols, sy.vals)
+    A, rhs, bd = assemble_stokes_device(th, 0.7, f, lid=lid, pin_pressure=pin)
+    ph, ch, vh = Ah.csr()
+    pg, cg, vg = A.csr()
+    assert np.array_equal(pg, ph) and np.array_equal(cg, ch)
+    np.testing.assert_allclose(vg, vh, rtol=1e-14, atol=1e-14 * np.abs(vh).max())
+    np.testing.assert_allclose(rhs, sy.rhs, rtol=1e-13, atol=1e-13 * np.abs(sy.rhs).max())
+    assert np.array_equal(bd, sy.velocity_boundary)
