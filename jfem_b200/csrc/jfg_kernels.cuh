@@ -103,6 +103,46 @@ __device__ __forceinline__ void load4(const __nv_bfloat16* p, float (&o)[4])
     float2 fl = __bfloat1622float2(lo), fh = __bfloat1622float2(hi);
     o[0] = fl.x; o[1] = fl.y; o[2] = fh.x; o[3] = fh.y;
 }
+// Matrix-stream loads: every value and column entry is read once per product,
+// so it is not allocated in L1 (which then keeps the x entries that
+// neighbouring rows gather) and each L2 miss fetches 256 bytes.
+__device__ __forceinline__ float ld_stream(const float* p)
+{
+    float v;
+    asm("ld.global.nc.L1::no_allocate.L2::256B.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ double ld_stream(const double* p)
+{
+    double v;
+    asm("ld.global.nc.L1::no_allocate.L2::256B.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ int ld_stream(const int* p)
+{
+    int v;
+    asm("ld.global.nc.L1::no_allocate.L2::256B.s32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ int ld_stream(const int16_t* p)
+{
+    short v;
+    asm("ld.global.nc.L1::no_allocate.L2::256B.s16 %0, [%1];" : "=h"(v) : "l"(p));
+    return (int)v;
+}
+__device__ __forceinline__ __half ld_stream(const __half* p)
+{
+    unsigned short v;
+    asm("ld.global.nc.L1::no_allocate.L2::256B.b16 %0, [%1];" : "=h"(v) : "l"(p));
+    return __ushort_as_half(v);
+}
+__device__ __forceinline__ __nv_bfloat16 ld_stream(const __nv_bfloat16* p)
+{
+    unsigned short v;
+    asm("ld.global.nc.L1::no_allocate.L2::256B.b16 %0, [%1];" : "=h"(v) : "l"(p));
+    return __ushort_as_bfloat16(v);
+}
+
 template <typename VT> struct AccOf { using T = VT; };
 template <> struct AccOf<__nv_bfloat16> { using T = float; };
 template <> struct AccOf<__half> { using T = float; };
@@ -186,8 +226,8 @@ k_spmv(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi
 #pragma unroll
                 for (int u = 0; u < U; u++) {
                     const bool ok = k + u * tpr < len;
-                    c[u] = ok ? base + __ldg(cp + 32 * k + u * st) : base;
-                    v[u] = ok ? to_acc(__ldg(vp + 32 * k + u * st)) : (AT)0;
+                    c[u] = ok ? base + ld_stream(cp + 32 * k + u * st) : base;
+                    v[u] = ok ? to_acc(ld_stream(vp + 32 * k + u * st)) : (AT)0;
                 }
 #pragma unroll
                 for (int u = 0; u < U; u++) xv[u] = k + u * tpr < len ? (AT)__ldg(x + c[u]) : (AT)0;
@@ -198,10 +238,10 @@ k_spmv(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi
         } else {
             const int* cp = m.col + o + lane;
             for (; k + 3 * tpr < len; k += 4 * tpr) {
-                const int c0 = __ldg(cp + 32 * k), c1 = __ldg(cp + 32 * k + st);
-                const int c2 = __ldg(cp + 32 * k + 2 * st), c3 = __ldg(cp + 32 * k + 3 * st);
-                const AT v0 = to_acc(__ldg(vp + 32 * k)), v1 = to_acc(__ldg(vp + 32 * k + st));
-                const AT v2 = to_acc(__ldg(vp + 32 * k + 2 * st)), v3 = to_acc(__ldg(vp + 32 * k + 3 * st));
+                const int c0 = ld_stream(cp + 32 * k), c1 = ld_stream(cp + 32 * k + st);
+                const int c2 = ld_stream(cp + 32 * k + 2 * st), c3 = ld_stream(cp + 32 * k + 3 * st);
+                const AT v0 = to_acc(ld_stream(vp + 32 * k)), v1 = to_acc(ld_stream(vp + 32 * k + st));
+                const AT v2 = to_acc(ld_stream(vp + 32 * k + 2 * st)), v3 = to_acc(ld_stream(vp + 32 * k + 3 * st));
                 const AT x0 = (AT)__ldg(x + c0), x1 = (AT)__ldg(x + c1), x2 = (AT)__ldg(x + c2),
                          x3 = (AT)__ldg(x + c3);
                 sum += v0 * x0;
@@ -209,7 +249,7 @@ k_spmv(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi
                 sum += v2 * x2;
                 sum += v3 * x3;
             }
-            for (; k < len; k += tpr) sum += to_acc(__ldg(vp + 32 * k)) * (AT)__ldg(x + __ldg(cp + 32 * k));
+            for (; k < len; k += tpr) sum += to_acc(ld_stream(vp + 32 * k)) * (AT)__ldg(x + ld_stream(cp + 32 * k));
         }
     }
     for (int o = tpr >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
