@@ -124,42 +124,134 @@ __device__ __forceinline__ double sell_row(const int* off, const int* col, const
     for (int k = 0; k < len; k++) sum += (double)val[o + 32 * k + lane] * (double)x[col[o + 32 * k + lane]];
     return sum;
 }
-__device__ __forceinline__ float sell_row32(const int* off, const int* col, const int16_t* col16, const float* val,
-                                            const float* x, int slot, int row)
+// The two passes of an inner PCG iteration take kRowsPerPass rows of a thread
+// at once (slots t, t + B, t + 2B, ... as in a plain strided loop): all loads
+// of those rows are issued before any of their results is used, so a thread
+// has several rows' gathers in flight instead of one dependent chain per row.
+// Row sums keep the entry order and partial dot products the row order of the
+// one-row-at-a-time loop, so the results are the same bits.
+constexpr int kRowsPerPass = 4;
+constexpr int kRowChunk = 3;     // entries of each row loaded together
+
+template <int U, int CH, bool I16>
+__device__ __forceinline__ void sell_rows32(const SysDesc& S, const int (&slot)[U], const int (&row)[U],
+                                            float (&q)[U])
 {
-    const int s = slot >> 5, lane = slot & 31;
-    const int o = off[s];
-    const int len = (off[s + 1] - o) >> 5;
-    const float* vp = val + o + lane;
-    float sum = 0;
-    int k = 0;
-    if (col16) {            // 2 bytes per entry instead of 4
-        const int16_t* cp = col16 + o + lane;
-        for (; k + 4 <= len; k += 4) {
-            const int c0 = row + cp[32 * k], c1 = row + cp[32 * (k + 1)];
-            const int c2 = row + cp[32 * (k + 2)], c3 = row + cp[32 * (k + 3)];
-            const float v0 = vp[32 * k], v1 = vp[32 * (k + 1)], v2 = vp[32 * (k + 2)], v3 = vp[32 * (k + 3)];
-            const float x0 = x[c0], x1 = x[c1], x2 = x[c2], x3 = x[c3];
-            sum += v0 * x0;
-            sum += v1 * x1;
-            sum += v2 * x2;
-            sum += v3 * x3;
+    const int* __restrict__ off = S.k_off;
+    const float* __restrict__ val = S.k_v32;
+    const float* x = S.z;                 // written inside the kernel: coherent loads
+    int o[U], len[U];
+    int maxlen = 0;
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        q[u] = 0.f;
+        o[u] = 0;
+        len[u] = 0;
+        if (row[u] >= 0) {
+            const int s = slot[u] >> 5;
+            const int a = __ldg(off + s);
+            o[u] = a + (slot[u] & 31);
+            len[u] = (__ldg(off + s + 1) - a) >> 5;
         }
-        for (; k < len; k++) sum += vp[32 * k] * x[row + cp[32 * k]];
-        return sum;
+        maxlen = max(maxlen, len[u]);
     }
-    const int* cp = col + o + lane;
-    for (; k + 4 <= len; k += 4) {
-        const int c0 = cp[32 * k], c1 = cp[32 * (k + 1)], c2 = cp[32 * (k + 2)], c3 = cp[32 * (k + 3)];
-        const float v0 = vp[32 * k], v1 = vp[32 * (k + 1)], v2 = vp[32 * (k + 2)], v3 = vp[32 * (k + 3)];
-        const float x0 = x[c0], x1 = x[c1], x2 = x[c2], x3 = x[c3];
-        sum += v0 * x0;
-        sum += v1 * x1;
-        sum += v2 * x2;
-        sum += v3 * x3;
+    for (int k = 0; k < maxlen; k += CH) {
+        int c[U][CH];
+        float v[U][CH], xv[U][CH];
+#pragma unroll
+        for (int u = 0; u < U; u++)
+#pragma unroll
+            for (int j = 0; j < CH; j++) {
+                const bool ok = k + j < len[u];
+                const int idx = o[u] + 32 * (k + j);
+                if constexpr (I16)
+                    c[u][j] = ok ? row[u] + (int)__ldg(S.k_col16 + idx) : 0;
+                else
+                    c[u][j] = ok ? __ldg(S.k_col + idx) : 0;
+                v[u][j] = ok ? __ldg(val + idx) : 0.f;
+            }
+#pragma unroll
+        for (int u = 0; u < U; u++)
+#pragma unroll
+            for (int j = 0; j < CH; j++) xv[u][j] = k + j < len[u] ? x[c[u][j]] : 0.f;
+#pragma unroll
+        for (int u = 0; u < U; u++)
+#pragma unroll
+            for (int j = 0; j < CH; j++)
+                if (k + j < len[u]) q[u] += v[u][j] * xv[u][j];
     }
-    for (; k < len; k++) sum += vp[32 * k] * x[cp[32 * k]];
-    return sum;
+}
+
+// p = z + beta p ; Ap = K z + beta Ap ; returns this thread's part of p.Ap.
+template <bool I16>
+__device__ __forceinline__ double pass_direction(const SysDesc& S, int s0, int s1, float bf)
+{
+    constexpr int U = kRowsPerPass;
+    const int B = blockDim.x;
+    double pap = 0;
+    for (int b0 = s0 + threadIdx.x; b0 < s1; b0 += U * B) {
+        int slot[U], row[U];
+        float zr[U], pr[U], ar[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            slot[u] = b0 + u * B;
+            row[u] = slot[u] < s1 ? __ldg(S.k_perm + slot[u]) : -1;
+            zr[u] = pr[u] = ar[u] = 0.f;
+            if (row[u] >= 0) {
+                zr[u] = S.z[row[u]];
+                pr[u] = S.p[row[u]];
+                ar[u] = S.Ap[row[u]];
+            }
+        }
+        float q[U];
+        sell_rows32<U, kRowChunk, I16>(S, slot, row, q);
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (row[u] < 0) continue;
+            const float pn = zr[u] + bf * pr[u];
+            const float apn = q[u] + bf * ar[u];
+            S.p[row[u]] = pn;
+            S.Ap[row[u]] = apn;
+            pap += (double)pn * apn;
+        }
+    }
+    return pap;
+}
+
+// e += alpha p ; r -= alpha Ap ; z = dinv r ; adds r.z and r.r of this thread.
+__device__ __forceinline__ void pass_update(const SysDesc& S, int s0, int s1, float alpha, double& rzn,
+                                            double& rrn)
+{
+    constexpr int U = kRowsPerPass;
+    const int B = blockDim.x;
+    for (int b0 = s0 + threadIdx.x; b0 < s1; b0 += U * B) {
+        int row[U];
+        float ev[U], pv[U], rv[U], av[U], dv[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int sl = b0 + u * B;
+            row[u] = sl < s1 ? __ldg(S.k_perm + sl) : -1;
+            ev[u] = pv[u] = rv[u] = av[u] = dv[u] = 0.f;
+            if (row[u] >= 0) {
+                ev[u] = S.e[row[u]];
+                pv[u] = S.p[row[u]];
+                rv[u] = S.r[row[u]];
+                av[u] = S.Ap[row[u]];
+                dv[u] = S.dinv[row[u]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            if (row[u] < 0) continue;
+            S.e[row[u]] = ev[u] + alpha * pv[u];
+            const float rn = rv[u] - alpha * av[u];
+            const float zn = dv[u] * rn;
+            S.r[row[u]] = rn;
+            S.z[row[u]] = zn;
+            rzn += (double)rn * zn;
+            rrn += (double)rn * rn;
+        }
+    }
 }
 
 __global__ void __launch_bounds__(512, 2) k_batch_heat(BatchParams P)
@@ -243,33 +335,15 @@ __global__ void __launch_bounds__(512, 2) k_batch_heat(BatchParams P)
                 int it = 0;
                 while (sqrt(rr32) > P.inner_rtol && it < P.inner_max) {
                     // p = z + beta p ; Ap = K z + beta Ap ; pAp
-                    double pap = 0, d3 = 0;
+                    double d3 = 0;
                     const float bf = (float)beta;
-                    for (int slot_i = s0 + threadIdx.x; slot_i < s1; slot_i += blockDim.x) {
-                        const int row = S.k_perm[slot_i];
-                        if (row < 0) continue;
-                        const float q = sell_row32(S.k_off, S.k_col, S.k_col16, S.k_v32, S.z, slot_i, row);
-                        const float pn = S.z[row] + bf * S.p[row];
-                        const float apn = q + bf * S.Ap[row];
-                        S.p[row] = pn;
-                        S.Ap[row] = apn;
-                        pap += (double)pn * apn;
-                    }
+                    double pap = S.k_col16 ? pass_direction<true>(S, s0, s1, bf)
+                                           : pass_direction<false>(S, s0, s1, bf);
                     cluster_sum2(cl, pap, d3, sh, slot, parity);
                     const float alpha = (float)(rz / pap);
                     // e += alpha p ; r -= alpha Ap ; z = dinv r
                     double rzn = 0, rrn = 0;
-                    for (int slot_i = s0 + threadIdx.x; slot_i < s1; slot_i += blockDim.x) {
-                        const int row = S.k_perm[slot_i];
-                        if (row < 0) continue;
-                        S.e[row] += alpha * S.p[row];
-                        const float rv = S.r[row] - alpha * S.Ap[row];
-                        const float zv = S.dinv[row] * rv;
-                        S.r[row] = rv;
-                        S.z[row] = zv;
-                        rzn += (double)rv * zv;
-                        rrn += (double)rv * rv;
-                    }
+                    pass_update(S, s0, s1, alpha, rzn, rrn);
                     cluster_sum2(cl, rzn, rrn, sh, slot, parity);
                     beta = rzn / rz;
                     rz = rzn;
