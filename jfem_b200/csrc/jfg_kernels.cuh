@@ -186,12 +186,82 @@ struct SpmvArgs {
 // gather latency); TPR = 4..8 on small levels, where the row loop would
 // otherwise be a chain of dependent gathers per thread.  No shared memory,
 // no barriers.
-template <typename VT, typename XT, int NR, int TPR, class Epi, class Fin, bool IDX16 = false>
+// Prefetching variant of the row loop (k_spmv with PF): the slot's header
+// and its first chunk of matrix entries are loaded before the wait for the
+// preceding kernel (programmatic dependent launch), so on small levels that
+// dependent chain of loads overlaps the predecessor's tail.  Only for
+// matrices that no kernel of the stream writes after set-up (the levels of a
+// multigrid hierarchy).  Same entry order and shuffle tree as k_spmv, so the
+// same bits.
+template <typename VT, typename XT, int NR, int TPR, class Epi, class Fin, bool IDX16>
+__device__ __forceinline__ void spmv_prefetched(const SpmvArgs& m, const VT* __restrict__ val,
+                                                const XT* __restrict__ x, const Epi& epi,
+                                                const GridRed<NR, Fin>& red, const int* __restrict__ done)
+{
+    using AT = typename AccOf<VT>::T;
+    constexpr int tpr = TPR;
+    constexpr int U = (IDX16 && TPR == 1) ? 8 : 4;
+    constexpr int st = 32 * tpr;
+    const int gid = blockIdx.x * kThreads + threadIdx.x;
+    const int slot = gid / TPR;
+    const int sub = gid % TPR;
+    int o = 0, len = 0, r = -1;
+    if (slot < m.nslots) {
+        const int s = slot >> 5;
+        const int a = __ldg(m.off + s);
+        o = a + (slot & 31);
+        len = (__ldg(m.off + s + 1) - a) >> 5;
+        r = __ldg(m.perm + slot);
+    }
+    const int base = r < 0 ? 0 : r;
+    int c[U];
+    AT v[U];
+    auto load_chunk = [&](int k) {
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const bool ok = k + u * tpr < len;
+            const int idx = o + 32 * k + u * st;
+            if constexpr (IDX16)
+                c[u] = ok ? base + ld_stream(m.col16 + idx) : base;
+            else
+                c[u] = ok ? ld_stream(m.col + idx) : 0;
+            v[u] = ok ? to_acc(ld_stream(val + idx)) : (AT)0;
+        }
+    };
+    load_chunk(sub);
+    pdl_wait();
+    if (done && *done) return;
+    double acc[NR > 0 ? NR : 1];
+#pragma unroll
+    for (int i = 0; i < (NR > 0 ? NR : 1); i++) acc[i] = 0;
+    AT sum = 0;
+    for (int k = sub; k < len; k += U * tpr) {
+        if (k != sub) load_chunk(k);
+        AT xv[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) xv[u] = k + u * tpr < len ? (AT)__ldg(x + c[u]) : (AT)0;
+#pragma unroll
+        for (int u = 0; u < U; u++)
+            if (k + u * tpr < len) sum += v[u] * xv[u];
+    }
+    for (int q = tpr >> 1; q > 0; q >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, q);
+    if constexpr (std::is_same<VT, __half>::value) sum *= m.vscale;
+    if (sub == 0 && r >= 0) epi(r, sum, acc);
+    pdl_launch_dependents();
+    if constexpr (NR > 0) red.reduce(acc);
+}
+
+// PF: use spmv_prefetched (matrices fixed after set-up only).
+template <typename VT, typename XT, int NR, int TPR, class Epi, class Fin, bool IDX16 = false, bool PF = false>
 __global__ void __launch_bounds__(kThreads)
 k_spmv(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi, GridRed<NR, Fin> red,
        const int* __restrict__ done)
 {
     using AT = typename AccOf<VT>::T;
+    if constexpr (PF) {
+        spmv_prefetched<VT, XT, NR, TPR, Epi, Fin, IDX16>(m, val, x, epi, red, done);
+        return;
+    }
     pdl_wait();
     if (done && *done) return;
     double acc[NR > 0 ? NR : 1];

@@ -517,17 +517,18 @@ template <typename T, int NR, class Epi, class Fin = NoFin>
 static void mg_spmv(const MGImpl<T>& g, cudaStream_t st, const Matrix* M, const T* x, Epi epi, const Scratch& sc,
                     const int* done, Fin fin = Fin())
 {
+    // the hierarchy's matrices are fixed after init: prefetched before the PDL wait
     if constexpr (std::is_same<T, float>::value) {
         if (g.vbf16) {
-            spmv_launch<__nv_bfloat16, float, NR>(st, M, M->val16.p, x, epi, sc, done, fin);
+            spmv_launch<__nv_bfloat16, float, NR, Epi, Fin, true>(st, M, M->val16.p, x, epi, sc, done, fin);
             return;
         }
         if (g.vfp16) {
-            spmv_launch<__half, float, NR>(st, M, M->valh.p, x, epi, sc, done, fin);
+            spmv_launch<__half, float, NR, Epi, Fin, true>(st, M, M->valh.p, x, epi, sc, done, fin);
             return;
         }
     }
-    spmv_launch<T, T, NR>(st, M, vals_of<T>(M), x, epi, sc, done, fin);
+    spmv_launch<T, T, NR, Epi, Fin, true>(st, M, vals_of<T>(M), x, epi, sc, done, fin);
 }
 
 template <typename T>

@@ -117,7 +117,9 @@ void launch_ex(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaS
 
 int sm_count();
 
-template <typename VT, typename XT, int NR, class Epi, class Fin = NoFin>
+// PF: prefetch the matrix before the PDL wait (see k_spmv); only for
+// matrices that are not written after set-up.
+template <typename VT, typename XT, int NR, class Epi, class Fin = NoFin, bool PF = false>
 void spmv_launch(cudaStream_t st, const Matrix* M, const VT* val, const XT* x, Epi epi, const Scratch& sc,
                  const int* done, Fin fin = Fin())
 {
@@ -128,16 +130,16 @@ void spmv_launch(cudaStream_t st, const Matrix* M, const VT* val, const XT* x, E
     const dim3 g(M->nblocks), b(kThreads);
     if (M->idx16) {
         switch (M->tpr_log2) {
-        case 0: launch_ex(k_spmv<VT, XT, NR, 1, Epi, Fin, true>, g, b, 0, st, a, val, x, epi, red, done); break;
-        case 2: launch_ex(k_spmv<VT, XT, NR, 4, Epi, Fin, true>, g, b, 0, st, a, val, x, epi, red, done); break;
-        default: launch_ex(k_spmv<VT, XT, NR, 8, Epi, Fin, true>, g, b, 0, st, a, val, x, epi, red, done); break;
+        case 0: launch_ex(k_spmv<VT, XT, NR, 1, Epi, Fin, true, false>, g, b, 0, st, a, val, x, epi, red, done); break;
+        case 2: launch_ex(k_spmv<VT, XT, NR, 4, Epi, Fin, true, PF>, g, b, 0, st, a, val, x, epi, red, done); break;
+        default: launch_ex(k_spmv<VT, XT, NR, 8, Epi, Fin, true, PF>, g, b, 0, st, a, val, x, epi, red, done); break;
         }
         return;
     }
     switch (M->tpr_log2) {
-    case 0: launch_ex(k_spmv<VT, XT, NR, 1, Epi, Fin>, g, b, 0, st, a, val, x, epi, red, done); break;
-    case 2: launch_ex(k_spmv<VT, XT, NR, 4, Epi, Fin>, g, b, 0, st, a, val, x, epi, red, done); break;
-    default: launch_ex(k_spmv<VT, XT, NR, 8, Epi, Fin>, g, b, 0, st, a, val, x, epi, red, done); break;
+    case 0: launch_ex(k_spmv<VT, XT, NR, 1, Epi, Fin, false, false>, g, b, 0, st, a, val, x, epi, red, done); break;
+    case 2: launch_ex(k_spmv<VT, XT, NR, 4, Epi, Fin, false, PF>, g, b, 0, st, a, val, x, epi, red, done); break;
+    default: launch_ex(k_spmv<VT, XT, NR, 8, Epi, Fin, false, PF>, g, b, 0, st, a, val, x, epi, red, done); break;
     }
 }
 
