@@ -330,6 +330,102 @@ k_spmv(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi
 }
 
 // ---------------------------------------------------------------------------
+// SELL SpMV with the matrix stream staged through shared memory (large levels)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc)
+{
+    asm volatile("cp.async.cg.shared.global.L2::256B [%0], [%1], 16;" ::"r"(smem_u32(sdst)), "l"(gsrc)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// One thread per row, 16-bit columns.  A warp owns one 32-row slice, whose
+// entries k..k+U-1 lie contiguously in the SELL arrays.  The warp keeps NS
+// such chunks of values and columns in flight into its shared-memory stages
+// with asynchronous 16-byte copies (no registers held while they are in
+// flight) while its lanes gather x for the current chunk, so the matrix
+// stream stays busy during the gather latency instead of alternating with
+// it.  Sums in entry order: the same bits as k_spmv.
+template <typename VT, typename XT, int NR, int U, int NS, class Epi, class Fin>
+__global__ void __launch_bounds__(kThreads)
+k_spmv_pipe(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi, GridRed<NR, Fin> red,
+            const int* __restrict__ done)
+{
+    using AT = typename AccOf<VT>::T;
+    constexpr int W = kThreads / 32;
+    constexpr int SV = U * 32;                 // entries of one stage
+    static_assert((SV * sizeof(VT)) % 16 == 0 && (SV * 2) % 16 == 0, "stage not a multiple of 16 bytes");
+    __shared__ __align__(16) VT s_val[W][NS][SV];
+    __shared__ __align__(16) int16_t s_col[W][NS][SV];
+    pdl_wait();
+    if (done && *done) return;
+    double acc[NR > 0 ? NR : 1];
+#pragma unroll
+    for (int i = 0; i < (NR > 0 ? NR : 1); i++) acc[i] = 0;
+    const int gid = blockIdx.x * kThreads + threadIdx.x;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    AT sum = 0;
+    int r = -1;
+    if (gid < m.nslots) {                      // warp-uniform: nslots is a multiple of 32
+        const int s = gid >> 5;
+        const int o = __ldg(m.off + s);
+        const int len = (__ldg(m.off + s + 1) - o) >> 5;
+        r = __ldg(m.perm + gid);
+        const int base = r < 0 ? 0 : r;
+        const int nch = (len + U - 1) / U;
+        // chunk j = entries [jU, jU + cnt) of the slice: [o + 32 jU, o + 32 (jU + cnt)); o is
+        // a multiple of 32, so every copy starts on a 16-byte boundary
+        auto issue = [&](int j) {
+            const int k = j * U, stg = j % NS;
+            const int cnt = min(U, len - k);
+            const char* vs = reinterpret_cast<const char*>(val + o + 32 * k);
+            char* vd = reinterpret_cast<char*>(&s_val[w][stg][0]);
+            const int nv = cnt * 32 * (int)sizeof(VT) / 16;
+            for (int i = lane; i < nv; i += 32) cp_async16(vd + 16 * i, vs + 16 * i);
+            const char* cs = reinterpret_cast<const char*>(m.col16 + o + 32 * k);
+            char* cd = reinterpret_cast<char*>(&s_col[w][stg][0]);
+            const int nc = cnt * 64 / 16;
+            for (int i = lane; i < nc; i += 32) cp_async16(cd + 16 * i, cs + 16 * i);
+        };
+#pragma unroll
+        for (int j = 0; j < NS - 1; j++) {
+            if (j < nch) issue(j);
+            cp_async_commit();                 // one group per chunk slot (empty past the end)
+        }
+        for (int j = 0; j < nch; j++) {
+            if (j + NS - 1 < nch) issue(j + NS - 1);
+            cp_async_commit();
+            cp_async_wait<NS - 1>();           // chunk j has landed
+            __syncwarp();
+            const int stg = j % NS, cnt = min(U, len - j * U);
+            int c[U];
+            AT v[U], xv[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const bool ok = u < cnt;
+                c[u] = ok ? base + (int)s_col[w][stg][32 * u + lane] : base;
+                v[u] = ok ? to_acc(s_val[w][stg][32 * u + lane]) : (AT)0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) xv[u] = u < cnt ? (AT)__ldg(x + c[u]) : (AT)0;
+#pragma unroll
+            for (int u = 0; u < U; u++)
+                if (u < cnt) sum += v[u] * xv[u];
+            __syncwarp();                      // the stage is refilled NS - 1 chunks later
+        }
+    }
+    if constexpr (std::is_same<VT, __half>::value) sum *= m.vscale;
+    if (r >= 0) epi(r, sum, acc);
+    pdl_launch_dependents();
+    if constexpr (NR > 0) red.reduce(acc);
+}
+
+// ---------------------------------------------------------------------------
 // grid-stride vector kernels: f(i, acc) per index, optional reduction
 // ---------------------------------------------------------------------------
 template <int NR, class F, class Fin>

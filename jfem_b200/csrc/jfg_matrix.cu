@@ -24,6 +24,16 @@ bool use_pdl()
     return v == 1;
 }
 
+bool spmv_pipe()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("JFEM_SPMV_PIPE");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v == 1;
+}
+
 int sm_count()
 {
     static int n = 0;

@@ -116,6 +116,15 @@ void launch_ex(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaS
 }
 
 int sm_count();
+// One-thread-per-row SpMVs with 16-bit columns use k_spmv_pipe (shared-memory
+// stages) unless the environment variable JFEM_SPMV_PIPE=0 selects the
+// register-only k_spmv.
+bool spmv_pipe();
+// k_spmv_pipe stage shape (measured on the Q2 512^2 level matrices): values of
+// at most 4 bytes take chunks of 4 entries, FP64 values chunks of 2 entries;
+// two stages.
+constexpr int kPipeU32 = 4, kPipeS32 = 2;
+constexpr int kPipeU64 = 2, kPipeS64 = 2;
 
 // PF: prefetch the matrix before the PDL wait (see k_spmv); only for
 // matrices that are not written after set-up.
@@ -130,7 +139,15 @@ void spmv_launch(cudaStream_t st, const Matrix* M, const VT* val, const XT* x, E
     const dim3 g(M->nblocks), b(kThreads);
     if (M->idx16) {
         switch (M->tpr_log2) {
-        case 0: launch_ex(k_spmv<VT, XT, NR, 1, Epi, Fin, true, false>, g, b, 0, st, a, val, x, epi, red, done); break;
+        case 0:
+            if (spmv_pipe()) {
+                constexpr int kU = sizeof(VT) <= 4 ? kPipeU32 : kPipeU64;
+                constexpr int kS = sizeof(VT) <= 4 ? kPipeS32 : kPipeS64;
+                launch_ex(k_spmv_pipe<VT, XT, NR, kU, kS, Epi, Fin>, g, b, 0, st, a, val, x, epi, red, done);
+                break;
+            }
+            launch_ex(k_spmv<VT, XT, NR, 1, Epi, Fin, true, false>, g, b, 0, st, a, val, x, epi, red, done);
+            break;
         case 2: launch_ex(k_spmv<VT, XT, NR, 4, Epi, Fin, true, PF>, g, b, 0, st, a, val, x, epi, red, done); break;
         default: launch_ex(k_spmv<VT, XT, NR, 8, Epi, Fin, true, PF>, g, b, 0, st, a, val, x, epi, red, done); break;
         }
