@@ -51,3 +51,23 @@ def test_start_vectors():
     assert s._start(3, zero=True).tolist() == [0, 0, 0]
     s.lastSolution = np.arange(3.0)
     assert s._start(3).tolist() == [0, 1, 2]      # warm start
+
+
+def test_block_sparse_matrix_partition_and_checks():
+    """BlockSparseMatrix: the partition comes from the diagonal blocks; blocks
+    off the partition or of the wrong shape are rejected (no device needed)."""
+    import numpy as np
+    import pytest
+    from jfem_b200.linalg import IllegalArgumentException
+    from jfem_b200.schur import BlockSparseMatrix
+    blocks = {(0, 0): np.eye(4), (4, 4): 2 * np.eye(3), (0, 4): np.ones((4, 3)), (4, 0): np.ones((3, 4))}
+    B = BlockSparseMatrix(blocks, 7)
+    assert list(B.getBlockStarts()) == [0, 4] and list(B.getBlockEnds()) == [4, 7]
+    parts = BlockSparseMatrix.partitionVector(np.arange(7.0), B.getBlockStarts(), B.getBlockEnds())
+    assert [list(p) for p in parts] == [[0, 1, 2, 3], [4, 5, 6]]
+    with pytest.raises(IllegalArgumentException):
+        BlockSparseMatrix({(0, 0): np.eye(4), (4, 4): np.eye(2)}, 7)
+    with pytest.raises(IllegalArgumentException):
+        BlockSparseMatrix({(0, 0): np.eye(4), (4, 4): np.eye(3), (0, 4): np.ones((4, 2))}, 7)
+    with pytest.raises(IllegalArgumentException):
+        BlockSparseMatrix({(0, 0): np.eye(4), (4, 4): np.eye(3), (0, 2): np.ones((4, 3))}, 7)
