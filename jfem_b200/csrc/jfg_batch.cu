@@ -130,7 +130,7 @@ __device__ __forceinline__ double sell_row(const int* off, const int* col, const
 // has several rows' gathers in flight instead of one dependent chain per row.
 // Row sums keep the entry order and partial dot products the row order of the
 // one-row-at-a-time loop, so the results are the same bits.
-constexpr int kRowsPerPass = 4;
+constexpr int kRowsPerPass = 3;
 constexpr int kRowChunk = 3;     // entries of each row loaded together
 
 template <int U, int CH, bool I16>
