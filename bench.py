@@ -754,7 +754,7 @@ def run_batch_heat(args):
                                    "systems": 256, "dofs": dofs, "nnz": nnz},
             "kernel_ms": last.ms, "total_inner_iterations": last.total_inner_iterations,
             "max_rel_residual": last.max_rel_residual, "failed": last.failed,
-            "cluster": last.cluster, "threads": last.threads, "clocks": clk.summary(), "cpu_baseline": cpu}
+            "cluster": last.cluster, "threads": last.threads, "rows_per_thread": last.rows_per_thread, "clocks": clk.summary(), "cpu_baseline": cpu}
     print(json.dumps(line))
 
 

@@ -355,6 +355,7 @@ typedef struct {
     double inner_rtol;  /* FP32 inner PCG relative tolerance (default 1e-5) */
     int inner_max;      /* inner iteration cap (default 500) */
     int max_refine;     /* refinement steps per time step (default 6) */
+    int rows_per_thread; /* rows of a thread in flight per inner pass (2, 3, 4); 0 = autotuned */
 } jfg_batch_opts;
 typedef struct {
     int total_inner_iterations;
@@ -363,6 +364,7 @@ typedef struct {
     int failed;                /* systems that missed rtol within max_refine */
     int cluster, threads;      /* configuration used */
     double ms;                 /* device time of the persistent launch */
+    int rows_per_thread;       /* configuration used */
 } jfg_batch_info;
 void jfg_batch_opts_default(jfg_batch_opts* o);
 /* K[s], M[s]: square matrices of the same size n_s; f (optional) packed

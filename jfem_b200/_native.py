@@ -79,13 +79,13 @@ class SolveInfo(C.Structure):
 
 class BatchOpts(C.Structure):
     _fields_ = [("cluster", C.c_int), ("threads", C.c_int), ("rtol", C.c_double), ("inner_rtol", C.c_double),
-                ("inner_max", C.c_int), ("max_refine", C.c_int)]
+                ("inner_max", C.c_int), ("max_refine", C.c_int), ("rows_per_thread", C.c_int)]
 
 
 class BatchInfo(C.Structure):
     _fields_ = [("total_inner_iterations", C.c_int), ("max_refine_used", C.c_int),
                 ("max_rel_residual", C.c_double), ("failed", C.c_int), ("cluster", C.c_int),
-                ("threads", C.c_int), ("ms", C.c_double)]
+                ("threads", C.c_int), ("ms", C.c_double), ("rows_per_thread", C.c_int)]
 
 
 class JfgError(RuntimeError):

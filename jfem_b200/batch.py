@@ -26,6 +26,7 @@ class BatchResult:
         self.failed = info.failed
         self.cluster = info.cluster
         self.threads = info.threads
+        self.rows_per_thread = info.rows_per_thread
         self.ms = info.ms
 
 
@@ -61,7 +62,7 @@ class BatchedParabolicIntegrator:
         return [packed[self.offsets[s]:self.offsets[s + 1]] for s in range(len(self._K))]
 
     def timeSteps(self, u0, steps, f=None, cluster=0, threads=0, rtol=1e-10, inner_rtol=1e-5, inner_max=500,
-                  max_refine=6):
+                  max_refine=6, rows_per_thread=0):
         """Advance every system `steps` steps; u0 / f: lists of vectors or packed arrays."""
         u = N.f64(u0 if isinstance(u0, np.ndarray) else self.pack(u0)).copy()
         if u.shape != (self.total,):
@@ -73,7 +74,7 @@ class BatchedParabolicIntegrator:
                 raise IllegalArgumentException("packed source has the wrong length")
         o = N.BatchOpts()
         N.load().jfg_batch_opts_default(C.byref(o))
-        o.cluster, o.threads = cluster, threads
+        o.cluster, o.threads, o.rows_per_thread = cluster, threads, rows_per_thread
         o.rtol, o.inner_rtol, o.inner_max, o.max_refine = rtol, inner_rtol, inner_max, max_refine
         info = N.BatchInfo()
         st = N.load().jfg_batch_heat(self._h, int(steps), N.dptr(fp) if fp is not None else None, N.dptr(u),

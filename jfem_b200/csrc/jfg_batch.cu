@@ -124,13 +124,12 @@ __device__ __forceinline__ double sell_row(const int* off, const int* col, const
     for (int k = 0; k < len; k++) sum += (double)val[o + 32 * k + lane] * (double)x[col[o + 32 * k + lane]];
     return sum;
 }
-// The two passes of an inner PCG iteration take kRowsPerPass rows of a thread
+// The two passes of an inner PCG iteration take U rows of a thread
 // at once (slots t, t + B, t + 2B, ... as in a plain strided loop): all loads
 // of those rows are issued before any of their results is used, so a thread
 // has several rows' gathers in flight instead of one dependent chain per row.
 // Row sums keep the entry order and partial dot products the row order of the
 // one-row-at-a-time loop, so the results are the same bits.
-constexpr int kRowsPerPass = 3;
 constexpr int kRowChunk = 3;     // entries of each row loaded together
 
 template <int U, int CH, bool I16>
@@ -183,10 +182,9 @@ __device__ __forceinline__ void sell_rows32(const SysDesc& S, const int (&slot)[
 }
 
 // p = z + beta p ; Ap = K z + beta Ap ; returns this thread's part of p.Ap.
-template <bool I16>
+template <int U, bool I16>
 __device__ __forceinline__ double pass_direction(const SysDesc& S, int s0, int s1, float bf)
 {
-    constexpr int U = kRowsPerPass;
     const int B = blockDim.x;
     double pap = 0;
     for (int b0 = s0 + threadIdx.x; b0 < s1; b0 += U * B) {
@@ -219,10 +217,10 @@ __device__ __forceinline__ double pass_direction(const SysDesc& S, int s0, int s
 }
 
 // e += alpha p ; r -= alpha Ap ; z = dinv r ; adds r.z and r.r of this thread.
+template <int U>
 __device__ __forceinline__ void pass_update(const SysDesc& S, int s0, int s1, float alpha, double& rzn,
                                             double& rrn)
 {
-    constexpr int U = kRowsPerPass;
     const int B = blockDim.x;
     for (int b0 = s0 + threadIdx.x; b0 < s1; b0 += U * B) {
         int row[U];
@@ -254,6 +252,8 @@ __device__ __forceinline__ void pass_update(const SysDesc& S, int s0, int s1, fl
     }
 }
 
+// U: rows of a thread in flight per pass (2, 3 or 4; picked by the autotuner)
+template <int U>
 __global__ void __launch_bounds__(512, 2) k_batch_heat(BatchParams P)
 {
     cg::cluster_group cl = cg::this_cluster();
@@ -337,13 +337,13 @@ __global__ void __launch_bounds__(512, 2) k_batch_heat(BatchParams P)
                     // p = z + beta p ; Ap = K z + beta Ap ; pAp
                     double d3 = 0;
                     const float bf = (float)beta;
-                    double pap = S.k_col16 ? pass_direction<true>(S, s0, s1, bf)
-                                           : pass_direction<false>(S, s0, s1, bf);
+                    double pap = S.k_col16 ? pass_direction<U, true>(S, s0, s1, bf)
+                                           : pass_direction<U, false>(S, s0, s1, bf);
                     cluster_sum2(cl, pap, d3, sh, slot, parity);
                     const float alpha = (float)(rz / pap);
                     // e += alpha p ; r -= alpha Ap ; z = dinv r
                     double rzn = 0, rrn = 0;
-                    pass_update(S, s0, s1, alpha, rzn, rrn);
+                    pass_update<U>(S, s0, s1, alpha, rzn, rrn);
                     cluster_sum2(cl, rzn, rrn, sh, slot, parity);
                     beta = rzn / rz;
                     rz = rzn;
@@ -396,7 +396,7 @@ struct jfg_batch {
     jfg::DevBuf<int> d_order, iters, refines, status;
     jfg::DevBuf<double> relres;
     jfg::DevBuf<unsigned> queue;
-    int tuned_cluster = 0, tuned_threads = 0;
+    int tuned_cluster = 0, tuned_threads = 0, tuned_rows = 0;
 };
 
 namespace {
@@ -438,8 +438,9 @@ void build_desc(jfg_batch* b, bool with_f)
 }
 
 // One persistent launch with cluster size C and T threads per CTA.
-float launch(jfg_batch* b, int C, int T, int steps, const jfg_batch_opts& o)
+float launch(jfg_batch* b, int C, int T, int U, int steps, const jfg_batch_opts& o)
 {
+    void (*kern)(BatchParams) = U == 2 ? k_batch_heat<2> : (U == 4 ? k_batch_heat<4> : k_batch_heat<3>);
     cudaStream_t st = jfg::ctx_stream(b->ctx);
     BatchParams P;
     P.sys = b->desc.p;
@@ -468,7 +469,7 @@ float launch(jfg_batch* b, int C, int T, int steps, const jfg_batch_opts& o)
     cfg.numAttrs = 1;
     int max_clusters = 0;
     cfg.gridDim = dim3(C);
-    JFG_CUDA(cudaOccupancyMaxActiveClusters(&max_clusters, k_batch_heat, &cfg));
+    JFG_CUDA(cudaOccupancyMaxActiveClusters(&max_clusters, kern, &cfg));
     if (max_clusters < 1) max_clusters = 1;
     int nclusters = std::min(max_clusters, b->nsys);
     cfg.gridDim = dim3(nclusters * C);
@@ -476,7 +477,7 @@ float launch(jfg_batch* b, int C, int T, int steps, const jfg_batch_opts& o)
     JFG_CUDA(cudaEventCreate(&e0));
     JFG_CUDA(cudaEventCreate(&e1));
     JFG_CUDA(cudaEventRecord(e0, st));
-    JFG_CUDA(cudaLaunchKernelEx(&cfg, k_batch_heat, P));
+    JFG_CUDA(cudaLaunchKernelEx(&cfg, kern, P));
     jfg::note_launch();
     JFG_CUDA(cudaEventRecord(e1, st));
     JFG_CUDA(cudaEventSynchronize(e1));
@@ -588,6 +589,8 @@ int jfg_batch_heat(jfg_batch* b, int steps, const double* h_f, double* h_u, cons
                   JFG_ERR_BAD_ARG, "cluster must be 1, 2, 4 or 8");
         JFG_CHECK(o.threads == 0 || o.threads == 256 || o.threads == 512, JFG_ERR_BAD_ARG,
                   "threads must be 256 or 512");
+        JFG_CHECK(o.rows_per_thread == 0 || (o.rows_per_thread >= 2 && o.rows_per_thread <= 4), JFG_ERR_BAD_ARG,
+                  "rows_per_thread must be 2, 3 or 4");
         JFG_CHECK(o.rtol > 0 && o.inner_rtol > 0 && o.inner_max > 0 && o.max_refine >= 0, JFG_ERR_BAD_ARG,
                   "bad tolerances or caps");
         cudaStream_t st = jfg::ctx_stream(b->ctx);
@@ -597,28 +600,32 @@ int jfg_batch_heat(jfg_batch* b, int steps, const double* h_f, double* h_u, cons
             JFG_CUDA(cudaMemcpyAsync(b->f.p, h_f, sizeof(double) * tot, cudaMemcpyHostToDevice, st));
         }
         build_desc(b, h_f != nullptr);
-        int C = o.cluster, T = o.threads;
-        if (C == 0 || T == 0) {
-            // autotune once: one step of every configuration from the given states
+        int C = o.cluster, T = o.threads, U = o.rows_per_thread;
+        if (C == 0 || T == 0 || U == 0) {
+            // autotune once: one step of every configuration (cluster size x
+            // threads per CTA x rows per thread in flight) from the given states
             if (!b->tuned_cluster) {
-                JFG_CUDA(cudaMemcpyAsync(b->pool64.p, h_u, sizeof(double) * tot, cudaMemcpyHostToDevice, st));
                 float best = 1e30f;
                 for (int c : {1, 2, 4, 8})
-                    for (int t : {256, 512}) {
-                        JFG_CUDA(cudaMemcpyAsync(b->pool64.p, h_u, sizeof(double) * tot, cudaMemcpyHostToDevice, st));
-                        float ms = launch(b, c, t, 1, o);
-                        if (ms < best) {
-                            best = ms;
-                            b->tuned_cluster = c;
-                            b->tuned_threads = t;
+                    for (int t : {256, 512})
+                        for (int u : {2, 3, 4}) {
+                            JFG_CUDA(cudaMemcpyAsync(b->pool64.p, h_u, sizeof(double) * tot, cudaMemcpyHostToDevice,
+                                                     st));
+                            float ms = launch(b, c, t, u, 1, o);
+                            if (ms < best) {
+                                best = ms;
+                                b->tuned_cluster = c;
+                                b->tuned_threads = t;
+                                b->tuned_rows = u;
+                            }
                         }
-                    }
             }
             if (C == 0) C = b->tuned_cluster;
             if (T == 0) T = b->tuned_threads;
+            if (U == 0) U = b->tuned_rows;
         }
         JFG_CUDA(cudaMemcpyAsync(b->pool64.p, h_u, sizeof(double) * tot, cudaMemcpyHostToDevice, st));
-        float ms = launch(b, C, T, steps, o);
+        float ms = launch(b, C, T, U, steps, o);
         JFG_CUDA(cudaMemcpyAsync(h_u, b->pool64.p, sizeof(double) * tot, cudaMemcpyDeviceToHost, st));
         std::vector<int> it(b->nsys), rf(b->nsys), stt(b->nsys);
         std::vector<double> rr(b->nsys);
@@ -641,6 +648,7 @@ int jfg_batch_heat(jfg_batch* b, int steps, const double* h_f, double* h_u, cons
         inf.failed = failed;
         inf.cluster = C;
         inf.threads = T;
+        inf.rows_per_thread = U;
         inf.ms = ms;
         if (info) *info = inf;
         return worst;

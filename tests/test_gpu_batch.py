@@ -28,15 +28,15 @@ def oracle_steps(s, steps):
     return u
 
 
-@pytest.mark.parametrize("cluster,threads", [(1, 256), (2, 512), (4, 256), (8, 512)])
-def test_batch_matches_oracle(ctx, cluster, threads):
+@pytest.mark.parametrize("cluster,threads,rows", [(1, 256, 2), (2, 512, 3), (4, 256, 4), (8, 512, 3)])
+def test_batch_matches_oracle(ctx, cluster, threads, rows):
     batch = problems.heat_batch(nsys=7, sizes=(4, 8, 12, 16, 24), dt=1e-3, seed=5)
     B = build(ctx, batch)
     steps = 4
-    u = B.timeSteps([s.u0 for s in batch], steps, cluster=cluster, threads=threads)
+    u = B.timeSteps([s.u0 for s in batch], steps, cluster=cluster, threads=threads, rows_per_thread=rows)
     assert B.last.status == 0 and B.last.failed == 0
     assert B.last.max_rel_residual <= 1e-10
-    assert (B.last.cluster, B.last.threads) == (cluster, threads)
+    assert (B.last.cluster, B.last.threads, B.last.rows_per_thread) == (cluster, threads, rows)
     for s, us in zip(batch, B.unpack(u)):
         ref = oracle_steps(s, steps)
         assert np.linalg.norm(us - ref) / np.linalg.norm(ref) < 1e-8
@@ -47,6 +47,9 @@ def test_batch_autotune_and_uneven_sizes(ctx):
     B = build(ctx, batch)
     u = B.timeSteps([s.u0 for s in batch], 3)
     assert B.last.failed == 0 and B.last.cluster in (1, 2, 4, 8) and B.last.threads in (256, 512)
+    assert B.last.rows_per_thread in (2, 3, 4)
+    with pytest.raises(Exception, match="rows_per_thread"):
+        B.timeSteps([s.u0 for s in batch], 1, rows_per_thread=5)
     for s, us in zip(batch[:4], B.unpack(u)[:4]):
         ref = oracle_steps(s, 3)
         assert np.linalg.norm(us - ref) / np.linalg.norm(ref) < 1e-8
