@@ -405,17 +405,29 @@ k_spmv_pipe(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Ep
             const int stg = j % NS, cnt = min(U, len - j * U);
             int c[U];
             AT v[U], xv[U];
+            if (cnt == U) {                    // full chunk (warp-uniform): no per-entry predicates
 #pragma unroll
-            for (int u = 0; u < U; u++) {
-                const bool ok = u < cnt;
-                c[u] = ok ? base + (int)s_col[w][stg][32 * u + lane] : base;
-                v[u] = ok ? to_acc(s_val[w][stg][32 * u + lane]) : (AT)0;
+                for (int u = 0; u < U; u++) {
+                    c[u] = base + (int)s_col[w][stg][32 * u + lane];
+                    v[u] = to_acc(s_val[w][stg][32 * u + lane]);
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++) xv[u] = (AT)__ldg(x + c[u]);
+#pragma unroll
+                for (int u = 0; u < U; u++) sum += v[u] * xv[u];
+            } else {
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const bool ok = u < cnt;
+                    c[u] = ok ? base + (int)s_col[w][stg][32 * u + lane] : base;
+                    v[u] = ok ? to_acc(s_val[w][stg][32 * u + lane]) : (AT)0;
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++) xv[u] = u < cnt ? (AT)__ldg(x + c[u]) : (AT)0;
+#pragma unroll
+                for (int u = 0; u < U; u++)
+                    if (u < cnt) sum += v[u] * xv[u];
             }
-#pragma unroll
-            for (int u = 0; u < U; u++) xv[u] = u < cnt ? (AT)__ldg(x + c[u]) : (AT)0;
-#pragma unroll
-            for (int u = 0; u < U; u++)
-                if (u < cnt) sum += v[u] * xv[u];
             __syncwarp();                      // the stage is refilled NS - 1 chunks later
         }
     }
