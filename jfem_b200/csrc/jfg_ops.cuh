@@ -120,11 +120,11 @@ int sm_count();
 // stages) unless the environment variable JFEM_SPMV_PIPE=0 selects the
 // register-only k_spmv.
 bool spmv_pipe();
-// k_spmv_pipe stage shape (measured on the Q2 512^2 level matrices): values of
-// at most 4 bytes take chunks of 4 entries, FP64 values chunks of 2 entries;
-// two stages.
-constexpr int kPipeU32 = 4, kPipeS32 = 2;
-constexpr int kPipeU64 = 2, kPipeS64 = 2;
+// k_spmv_pipe stage shape (measured on the Q2 512^2 level matrices): chunks of
+// 8 entries for 2-byte values, 4 entries for FP32 and FP64 values; two stages.
+template <typename VT>
+constexpr int pipe_chunk() { return sizeof(VT) <= 2 ? 8 : 4; }
+constexpr int kPipeStages = 2;
 
 // PF: prefetch the matrix before the PDL wait (see k_spmv); only for
 // matrices that are not written after set-up.
@@ -141,9 +141,8 @@ void spmv_launch(cudaStream_t st, const Matrix* M, const VT* val, const XT* x, E
         switch (M->tpr_log2) {
         case 0:
             if (spmv_pipe()) {
-                constexpr int kU = sizeof(VT) <= 4 ? kPipeU32 : kPipeU64;
-                constexpr int kS = sizeof(VT) <= 4 ? kPipeS32 : kPipeS64;
-                launch_ex(k_spmv_pipe<VT, XT, NR, kU, kS, Epi, Fin>, g, b, 0, st, a, val, x, epi, red, done);
+                launch_ex(k_spmv_pipe<VT, XT, NR, pipe_chunk<VT>(), kPipeStages, Epi, Fin>, g, b, 0, st, a, val, x,
+                          epi, red, done);
                 break;
             }
             launch_ex(k_spmv<VT, XT, NR, 1, Epi, Fin, true, false>, g, b, 0, st, a, val, x, epi, red, done);
