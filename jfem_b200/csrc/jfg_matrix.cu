@@ -237,9 +237,12 @@ static Matrix* build_from_sorted(Context* c, int rows, int cols, int64_t m, cons
     off[nslices] = (int)total;
     M->nslices = nslices;
     M->sell_len = total;
-    // threads per row: 1 on large matrices, 4 or 8 on small ones (JFEM_TPR overrides)
+    // threads per row: 1 from 262,144 rows (the staged one-thread-per-row
+    // kernel), 4 from 32,768 rows or with short rows, 8 on small matrices with
+    // rows of 10 or more entries (measured on the Q2 multigrid levels;
+    // JFEM_TPR overrides)
     double avg = rows ? (double)m / rows : 0.0;
-    int tl = rows >= 262144 ? 0 : (avg >= 10.0 ? 3 : 2);
+    int tl = rows >= 262144 ? 0 : (avg >= 10.0 ? (rows >= 32768 ? 2 : 3) : 2);
     if (const char* e = getenv("JFEM_TPR")) {
         int v = atoi(e);
         tl = v <= 0 ? 0 : (v <= 2 ? 2 : 3);   // the SpMV is instantiated for 1, 4 and 8 threads per row
