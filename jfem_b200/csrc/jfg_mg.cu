@@ -541,11 +541,29 @@ void MGImpl<T>::coarse(const T* rhs, T* out, const int* done, cudaStream_t st)
 // Smoother.smooth on level l with rhs; the result ends in x[l].
 template <typename T>
 void MGImpl<T>::smooth(int l, const T* rhs, bool xzero, const Scratch& sc, const int* done, cudaStream_t st,
-                       bool first_sweep_done)
+                       bool first_sweep_done, T* dest)
 {
     const SmootherDesc& d = sm[l];
     Matrix* M = A[l];
     int m = n[l];
+    if (dest && d.kind == JFG_SMOOTH_JACOBI && d.runs >= 1 && !xzero) {
+        // the result goes to dest instead of x[l]: the last sweep writes it there
+        T om = (T)d.omega;
+        T* cur = x[l].p;
+        T* alt = t[l].p;
+        for (int k = 0; k < d.runs; k++) {
+            T* o = (k == d.runs - 1) ? dest : alt;
+            mg_spmv<T, 0>(*this, st, M, cur, EpiJacobi<T>{cur, rhs, dinv[l].p, o, om}, sc, done);
+            alt = cur;
+            cur = o;
+        }
+        return;
+    }
+    if (dest) {
+        smooth(l, rhs, xzero, sc, done, st, first_sweep_done, nullptr);
+        vec_launch<0>(st, m, VCopy<T>{x[l].p, dest}, sc, done);
+        return;
+    }
     if (d.runs <= 0) {
         if (xzero) vec_launch<0>(st, m, VZero<T>{x[l].p}, sc, done);
         return;
@@ -643,8 +661,13 @@ void MGImpl<T>::bottom(bool first_sweep_done, const int* done, cudaStream_t st)
 // rhs given; result in x[l].
 template <typename T>
 void MGImpl<T>::vstep(int l, const T* rhs, bool xzero, const Scratch& sc, const int* done, cudaStream_t st,
-                      bool first_sweep_done)
+                      bool first_sweep_done, T* dest)
 {
+    if (dest && l == 0) {
+        vstep(l, rhs, xzero, sc, done, st, first_sweep_done, nullptr);
+        vec_launch<0>(st, n[0], VCopy<T>{x[0].p, dest}, sc, done);
+        return;
+    }
     if (l == bot && xzero && rhs == b[l].p) {    // the whole bottom of the cycle in one cluster launch
         bottom(first_sweep_done, done, st);
         return;
@@ -666,7 +689,7 @@ void MGImpl<T>::vstep(int l, const T* rhs, bool xzero, const Scratch& sc, const 
     }
     vstep(lc, b[lc].p, true, sc, done, st, fuse_sweep);
     mg_spmv<T, 0>(*this, st, P[lc], x[lc].p, EpiMaskedAdd<T>{mask[l].p, x[l].p}, sc, done);
-    smooth(l, rhs, false, sc, done, st);
+    smooth(l, rhs, false, sc, done, st, false, dest);
 }
 
 // fullVCycleCorrection (MGPreconditionerInterface.java:307-326); result in x[L-1].
@@ -708,13 +731,14 @@ void MGImpl<T>::apply(const T* v, T* out, const Scratch& sc, const int* done, cu
         for (int cyc = 0; cyc < cycles; cyc++) coarse(defect, x[0].p, done, st);
         if (cycles == 0 && xzero) vec_launch<0>(st, m, VZero<T>{x[0].p}, sc, done);
     } else {
+        // the last cycle's post-smoothing writes the result straight into out
         for (int cyc = 0; cyc < cycles; cyc++) {
-            vstep(Lf, defect, xzero, sc, done, st);
+            vstep(Lf, defect, xzero, sc, done, st, false, cyc == cycles - 1 ? out : nullptr);
             xzero = false;
         }
         if (xzero) vec_launch<0>(st, m, VZero<T>{x[Lf].p}, sc, done);
     }
-    vec_launch<0>(st, m, VCopy<T>{x[Lf].p, out}, sc, done);
+    if (L == 1 || cycles == 0) vec_launch<0>(st, m, VCopy<T>{x[Lf].p, out}, sc, done);
     if (nbd_fine) {
         launch_ex(k_bc_add<T>, dim3(nb(nbd_fine)), dim3(256), 0, st, nbd_fine, (const int*)bd_fine.p, v, out, done);
     }

@@ -65,10 +65,11 @@ struct MGImpl {
     void fmg(const T* defect, T* out, const Scratch& sc, const int* done, cudaStream_t st);
 
     // internals
+    // dest (optional): where the level's final smoothing result goes instead of x[l]
     void vstep(int l, const T* rhs, bool xzero, const Scratch& sc, const int* done, cudaStream_t st,
-               bool first_sweep_done = false);
+               bool first_sweep_done = false, T* dest = nullptr);
     void smooth(int l, const T* rhs, bool xzero, const Scratch& sc, const int* done, cudaStream_t st,
-                bool first_sweep_done = false);
+                bool first_sweep_done = false, T* dest = nullptr);
     void coarse(const T* rhs, T* out, const int* done, cudaStream_t st);
     // the V-cycle below and including level `bot`, entered from the restriction above
     void bottom(bool first_sweep_done, const int* done, cudaStream_t st);
