@@ -81,6 +81,19 @@ int jfg_spmv_dev(jfg_mat* m, const double* d_x, double* d_y);
 int jfg_spmv_t_dev(jfg_mat* m, const double* d_x, double* d_y);
 /* FP32 product on FP32 device vectors (values rounded to FP32 once). */
 int jfg_spmv_f32_dev(jfg_mat* m, const float* d_x, float* d_y);
+/* Product y = A x with FP32 vectors and sums and the matrix values read as
+ * values = 0: FP32, 1: BF16, 2: FP16 scaled by a power of two (the storage
+ * formats of the mixed-precision multigrid levels).  Checking and
+ * measurement helper, not part of the reference surface. */
+int jfg_spmv_lowp_dev(jfg_mat* m, int values, const float* d_x, float* d_y);
+/* The product layout the library picked for the matrix: *stencil = 1 when
+ * the rows [lo, lo + regular_rows) use the values-only 9-point layout with
+ * grid stride *stride (no column indices; the other_rows rows, with
+ * other_nnz entries, keep a CSR copy), 0 for SELL-32 (then other_rows =
+ * rows and other_nnz = nnz).  fp16_scale_inv: the factor of the FP16 copy's
+ * row sums (0 before that copy exists).  Informational. */
+int jfg_matrix_layout(jfg_mat* m, int* stencil, int* stride, int* regular_rows, int* other_rows,
+                      int64_t* other_nnz, double* fp16_scale_inv);
 /* Diagonal with duplicates summed.  Replaces Matrix.diag (Core/src/main/java/linalg/Matrix.java:157-175). */
 int jfg_matrix_diag(jfg_mat* m, double* h_diag);
 /* The merged CSR of the matrix (rows sorted, columns ascending within a row):
@@ -247,6 +260,8 @@ typedef struct {
                           2: FP32 hierarchy whose SpMVs read BF16 matrix values (FP32 vectors and sums);
                           3: FP32 hierarchy whose SpMVs read FP16 matrix values scaled by a power of two
                              per matrix (max |a| * 2^k in [2^14, 2^15)), FP32 vectors and sums */
+    int cycle;         /* 0: the application runs V-cycles (mvMul);
+                          1: W-cycles, MGPreconditionerSpace.mvMulW (multigrid/MGPreconditionerSpace.java:165-183) */
 } jfg_mg_desc;
 /* Builds a hierarchy from per-level systems A[0..levels) (0 = coarsest),
  * prolongations P[l] (n_{l+1} x n_l, l < levels-1), Dirichlet node lists and
@@ -262,6 +277,9 @@ int jfg_mg_free(jfg_mg* mg);
 int jfg_mg_apply(jfg_mg* mg, const double* h_v, double* h_out);
 /* out = vCycle(x0, rhs).  Replaces MGPreconditionerInterface.vCycle (:293-298). */
 int jfg_mg_vcycle(jfg_mg* mg, const double* h_x0, const double* h_rhs, double* h_out);
+/* out = wCycle(x0, rhs).  Replaces MGPreconditionerInterface.wCycle (:300-305), i.e. mgStepW
+ * (:200-291): smoothing, two coarse-grid corrections by mgStepV on the next coarser level, smoothing. */
+int jfg_mg_wcycle(jfg_mg* mg, const double* h_x0, const double* h_rhs, double* h_out);
 /* out = fullVCycleCorrection(defect).  Replaces MGPreconditionerInterface.fullVCycleCorrection (:307-326). */
 int jfg_mg_fmg(jfg_mg* mg, const double* h_defect, double* h_out);
 
@@ -442,8 +460,9 @@ int jfg_dense_solve(jfg_ctx* ctx, int n, const double* h_A, const double* h_b, d
 int jfg_dense_inverse(jfg_ctx* ctx, int n, const double* h_A, double* h_Ainv);
 /* CG on a system the caller already holds on the device as CSR (row
  * pointers, column indices, values; no duplicates), for callers that must not
- * allocate device memory while they solve -- e.g. code running under CUDA
- * stream capture or inside a framework that owns the device heap.  No
+ * allocate device memory while they solve -- e.g. a host framework that owns
+ * the device heap (a pool or budget the library must not touch), or a loop
+ * that cannot take cudaMalloc's latency and implicit synchronisation.  No
  * counterpart in the reference: it is the allocation-free twin of
  * jfg_solve_dev(JFG_CG, ...), with the same iteration and semantics (x holds
  * the start iterate on entry, the solution on exit; absolute tolerance;
@@ -452,8 +471,12 @@ int jfg_dense_inverse(jfg_ctx* ctx, int n, const double* h_A, double* h_Ainv);
  * about 6.3 MB per GPU: n is limited to 262,144 unknowns (larger n is
  * rejected with JFG_ERR_BAD_ARG).  The array is shared by every call and
  * keeps the last call's contents; calls that overlap on the GPU race on it.
- * The first call on a device looks up the array's address and should come
- * before any stream capture.  Calls no cudaMalloc/cudaFree. */
+ * The call runs eagerly on the context's stream and synchronises the host
+ * with it (it polls the convergence flag every 8 iterations).  The first call
+ * on a device looks up the array's address and caches it for the process
+ * lifetime (the device's primary context; no cudaDeviceReset in between).
+ * A met p.Ap <= 0 (indefinite matrix) is reported through jfg_last_error.
+ * Calls no cudaMalloc/cudaFree. */
 int jfg_cg_noalloc(jfg_ctx* ctx, int n, const int* d_rowptr, const int* d_col, const double* d_val,
                    const double* d_b, double* d_x, double tol, int maxit, int* iterations, double* final_norm);
 

@@ -32,11 +32,11 @@ EXPORTED = [
     "jfg_version",
     "jfg_kernel_launches",
     "jfg_matrix_from_coo", "jfg_matrix_free", "jfg_matrix_info", "jfg_spmv", "jfg_spmv_t", "jfg_spmv_dev",
-    "jfg_spmv_t_dev", "jfg_spmv_f32_dev", "jfg_matrix_diag", "jfg_spmv_time", "jfg_smooth",
+    "jfg_spmv_t_dev", "jfg_spmv_f32_dev", "jfg_spmv_lowp_dev", "jfg_matrix_layout", "jfg_matrix_diag", "jfg_spmv_time", "jfg_smooth",
     "jfg_matrix_csr", "jfg_matrix_mmmul", "jfg_matrix_tmmul", "jfg_matrix_galerkin",
     "jfg_gs_create", "jfg_gs_free", "jfg_gs_info", "jfg_gs_ranks", "jfg_assemble_tp",
     "jfg_assemble_taylor_hood",
-    "jfg_mg_create", "jfg_mg_free", "jfg_mg_apply", "jfg_mg_vcycle", "jfg_mg_fmg",
+    "jfg_mg_create", "jfg_mg_free", "jfg_mg_apply", "jfg_mg_vcycle", "jfg_mg_wcycle", "jfg_mg_fmg",
     "jfg_solver_opts_default", "jfg_solve", "jfg_solve_dev",
     "jfg_dense_solve", "jfg_dense_inverse", "jfg_sparse_solve", "jfg_cg_noalloc",
     "jfg_batch_opts_default", "jfg_batch_create", "jfg_batch_free", "jfg_batch_layout", "jfg_batch_heat",
@@ -61,7 +61,7 @@ class TPDesc(C.Structure):
 
 
 class MGDesc(C.Structure):
-    _fields_ = [("cycles", C.c_int), ("use_fmg", C.c_int), ("precision", C.c_int)]
+    _fields_ = [("cycles", C.c_int), ("use_fmg", C.c_int), ("precision", C.c_int), ("cycle", C.c_int)]
 
 
 class SolverOpts(C.Structure):
@@ -126,6 +126,8 @@ def load():
         getattr(L, f).argtypes = [_P, _D, _D]
     for f in ("jfg_spmv_dev", "jfg_spmv_t_dev", "jfg_spmv_f32_dev"):
         getattr(L, f).argtypes = [_P, _P, _P]
+    L.jfg_spmv_lowp_dev.argtypes = [_P, C.c_int, _P, _P]
+    L.jfg_matrix_layout.argtypes = [_P, _I, _I, _I, _I, C.POINTER(C.c_int64), _D]
     L.jfg_matrix_diag.argtypes = [_P, _D]
     L.jfg_spmv_time.argtypes = [_P, C.c_int, C.c_int, _D]
     L.jfg_matrix_csr.argtypes = [_P, _I, _I, _D]
@@ -145,6 +147,7 @@ def load():
     L.jfg_mg_free.argtypes = [_P]
     L.jfg_mg_apply.argtypes = [_P, _D, _D]
     L.jfg_mg_vcycle.argtypes = [_P, _D, _D, _D]
+    L.jfg_mg_wcycle.argtypes = [_P, _D, _D, _D]
     L.jfg_mg_fmg.argtypes = [_P, _D, _D]
     L.jfg_solver_opts_default.restype = None
     L.jfg_solver_opts_default.argtypes = [C.POINTER(SolverOpts)]

@@ -245,6 +245,42 @@ int jfg_spmv_f32_dev(jfg_mat* m, const float* x, float* y)
     });
 }
 
+int jfg_spmv_lowp_dev(jfg_mat* m, int values, const float* x, float* y)
+{
+    if (!m || (!x && m->m->cols) || (!y && m->m->rows) || values < 0 || values > 2) return JFG_ERR_BAD_ARG;
+    jfg_ctx* ctx = m->ctx;
+    return guard(ctx, [&]() -> int {
+        jfg::Matrix* M = m->m;
+        jfg::Scratch sc = ctx_scratch(ctx, M->nblocks);
+        cudaStream_t st = ctx->c.stream;
+        if (values == 0) {
+            jfg::matrix_ensure_fp32(M);
+            jfg::spmv_launch<float, float, 0>(st, M, M->val32.p, x, jfg::EpiStore<float>{y}, sc, nullptr);
+        } else if (values == 1) {
+            jfg::matrix_ensure_bf16(M);
+            jfg::spmv_launch<__nv_bfloat16, float, 0>(st, M, M->val16.p, x, jfg::EpiStore<float>{y}, sc, nullptr);
+        } else {
+            jfg::matrix_ensure_fp16(M);
+            jfg::spmv_launch<__half, float, 0>(st, M, M->valh.p, x, jfg::EpiStore<float>{y}, sc, nullptr);
+        }
+        return JFG_OK;
+    });
+}
+
+int jfg_matrix_layout(jfg_mat* m, int* stencil, int* stride, int* regular_rows, int* other_rows,
+                      int64_t* other_nnz, double* fp16_scale_inv)
+{
+    if (!m) return JFG_ERR_BAD_ARG;
+    const jfg::Matrix* M = m->m;
+    if (stencil) *stencil = M->st;
+    if (stride) *stride = M->st ? M->st_S : 0;
+    if (regular_rows) *regular_rows = M->st ? M->st_hi - M->st_lo : 0;
+    if (other_rows) *other_rows = M->st ? M->st_nirr : M->rows;
+    if (other_nnz) *other_nnz = M->st ? M->st_len - 9 * (int64_t)(M->st_hi - M->st_lo) : M->nnz;
+    if (fp16_scale_inv) *fp16_scale_inv = M->hash ? (double)M->hscale_inv : 0.0;
+    return JFG_OK;
+}
+
 int jfg_spmv(jfg_mat* m, const double* x, double* y)
 {
     if (!m || (!x && m->m->cols) || (!y && m->m->rows)) return JFG_ERR_BAD_ARG;
@@ -467,7 +503,9 @@ int jfg_mg_create(jfg_ctx* ctx, int levels, jfg_mat* const* A, jfg_mat* const* P
             g->cycles = desc ? desc->cycles : 3;
             g->use_fmg = desc ? desc->use_fmg : 1;
             g->precision = desc ? desc->precision : 0;
+            g->wcycle = desc ? desc->cycle : 0;
             JFG_CHECK(g->cycles >= 0, JFG_ERR_BAD_ARG, "negative cycle count");
+            JFG_CHECK(g->wcycle == 0 || g->wcycle == 1, JFG_ERR_BAD_ARG, "cycle must be 0 (V) or 1 (W)");
             for (int l = 0; l < levels; l++) {
                 JFG_CHECK(A[l] && A[l]->ctx == ctx, JFG_ERR_BAD_ARG, "level matrix from another context");
                 g->A.push_back(A[l]->m);
@@ -510,6 +548,7 @@ int jfg_mg_create(jfg_ctx* ctx, int levels, jfg_mat* const* A, jfg_mat* const* P
             g->d64.reset(new jfg::MGImpl<double>());
             g->d64->init(&ctx->c, levels, g->A.data(), g->P.data(), bp.data(), nbp.data(), g->sm.data(), g->cycles,
                          g->use_fmg);
+            g->d64->wcycle = g->wcycle;
             if (g->d64->coarse_status != JFG_OK) throw Error{JFG_ERR_SINGULAR, "coarsest-level matrix is singular"};
             JFG_CHECK(g->precision >= 0 && g->precision <= 3, JFG_ERR_BAD_ARG, "unknown hierarchy precision");
             if (g->precision >= 1) g->fp32();
@@ -562,6 +601,22 @@ int jfg_mg_vcycle(jfg_mg* g, const double* x0, const double* rhs, double* out)
         ctx->stage_c.alloc(n);
         jfg::Scratch sc = ctx_scratch(ctx, g->d64->max_blocks());
         g->d64->vcycle(ctx->stage_a.p, ctx->stage_b.p, ctx->stage_c.p, sc, nullptr, ctx->c.stream);
+        stage_out(ctx, ctx->stage_c.p, out, n);
+        return JFG_OK;
+    });
+}
+
+int jfg_mg_wcycle(jfg_mg* g, const double* x0, const double* rhs, double* out)
+{
+    if (!g || !x0 || !rhs || !out) return JFG_ERR_BAD_ARG;
+    jfg_ctx* ctx = ctx_of(g);
+    return guard(ctx, [&]() -> int {
+        int n = g->d64->n[g->levels - 1];
+        stage_in(ctx, ctx->stage_a, x0, n);
+        stage_in(ctx, ctx->stage_b, rhs, n);
+        ctx->stage_c.alloc(n);
+        jfg::Scratch sc = ctx_scratch(ctx, g->d64->max_blocks());
+        g->d64->wcycle_apply(ctx->stage_a.p, ctx->stage_b.p, ctx->stage_c.p, sc, nullptr, ctx->c.stream);
         stage_out(ctx, ctx->stage_c.p, out, n);
         return JFG_OK;
     });

@@ -128,6 +128,26 @@ struct Matrix {
     float hscale_inv = 1.0f;      // 2^-k: row sums of valh times this are the sums of the values
     int has32 = 0, has16 = 0, hash = 0;
     int csr_only = 0;             // no SELL layout (an intermediate of a sparse product)
+    // Values-only 9-point stencil layout (square matrices of 2-D Q1 grids
+    // numbered lexicographically with stride st_S over a contiguous range of
+    // rows): row r in [st_lo, st_hi) couples only to the columns
+    // r + {-S-1, -S, -S+1, -1, 0, 1, S-1, S, S+1}, and all nine of those
+    // columns exist.  Its values are stored per offset, st_val[k * nreg +
+    // (r - st_lo)] (zero where the matrix has no entry), with no column
+    // indices at all.  The rows outside the range ("irregular", a prefix and
+    // a suffix of the numbering) keep a CSR copy: st_irow / st_iptr / st_icol
+    // and their values at st_val[9 * nreg + k].  The SELL layout is kept as
+    // well (other kernels read it); products with a stencil copy of their
+    // value type use this layout.
+    int st = 0;
+    int st_S = 0, st_lo = 0, st_hi = 0, st_nirr = 0;
+    int st_nb_reg = 0, st_nb_irr = 0;   // CTAs of the regular and the irregular rows
+    int64_t st_len = 0;                 // 9 * nreg + irregular entries
+    DevBuf<int> st_irow, st_iptr, st_icol;
+    DevBuf<double> st_val;
+    DevBuf<float> st_val32;
+    DevBuf<__nv_bfloat16> st_val16;
+    DevBuf<__half> st_valh;
     int cg_small_nnz = -1;        // small-system CG: largest CSR slice of its 8 row blocks (-1: not computed)
     Matrix* transposed = nullptr; // lazily built for tvMul
     uint64_t uid = 0;             // unique id (keys of cached CUDA graphs)

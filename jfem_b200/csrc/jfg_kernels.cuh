@@ -438,6 +438,81 @@ k_spmv_pipe(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Ep
 }
 
 // ---------------------------------------------------------------------------
+// values-only 9-point stencil SpMV (Matrix::st)
+// ---------------------------------------------------------------------------
+struct StArgs {
+    int S, lo, nreg, nirr, nb_reg;
+    const int* irow;
+    const int* iptr;
+    const int* icol;
+    float vscale;          // FP16 values: factor of the row sums
+};
+
+// One thread per row.  A regular row r reads its nine values (one coalesced
+// stream per offset, no column indices) and x[r + offset] for the offsets in
+// ascending column order; the CTAs past the regular range take the
+// irregular rows from their CSR copy.  Each row is summed in ascending
+// column order from 0 with the same multiply-adds as k_spmv (a stored zero
+// adds exactly 0 for finite x), so the result equals the SELL kernels' bit
+// for bit.  PF: the values are loaded before the wait for the preceding
+// kernel (matrices that are not written after set-up).
+template <typename VT, typename XT, int NR, class Epi, class Fin, bool PF = false>
+__global__ void __launch_bounds__(kThreads)
+k_spmv_st(StArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi, GridRed<NR, Fin> red,
+          const int* __restrict__ done)
+{
+    using AT = typename AccOf<VT>::T;
+    const bool regular = (int)blockIdx.x < m.nb_reg;
+    const int i = (regular ? (int)blockIdx.x : (int)blockIdx.x - m.nb_reg) * kThreads + threadIdx.x;
+    AT v[9];
+    if (PF && regular && i < m.nreg) {
+#pragma unroll
+        for (int k = 0; k < 9; k++) v[k] = to_acc(ld_stream(val + (int64_t)k * m.nreg + i));
+    }
+    pdl_wait();
+    if (done && *done) return;
+    double acc[NR > 0 ? NR : 1];
+#pragma unroll
+    for (int q = 0; q < (NR > 0 ? NR : 1); q++) acc[q] = 0;
+    if (regular) {
+        if (i < m.nreg) {
+            if (!PF) {
+#pragma unroll
+                for (int k = 0; k < 9; k++) v[k] = to_acc(ld_stream(val + (int64_t)k * m.nreg + i));
+            }
+            const int r = m.lo + i;
+            const XT* xa = x + (r - m.S - 1);
+            const XT* xc = x + (r - 1);
+            const XT* xb = x + (r + m.S - 1);
+            AT xv[9];
+            xv[0] = (AT)__ldg(xa);
+            xv[1] = (AT)__ldg(xa + 1);
+            xv[2] = (AT)__ldg(xa + 2);
+            xv[3] = (AT)__ldg(xc);
+            xv[4] = (AT)__ldg(xc + 1);
+            xv[5] = (AT)__ldg(xc + 2);
+            xv[6] = (AT)__ldg(xb);
+            xv[7] = (AT)__ldg(xb + 1);
+            xv[8] = (AT)__ldg(xb + 2);
+            AT sum = 0;
+#pragma unroll
+            for (int k = 0; k < 9; k++) sum += v[k] * xv[k];
+            if constexpr (std::is_same<VT, __half>::value) sum *= m.vscale;
+            epi(r, sum, acc);
+        }
+    } else if (i < m.nirr) {
+        const int r = m.irow[i];
+        const VT* iv = val + 9 * (int64_t)m.nreg;
+        AT sum = 0;
+        for (int k = m.iptr[i]; k < m.iptr[i + 1]; k++) sum += to_acc(iv[k]) * (AT)__ldg(x + m.icol[k]);
+        if constexpr (std::is_same<VT, __half>::value) sum *= m.vscale;
+        epi(r, sum, acc);
+    }
+    pdl_launch_dependents();
+    if constexpr (NR > 0) red.reduce(acc);
+}
+
+// ---------------------------------------------------------------------------
 // grid-stride vector kernels: f(i, acc) per index, optional reduction
 // ---------------------------------------------------------------------------
 template <int NR, class F, class Fin>

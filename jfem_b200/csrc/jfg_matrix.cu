@@ -160,6 +160,52 @@ __global__ void k_expand_rows(int rows, const int* ptr, int* ri)
     for (int k = ptr[r]; k < ptr[r + 1]; k++) ri[k] = r;
 }
 
+// stencil layout: a row is regular when it couples only to r + {-S-1..-S+1,
+// -1..1, S-1..S+1} and all nine of those columns exist
+__global__ void k_st_classify(int rows, int S, const int* __restrict__ ptr, const int* __restrict__ col,
+                              unsigned char* __restrict__ reg)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    bool ok = r - S - 1 >= 0 && r + S + 1 < rows;
+    for (int k = ptr[r]; ok && k < ptr[r + 1]; k++) {
+        const int d = col[k] - r;
+        const int a = d < 0 ? -d : d;
+        ok = a <= 1 || (a >= S - 1 && a <= S + 1);
+    }
+    reg[r] = ok ? 1 : 0;
+}
+
+// offset d of a regular row -> slot 0..8 in ascending column order
+__device__ __forceinline__ int st_slot(int d, int S)
+{
+    return d <= -S + 1 ? d + S + 1 : (d >= S - 1 ? d - S + 7 : d + 4);
+}
+
+__global__ void k_st_fill(int lo, int nreg, int S, const int* __restrict__ ptr, const int* __restrict__ col,
+                          const double* __restrict__ val, double* __restrict__ st)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nreg) return;
+    const int r = lo + i;
+    for (int k = ptr[r]; k < ptr[r + 1]; k++) st[(int64_t)st_slot(col[k] - r, S) * nreg + i] = val[k];
+}
+
+// CSR copy of the irregular rows (their entries in column order)
+__global__ void k_st_irregular(int nirr, const int* __restrict__ irow, const int* __restrict__ iptr,
+                               const int* __restrict__ ptr, const int* __restrict__ col,
+                               const double* __restrict__ val, int* __restrict__ icol, double* __restrict__ ival)
+{
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nirr) return;
+    const int r = irow[j];
+    int o = iptr[j];
+    for (int k = ptr[r]; k < ptr[r + 1]; k++, o++) {
+        icol[o] = col[k];
+        ival[o] = val[k];
+    }
+}
+
 __global__ void k_to_f32(int64_t n, const double* a, float* b)
 {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -172,6 +218,96 @@ __global__ void k_to_bf16(int64_t n, const double* a, __nv_bfloat16* b)
 }
 
 }  // namespace
+
+// JFEM_STENCIL=0 keeps every matrix built afterwards in SELL-32 only (read
+// at each build: products of one matrix in both layouts can be compared)
+bool stencil_enabled()
+{
+    const char* e = getenv("JFEM_STENCIL");
+    return !(e && e[0] == '0');
+}
+
+// Values-only 9-point layout (see Matrix::st).  The stride S is read off a
+// few middle rows (largest column offset - 1); the layout is kept when the
+// contiguous run of regular rows around the middle row leaves at most a
+// quarter of the rows outside it.
+static void build_stencil(Matrix* M, const std::vector<int>& len)
+{
+    const int n = M->rows;
+    if (n < 256 || M->rows != M->cols || !stencil_enabled()) return;
+    cudaStream_t s = M->ctx->stream;
+    std::vector<int> hp(n + 1);
+    JFG_CUDA(cudaMemcpyAsync(hp.data(), M->csr_ptr.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
+    JFG_CUDA(cudaStreamSynchronize(s));
+    int S = 0;
+    for (int j = 0; j < 16 && !S; j++) {
+        const int r = n / 2 + j;
+        const int a = hp[r], e = hp[r + 1];
+        if (e - a < 2 || e - a > 9) continue;
+        std::vector<int> c(e - a);
+        JFG_CUDA(cudaMemcpyAsync(c.data(), M->csr_col.p + a, sizeof(int) * (e - a), cudaMemcpyDeviceToHost, s));
+        JFG_CUDA(cudaStreamSynchronize(s));
+        const int cand = c.back() - r - 1;
+        if (cand < 3) continue;
+        bool ok = true;
+        for (int v : c) {
+            const int d = std::abs(v - r);
+            ok = ok && (d <= 1 || (d >= cand - 1 && d <= cand + 1));
+        }
+        if (ok) S = cand;
+    }
+    if (!S) return;
+    DevBuf<unsigned char> reg;
+    reg.alloc((size_t)n);
+    k_st_classify<<<nblk(n), 256, 0, s>>>(n, S, M->csr_ptr.p, M->csr_col.p, reg.p);
+    JFG_CUDA(cudaGetLastError());
+    std::vector<unsigned char> hr(n);
+    JFG_CUDA(cudaMemcpyAsync(hr.data(), reg.p, (size_t)n, cudaMemcpyDeviceToHost, s));
+    JFG_CUDA(cudaStreamSynchronize(s));
+    // the stencil range: from the row after the last irregular row of the
+    // first half to the first irregular row of the second half (on 2-D grids
+    // numbered by first appearance the irregular rows are the first three and
+    // the last grid lines; the regular Dirichlet rows among them go to CSR)
+    const int mid = n / 2;
+    int lo = mid, hi = mid;
+    while (lo > 0 && hr[lo - 1]) lo--;
+    while (hi < n && hr[hi]) hi++;
+    if (hi - lo < 64) return;
+    const int nreg = hi - lo, nirr = n - nreg;
+    if ((int64_t)nirr * 4 > n) return;
+    std::vector<int> irow, iptr{0};
+    irow.reserve(nirr);
+    for (int r = 0; r < n; r++)
+        if (r < lo || r >= hi) {
+            irow.push_back(r);
+            iptr.push_back(iptr.back() + len[r]);
+        }
+    const int64_t irr_nnz = iptr.back();
+    M->st_S = S;
+    M->st_lo = lo;
+    M->st_hi = hi;
+    M->st_nirr = nirr;
+    M->st_len = 9 * (int64_t)nreg + irr_nnz;
+    M->st_val.alloc((size_t)M->st_len);
+    M->st_irow.alloc(nirr ? (size_t)nirr : 1);
+    M->st_iptr.alloc((size_t)nirr + 1);
+    M->st_icol.alloc(irr_nnz ? (size_t)irr_nnz : 1);
+    JFG_CUDA(cudaMemsetAsync(M->st_val.p, 0, sizeof(double) * 9 * (size_t)nreg, s));
+    k_st_fill<<<nblk(nreg), 256, 0, s>>>(lo, nreg, S, M->csr_ptr.p, M->csr_col.p, M->csr_val.p, M->st_val.p);
+    JFG_CUDA(cudaGetLastError());
+    if (nirr) {
+        JFG_CUDA(cudaMemcpyAsync(M->st_irow.p, irow.data(), sizeof(int) * nirr, cudaMemcpyHostToDevice, s));
+        JFG_CUDA(cudaMemcpyAsync(M->st_iptr.p, iptr.data(), sizeof(int) * (nirr + 1), cudaMemcpyHostToDevice, s));
+        k_st_irregular<<<nblk(nirr), 256, 0, s>>>(nirr, M->st_irow.p, M->st_iptr.p, M->csr_ptr.p, M->csr_col.p,
+                                                 M->csr_val.p, M->st_icol.p, M->st_val.p + 9 * (int64_t)nreg);
+        JFG_CUDA(cudaGetLastError());
+    }
+    M->st_nb_reg = (int)nblk(nreg, kThreads);
+    M->st_nb_irr = (int)nblk(nirr, kThreads);
+    M->nblocks = std::max(M->nblocks, M->st_nb_reg + M->st_nb_irr);
+    JFG_CUDA(cudaStreamSynchronize(s));
+    M->st = 1;
+}
 
 // Builds CSR and SELL-32-sigma from merged, sorted, zero-free COO that is
 // already on the device (keys = row*cols+col ascending, values alongside).
@@ -277,6 +413,7 @@ static Matrix* build_from_sorted(Context* c, int rows, int cols, int64_t m, cons
         if (hb) M->col16.release();
     }
     JFG_CUDA(cudaStreamSynchronize(s));
+    build_stencil(M, len);
     return M;
 }
 
@@ -401,6 +538,11 @@ void matrix_ensure_fp32(Matrix* M)
     M->val32.alloc(M->sell_len ? (size_t)M->sell_len : 1);
     if (M->sell_len) k_to_f32<<<nblk(M->sell_len), 256, 0, M->ctx->stream>>>(M->sell_len, M->val.p, M->val32.p);
     JFG_CUDA(cudaGetLastError());
+    if (M->st) {
+        M->st_val32.alloc((size_t)M->st_len);
+        k_to_f32<<<nblk(M->st_len), 256, 0, M->ctx->stream>>>(M->st_len, M->st_val.p, M->st_val32.p);
+        JFG_CUDA(cudaGetLastError());
+    }
     M->has32 = 1;
 }
 
@@ -450,6 +592,11 @@ void matrix_ensure_fp16(Matrix* M)
     M->valh.alloc(M->sell_len ? (size_t)M->sell_len : 1);
     if (M->sell_len) k_to_f16<<<nblk(M->sell_len), 256, 0, st>>>(M->sell_len, M->val.p, s, M->valh.p);
     JFG_CUDA(cudaGetLastError());
+    if (M->st) {
+        M->st_valh.alloc((size_t)M->st_len);
+        k_to_f16<<<nblk(M->st_len), 256, 0, st>>>(M->st_len, M->st_val.p, s, M->st_valh.p);
+        JFG_CUDA(cudaGetLastError());
+    }
     M->hash = 1;
 }
 
@@ -459,6 +606,11 @@ void matrix_ensure_bf16(Matrix* M)
     M->val16.alloc(M->sell_len ? (size_t)M->sell_len : 1);
     if (M->sell_len) k_to_bf16<<<nblk(M->sell_len), 256, 0, M->ctx->stream>>>(M->sell_len, M->val.p, M->val16.p);
     JFG_CUDA(cudaGetLastError());
+    if (M->st) {
+        M->st_val16.alloc((size_t)M->st_len);
+        k_to_bf16<<<nblk(M->st_len), 256, 0, M->ctx->stream>>>(M->st_len, M->st_val.p, M->st_val16.p);
+        JFG_CUDA(cudaGetLastError());
+    }
     M->has16 = 1;
 }
 

@@ -677,6 +677,13 @@ void MGImpl<T>::vstep(int l, const T* rhs, bool xzero, const Scratch& sc, const 
         return;
     }
     smooth(l, rhs, xzero, sc, done, st, first_sweep_done);
+    coarse_correction(l, rhs, sc, done, st);
+    smooth(l, rhs, false, sc, done, st, false, dest);
+}
+
+template <typename T>
+void MGImpl<T>::coarse_correction(int l, const T* rhs, const Scratch& sc, const int* done, cudaStream_t st)
+{
     mg_spmv<T, 0>(*this, st, A[l], x[l].p, EpiResid<T>{rhs, r[l].p}, sc, done);
     const int lc = l - 1;
     const bool fuse_sweep = lc >= 1 && sm[lc].kind == JFG_SMOOTH_JACOBI && sm[lc].runs > 0;
@@ -689,6 +696,22 @@ void MGImpl<T>::vstep(int l, const T* rhs, bool xzero, const Scratch& sc, const 
     }
     vstep(lc, b[lc].p, true, sc, done, st, fuse_sweep);
     mg_spmv<T, 0>(*this, st, P[lc], x[lc].p, EpiMaskedAdd<T>{mask[l].p, x[l].p}, sc, done);
+}
+
+// mgStepW (MGPreconditionerInterface.java:200-291): pre-smoothing, two
+// coarse-grid corrections in a row, each by mgStepV on level l-1 from a zero
+// start, post-smoothing; result in x[l] (or dest).
+template <typename T>
+void MGImpl<T>::wstep(int l, const T* rhs, bool xzero, const Scratch& sc, const int* done, cudaStream_t st, T* dest)
+{
+    if (l == 0) {
+        coarse(rhs, x[0].p, done, st);
+        if (dest) vec_launch<0>(st, n[0], VCopy<T>{x[0].p, dest}, sc, done);
+        return;
+    }
+    smooth(l, rhs, xzero, sc, done, st);
+    coarse_correction(l, rhs, sc, done, st);
+    coarse_correction(l, rhs, sc, done, st);
     smooth(l, rhs, false, sc, done, st, false, dest);
 }
 
@@ -733,7 +756,10 @@ void MGImpl<T>::apply(const T* v, T* out, const Scratch& sc, const int* done, cu
     } else {
         // the last cycle's post-smoothing writes the result straight into out
         for (int cyc = 0; cyc < cycles; cyc++) {
-            vstep(Lf, defect, xzero, sc, done, st, false, cyc == cycles - 1 ? out : nullptr);
+            if (wcycle)
+                wstep(Lf, defect, xzero, sc, done, st, cyc == cycles - 1 ? out : nullptr);
+            else
+                vstep(Lf, defect, xzero, sc, done, st, false, cyc == cycles - 1 ? out : nullptr);
             xzero = false;
         }
         if (xzero) vec_launch<0>(st, m, VZero<T>{x[Lf].p}, sc, done);
@@ -751,6 +777,17 @@ void MGImpl<T>::vcycle(const T* x0, const T* rhs, T* out, const Scratch& sc, con
     vec_launch<0>(st, m, VCopy<T>{rhs, b[Lf].p}, sc, done);
     vec_launch<0>(st, m, VCopy<T>{x0, x[Lf].p}, sc, done);
     vstep(Lf, b[Lf].p, false, sc, done, st);
+    vec_launch<0>(st, m, VCopy<T>{x[Lf].p, out}, sc, done);
+}
+
+template <typename T>
+void MGImpl<T>::wcycle_apply(const T* x0, const T* rhs, T* out, const Scratch& sc, const int* done,
+                             cudaStream_t st)
+{
+    int Lf = L - 1, m = n[Lf];
+    vec_launch<0>(st, m, VCopy<T>{rhs, b[Lf].p}, sc, done);
+    vec_launch<0>(st, m, VCopy<T>{x0, x[Lf].p}, sc, done);
+    wstep(Lf, b[Lf].p, false, sc, done, st);
     vec_launch<0>(st, m, VCopy<T>{x[Lf].p, out}, sc, done);
 }
 
@@ -835,6 +872,7 @@ jfg::MGImpl<float>* jfg_mg::fp32()
         const char* e = getenv("JFEM_MG_BF16");
         const int vfmt = precision == 3 ? 2 : ((precision == 2 || (e && e[0] == '1')) ? 1 : 0);
         d32->init(ctx, levels, A.data(), P.data(), bp.data(), nbp.data(), sm.data(), cycles, use_fmg, vfmt);
+        d32->wcycle = wcycle;
     }
     return d32.get();
 }

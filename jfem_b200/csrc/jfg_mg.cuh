@@ -29,6 +29,7 @@ struct MGImpl {
     int L = 0;
     int cycles = 3;
     int use_fmg = 1;
+    int wcycle = 0;                         // apply: mgStepW (MGPreconditionerSpace.mvMulW) instead of mgStepV
     int vbf16 = 0;                          // float hierarchy: matrices read as BF16 (FP32 vectors, FP32 sums)
     int vfp16 = 0;                          // float hierarchy: matrices read as scaled FP16 (FP32 vectors, sums)
     int bot = -1;                           // levels 0..bot run as one cluster kernel (-1: none)
@@ -61,6 +62,8 @@ struct MGImpl {
     void apply(const T* v, T* out, const Scratch& sc, const int* done, cudaStream_t st);
     // out = vCycle(x0, rhs) on the finest level.
     void vcycle(const T* x0, const T* rhs, T* out, const Scratch& sc, const int* done, cudaStream_t st);
+    // out = wCycle(x0, rhs) on the finest level.
+    void wcycle_apply(const T* x0, const T* rhs, T* out, const Scratch& sc, const int* done, cudaStream_t st);
     // out = fullVCycleCorrection(defect).
     void fmg(const T* defect, T* out, const Scratch& sc, const int* done, cudaStream_t st);
 
@@ -68,6 +71,12 @@ struct MGImpl {
     // dest (optional): where the level's final smoothing result goes instead of x[l]
     void vstep(int l, const T* rhs, bool xzero, const Scratch& sc, const int* done, cudaStream_t st,
                bool first_sweep_done = false, T* dest = nullptr);
+    // mgStepW: guess in x[l] (or zero); two coarse-grid corrections by mgStepV
+    void wstep(int l, const T* rhs, bool xzero, const Scratch& sc, const int* done, cudaStream_t st,
+               T* dest = nullptr);
+    // restricted defect of x[l] into level l-1 (with the fused first Jacobi
+    // sweep there when possible), mgStepV on l-1 from zero, prolongation + add
+    void coarse_correction(int l, const T* rhs, const Scratch& sc, const int* done, cudaStream_t st);
     void smooth(int l, const T* rhs, bool xzero, const Scratch& sc, const int* done, cudaStream_t st,
                 bool first_sweep_done = false, T* dest = nullptr);
     void coarse(const T* rhs, T* out, const int* done, cudaStream_t st);
@@ -96,7 +105,7 @@ struct jfg_mg {
     std::vector<jfg::Matrix*> A, P;
     std::vector<std::vector<int>> bdry;
     std::vector<jfg::SmootherDesc> sm;
-    int cycles = 3, use_fmg = 1, precision = 0;
+    int cycles = 3, use_fmg = 1, precision = 0, wcycle = 0;
     std::unique_ptr<jfg::MGImpl<double>> d64;
     std::unique_ptr<jfg::MGImpl<float>> d32;
     jfg::MGImpl<float>* fp32();

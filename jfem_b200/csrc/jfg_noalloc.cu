@@ -1,21 +1,26 @@
 // CG on caller-owned device CSR arrays without any device allocation.
 //
-// Some callers cannot allocate device memory at the moment they solve: code
-// that runs while a CUDA stream is being captured, or inside a host
-// framework that owns the device heap (a pool or budget that the library must
-// not touch), or a real-time loop that forbids cudaMalloc/cudaFree latency.
-// For them this file offers jfg_cg_noalloc: the same CG iteration as
+// Some callers cannot allocate device memory at the moment they solve: a host
+// framework that owns the device heap (a memory pool or budget that the
+// library must not grow or fragment), or a real-time loop that cannot afford
+// the latency and implicit synchronisation of cudaMalloc/cudaFree.  For them
+// this file offers jfg_cg_noalloc: the same CG iteration as
 // jfg_solve_dev(JFG_CG, ...) (IterativeSolver.solveCG semantics: start iterate
 // taken from x, absolute tolerance, iteration cap), but every work vector,
 // the reduction partials and the control block live in one file-scope
 // __device__ array of fixed size.  The caller passes the matrix (CSR), the
 // right-hand side and the iterate as device pointers.
 //
+// The call runs eagerly on the context's stream and synchronises the host
+// with it: every 8 iterations it reads the device convergence flag back.
+//
 // The array is a single process-wide resource per GPU: every call shares it
 // and it keeps the contents of the last call.  Calls that overlap on the GPU
 // (two streams, two host threads) race on it.  The first call on a device
 // looks up the array's device address (cudaGetSymbolAddress) with that
-// device current; make that first call before any stream capture.
+// device current and caches it for the rest of the process; the cache
+// assumes the runtime's primary context of that device stays the same for
+// the process lifetime (no cudaDeviceReset in between).
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -148,6 +153,20 @@ struct VNcUpdate {   // x += p*alpha; r = r - Ap*alpha; acc += r^2
         acc[0] += rn * rn;
     }
 };
+struct NcReset {     // the array keeps the previous call's contents: a fresh control block
+    Ctl* c;
+    double tol;
+    int maxit, n;
+    __device__ void operator()() const
+    {
+        Ctl h{};
+        h.tol = tol;
+        h.maxit = maxit;
+        h.n = n;
+        h.status = JFG_NOT_CONVERGED;
+        *c = h;
+    }
+};
 struct VNcDir {      // p = r + p*beta
     const double* r;
     double* p;
@@ -190,15 +209,10 @@ extern "C" int jfg_cg_noalloc(jfg_ctx* ctx, int n, const int* d_rowptr, const in
         cudaStream_t st = jfg::ctx_stream(ctx);
         ScratchLayout L = scratch_for_device(jfg::ctx_device(ctx));
         if (maxit <= 0) maxit = n;
-        // the array keeps the previous call's contents: reset the control
-        // block and the reduction counter
-        Ctl h{};
-        h.tol = tol;
-        h.maxit = maxit;
-        h.n = n;
-        h.status = JFG_NOT_CONVERGED;
+        // the array keeps the previous call's contents: reset the reduction
+        // counter and the control block on the device
         JFG_CUDA(cudaMemsetAsync(L.counter, 0, kCounterBytes, st));
-        JFG_CUDA(cudaMemcpyAsync(L.ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, st));
+        scalar_launch(st, NcReset{L.ctl, tol, maxit, n}, nullptr);
         int it = 0;
         double rn = 0;
         if (n > 0) {
@@ -225,6 +239,8 @@ extern "C" int jfg_cg_noalloc(jfg_ctx* ctx, int n, const int* d_rowptr, const in
         rn = out.res_norm;
         if (iterations) *iterations = it;
         if (final_norm) *final_norm = rn;
+        if (n > 0 && out.not_pd)   // the same condition jfg_solve_dev reports in jfg_solve_info.not_pd
+            jfg::ctx_set_error(ctx, "jfg_cg_noalloc: p.Ap <= 0 met (matrix not positive definite)");
         return n == 0 ? JFG_OK : out.status;
     } catch (const jfg::Error& e) {
         jfg::ctx_set_error(ctx, e.msg);

@@ -19,6 +19,24 @@ inline int ilog2(int v)
 }
 
 template <typename T> const T* vals_of(const Matrix* M);
+// the SELL value copy of type VT and its stencil-layout twin
+template <typename VT> struct LayoutVals;
+template <> struct LayoutVals<double> {
+    static const double* sell(const Matrix* M) { return M->val.p; }
+    static const double* st(const Matrix* M) { return M->st_val.p; }
+};
+template <> struct LayoutVals<float> {
+    static const float* sell(const Matrix* M) { return M->val32.p; }
+    static const float* st(const Matrix* M) { return M->st_val32.p; }
+};
+template <> struct LayoutVals<__nv_bfloat16> {
+    static const __nv_bfloat16* sell(const Matrix* M) { return M->val16.p; }
+    static const __nv_bfloat16* st(const Matrix* M) { return M->st_val16.p; }
+};
+template <> struct LayoutVals<__half> {
+    static const __half* sell(const Matrix* M) { return M->valh.p; }
+    static const __half* st(const Matrix* M) { return M->st_valh.p; }
+};
 template <> inline const double* vals_of<double>(const Matrix* M) { return M->val.p; }
 template <> inline const float* vals_of<float>(const Matrix* M) { return M->val32.p; }
 
@@ -134,6 +152,14 @@ void spmv_launch(cudaStream_t st, const Matrix* M, const VT* val, const XT* x, E
 {
     if (M->rows == 0) return;
     GridRed<NR, Fin> red{sc.partials, sc.counter, fin};
+    // the values-only stencil layout, when the matrix has one in this value type
+    if (M->st && val == LayoutVals<VT>::sell(M) && LayoutVals<VT>::st(M)) {
+        StArgs sa{M->st_S, M->st_lo, M->st_hi - M->st_lo, M->st_nirr, M->st_nb_reg, M->st_irow.p, M->st_iptr.p,
+                  M->st_icol.p, std::is_same<VT, __half>::value ? M->hscale_inv : 1.0f};
+        launch_ex(k_spmv_st<VT, XT, NR, Epi, Fin, PF>, dim3(M->st_nb_reg + M->st_nb_irr), dim3(kThreads), 0, st, sa,
+                  LayoutVals<VT>::st(M), x, epi, red, done);
+        return;
+    }
     SpmvArgs a{M->off.p, M->perm.p, M->col.p, M->nslices * kSliceRows, M->tpr_log2, M->col16.p,
                std::is_same<VT, __half>::value ? M->hscale_inv : 1.0f};
     const dim3 g(M->nblocks), b(kThreads);

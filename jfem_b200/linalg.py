@@ -306,6 +306,29 @@ class DeviceMatrix:
         self.ctx.check(N.load().jfg_matrix_diag(self._h, N.dptr(d)))
         return d
 
+    def spmv_lowp_dev(self, x, values="fp32", y=None):
+        """y = A x on FP32 CUDA tensors with the matrix values read as FP32,
+        BF16 or scaled FP16 (the formats of the mixed-precision levels)."""
+        import torch
+        fmt = {"fp32": 0, "bf16": 1, "fp16": 2}[values]
+        if y is None:
+            y = torch.empty(self.rows, dtype=torch.float32, device=x.device)
+        torch.cuda.synchronize()
+        self.ctx.check(N.load().jfg_spmv_lowp_dev(self._h, fmt, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr())))
+        self.ctx.check(N.load().jfg_synchronize(self.ctx.handle))
+        return y
+
+    def layout(self) -> dict:
+        """The product layout: {'stencil': bool, 'stride', 'regular_rows',
+        'other_rows', 'other_nnz', 'fp16_scale_inv'}."""
+        st, S, nreg, noth = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        onnz = C.c_int64()
+        hs = C.c_double()
+        self.ctx.check(N.load().jfg_matrix_layout(self._h, C.byref(st), C.byref(S), C.byref(nreg), C.byref(noth),
+                                                  C.byref(onnz), C.byref(hs)))
+        return {"stencil": bool(st.value), "stride": S.value, "regular_rows": nreg.value, "other_rows": noth.value,
+                "other_nnz": int(onnz.value), "fp16_scale_inv": hs.value}
+
     def time_spmv(self, precision=0, iters=50):
         ms = C.c_double()
         self.ctx.check(N.load().jfg_spmv_time(self._h, precision, iters, C.byref(ms)))

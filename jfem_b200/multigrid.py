@@ -114,10 +114,12 @@ class MGPreconditioner(VectorMultiplyable):
     precision="mixed" also builds the FP32 hierarchy used by mixed solves;
     "mixed-bf16" builds it with BF16 matrix values (FP32 vectors and sums);
     "mixed-fp16" with FP16 matrix values scaled by a power of two per matrix.
+    cycle="W" makes the application MGPreconditionerSpace.mvMulW (wCycle in
+    place of vCycle, multigrid/MGPreconditionerSpace.java:165-183).
     """
 
     def __init__(self, systems, prolongations, boundary, smoothers, cycles=3, use_fmg=True, precision="fp64",
-                 ctx=None):
+                 ctx=None, cycle="V"):
         L = len(systems)
         if len(prolongations) != L - 1 or len(boundary) != L:
             raise IllegalArgumentException("level data of inconsistent length")
@@ -142,7 +144,9 @@ class MGPreconditioner(VectorMultiplyable):
         levels = {"fp64": 0, "mixed": 1, "mixed-bf16": 2, "mixed-fp16": 3}
         if precision not in levels:
             raise IllegalArgumentException(f"unknown hierarchy precision {precision!r}")
-        desc = N.MGDesc(int(cycles), 1 if use_fmg else 0, levels[precision])
+        if cycle not in ("V", "W"):
+            raise IllegalArgumentException(f"unknown cycle {cycle!r}")
+        desc = N.MGDesc(int(cycles), 1 if use_fmg else 0, levels[precision], 1 if cycle == "W" else 0)
         h = C.c_void_p()
         st = N.load().jfg_mg_create(self.ctx.handle, L, Ah, Ph, Bh, N.iptr(nb), descs, C.byref(desc), C.byref(h))
         if st == N.ERR_BAD_ARG:
@@ -153,6 +157,7 @@ class MGPreconditioner(VectorMultiplyable):
         self.cycles = cycles
         self.use_fmg = use_fmg
         self.precision = precision
+        self.cycle = cycle
 
     @property
     def handle(self):
@@ -207,7 +212,8 @@ class MGPreconditioner(VectorMultiplyable):
         smoothers = [None] + [levelToSmoother(l, systems[l]) for l in range(1, level + 1)]
         return MGPreconditioner(systems, self._P[:level], self._bd[:level + 1], smoothers,
                                 cycles=self.cycles if cycles is None else cycles, use_fmg=self.use_fmg,
-                                precision=self.precision if precision is None else precision, ctx=self.ctx)
+                                precision=self.precision if precision is None else precision, ctx=self.ctx,
+                                cycle=self.cycle)
 
     def vCycle(self, initialIterate, rhs):
         x0, b = N.f64(initialIterate), N.f64(rhs)
@@ -215,6 +221,15 @@ class MGPreconditioner(VectorMultiplyable):
             raise IllegalArgumentException("wrong size")
         out = np.empty(self.n)
         self.ctx.check(N.load().jfg_mg_vcycle(self._h, N.dptr(x0), N.dptr(b), N.dptr(out)))
+        return out
+
+    def wCycle(self, initialIterate, rhs):
+        """MGPreconditionerInterface.wCycle (multigrid/MGPreconditionerInterface.java:300-305)."""
+        x0, b = N.f64(initialIterate), N.f64(rhs)
+        if x0.shape != (self.n,) or b.shape != (self.n,):
+            raise IllegalArgumentException("wrong size")
+        out = np.empty(self.n)
+        self.ctx.check(N.load().jfg_mg_wcycle(self._h, N.dptr(x0), N.dptr(b), N.dptr(out)))
         return out
 
     def fullVCycleCorrection(self, defect):

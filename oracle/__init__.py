@@ -94,8 +94,12 @@ def lib():
         L.or_mg_fmg.argtypes = [_P, _D, _D]
         L.or_mg_apply.argtypes = [_P, _D, _D]
         L.or_mg_apply_ex.argtypes = [_P, C.c_int, C.c_int, _D, _D]
+        L.or_mg_apply_kind.argtypes = [_P, C.c_int, C.c_int, C.c_int, _D, _D]
+        L.or_mg_wcycle.argtypes = [_P, _D, _D, _D]
         L.or_op_mg.restype = _P
         L.or_op_mg.argtypes = [_P, C.c_int, C.c_int]
+        L.or_op_mg_kind.restype = _P
+        L.or_op_mg_kind.argtypes = [_P, C.c_int, C.c_int, C.c_int]
         L.or_op_mg_free.argtypes = [_P]
         L.or_mg_coarse_status.argtypes = [_P]
         L.or_mg_set_schwarz.argtypes = [_P, C.c_int, _P, C.c_int]
@@ -352,10 +356,11 @@ class MGPreconditioner:
     n_{l+1} x n_l prolongation, ``bdry[l]`` the Dirichlet node list,
     ``smoothers[l]`` a (kind, runs, omega) triple for l >= 1.
     use_fmg/cycles select the reference mvMul (FMG + cycles V-cycles) or a
-    single V-cycle (use_fmg=False, cycles=1).
+    single V-cycle (use_fmg=False, cycles=1); cycle="W" selects mvMulW
+    (wCycle in place of vCycle, MGPreconditionerSpace.java:165-183).
     """
 
-    def __init__(self, mats, prolong, bdry, smoothers, cycles=3, use_fmg=True):
+    def __init__(self, mats, prolong, bdry, smoothers, cycles=3, use_fmg=True, cycle="V"):
         L = len(mats)
         self.mats, self.prolong = mats, prolong
         self._bd = [_i32(b) for b in bdry]
@@ -370,7 +375,9 @@ class MGPreconditioner:
         self._h = lib().or_mg_new(L, A, P, BD, _i(NBD), _i(kind), _i(runs), _d(omg), cycles)
         if lib().or_mg_coarse_status(self._h) != OK:
             raise np.linalg.LinAlgError("coarsest matrix singular")
-        self._op = lib().or_op_mg(self._h, 1 if use_fmg else 0, cycles)
+        if cycle not in ("V", "W"):
+            raise ValueError("cycle must be 'V' or 'W'")
+        self._op = lib().or_op_mg_kind(self._h, 1 if use_fmg else 0, cycles, 1 if cycle == "W" else 0)
         self.n = mats[-1].rows
 
     def __del__(self):
@@ -385,15 +392,20 @@ class MGPreconditioner:
         lib().or_mg_vcycle(self._h, _d(_f64(x0)), _d(_f64(rhs)), _d(out))
         return out
 
+    def wcycle(self, x0, rhs):
+        out = np.empty(self.n)
+        lib().or_mg_wcycle(self._h, _d(_f64(x0)), _d(_f64(rhs)), _d(out))
+        return out
+
     def fmg(self, defect):
         out = np.empty(self.n)
         lib().or_mg_fmg(self._h, _d(_f64(defect)), _d(out))
         return out
 
-    def apply(self, v, use_fmg=True, cycles=None):
+    def apply(self, v, use_fmg=True, cycles=None, cycle="V"):
         out = np.empty(self.n)
-        lib().or_mg_apply_ex(self._h, 1 if use_fmg else 0, 3 if cycles is None else cycles,
-                             _d(_f64(v)), _d(out))
+        lib().or_mg_apply_kind(self._h, 1 if use_fmg else 0, 3 if cycles is None else cycles,
+                               1 if cycle == "W" else 0, _d(_f64(v)), _d(out))
         return out
 
     def mvmul(self, v):

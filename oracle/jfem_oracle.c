@@ -1343,6 +1343,44 @@ static void mg_step_v(const or_mg* g, int level, double* guess, const double* rh
     free(r); free(rc); free(cc);
 }
 
+/* mgStepW (MGPreconditionerInterface.java:200-291); guess is updated in
+ * place.  Despite its name the reference recurses through mgStepV: on the
+ * level it is called on it smooths, applies two coarse-grid corrections in a
+ * row (each a restricted defect of the current guess, one mgStepV on level-1
+ * from a zero start, prolonged and added), then smooths again. */
+static void mg_step_w(const or_mg* g, int level, double* guess, const double* rhs)
+{
+    int n = g->A[level]->rows;
+    if (level == 0) {
+        lu_solve(&g->coarse, rhs, guess);      /* lines 203-218 */
+        return;
+    }
+    double* r = vnew(n);
+    smooth(&g->sm[level], g->A[level], rhs, guess, r);          /* pre-smooth, lines 226-227 */
+    int nc = g->A[level - 1]->rows;
+    double* rc = vnew(nc);
+    double* cc = vnew(nc);
+    for (int pass = 0; pass < 2; pass++) {                     /* lines 229-247 and 249-267 */
+        or_mat_mvmul(g->A[level], guess, r);
+        for (int i = 0; i < n; i++) r[i] = rhs[i] - r[i];
+        mg_restrict(g, level - 1, r, rc);
+        memset(cc, 0, sizeof(double) * nc);
+        mg_step_v(g, level - 1, cc, rc);
+        mg_prolong(g, level - 1, cc, r);
+        for (int i = 0; i < n; i++) guess[i] = guess[i] + r[i];
+    }
+    smooth(&g->sm[level], g->A[level], rhs, guess, r);          /* post-smooth, lines 282-283 */
+    free(r); free(rc); free(cc);
+}
+
+/* wCycle (MGPreconditionerInterface.java:300-305). */
+void or_mg_wcycle(const or_mg* g, const double* x0, const double* rhs, double* out)
+{
+    int n = g->A[g->L - 1]->rows;
+    memcpy(out, x0, sizeof(double) * n);
+    mg_step_w(g, g->L - 1, out, rhs);
+}
+
 /* vCycle (MGPreconditionerInterface.java:293-298). */
 void or_mg_vcycle(const or_mg* g, const double* x0, const double* rhs, double* out)
 {
@@ -1380,8 +1418,10 @@ void or_mg_fmg(const or_mg* g, const double* defect, double* out)
 /* Preconditioner application mvMul (MGPreconditionerInterface.java:352-379):
  * boundary values copied into a zero start, FMG correction of the defect,
  * then `cycles` V-cycles.  use_fmg = 0 replaces the FMG correction by a zero
- * start (plain V-cycle preconditioner). */
-void or_mg_apply_ex(const or_mg* g, int use_fmg, int cycles, const double* v, double* out)
+ * start (plain V-cycle preconditioner).  wcycle = 1 is mvMulW
+ * (MGPreconditionerSpace.java:165-183): the same with wCycle in place of
+ * vCycle. */
+void or_mg_apply_kind(const or_mg* g, int use_fmg, int cycles, int wcycle, const double* v, double* out)
 {
     int L = g->L, n = g->A[L - 1]->rows;
     double* initial = vnew(n);
@@ -1391,32 +1431,41 @@ void or_mg_apply_ex(const or_mg* g, int use_fmg, int cycles, const double* v, do
     for (int i = 0; i < n; i++) defect[i] = v[i] - defect[i];
     double* iter = vnew(n);
     if (use_fmg) or_mg_fmg(g, defect, iter);
-    for (int c = 0; c < cycles; c++) mg_step_v(g, L - 1, iter, defect);
+    for (int c = 0; c < cycles; c++) {
+        if (wcycle) mg_step_w(g, L - 1, iter, defect);
+        else mg_step_v(g, L - 1, iter, defect);
+    }
     for (int i = 0; i < n; i++) out[i] = initial[i] + iter[i];
     free(initial); free(defect); free(iter);
 }
 
+void or_mg_apply_ex(const or_mg* g, int use_fmg, int cycles, const double* v, double* out)
+{
+    or_mg_apply_kind(g, use_fmg, cycles, 0, v, out);
+}
+
 void or_mg_apply(const or_mg* g, const double* v, double* out) { or_mg_apply_ex(g, 1, g->cycles, v, out); }
 
-typedef struct { const or_mg* g; int use_fmg; int cycles; } mg_op_data;
+typedef struct { const or_mg* g; int use_fmg; int cycles; int wcycle; } mg_op_data;
 static void op_mg_mv(const or_op* o, const double* x, double* y)
 {
     const mg_op_data* d = (const mg_op_data*)o->data;
-    or_mg_apply_ex(d->g, d->use_fmg, d->cycles, x, y);
+    or_mg_apply_kind(d->g, d->use_fmg, d->cycles, d->wcycle, x, y);
 }
 static void op_mg_free_data(or_op* o) { free((void*)o->data); }
 
 /* The MG preconditioner as an operator.  use_fmg=1, cycles=g->cycles is the
  * reference's mvMul; use_fmg=0, cycles=1 is a single V-cycle from zero with
  * the boundary copy. */
-or_op* or_op_mg(const or_mg* g, int use_fmg, int cycles)
+or_op* or_op_mg_kind(const or_mg* g, int use_fmg, int cycles, int wcycle)
 {
     or_op* o = (or_op*)calloc(1, sizeof(or_op));
     mg_op_data* d = (mg_op_data*)malloc(sizeof(mg_op_data));
-    d->g = g; d->use_fmg = use_fmg; d->cycles = cycles;
+    d->g = g; d->use_fmg = use_fmg; d->cycles = cycles; d->wcycle = wcycle;
     o->n = g->A[g->L - 1]->rows; o->mv = op_mg_mv; o->data = d;
     return o;
 }
+or_op* or_op_mg(const or_mg* g, int use_fmg, int cycles) { return or_op_mg_kind(g, use_fmg, cycles, 0); }
 void or_op_mg_free(or_op* o)
 {
     if (!o) return;

@@ -90,3 +90,40 @@ def test_cluster_bottom_is_bit_identical(ctx, monkeypatch, precision):
     assert i1 == i0
     assert np.array_equal(h1, h0)
     assert np.array_equal(x1, x0)
+
+
+@pytest.mark.parametrize("p,coarse,L", [(1, 4, 5), (2, 2, 4)])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_wcycle_and_mvmulw(ctx, p, coarse, L, precision):
+    """wCycle (MGPreconditionerInterface.java:300-305, mgStepW :200-291) and the
+    preconditioner mvMulW (MGPreconditionerSpace.java:165-183: FMG + cycles
+    W-cycles) against the oracle to 1e-10; the FP32 hierarchy inside a PCG
+    solve reaches the tolerance in the oracle's FP64 iteration count."""
+    from jfem_b200 import IterativeSolver
+    h = mg_levels(p, coarse, L, modes=6, seed=7)
+    sm = (O.SMOOTH_JACOBI, 2, 2 / 3)
+    mats_o = [coo_oracle(s) for s in h.systems]
+    prol_o = [O.CooMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l]) for l in range(L - 1)]
+    mg_o = O.MGPreconditioner(mats_o, prol_o, h.boundary, [None] + [sm] * (L - 1), cycles=2, use_fmg=True,
+                              cycle="W")
+    mats = [dev(s, ctx) for s in h.systems]
+    prol = [DeviceMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l], ctx) for l in range(L - 1)]
+    mg = MGPreconditioner(mats, prol, h.boundary, [None] + [JacobiSmoother(2, 2 / 3)] * (L - 1), cycles=2,
+                          use_fmg=True, precision=precision, ctx=ctx, cycle="W")
+    b = h.finest.rhs
+    x0 = np.random.default_rng(2).standard_normal(b.size) * 0.1
+    for got, ref in ((mg.wCycle(x0, b), mg_o.wcycle(x0, b)), (mg.mvMul(b), mg_o.mvmul(b))):
+        np.testing.assert_allclose(got, ref, rtol=1e-10, atol=1e-10 * np.abs(ref).max())
+    # the W-cycle smooths more than the V-cycle: its error reduction is at least as good
+    e_w = np.linalg.norm(b - mats_o[-1].mvmul(mg_o.wcycle(np.zeros(b.size), b)))
+    e_v = np.linalg.norm(b - mats_o[-1].mvmul(mg_o.vcycle(np.zeros(b.size), b)))
+    assert e_w <= e_v
+    tol = 1e-8 * np.linalg.norm(b)
+    ref = O.solve_pcg(mats_o[-1], mg_o, b, tol)
+    s = IterativeSolver(ctx=ctx)
+    s.precision = "fp64" if precision == "fp64" else "mixed-precond"
+    x = s.solvePCG(mats[-1], mg, b, tol)
+    assert s.iterations == ref.iterations
+    assert np.linalg.norm(b - mats_o[-1].mvmul(x)) <= tol
+    if precision == "fp64":
+        assert np.linalg.norm(x - ref.x) / np.linalg.norm(ref.x) < 1e-8

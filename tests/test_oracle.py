@@ -171,3 +171,42 @@ def test_oracle_gauss_seidel_dense():
         ref = np.linalg.solve(L, bp - np.triu(ap, 1) @ xp)
         got = O.gs_smooth(A, O.SMOOTH_GS, 1, b, x0, rank)
         np.testing.assert_allclose(got[p], ref, rtol=1e-13, atol=1e-13)
+
+
+def test_mg_wcycle_composition():
+    """mgStepW (MGPreconditionerInterface.java:200-291) restated from public
+    pieces: smooth, then twice [restrict the defect with zero boundary values,
+    one V-cycle of the next coarser hierarchy from zero, prolong with zero
+    boundary values, add], then smooth; mvMulW = boundary copy + FMG + W-cycles."""
+    import scipy.sparse as sps
+    L = 4
+    h = mg_levels(1, 4, L, modes=4, seed=2)
+    sm = (O.SMOOTH_JACOBI, 2, 2 / 3)
+    mats = [O.CooMatrix(s.n, s.n, s.rows, s.cols, s.vals) for s in h.systems]
+    prol = [O.CooMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l]) for l in range(L - 1)]
+    mg = O.MGPreconditioner(mats, prol, h.boundary, [None] + [sm] * (L - 1), cycles=2, use_fmg=True, cycle="W")
+    sub = O.MGPreconditioner(mats[:-1], prol[:-1], h.boundary[:-1], [None] + [sm] * (L - 2), cycles=1,
+                             use_fmg=False)
+    P = sps.csr_matrix((h.prolong[-1][2], (h.prolong[-1][0], h.prolong[-1][1])),
+                       shape=(h.systems[-1].n, h.systems[-2].n))
+    A = mats[-1]
+    b = h.finest.rhs
+    x0 = np.random.default_rng(5).standard_normal(b.size) * 0.1
+
+    def zero(v, l):
+        v = v.copy()
+        v[np.asarray(h.boundary[l], dtype=np.int64)] = 0.0
+        return v
+
+    x = O.smooth(A, *sm, b, x0)
+    for _ in range(2):
+        rc = zero(P.T @ (b - A.mvmul(x)), L - 2)
+        x = x + zero(P @ sub.vcycle(np.zeros(rc.size), rc), L - 1)
+    x = O.smooth(A, *sm, b, x)
+    np.testing.assert_allclose(mg.wcycle(x0, b), x, rtol=1e-12, atol=1e-14 * np.abs(x).max())
+    # mvMulW with cycles = 2 (boundary values zero here: Dirichlet data 0)
+    d = b.copy()
+    it = mg.fmg(d)
+    for _ in range(2):
+        it = mg.wcycle(it, d)
+    np.testing.assert_allclose(mg.mvmul(b), it, rtol=1e-13, atol=1e-15 * np.abs(it).max())
