@@ -1,13 +1,23 @@
-"""Benchmark: time to a 1e-8 relative FP64 residual and SpMV GB/s on one B200.
+"""Benchmark: time to a 1e-8 FP64 residual and SpMV GB/s on one B200.
 
-Workload (one "step" = one solve): -Laplace u + 5u = f on the unit square,
-Q2 elements on a 512x512 cell grid (1,050,625 dofs, 8-level geometric
-multigrid, 2+2 damped-Jacobi sweeps with omega = 2/3, coarsest 4x4 cells
-solved by a dense FP64 inverse), f from 16x16 seeded sine modes.  The headline
-solve is the mixed-precision GMG-PCG (FP64 defect correction around FP32
-V-cycle-preconditioned CG); the plain FP64 GMG-PCG on the same GPU is timed
-beside it.  The matrix (202 MB FP64 / 134 MB FP32 values + indices) is larger
-than L2, so no flush is needed between steps.
+Default workload (one "step" = one solve): -div(kappa grad u) = f on the unit
+square, Q1 elements on a 1024x1024 cell grid (1,050,625 unknowns), kappa =
+exp(g) with g a seeded Gaussian random field (squared-exponential
+covariance, length 0.05, variance 1), zero Dirichlet data, f from 4x4 seeded
+sine modes; 9-level geometric multigrid (coarse levels rediscretised with
+2x2-averaged kappa), 2+2 damped-Jacobi sweeps (omega = 2/3), coarsest 4x4
+cells solved by a dense FP64 inverse.  Arms, each a whole solve to
+||b - A x|| <= 1e-8 ||b|| in FP64:
+
+  fp64      plain FP64 GMG-PCG from e0 (the drop-in; the judge)
+  mixed     FP64 PCG + FP32 V-cycle preconditioner
+  fp16      FP64 PCG + V-cycle reading scaled-FP16 matrices (FP32 vectors)
+  fgmres    FGMRES(30) + FP32 V-cycle
+  learned   FGMRES(30) + FP32 V-cycle + learned smoother (the headline value)
+
+The working set (FP64 finest matrix, hierarchy, vectors) is larger than L2,
+so solves run back to back without a flush.  The Q2 512x512 -Lap u + 5u = f
+GMG-PCG (configs' multigrid case) is timed too and reported as extra keys.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
 
@@ -15,11 +25,10 @@ Under torchrun every rank solves its own replica (no data-path collective;
 "replicas only"); the step time is the max over ranks.
 
 The other configurations are measured with --workload (one JSON line each,
-1 GPU, no reference arm): batch-heat (256 uneven Q1 heat systems, 50
-implicit-Euler steps in one persistent launch), stokes (Taylor-Hood Q2/Q1
-on 256x256 cells, GMRES(50) with the block-diagonal preconditioner) and
-learned (-div(kappa grad u) = f on Q1 1024x1024: FGMRES(30) with the
-V-cycle + learned smoother against FP64 GMG-PCG).
+1 GPU, no reference arm): gmg-pcg (the Q2 512x512 case alone), cg-small,
+batch-heat (256 uneven Q1 heat systems, 50 implicit-Euler steps in one
+persistent launch), stokes (Taylor-Hood Q2/Q1 on 256x256 cells, GMRES(50)
+with the block-diagonal preconditioner), galerkin, gs-pcg, assemble.
 """
 from __future__ import annotations
 
@@ -52,10 +61,13 @@ def parse():
     ap.add_argument("--levels", type=int, default=LEVELS)
     ap.add_argument("--vcycle", default="fp32", choices=["fp32", "fp16", "bf16"],
                     help="storage of the V-cycle matrices of the mixed solve (FP32 vectors and sums in every case)")
-    ap.add_argument("--workload", default="gmg-pcg", choices=["gmg-pcg", "cg-small", "batch-heat", "stokes", "learned", "galerkin", "gs-pcg",
-                                                        "assemble"])
+    ap.add_argument("--workload", default="kappa",
+                    choices=["kappa", "gmg-pcg", "cg-small", "batch-heat", "stokes", "learned", "galerkin", "gs-pcg",
+                             "assemble"])
+    ap.add_argument("--no-q2", action="store_true", help="kappa workload: skip the Q2 512x512 extra keys")
     ap.add_argument("--profile", default=None,
-                    choices=["solve-fp64", "solve-mixed", "solve-mixed-nograph", "gs-mixed-nograph", "spmv64", "spmv32"],
+                    choices=["solve-fp64", "solve-mixed", "solve-mixed-nograph", "gs-mixed-nograph", "spmv64", "spmv32",
+                             "solve-learned", "solve-learned-nograph", "solve-fp64-nograph"],
                     help="set up, run the named operation --warmup + 1 times and exit (for ncu captures)")
     return ap.parse_args()
 
@@ -349,7 +361,7 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and os.environ.get("JFEM_BENCH_NO_CPU") != "1":
-        cpu = cpu_baseline(h, tol, it64)
+        cpu = cpu_baseline(h, tol)
 
     if rank == 0:
         line = {
@@ -387,8 +399,10 @@ def run_ours(args):
                     "path": "jfg_solve (C ABI) with pinned host rhs in and solution out; start e0 (opts.start=1)"},
             "gpu_launches": int(round(launches)),
             "roofline": {"bound": "hbm", "achieved": gbs32, "peak": peak, "unit": "GB/s", "frac": gbs32 / peak,
-                         "traffic": SPMV32_TRAFFIC_BYTES if (n, nnz) == SPMV32_TRAFFIC_CASE else None, "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
-                         "one cold launch (profiles/k_spmv_sell_fp32_q2_512.md)",
+                         "traffic": SPMV32_TRAFFIC_BYTES if (n, nnz) == SPMV32_TRAFFIC_CASE else None,
+                         "traffic_source": "constant from an earlier ncu capture of this kernel on this matrix "
+                                           "(dram__bytes_read.sum + dram__bytes_write.sum, one cold launch); "
+                                           "not measured in this run",
                          "kernel": "k_spmv_pipe<float> finest level", "peak_source": peak_src,
                          "bytes_per_launch": b32, "ms_per_launch": ms_spmv32},
             "clocks": clk.summary(),
@@ -397,6 +411,310 @@ def run_ours(args):
         }
         print(json.dumps(line))
     reps.close()
+
+
+KAPPA_CELLS, KAPPA_LEVELS, KAPPA_SEED = 1024, 9, 0
+KAPPA_WORKLOAD = ("Q1 1024x1024 -div(kappa grad u) = f, kappa = exp(GRF l=0.05 var=1), 9-level GMG, "
+                  "Jacobi 2+2, to 1e-8 relative FP64 residual")
+
+
+def kappa_size(args):
+    """(cells, levels) of the kappa workload: 1024^2 cells and 9 levels unless
+    --cells / --levels are given (the coarsest grid stays 4x4 cells)."""
+    if args.cells != CELLS:
+        return args.cells, int(round(np.log2(args.cells // 4))) + 1
+    return KAPPA_CELLS, KAPPA_LEVELS
+
+
+def layout_bytes(A, sval, sx):
+    """Algorithmic bytes of one product in the layout the library picked:
+    values-only stencil rows (9 values, no indices) + CSR rows (values,
+    columns, row list and pointers) + x read once + y written once; the CSR
+    formula when the matrix has no stencil layout."""
+    lay = A.layout()
+    n = A.rows
+    if not lay["stencil"]:
+        return spmv_bytes(n, A.nnz, sval, sx), lay
+    b = 9 * lay["regular_rows"] * sval + lay["other_nnz"] * (sval + 4) + lay["other_rows"] * 4 \
+        + (lay["other_rows"] + 1) * 4 + n * sx + n * sx
+    return b, lay
+
+
+def run_kappa(args):
+    import ctypes as C
+    import torch
+    from jfem_b200.replicas import Replicas
+    reps = Replicas(timeout_s=120)
+    rank, world, local = reps.rank, reps.world, reps.local
+    torch.cuda.set_device(local)
+    os.environ["JFEM_DEVICE"] = str(local)
+    from jfem_b200 import _native as N
+    from jfem_b200.cnn import LearnedSmoother
+    from jfem_b200.learned import WEIGHTS, KappaSystem
+    from jfem_b200.multigrid import JacobiSmoother, MGPreconditioner
+
+    ctx = N.Context(local)
+    t0 = time.time()
+    ks = KappaSystem(ctx, kappa_size(args)[0], kseed=KAPPA_SEED)
+    L = len(ks.mats)
+    mg16 = MGPreconditioner(ks.mats, ks._prol, ks.h.boundary, [None] + [JacobiSmoother(2, 2 / 3)] * (L - 1),
+                            cycles=1, use_fmg=False, precision="mixed-fp16", ctx=ctx)
+    net = LearnedSmoother(ctx, weights=np.load(WEIGHTS))
+    pc_v = ks.preconditioner(net, use_net=False)
+    pc_net = ks.preconditioner(net, use_net=True)
+    A = ks.A
+    n = ks.n
+    b_host = ks.b.copy()
+    bnorm = float(np.linalg.norm(b_host))
+    tol = RTOL * bnorm
+    setup_s = time.time() - t0
+
+    stream = torch.cuda.ExternalStream(ctx.stream_ptr())
+    dev = f"cuda:{local}"
+    db = torch.from_numpy(b_host).to(dev)
+    e0 = torch.zeros(n, dtype=torch.float64, device=dev)
+    e0[0] = 1.0
+    z0 = torch.zeros(n, dtype=torch.float64, device=dev)
+    dx = torch.empty_like(e0)
+    torch.cuda.synchronize()
+    info = N.SolveInfo()
+    arms = {
+        "fp64": (N.PCG, N.PREC_MG, ks.mg, N.FP64, e0, "FP64 GMG-PCG from e0 (the plain drop-in)"),
+        "mixed": (N.PCG, N.PREC_MG, ks.mg, N.MIXED_PRECOND, e0, "FP64 PCG + FP32 V-cycle, from e0"),
+        "fp16": (N.PCG, N.PREC_MG, mg16, N.MIXED_PRECOND, e0,
+                 "FP64 PCG + V-cycle reading scaled-FP16 matrices (FP32 vectors and sums), from e0"),
+        "fgmres": (N.FGMRES, N.PREC_MG_CNN, pc_v, N.FP64, z0, "FGMRES(30) + FP32 V-cycle, from zero"),
+        "learned": (N.FGMRES, N.PREC_MG_CNN, pc_net, N.FP64, z0,
+                    "FGMRES(30) + FP32 V-cycle + learned smoother (BF16 network), from zero"),
+    }
+    HEAD = "learned"
+
+    def opts(precision, graph=True):
+        o = N.SolverOpts()
+        N.load().jfg_solver_opts_default(C.byref(o))
+        o.tol = tol
+        o.precision = precision
+        o.inner_rtol = 1e-4
+        o.restart = 30
+        o.use_graph = 1 if graph else 0
+        return o
+
+    def solve_dev(arm, graph=True):
+        kind, pk, pc, prec, start, _ = arms[arm]
+        with torch.cuda.stream(stream):
+            dx.copy_(start)
+        st = N.load().jfg_solve_dev(ctx.handle, kind, A.handle, pk, pc.handle, C.c_void_p(db.data_ptr()),
+                                    C.c_void_p(dx.data_ptr()), C.byref(opts(prec, graph)), C.byref(info))
+        ctx.check(st)
+        return info.iterations
+
+    def timed(fn, steps, warmup, clk=None):
+        for _ in range(warmup):
+            fn()
+        reps.barrier()
+        torch.cuda.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        if clk:
+            clk.mark_start()
+        ev0.record(stream)
+        for _ in range(steps):
+            fn()
+        ev1.record(stream)
+        ev1.synchronize()
+        torch.cuda.synchronize()
+        if clk:
+            clk.mark_end()
+        reps.barrier()
+        return reps.max(ev0.elapsed_time(ev1) / steps)
+
+    if args.profile:
+        name = {"solve-learned": ("learned", True), "solve-learned-nograph": ("learned", False),
+                "solve-fp64": ("fp64", True), "solve-fp64-nograph": ("fp64", False),
+                "solve-mixed": ("mixed", True), "solve-mixed-nograph": ("mixed", False)}.get(args.profile)
+        for _ in range(args.warmup + 1):
+            if name:
+                solve_dev(name[0], name[1])
+            else:
+                A.time_spmv(precision=1 if args.profile == "spmv32" else 0, iters=1)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": args.profile, "iterations": info.iterations}))
+        reps.close()
+        return
+
+    out = {}
+    x64 = None
+    for arm in ("fp64", "mixed", "fp16", "fgmres"):
+        ms_a = timed(lambda a=arm: solve_dev(a), max(2, args.steps // 2), max(3, args.warmup))
+        it = solve_dev(arm)
+        x = dx.cpu().numpy().copy()
+        r = float(np.linalg.norm(b_host - A.spmv(x)))
+        if arm == "fp64":
+            x64 = x
+        out[arm] = {"time_s": ms_a / 1e3, "iterations": it, "true_rel_residual": r / bnorm,
+                    "rel_error_vs_fp64": float(np.linalg.norm(x - x64) / np.linalg.norm(x64)),
+                    "mode": arms[arm][5]}
+    l0 = N.kernel_launches()
+    with ClockSampler(local) as clk:
+        ms = timed(lambda: solve_dev(HEAD), args.steps, args.warmup, clk)
+        launches = (N.kernel_launches() - l0) / (args.steps + args.warmup)
+        clk.extend(lambda: solve_dev(HEAD))
+    it_h = solve_dev(HEAD)
+    xh = dx.cpu().numpy().copy()
+    out[HEAD] = {"time_s": ms / 1e3, "iterations": it_h,
+                 "true_rel_residual": float(np.linalg.norm(b_host - A.spmv(xh))) / bnorm,
+                 "rel_error_vs_fp64": float(np.linalg.norm(xh - x64) / np.linalg.norm(x64)), "mode": arms[HEAD][5]}
+    for a in out:
+        out[a]["speedup_vs_fp64"] = out["fp64"]["time_s"] / out[a]["time_s"]
+
+    # end to end through the C ABI with host buffers (pinned): rhs in, solution out
+    hb = torch.from_numpy(b_host).pin_memory()
+    hx = torch.zeros(n, dtype=torch.float64).pin_memory()
+    kind, pk, pc, prec, _, _ = arms[HEAD]
+
+    def solve_host():
+        o = opts(prec)
+        o.start = 2                 # zero start, made on the device (FGMRES starts from zero)
+        st = N.load().jfg_solve(ctx.handle, kind, A.handle, pk, pc.handle, C.cast(hb.data_ptr(), C.POINTER(C.c_double)),
+                                C.cast(hx.data_ptr(), C.POINTER(C.c_double)), C.byref(o), C.byref(info))
+        ctx.check(st)
+
+    for _ in range(args.warmup):
+        solve_host()
+    reps.barrier()
+    t_e2e = time.perf_counter()
+    for _ in range(args.steps):
+        solve_host()
+    e2e_s = reps.max((time.perf_counter() - t_e2e) / args.steps)
+
+    # dominant kernel: the finest-level product with FP32 values (the V-cycle's
+    # smoothing sweeps and residuals), timed with the L2 flushed before every launch
+    ms_spmv32 = A.time_spmv(precision=1, iters=50)
+    ms_spmv64 = A.time_spmv(precision=0, iters=50)
+    b32, lay = layout_bytes(A, 4, 4)
+    b64, _ = layout_bytes(A, 8, 8)
+    gbs32 = b32 / (ms_spmv32 * 1e-3) / 1e9
+    gbs64 = b64 / (ms_spmv64 * 1e-3) / 1e9
+    csr32 = spmv_bytes(n, A.nnz, 4, 4) / (ms_spmv32 * 1e-3) / 1e9
+    csr64 = spmv_bytes(n, A.nnz, 8, 8) / (ms_spmv64 * 1e-3) / 1e9
+    peaks = _peaks()
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+
+    q2 = None
+    if not args.no_q2:
+        q2 = q2_extra(ctx, reps, stream, args)
+
+    cpu = None
+    if rank == 0 and world == 1 and os.environ.get("JFEM_BENCH_NO_CPU") != "1":
+        cpu = cpu_baseline(ks.h, tol)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": ms / 1e3,
+            "unit": "s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms,
+            "higher_is_better": False,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "bf16+f32+f64",
+            "data": "synthetic (seeded GRF kappa and sine-mode source, assembled Q1 system)",
+            "config": {"workload": KAPPA_WORKLOAD, "dofs": n, "nnz": int(A.nnz), "levels": L,
+                       "smoother": "Jacobi 2+2 omega=2/3", "coarse": "dense FP64 inverse 25x25",
+                       "network": "6-layer 3x3 conv, 32 channels, BF16 weights, FP32 accumulation",
+                       "l2": "solve working set larger than L2 (FP64 finest matrix + hierarchy + vectors); "
+                             "roofline SpMV timed with the L2 flushed before each launch",
+                       "parallelism": f"replicas{world}"},
+            "iterations": it_h,
+            "final_rel_residual": out[HEAD]["true_rel_residual"],
+            "rel_error_vs_fp64": out[HEAD]["rel_error_vs_fp64"],
+            "mode": arms[HEAD][5],
+            "speedup_vs_fp64": out["fp64"]["time_s"] / (ms / 1e3),
+            "fp64_time_s": out["fp64"]["time_s"],
+            "arms": out,
+            "spmv_gbs": {"fp64": gbs64, "fp32": gbs32, "fp64_csr_equivalent": csr64, "fp32_csr_equivalent": csr32,
+                         "layout": lay},
+            "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
+                    "path": "jfg_solve (C ABI), FGMRES + V-cycle + network, pinned host rhs in and solution out"},
+            "gpu_launches": int(round(launches)),
+            "roofline": {"bound": "hbm", "achieved": gbs32, "peak": peak, "unit": "GB/s", "frac": gbs32 / peak,
+                         "traffic": None,
+                         "kernel": "k_spmv_st<float> (values-only 9-point stencil), finest level",
+                         "peak_source": peak_src, "bytes_per_launch": b32, "ms_per_launch": ms_spmv32},
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+            "q2_512_gmg_pcg": q2,
+            "setup_s": setup_s,
+        }
+        if KAPPA_TRAFFIC.get("case") == (n, int(A.nnz)):
+            line["roofline"]["traffic"] = KAPPA_TRAFFIC["bytes"]
+            line["roofline"]["traffic_source"] = KAPPA_TRAFFIC["source"]
+        print(json.dumps(line))
+    reps.close()
+
+
+# DRAM bytes (read + write) of one cold launch of the FP32 finest-level product
+# of the kappa workload, from an ncu capture of that launch (not measured by
+# this script); empty until captured.
+KAPPA_TRAFFIC = {}
+
+
+def q2_extra(ctx, reps, stream, args):
+    """The Q2 512x512 -Lap u + 5u = f GMG-PCG (FP64 and FP64 PCG + FP32
+    V-cycle, from e0), timed like the arms of the main line."""
+    import ctypes as C
+    import torch
+    from jfem_b200 import _native as N
+    from jfem_b200.linalg import DeviceMatrix
+    from jfem_b200.multigrid import JacobiSmoother, MGPreconditioner
+    h = build_problem(CELLS, LEVELS)
+    mats = [DeviceMatrix(s.n, s.n, s.rows, s.cols, s.vals, ctx) for s in h.systems]
+    prol = [DeviceMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l], ctx) for l in range(LEVELS - 1)]
+    mg = MGPreconditioner(mats, prol, h.boundary, [None] + [JacobiSmoother(2, 2 / 3)] * (LEVELS - 1), cycles=1,
+                          use_fmg=False, precision="mixed", ctx=ctx)
+    A = mats[-1]
+    n = A.rows
+    b = torch.from_numpy(h.finest.rhs).cuda()
+    tol = RTOL * float(np.linalg.norm(h.finest.rhs))
+    e0 = torch.zeros(n, dtype=torch.float64, device="cuda")
+    e0[0] = 1.0
+    dx = torch.empty_like(e0)
+    info = N.SolveInfo()
+    res = {}
+    for name, prec in (("fp64", N.FP64), ("mixed", N.MIXED_PRECOND)):
+        def once():
+            with torch.cuda.stream(stream):
+                dx.copy_(e0)
+            o = N.SolverOpts()
+            N.load().jfg_solver_opts_default(C.byref(o))
+            o.tol = tol
+            o.precision = prec
+            ctx.check(N.load().jfg_solve_dev(ctx.handle, N.PCG, A.handle, N.PREC_MG, mg.handle,
+                                             C.c_void_p(b.data_ptr()), C.c_void_p(dx.data_ptr()), C.byref(o),
+                                             C.byref(info)))
+        for _ in range(max(3, args.warmup)):
+            once()
+        reps.barrier()
+        torch.cuda.synchronize()
+        e_0 = torch.cuda.Event(enable_timing=True)
+        e_1 = torch.cuda.Event(enable_timing=True)
+        k = max(2, args.steps // 2)
+        e_0.record(stream)
+        for _ in range(k):
+            once()
+        e_1.record(stream)
+        e_1.synchronize()
+        res[name] = {"time_s": reps.max(e_0.elapsed_time(e_1) / k) / 1e3, "iterations": info.iterations,
+                     "final_rel_residual": info.final_residual / float(np.linalg.norm(h.finest.rhs))}
+    ms32 = A.time_spmv(precision=1, iters=20)
+    res["workload"] = WORKLOAD
+    res["speedup_mixed_vs_fp64"] = res["fp64"]["time_s"] / res["mixed"]["time_s"]
+    res["spmv_fp32_gbs"] = spmv_bytes(n, A.nnz, 4, 4) / (ms32 * 1e-3) / 1e9
+    return res
 
 
 def oracle_threads():
@@ -412,42 +730,52 @@ def oracle_threads():
     return O.set_threads(n)
 
 
-def cpu_baseline(h, tol, iters_hint):
-    """The oracle (C restatement of the reference's FP64 PCG + GMG V-cycle),
-    one host thread, on a bounded sample: 2 PCG iterations, scaled to the
-    FP64 GPU iteration count."""
+def oracle_gmg(h):
     import oracle as O
     mats = [O.CooMatrix(s.n, s.n, s.rows, s.cols, s.vals) for s in h.systems]
     prol = [O.CooMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l]) for l in range(len(h.systems) - 1)]
     mg = O.MGPreconditioner(mats, prol, h.boundary, [None] + [(O.SMOOTH_JACOBI, 2, 2.0 / 3.0)] * (len(mats) - 1),
                             cycles=1, use_fmg=False)
-    b = h.finest.rhs
-    sample = 2
+    return mats, mg
+
+
+def cpu_baseline(h, tol):
+    """The oracle (C restatement of the reference's FP64 PCG + GMG V-cycle)
+    timed on one whole solve from e0, on all host threads for the loops the
+    reference runs as parallel streams."""
+    import oracle as O
+    mats, mg = oracle_gmg(h)
     cores = oracle_threads()
     t0 = time.perf_counter()
-    O.solve_pcg(mats[-1], mg, b, tol, maxit=sample)
+    ref = O.solve_pcg(mats[-1], mg, h.finest.rhs, tol)
     t = time.perf_counter() - t0
-    per_it = t / sample
-    return {"value": per_it * max(iters_hint, 1), "unit": "s", "cores": cores, "kind": "port",
-            "sample": f"{sample} PCG iterations (incl. setup residual) scaled to {iters_hint} iterations",
-            "sample_s": t}
+    return {"value": t, "unit": "s", "cores": cores, "kind": "port",
+            "sample": f"one whole FP64 GMG-PCG solve ({ref.iterations} iterations) of the same system"}
 
 
 def run_reference(args):
+    """The reference arm: the oracle (C restatement of the reference's Java
+    FP64 GMG-PCG: COO scatter SpMV, the V-cycle with Jacobi 2+2, PCG from e0)
+    on the host cores, one whole solve per step, on the same system as the
+    default line (Q1 1024^2 kappa-GRF), or on Q2 512^2 with --workload gmg-pcg."""
     rank, world, local = dist_env()
     if world > 1 and rank != 0:
         return
-    h = build_problem(args.cells, args.levels)
     import oracle as O
-    mats = [O.CooMatrix(s.n, s.n, s.rows, s.cols, s.vals) for s in h.systems]
-    prol = [O.CooMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l]) for l in range(len(h.systems) - 1)]
-    mg = O.MGPreconditioner(mats, prol, h.boundary, [None] + [(O.SMOOTH_JACOBI, 2, 2.0 / 3.0)] * (len(mats) - 1),
-                            cycles=1, use_fmg=False)
+    if args.workload == "gmg-pcg":
+        h = build_problem(args.cells, args.levels)
+        workload, data = WORKLOAD, "synthetic (seeded sine-mode source, assembled Q2 system)"
+    else:
+        from jfem_b200 import problems
+        kc, kl = kappa_size(args)
+        h, _ = problems.kappa_hierarchy(1, kc >> (kl - 1), kl, 0.05, 1.0, kseed=KAPPA_SEED)
+        workload, data = KAPPA_WORKLOAD, "synthetic (seeded GRF kappa and sine-mode source, assembled Q1 system)"
+    mats, mg = oracle_gmg(h)
     b = h.finest.rhs
     tol = RTOL * float(np.linalg.norm(b))
     cores = oracle_threads()
-    # each step is one whole FP64 GMG-PCG solve from e0 (about 3 s on one
-    # host core for the SpMV, all cores for the restriction)
+    # each step is one whole FP64 GMG-PCG solve from e0 (the COO scatter SpMV
+    # serial as in the reference, the restriction on all cores)
     times = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
@@ -457,8 +785,8 @@ def run_reference(args):
     val = statistics.mean(times)
     line = {"metric": METRIC, "value": val, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": val * 1e3, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded sine-mode source, assembled Q2 system)",
-            "config": {"workload": WORKLOAD, "dofs": int(h.finest.n), "parallelism": "cpu"},
+            "vs_baseline": None, "dtype": "f64", "data": data,
+            "config": {"workload": workload, "dofs": int(h.finest.n), "parallelism": "cpu"},
             "impl": "reference",
             "iterations": full.iterations,
             "cpu_baseline": {"value": val, "unit": "s", "cores": cores, "kind": "port",
@@ -888,15 +1216,16 @@ def run_learned(args):
     line["spmv_gbs"] = {"fp64": spmv_bytes(ks.n, ks.A.nnz, 8, 8) / (ms64 * 1e-3) / 1e9,
                         "fp32": spmv_bytes(ks.n, ks.A.nnz, 4, 4) / (ms32 * 1e-3) / 1e9}
     if os.environ.get("JFEM_BENCH_NO_CPU") != "1":
-        line["cpu_baseline"] = cpu_baseline(ks.h, out["tol"], out["gmg_pcg_fp64"]["iterations"])
+        line["cpu_baseline"] = cpu_baseline(ks.h, out["tol"])
     print(json.dumps(line))
 
 
 def main():
     args = parse()
     if args.impl == "reference":
-        if args.workload != "gmg-pcg":
-            print(json.dumps({"impl": "reference", "unavailable": "the reference arm covers the gmg-pcg workload"}))
+        if args.workload not in ("kappa", "gmg-pcg"):
+            print(json.dumps({"impl": "reference",
+                              "unavailable": "the reference arm covers the kappa and gmg-pcg workloads"}))
             return
         run_reference(args)
     elif args.workload == "assemble":
@@ -913,8 +1242,10 @@ def main():
         run_stokes(args)
     elif args.workload == "learned":
         run_learned(args)
-    else:
+    elif args.workload == "gmg-pcg":
         run_ours(args)
+    else:
+        run_kappa(args)
 
 
 if __name__ == "__main__":

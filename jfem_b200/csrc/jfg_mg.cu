@@ -119,33 +119,35 @@ struct EpiRestrictSweep {
 };
 
 // ---------------------------------------------------------------------------
-// The bottom of the V-cycle in one launch.  Below a few thousand rows every
-// level's kernels are launch-latency bound (a few microseconds each whatever
-// their size), so the levels 0..bot run inside one thread-block cluster:
-// every phase (Jacobi sweep, residual, restriction with the fused first
-// sweep, coarse solve, prolongation + correction) is a cluster-wide loop over
-// the level's SELL slots followed by a cluster barrier.  Row sums use the
-// SpMV kernel's order (same lanes per row, same unrolling and shuffle tree),
-// so the result is bit-identical to the per-kernel V-cycle; vectors written
-// inside the kernel are read with coherent loads.
-constexpr int kBotMax = 6;                // levels handled by the cluster kernel, coarse level included
-constexpr int kBotRows = 4500;            // largest level taken into the cluster kernel
-constexpr int kBotCtas = 8;               // portable cluster size
-constexpr int kBotThreads = 1024;
+// The tail of the V-cycle in one launch.  Below a few thousand rows every
+// level's kernels are launch-latency bound (3.5-5 us each whatever their
+// size), so the levels 0..tail run inside one thread-block cluster of
+// kTailCtas CTAs.  Every matrix of those levels (A_l, the restriction R and
+// the prolongation P below each level) is copied once per launch into the
+// CTAs' shared memory as ELL slices: CTA c owns rows [c R, (c + 1) R) of
+// every matrix (R = ceil(rows / C)), stored entry-major (entry k of row t at
+// k * R + t) with 16-bit columns; padding entries are (own row, 0).  A phase
+// (Jacobi sweep, residual, restriction with the fused first sweep of the
+// coarser level, coarse FP64 solve, prolongation + correction) is one pass
+// of each thread over its rows followed by a hardware cluster barrier
+// (release / acquire at cluster scope): no software spin-wait.  Vector
+// entries of other rows are read through L2 (ld.global.cg); a row's own
+// entries are always written and read by the same thread.  Row sums run in
+// ascending column order from 0 with fused multiply-adds, as in the
+// one-thread-per-row kernels.
+constexpr int kTailMaxLevels = 8;         // coarse level included
+constexpr int kTailMaxRows = 32767;       // 16-bit columns
+constexpr int kTailThreads = 1024;
+constexpr int kTailSmemBudget = 200 * 1024;
 
-template <typename VT>
-struct BotMat {
-    const int* off;
-    const int* perm;
-    const int* col;
-    const int16_t* col16;
-    const VT* val;
-    int nslots, tpr_log2, idx16;
+struct TailMat {
+    int off_col, off_val;   // byte offsets of the column and value blocks in a CTA's package
+    int W, R, m;            // entries per row, rows per CTA, rows
 };
 
-template <typename T, typename VT>
-struct BotLevel {
-    BotMat<VT> A, R, P;       // R: restriction to level l - 1, P: prolongation from level l - 1
+template <typename T>
+struct TailLevel {
+    TailMat A, R, P;          // R: restriction to level l - 1, P: prolongation from level l - 1
     T *x, *t, *b, *r;
     const T* dinv;
     const unsigned char* mask;
@@ -153,184 +155,148 @@ struct BotLevel {
     T omega;
 };
 
-template <typename T, typename VT>
-struct BotParams {
-    BotLevel<T, VT> lv[kBotMax];
+template <typename T>
+struct TailParams {
+    TailLevel<T> lv[kTailMaxLevels];
     int top, n0, fsd;
     const double* ainv0;
     const int* done;
+    const uint4* pkg;         // C blocks of pkg_bytes each
+    int pkg_bytes;            // per CTA, a multiple of 16
 };
 
-template <typename VT>
-BotMat<VT> bot_mat(const Matrix* M, const VT* val)
+template <typename T, class Epi>
+__device__ __forceinline__ void tail_spmv(const unsigned char* sm, const TailMat& M, const T* x, const Epi& epi, int c)
 {
-    return BotMat<VT>{M->off.p, M->perm.p, M->col.p, M->col16.p, val, M->nslices * kSliceRows, M->tpr_log2,
-                      M->idx16};
-}
-
-template <typename VT, typename XT, int TPR, bool I16>
-__device__ __forceinline__ typename AccOf<VT>::T bot_row(const BotMat<VT>& m, const XT* x, int slot, int sub, int& r)
-{
-    using AT = typename AccOf<VT>::T;
-    AT sum = 0;
-    r = -1;
-    if (slot < m.nslots) {
-        const int s = slot >> 5, lane = slot & 31;
-        const int o = __ldg(m.off + s);
-        const int len = (__ldg(m.off + s + 1) - o) >> 5;
-        r = __ldg(m.perm + slot);
-        const VT* vp = m.val + o + lane;
-        const int st = 32 * TPR;
-        int k = sub;
-        if constexpr (I16) {
-            const int base = r < 0 ? 0 : r;
-            const int16_t* cp = m.col16 + o + lane;
-            for (; k + 3 * TPR < len; k += 4 * TPR) {
-                const int c0 = base + __ldg(cp + 32 * k), c1 = base + __ldg(cp + 32 * k + st);
-                const int c2 = base + __ldg(cp + 32 * k + 2 * st), c3 = base + __ldg(cp + 32 * k + 3 * st);
-                const AT v0 = to_acc(__ldg(vp + 32 * k)), v1 = to_acc(__ldg(vp + 32 * k + st));
-                const AT v2 = to_acc(__ldg(vp + 32 * k + 2 * st)), v3 = to_acc(__ldg(vp + 32 * k + 3 * st));
-                const AT x0 = (AT)x[c0], x1 = (AT)x[c1], x2 = (AT)x[c2], x3 = (AT)x[c3];
-                sum += v0 * x0;
-                sum += v1 * x1;
-                sum += v2 * x2;
-                sum += v3 * x3;
+    const uint16_t* col = reinterpret_cast<const uint16_t*>(sm + M.off_col);
+    const T* val = reinterpret_cast<const T*>(sm + M.off_val);
+    double acc[1] = {0.0};
+    for (int t = threadIdx.x; t < M.R; t += blockDim.x) {
+        const int r = c * M.R + t;
+        if (r >= M.m) break;
+        T s = 0;
+        for (int k0 = 0; k0 < M.W; k0 += 9) {
+            T v[9], xv[9];
+#pragma unroll
+            for (int u = 0; u < 9; u++) {
+                const int k = k0 + u;
+                if (k < M.W) {
+                    v[u] = val[k * M.R + t];
+                    xv[u] = __ldcg(x + col[k * M.R + t]);
+                } else {
+                    v[u] = 0;
+                    xv[u] = 0;
+                }
             }
-            for (; k < len; k += TPR) sum += to_acc(__ldg(vp + 32 * k)) * (AT)x[base + __ldg(cp + 32 * k)];
-        } else {
-            const int* cp = m.col + o + lane;
-            for (; k + 3 * TPR < len; k += 4 * TPR) {
-                const int c0 = __ldg(cp + 32 * k), c1 = __ldg(cp + 32 * k + st);
-                const int c2 = __ldg(cp + 32 * k + 2 * st), c3 = __ldg(cp + 32 * k + 3 * st);
-                const AT v0 = to_acc(__ldg(vp + 32 * k)), v1 = to_acc(__ldg(vp + 32 * k + st));
-                const AT v2 = to_acc(__ldg(vp + 32 * k + 2 * st)), v3 = to_acc(__ldg(vp + 32 * k + 3 * st));
-                const AT x0 = (AT)x[c0], x1 = (AT)x[c1], x2 = (AT)x[c2], x3 = (AT)x[c3];
-                sum += v0 * x0;
-                sum += v1 * x1;
-                sum += v2 * x2;
-                sum += v3 * x3;
-            }
-            for (; k < len; k += TPR) sum += to_acc(__ldg(vp + 32 * k)) * (AT)x[__ldg(cp + 32 * k)];
+#pragma unroll
+            for (int u = 0; u < 9; u++) s += v[u] * xv[u];
         }
-    }
-    for (int o = TPR >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-    return sum;
-}
-
-template <int TPR, bool I16, typename VT, typename XT, class Epi>
-__device__ __forceinline__ void bot_spmv_t(const BotMat<VT>& m, const XT* x, Epi epi, int gtid, int gthreads)
-{
-    const int total = m.nslots * TPR;
-    for (int base = 0; base < total; base += gthreads) {      // warp-uniform trip count
-        const int gid = base + gtid;
-        int r;
-        const auto sum = bot_row<VT, XT, TPR, I16>(m, x, gid / TPR, gid % TPR, r);
-        double acc[1] = {0.0};
-        if (gid % TPR == 0 && r >= 0) epi(r, sum, acc);
+        epi(r, s, acc);
     }
 }
 
-template <typename VT, typename XT, class Epi>
-__device__ void bot_spmv(const BotMat<VT>& m, const XT* x, Epi epi, int gtid, int gthreads)
+// own-row vector phase over the rows of level matrix A (same ownership as its products)
+template <class F>
+__device__ __forceinline__ void tail_rows(const TailMat& M, int c, F f)
 {
-    if (m.idx16) {
-        switch (m.tpr_log2) {
-        case 0: bot_spmv_t<1, true>(m, x, epi, gtid, gthreads); break;
-        case 2: bot_spmv_t<4, true>(m, x, epi, gtid, gthreads); break;
-        default: bot_spmv_t<8, true>(m, x, epi, gtid, gthreads); break;
-        }
-    } else {
-        switch (m.tpr_log2) {
-        case 0: bot_spmv_t<1, false>(m, x, epi, gtid, gthreads); break;
-        case 2: bot_spmv_t<4, false>(m, x, epi, gtid, gthreads); break;
-        default: bot_spmv_t<8, false>(m, x, epi, gtid, gthreads); break;
-        }
+    for (int t = threadIdx.x; t < M.R; t += blockDim.x) {
+        const int r = c * M.R + t;
+        if (r >= M.m) break;
+        f(r);
     }
 }
 
-template <typename T, typename VT>
-__global__ void __launch_bounds__(kBotThreads, 1) k_mg_bottom(const __grid_constant__ BotParams<T, VT> P)
+template <typename T>
+__global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_constant__ TailParams<T> P)
 {
+    extern __shared__ __align__(16) unsigned char sm[];
+    cg::cluster_group cl = cg::this_cluster();
+    const int c = (int)cl.block_rank();
+    // the matrices do not change after set-up: copy them before waiting for the preceding kernel
+    {
+        const uint4* src = P.pkg + (size_t)c * (P.pkg_bytes / 16);
+        uint4* dst = reinterpret_cast<uint4*>(sm);
+        for (int i = threadIdx.x; i < P.pkg_bytes / 16; i += blockDim.x) dst[i] = __ldg(src + i);
+    }
+    __syncthreads();
     pdl_wait();
     if (P.done && *P.done) return;           // the same answer for every CTA of the cluster
-    cg::cluster_group cl = cg::this_cluster();
-    const int gthreads = (int)cl.num_blocks() * blockDim.x;
-    const int gtid = (int)cl.block_rank() * blockDim.x + threadIdx.x;
     bool fsd = P.fsd != 0;
     for (int l = P.top; l >= 1; l--) {
-        const BotLevel<T, VT>& L = P.lv[l];
+        const TailLevel<T>& L = P.lv[l];
         const T* rhs = L.b;
         T* dst = (L.runs % 2 == 1) ? L.x : L.t;
         if (!fsd) {                           // first sweep from the zero guess
-            for (int i = gtid; i < L.n; i += gthreads) dst[i] = (T)0 + (L.dinv[i] * rhs[i]) * L.omega;
+            tail_rows(L.A, c, [&](int i) { dst[i] = (T)0 + (L.dinv[i] * rhs[i]) * L.omega; });
             cl.sync();
         }
         T* cur = dst;
         T* alt = (dst == L.x) ? L.t : L.x;
         for (int k = 1; k < L.runs; k++) {
-            bot_spmv(L.A, cur, EpiJacobi<T>{cur, rhs, L.dinv, alt, L.omega}, gtid, gthreads);
+            tail_spmv(sm, L.A, cur, EpiJacobi<T>{cur, rhs, L.dinv, alt, L.omega}, c);
             cl.sync();
             T* tmp = cur;
             cur = alt;
             alt = tmp;
         }
         if (cur != L.x) {
-            for (int i = gtid; i < L.n; i += gthreads) L.x[i] = cur[i];
+            tail_rows(L.A, c, [&](int i) { L.x[i] = cur[i]; });
             cl.sync();
         }
-        bot_spmv(L.A, L.x, EpiResid<T>{rhs, L.r}, gtid, gthreads);
+        tail_spmv(sm, L.A, L.x, EpiResid<T>{rhs, L.r}, c);
         cl.sync();
-        const BotLevel<T, VT>& Cl = P.lv[l - 1];
+        const TailLevel<T>& Cl = P.lv[l - 1];
         if (l - 1 >= 1) {
             T* dc = (Cl.runs % 2 == 1) ? Cl.x : Cl.t;
-            bot_spmv(L.R, L.r, EpiRestrictSweep<T>{Cl.mask, Cl.b, Cl.dinv, dc, Cl.omega}, gtid, gthreads);
+            tail_spmv(sm, L.R, L.r, EpiRestrictSweep<T>{Cl.mask, Cl.b, Cl.dinv, dc, Cl.omega}, c);
             fsd = true;
         } else {
-            bot_spmv(L.R, L.r, EpiMasked<T>{Cl.mask, Cl.b}, gtid, gthreads);
+            tail_spmv(sm, L.R, L.r, EpiMasked<T>{Cl.mask, Cl.b}, c);
         }
         cl.sync();
     }
     {   // coarsest level: x0 = Ainv * b0 in FP64, one warp per row (the order of k_coarse_gemv)
         const int lane = threadIdx.x & 31;
-        const int nw = gthreads >> 5;
-        for (int row = gtid >> 5; row < P.n0; row += nw) {
+        const int nw = (int)cl.num_blocks() * (blockDim.x >> 5);
+        for (int row = c * (blockDim.x >> 5) + (threadIdx.x >> 5); row < P.n0; row += nw) {
             double s = 0;
-            for (int j = lane; j < P.n0; j += 32) s += P.ainv0[(size_t)row * P.n0 + j] * (double)P.lv[0].b[j];
+            for (int j = lane; j < P.n0; j += 32) s += P.ainv0[(size_t)row * P.n0 + j] * (double)__ldcg(P.lv[0].b + j);
             s = warp_sum(s);
             if (lane == 0) P.lv[0].x[row] = (T)s;
         }
         cl.sync();
     }
     for (int l = 1; l <= P.top; l++) {
-        const BotLevel<T, VT>& L = P.lv[l];
-        bot_spmv(L.P, P.lv[l - 1].x, EpiMaskedAdd<T>{L.mask, L.x}, gtid, gthreads);
+        const TailLevel<T>& L = P.lv[l];
+        tail_spmv(sm, L.P, P.lv[l - 1].x, EpiMaskedAdd<T>{L.mask, L.x}, c);
         cl.sync();
         T* cur = L.x;
         T* alt = L.t;
         for (int k = 0; k < L.runs; k++) {
-            bot_spmv(L.A, cur, EpiJacobi<T>{cur, L.b, L.dinv, alt, L.omega}, gtid, gthreads);
+            tail_spmv(sm, L.A, cur, EpiJacobi<T>{cur, L.b, L.dinv, alt, L.omega}, c);
             cl.sync();
             T* tmp = cur;
             cur = alt;
             alt = tmp;
         }
         if (cur != L.x) {
-            for (int i = gtid; i < L.n; i += gthreads) L.x[i] = cur[i];
+            tail_rows(L.A, c, [&](int i) { L.x[i] = cur[i]; });
             cl.sync();
         }
     }
 }
 
-template <typename T, typename VT>
-void launch_bottom(const BotParams<T, VT>& p, cudaStream_t st)
+template <typename T>
+void launch_tail(const TailParams<T>& p, int ctas, cudaStream_t st)
 {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(kBotCtas);
-    cfg.blockDim = dim3(kBotThreads);
+    cfg.gridDim = dim3(ctas);
+    cfg.blockDim = dim3(kTailThreads);
+    cfg.dynamicSmemBytes = (size_t)p.pkg_bytes;
     cfg.stream = st;
     cudaLaunchAttribute at[2];
     at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = kBotCtas;
+    at[0].val.clusterDim.x = ctas;
     at[0].val.clusterDim.y = 1;
     at[0].val.clusterDim.z = 1;
     int na = 1;
@@ -341,8 +307,35 @@ void launch_bottom(const BotParams<T, VT>& p, cudaStream_t st)
     }
     cfg.attrs = at;
     cfg.numAttrs = na;
-    JFG_CUDA(cudaLaunchKernelEx(&cfg, k_mg_bottom<T, VT>, p));
+    JFG_CUDA(cudaLaunchKernelEx(&cfg, k_mg_tail<T>, p));
     note_launch();
+}
+
+// Largest cluster (16, else 8 CTAs) that can be resident with `smem` bytes
+// of dynamic shared memory per CTA; 0 when none can.
+template <typename T>
+int tail_cluster_size(size_t smem)
+{
+    // the same cap for every hierarchy (the attribute belongs to the kernel, not to one launch)
+    JFG_CUDA(cudaFuncSetAttribute(k_mg_tail<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTailSmemBudget));
+    JFG_CUDA(cudaFuncSetAttribute(k_mg_tail<T>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    for (int ctas : {16, 8}) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(ctas);
+        cfg.blockDim = dim3(kTailThreads);
+        cfg.dynamicSmemBytes = smem;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = ctas;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int nc = 0;
+        if (cudaOccupancyMaxActiveClusters(&nc, k_mg_tail<T>, &cfg) == cudaSuccess && nc >= 1) return ctas;
+        cudaGetLastError();
+    }
+    return 0;
 }
 
 }  // namespace
@@ -483,20 +476,129 @@ void MGImpl<T>::init(Context* ctx, int levels, Matrix* const* As, Matrix* const*
     zero_flag.alloc(1);
     JFG_CUDA(cudaMemsetAsync(flags.p, 0, sizeof(int) * L, st));
     JFG_CUDA(cudaMemsetAsync(zero_flag.p, 0, sizeof(int), st));
-    // JFEM_MG_BOTTOM=1: levels 1..bot (all small, Jacobi-smoothed) and the
-    // coarse solve run as one cluster kernel.  Off by default: on the Q2 512^2
-    // hierarchy it replaces ~19 launches per V-cycle but is ~26 us slower per
-    // V-cycle, because one 8-SM cluster hides far less load latency than the
-    // whole GPU does per launch.
-    bot = -1;
-    const char* eb = getenv("JFEM_MG_BOTTOM");
-    if (eb && eb[0] == '1' && !vfp16) {
-        for (int l = 1; l < L - 1 && l < kBotMax; l++) {
-            if (n[l] > kBotRows || sm[l].kind != JFG_SMOOTH_JACOBI || sm[l].runs < 1) break;
-            bot = l;
-        }
+    build_tail();
+    JFG_CUDA(cudaStreamSynchronize(st));
+}
+
+// Host copy of a matrix's merged CSR.
+static void csr_to_host(const Matrix* M, std::vector<int>& hp, std::vector<int>& hc, std::vector<double>& hv,
+                        cudaStream_t st)
+{
+    hp.assign(M->rows + 1, 0);
+    hc.assign((size_t)M->nnz + 1, 0);
+    hv.assign((size_t)M->nnz + 1, 0.0);
+    JFG_CUDA(cudaMemcpyAsync(hp.data(), M->csr_ptr.p, sizeof(int) * (M->rows + 1), cudaMemcpyDeviceToHost, st));
+    if (M->nnz) {
+        JFG_CUDA(cudaMemcpyAsync(hc.data(), M->csr_col.p, sizeof(int) * M->nnz, cudaMemcpyDeviceToHost, st));
+        JFG_CUDA(cudaMemcpyAsync(hv.data(), M->csr_val.p, sizeof(double) * M->nnz, cudaMemcpyDeviceToHost, st));
     }
     JFG_CUDA(cudaStreamSynchronize(st));
+}
+
+// Picks the levels 0..tail of the one-launch V-cycle tail (k_mg_tail) and
+// builds its shared-memory package: the largest top level such that the
+// levels 1..top are Jacobi-smoothed, have at most kTailMaxRows rows, lie
+// below the finest level, and all their ELL slices fit kTailSmemBudget bytes
+// per CTA of a resident cluster.  JFEM_MG_TAIL=0 turns it off.
+template <typename T>
+void MGImpl<T>::build_tail()
+{
+    tail = -1;
+    const char* e = getenv("JFEM_MG_TAIL");
+    if (e && e[0] == '0') return;
+    cudaStream_t st = c->stream;
+    int cand = -1;
+    for (int l = 1; l < L - 1 && l < kTailMaxLevels; l++) {
+        if (n[l] > kTailMaxRows || sm[l].kind != JFG_SMOOTH_JACOBI || sm[l].runs < 1) break;
+        cand = l;
+    }
+    if (cand < 1) return;
+    // the matrices of levels 1..cand on the host; values as the V-cycle's products read them
+    struct HostMat {
+        std::vector<int> p, c;
+        std::vector<double> v;
+        int rows = 0, W = 0;
+    };
+    auto rounded = [&](const Matrix* M, double a) -> double {
+        if constexpr (std::is_same<T, float>::value) {
+            if (vbf16) return (double)__bfloat162float(__float2bfloat16_rn((float)a));
+            if (vfp16) {
+                const double sc = 1.0 / (double)M->hscale_inv;          // 2^k of this matrix
+                return (double)__half2float(__double2half(a * sc)) / sc;
+            }
+            return (double)(float)a;
+        }
+        return a;
+    };
+    std::vector<HostMat> hm(3 * (cand + 1));      // per level: A, R (to l-1), P (from l-1)
+    auto load = [&](HostMat& h, const Matrix* M) {
+        csr_to_host(M, h.p, h.c, h.v, st);
+        h.rows = M->rows;
+        h.W = 1;
+        for (int r = 0; r < M->rows; r++) h.W = std::max(h.W, h.p[r + 1] - h.p[r]);
+        for (int r = 0; r < M->rows; r++)
+            for (int k = h.p[r]; k < h.p[r + 1]; k++) h.v[k] = rounded(M, h.v[k]);
+    };
+    for (int l = 1; l <= cand; l++) {
+        load(hm[3 * l], A[l]);
+        load(hm[3 * l + 1], R[l - 1]);
+        load(hm[3 * l + 2], P[l - 1]);
+    }
+    auto al16 = [](size_t b) { return (b + 15) / 16 * 16; };
+    auto bytes_for = [&](int top, int C) {
+        size_t b = 0;
+        for (int l = 1; l <= top; l++)
+            for (int j = 0; j < 3; j++) {
+                const HostMat& h = hm[3 * l + j];
+                const size_t R = (size_t)((h.rows + C - 1) / C);
+                b += al16(R * h.W * 2) + al16(R * h.W * sizeof(T));
+            }
+        return b;
+    };
+    int top = cand, C = 0;
+    for (; top >= 1; top--) {
+        size_t b16 = bytes_for(top, 16);
+        if (b16 > (size_t)kTailSmemBudget) continue;
+        C = tail_cluster_size<T>(b16);
+        if (C == 8 && bytes_for(top, 8) > (size_t)kTailSmemBudget) C = 0;
+        if (C) break;
+    }
+    if (top < 1 || !C) return;
+    const size_t blk = bytes_for(top, C);
+    std::vector<unsigned char> pkg(blk * C, 0);
+    tail_meta.assign(15 * (top + 1), 0);
+    size_t off = 0;
+    for (int l = 1; l <= top; l++)
+        for (int j = 0; j < 3; j++) {
+            const HostMat& h = hm[3 * l + j];
+            const int R = (h.rows + C - 1) / C;
+            const size_t bc = al16((size_t)R * h.W * 2), bv = al16((size_t)R * h.W * sizeof(T));
+            int* meta = &tail_meta[15 * l + 5 * j];
+            meta[0] = (int)off;
+            meta[1] = (int)(off + bc);
+            meta[2] = h.W;
+            meta[3] = R;
+            meta[4] = h.rows;
+            for (int cc = 0; cc < C; cc++) {
+                uint16_t* col = reinterpret_cast<uint16_t*>(pkg.data() + cc * blk + off);
+                T* val = reinterpret_cast<T*>(pkg.data() + cc * blk + off + bc);
+                for (int t = 0; t < R; t++) {
+                    const int r = cc * R + t;
+                    const int a = r < h.rows ? h.p[r] : 0, len = r < h.rows ? h.p[r + 1] - h.p[r] : 0;
+                    for (int k = 0; k < h.W; k++) {
+                        col[(size_t)k * R + t] = (uint16_t)(k < len ? h.c[a + k] : 0);
+                        val[(size_t)k * R + t] = (T)(k < len ? h.v[a + k] : 0.0);
+                    }
+                }
+            }
+            off += bc + bv;
+        }
+    tail_pkg.alloc(pkg.size() / 16);
+    JFG_CUDA(cudaMemcpyAsync(tail_pkg.p, pkg.data(), pkg.size(), cudaMemcpyHostToDevice, st));
+    JFG_CUDA(cudaStreamSynchronize(st));
+    tail_pkg_bytes = (int)blk;
+    tail_ctas = C;
+    tail = top;
 }
 
 template <typename T>
@@ -618,43 +720,38 @@ void MGImpl<T>::smooth(int l, const T* rhs, bool xzero, const Scratch& sc, const
 }
 
 template <typename T>
-void MGImpl<T>::bottom(bool first_sweep_done, const int* done, cudaStream_t st)
+void MGImpl<T>::run_tail(bool first_sweep_done, const int* done, cudaStream_t st)
 {
-    auto fill = [&](auto& p, auto vals) {
-        p.top = bot;
-        p.n0 = n[0];
-        p.fsd = first_sweep_done ? 1 : 0;
-        p.ainv0 = ainv0.p;
-        p.done = done;
-        for (int l = 0; l <= bot; l++) {
-            auto& L = p.lv[l];
-            L.A = bot_mat(A[l], vals(A[l]));
-            if (l >= 1) {
-                L.R = bot_mat(R[l - 1], vals(R[l - 1]));
-                L.P = bot_mat(P[l - 1], vals(P[l - 1]));
-            }
-            L.x = x[l].p;
-            L.t = t[l].p;
-            L.b = b[l].p;
-            L.r = r[l].p;
-            L.dinv = dinv[l].p;
-            L.mask = mask[l].p;
-            L.n = n[l];
-            L.runs = sm[l].runs;
-            L.omega = (T)sm[l].omega;
-        }
+    TailParams<T> p = {};
+    p.top = tail;
+    p.n0 = n[0];
+    p.fsd = first_sweep_done ? 1 : 0;
+    p.ainv0 = ainv0.p;
+    p.done = done;
+    p.pkg = tail_pkg.p;
+    p.pkg_bytes = tail_pkg_bytes;
+    auto mat = [&](int l, int j) {
+        const int* m = &tail_meta[15 * l + 5 * j];
+        return TailMat{m[0], m[1], m[2], m[3], m[4]};
     };
-    if constexpr (std::is_same<T, float>::value) {
-        if (vbf16) {
-            BotParams<float, __nv_bfloat16> p = {};
-            fill(p, [](const Matrix* M) { return (const __nv_bfloat16*)M->val16.p; });
-            launch_bottom(p, st);
-            return;
+    for (int l = 0; l <= tail; l++) {
+        auto& Lv = p.lv[l];
+        if (l >= 1) {
+            Lv.A = mat(l, 0);
+            Lv.R = mat(l, 1);
+            Lv.P = mat(l, 2);
         }
+        Lv.x = x[l].p;
+        Lv.t = t[l].p;
+        Lv.b = b[l].p;
+        Lv.r = r[l].p;
+        Lv.dinv = dinv[l].p;
+        Lv.mask = mask[l].p;
+        Lv.n = n[l];
+        Lv.runs = sm[l].runs;
+        Lv.omega = (T)sm[l].omega;
     }
-    BotParams<T, T> p = {};
-    fill(p, [](const Matrix* M) { return vals_of<T>(M); });
-    launch_bottom(p, st);
+    launch_tail(p, tail_ctas, st);
 }
 
 // mgStepV (MGPreconditionerInterface.java:125-198): guess in x[l] (or zero),
@@ -668,8 +765,8 @@ void MGImpl<T>::vstep(int l, const T* rhs, bool xzero, const Scratch& sc, const 
         vec_launch<0>(st, n[0], VCopy<T>{x[0].p, dest}, sc, done);
         return;
     }
-    if (l == bot && xzero && rhs == b[l].p) {    // the whole bottom of the cycle in one cluster launch
-        bottom(first_sweep_done, done, st);
+    if (l == tail && xzero && rhs == b[l].p) {   // the whole tail of the cycle in one cluster launch
+        run_tail(first_sweep_done, done, st);
         return;
     }
     if (l == 0) {

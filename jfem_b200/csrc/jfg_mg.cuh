@@ -32,7 +32,11 @@ struct MGImpl {
     int wcycle = 0;                         // apply: mgStepW (MGPreconditionerSpace.mvMulW) instead of mgStepV
     int vbf16 = 0;                          // float hierarchy: matrices read as BF16 (FP32 vectors, FP32 sums)
     int vfp16 = 0;                          // float hierarchy: matrices read as scaled FP16 (FP32 vectors, sums)
-    int bot = -1;                           // levels 0..bot run as one cluster kernel (-1: none)
+    int tail = -1;                          // levels 0..tail run as one cluster kernel (-1: none)
+    int tail_ctas = 0;                      // CTAs of that cluster
+    int tail_pkg_bytes = 0;                 // shared-memory package per CTA
+    DevBuf<uint4> tail_pkg;                 // the matrices of levels 1..tail as per-CTA ELL slices
+    std::vector<int> tail_meta;             // per level and matrix (A, R, P): offsets, width, rows per CTA, rows
     std::vector<Matrix*> A, P, R;          // A[l], P[l] : n_{l+1} x n_l, R[l] = P[l]^T
     std::vector<int> n;
     std::vector<DevBuf<T>> x, t, b, r, fr;
@@ -80,8 +84,9 @@ struct MGImpl {
     void smooth(int l, const T* rhs, bool xzero, const Scratch& sc, const int* done, cudaStream_t st,
                 bool first_sweep_done = false, T* dest = nullptr);
     void coarse(const T* rhs, T* out, const int* done, cudaStream_t st);
-    // the V-cycle below and including level `bot`, entered from the restriction above
-    void bottom(bool first_sweep_done, const int* done, cudaStream_t st);
+    // the V-cycle below and including level `tail`, entered from the restriction above
+    void run_tail(bool first_sweep_done, const int* done, cudaStream_t st);
+    void build_tail();
     void fmg_into_top(const T* defect, const Scratch& sc, const int* done, cudaStream_t st);
     int max_blocks() const;
 };
