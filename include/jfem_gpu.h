@@ -451,6 +451,26 @@ int jfg_blockdiag_create(jfg_ctx* ctx, jfg_mg* mg, int nv, int np, const double*
 int jfg_blockdiag_apply(jfg_blockdiag* b, const double* h_v, double* h_out);
 int jfg_blockdiag_free(jfg_blockdiag* b);
 
+/* ---- implicit Schur complement (DLM block solvers) ------------------- */
+/* S x = A00 x - sum_i T_i (Dinv_i (L_i x)) as a composed device operator,
+ * never formed: the Schur operator of ImplicitSchurSolver.schurMvMul
+ * (linalg/ImplicitSchurSolver.java:17-57).  A00 is n0 x n0, T_i n0 x n_i,
+ * Dinv_i n_i x n_i (the inverse of the diagonal block D_i, as a matrix), L_i
+ * n_i x n0; the matrices are borrowed (they must outlive the handle). */
+typedef struct jfg_schur jfg_schur;
+int jfg_schur_create(jfg_ctx* ctx, jfg_mat* A00, int k, jfg_mat* const* T, jfg_mat* const* Dinv,
+                     jfg_mat* const* L, jfg_schur** out);
+/* y = S x (host vectors of n0 entries). */
+int jfg_schur_apply(jfg_schur* s, const double* h_x, double* h_y);
+/* GMRES (kind JFG_GMRES) or preconditioned GMRES (JFG_PGMRES, e.g. with
+ * the dense inverse of A00 as a JFG_PREC_MATRIX preconditioner) on S, with
+ * jfg_solve's options and report; the final residual is ||b - S x||.
+ * IterativeImplicitSchur.solveSchur (linalg/IterativeImplicitSchur.java:19-23)
+ * is JFG_PGMRES to 1e-9 preconditioned by the inverse of A00. */
+int jfg_schur_solve(jfg_schur* s, int kind, int precond_kind, void* precond, const double* h_b, double* h_x,
+                    const jfg_solver_opts* opts, jfg_solve_info* info);
+int jfg_schur_free(jfg_schur* s);
+
 /* ---- dense direct solves --------------------------------------------- */
 /* x = A^-1 b for a dense row-major n x n A (partial-pivot LU on the GPU).
  * Replaces DenseMatrix.solve (linalg/DenseMatrix.java:516-519) and the JNI

@@ -10,11 +10,11 @@ from .linalg import (DenseMatrix, DeviceMatrix, GMRES, IllegalArgumentException,
                      SingularMatrixException, SparseMatrix, VectorMultiplyable)
 from .multigrid import (ForwardBackwardGaussSeidelSmoother, GaussSeidelSmoother, JacobiSmoother,
                         MGPreconditioner, RichardsonSmoother)
-from .schur import (BlockSparseMatrix, DirectSchur, ExplicitSchurSolver, IterativeExplicitSchur,
-                    RichardsonExplicitSchur)
+from .schur import (BlockSparseMatrix, DirectSchur, ExplicitSchurSolver, ImplicitSchurSolver,
+                    IterativeExplicitSchur, IterativeImplicitSchur, RichardsonExplicitSchur)
 
 __all__ = ["DenseMatrix", "DeviceMatrix", "GMRES", "IllegalArgumentException", "IterativeSolver",
            "SingularMatrixException", "SparseMatrix", "VectorMultiplyable", "JacobiSmoother",
            "MGPreconditioner", "RichardsonSmoother", "ForwardBackwardGaussSeidelSmoother", "GaussSeidelSmoother",
            "BlockSparseMatrix", "ExplicitSchurSolver", "IterativeExplicitSchur", "DirectSchur",
-           "RichardsonExplicitSchur"]
+           "RichardsonExplicitSchur", "ImplicitSchurSolver", "IterativeImplicitSchur"]

@@ -46,6 +46,7 @@ EXPORTED = [
     "jfg_schwarz_create", "jfg_schwarz_free", "jfg_schwarz_info", "jfg_schwarz_apply", "jfg_schwarz_solve",
     "jfg_schwarz_smooth", "jfg_schwarz_smooth_dev", "jfg_schwarz_local_inverse", "jfg_schwarz_time",
     "jfg_blockdiag_create", "jfg_blockdiag_apply", "jfg_blockdiag_free",
+    "jfg_schur_create", "jfg_schur_apply", "jfg_schur_solve", "jfg_schur_free",
 ]
 
 
@@ -191,6 +192,10 @@ def load():
     L.jfg_blockdiag_create.argtypes = [_P, _P, C.c_int, C.c_int, _D, C.c_int, C.POINTER(_P)]
     L.jfg_blockdiag_apply.argtypes = [_P, _D, _D]
     L.jfg_blockdiag_free.argtypes = [_P]
+    L.jfg_schur_create.argtypes = [_P, _P, C.c_int, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]
+    L.jfg_schur_apply.argtypes = [_P, _D, _D]
+    L.jfg_schur_solve.argtypes = [_P, C.c_int, C.c_int, _P, _D, _D, C.POINTER(SolverOpts), C.POINTER(SolveInfo)]
+    L.jfg_schur_free.argtypes = [_P]
     _lib = L
     return L
 

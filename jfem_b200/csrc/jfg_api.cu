@@ -652,11 +652,14 @@ void jfg_solver_opts_default(jfg_solver_opts* o)
     o->graph_chunk = 8;
 }
 
+// opx: solve with a composed operator (GMRES / PGMRES only) whose sizes are A's
 static int solve_impl(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, const double* d_b, double* d_x,
-                      const jfg_solver_opts* o, jfg_solve_info* info)
+                      const jfg_solver_opts* o, jfg_solve_info* info, const jfg::Operator* opx = nullptr)
 {
     using namespace jfg;
     JFG_CHECK(A && A->ctx == ctx, JFG_ERR_BAD_ARG, "matrix from another context");
+    JFG_CHECK(!opx || kind == JFG_GMRES || kind == JFG_PGMRES, JFG_ERR_UNSUPPORTED,
+              "a composed operator is solved with GMRES or PGMRES");
     Matrix* M = A->m;
     JFG_CHECK(M->rows == M->cols, JFG_ERR_BAD_ARG, "matrix is not square");
     JFG_CHECK(kind >= JFG_CG && kind <= JFG_FGMRES, JFG_ERR_BAD_ARG, "unknown solver kind");
@@ -846,15 +849,15 @@ static int solve_impl(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, cons
         h.restart_len = o->restart > 0 ? o->restart : 150;
         h.status = JFG_NOT_CONVERGED;
         JFG_CUDA(cudaMemcpyAsync(w.ctl.p, &h, sizeof(Ctl), cudaMemcpyHostToDevice, st));
-        restarts = run_gmres(w, M, P64, d_b, d_x, h.restart_len, o->max_restarts >= 0 ? o->max_restarts : 200,
-                             use_graph, chunk);
+        restarts = run_gmres(w, opx ? *opx : op_of(M), P64, d_b, d_x, h.restart_len,
+                             o->max_restarts >= 0 ? o->max_restarts : 200, use_graph, chunk);
         JFG_CUDA(cudaMemcpyAsync(&res, w.ctl.p, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
         JFG_CUDA(cudaStreamSynchronize(st));
     }
     // FP64 true residual ||b - A x||
     double* r = w.v64[10].p;
-    spmv_launch<double, double, 1>(st, M, M->val.p, d_x, EpiResid<double>{d_b, r}, w.sc, nullptr,
-                                   FinStoreD{&w.ctl.p[1].true_res});
+    op_launch<1>(st, opx ? *opx : op_of(M), d_x, EpiResid<double>{d_b, r}, w.sc, nullptr,
+                 FinStoreD{&w.ctl.p[1].true_res});
     double ss = 0;
     JFG_CUDA(cudaMemcpyAsync(&ss, &w.ctl.p[1].true_res, sizeof(double), cudaMemcpyDeviceToHost, st));
     JFG_CUDA(cudaStreamSynchronize(st));
@@ -879,6 +882,146 @@ static int solve_impl(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, cons
     }
     (void)inner;
     return res.status == JFG_BREAKDOWN ? JFG_OK : (res.status == JFG_OK ? JFG_OK : res.status);
+}
+
+// ---------------------------------------------------------------------------
+// The implicit Schur complement S x = A00 x - sum_i T_i (Dinv_i (L_i x))
+// (ImplicitSchurSolver.schurMvMul, linalg/ImplicitSchurSolver.java:17-57)
+// ---------------------------------------------------------------------------
+struct jfg_schur {
+    jfg_ctx* ctx = nullptr;
+    jfg::Matrix* A00 = nullptr;
+    std::vector<jfg::Matrix*> T, Dinv, L;
+    jfg::DevBuf<double> y, t1, t2;
+    uint64_t uid = jfg::next_uid();
+};
+
+}  // extern "C"
+
+namespace {
+template <typename T>
+struct EpiSubFrom {  // y = y - A x   (v.addInPlace(-(T (D^-1 (L x)))), ImplicitSchurSolver.java:49-51)
+    T* y;
+    template <typename AT, int K>
+    __device__ void operator()(int r, AT s, double (&)[K]) const { y[r] = y[r] + -(T)s; }
+};
+
+void schur_apply(void* self, const double* x, double* y, const jfg::Scratch& sc, const int* done, cudaStream_t st)
+{
+    using namespace jfg;
+    auto* S = static_cast<jfg_schur*>(self);
+    spmv_launch<double, double, 0>(st, S->A00, S->A00->val.p, x, EpiStore<double>{y}, sc, done);
+    for (size_t i = 0; i < S->T.size(); i++) {
+        spmv_launch<double, double, 0>(st, S->L[i], S->L[i]->val.p, x, EpiStore<double>{S->t1.p}, sc, done);
+        spmv_launch<double, double, 0>(st, S->Dinv[i], S->Dinv[i]->val.p, S->t1.p, EpiStore<double>{S->t2.p}, sc,
+                                       done);
+        spmv_launch<double, double, 0>(st, S->T[i], S->T[i]->val.p, S->t2.p, EpiSubFrom<double>{y}, sc, done);
+    }
+}
+
+jfg::Operator schur_operator(jfg_schur* S)
+{
+    jfg::Operator o;
+    o.A = S->A00;
+    o.n = S->A00->rows;
+    o.uid = S->uid;
+    o.apply = schur_apply;
+    o.self = S;
+    o.tmp = S->y.p;
+    return o;
+}
+}  // namespace
+
+extern "C" {
+
+int jfg_schur_create(jfg_ctx* ctx, jfg_mat* A00, int k, jfg_mat* const* T, jfg_mat* const* Dinv,
+                     jfg_mat* const* L, jfg_schur** out)
+{
+    if (!ctx || !A00 || !out || k < 0 || (k > 0 && (!T || !Dinv || !L))) return JFG_ERR_BAD_ARG;
+    *out = nullptr;
+    return guard(ctx, [&]() -> int {
+        auto S = std::make_unique<jfg_schur>();
+        S->ctx = ctx;
+        JFG_CHECK(A00->ctx == ctx && A00->m->rows == A00->m->cols, JFG_ERR_BAD_ARG,
+                  "Schur block missing, from another context or not square");
+        S->A00 = A00->m;
+        const int n0 = A00->m->rows;
+        int mx = 1;
+        for (int i = 0; i < k; i++) {
+            JFG_CHECK(T[i] && Dinv[i] && L[i], JFG_ERR_BAD_ARG, "matrix does not contain necessary blocks");
+            JFG_CHECK(T[i]->ctx == ctx && Dinv[i]->ctx == ctx && L[i]->ctx == ctx, JFG_ERR_BAD_ARG,
+                      "block from another context");
+            const int ni = Dinv[i]->m->rows;
+            JFG_CHECK(Dinv[i]->m->cols == ni && L[i]->m->rows == ni && L[i]->m->cols == n0 && T[i]->m->rows == n0 &&
+                          T[i]->m->cols == ni,
+                      JFG_ERR_BAD_ARG, "block sizes do not match the partition");
+            S->T.push_back(T[i]->m);
+            S->Dinv.push_back(Dinv[i]->m);
+            S->L.push_back(L[i]->m);
+            mx = std::max(mx, ni);
+        }
+        S->y.alloc(n0 ? n0 : 1);
+        S->t1.alloc(mx);
+        S->t2.alloc(mx);
+        *out = S.release();
+        return JFG_OK;
+    });
+}
+
+int jfg_schur_apply(jfg_schur* S, const double* h_x, double* h_y)
+{
+    if (!S || !h_x || !h_y) return JFG_ERR_BAD_ARG;
+    jfg_ctx* ctx = S->ctx;
+    return guard(ctx, [&]() -> int {
+        int n = S->A00->rows;
+        int mb = S->A00->nblocks;
+        for (size_t i = 0; i < S->T.size(); i++)
+            mb = std::max({mb, S->T[i]->nblocks, S->Dinv[i]->nblocks, S->L[i]->nblocks});
+        stage_in(ctx, ctx->stage_a, h_x, n);
+        jfg::Scratch sc = ctx_scratch(ctx, mb);
+        schur_apply(S, ctx->stage_a.p, S->y.p, sc, nullptr, ctx->c.stream);
+        stage_out(ctx, S->y.p, h_y, n);
+        return JFG_OK;
+    });
+}
+
+int jfg_schur_solve(jfg_schur* S, int kind, int pk, void* ph, const double* h_b, double* h_x,
+                    const jfg_solver_opts* opts, jfg_solve_info* info)
+{
+    if (!S || !h_b || !h_x) return JFG_ERR_BAD_ARG;
+    jfg_ctx* ctx = S->ctx;
+    jfg_solver_opts o;
+    if (opts)
+        o = *opts;
+    else
+        jfg_solver_opts_default(&o);
+    if (o.start < 0 || o.start > 2) return JFG_ERR_BAD_ARG;
+    return guard(ctx, [&]() -> int {
+        int n = S->A00->rows;
+        jfg_mat A{ctx, S->A00};
+        stage_in(ctx, ctx->stage_a, h_b, n);
+        if (o.start == 0)
+            stage_in(ctx, ctx->stage_b, h_x, n);
+        else
+            ctx->stage_b.alloc(n);
+        if (o.start != 0) set_start(ctx, ctx->stage_b.p, n, o.start);
+        int mb = S->A00->nblocks;
+        for (size_t i = 0; i < S->T.size(); i++)
+            mb = std::max({mb, S->T[i]->nblocks, S->Dinv[i]->nblocks, S->L[i]->nblocks});
+        ctx_scratch(ctx, mb);
+        jfg::Operator op = schur_operator(S);
+        int st = solve_impl(ctx, kind, &A, pk, ph, ctx->stage_a.p, ctx->stage_b.p, &o, info, &op);
+        stage_out(ctx, ctx->stage_b.p, h_x, n);
+        return st;
+    });
+}
+
+int jfg_schur_free(jfg_schur* S)
+{
+    if (!S) return JFG_ERR_BAD_ARG;
+    cudaStreamSynchronize(S->ctx->c.stream);
+    delete S;
+    return JFG_OK;
 }
 
 int jfg_solve_dev(jfg_ctx* ctx, int kind, jfg_mat* A, int pk, void* ph, const double* d_b, double* d_x,

@@ -772,12 +772,17 @@ int run_bicgstab(SolverWork& w, int ci, Matrix* A, const Precond<T>& M, const T*
 int run_gmres(SolverWork& w, Matrix* A, const Precond<double>& M, const double* b, double* x, int IBR,
               int max_restarts, int use_graph, int chunk)
 {
+    return run_gmres(w, op_of(A), M, b, x, IBR, max_restarts, use_graph, chunk);
+}
+
+int run_gmres(SolverWork& w, const Operator& op, const Precond<double>& M, const double* b, double* x, int IBR,
+              int max_restarts, int use_graph, int chunk)
+{
     cudaStream_t st = w.c->stream;
     Ctl* c = w.ctl.p;
     const int* cdone = &c->cycle_done;
-    int n = A->rows;
+    int n = op.n;
     const Scratch& sc = w.sc;
-    const double* val = A->val.p;
     bool pre = M.kind != JFG_PREC_NONE;
     int m = IBR + 3;
     int ldh = IBR + 10;
@@ -801,12 +806,12 @@ int run_gmres(SolverWork& w, Matrix* A, const Precond<double>& M, const double* 
     for (;;) {
         JFG_CUDA(cudaMemsetAsync(w.H.p, 0, sizeof(double) * ldh * ldh, st));
         JFG_CUDA(cudaMemsetAsync(w.gam.p, 0, sizeof(double) * ldh, st));
-        spmv_launch<double, double, 0>(st, A, val, x, EpiResid<double>{b, pre ? t : rr}, sc, nullptr);
+        op_launch<0>(st, op, x, EpiResid<double>{b, pre ? t : rr}, sc, nullptr);
         if (pre) M.apply(t, rr, sc, nullptr, st);
         vec_launch<1>(st, n, VNorm2<double>{rr}, sc, nullptr, FinGamma0{c, w.gam.p});
         vec_launch<0>(st, n, VScaleInto2<double>{V, vcur, rr, w.gam.p}, sc, cdone);
         auto iter = [&]() {
-            spmv_launch<double, double, 0>(st, A, val, vcur, EpiStore<double>{t}, sc, cdone);
+            op_launch<0>(st, op, vcur, EpiStore<double>{t}, sc, cdone);
             if (pre) M.apply(t, q, sc, cdone, st);
             dim3 g1(gx, m);
             launch_ex(k_mdot<double>, g1, dim3(kThreads), 0, st, n, (const double*)V, qq, (const Ctl*)c,
@@ -818,7 +823,7 @@ int run_gmres(SolverWork& w, Matrix* A, const Precond<double>& M, const double* 
             vec_launch<0>(st, n, VGmresNext<double>{V, vcur, wv, w.H.p, c, n, ldh}, sc, cdone);
             scalar_launch(st, GmresAdvance{c}, cdone);
         };
-        std::vector<uintptr_t> key{3, (uintptr_t)A->uid, (uintptr_t)(M.mg ? M.mg->uid : 0), (uintptr_t)M.hook_uid, (uintptr_t)(M.M ? M.M->uid : 0), (uintptr_t)(M.mg32 ? M.mg32->uid : 0), (uintptr_t)M.r32, (uintptr_t)M.dinv,
+        std::vector<uintptr_t> key{3, (uintptr_t)op.uid, (uintptr_t)(M.mg ? M.mg->uid : 0), (uintptr_t)M.hook_uid, (uintptr_t)(M.M ? M.M->uid : 0), (uintptr_t)(M.mg32 ? M.mg32->uid : 0), (uintptr_t)M.r32, (uintptr_t)M.dinv,
                                    (uintptr_t)x, (uintptr_t)V, (uintptr_t)M.kind, (uintptr_t)m, (uintptr_t)t,
                                    (uintptr_t)q, (uintptr_t)wv, (uintptr_t)vcur, (uintptr_t)w.H.p,
                                    (uintptr_t)w.fac.p, (uintptr_t)w.mdot_part.p, (uintptr_t)cdone};
@@ -829,7 +834,7 @@ int run_gmres(SolverWork& w, Matrix* A, const Precond<double>& M, const double* 
         if (h.done) break;   // converged at the cycle start (or non-finite)
         scalar_launch(st, GmresAlpha{c, w.H.p, w.gam.p, w.alpha.p, ldh}, nullptr);
         vec_launch<0>(st, n, VGmresX<double>{x, V, w.alpha.p, c, n}, sc, nullptr);
-        spmv_launch<double, double, 1>(st, A, val, x, EpiResid<double>{b, t}, sc, nullptr, FinTrueRes{c});
+        op_launch<1>(st, op, x, EpiResid<double>{b, t}, sc, nullptr, FinTrueRes{c});
         h = read_ctl(w, 0);
         bool nonfinite = !std::isfinite(h.true_res) || h.status == JFG_NONFINITE;
         if (nonfinite) {

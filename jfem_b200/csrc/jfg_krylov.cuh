@@ -71,7 +71,51 @@ void run_cg_small(SolverWork& w, Matrix* A, const double* b, double* x);
 template <typename T>
 int run_bicgstab(SolverWork& w, int ci, Matrix* A, const Precond<T>& M, const T* b, T* x, T* const* v,
                   int use_graph, int chunk);
+// A linear operator of the GMRES loop: a matrix, or (apply set) a
+// composition of device products that writes A x into tmp -- the implicit
+// Schur complement of ImplicitSchurSolver.  A gives the sizes and the
+// product grid of the composition.
+struct Operator {
+    Matrix* A = nullptr;
+    int n = 0;
+    uint64_t uid = 0;
+    void (*apply)(void* self, const double* x, double* y, const Scratch& sc, const int* done, cudaStream_t st) = nullptr;
+    void* self = nullptr;
+    double* tmp = nullptr;
+};
+inline Operator op_of(Matrix* A)
+{
+    Operator o;
+    o.A = A;
+    o.n = A->rows;
+    o.uid = A->uid;
+    return o;
+}
+
+template <class Epi>
+struct VEpi {   // an SpMV epilogue applied to row sums already in s
+    const double* s;
+    Epi epi;
+    template <int K> __device__ void operator()(int i, double (&acc)[K]) const { epi(i, s[i], acc); }
+};
+
+// y-epilogue product with the operator: one SpMV for a matrix; the
+// composition into tmp, then the epilogue as a vector pass, for the rest.
+template <int NR, class Epi, class Fin = NoFin>
+void op_launch(cudaStream_t st, const Operator& op, const double* x, Epi epi, const Scratch& sc, const int* done,
+               Fin fin = Fin())
+{
+    if (!op.apply) {
+        spmv_launch<double, double, NR, Epi, Fin>(st, op.A, op.A->val.p, x, epi, sc, done, fin);
+        return;
+    }
+    op.apply(op.self, x, op.tmp, sc, done, st);
+    vec_launch<NR>(st, op.n, VEpi<Epi>{op.tmp, epi}, sc, done, fin);
+}
+
 int run_gmres(SolverWork& w, Matrix* A, const Precond<double>& M, const double* b, double* x, int IBR,
+              int max_restarts, int use_graph, int chunk);
+int run_gmres(SolverWork& w, const Operator& op, const Precond<double>& M, const double* b, double* x, int IBR,
               int max_restarts, int use_graph, int chunk);
 int run_mixed_cg(SolverWork& w, Matrix* A, const Precond<float>& M, const double* b, double* x, double tol,
                  int maxit, double inner_rtol, int use_graph, int chunk, int* inner_iters, double* hist, int hist_cap);

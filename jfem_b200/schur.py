@@ -31,11 +31,14 @@ from __future__ import annotations
 import numpy as np
 
 from . import _native as N
-from .linalg import (DenseMatrix, DeviceMatrix, IllegalArgumentException, IterativeSolver, SparseMatrix,
-                     VectorMultiplyable)
+import ctypes as C
+
+from .linalg import (DenseMatrix, DeviceMatrix, IllegalArgumentException, IterativeSolver, SolveResult,
+                     SparseMatrix, VectorMultiplyable)
 
 __all__ = ["BlockSparseMatrix", "AbstractSchurSolver", "ExplicitSchurSolver", "IterativeExplicitSchur",
-           "DirectSchur", "RichardsonExplicitSchur"]
+           "DirectSchur", "RichardsonExplicitSchur", "ImplicitSchurSolver", "IterativeImplicitSchur",
+           "SchurOperator"]
 
 
 def _coo_of(block):
@@ -328,3 +331,110 @@ class RichardsonExplicitSchur(ExplicitSchurSolver):
             k += 1
         self.iterations = k
         return x
+
+
+class SchurOperator(VectorMultiplyable):
+    """The implicit Schur complement S v = A00 v - sum_i T_i D_i^-1 L_i v as a
+    composed device operator (libjfem_gpu's jfg_schur): the VectorMultiplyable
+    that ImplicitSchurSolver.schurMvMul returns
+    (linalg/ImplicitSchurSolver.java:17-57); S is never formed."""
+
+    def __init__(self, solver: "AbstractSchurSolver"):
+        self.ctx = solver.ctx
+        self._keep = (solver.getSchurBlock(), [solver.getTopBlock(i) for i in range(len(solver._dinv_dev))],
+                      list(solver._dinv_dev), [solver.getLeftBlock(i) for i in range(len(solver._dinv_dev))])
+        A00, T, D, L = self._keep
+        k = len(D)
+        arr = lambda ms: (C.c_void_p * max(k, 1))(*([m.handle for m in ms] + ([None] if k == 0 else [])))
+        h = C.c_void_p()
+        st = N.load().jfg_schur_create(self.ctx.handle, A00.handle, k, arr(T), arr(D), arr(L), C.byref(h))
+        if st == N.ERR_BAD_ARG:
+            raise IllegalArgumentException(N.load().jfg_last_error(self.ctx.handle).decode())
+        self.ctx.check(st)
+        self._h = h
+        self.n = A00.rows
+
+    @property
+    def handle(self):
+        return self._h
+
+    def getVectorSize(self):
+        return self.n
+
+    def getTVectorSize(self):
+        return self.n
+
+    def mvMul(self, vector):
+        v = N.f64(vector)
+        if v.shape != (self.n,):
+            raise IllegalArgumentException("Vectors are of different size")
+        out = np.empty(self.n)
+        self.ctx.check(N.load().jfg_schur_apply(self._h, N.dptr(v), N.dptr(out)))
+        return out
+
+    def tvMul(self, vector):
+        raise NotImplementedError("not implemented yet")   # ImplicitSchurSolver.java:53-56
+
+    def solvePGMRES(self, preconditioner: DeviceMatrix, rhs, tol, it: IterativeSolver | None = None):
+        """IterativeSolver.solvePGMRES on S from zero (GMRES.java:59-60), on the GPU."""
+        b = N.f64(rhs)
+        if b.shape != (self.n,):
+            raise IllegalArgumentException("Vectors are of different size")
+        x = np.zeros(self.n)
+        it = it or IterativeSolver(ctx=self.ctx)
+        opts = N.SolverOpts()
+        N.load().jfg_solver_opts_default(C.byref(opts))
+        opts.tol = tol
+        opts.restart = it.gm.ITERATIONS_BEFORE_RESTART
+        opts.max_restarts = it.gm.MAX_RESTARTS
+        hist = np.zeros(max(it.history_cap, 1))
+        opts.h_history = N.dptr(hist)
+        opts.history_cap = it.history_cap
+        info = N.SolveInfo()
+        st = N.load().jfg_schur_solve(self._h, N.PGMRES, N.PREC_MATRIX, preconditioner.handle, N.dptr(b), N.dptr(x),
+                                      C.byref(opts), C.byref(info))
+        self.ctx.check(st, allow=(N.OK, N.NOT_CONVERGED, N.NONFINITE))
+        it.last = SolveResult(info, hist)
+        it.iterations = info.iterations
+        it.lastSolution = x
+        return x
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                N.load().jfg_schur_free(self._h)
+        except Exception:
+            pass
+
+
+class ImplicitSchurSolver(AbstractSchurSolver):
+    """linalg/ImplicitSchurSolver.java: the Schur system is solved through
+    the composed operator S v = A00 v - sum_i T_i D_i^-1 L_i v without forming
+    S (schurMvMul, lines 17-57)."""
+
+    def __init__(self, blockMatrix: BlockSparseMatrix):
+        super().__init__(blockMatrix)
+        self._op = None
+
+    def schurMvMul(self) -> SchurOperator:
+        if self._op is None:
+            self._op = SchurOperator(self)
+        return self._op
+
+
+class IterativeImplicitSchur(ImplicitSchurSolver):
+    """linalg/IterativeImplicitSchur.java: PGMRES on the implicit Schur
+    operator, preconditioned by the dense inverse of A00, to 1e-9."""
+
+    def __init__(self, blockMatrix: BlockSparseMatrix):
+        super().__init__(blockMatrix)
+        r, c, v, (n0, _) = blockMatrix.getBlockCoo(0, 0)
+        a = np.zeros((n0, n0))
+        np.add.at(a, (r, c), v)
+        inv = DenseMatrix(a, self.ctx).inverse()              # firstInverse (lines 12-14), device LU
+        ri, ci = np.nonzero(inv)
+        self.firstInverse = DeviceMatrix(n0, n0, ri, ci, inv[ri, ci], self.ctx)
+        self.it = IterativeSolver(ctx=self.ctx)
+
+    def solveSchur(self, A, b):
+        return A.solvePGMRES(self.firstInverse, b, 1e-9, self.it)

@@ -98,3 +98,38 @@ def test_missing_blocks_are_rejected(ctx):
     del blocks[(n0, 0)]
     with pytest.raises(IllegalArgumentException, match="left block"):
         DirectSchur(BlockSparseMatrix(blocks, M.shape[0], ctx=ctx))
+
+
+def test_implicit_schur_operator_and_solve(ctx):
+    """ImplicitSchurSolver (linalg/ImplicitSchurSolver.java:17-57): the
+    composed operator equals the dense Schur complement; IterativeImplicitSchur
+    (IterativeImplicitSchur.java:19-23: PGMRES with the inverse of A00, 1e-9)
+    solves the block system like the explicit solver does."""
+    from jfem_b200.schur import ImplicitSchurSolver, IterativeImplicitSchur
+    blocks, M, n0, sizes = block_system(seed=5)
+    B = BlockSparseMatrix(blocks, M.shape[0], ctx=ctx)
+    Sd = dense_schur(M, n0, sizes)
+    op = ImplicitSchurSolver(B).schurMvMul()
+    rng = np.random.default_rng(2)
+    for _ in range(2):
+        v = rng.standard_normal(n0)
+        np.testing.assert_allclose(op.mvMul(v), Sd @ v, rtol=1e-12, atol=1e-12 * np.abs(Sd @ v).max())
+    solver = IterativeImplicitSchur(B)
+    f = rng.standard_normal(M.shape[0])
+    u = solver.mvMul(f)
+    np.testing.assert_allclose(u, np.linalg.solve(M, f), rtol=1e-7, atol=1e-7 * np.abs(u).max())
+    assert solver.it.last.status == 0 and solver.it.iterations >= 1
+    # the same PGMRES on the explicit complement: same iteration count within one
+    ex = IterativeExplicitSchur(B)
+    u2 = ex.mvMul(f)
+    np.testing.assert_allclose(u2, u, rtol=1e-7, atol=1e-7 * np.abs(u).max())
+    assert abs(ex.it.iterations - solver.it.iterations) <= 1
+
+
+def test_implicit_schur_missing_block(ctx):
+    from jfem_b200.schur import IterativeImplicitSchur
+    blocks, M, n0, sizes = block_system(k=2)
+    s = n0
+    del blocks[(s, 0)]
+    with pytest.raises(IllegalArgumentException):
+        IterativeImplicitSchur(BlockSparseMatrix(blocks, M.shape[0], ctx=ctx))
