@@ -276,7 +276,7 @@ int jfg_matrix_layout(jfg_mat* m, int* stencil, int* stride, int* regular_rows, 
     if (stride) *stride = M->st ? M->st_S : 0;
     if (regular_rows) *regular_rows = M->st ? M->st_hi - M->st_lo : 0;
     if (other_rows) *other_rows = M->st ? M->st_nirr : M->rows;
-    if (other_nnz) *other_nnz = M->st ? M->st_len - 9 * (int64_t)(M->st_hi - M->st_lo) : M->nnz;
+    if (other_nnz) *other_nnz = M->st ? M->st_len - 9 * (int64_t)M->st_ld : M->nnz;
     if (fp16_scale_inv) *fp16_scale_inv = M->hash ? (double)M->hscale_inv : 0.0;
     return JFG_OK;
 }

@@ -441,33 +441,75 @@ k_spmv_pipe(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Ep
 // values-only 9-point stencil SpMV (Matrix::st)
 // ---------------------------------------------------------------------------
 struct StArgs {
-    int S, lo, nreg, nirr, nb_reg;
+    int S, lo, nreg, ld, nirr, nb_reg;
     const int* irow;
     const int* iptr;
     const int* icol;
     float vscale;          // FP16 values: factor of the row sums
 };
 
-// One thread per row.  A regular row r reads its nine values (one coalesced
-// stream per offset, no column indices) and x[r + offset] for the offsets in
-// ascending column order; the CTAs past the regular range take the
-// irregular rows from their CSR copy.  Each row is summed in ascending
-// column order from 0 with the same multiply-adds as k_spmv (a stored zero
-// adds exactly 0 for finite x), so the result equals the SELL kernels' bit
-// for bit.  PF: the values are loaded before the wait for the preceding
-// kernel (matrices that are not written after set-up).
+// RPT consecutive values of one offset stream (the group's start is a
+// multiple of RPT and the stream stride a multiple of 8 entries: aligned
+// vector loads), read once, not allocated in L1
+template <int RPT>
+__device__ __forceinline__ void ldv(const double* p, double (&o)[RPT])
+{
+    static_assert(RPT == 2, "FP64 groups are 2 rows");
+    asm("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(o[0]), "=d"(o[1]) : "l"(p));
+}
+template <int RPT>
+__device__ __forceinline__ void ldv(const float* p, float (&o)[RPT])
+{
+    static_assert(RPT == 4, "FP32 groups are 4 rows");
+    asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+        : "=f"(o[0]), "=f"(o[1]), "=f"(o[2]), "=f"(o[3])
+        : "l"(p));
+}
+template <typename H, int RPT>
+__device__ __forceinline__ void ldv16(const H* p, float (&o)[RPT])
+{
+    static_assert(RPT == 4, "16-bit groups are 4 rows");
+    unsigned a, b;
+    asm("ld.global.nc.L1::no_allocate.v2.b32 {%0, %1}, [%2];" : "=r"(a), "=r"(b) : "l"(p));
+    const H* h = reinterpret_cast<const H*>(&a);
+    const H* g = reinterpret_cast<const H*>(&b);
+    o[0] = to_acc(h[0]);
+    o[1] = to_acc(h[1]);
+    o[2] = to_acc(g[0]);
+    o[3] = to_acc(g[1]);
+}
+template <int RPT>
+__device__ __forceinline__ void ldv(const __half* p, float (&o)[RPT]) { ldv16<__half, RPT>(p, o); }
+template <int RPT>
+__device__ __forceinline__ void ldv(const __nv_bfloat16* p, float (&o)[RPT]) { ldv16<__nv_bfloat16, RPT>(p, o); }
+
+template <typename VT> __host__ __device__ constexpr int st_rows_per_thread() { return sizeof(VT) == 8 ? 2 : 4; }
+
+// Values-only stencil SpMV.  A thread takes RPT consecutive regular rows
+// (RPT = 4, or 2 for FP64 values): nine aligned vector loads of their values
+// (one per offset stream, no column indices) and three runs of RPT + 2
+// consecutive x entries (the grid lines below, at and above the rows), so
+// neighbouring rows share their x loads.  The CTAs past the regular range
+// take the irregular rows from their CSR copy, one row per thread.  Every row
+// is summed in ascending column order from 0 with the same multiply-adds as
+// k_spmv (a stored zero adds exactly 0 for finite x): the result equals the
+// SELL kernels' bit for bit.  PF: the values are loaded before the wait for
+// the preceding kernel (matrices that are not written after set-up).
 template <typename VT, typename XT, int NR, class Epi, class Fin, bool PF = false>
 __global__ void __launch_bounds__(kThreads)
 k_spmv_st(StArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi, GridRed<NR, Fin> red,
           const int* __restrict__ done)
 {
     using AT = typename AccOf<VT>::T;
+    constexpr int RPT = st_rows_per_thread<VT>();
     const bool regular = (int)blockIdx.x < m.nb_reg;
-    const int i = (regular ? (int)blockIdx.x : (int)blockIdx.x - m.nb_reg) * kThreads + threadIdx.x;
-    AT v[9];
-    if (PF && regular && i < m.nreg) {
+    const int g = (regular ? (int)blockIdx.x : (int)blockIdx.x - m.nb_reg) * kThreads + threadIdx.x;
+    const int i0 = g * RPT;
+    AT v[9][RPT];
+    const bool full = regular && i0 + RPT <= m.nreg;
+    if (PF && full) {
 #pragma unroll
-        for (int k = 0; k < 9; k++) v[k] = to_acc(ld_stream(val + (int64_t)k * m.nreg + i));
+        for (int k = 0; k < 9; k++) ldv<RPT>(val + (int64_t)k * m.ld + i0, v[k]);
     }
     pdl_wait();
     if (done && *done) return;
@@ -475,36 +517,45 @@ k_spmv_st(StArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi ep
 #pragma unroll
     for (int q = 0; q < (NR > 0 ? NR : 1); q++) acc[q] = 0;
     if (regular) {
-        if (i < m.nreg) {
+        if (full) {
             if (!PF) {
 #pragma unroll
-                for (int k = 0; k < 9; k++) v[k] = to_acc(ld_stream(val + (int64_t)k * m.nreg + i));
+                for (int k = 0; k < 9; k++) ldv<RPT>(val + (int64_t)k * m.ld + i0, v[k]);
             }
-            const int r = m.lo + i;
-            const XT* xa = x + (r - m.S - 1);
-            const XT* xc = x + (r - 1);
-            const XT* xb = x + (r + m.S - 1);
-            AT xv[9];
-            xv[0] = (AT)__ldg(xa);
-            xv[1] = (AT)__ldg(xa + 1);
-            xv[2] = (AT)__ldg(xa + 2);
-            xv[3] = (AT)__ldg(xc);
-            xv[4] = (AT)__ldg(xc + 1);
-            xv[5] = (AT)__ldg(xc + 2);
-            xv[6] = (AT)__ldg(xb);
-            xv[7] = (AT)__ldg(xb + 1);
-            xv[8] = (AT)__ldg(xb + 2);
-            AT sum = 0;
+            const int r0 = m.lo + i0;
+            AT xs[3][RPT + 2];
 #pragma unroll
-            for (int k = 0; k < 9; k++) sum += v[k] * xv[k];
-            if constexpr (std::is_same<VT, __half>::value) sum *= m.vscale;
-            epi(r, sum, acc);
+            for (int j = 0; j < 3; j++) {
+                const XT* xp = x + (r0 + (j - 1) * m.S - 1);
+#pragma unroll
+                for (int e = 0; e < RPT + 2; e++) xs[j][e] = (AT)__ldg(xp + e);
+            }
+#pragma unroll
+            for (int q = 0; q < RPT; q++) {
+                AT sum = 0;
+#pragma unroll
+                for (int k = 0; k < 9; k++) sum += v[k][q] * xs[k / 3][q + k % 3];
+                if constexpr (std::is_same<VT, __half>::value) sum *= m.vscale;
+                epi(r0 + q, sum, acc);
+            }
+        } else if (i0 < m.nreg) {           // the last, partial group: row by row
+            for (int q = 0; q < RPT && i0 + q < m.nreg; q++) {
+                const int i = i0 + q, r = m.lo + i;
+                AT sum = 0;
+#pragma unroll
+                for (int k = 0; k < 9; k++) {
+                    const int d = (k / 3 - 1) * m.S + (k % 3 - 1);
+                    sum += to_acc(val[(int64_t)k * m.ld + i]) * (AT)__ldg(x + r + d);
+                }
+                if constexpr (std::is_same<VT, __half>::value) sum *= m.vscale;
+                epi(r, sum, acc);
+            }
         }
-    } else if (i < m.nirr) {
-        const int r = m.irow[i];
-        const VT* iv = val + 9 * (int64_t)m.nreg;
+    } else if (g < m.nirr) {
+        const int r = m.irow[g];
+        const VT* iv = val + 9 * (int64_t)m.ld;
         AT sum = 0;
-        for (int k = m.iptr[i]; k < m.iptr[i + 1]; k++) sum += to_acc(iv[k]) * (AT)__ldg(x + m.icol[k]);
+        for (int k = m.iptr[g]; k < m.iptr[g + 1]; k++) sum += to_acc(iv[k]) * (AT)__ldg(x + m.icol[k]);
         if constexpr (std::is_same<VT, __half>::value) sum *= m.vscale;
         epi(r, sum, acc);
     }

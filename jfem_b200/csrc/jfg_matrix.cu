@@ -182,13 +182,13 @@ __device__ __forceinline__ int st_slot(int d, int S)
     return d <= -S + 1 ? d + S + 1 : (d >= S - 1 ? d - S + 7 : d + 4);
 }
 
-__global__ void k_st_fill(int lo, int nreg, int S, const int* __restrict__ ptr, const int* __restrict__ col,
+__global__ void k_st_fill(int lo, int nreg, int ld, int S, const int* __restrict__ ptr, const int* __restrict__ col,
                           const double* __restrict__ val, double* __restrict__ st)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nreg) return;
     const int r = lo + i;
-    for (int k = ptr[r]; k < ptr[r + 1]; k++) st[(int64_t)st_slot(col[k] - r, S) * nreg + i] = val[k];
+    for (int k = ptr[r]; k < ptr[r + 1]; k++) st[(int64_t)st_slot(col[k] - r, S) * ld + i] = val[k];
 }
 
 // CSR copy of the irregular rows (their entries in column order)
@@ -283,28 +283,31 @@ static void build_stencil(Matrix* M, const std::vector<int>& len)
             iptr.push_back(iptr.back() + len[r]);
         }
     const int64_t irr_nnz = iptr.back();
+    const int ld = (nreg + 7) / 8 * 8;
     M->st_S = S;
     M->st_lo = lo;
     M->st_hi = hi;
     M->st_nirr = nirr;
-    M->st_len = 9 * (int64_t)nreg + irr_nnz;
+    M->st_ld = ld;
+    M->st_len = 9 * (int64_t)ld + irr_nnz;
     M->st_val.alloc((size_t)M->st_len);
     M->st_irow.alloc(nirr ? (size_t)nirr : 1);
     M->st_iptr.alloc((size_t)nirr + 1);
     M->st_icol.alloc(irr_nnz ? (size_t)irr_nnz : 1);
-    JFG_CUDA(cudaMemsetAsync(M->st_val.p, 0, sizeof(double) * 9 * (size_t)nreg, s));
-    k_st_fill<<<nblk(nreg), 256, 0, s>>>(lo, nreg, S, M->csr_ptr.p, M->csr_col.p, M->csr_val.p, M->st_val.p);
+    JFG_CUDA(cudaMemsetAsync(M->st_val.p, 0, sizeof(double) * 9 * (size_t)ld, s));
+    k_st_fill<<<nblk(nreg), 256, 0, s>>>(lo, nreg, ld, S, M->csr_ptr.p, M->csr_col.p, M->csr_val.p, M->st_val.p);
     JFG_CUDA(cudaGetLastError());
     if (nirr) {
         JFG_CUDA(cudaMemcpyAsync(M->st_irow.p, irow.data(), sizeof(int) * nirr, cudaMemcpyHostToDevice, s));
         JFG_CUDA(cudaMemcpyAsync(M->st_iptr.p, iptr.data(), sizeof(int) * (nirr + 1), cudaMemcpyHostToDevice, s));
         k_st_irregular<<<nblk(nirr), 256, 0, s>>>(nirr, M->st_irow.p, M->st_iptr.p, M->csr_ptr.p, M->csr_col.p,
-                                                 M->csr_val.p, M->st_icol.p, M->st_val.p + 9 * (int64_t)nreg);
+                                                 M->csr_val.p, M->st_icol.p, M->st_val.p + 9 * (int64_t)ld);
         JFG_CUDA(cudaGetLastError());
     }
-    M->st_nb_reg = (int)nblk(nreg, kThreads);
+    M->st_nb_reg[0] = (int)nblk(nreg, kThreads * 4);      // 4 rows per thread (4- and 2-byte values)
+    M->st_nb_reg[1] = (int)nblk(nreg, kThreads * 2);      // 2 rows per thread (FP64 values)
     M->st_nb_irr = (int)nblk(nirr, kThreads);
-    M->nblocks = std::max(M->nblocks, M->st_nb_reg + M->st_nb_irr);
+    M->nblocks = std::max(M->nblocks, std::max(M->st_nb_reg[0], M->st_nb_reg[1]) + M->st_nb_irr);
     JFG_CUDA(cudaStreamSynchronize(s));
     M->st = 1;
 }

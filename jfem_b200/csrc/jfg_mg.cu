@@ -122,58 +122,88 @@ struct EpiRestrictSweep {
 // The tail of the V-cycle in one launch.  Below a few thousand rows every
 // level's kernels are launch-latency bound (3.5-5 us each whatever their
 // size), so the levels 0..tail run inside one thread-block cluster of
-// kTailCtas CTAs.  Every matrix of those levels (A_l, the restriction R and
-// the prolongation P below each level) is copied once per launch into the
-// CTAs' shared memory as ELL slices: CTA c owns rows [c R, (c + 1) R) of
-// every matrix (R = ceil(rows / C)), stored entry-major (entry k of row t at
-// k * R + t) with 16-bit columns; padding entries are (own row, 0).  A phase
-// (Jacobi sweep, residual, restriction with the fused first sweep of the
-// coarser level, coarse FP64 solve, prolongation + correction) is one pass
-// of each thread over its rows followed by a hardware cluster barrier
-// (release / acquire at cluster scope): no software spin-wait.  Vector
-// entries of other rows are read through L2 (ld.global.cg); a row's own
-// entries are always written and read by the same thread.  Row sums run in
+// C = 16 (or 8) CTAs that keeps the whole tail in distributed shared
+// memory.  CTA c owns rows [c R_l, (c + 1) R_l) of level l (R_l =
+// ceil(n_l / C)) and holds, in its shared memory:
+//   * copied once per launch (before the wait for the preceding kernel):
+//     its rows of every tail matrix -- A_l, the restriction R_l into level
+//     l - 1 and the prolongation P_l from level l - 1 -- as ELL slices
+//     (entry k of local row t at k * R + t, padding (column 0, value 0)),
+//     and its rows of the Jacobi diagonal inverse and the Dirichlet mask;
+//     a column is stored as (owning CTA << 12 | local row), so a product
+//     reads x of another CTA straight from that CTA's shared memory
+//     (mapa + ld.shared::cluster);
+//   * the level vectors x, t, b, r of its rows.
+// A phase (Jacobi sweep, residual, restriction with the fused first sweep of
+// the coarser level, coarse FP64 solve, prolongation + correction) is one
+// pass of each thread over its rows followed by a hardware cluster barrier
+// (barrier.cluster arrive.release / wait.acquire): no software spin-wait,
+// and no global-memory traffic inside the cycle.  The level entered from
+// above reads its restricted right-hand side from global memory and the
+// result x of that level is written back at the end.  Row sums run in
 // ascending column order from 0 with fused multiply-adds, as in the
 // one-thread-per-row kernels.
 constexpr int kTailMaxLevels = 8;         // coarse level included
-constexpr int kTailMaxRows = 32767;       // 16-bit columns
+constexpr int kTailMaxRowsPerCta = 4095;  // 12-bit local row of a packed column
 constexpr int kTailThreads = 1024;
 constexpr int kTailSmemBudget = 200 * 1024;
+constexpr int kTailMetaInts = 22;         // per level: A, R, P (5 each), dinv, mask, rows per CTA, x, t, b, r
 
 struct TailMat {
-    int off_col, off_val;   // byte offsets of the column and value blocks in a CTA's package
+    int off_col, off_val;   // byte offsets of the column and value blocks in a CTA's shared memory
     int W, R, m;            // entries per row, rows per CTA, rows
+    int xoff;               // byte offset of the vector the columns index (set per product)
 };
 
 template <typename T>
 struct TailLevel {
-    TailMat A, R, P;          // R: restriction to level l - 1, P: prolongation from level l - 1
-    T *x, *t, *b, *r;
-    const T* dinv;
-    const unsigned char* mask;
-    int n, runs;
+    TailMat A, R, P;          // R: restriction into level l - 1, P: prolongation from level l - 1
+    int Rl, n, runs;          // rows per CTA, rows, Jacobi sweeps
+    int off_dinv, off_mask, off_x, off_t, off_b, off_r;
     T omega;
 };
 
 template <typename T>
 struct TailParams {
     TailLevel<T> lv[kTailMaxLevels];
-    int top, n0, fsd;
+    int top, n0;
     const double* ainv0;
+    const T* b_top;           // the restricted right-hand side of level top (global)
+    T* x_top;                 // its result (global)
     const int* done;
     const uint4* pkg;         // C blocks of pkg_bytes each
-    int pkg_bytes;            // per CTA, a multiple of 16
+    int pkg_bytes;            // constant part per CTA, a multiple of 16
+    int smem_bytes;           // package + vectors
 };
 
-template <typename T, class Epi>
-__device__ __forceinline__ void tail_spmv(const unsigned char* sm, const TailMat& M, const T* x, const Epi& epi, int c)
+__device__ __forceinline__ uint32_t cluster_addr(uint32_t local, uint32_t rank)
+{
+    uint32_t a;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(local), "r"(rank));
+    return a;
+}
+__device__ __forceinline__ float ld_cluster(uint32_t a, float)
+{
+    float v;
+    asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(a) : "memory");
+    return v;
+}
+__device__ __forceinline__ double ld_cluster(uint32_t a, double)
+{
+    double v;
+    asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(a) : "memory");
+    return v;
+}
+
+// row sums of M times the distributed vector at byte offset M.xoff; f(t, s) per own row t
+template <typename T, class F>
+__device__ __forceinline__ void tail_spmv(unsigned char* sm, const TailMat& M, int c, F f)
 {
     const uint16_t* col = reinterpret_cast<const uint16_t*>(sm + M.off_col);
     const T* val = reinterpret_cast<const T*>(sm + M.off_val);
-    double acc[1] = {0.0};
+    const uint32_t xb = smem_u32(sm + M.xoff);
     for (int t = threadIdx.x; t < M.R; t += blockDim.x) {
-        const int r = c * M.R + t;
-        if (r >= M.m) break;
+        if (c * M.R + t >= M.m) break;
         T s = 0;
         for (int k0 = 0; k0 < M.W; k0 += 9) {
             T v[9], xv[9];
@@ -181,8 +211,9 @@ __device__ __forceinline__ void tail_spmv(const unsigned char* sm, const TailMat
             for (int u = 0; u < 9; u++) {
                 const int k = k0 + u;
                 if (k < M.W) {
+                    const unsigned q = col[k * M.R + t];
                     v[u] = val[k * M.R + t];
-                    xv[u] = __ldcg(x + col[k * M.R + t]);
+                    xv[u] = ld_cluster(cluster_addr(xb + (q & 0xFFFu) * (unsigned)sizeof(T), q >> 12), T());
                 } else {
                     v[u] = 0;
                     xv[u] = 0;
@@ -191,18 +222,16 @@ __device__ __forceinline__ void tail_spmv(const unsigned char* sm, const TailMat
 #pragma unroll
             for (int u = 0; u < 9; u++) s += v[u] * xv[u];
         }
-        epi(r, s, acc);
+        f(t, s);
     }
 }
 
-// own-row vector phase over the rows of level matrix A (same ownership as its products)
 template <class F>
-__device__ __forceinline__ void tail_rows(const TailMat& M, int c, F f)
+__device__ __forceinline__ void tail_own(int R, int n, int c, F f)
 {
-    for (int t = threadIdx.x; t < M.R; t += blockDim.x) {
-        const int r = c * M.R + t;
-        if (r >= M.m) break;
-        f(r);
+    for (int t = threadIdx.x; t < R; t += blockDim.x) {
+        if (c * R + t >= n) break;
+        f(t);
     }
 }
 
@@ -212,77 +241,127 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
     extern __shared__ __align__(16) unsigned char sm[];
     cg::cluster_group cl = cg::this_cluster();
     const int c = (int)cl.block_rank();
-    // the matrices do not change after set-up: copy them before waiting for the preceding kernel
+    // the matrices, diagonals and masks do not change after set-up: copy them
+    // before waiting for the preceding kernel
     {
         const uint4* src = P.pkg + (size_t)c * (P.pkg_bytes / 16);
         uint4* dst = reinterpret_cast<uint4*>(sm);
         for (int i = threadIdx.x; i < P.pkg_bytes / 16; i += blockDim.x) dst[i] = __ldg(src + i);
     }
-    __syncthreads();
     pdl_wait();
     if (P.done && *P.done) return;           // the same answer for every CTA of the cluster
-    bool fsd = P.fsd != 0;
+    auto vec = [&](int off) { return reinterpret_cast<T*>(sm + off); };
+    {   // the restricted right-hand side of the top level, own rows
+        const TailLevel<T>& L = P.lv[P.top];
+        T* b = vec(L.off_b);
+        tail_own(L.Rl, L.n, c, [&](int t) { b[t] = P.b_top[c * L.Rl + t]; });
+    }
+    __syncthreads();
     for (int l = P.top; l >= 1; l--) {
         const TailLevel<T>& L = P.lv[l];
-        const T* rhs = L.b;
-        T* dst = (L.runs % 2 == 1) ? L.x : L.t;
-        if (!fsd) {                           // first sweep from the zero guess
-            tail_rows(L.A, c, [&](int i) { dst[i] = (T)0 + (L.dinv[i] * rhs[i]) * L.omega; });
+        const T* b = vec(L.off_b);
+        const T* dinv = vec(L.off_dinv);
+        const T om = L.omega;
+        // the first sweep from the zero guess lands where the last one ends in x
+        T* cur = vec((L.runs % 2 == 1) ? L.off_x : L.off_t);
+        int cur_off = (L.runs % 2 == 1) ? L.off_x : L.off_t;
+        if (l == P.top) {   // below the top the restriction phase did it
+            tail_own(L.Rl, L.n, c, [&](int t) { cur[t] = (T)0 + (dinv[t] * b[t]) * om; });
             cl.sync();
         }
-        T* cur = dst;
-        T* alt = (dst == L.x) ? L.t : L.x;
         for (int k = 1; k < L.runs; k++) {
-            tail_spmv(sm, L.A, cur, EpiJacobi<T>{cur, rhs, L.dinv, alt, L.omega}, c);
+            const int alt_off = cur_off == L.off_x ? L.off_t : L.off_x;
+            T* alt = vec(alt_off);
+            TailMat A = L.A;
+            A.xoff = cur_off;
+            const T* cu = cur;
+            tail_spmv<T>(sm, A, c, [&](int t, T s) { alt[t] = cu[t] + (dinv[t] * (b[t] - s)) * om; });
             cl.sync();
-            T* tmp = cur;
             cur = alt;
-            alt = tmp;
+            cur_off = alt_off;
         }
-        if (cur != L.x) {
-            tail_rows(L.A, c, [&](int i) { L.x[i] = cur[i]; });
+        {   // residual r = b - A x
+            T* r = vec(L.off_r);
+            TailMat A = L.A;
+            A.xoff = L.off_x;
+            tail_spmv<T>(sm, A, c, [&](int t, T s) { r[t] = b[t] - s; });
             cl.sync();
         }
-        tail_spmv(sm, L.A, L.x, EpiResid<T>{rhs, L.r}, c);
-        cl.sync();
-        const TailLevel<T>& Cl = P.lv[l - 1];
-        if (l - 1 >= 1) {
-            T* dc = (Cl.runs % 2 == 1) ? Cl.x : Cl.t;
-            tail_spmv(sm, L.R, L.r, EpiRestrictSweep<T>{Cl.mask, Cl.b, Cl.dinv, dc, Cl.omega}, c);
-            fsd = true;
-        } else {
-            tail_spmv(sm, L.R, L.r, EpiMasked<T>{Cl.mask, Cl.b}, c);
+        {   // restriction into level l - 1 with zero boundary values (and its fused first sweep)
+            const TailLevel<T>& Cl = P.lv[l - 1];
+            TailMat R = L.R;
+            R.xoff = L.off_r;
+            T* bc = vec(Cl.off_b);
+            const unsigned char* mask = sm + Cl.off_mask;
+            if (l - 1 >= 1) {
+                const T* dc = vec(Cl.off_dinv);
+                T* xd = vec((Cl.runs % 2 == 1) ? Cl.off_x : Cl.off_t);
+                const T oc = Cl.omega;
+                tail_spmv<T>(sm, R, c, [&](int t, T s) {
+                    const T v = mask[t] ? (T)0 : s;
+                    bc[t] = v;
+                    xd[t] = (T)0 + (dc[t] * v) * oc;
+                });
+            } else {
+                tail_spmv<T>(sm, R, c, [&](int t, T s) { bc[t] = mask[t] ? (T)0 : s; });
+            }
+            cl.sync();
         }
-        cl.sync();
     }
-    {   // coarsest level: x0 = Ainv * b0 in FP64, one warp per row (the order of k_coarse_gemv)
-        const int lane = threadIdx.x & 31;
-        const int nw = (int)cl.num_blocks() * (blockDim.x >> 5);
-        for (int row = c * (blockDim.x >> 5) + (threadIdx.x >> 5); row < P.n0; row += nw) {
+    {   // coarsest level: x0 = Ainv * b0 in FP64, one warp per own row (the order of k_coarse_gemv)
+        const TailLevel<T>& L0 = P.lv[0];
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        const uint32_t bb = smem_u32(sm + L0.off_b);
+        T* x0 = vec(L0.off_x);
+        for (int t = w; t < L0.Rl; t += blockDim.x >> 5) {
+            const int row = c * L0.Rl + t;
+            if (row >= P.n0) break;
             double s = 0;
-            for (int j = lane; j < P.n0; j += 32) s += P.ainv0[(size_t)row * P.n0 + j] * (double)__ldcg(P.lv[0].b + j);
+            for (int j = lane; j < P.n0; j += 32) {
+                const int owner = j / L0.Rl, loc = j - owner * L0.Rl;
+                s += P.ainv0[(size_t)row * P.n0 + j] *
+                     (double)ld_cluster(cluster_addr(bb + loc * (unsigned)sizeof(T), owner), T());
+            }
             s = warp_sum(s);
-            if (lane == 0) P.lv[0].x[row] = (T)s;
+            if (lane == 0) x0[t] = (T)s;
         }
         cl.sync();
     }
     for (int l = 1; l <= P.top; l++) {
         const TailLevel<T>& L = P.lv[l];
-        tail_spmv(sm, L.P, P.lv[l - 1].x, EpiMaskedAdd<T>{L.mask, L.x}, c);
-        cl.sync();
-        T* cur = L.x;
-        T* alt = L.t;
+        const T* b = vec(L.off_b);
+        const T* dinv = vec(L.off_dinv);
+        const T om = L.omega;
+        {   // x += mask ? 0 : P x_{l-1}
+            T* x = vec(L.off_x);
+            const unsigned char* mask = sm + L.off_mask;
+            TailMat Pm = L.P;
+            Pm.xoff = P.lv[l - 1].off_x;
+            tail_spmv<T>(sm, Pm, c, [&](int t, T s) { x[t] = x[t] + (mask[t] ? (T)0 : s); });
+            cl.sync();
+        }
+        int cur_off = L.off_x;
         for (int k = 0; k < L.runs; k++) {
-            tail_spmv(sm, L.A, cur, EpiJacobi<T>{cur, L.b, L.dinv, alt, L.omega}, c);
+            const int alt_off = cur_off == L.off_x ? L.off_t : L.off_x;
+            const T* cu = vec(cur_off);
+            T* alt = vec(alt_off);
+            TailMat A = L.A;
+            A.xoff = cur_off;
+            tail_spmv<T>(sm, A, c, [&](int t, T s) { alt[t] = cu[t] + (dinv[t] * (b[t] - s)) * om; });
             cl.sync();
-            T* tmp = cur;
-            cur = alt;
-            alt = tmp;
+            cur_off = alt_off;
         }
-        if (cur != L.x) {
-            tail_rows(L.A, c, [&](int i) { L.x[i] = cur[i]; });
+        if (cur_off != L.off_x) {
+            const T* cu = vec(cur_off);
+            T* x = vec(L.off_x);
+            tail_own(L.Rl, L.n, c, [&](int t) { x[t] = cu[t]; });
             cl.sync();
         }
+    }
+    {   // the result of the top level back to global memory
+        const TailLevel<T>& L = P.lv[P.top];
+        const T* x = vec(L.off_x);
+        tail_own(L.Rl, L.n, c, [&](int t) { P.x_top[c * L.Rl + t] = x[t]; });
     }
 }
 
@@ -292,7 +371,7 @@ void launch_tail(const TailParams<T>& p, int ctas, cudaStream_t st)
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ctas);
     cfg.blockDim = dim3(kTailThreads);
-    cfg.dynamicSmemBytes = (size_t)p.pkg_bytes;
+    cfg.dynamicSmemBytes = (size_t)p.smem_bytes;
     cfg.stream = st;
     cudaLaunchAttribute at[2];
     at[0].id = cudaLaunchAttributeClusterDimension;
@@ -497,9 +576,10 @@ static void csr_to_host(const Matrix* M, std::vector<int>& hp, std::vector<int>&
 
 // Picks the levels 0..tail of the one-launch V-cycle tail (k_mg_tail) and
 // builds its shared-memory package: the largest top level such that the
-// levels 1..top are Jacobi-smoothed, have at most kTailMaxRows rows, lie
-// below the finest level, and all their ELL slices fit kTailSmemBudget bytes
-// per CTA of a resident cluster.  JFEM_MG_TAIL=0 turns it off.
+// levels 1..top are Jacobi-smoothed and lie below the finest level, every
+// level has at most kTailMaxRowsPerCta rows per CTA, and the package plus
+// the level vectors fit kTailSmemBudget bytes per CTA of a resident
+// cluster.  JFEM_MG_TAIL=0 turns it off.
 template <typename T>
 void MGImpl<T>::build_tail()
 {
@@ -509,94 +589,155 @@ void MGImpl<T>::build_tail()
     cudaStream_t st = c->stream;
     int cand = -1;
     for (int l = 1; l < L - 1 && l < kTailMaxLevels; l++) {
-        if (n[l] > kTailMaxRows || sm[l].kind != JFG_SMOOTH_JACOBI || sm[l].runs < 1) break;
+        if (sm[l].kind != JFG_SMOOTH_JACOBI || sm[l].runs < 1 || (n[l] + 15) / 16 > kTailMaxRowsPerCta) break;
         cand = l;
     }
     if (cand < 1) return;
-    // the matrices of levels 1..cand on the host; values as the V-cycle's products read them
     struct HostMat {
         std::vector<int> p, c;
         std::vector<double> v;
-        int rows = 0, W = 0;
+        int rows = 0, W = 1;
     };
-    auto rounded = [&](const Matrix* M, double a) -> double {
+    auto rounded = [&](const Matrix* M, double a) -> double {   // the value the level's products read
         if constexpr (std::is_same<T, float>::value) {
             if (vbf16) return (double)__bfloat162float(__float2bfloat16_rn((float)a));
             if (vfp16) {
-                const double sc = 1.0 / (double)M->hscale_inv;          // 2^k of this matrix
+                const double sc = 1.0 / (double)M->hscale_inv;
                 return (double)__half2float(__double2half(a * sc)) / sc;
             }
             return (double)(float)a;
         }
         return a;
     };
-    std::vector<HostMat> hm(3 * (cand + 1));      // per level: A, R (to l-1), P (from l-1)
+    std::vector<HostMat> hm(3 * (cand + 1));      // per level l >= 1: A_l, R (into l-1), P (from l-1)
     auto load = [&](HostMat& h, const Matrix* M) {
         csr_to_host(M, h.p, h.c, h.v, st);
         h.rows = M->rows;
-        h.W = 1;
         for (int r = 0; r < M->rows; r++) h.W = std::max(h.W, h.p[r + 1] - h.p[r]);
-        for (int r = 0; r < M->rows; r++)
-            for (int k = h.p[r]; k < h.p[r + 1]; k++) h.v[k] = rounded(M, h.v[k]);
+        for (int k = 0; k < (int)M->nnz; k++) h.v[k] = rounded(M, h.v[k]);
     };
     for (int l = 1; l <= cand; l++) {
         load(hm[3 * l], A[l]);
         load(hm[3 * l + 1], R[l - 1]);
         load(hm[3 * l + 2], P[l - 1]);
     }
+    std::vector<double> hdinv;
     auto al16 = [](size_t b) { return (b + 15) / 16 * 16; };
-    auto bytes_for = [&](int top, int C) {
-        size_t b = 0;
-        for (int l = 1; l <= top; l++)
-            for (int j = 0; j < 3; j++) {
-                const HostMat& h = hm[3 * l + j];
-                const size_t R = (size_t)((h.rows + C - 1) / C);
-                b += al16(R * h.W * 2) + al16(R * h.W * sizeof(T));
+    auto rows_per = [&](int l, int C) { return (n[l] + C - 1) / C; };
+    // byte sizes: constant package, then vectors
+    auto sizes = [&](int top, int C, size_t& pkg, size_t& total) {
+        pkg = 0;
+        for (int l = 0; l <= top; l++) {
+            const size_t Rl = (size_t)rows_per(l, C);
+            if (l >= 1) {
+                const size_t Rc = (size_t)rows_per(l - 1, C);
+                const HostMat &a = hm[3 * l], &r = hm[3 * l + 1], &p = hm[3 * l + 2];
+                pkg += al16(Rl * a.W * 2) + al16(Rl * a.W * sizeof(T));
+                pkg += al16(Rc * r.W * 2) + al16(Rc * r.W * sizeof(T));
+                pkg += al16(Rl * p.W * 2) + al16(Rl * p.W * sizeof(T));
+                pkg += al16(Rl * sizeof(T));                 // dinv
             }
-        return b;
+            pkg += al16(Rl);                                 // mask
+        }
+        total = pkg;
+        for (int l = 0; l <= top; l++) total += 4 * al16((size_t)rows_per(l, C) * sizeof(T));
     };
     int top = cand, C = 0;
+    size_t pkg_b = 0, tot_b = 0;
     for (; top >= 1; top--) {
-        size_t b16 = bytes_for(top, 16);
-        if (b16 > (size_t)kTailSmemBudget) continue;
-        C = tail_cluster_size<T>(b16);
-        if (C == 8 && bytes_for(top, 8) > (size_t)kTailSmemBudget) C = 0;
+        for (int cs : {16, 8}) {
+            if ((n[top] + cs - 1) / cs > kTailMaxRowsPerCta) continue;
+            sizes(top, cs, pkg_b, tot_b);
+            if (tot_b > (size_t)kTailSmemBudget) continue;
+            if (tail_cluster_size<T>(tot_b) >= cs) {
+                C = cs;
+                break;
+            }
+        }
         if (C) break;
     }
     if (top < 1 || !C) return;
-    const size_t blk = bytes_for(top, C);
-    std::vector<unsigned char> pkg(blk * C, 0);
-    tail_meta.assign(15 * (top + 1), 0);
+    sizes(top, C, pkg_b, tot_b);
+    // host copies of the diagonal inverses and masks
+    std::vector<std::vector<T>> dv(top + 1);
+    std::vector<std::vector<unsigned char>> mk(top + 1);
+    for (int l = 0; l <= top; l++) {
+        dv[l].resize(n[l]);
+        mk[l].resize(n[l]);
+        if (n[l]) {
+            JFG_CUDA(cudaMemcpyAsync(dv[l].data(), dinv[l].p, sizeof(T) * n[l], cudaMemcpyDeviceToHost, st));
+            JFG_CUDA(cudaMemcpyAsync(mk[l].data(), mask[l].p, n[l], cudaMemcpyDeviceToHost, st));
+        }
+    }
+    JFG_CUDA(cudaStreamSynchronize(st));
+    std::vector<unsigned char> pkg(pkg_b * C, 0);
+    tail_meta.assign(kTailMetaInts * (top + 1), 0);
     size_t off = 0;
-    for (int l = 1; l <= top; l++)
-        for (int j = 0; j < 3; j++) {
-            const HostMat& h = hm[3 * l + j];
-            const int R = (h.rows + C - 1) / C;
-            const size_t bc = al16((size_t)R * h.W * 2), bv = al16((size_t)R * h.W * sizeof(T));
-            int* meta = &tail_meta[15 * l + 5 * j];
-            meta[0] = (int)off;
-            meta[1] = (int)(off + bc);
-            meta[2] = h.W;
-            meta[3] = R;
-            meta[4] = h.rows;
-            for (int cc = 0; cc < C; cc++) {
-                uint16_t* col = reinterpret_cast<uint16_t*>(pkg.data() + cc * blk + off);
-                T* val = reinterpret_cast<T*>(pkg.data() + cc * blk + off + bc);
-                for (int t = 0; t < R; t++) {
-                    const int r = cc * R + t;
-                    const int a = r < h.rows ? h.p[r] : 0, len = r < h.rows ? h.p[r + 1] - h.p[r] : 0;
-                    for (int k = 0; k < h.W; k++) {
-                        col[(size_t)k * R + t] = (uint16_t)(k < len ? h.c[a + k] : 0);
-                        val[(size_t)k * R + t] = (T)(k < len ? h.v[a + k] : 0.0);
+    // one matrix: rows of `row_level` owned per CTA, columns packed in the ownership of `col_level`
+    auto put_mat = [&](const HostMat& h, int row_level, int col_level, int* meta) {
+        const int Rr = rows_per(row_level, C), Rc = rows_per(col_level, C);
+        const size_t bc = al16((size_t)Rr * h.W * 2), bv = al16((size_t)Rr * h.W * sizeof(T));
+        meta[0] = (int)off;
+        meta[1] = (int)(off + bc);
+        meta[2] = h.W;
+        meta[3] = Rr;
+        meta[4] = h.rows;
+        for (int cc = 0; cc < C; cc++) {
+            uint16_t* col = reinterpret_cast<uint16_t*>(pkg.data() + cc * pkg_b + off);
+            T* val = reinterpret_cast<T*>(pkg.data() + cc * pkg_b + off + bc);
+            for (int t = 0; t < Rr; t++) {
+                const int r = cc * Rr + t;
+                const int a = r < h.rows ? h.p[r] : 0, len = r < h.rows ? h.p[r + 1] - h.p[r] : 0;
+                for (int k = 0; k < h.W; k++) {
+                    uint16_t q = 0;
+                    double v = 0.0;
+                    if (k < len) {
+                        const int j = h.c[a + k];
+                        q = (uint16_t)(((j / Rc) << 12) | (j % Rc));
+                        v = h.v[a + k];
                     }
+                    col[(size_t)k * Rr + t] = q;
+                    val[(size_t)k * Rr + t] = (T)v;
                 }
             }
-            off += bc + bv;
         }
+        off += bc + bv;
+    };
+    for (int l = 0; l <= top; l++) {
+        int* meta = &tail_meta[kTailMetaInts * l];
+        const int Rl = rows_per(l, C);
+        if (l >= 1) {
+            put_mat(hm[3 * l], l, l, meta);
+            put_mat(hm[3 * l + 1], l - 1, l, meta + 5);
+            put_mat(hm[3 * l + 2], l, l - 1, meta + 10);
+            meta[15] = (int)off;                          // dinv
+            for (int cc = 0; cc < C; cc++) {
+                T* d = reinterpret_cast<T*>(pkg.data() + cc * pkg_b + off);
+                for (int t = 0; t < Rl && cc * Rl + t < n[l]; t++) d[t] = dv[l][cc * Rl + t];
+            }
+            off += al16((size_t)Rl * sizeof(T));
+        }
+        meta[16] = (int)off;                              // mask
+        for (int cc = 0; cc < C; cc++)
+            for (int t = 0; t < Rl && cc * Rl + t < n[l]; t++) pkg[cc * pkg_b + off + t] = mk[l][cc * Rl + t];
+        off += al16((size_t)Rl);
+        meta[17] = Rl;
+    }
+    JFG_CHECK(off == pkg_b, JFG_ERR_CUDA, "tail package layout mismatch");
+    for (int l = 0; l <= top; l++) {                      // vectors x, t, b, r
+        int* meta = &tail_meta[kTailMetaInts * l];
+        const size_t vb = al16((size_t)rows_per(l, C) * sizeof(T));
+        for (int q = 0; q < 4; q++) {
+            meta[18 + q] = (int)off;
+            off += vb;
+        }
+    }
+    JFG_CHECK(off == tot_b, JFG_ERR_CUDA, "tail vector layout mismatch");
     tail_pkg.alloc(pkg.size() / 16);
     JFG_CUDA(cudaMemcpyAsync(tail_pkg.p, pkg.data(), pkg.size(), cudaMemcpyHostToDevice, st));
     JFG_CUDA(cudaStreamSynchronize(st));
-    tail_pkg_bytes = (int)blk;
+    tail_pkg_bytes = (int)pkg_b;
+    tail_smem_bytes = (int)tot_b;
     tail_ctas = C;
     tail = top;
 }
@@ -722,31 +863,30 @@ void MGImpl<T>::smooth(int l, const T* rhs, bool xzero, const Scratch& sc, const
 template <typename T>
 void MGImpl<T>::run_tail(bool first_sweep_done, const int* done, cudaStream_t st)
 {
+    (void)first_sweep_done;     // the tail redoes the top level's first sweep from b
     TailParams<T> p = {};
     p.top = tail;
     p.n0 = n[0];
-    p.fsd = first_sweep_done ? 1 : 0;
     p.ainv0 = ainv0.p;
+    p.b_top = b[tail].p;
+    p.x_top = x[tail].p;
     p.done = done;
     p.pkg = tail_pkg.p;
     p.pkg_bytes = tail_pkg_bytes;
-    auto mat = [&](int l, int j) {
-        const int* m = &tail_meta[15 * l + 5 * j];
-        return TailMat{m[0], m[1], m[2], m[3], m[4]};
-    };
+    p.smem_bytes = tail_smem_bytes;
     for (int l = 0; l <= tail; l++) {
+        const int* m = &tail_meta[kTailMetaInts * l];
         auto& Lv = p.lv[l];
-        if (l >= 1) {
-            Lv.A = mat(l, 0);
-            Lv.R = mat(l, 1);
-            Lv.P = mat(l, 2);
-        }
-        Lv.x = x[l].p;
-        Lv.t = t[l].p;
-        Lv.b = b[l].p;
-        Lv.r = r[l].p;
-        Lv.dinv = dinv[l].p;
-        Lv.mask = mask[l].p;
+        Lv.A = TailMat{m[0], m[1], m[2], m[3], m[4], 0};
+        Lv.R = TailMat{m[5], m[6], m[7], m[8], m[9], 0};
+        Lv.P = TailMat{m[10], m[11], m[12], m[13], m[14], 0};
+        Lv.off_dinv = m[15];
+        Lv.off_mask = m[16];
+        Lv.Rl = m[17];
+        Lv.off_x = m[18];
+        Lv.off_t = m[19];
+        Lv.off_b = m[20];
+        Lv.off_r = m[21];
         Lv.n = n[l];
         Lv.runs = sm[l].runs;
         Lv.omega = (T)sm[l].omega;

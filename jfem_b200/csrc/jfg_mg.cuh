@@ -34,9 +34,10 @@ struct MGImpl {
     int vfp16 = 0;                          // float hierarchy: matrices read as scaled FP16 (FP32 vectors, sums)
     int tail = -1;                          // levels 0..tail run as one cluster kernel (-1: none)
     int tail_ctas = 0;                      // CTAs of that cluster
-    int tail_pkg_bytes = 0;                 // shared-memory package per CTA
+    int tail_pkg_bytes = 0;                 // constant shared-memory package per CTA
+    int tail_smem_bytes = 0;                // package + the level vectors per CTA
     DevBuf<uint4> tail_pkg;                 // the matrices of levels 1..tail as per-CTA ELL slices
-    std::vector<int> tail_meta;             // per level and matrix (A, R, P): offsets, width, rows per CTA, rows
+    std::vector<int> tail_meta;             // per level: shared-memory layout (see build_tail)
     std::vector<Matrix*> A, P, R;          // A[l], P[l] : n_{l+1} x n_l, R[l] = P[l]^T
     std::vector<int> n;
     std::vector<DevBuf<T>> x, t, b, r, fr;

@@ -154,9 +154,10 @@ void spmv_launch(cudaStream_t st, const Matrix* M, const VT* val, const XT* x, E
     GridRed<NR, Fin> red{sc.partials, sc.counter, fin};
     // the values-only stencil layout, when the matrix has one in this value type
     if (M->st && val == LayoutVals<VT>::sell(M) && LayoutVals<VT>::st(M)) {
-        StArgs sa{M->st_S, M->st_lo, M->st_hi - M->st_lo, M->st_nirr, M->st_nb_reg, M->st_irow.p, M->st_iptr.p,
+        const int nbr = M->st_nb_reg[st_rows_per_thread<VT>() == 4 ? 0 : 1];
+        StArgs sa{M->st_S, M->st_lo, M->st_hi - M->st_lo, M->st_ld, M->st_nirr, nbr, M->st_irow.p, M->st_iptr.p,
                   M->st_icol.p, std::is_same<VT, __half>::value ? M->hscale_inv : 1.0f};
-        launch_ex(k_spmv_st<VT, XT, NR, Epi, Fin, PF>, dim3(M->st_nb_reg + M->st_nb_irr), dim3(kThreads), 0, st, sa,
+        launch_ex(k_spmv_st<VT, XT, NR, Epi, Fin, PF>, dim3(nbr + M->st_nb_irr), dim3(kThreads), 0, st, sa,
                   LayoutVals<VT>::st(M), x, epi, red, done);
         return;
     }
