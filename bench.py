@@ -65,6 +65,10 @@ def parse():
                     choices=["kappa", "gmg-pcg", "cg-small", "batch-heat", "stokes", "learned", "galerkin", "gs-pcg",
                              "assemble"])
     ap.add_argument("--no-q2", action="store_true", help="kappa workload: skip the Q2 512x512 extra keys")
+    ap.add_argument("--batch-systems", type=int, default=256,
+                    help="batch-heat: number of systems (the configuration has 256; fewer only for profiling)")
+    ap.add_argument("--heat-steps", type=int, default=50,
+                    help="batch-heat: implicit-Euler steps (the configuration has 50; fewer only for profiling)")
     ap.add_argument("--profile", default=None,
                     choices=["solve-fp64", "solve-mixed", "solve-mixed-nograph", "gs-mixed-nograph", "spmv64", "spmv32",
                              "solve-learned", "solve-learned-nograph", "solve-fp64-nograph"],
@@ -1038,12 +1042,12 @@ def run_batch_heat(args):
     from jfem_b200.batch import BatchedParabolicIntegrator
     from jfem_b200.linalg import DeviceMatrix
     ctx = N.default_context()
-    batch = problems.heat_batch(nsys=256, dt=1e-3, seed=0)
+    batch = problems.heat_batch(nsys=args.batch_systems, dt=1e-3, seed=0)
     K = [DeviceMatrix(s.K.n, s.K.n, s.K.rows, s.K.cols, s.K.vals, ctx) for s in batch]
     M = [DeviceMatrix(s.M.n, s.M.n, s.M.rows, s.M.cols, s.M.vals, ctx) for s in batch]
     B = BatchedParabolicIntegrator(K, M, ctx)
     u0 = B.pack([s.u0 for s in batch])
-    steps = 50
+    steps = args.heat_steps
     for _ in range(max(3, args.warmup)):
         B.timeSteps(u0, steps)
     ms = []
@@ -1060,7 +1064,7 @@ def run_batch_heat(args):
     cpu = None
     if os.environ.get("JFEM_BENCH_NO_CPU") != "1":
         import oracle as O
-        pick = list(range(0, 256, 32))
+        pick = list(range(0, len(batch), 32))
         t0 = time.perf_counter()
         n_s = 0
         for i in pick:
@@ -1072,14 +1076,16 @@ def run_batch_heat(args):
             n_s += s.K.n
         t = time.perf_counter() - t0
         cpu = {"value": t / n_s * dofs * steps, "unit": "s", "cores": 1, "kind": "port",
-               "sample": f"one CG step (1e-10) of {len(pick)} systems, scaled by unknowns to 256 systems x 50 steps; "
+               "sample": f"one CG step (1e-10) of {len(pick)} systems, scaled by unknowns to {len(batch)} systems x "
+                         f"{steps} steps; "
                          "serial: the reference's CG has no parallel loop"}
-    line = {"metric": "time for 50 implicit-Euler steps of 256 uneven Q1 heat systems (s)",
+    line = {"metric": f"time for {steps} implicit-Euler steps of {len(batch)} uneven Q1 heat systems (s)",
             "value": statistics.median(ms) / 1e3, "unit": "s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": statistics.median(ms), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded bumps)",
-            "config": {"workload": "batch-heat: 256 Q1 systems, cells {32..256 step 16}^2, dt=1e-3, 50 steps",
-                                   "systems": 256, "dofs": dofs, "nnz": nnz},
+            "config": {"workload": f"batch-heat: {len(batch)} Q1 systems, cells {{32..256 step 16}}^2, dt=1e-3, "
+                                   f"{steps} steps",
+                                   "systems": len(batch), "steps": steps, "dofs": dofs, "nnz": nnz},
             "kernel_ms": last.ms, "total_inner_iterations": last.total_inner_iterations,
             "max_rel_residual": last.max_rel_residual, "failed": last.failed,
             "cluster": last.cluster, "threads": last.threads, "rows_per_thread": last.rows_per_thread, "clocks": clk.summary(), "cpu_baseline": cpu}

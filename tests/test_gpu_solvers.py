@@ -349,7 +349,7 @@ def test_cg_small_cluster_path(ctx, monkeypatch, p, cells):
         assert abs(it1 - ref.iterations) <= 2 and abs(it1 - it0) <= 2
         assert rel(x1, ref.x) < 1e-8 and rel(x1, x0) < 1e-8
         # histories agree until rounding differences are amplified (as for the oracle)
-        np.testing.assert_allclose(h1[:5], h0[:5], rtol=1e-8)
+        np.testing.assert_allclose(h1[:5], h0[:5], rtol=1e-7)
     monkeypatch.setenv("JFEM_SMALL_CG_SMEM", "1")
     monkeypatch.setenv("JFEM_SMALL_CG", "1")
     s = IterativeSolver(ctx=ctx)
