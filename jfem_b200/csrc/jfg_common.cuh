@@ -137,13 +137,13 @@ struct Matrix {
     // indices at all.  The rows outside the range ("irregular", a prefix and
     // a suffix of the numbering) keep a CSR copy: st_irow / st_iptr / st_icol
     // and their values at st_val[9 * st_ld + k].  The per-offset stride st_ld
-    // is nreg rounded up to a multiple of 8, so a thread's group of rows
-    // loads its values with 8- or 16-byte vector loads.  The SELL layout is kept as
+    // is nreg rounded up to a multiple of 8, so a thread's pair of rows loads
+    // its values with one aligned vector load per offset.  The SELL layout is kept as
     // well (other kernels read it); products with a stencil copy of their
     // value type use this layout.
     int st = 0;
     int st_S = 0, st_lo = 0, st_hi = 0, st_nirr = 0, st_ld = 0;
-    int st_nb_reg[2] = {0, 0};          // CTAs of the regular rows (4 rows per thread; 2 for FP64 values)
+    int st_nb_reg = 0;                  // CTAs of the regular rows (a persistent grid over row pairs)
     int st_nb_irr = 0;                  // CTAs of the irregular rows
     int64_t st_len = 0;                 // 9 * st_ld + irregular entries
     DevBuf<int> st_irow, st_iptr, st_icol;

@@ -448,68 +448,63 @@ struct StArgs {
     float vscale;          // FP16 values: factor of the row sums
 };
 
-// RPT consecutive values of one offset stream (the group's start is a
-// multiple of RPT and the stream stride a multiple of 8 entries: aligned
-// vector loads), read once, not allocated in L1
-template <int RPT>
-__device__ __forceinline__ void ldv(const double* p, double (&o)[RPT])
+// Two consecutive values of one offset stream (the group's start is even and
+// the stream stride a multiple of 8 entries: aligned vector loads), read
+// once, not allocated in L1.
+__device__ __forceinline__ void ldv2(const double* p, double (&o)[2])
 {
-    static_assert(RPT == 2, "FP64 groups are 2 rows");
     asm("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(o[0]), "=d"(o[1]) : "l"(p));
 }
-template <int RPT>
-__device__ __forceinline__ void ldv(const float* p, float (&o)[RPT])
+__device__ __forceinline__ void ldv2(const float* p, float (&o)[2])
 {
-    static_assert(RPT == 4, "FP32 groups are 4 rows");
-    asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
-        : "=f"(o[0]), "=f"(o[1]), "=f"(o[2]), "=f"(o[3])
-        : "l"(p));
+    asm("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(o[0]), "=f"(o[1]) : "l"(p));
 }
-template <typename H, int RPT>
-__device__ __forceinline__ void ldv16(const H* p, float (&o)[RPT])
+template <typename H>
+__device__ __forceinline__ void ldv2_16(const H* p, float (&o)[2])
 {
-    static_assert(RPT == 4, "16-bit groups are 4 rows");
-    unsigned a, b;
-    asm("ld.global.nc.L1::no_allocate.v2.b32 {%0, %1}, [%2];" : "=r"(a), "=r"(b) : "l"(p));
+    unsigned a;
+    asm("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(a) : "l"(p));
     const H* h = reinterpret_cast<const H*>(&a);
-    const H* g = reinterpret_cast<const H*>(&b);
     o[0] = to_acc(h[0]);
     o[1] = to_acc(h[1]);
-    o[2] = to_acc(g[0]);
-    o[3] = to_acc(g[1]);
 }
-template <int RPT>
-__device__ __forceinline__ void ldv(const __half* p, float (&o)[RPT]) { ldv16<__half, RPT>(p, o); }
-template <int RPT>
-__device__ __forceinline__ void ldv(const __nv_bfloat16* p, float (&o)[RPT]) { ldv16<__nv_bfloat16, RPT>(p, o); }
+__device__ __forceinline__ void ldv2(const __half* p, float (&o)[2]) { ldv2_16(p, o); }
+__device__ __forceinline__ void ldv2(const __nv_bfloat16* p, float (&o)[2]) { ldv2_16(p, o); }
 
-template <typename VT> __host__ __device__ constexpr int st_rows_per_thread() { return sizeof(VT) == 8 ? 2 : 4; }
+// CTAs per SM of the regular part of k_spmv_st (a persistent grid-stride
+// loop) for 4- and 2-byte values (64 registers at most); FP64 values take 2
+constexpr int kStCtasPerSm = 4;
 
-// Values-only stencil SpMV.  A thread takes RPT consecutive regular rows
-// (RPT = 4, or 2 for FP64 values): nine aligned vector loads of their values
-// (one per offset stream, no column indices) and three runs of RPT + 2
-// consecutive x entries (the grid lines below, at and above the rows), so
-// neighbouring rows share their x loads.  The CTAs past the regular range
-// take the irregular rows from their CSR copy, one row per thread.  Every row
-// is summed in ascending column order from 0 with the same multiply-adds as
-// k_spmv (a stored zero adds exactly 0 for finite x): the result equals the
-// SELL kernels' bit for bit.  PF: the values are loaded before the wait for
-// the preceding kernel (matrices that are not written after set-up).
+// Values-only stencil SpMV.  The regular rows are taken in pairs by a
+// persistent grid of CTAs striding over the pairs: for a pair, nine aligned
+// vector loads of its values (one per offset stream, no column indices) and
+// three runs of four consecutive x entries (the grid lines below, at and
+// above the rows; the two rows share them).  The values of a thread's next
+// pair are loaded before the current pair is summed, so each thread keeps
+// two pairs of the matrix stream in flight and no CTA waits on a second
+// wave of launches.  The CTAs past the regular part take the irregular rows
+// from their CSR copy, one row per thread.  Every row is summed in ascending
+// column order from 0 with the same multiply-adds as k_spmv (a stored zero
+// adds exactly 0 for finite x): the result equals the SELL kernels' bit for
+// bit.  PF: the first pair's values are loaded before the wait for the
+// preceding kernel (matrices that are not written after set-up).
 template <typename VT, typename XT, int NR, class Epi, class Fin, bool PF = false>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, sizeof(VT) == 8 ? 2 : kStCtasPerSm)
 k_spmv_st(StArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi, GridRed<NR, Fin> red,
           const int* __restrict__ done)
 {
     using AT = typename AccOf<VT>::T;
-    constexpr int RPT = st_rows_per_thread<VT>();
     const bool regular = (int)blockIdx.x < m.nb_reg;
-    const int g = (regular ? (int)blockIdx.x : (int)blockIdx.x - m.nb_reg) * kThreads + threadIdx.x;
-    const int i0 = g * RPT;
-    AT v[9][RPT];
-    const bool full = regular && i0 + RPT <= m.nreg;
-    if (PF && full) {
+    const int npairs = (m.nreg + 1) >> 1;
+    const int stride = m.nb_reg * kThreads;
+    int g = (regular ? (int)blockIdx.x : (int)blockIdx.x - m.nb_reg) * kThreads + threadIdx.x;
+    auto full = [&](int gg) { return 2 * gg + 2 <= m.nreg; };
+    AT v[9][2];
+    bool have = false;
+    if (PF && regular && g < npairs && full(g)) {
 #pragma unroll
-        for (int k = 0; k < 9; k++) ldv<RPT>(val + (int64_t)k * m.ld + i0, v[k]);
+        for (int k = 0; k < 9; k++) ldv2(val + (int64_t)k * m.ld + 2 * g, v[k]);
+        have = true;
     }
     pdl_wait();
     if (done && *done) return;
@@ -517,30 +512,46 @@ k_spmv_st(StArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi ep
 #pragma unroll
     for (int q = 0; q < (NR > 0 ? NR : 1); q++) acc[q] = 0;
     if (regular) {
-        if (full) {
-            if (!PF) {
+        for (; g < npairs; g += stride) {
+            const int i0 = 2 * g;
+            if (full(g)) {
+                if (!have) {
 #pragma unroll
-                for (int k = 0; k < 9; k++) ldv<RPT>(val + (int64_t)k * m.ld + i0, v[k]);
-            }
-            const int r0 = m.lo + i0;
-            AT xs[3][RPT + 2];
+                    for (int k = 0; k < 9; k++) ldv2(val + (int64_t)k * m.ld + i0, v[k]);
+                }
+                const int gn = g + stride;      // prefetch the next pair's values
+                AT vn[9][2];
+                const bool haven = gn < npairs && full(gn);
+                if (haven) {
 #pragma unroll
-            for (int j = 0; j < 3; j++) {
-                const XT* xp = x + (r0 + (j - 1) * m.S - 1);
+                    for (int k = 0; k < 9; k++) ldv2(val + (int64_t)k * m.ld + 2 * gn, vn[k]);
+                }
+                const int r0 = m.lo + i0;
+                AT xs[3][4];
 #pragma unroll
-                for (int e = 0; e < RPT + 2; e++) xs[j][e] = (AT)__ldg(xp + e);
-            }
+                for (int j = 0; j < 3; j++) {
+                    const XT* xp = x + (r0 + (j - 1) * m.S - 1);
 #pragma unroll
-            for (int q = 0; q < RPT; q++) {
-                AT sum = 0;
+                    for (int e = 0; e < 4; e++) xs[j][e] = (AT)__ldg(xp + e);
+                }
 #pragma unroll
-                for (int k = 0; k < 9; k++) sum += v[k][q] * xs[k / 3][q + k % 3];
-                if constexpr (std::is_same<VT, __half>::value) sum *= m.vscale;
-                epi(r0 + q, sum, acc);
-            }
-        } else if (i0 < m.nreg) {           // the last, partial group: row by row
-            for (int q = 0; q < RPT && i0 + q < m.nreg; q++) {
-                const int i = i0 + q, r = m.lo + i;
+                for (int q = 0; q < 2; q++) {
+                    AT sum = 0;
+#pragma unroll
+                    for (int k = 0; k < 9; k++) sum += v[k][q] * xs[k / 3][q + k % 3];
+                    if constexpr (std::is_same<VT, __half>::value) sum *= m.vscale;
+                    epi(r0 + q, sum, acc);
+                }
+                if (haven) {
+#pragma unroll
+                    for (int k = 0; k < 9; k++) {
+                        v[k][0] = vn[k][0];
+                        v[k][1] = vn[k][1];
+                    }
+                }
+                have = haven;
+            } else {                            // the last row of an odd count
+                const int i = i0, r = m.lo + i;
                 AT sum = 0;
 #pragma unroll
                 for (int k = 0; k < 9; k++) {
@@ -549,6 +560,7 @@ k_spmv_st(StArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi ep
                 }
                 if constexpr (std::is_same<VT, __half>::value) sum *= m.vscale;
                 epi(r, sum, acc);
+                have = false;
             }
         }
     } else if (g < m.nirr) {

@@ -304,10 +304,9 @@ static void build_stencil(Matrix* M, const std::vector<int>& len)
                                                  M->csr_val.p, M->st_icol.p, M->st_val.p + 9 * (int64_t)ld);
         JFG_CUDA(cudaGetLastError());
     }
-    M->st_nb_reg[0] = (int)nblk(nreg, kThreads * 4);      // 4 rows per thread (4- and 2-byte values)
-    M->st_nb_reg[1] = (int)nblk(nreg, kThreads * 2);      // 2 rows per thread (FP64 values)
+    M->st_nb_reg = (int)nblk(nreg, kThreads * 2);          // one pair per thread (the launch caps the grid)
     M->st_nb_irr = (int)nblk(nirr, kThreads);
-    M->nblocks = std::max(M->nblocks, std::max(M->st_nb_reg[0], M->st_nb_reg[1]) + M->st_nb_irr);
+    M->nblocks = std::max(M->nblocks, M->st_nb_reg + M->st_nb_irr);
     JFG_CUDA(cudaStreamSynchronize(s));
     M->st = 1;
 }
