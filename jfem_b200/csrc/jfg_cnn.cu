@@ -449,11 +449,16 @@ __global__ void k_wgrad_edge_reduce(int nparts, const float* __restrict__ part, 
     dw[i] = s;
 }
 
-// g = d * (a > 0)
-__global__ void k_relu_mask(size_t n, const float* __restrict__ d, const bf16* __restrict__ a, float* __restrict__ g)
+// g = d * (a > 0), and g16 = the same in BF16 when given (the TMA input of
+// the tensor-core input-gradient convolution)
+__global__ void k_relu_mask(size_t n, const float* __restrict__ d, const bf16* __restrict__ a, float* __restrict__ g,
+                            bf16* __restrict__ g16)
 {
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-        g[i] = __bfloat162float(a[i]) > 0.f ? d[i] : 0.f;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float v = __bfloat162float(a[i]) > 0.f ? d[i] : 0.f;
+        g[i] = v;
+        if (g16) g16[i] = __float2bfloat16_rn(v);
+    }
 }
 
 // BF16 weight layouts from the FP32 master (co, ci, dy, dx):
@@ -489,6 +494,8 @@ __global__ void k_adam(int n, float* __restrict__ w, const float* __restrict__ g
 
 void conv_mid_tc(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* in, const __nv_bfloat16* wk,
                  const __nv_bfloat16* skip, __nv_bfloat16* out, int* err);
+void conv_mid_tc_bwd(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* gin, const __nv_bfloat16* wt,
+                     const __nv_bfloat16* mask, const float* skip, float* out, __nv_bfloat16* out16, int* err);
 }  // namespace jfg
 
 // ---------------------------------------------------------------------------
@@ -506,6 +513,7 @@ struct jfg_cnn {
     jfg::DevBuf<float> w32, g32, m, v, part;
     jfg::DevBuf<__nv_bfloat16> wk, wt, h1, a2, h3, a4, h5;
     jfg::DevBuf<float> y, dy, gA, gB, gC;
+    jfg::DevBuf<__nv_bfloat16> gB16, gC16;   // BF16 copies of gB / gC: inputs of the tensor-core input gradients
     jfg::DevBuf<double> loss;
     jfg::DevBuf<double> partials;
     jfg::DevBuf<unsigned> counter;
@@ -534,6 +542,8 @@ void cnn_reserve(jfg_cnn* n, size_t npx)
     n->gA.alloc(npx * kC);
     n->gB.alloc(npx * kC);
     n->gC.alloc(npx * kC);
+    n->gB16.alloc(npx * kC);
+    n->gC16.alloc(npx * kC);
     n->cap = npx;
 }
 
@@ -623,22 +633,40 @@ void cnn_backward(jfg_cnn* n, cudaStream_t st, int B, int H, int W, const float*
     k_wgrad_edge<1><<<kEdgeCtas, 256, 0, st>>>(B, H, W, nullptr, n->dy.p, n->h5.p, n->part.p);
     k_wgrad_edge_reduce<<<2, 256, 0, st>>>(kEdgeCtas, n->part.p, g + kLayerOff[5]);
     k_conv_out_bwd<<<grid1d(npx), 256, 0, st>>>(B, H, W, n->dy.p, n->w32.p + kLayerOff[5], n->gA.p);
-    k_relu_mask<<<grid1d(npx * kC), 256, 0, st>>>(npx * kC, n->gA.p, n->h5.p, n->gB.p);            // g5
+    // input gradients on the tensor cores (BF16 copies of the gradient images
+    // as their TMA inputs) unless JFEM_CNN_TC=0 selects the mma.sync kernels;
+    // both round the gradient images to BF16 for the products
+    const bool tc = use_tc();
+    bf16* gB16 = tc ? n->gB16.p : nullptr;
+    int* err = n->tc_err.p;
+    k_relu_mask<<<grid1d(npx * kC), 256, 0, st>>>(npx * kC, n->gA.p, n->h5.p, n->gB.p, gB16);      // g5
     JFG_CUDA(cudaGetLastError());
     wgrad_mid(n, st, B, H, W, n->gB.p, n->a4.p, g + kLayerOff[4]);                                  // dW5
-    conv_mid<float, float, 0, false, true>(st, B, H, W, n->gB.p, wt + 3 * kMidParams, nullptr, n->a4.p,
-                                           n->gC.p);                                                // g4
+    if (tc)
+        conv_mid_tc_bwd(st, B, H, W, gB16, wt + 3 * kMidParams, n->a4.p, nullptr, n->gC.p, n->gC16.p, err);
+    else
+        conv_mid<float, float, 0, false, true>(st, B, H, W, n->gB.p, wt + 3 * kMidParams, nullptr, n->a4.p,
+                                               n->gC.p);                                            // g4
     wgrad_mid(n, st, B, H, W, n->gC.p, n->h3.p, g + kLayerOff[3]);                                  // dW4
-    conv_mid<float, float, 2, false, false>(st, B, H, W, n->gC.p, wt + 2 * kMidParams, n->gB.p, nullptr,
-                                            n->gA.p);                                               // dh3
-    k_relu_mask<<<grid1d(npx * kC), 256, 0, st>>>(npx * kC, n->gA.p, n->h3.p, n->gB.p);            // g3
+    if (tc)
+        conv_mid_tc_bwd(st, B, H, W, n->gC16.p, wt + 2 * kMidParams, nullptr, n->gB.p, n->gA.p, nullptr, err);
+    else
+        conv_mid<float, float, 2, false, false>(st, B, H, W, n->gC.p, wt + 2 * kMidParams, n->gB.p, nullptr,
+                                                n->gA.p);                                           // dh3
+    k_relu_mask<<<grid1d(npx * kC), 256, 0, st>>>(npx * kC, n->gA.p, n->h3.p, n->gB.p, gB16);      // g3
     wgrad_mid(n, st, B, H, W, n->gB.p, n->a2.p, g + kLayerOff[2]);                                  // dW3
-    conv_mid<float, float, 0, false, true>(st, B, H, W, n->gB.p, wt + 1 * kMidParams, nullptr, n->a2.p,
-                                           n->gC.p);                                                // g2
+    if (tc)
+        conv_mid_tc_bwd(st, B, H, W, gB16, wt + 1 * kMidParams, n->a2.p, nullptr, n->gC.p, n->gC16.p, err);
+    else
+        conv_mid<float, float, 0, false, true>(st, B, H, W, n->gB.p, wt + 1 * kMidParams, nullptr, n->a2.p,
+                                               n->gC.p);                                            // g2
     wgrad_mid(n, st, B, H, W, n->gC.p, n->h1.p, g + kLayerOff[1]);                                  // dW2
-    conv_mid<float, float, 2, false, false>(st, B, H, W, n->gC.p, wt + 0 * kMidParams, n->gB.p, nullptr,
-                                            n->gA.p);                                               // dh1
-    k_relu_mask<<<grid1d(npx * kC), 256, 0, st>>>(npx * kC, n->gA.p, n->h1.p, n->gB.p);            // g1
+    if (tc)
+        conv_mid_tc_bwd(st, B, H, W, n->gC16.p, wt + 0 * kMidParams, nullptr, n->gB.p, n->gA.p, nullptr, err);
+    else
+        conv_mid<float, float, 2, false, false>(st, B, H, W, n->gC.p, wt + 0 * kMidParams, n->gB.p, nullptr,
+                                                n->gA.p);                                           // dh1
+    k_relu_mask<<<grid1d(npx * kC), 256, 0, st>>>(npx * kC, n->gA.p, n->h1.p, n->gB.p, nullptr);   // g1
     k_wgrad_edge<0><<<kEdgeCtas, 256, 0, st>>>(B, H, W, n->gB.p, x, nullptr, n->part.p);
     k_wgrad_edge_reduce<<<2, 256, 0, st>>>(kEdgeCtas, n->part.p, g + kLayerOff[0]);
     JFG_CUDA(cudaGetLastError());

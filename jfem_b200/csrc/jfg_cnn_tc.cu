@@ -1,6 +1,7 @@
-// 32 -> 32 3x3 convolution of the learned smoother's forward pass on the
-// fifth-generation tensor cores (tcgen05.mma, accumulators in TMEM), fed by
-// TMA.
+// 32 -> 32 3x3 convolutions of the learned smoother on the fifth-generation
+// tensor cores (tcgen05.mma, accumulators in TMEM), fed by TMA: the forward
+// layers and, with flipped channel-transposed weights and FP32 epilogues, the
+// input gradients of the backward pass.
 //
 // Implicit GEMM per tile of 16 x 8 = 128 output pixels (the MMA's M):
 //   D[p][co] = sum_{tap, ci} X[p + tap][ci] * W[co][tap * 32 + ci]
@@ -84,10 +85,19 @@ __device__ __forceinline__ void tma_plane(uint32_t dst, const CUtensorMap* map, 
         : "memory");
 }
 
-template <int SK>
+// Epilogue modes (acc = the convolution, FP32 from TMEM; one pixel per thread):
+//   kFwd:     out(bf16) = relu(acc)                          forward, no skip
+//   kFwdSkip: out(bf16) = relu(acc + skip(bf16))             forward with the residual input
+//   kBwdMask: out(f32) = acc * (mask(bf16) > 0), out16 = the same in BF16
+//             (an input gradient through the next layer's ReLU, and its BF16
+//             copy: the TMA input of the following input-gradient convolution)
+//   kBwdSkip: out(f32) = acc + skip(f32)                     input gradient plus the skip path's
+constexpr int kFwd = 0, kFwdSkip = 1, kBwdMask = 2, kBwdSkip = 3;
+
+template <int MODE>
 __global__ void __launch_bounds__(kTcThreads)
 k_conv_mid_tc(const __grid_constant__ CUtensorMap tin, int B, int H, int W, const bf16* __restrict__ wk,
-              const bf16* __restrict__ skip, bf16* __restrict__ out, int* __restrict__ err)
+              const void* __restrict__ aux, void* __restrict__ out, bf16* __restrict__ out16, int* __restrict__ err)
 {
     __shared__ __align__(128) unsigned char wsm[kWBytes];
     __shared__ __align__(128) unsigned char halo[kStages][kHaloBytes];
@@ -227,22 +237,61 @@ k_conv_mid_tc(const __grid_constant__ CUtensorMap tin, int B, int H, int W, cons
         const int gy = y0 + (m >> 3), gx = x0 + (m & 7);
         if (gy < H && gx < W) {
             const size_t base = (((size_t)b * H + gy) * W + gx) * 32;
-            __align__(16) bf16 o[32];
-            __align__(16) bf16 sv[32];
-            if (SK) {
+            if constexpr (MODE == kFwd || MODE == kFwdSkip) {
+                __align__(16) bf16 o[32];
+                __align__(16) bf16 sv[32];
+                if (MODE == kFwdSkip) {
+                    const bf16* skip = static_cast<const bf16*>(aux);
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                        *reinterpret_cast<uint4*>(sv + 8 * q) =
+                            __ldg(reinterpret_cast<const uint4*>(skip + base + 8 * q));
+                }
+#pragma unroll
+                for (int c = 0; c < 32; c++) {
+                    float v = __uint_as_float(r[c]);
+                    if (MODE == kFwdSkip) v += __bfloat162float(sv[c]);
+                    o[c] = __float2bfloat16_rn(fmaxf(v, 0.f));
+                }
+                bf16* ob = static_cast<bf16*>(out);
 #pragma unroll
                 for (int q = 0; q < 4; q++)
-                    *reinterpret_cast<uint4*>(sv + 8 * q) = __ldg(reinterpret_cast<const uint4*>(skip + base + 8 * q));
-            }
+                    *reinterpret_cast<uint4*>(ob + base + 8 * q) = *reinterpret_cast<const uint4*>(o + 8 * q);
+            } else if constexpr (MODE == kBwdMask) {
+                const bf16* mask = static_cast<const bf16*>(aux);
+                __align__(16) bf16 mv[32];
 #pragma unroll
-            for (int c = 0; c < 32; c++) {
-                float v = __uint_as_float(r[c]);
-                if (SK) v += __bfloat162float(sv[c]);
-                o[c] = __float2bfloat16_rn(fmaxf(v, 0.f));
-            }
+                for (int q = 0; q < 4; q++)
+                    *reinterpret_cast<uint4*>(mv + 8 * q) = __ldg(reinterpret_cast<const uint4*>(mask + base + 8 * q));
+                __align__(16) float f[32];
+                __align__(16) bf16 o[32];
 #pragma unroll
-            for (int q = 0; q < 4; q++)
-                *reinterpret_cast<uint4*>(out + base + 8 * q) = *reinterpret_cast<const uint4*>(o + 8 * q);
+                for (int c = 0; c < 32; c++) {
+                    const float v = __bfloat162float(mv[c]) > 0.f ? __uint_as_float(r[c]) : 0.f;
+                    f[c] = v;
+                    o[c] = __float2bfloat16_rn(v);
+                }
+                float* of = static_cast<float*>(out);
+#pragma unroll
+                for (int q = 0; q < 8; q++)
+                    *reinterpret_cast<float4*>(of + base + 4 * q) = *reinterpret_cast<const float4*>(f + 4 * q);
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    *reinterpret_cast<uint4*>(out16 + base + 8 * q) = *reinterpret_cast<const uint4*>(o + 8 * q);
+            } else {
+                const float* skip = static_cast<const float*>(aux);
+                float* of = static_cast<float*>(out);
+#pragma unroll
+                for (int q = 0; q < 8; q++) {
+                    const float4 sk = __ldg(reinterpret_cast<const float4*>(skip + base + 4 * q));
+                    float4 v;
+                    v.x = __uint_as_float(r[4 * q]) + sk.x;
+                    v.y = __uint_as_float(r[4 * q + 1]) + sk.y;
+                    v.z = __uint_as_float(r[4 * q + 2]) + sk.z;
+                    v.w = __uint_as_float(r[4 * q + 3]) + sk.w;
+                    *reinterpret_cast<float4*>(of + base + 4 * q) = v;
+                }
+            }
         }
         // every thread's TMEM reads are done before the MMAs two tiles on overwrite this stage
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -279,17 +328,8 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
     return fn;
 }
 
-// out = relu(conv3x3(in, wk) [+ skip]) for BF16 (B, H, W, 32) images; wk is
-// BF16 [32 outputs][9 taps x 32 inputs].  err is set to 1 if a TMA or MMA
-// wait timed out (the output is then incomplete).
-void conv_mid_tc(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* in, const __nv_bfloat16* wk,
-                 const __nv_bfloat16* skip, __nv_bfloat16* out, int* err)
+static CUtensorMap conv_input_map(int B, int H, int W, const __nv_bfloat16* in)
 {
-    const long long ntiles = (long long)((W + kTW - 1) / kTW) * ((H + kTH - 1) / kTH) * B;
-    JFG_CHECK(ntiles < (1LL << 31), JFG_ERR_UNSUPPORTED, "image too large for the tensor-core convolution");
-    JFG_CHECK(((uintptr_t)in & 15) == 0, JFG_ERR_BAD_ARG, "convolution input not 16-byte aligned");
-    const int grid = (int)std::min<long long>(ntiles, (long long)sm_count() * kTcCtasPerSm);
-    if (grid <= 0) return;
     CUtensorMap map;
     const cuuint64_t dims[4] = {32, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
     const cuuint64_t strides[3] = {64, (cuuint64_t)W * 64, (cuuint64_t)W * H * 64};
@@ -300,10 +340,48 @@ void conv_mid_tc(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* in, 
                                       CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     JFG_CHECK(r == CUDA_SUCCESS, JFG_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    return map;
+}
+
+static int conv_grid(int B, int H, int W, const void* in)
+{
+    const long long ntiles = (long long)((W + kTW - 1) / kTW) * ((H + kTH - 1) / kTH) * B;
+    JFG_CHECK(ntiles < (1LL << 31), JFG_ERR_UNSUPPORTED, "image too large for the tensor-core convolution");
+    JFG_CHECK(((uintptr_t)in & 15) == 0, JFG_ERR_BAD_ARG, "convolution input not 16-byte aligned");
+    return (int)std::min<long long>(ntiles, (long long)sm_count() * kTcCtasPerSm);
+}
+
+// out = relu(conv3x3(in, wk) [+ skip]) for BF16 (B, H, W, 32) images; wk is
+// BF16 [32 outputs][9 taps x 32 inputs].  err is set to 1 if a TMA or MMA
+// wait timed out (the output is then incomplete).
+void conv_mid_tc(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* in, const __nv_bfloat16* wk,
+                 const __nv_bfloat16* skip, __nv_bfloat16* out, int* err)
+{
+    const int grid = conv_grid(B, H, W, in);
+    if (grid <= 0) return;
+    const CUtensorMap map = conv_input_map(B, H, W, in);
     if (skip)
-        k_conv_mid_tc<1><<<grid, kTcThreads, 0, st>>>(map, B, H, W, wk, skip, out, err);
+        k_conv_mid_tc<kFwdSkip><<<grid, kTcThreads, 0, st>>>(map, B, H, W, wk, skip, out, nullptr, err);
     else
-        k_conv_mid_tc<0><<<grid, kTcThreads, 0, st>>>(map, B, H, W, wk, nullptr, out, err);
+        k_conv_mid_tc<kFwd><<<grid, kTcThreads, 0, st>>>(map, B, H, W, wk, nullptr, out, nullptr, err);
+    JFG_CUDA(cudaGetLastError());
+    note_launch();
+}
+
+// Input gradient of a 32 -> 32 layer on the tensor cores: conv3x3 of the
+// BF16 gradient image gin with the flipped, channel-transposed weights wt
+// (the layout of wk), FP32 accumulation.  mask != nullptr: out = acc *
+// (mask > 0) and out16 = its BF16 copy; else out = acc + skip (FP32).
+void conv_mid_tc_bwd(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* gin, const __nv_bfloat16* wt,
+                     const __nv_bfloat16* mask, const float* skip, float* out, __nv_bfloat16* out16, int* err)
+{
+    const int grid = conv_grid(B, H, W, gin);
+    if (grid <= 0) return;
+    const CUtensorMap map = conv_input_map(B, H, W, gin);
+    if (mask)
+        k_conv_mid_tc<kBwdMask><<<grid, kTcThreads, 0, st>>>(map, B, H, W, wt, mask, out, out16, err);
+    else
+        k_conv_mid_tc<kBwdSkip><<<grid, kTcThreads, 0, st>>>(map, B, H, W, wt, skip, out, nullptr, err);
     JFG_CUDA(cudaGetLastError());
     note_launch();
 }

@@ -85,3 +85,24 @@ def test_tcgen05_forward_matches_mma_sync(ctx, shape, monkeypatch):
     assert np.all(np.isfinite(y_tc))
     err = np.linalg.norm(y_tc - y_ms) / np.linalg.norm(y_ms)
     assert err < 1e-2, err
+
+
+@pytest.mark.parametrize("shape", [(2, 45, 27), (1, 131, 66)])
+def test_tcgen05_backward_matches_mma_sync(ctx, shape, monkeypatch):
+    """The input gradients of the backward pass on tcgen05 (flipped,
+    channel-transposed weights, FP32 epilogues with the ReLU masks and the
+    skip path) and on mma.sync read the same BF16-rounded gradient images:
+    the weight gradients agree to FP32 accumulation-order rounding."""
+    rng = np.random.default_rng(12)
+    w = he_init(seed=7, gain_last=1.0)
+    x = torch.from_numpy(rng.standard_normal(shape).astype(np.float32)).cuda()
+    t = torch.from_numpy(rng.standard_normal(shape).astype(np.float32)).cuda()
+    net = LearnedSmoother(ctx, w)
+    monkeypatch.setenv("JFEM_CNN_TC", "1")
+    l_tc, g_tc = net.loss_and_grad(x, t)
+    monkeypatch.setenv("JFEM_CNN_TC", "0")
+    l_ms, g_ms = net.loss_and_grad(x, t)
+    assert np.all(np.isfinite(g_tc))
+    for l, (a, b) in enumerate(zip(unpack(g_tc), unpack(g_ms))):
+        err = np.linalg.norm(a - b) / np.linalg.norm(b)
+        assert err < 1e-2, (l, err)
