@@ -482,8 +482,8 @@ constexpr int kStCtasPerSm = 4;
 // above the rows; the two rows share them).  The values of a thread's next
 // pair are loaded before the current pair is summed, so each thread keeps
 // two pairs of the matrix stream in flight and no CTA waits on a second
-// wave of launches.  The CTAs past the regular part take the irregular rows
-// from their CSR copy, one row per thread.  Every row is summed in ascending
+// wave of launches.  The first CTAs of the grid take the irregular rows from
+// their CSR copy, one row per thread.  Every row is summed in ascending
 // column order from 0 with the same multiply-adds as k_spmv (a stored zero
 // adds exactly 0 for finite x): the result equals the SELL kernels' bit for
 // bit.  PF: the first pair's values are loaded before the wait for the
@@ -494,10 +494,13 @@ k_spmv_st(StArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi ep
           const int* __restrict__ done)
 {
     using AT = typename AccOf<VT>::T;
-    const bool regular = (int)blockIdx.x < m.nb_reg;
+    // the irregular rows' CTAs come first: they start in the first wave
+    // instead of trailing the persistent regular CTAs
+    const int nb_irr = (m.nirr + kThreads - 1) / kThreads;
+    const bool regular = (int)blockIdx.x >= nb_irr;
     const int npairs = (m.nreg + 1) >> 1;
     const int stride = m.nb_reg * kThreads;
-    int g = (regular ? (int)blockIdx.x : (int)blockIdx.x - m.nb_reg) * kThreads + threadIdx.x;
+    int g = (regular ? (int)blockIdx.x - nb_irr : (int)blockIdx.x) * kThreads + threadIdx.x;
     auto full = [&](int gg) { return 2 * gg + 2 <= m.nreg; };
     AT v[9][2];
     bool have = false;

@@ -146,8 +146,9 @@ struct EpiRestrictSweep {
 constexpr int kTailMaxLevels = 8;         // coarse level included
 constexpr int kTailMaxRowsPerCta = 4095;  // 12-bit local row of a packed column
 constexpr int kTailThreads = 1024;
-constexpr int kTailSmemBudget = 200 * 1024;
-constexpr int kTailMetaInts = 22;         // per level: A, R, P (5 each), dinv, mask, rows per CTA, x, t, b, r
+constexpr int kTailSmemBudget = 224 * 1024;
+constexpr int kTailMetaInts = 23;         // per level: A, R, P (5 each), dinv, mask, rows per CTA, x, t, b, r, solo
+constexpr int kTailSoloRows = 320;        // levels this small run on CTA 0 alone (CTA barriers, no cluster barriers)
 
 struct TailMat {
     int off_col, off_val;   // byte offsets of the column and value blocks in a CTA's shared memory
@@ -159,6 +160,7 @@ template <typename T>
 struct TailLevel {
     TailMat A, R, P;          // R: restriction into level l - 1, P: prolongation from level l - 1
     int Rl, n, runs;          // rows per CTA, rows, Jacobi sweeps
+    int solo;                 // all rows on CTA 0 (R = n): its phases end with CTA barriers of CTA 0 only
     int off_dinv, off_mask, off_x, off_t, off_b, off_r;
     T omega;
 };
@@ -251,6 +253,15 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
     pdl_wait();
     if (P.done && *P.done) return;           // the same answer for every CTA of the cluster
     auto vec = [&](int off) { return reinterpret_cast<T*>(sm + off); };
+    // the barrier after a phase that wrote a level's vectors: the whole
+    // cluster for a distributed level, CTA 0 alone for a level it holds alone
+    // (the other CTAs skip it; every CTA runs the same cluster barriers)
+    auto sync_after = [&](int solo) {
+        if (!solo)
+            cl.sync();
+        else if (c == 0)
+            __syncthreads();
+    };
     {   // the restricted right-hand side of the top level, own rows
         const TailLevel<T>& L = P.lv[P.top];
         T* b = vec(L.off_b);
@@ -267,7 +278,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
         int cur_off = (L.runs % 2 == 1) ? L.off_x : L.off_t;
         if (l == P.top) {   // below the top the restriction phase did it
             tail_own(L.Rl, L.n, c, [&](int t) { cur[t] = (T)0 + (dinv[t] * b[t]) * om; });
-            cl.sync();
+            sync_after(L.solo);
         }
         for (int k = 1; k < L.runs; k++) {
             const int alt_off = cur_off == L.off_x ? L.off_t : L.off_x;
@@ -276,7 +287,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
             A.xoff = cur_off;
             const T* cu = cur;
             tail_spmv<T>(sm, A, c, [&](int t, T s) { alt[t] = cu[t] + (dinv[t] * (b[t] - s)) * om; });
-            cl.sync();
+            sync_after(L.solo);
             cur = alt;
             cur_off = alt_off;
         }
@@ -285,7 +296,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
             TailMat A = L.A;
             A.xoff = L.off_x;
             tail_spmv<T>(sm, A, c, [&](int t, T s) { r[t] = b[t] - s; });
-            cl.sync();
+            sync_after(L.solo);
         }
         {   // restriction into level l - 1 with zero boundary values (and its fused first sweep)
             const TailLevel<T>& Cl = P.lv[l - 1];
@@ -305,7 +316,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
             } else {
                 tail_spmv<T>(sm, R, c, [&](int t, T s) { bc[t] = mask[t] ? (T)0 : s; });
             }
-            cl.sync();
+            sync_after(Cl.solo);
         }
     }
     {   // coarsest level: x0 = Ainv * b0 in FP64, one warp per own row (the order of k_coarse_gemv)
@@ -325,20 +336,21 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
             s = warp_sum(s);
             if (lane == 0) x0[t] = (T)s;
         }
-        cl.sync();
+        sync_after(L0.solo);
     }
     for (int l = 1; l <= P.top; l++) {
         const TailLevel<T>& L = P.lv[l];
         const T* b = vec(L.off_b);
         const T* dinv = vec(L.off_dinv);
         const T om = L.omega;
+        if (!L.solo && P.lv[l - 1].solo) cl.sync();    // the other CTAs wait for CTA 0's levels
         {   // x += mask ? 0 : P x_{l-1}
             T* x = vec(L.off_x);
             const unsigned char* mask = sm + L.off_mask;
             TailMat Pm = L.P;
             Pm.xoff = P.lv[l - 1].off_x;
             tail_spmv<T>(sm, Pm, c, [&](int t, T s) { x[t] = x[t] + (mask[t] ? (T)0 : s); });
-            cl.sync();
+            sync_after(L.solo);
         }
         int cur_off = L.off_x;
         for (int k = 0; k < L.runs; k++) {
@@ -348,14 +360,14 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
             TailMat A = L.A;
             A.xoff = cur_off;
             tail_spmv<T>(sm, A, c, [&](int t, T s) { alt[t] = cu[t] + (dinv[t] * (b[t] - s)) * om; });
-            cl.sync();
+            sync_after(L.solo);
             cur_off = alt_off;
         }
         if (cur_off != L.off_x) {
             const T* cu = vec(cur_off);
             T* x = vec(L.off_x);
             tail_own(L.Rl, L.n, c, [&](int t) { x[t] = cu[t]; });
-            cl.sync();
+            sync_after(L.solo);
         }
     }
     {   // the result of the top level back to global memory
@@ -623,7 +635,9 @@ void MGImpl<T>::build_tail()
     }
     std::vector<double> hdinv;
     auto al16 = [](size_t b) { return (b + 15) / 16 * 16; };
-    auto rows_per = [&](int l, int C) { return (n[l] + C - 1) / C; };
+    // the smallest levels live on CTA 0 alone
+    auto solo = [&](int l) { return n[l] <= kTailSoloRows; };
+    auto rows_per = [&](int l, int C) { return solo(l) ? n[l] : (n[l] + C - 1) / C; };
     // byte sizes: constant package, then vectors
     auto sizes = [&](int top, int C, size_t& pkg, size_t& total) {
         pkg = 0;
@@ -722,6 +736,7 @@ void MGImpl<T>::build_tail()
             for (int t = 0; t < Rl && cc * Rl + t < n[l]; t++) pkg[cc * pkg_b + off + t] = mk[l][cc * Rl + t];
         off += al16((size_t)Rl);
         meta[17] = Rl;
+        meta[22] = solo(l) ? 1 : 0;
     }
     JFG_CHECK(off == pkg_b, JFG_ERR_CUDA, "tail package layout mismatch");
     for (int l = 0; l <= top; l++) {                      // vectors x, t, b, r
@@ -887,6 +902,7 @@ void MGImpl<T>::run_tail(bool first_sweep_done, const int* done, cudaStream_t st
         Lv.off_t = m[19];
         Lv.off_b = m[20];
         Lv.off_r = m[21];
+        Lv.solo = m[22];
         Lv.n = n[l];
         Lv.runs = sm[l].runs;
         Lv.omega = (T)sm[l].omega;

@@ -154,8 +154,10 @@ void spmv_launch(cudaStream_t st, const Matrix* M, const VT* val, const XT* x, E
     GridRed<NR, Fin> red{sc.partials, sc.counter, fin};
     // the values-only stencil layout, when the matrix has one in this value type
     if (M->st && val == LayoutVals<VT>::sell(M) && LayoutVals<VT>::st(M)) {
-        // persistent: as many CTAs as stay resident (FP64 values: 104 registers, 2 per SM)
-        const int nbr = std::min(M->st_nb_reg, sm_count() * (sizeof(VT) == 8 ? 2 : kStCtasPerSm));
+        // persistent: as many regular CTAs as stay resident next to the irregular ones
+        // (FP64 values: up to 128 registers, 2 CTAs per SM)
+        const int nbr = std::max(1, std::min(M->st_nb_reg, sm_count() * (sizeof(VT) == 8 ? 2 : kStCtasPerSm) -
+                                                                M->st_nb_irr));
         StArgs sa{M->st_S, M->st_lo, M->st_hi - M->st_lo, M->st_ld, M->st_nirr, nbr, M->st_irow.p, M->st_iptr.p,
                   M->st_icol.p, std::is_same<VT, __half>::value ? M->hscale_inv : 1.0f};
         launch_ex(k_spmv_st<VT, XT, NR, Epi, Fin, PF>, dim3(nbr + M->st_nb_irr), dim3(kThreads), 0, st, sa,
