@@ -415,7 +415,7 @@ void build_desc(jfg_batch* b, bool with_f)
         d.k_off = K->off.p;
         d.k_perm = K->perm.p;
         d.k_col = K->col.p;
-        d.k_col16 = K->idx16 ? K->col16.p : nullptr;
+        d.k_col16 = K->idx16 == 1 ? K->col16.p : nullptr;   // offsets from the row only
         d.k_v64 = K->val.p;
         d.k_v32 = K->val32.p;
         d.m_off = M->off.p;

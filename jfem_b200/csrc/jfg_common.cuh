@@ -118,7 +118,9 @@ struct Matrix {
     DevBuf<int> off;              // nslices + 1 slice offsets
     DevBuf<int> perm;             // nslices * 32 original row of each slot
     DevBuf<int> col;              // sell_len
-    DevBuf<int16_t> col16;        // sell_len: col - max(row, 0) when every entry fits 16 bits
+    DevBuf<int16_t> col16;        // sell_len: 16-bit column offsets (idx16 = 1: col - max(row, 0);
+                                  // idx16 = 2: col - cbase[slice])
+    DevBuf<int> cbase;            // nslices: base column of each slice (idx16 = 2; rectangular matrices)
     int idx16 = 0;                // the SpMV reads col16 instead of col
     DevBuf<double> val;           // sell_len
     DevBuf<float> val32;          // optional FP32 copy

@@ -174,7 +174,8 @@ struct SpmvArgs {
     const int* col;     // SELL column indices
     int nslots;         // nslices * 32
     int tpr_log2;       // log2 of the threads that share one row (0..3)
-    const int16_t* col16;  // SELL column offsets from the slot's row (IDX16 kernels)
+    const int16_t* col16;  // SELL 16-bit column offsets (IDX16 kernels) from the slot's row, or from
+    const int* cbase;      // the slice's base column cbase[slice] when not null
     float vscale;          // FP16 values: factor of the row sums (2^-k of the value scaling)
 };
 
@@ -205,15 +206,16 @@ __device__ __forceinline__ void spmv_prefetched(const SpmvArgs& m, const VT* __r
     const int gid = blockIdx.x * kThreads + threadIdx.x;
     const int slot = gid / TPR;
     const int sub = gid % TPR;
-    int o = 0, len = 0, r = -1;
+    int o = 0, len = 0, r = -1, sb = 0;
     if (slot < m.nslots) {
         const int s = slot >> 5;
         const int a = __ldg(m.off + s);
         o = a + (slot & 31);
         len = (__ldg(m.off + s + 1) - a) >> 5;
         r = __ldg(m.perm + slot);
+        if (IDX16 && m.cbase) sb = __ldg(m.cbase + s);
     }
-    const int base = r < 0 ? 0 : r;
+    const int base = (IDX16 && m.cbase) ? sb : (r < 0 ? 0 : r);
     int c[U];
     AT v[U];
     auto load_chunk = [&](int k) {
@@ -288,7 +290,7 @@ k_spmv(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi
             // (entries past the slice length are predicated off), so a
             // thread has U entries of the matrix stream in flight.
             constexpr int U = TPR == 1 ? 8 : 4;
-            const int base = r < 0 ? 0 : r;
+            const int base = m.cbase ? __ldg(m.cbase + s) : (r < 0 ? 0 : r);
             const int16_t* cp = m.col16 + o + lane;
             for (; k < len; k += U * tpr) {
                 int c[U];
@@ -376,7 +378,7 @@ k_spmv_pipe(SpmvArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Ep
         const int o = __ldg(m.off + s);
         const int len = (__ldg(m.off + s + 1) - o) >> 5;
         r = __ldg(m.perm + gid);
-        const int base = r < 0 ? 0 : r;
+        const int base = m.cbase ? __ldg(m.cbase + s) : (r < 0 ? 0 : r);
         const int nch = (len + U - 1) / U;
         // chunk j = entries [jU, jU + cnt) of the slice: [o + 32 jU, o + 32 (jU + cnt)); o is
         // a multiple of 32, so every copy starts on a 16-byte boundary

@@ -2,6 +2,8 @@
 // precision copies.
 #include <cub/cub.cuh>
 
+#include <climits>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -150,6 +152,42 @@ __global__ void k_make_col16(int nslots, const int* perm, const int* off, const 
             return;
         }
         col16[at] = (int16_t)d;
+    }
+}
+
+// 16-bit column offsets from a per-slice base column (matrices whose columns
+// are far from their rows, e.g. transfers between grids): one warp per slice,
+// base = (smallest column of the slice's rows) + 32768, so a span of up to
+// 65,535 columns fits; padding slots (no row) point at the smallest column.
+__global__ void k_make_col16_slice(int nslots, const int* perm, const int* off, const int* col, int16_t* col16,
+                                   int* cbase, int* bad)
+{
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in = slot < nslots;                      // nslots is a multiple of 32: warp-uniform
+    if (!in) return;
+    const int s = slot >> 5, lane = slot & 31;
+    const int o = off[s];
+    const int len = (off[s + 1] - o) >> 5;
+    const bool real = perm[slot] >= 0;
+    int mn = INT_MAX, mx = INT_MIN;
+    if (real)
+        for (int k = 0; k < len; k++) {
+            const int c = col[(int64_t)o + (int64_t)k * 32 + lane];
+            mn = min(mn, c);
+            mx = max(mx, c);
+        }
+    mn = __reduce_min_sync(0xffffffffu, mn);
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if (mn == INT_MAX) mn = mx = 0;                     // a slice of padding slots only
+    if ((int64_t)mx - mn > 65535) {
+        if (lane == 0) atomicOr(bad, 1);
+        return;
+    }
+    const int base = mn + 32768;
+    if (lane == 0) cbase[s] = base;
+    for (int k = 0; k < len; k++) {
+        const int64_t at = (int64_t)o + (int64_t)k * 32 + lane;
+        col16[at] = (int16_t)((real ? col[at] : mn) - base);
     }
 }
 
@@ -412,7 +450,20 @@ static Matrix* build_from_sorted(Context* c, int rows, int cols, int64_t m, cons
         JFG_CUDA(cudaMemcpyAsync(&hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
         JFG_CUDA(cudaStreamSynchronize(s));
         M->idx16 = hb ? 0 : 1;
-        if (hb) M->col16.release();
+        if (hb) {       // columns far from the rows: try offsets from a base column per slice
+            JFG_CUDA(cudaMemsetAsync(bad.p, 0, sizeof(int), s));
+            M->cbase.alloc((size_t)nslices);
+            k_make_col16_slice<<<nblk((int64_t)nslices * kSliceRows), 256, 0, s>>>(
+                nslices * kSliceRows, M->perm.p, M->off.p, M->col.p, M->col16.p, M->cbase.p, bad.p);
+            JFG_CUDA(cudaGetLastError());
+            JFG_CUDA(cudaMemcpyAsync(&hb, bad.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+            JFG_CUDA(cudaStreamSynchronize(s));
+            M->idx16 = hb ? 0 : 2;
+            if (hb) {
+                M->col16.release();
+                M->cbase.release();
+            }
+        }
     }
     JFG_CUDA(cudaStreamSynchronize(s));
     build_stencil(M, len);

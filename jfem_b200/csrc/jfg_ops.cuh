@@ -165,7 +165,7 @@ void spmv_launch(cudaStream_t st, const Matrix* M, const VT* val, const XT* x, E
         return;
     }
     SpmvArgs a{M->off.p, M->perm.p, M->col.p, M->nslices * kSliceRows, M->tpr_log2, M->col16.p,
-               std::is_same<VT, __half>::value ? M->hscale_inv : 1.0f};
+               M->idx16 == 2 ? M->cbase.p : nullptr, std::is_same<VT, __half>::value ? M->hscale_inv : 1.0f};
     const dim3 g(M->nblocks), b(kThreads);
     if (M->idx16) {
         switch (M->tpr_log2) {

@@ -112,3 +112,25 @@ def test_16bit_offsets_match_32bit(ctx, monkeypatch):
     A32 = DeviceMatrix(sy.n, sy.n, sy.rows, sy.cols, sy.vals, ctx)
     assert np.array_equal(A16.spmv(x), A32.spmv(x))
     assert np.array_equal(A16.spmv_t(x), A32.spmv_t(x))
+
+
+def test_transfer_matrices_slice_base_columns(ctx, monkeypatch):
+    """Rectangular transfer matrices (the nodal prolongation between Q1
+    grids of 256^2 and 512^2 cells: 263,169 x 66,049, and its transpose)
+    have columns far from their rows; their 16-bit column offsets are taken
+    from a base column per 32-row slice.  Products equal the oracle's COO
+    scatter and, bit for bit, the 32-bit-column layout."""
+    from fixtures import mg_levels
+    h = mg_levels(1, 256, 2)
+    ri, ci, v = h.prolong[0]
+    nf, nc = h.systems[1].n, h.systems[0].n
+    P = DeviceMatrix(nf, nc, ri, ci, v, ctx)
+    ref = O.CooMatrix(nf, nc, ri, ci, v)
+    rng = np.random.default_rng(21)
+    xc, xf = rng.standard_normal(nc), rng.standard_normal(nf)
+    y, z = P.spmv(xc), P.spmv_t(xf)
+    np.testing.assert_allclose(y, ref.mvmul(xc), rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(z, ref.tvmul(xf), rtol=1e-12, atol=1e-13)
+    monkeypatch.setenv("JFEM_IDX16", "0")
+    P32 = DeviceMatrix(nf, nc, ri, ci, v, ctx)
+    assert np.array_equal(P32.spmv(xc), y) and np.array_equal(P32.spmv_t(xf), z)
