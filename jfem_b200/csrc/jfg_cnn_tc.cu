@@ -94,6 +94,69 @@ __device__ __forceinline__ void tma_plane(uint32_t dst, const CUtensorMap* map, 
 //   kBwdSkip: out(f32) = acc + skip(f32)                     input gradient plus the skip path's
 constexpr int kFwd = 0, kFwdSkip = 1, kBwdMask = 2, kBwdSkip = 3;
 
+// The epilogue of one output pixel: its 32 FP32 channel sums r (from TMEM)
+// combined and stored as MODE says; base = the pixel's first channel.
+template <int MODE>
+__device__ __forceinline__ void conv_store(const uint32_t (&r)[32], size_t base, const void* __restrict__ aux,
+                                           void* __restrict__ out, bf16* __restrict__ out16)
+{
+    if constexpr (MODE == kFwd || MODE == kFwdSkip) {
+        __align__(16) bf16 o[32];
+        __align__(16) bf16 sv[32];
+        if (MODE == kFwdSkip) {
+            const bf16* skip = static_cast<const bf16*>(aux);
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                *reinterpret_cast<uint4*>(sv + 8 * q) =
+                    __ldg(reinterpret_cast<const uint4*>(skip + base + 8 * q));
+        }
+#pragma unroll
+        for (int c = 0; c < 32; c++) {
+            float v = __uint_as_float(r[c]);
+            if (MODE == kFwdSkip) v += __bfloat162float(sv[c]);
+            o[c] = __float2bfloat16_rn(fmaxf(v, 0.f));
+        }
+        bf16* ob = static_cast<bf16*>(out);
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            *reinterpret_cast<uint4*>(ob + base + 8 * q) = *reinterpret_cast<const uint4*>(o + 8 * q);
+    } else if constexpr (MODE == kBwdMask) {
+        const bf16* mask = static_cast<const bf16*>(aux);
+        __align__(16) bf16 mv[32];
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            *reinterpret_cast<uint4*>(mv + 8 * q) = __ldg(reinterpret_cast<const uint4*>(mask + base + 8 * q));
+        __align__(16) float f[32];
+        __align__(16) bf16 o[32];
+#pragma unroll
+        for (int c = 0; c < 32; c++) {
+            const float v = __bfloat162float(mv[c]) > 0.f ? __uint_as_float(r[c]) : 0.f;
+            f[c] = v;
+            o[c] = __float2bfloat16_rn(v);
+        }
+        float* of = static_cast<float*>(out);
+#pragma unroll
+        for (int q = 0; q < 8; q++)
+            *reinterpret_cast<float4*>(of + base + 4 * q) = *reinterpret_cast<const float4*>(f + 4 * q);
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+            *reinterpret_cast<uint4*>(out16 + base + 8 * q) = *reinterpret_cast<const uint4*>(o + 8 * q);
+    } else {
+        const float* skip = static_cast<const float*>(aux);
+        float* of = static_cast<float*>(out);
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const float4 sk = __ldg(reinterpret_cast<const float4*>(skip + base + 4 * q));
+            float4 v;
+            v.x = __uint_as_float(r[4 * q]) + sk.x;
+            v.y = __uint_as_float(r[4 * q + 1]) + sk.y;
+            v.z = __uint_as_float(r[4 * q + 2]) + sk.z;
+            v.w = __uint_as_float(r[4 * q + 3]) + sk.w;
+            *reinterpret_cast<float4*>(of + base + 4 * q) = v;
+        }
+    }
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(kTcThreads)
 k_conv_mid_tc(const __grid_constant__ CUtensorMap tin, int B, int H, int W, const bf16* __restrict__ wk,
@@ -237,61 +300,7 @@ k_conv_mid_tc(const __grid_constant__ CUtensorMap tin, int B, int H, int W, cons
         const int gy = y0 + (m >> 3), gx = x0 + (m & 7);
         if (gy < H && gx < W) {
             const size_t base = (((size_t)b * H + gy) * W + gx) * 32;
-            if constexpr (MODE == kFwd || MODE == kFwdSkip) {
-                __align__(16) bf16 o[32];
-                __align__(16) bf16 sv[32];
-                if (MODE == kFwdSkip) {
-                    const bf16* skip = static_cast<const bf16*>(aux);
-#pragma unroll
-                    for (int q = 0; q < 4; q++)
-                        *reinterpret_cast<uint4*>(sv + 8 * q) =
-                            __ldg(reinterpret_cast<const uint4*>(skip + base + 8 * q));
-                }
-#pragma unroll
-                for (int c = 0; c < 32; c++) {
-                    float v = __uint_as_float(r[c]);
-                    if (MODE == kFwdSkip) v += __bfloat162float(sv[c]);
-                    o[c] = __float2bfloat16_rn(fmaxf(v, 0.f));
-                }
-                bf16* ob = static_cast<bf16*>(out);
-#pragma unroll
-                for (int q = 0; q < 4; q++)
-                    *reinterpret_cast<uint4*>(ob + base + 8 * q) = *reinterpret_cast<const uint4*>(o + 8 * q);
-            } else if constexpr (MODE == kBwdMask) {
-                const bf16* mask = static_cast<const bf16*>(aux);
-                __align__(16) bf16 mv[32];
-#pragma unroll
-                for (int q = 0; q < 4; q++)
-                    *reinterpret_cast<uint4*>(mv + 8 * q) = __ldg(reinterpret_cast<const uint4*>(mask + base + 8 * q));
-                __align__(16) float f[32];
-                __align__(16) bf16 o[32];
-#pragma unroll
-                for (int c = 0; c < 32; c++) {
-                    const float v = __bfloat162float(mv[c]) > 0.f ? __uint_as_float(r[c]) : 0.f;
-                    f[c] = v;
-                    o[c] = __float2bfloat16_rn(v);
-                }
-                float* of = static_cast<float*>(out);
-#pragma unroll
-                for (int q = 0; q < 8; q++)
-                    *reinterpret_cast<float4*>(of + base + 4 * q) = *reinterpret_cast<const float4*>(f + 4 * q);
-#pragma unroll
-                for (int q = 0; q < 4; q++)
-                    *reinterpret_cast<uint4*>(out16 + base + 8 * q) = *reinterpret_cast<const uint4*>(o + 8 * q);
-            } else {
-                const float* skip = static_cast<const float*>(aux);
-                float* of = static_cast<float*>(out);
-#pragma unroll
-                for (int q = 0; q < 8; q++) {
-                    const float4 sk = __ldg(reinterpret_cast<const float4*>(skip + base + 4 * q));
-                    float4 v;
-                    v.x = __uint_as_float(r[4 * q]) + sk.x;
-                    v.y = __uint_as_float(r[4 * q + 1]) + sk.y;
-                    v.z = __uint_as_float(r[4 * q + 2]) + sk.z;
-                    v.w = __uint_as_float(r[4 * q + 3]) + sk.w;
-                    *reinterpret_cast<float4*>(of + base + 4 * q) = v;
-                }
-            }
+            conv_store<MODE>(r, base, aux, out, out16);
         }
         // every thread's TMEM reads are done before the MMAs two tiles on overwrite this stage
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -302,6 +311,188 @@ k_conv_mid_tc(const __grid_constant__ CUtensorMap tin, int B, int H, int W, cons
         atomicOr(err, 1);
         for (int k = loads_done; k < loads_issued; k++) mbar_wait(smem_u32(&full[k & 1]), (uint32_t)((k >> 1) & 1));
         for (int k = i; k < mmas_issued; k++) mbar_wait(smem_u32(&mdone[k & 1]), (uint32_t)((k >> 1) & 1));
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 64;" ::"r"(tmem) : "memory");
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Warp-specialised pipeline (the default).  Per CTA of 192 threads:
+//   warp 0 (one lane): TMA producer -- the four 8-channel halo planes of tile
+//     i into halo stage i % kWsStages, once the MMAs of tile i - kWsStages
+//     released that stage (mbarrier `empty`);
+//   warp 1 (one lane): MMA issuer -- waits for the stage (`full`, TMA
+//     transaction bytes) and for a free TMEM accumulator (`tempty`), issues
+//     the 18 MMAs, and commits them to `empty` (stage free) and `tfull`
+//     (accumulator ready);
+//   warps 2-5: epilogue -- each reads its 32 TMEM lanes (warp w owns lanes
+//     32 (w % 4) ...) of the ready accumulator, releases it (`tempty`, one
+//     arrival per warp), then combines and stores its 32 pixels.
+// Loads run up to kWsStages tiles ahead and the MMAs of the next tile overlap
+// the epilogue of the current one; no CTA-wide barrier inside the tile loop.
+// Every wait is bounded (mbar_wait); a timeout sets *err, the roles stop, and
+// the copies and MMAs still in flight are waited for (bounded) before TMEM is
+// released.
+constexpr int kWsStages = 4;
+constexpr int kWsAcc = 2;
+constexpr int kWsThreads = 192;
+constexpr int kWsCtasPerSm = 3;
+constexpr int kWsSmem = kWBytes + kWsStages * kHaloBytes + 128;   // + alignment slack
+
+template <int MODE>
+__global__ void __launch_bounds__(kWsThreads)
+k_conv_ws(const __grid_constant__ CUtensorMap tin, int B, int H, int W, const bf16* __restrict__ wk,
+          const void* __restrict__ aux, void* __restrict__ out, bf16* __restrict__ out16, int* __restrict__ err)
+{
+    extern __shared__ unsigned char dsm_raw[];
+    unsigned char* dsm = reinterpret_cast<unsigned char*>(((uintptr_t)dsm_raw + 127) & ~(uintptr_t)127);
+    unsigned char* wsm = dsm;                          // weights, kWBytes
+    unsigned char* halo = dsm + kWBytes;               // kWsStages x kHaloBytes
+    __shared__ __align__(8) uint64_t full[kWsStages], empty[kWsStages], tfull[kWsAcc], tempty[kWsAcc];
+    __shared__ uint32_t tmem_sh;
+    __shared__ volatile int s_stop;
+    __shared__ int s_loads, s_mmas;                    // issued counts, for the error path
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int i = tid; i < 32 * 36; i += kWsThreads) {
+        const int co = i / 36, j = i % 36;
+        const uint4 v = *reinterpret_cast<const uint4*>(wk + co * 288 + j * 8);
+        *reinterpret_cast<uint4*>(wsm + (co >> 3) * kWRowGroup + j * 128 + (co & 7) * 16) = v;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(smem_u32(&tmem_sh))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 32) {
+        s_stop = 0;
+        s_loads = 0;
+        s_mmas = 0;
+        for (int q = 0; q < kWsStages; q++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[q])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[q])) : "memory");
+        }
+        for (int q = 0; q < kWsAcc; q++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&tfull[q])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(smem_u32(&tempty[q])) : "memory");
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // weights: generic writes, async-proxy reads
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_sh;
+    const uint32_t wbase = smem_u32(wsm);
+    const int tilesx = (W + kTW - 1) / kTW, tilesy = (H + kTH - 1) / kTH;
+    const int per_img = tilesx * tilesy;
+    const int ntiles = per_img * B;
+    const int cnt = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    auto tile_of = [&](int i) { return (int)blockIdx.x + i * (int)gridDim.x; };
+
+    if (warp == 0) {
+        if (lane == 0) {                               // TMA producer
+            for (int i = 0; i < cnt && !s_stop; i++) {
+                const int q = i % kWsStages;
+                if (i >= kWsStages && !mbar_wait(smem_u32(&empty[q]), (uint32_t)((i / kWsStages - 1) & 1))) {
+                    s_stop = 1;
+                    break;
+                }
+                const int t = tile_of(i);
+                const int b = t / per_img, rem = t - b * per_img;
+                const int y0 = (rem / tilesx) * kTH, x0 = (rem % tilesx) * kTW;
+                const uint32_t bar = smem_u32(&full[q]);
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(4 * kPlaneData)
+                             : "memory");
+                const uint32_t dst = smem_u32(halo + q * kHaloBytes);
+#pragma unroll
+                for (int p = 0; p < 4; p++) tma_plane(dst + p * kPlane, &tin, 8 * p, x0 - 1, y0 - 1, b, bar);
+                s_loads = i + 1;
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {                               // MMA issuer
+            for (int i = 0; i < cnt && !s_stop; i++) {
+                const int q = i % kWsStages, a = i % kWsAcc;
+                if (!mbar_wait(smem_u32(&full[q]), (uint32_t)((i / kWsStages) & 1))) {
+                    s_stop = 1;
+                    break;
+                }
+                if (i >= kWsAcc && !mbar_wait(smem_u32(&tempty[a]), (uint32_t)((i / kWsAcc - 1) & 1))) {
+                    s_stop = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t hb = smem_u32(halo + q * kHaloBytes);
+#pragma unroll
+                for (int tap = 0; tap < 9; tap++) {
+                    const int dy = tap / 3, dx = tap % 3;
+#pragma unroll
+                    for (int k = 0; k < 2; k++) {
+                        const uint64_t da = umma_desc(hb + 2 * k * kPlane + (dy * kHW + dx) * 16, kPlane, kHW * 16);
+                        const uint64_t db = umma_desc(wbase + (4 * tap + 2 * k) * 128, 128, kWRowGroup);
+                        const uint32_t accum = (tap | k) ? 1u : 0u;
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                            ::"r"(tmem + (uint32_t)(a * 32)), "l"(da), "l"(db), "r"(kIdesc), "r"(accum)
+                            : "memory");
+                    }
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&empty[q]))
+                             : "memory");
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&tfull[a]))
+                             : "memory");
+                s_mmas = i + 1;
+            }
+        }
+    } else {                                           // epilogue warps 2..5
+        const int lg = warp & 3;                       // TMEM lane group this warp may access
+        const int m = lg * 32 + lane;                  // pixel of the 16 x 8 tile
+        for (int i = 0; i < cnt; i++) {
+            const int a = i % kWsAcc;
+            const bool ok = !s_stop && mbar_wait(smem_u32(&tfull[a]), (uint32_t)((i / kWsAcc) & 1));
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (lane == 0) s_stop = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            uint32_t r[32];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                : "r"(tmem + ((uint32_t)(lg * 32) << 16) + (uint32_t)(a * 32))
+                : "memory");
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[a])) : "memory");
+            const int t = tile_of(i);
+            const int b = t / per_img, rem = t - b * per_img;
+            const int gy = (rem / tilesx) * kTH + (m >> 3), gx = (rem % tilesx) * kTW + (m & 7);
+            if (gy < H && gx < W) conv_store<MODE>(r, (((size_t)b * H + gy) * W + gx) * 32, aux, out, out16);
+        }
+    }
+    __syncthreads();
+    if (s_stop && tid == 32) {
+        // report, then let the copies and MMAs still in flight finish (bounded) before TMEM is freed
+        atomicOr(err, 1);
+        const int nl = s_loads, nm = s_mmas;
+        for (int k = nm; k < nl; k++) mbar_wait(smem_u32(&full[k % kWsStages]), (uint32_t)((k / kWsStages) & 1));
+        if (nm > 0) mbar_wait(smem_u32(&tfull[(nm - 1) % kWsAcc]), (uint32_t)(((nm - 1) / kWsAcc) & 1));
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -343,12 +534,39 @@ static CUtensorMap conv_input_map(int B, int H, int W, const __nv_bfloat16* in)
     return map;
 }
 
+// JFEM_CNN_WS=0 selects the single-role kernel (k_conv_mid_tc) instead of the
+// warp-specialised pipeline (k_conv_ws)
+static bool use_ws()
+{
+    const char* e = getenv("JFEM_CNN_WS");
+    return !(e && e[0] == '0');
+}
+
 static int conv_grid(int B, int H, int W, const void* in)
 {
     const long long ntiles = (long long)((W + kTW - 1) / kTW) * ((H + kTH - 1) / kTH) * B;
     JFG_CHECK(ntiles < (1LL << 31), JFG_ERR_UNSUPPORTED, "image too large for the tensor-core convolution");
     JFG_CHECK(((uintptr_t)in & 15) == 0, JFG_ERR_BAD_ARG, "convolution input not 16-byte aligned");
-    return (int)std::min<long long>(ntiles, (long long)sm_count() * kTcCtasPerSm);
+    const int per_sm = use_ws() ? kWsCtasPerSm : kTcCtasPerSm;
+    return (int)std::min<long long>(ntiles, (long long)sm_count() * per_sm);
+}
+
+template <int MODE>
+static void launch_conv(cudaStream_t st, int grid, const CUtensorMap& map, int B, int H, int W, const bf16* w,
+                        const void* aux, void* out, bf16* out16, int* err)
+{
+    if (use_ws()) {
+        static bool attr = false;
+        if (!attr) {
+            JFG_CUDA(cudaFuncSetAttribute(k_conv_ws<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kWsSmem));
+            attr = true;
+        }
+        k_conv_ws<MODE><<<grid, kWsThreads, kWsSmem, st>>>(map, B, H, W, w, aux, out, out16, err);
+    } else {
+        k_conv_mid_tc<MODE><<<grid, kTcThreads, 0, st>>>(map, B, H, W, w, aux, out, out16, err);
+    }
+    JFG_CUDA(cudaGetLastError());
+    note_launch();
 }
 
 // out = relu(conv3x3(in, wk) [+ skip]) for BF16 (B, H, W, 32) images; wk is
@@ -361,11 +579,9 @@ void conv_mid_tc(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* in, 
     if (grid <= 0) return;
     const CUtensorMap map = conv_input_map(B, H, W, in);
     if (skip)
-        k_conv_mid_tc<kFwdSkip><<<grid, kTcThreads, 0, st>>>(map, B, H, W, wk, skip, out, nullptr, err);
+        launch_conv<kFwdSkip>(st, grid, map, B, H, W, wk, skip, out, nullptr, err);
     else
-        k_conv_mid_tc<kFwd><<<grid, kTcThreads, 0, st>>>(map, B, H, W, wk, nullptr, out, nullptr, err);
-    JFG_CUDA(cudaGetLastError());
-    note_launch();
+        launch_conv<kFwd>(st, grid, map, B, H, W, wk, nullptr, out, nullptr, err);
 }
 
 // Input gradient of a 32 -> 32 layer on the tensor cores: conv3x3 of the
@@ -379,11 +595,9 @@ void conv_mid_tc_bwd(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* 
     if (grid <= 0) return;
     const CUtensorMap map = conv_input_map(B, H, W, gin);
     if (mask)
-        k_conv_mid_tc<kBwdMask><<<grid, kTcThreads, 0, st>>>(map, B, H, W, wt, mask, out, out16, err);
+        launch_conv<kBwdMask>(st, grid, map, B, H, W, wt, mask, out, out16, err);
     else
-        k_conv_mid_tc<kBwdSkip><<<grid, kTcThreads, 0, st>>>(map, B, H, W, wt, skip, out, nullptr, err);
-    JFG_CUDA(cudaGetLastError());
-    note_launch();
+        launch_conv<kBwdSkip>(st, grid, map, B, H, W, wt, skip, out, nullptr, err);
 }
 
 }  // namespace jfg

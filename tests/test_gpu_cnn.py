@@ -106,3 +106,25 @@ def test_tcgen05_backward_matches_mma_sync(ctx, shape, monkeypatch):
     for l, (a, b) in enumerate(zip(unpack(g_tc), unpack(g_ms))):
         err = np.linalg.norm(a - b) / np.linalg.norm(b)
         assert err < 1e-2, (l, err)
+
+
+@pytest.mark.parametrize("shape", [(2, 45, 27), (1, 1025, 1025)])
+def test_warp_specialised_conv_equals_single_role(ctx, shape, monkeypatch):
+    """The warp-specialised tcgen05 pipeline (TMA, MMA and epilogue warps,
+    four halo stages, two TMEM accumulators) issues the same MMAs per tile as
+    the single-role kernel: forward outputs and gradients are bit-identical."""
+    rng = np.random.default_rng(13)
+    w = he_init(seed=8, gain_last=1.0)
+    x = torch.from_numpy(rng.standard_normal(shape).astype(np.float32)).cuda()
+    t = torch.from_numpy(rng.standard_normal(shape).astype(np.float32)).cuda()
+    net = LearnedSmoother(ctx, w)
+    monkeypatch.setenv("JFEM_CNN_TC", "1")
+    outs = []
+    for ws in ("1", "0"):
+        monkeypatch.setenv("JFEM_CNN_WS", ws)
+        y = net.forward(x).cpu().numpy()
+        _, g = net.loss_and_grad(x, t)
+        outs.append((y, g))
+    assert np.all(np.isfinite(outs[0][0]))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
