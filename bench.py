@@ -71,7 +71,7 @@ def parse():
                     help="batch-heat: implicit-Euler steps (the configuration has 50; fewer only for profiling)")
     ap.add_argument("--profile", default=None,
                     choices=["solve-fp64", "solve-mixed", "solve-mixed-nograph", "gs-mixed-nograph", "spmv64", "spmv32",
-                             "solve-learned", "solve-learned-nograph", "solve-fp64-nograph"],
+                             "solve-learned", "solve-learned-nograph", "solve-fp64-nograph", "precond-apply"],
                     help="set up, run the named operation --warmup + 1 times and exit (for ncu captures)")
     return ap.parse_args()
 
@@ -1138,6 +1138,14 @@ def run_stokes(args):
     t0 = time.time()
     prob = stokes_problem(args.cells if args.cells != CELLS else 256, 4, seed=0, pin_pressure=False)
     assemble_s = time.time() - t0
+    if args.profile == "precond-apply":      # the Schwarz-smoothed block preconditioner, --warmup + 1 times
+        sol = StokesSolver(ctx, prob)
+        v = np.random.default_rng(0).standard_normal(prob.system.n)
+        for _ in range(args.warmup + 1):
+            sol.P.mvMul(v)
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": args.profile}))
+        return
     b = prob.system.rhs
     tol = RTOL * float(np.linalg.norm(b))
     out = {}

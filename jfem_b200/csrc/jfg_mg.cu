@@ -147,8 +147,7 @@ constexpr int kTailMaxLevels = 8;         // coarse level included
 constexpr int kTailMaxRowsPerCta = 4095;  // 12-bit local row of a packed column
 constexpr int kTailThreads = 1024;
 constexpr int kTailSmemBudget = 224 * 1024;
-constexpr int kTailMetaInts = 23;         // per level: A, R, P (5 each), dinv, mask, rows per CTA, x, t, b, r, solo
-constexpr int kTailSoloRows = 320;        // levels this small run on CTA 0 alone (CTA barriers, no cluster barriers)
+constexpr int kTailMetaInts = 22;         // per level: A, R, P (5 each), dinv, mask, rows per CTA, x, t, b, r
 
 struct TailMat {
     int off_col, off_val;   // byte offsets of the column and value blocks in a CTA's shared memory
@@ -160,7 +159,6 @@ template <typename T>
 struct TailLevel {
     TailMat A, R, P;          // R: restriction into level l - 1, P: prolongation from level l - 1
     int Rl, n, runs;          // rows per CTA, rows, Jacobi sweeps
-    int solo;                 // all rows on CTA 0 (R = n): its phases end with CTA barriers of CTA 0 only
     int off_dinv, off_mask, off_x, off_t, off_b, off_r;
     T omega;
 };
@@ -197,34 +195,50 @@ __device__ __forceinline__ double ld_cluster(uint32_t a, double)
     return v;
 }
 
-// row sums of M times the distributed vector at byte offset M.xoff; f(t, s) per own row t
+// row sums of M times the distributed vector at byte offset M.xoff; f(t, s)
+// per own row t.  A thread takes rows t and t + blockDim together (all the
+// loads of both rows before their sums), so a level slightly larger than the
+// CTA's threads costs no second pass.
 template <typename T, class F>
 __device__ __forceinline__ void tail_spmv(unsigned char* sm, const TailMat& M, int c, F f)
 {
     const uint16_t* col = reinterpret_cast<const uint16_t*>(sm + M.off_col);
     const T* val = reinterpret_cast<const T*>(sm + M.off_val);
     const uint32_t xb = smem_u32(sm + M.xoff);
-    for (int t = threadIdx.x; t < M.R; t += blockDim.x) {
-        if (c * M.R + t >= M.m) break;
-        T s = 0;
+    const int nt = blockDim.x;
+    for (int t0 = threadIdx.x; t0 < M.R; t0 += 2 * nt) {
+        if (c * M.R + t0 >= M.m) break;
+        const int t1 = t0 + nt;
+        const bool two = t1 < M.R && c * M.R + t1 < M.m;
+        T s0 = 0, s1 = 0;
         for (int k0 = 0; k0 < M.W; k0 += 9) {
-            T v[9], xv[9];
+            // the remote x entries first (the long latency), the values from
+            // this CTA's shared memory while summing
+            T x0[9], x1[9];
+#pragma unroll
+            for (int u = 0; u < 9; u++) {
+                const int k = k0 + u;
+                x0[u] = x1[u] = 0;
+                if (k < M.W) {
+                    const unsigned q0 = col[k * M.R + t0];
+                    x0[u] = ld_cluster(cluster_addr(xb + (q0 & 0xFFFu) * (unsigned)sizeof(T), q0 >> 12), T());
+                    if (two) {
+                        const unsigned q1 = col[k * M.R + t1];
+                        x1[u] = ld_cluster(cluster_addr(xb + (q1 & 0xFFFu) * (unsigned)sizeof(T), q1 >> 12), T());
+                    }
+                }
+            }
 #pragma unroll
             for (int u = 0; u < 9; u++) {
                 const int k = k0 + u;
                 if (k < M.W) {
-                    const unsigned q = col[k * M.R + t];
-                    v[u] = val[k * M.R + t];
-                    xv[u] = ld_cluster(cluster_addr(xb + (q & 0xFFFu) * (unsigned)sizeof(T), q >> 12), T());
-                } else {
-                    v[u] = 0;
-                    xv[u] = 0;
+                    s0 += val[k * M.R + t0] * x0[u];
+                    if (two) s1 += val[k * M.R + t1] * x1[u];
                 }
             }
-#pragma unroll
-            for (int u = 0; u < 9; u++) s += v[u] * xv[u];
         }
-        f(t, s);
+        f(t0, s0);
+        if (two) f(t1, s1);
     }
 }
 
@@ -253,15 +267,6 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
     pdl_wait();
     if (P.done && *P.done) return;           // the same answer for every CTA of the cluster
     auto vec = [&](int off) { return reinterpret_cast<T*>(sm + off); };
-    // the barrier after a phase that wrote a level's vectors: the whole
-    // cluster for a distributed level, CTA 0 alone for a level it holds alone
-    // (the other CTAs skip it; every CTA runs the same cluster barriers)
-    auto sync_after = [&](int solo) {
-        if (!solo)
-            cl.sync();
-        else if (c == 0)
-            __syncthreads();
-    };
     {   // the restricted right-hand side of the top level, own rows
         const TailLevel<T>& L = P.lv[P.top];
         T* b = vec(L.off_b);
@@ -278,7 +283,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
         int cur_off = (L.runs % 2 == 1) ? L.off_x : L.off_t;
         if (l == P.top) {   // below the top the restriction phase did it
             tail_own(L.Rl, L.n, c, [&](int t) { cur[t] = (T)0 + (dinv[t] * b[t]) * om; });
-            sync_after(L.solo);
+            cl.sync();
         }
         for (int k = 1; k < L.runs; k++) {
             const int alt_off = cur_off == L.off_x ? L.off_t : L.off_x;
@@ -287,7 +292,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
             A.xoff = cur_off;
             const T* cu = cur;
             tail_spmv<T>(sm, A, c, [&](int t, T s) { alt[t] = cu[t] + (dinv[t] * (b[t] - s)) * om; });
-            sync_after(L.solo);
+            cl.sync();
             cur = alt;
             cur_off = alt_off;
         }
@@ -296,7 +301,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
             TailMat A = L.A;
             A.xoff = L.off_x;
             tail_spmv<T>(sm, A, c, [&](int t, T s) { r[t] = b[t] - s; });
-            sync_after(L.solo);
+            cl.sync();
         }
         {   // restriction into level l - 1 with zero boundary values (and its fused first sweep)
             const TailLevel<T>& Cl = P.lv[l - 1];
@@ -316,7 +321,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
             } else {
                 tail_spmv<T>(sm, R, c, [&](int t, T s) { bc[t] = mask[t] ? (T)0 : s; });
             }
-            sync_after(Cl.solo);
+            cl.sync();
         }
     }
     {   // coarsest level: x0 = Ainv * b0 in FP64, one warp per own row (the order of k_coarse_gemv)
@@ -336,21 +341,20 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
             s = warp_sum(s);
             if (lane == 0) x0[t] = (T)s;
         }
-        sync_after(L0.solo);
+        cl.sync();
     }
     for (int l = 1; l <= P.top; l++) {
         const TailLevel<T>& L = P.lv[l];
         const T* b = vec(L.off_b);
         const T* dinv = vec(L.off_dinv);
         const T om = L.omega;
-        if (!L.solo && P.lv[l - 1].solo) cl.sync();    // the other CTAs wait for CTA 0's levels
         {   // x += mask ? 0 : P x_{l-1}
             T* x = vec(L.off_x);
             const unsigned char* mask = sm + L.off_mask;
             TailMat Pm = L.P;
             Pm.xoff = P.lv[l - 1].off_x;
             tail_spmv<T>(sm, Pm, c, [&](int t, T s) { x[t] = x[t] + (mask[t] ? (T)0 : s); });
-            sync_after(L.solo);
+            cl.sync();
         }
         int cur_off = L.off_x;
         for (int k = 0; k < L.runs; k++) {
@@ -360,14 +364,14 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
             TailMat A = L.A;
             A.xoff = cur_off;
             tail_spmv<T>(sm, A, c, [&](int t, T s) { alt[t] = cu[t] + (dinv[t] * (b[t] - s)) * om; });
-            sync_after(L.solo);
+            cl.sync();
             cur_off = alt_off;
         }
         if (cur_off != L.off_x) {
             const T* cu = vec(cur_off);
             T* x = vec(L.off_x);
             tail_own(L.Rl, L.n, c, [&](int t) { x[t] = cu[t]; });
-            sync_after(L.solo);
+            cl.sync();
         }
     }
     {   // the result of the top level back to global memory
@@ -635,9 +639,7 @@ void MGImpl<T>::build_tail()
     }
     std::vector<double> hdinv;
     auto al16 = [](size_t b) { return (b + 15) / 16 * 16; };
-    // the smallest levels live on CTA 0 alone
-    auto solo = [&](int l) { return n[l] <= kTailSoloRows; };
-    auto rows_per = [&](int l, int C) { return solo(l) ? n[l] : (n[l] + C - 1) / C; };
+    auto rows_per = [&](int l, int C) { return (n[l] + C - 1) / C; };
     // byte sizes: constant package, then vectors
     auto sizes = [&](int top, int C, size_t& pkg, size_t& total) {
         pkg = 0;
@@ -736,7 +738,6 @@ void MGImpl<T>::build_tail()
             for (int t = 0; t < Rl && cc * Rl + t < n[l]; t++) pkg[cc * pkg_b + off + t] = mk[l][cc * Rl + t];
         off += al16((size_t)Rl);
         meta[17] = Rl;
-        meta[22] = solo(l) ? 1 : 0;
     }
     JFG_CHECK(off == pkg_b, JFG_ERR_CUDA, "tail package layout mismatch");
     for (int l = 0; l <= top; l++) {                      // vectors x, t, b, r
@@ -902,7 +903,6 @@ void MGImpl<T>::run_tail(bool first_sweep_done, const int* done, cudaStream_t st
         Lv.off_t = m[19];
         Lv.off_b = m[20];
         Lv.off_r = m[21];
-        Lv.solo = m[22];
         Lv.n = n[l];
         Lv.runs = sm[l].runs;
         Lv.omega = (T)sm[l].omega;
