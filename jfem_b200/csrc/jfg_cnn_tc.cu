@@ -337,13 +337,14 @@ k_conv_mid_tc(const __grid_constant__ CUtensorMap tin, int B, int H, int W, cons
 // Every wait is bounded (mbar_wait); a timeout sets *err, the roles stop, and
 // the copies and MMAs still in flight are waited for (bounded) before TMEM is
 // released.
-constexpr int kWsStages = 4;
 constexpr int kWsAcc = 2;
 constexpr int kWsThreads = 192;
-constexpr int kWsCtasPerSm = 3;
-constexpr int kWsSmem = kWBytes + kWsStages * kHaloBytes + 128;   // + alignment slack
+// shared memory of a CTA with ST halo stages (+ alignment slack); CTAs per SM
+// as many as fit 228 KB, at most 8 (64 TMEM columns each)
+template <int ST> constexpr int ws_smem() { return kWBytes + ST * kHaloBytes + 128; }
+template <int ST> constexpr int ws_ctas_per_sm() { return 228 * 1024 / (ws_smem<ST>() + 1024) < 8 ? 228 * 1024 / (ws_smem<ST>() + 1024) : 8; }
 
-template <int MODE>
+template <int MODE, int kWsStages>
 __global__ void __launch_bounds__(kWsThreads)
 k_conv_ws(const __grid_constant__ CUtensorMap tin, int B, int H, int W, const bf16* __restrict__ wk,
           const void* __restrict__ aux, void* __restrict__ out, bf16* __restrict__ out16, int* __restrict__ err)
@@ -535,20 +536,41 @@ static CUtensorMap conv_input_map(int B, int H, int W, const __nv_bfloat16* in)
 }
 
 // JFEM_CNN_WS=0 selects the single-role kernel (k_conv_mid_tc) instead of the
-// warp-specialised pipeline (k_conv_ws)
+// warp-specialised pipeline (k_conv_ws); JFEM_CNN_WS_STAGES = 2, 3 or 4 sets
+// its halo stages (default kWsDefaultStages)
+constexpr int kWsDefaultStages = 4;
 static bool use_ws()
 {
     const char* e = getenv("JFEM_CNN_WS");
     return !(e && e[0] == '0');
 }
+static int ws_stages()
+{
+    const char* e = getenv("JFEM_CNN_WS_STAGES");
+    const int v = e ? atoi(e) : kWsDefaultStages;
+    return (v == 2 || v == 3 || v == 4) ? v : kWsDefaultStages;
+}
+static int ws_ctas(int st) { return st == 2 ? ws_ctas_per_sm<2>() : (st == 3 ? ws_ctas_per_sm<3>() : ws_ctas_per_sm<4>()); }
 
 static int conv_grid(int B, int H, int W, const void* in)
 {
     const long long ntiles = (long long)((W + kTW - 1) / kTW) * ((H + kTH - 1) / kTH) * B;
     JFG_CHECK(ntiles < (1LL << 31), JFG_ERR_UNSUPPORTED, "image too large for the tensor-core convolution");
     JFG_CHECK(((uintptr_t)in & 15) == 0, JFG_ERR_BAD_ARG, "convolution input not 16-byte aligned");
-    const int per_sm = use_ws() ? kWsCtasPerSm : kTcCtasPerSm;
+    const int per_sm = use_ws() ? ws_ctas(ws_stages()) : kTcCtasPerSm;
     return (int)std::min<long long>(ntiles, (long long)sm_count() * per_sm);
+}
+
+template <int MODE, int ST>
+static void launch_ws(cudaStream_t st, int grid, const CUtensorMap& map, int B, int H, int W, const bf16* w,
+                      const void* aux, void* out, bf16* out16, int* err)
+{
+    static bool attr = false;
+    if (!attr) {
+        JFG_CUDA(cudaFuncSetAttribute(k_conv_ws<MODE, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, ws_smem<ST>()));
+        attr = true;
+    }
+    k_conv_ws<MODE, ST><<<grid, kWsThreads, ws_smem<ST>(), st>>>(map, B, H, W, w, aux, out, out16, err);
 }
 
 template <int MODE>
@@ -556,12 +578,11 @@ static void launch_conv(cudaStream_t st, int grid, const CUtensorMap& map, int B
                         const void* aux, void* out, bf16* out16, int* err)
 {
     if (use_ws()) {
-        static bool attr = false;
-        if (!attr) {
-            JFG_CUDA(cudaFuncSetAttribute(k_conv_ws<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kWsSmem));
-            attr = true;
+        switch (ws_stages()) {
+        case 2: launch_ws<MODE, 2>(st, grid, map, B, H, W, w, aux, out, out16, err); break;
+        case 3: launch_ws<MODE, 3>(st, grid, map, B, H, W, w, aux, out, out16, err); break;
+        default: launch_ws<MODE, 4>(st, grid, map, B, H, W, w, aux, out, out16, err); break;
         }
-        k_conv_ws<MODE><<<grid, kWsThreads, kWsSmem, st>>>(map, B, H, W, w, aux, out, out16, err);
     } else {
         k_conv_mid_tc<MODE><<<grid, kTcThreads, 0, st>>>(map, B, H, W, w, aux, out, out16, err);
     }

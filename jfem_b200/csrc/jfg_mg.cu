@@ -195,50 +195,34 @@ __device__ __forceinline__ double ld_cluster(uint32_t a, double)
     return v;
 }
 
-// row sums of M times the distributed vector at byte offset M.xoff; f(t, s)
-// per own row t.  A thread takes rows t and t + blockDim together (all the
-// loads of both rows before their sums), so a level slightly larger than the
-// CTA's threads costs no second pass.
+// row sums of M times the distributed vector at byte offset M.xoff; f(t, s) per own row t
 template <typename T, class F>
 __device__ __forceinline__ void tail_spmv(unsigned char* sm, const TailMat& M, int c, F f)
 {
     const uint16_t* col = reinterpret_cast<const uint16_t*>(sm + M.off_col);
     const T* val = reinterpret_cast<const T*>(sm + M.off_val);
     const uint32_t xb = smem_u32(sm + M.xoff);
-    const int nt = blockDim.x;
-    for (int t0 = threadIdx.x; t0 < M.R; t0 += 2 * nt) {
-        if (c * M.R + t0 >= M.m) break;
-        const int t1 = t0 + nt;
-        const bool two = t1 < M.R && c * M.R + t1 < M.m;
-        T s0 = 0, s1 = 0;
+    for (int t = threadIdx.x; t < M.R; t += blockDim.x) {
+        if (c * M.R + t >= M.m) break;
+        T s = 0;
         for (int k0 = 0; k0 < M.W; k0 += 9) {
-            // the remote x entries first (the long latency), the values from
-            // this CTA's shared memory while summing
-            T x0[9], x1[9];
-#pragma unroll
-            for (int u = 0; u < 9; u++) {
-                const int k = k0 + u;
-                x0[u] = x1[u] = 0;
-                if (k < M.W) {
-                    const unsigned q0 = col[k * M.R + t0];
-                    x0[u] = ld_cluster(cluster_addr(xb + (q0 & 0xFFFu) * (unsigned)sizeof(T), q0 >> 12), T());
-                    if (two) {
-                        const unsigned q1 = col[k * M.R + t1];
-                        x1[u] = ld_cluster(cluster_addr(xb + (q1 & 0xFFFu) * (unsigned)sizeof(T), q1 >> 12), T());
-                    }
-                }
-            }
+            T v[9], xv[9];
 #pragma unroll
             for (int u = 0; u < 9; u++) {
                 const int k = k0 + u;
                 if (k < M.W) {
-                    s0 += val[k * M.R + t0] * x0[u];
-                    if (two) s1 += val[k * M.R + t1] * x1[u];
+                    const unsigned q = col[k * M.R + t];
+                    v[u] = val[k * M.R + t];
+                    xv[u] = ld_cluster(cluster_addr(xb + (q & 0xFFFu) * (unsigned)sizeof(T), q >> 12), T());
+                } else {
+                    v[u] = 0;
+                    xv[u] = 0;
                 }
             }
+#pragma unroll
+            for (int u = 0; u < 9; u++) s += v[u] * xv[u];
         }
-        f(t0, s0);
-        if (two) f(t1, s1);
+        f(t, s);
     }
 }
 

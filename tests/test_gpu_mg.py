@@ -89,7 +89,7 @@ def test_vcycle_tail_matches_per_launch(ctx, monkeypatch, p, coarse, L, precisio
     (v1, x1, i1, h1), (v0, x0, i0, h0) = outs
     np.testing.assert_allclose(v1, v0, rtol=1e-11, atol=1e-12 * np.abs(v0).max())
     assert i1 == i0
-    np.testing.assert_allclose(h1, h0, rtol=1e-5 if precision != "fp64" else 1e-9)
+    np.testing.assert_allclose(h1, h0, rtol=1e-4 if precision != "fp64" else 1e-9)
     np.testing.assert_allclose(x1, x0, rtol=1e-7, atol=1e-9 * np.abs(x0).max())
     mats_o = [coo_oracle(s) for s in h.systems]
     prol_o = [O.CooMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l]) for l in range(L - 1)]
