@@ -321,42 +321,52 @@ k_conv_mid_tc(const __grid_constant__ CUtensorMap tin, int B, int H, int W, cons
 }
 
 // ---------------------------------------------------------------------------
-// Warp-specialised pipeline (the default).  Per CTA of 192 threads:
-//   warp 0 (one lane): TMA producer -- the four 8-channel halo planes of tile
-//     i into halo stage i % kWsStages, once the MMAs of tile i - kWsStages
-//     released that stage (mbarrier `empty`);
-//   warp 1 (one lane): MMA issuer -- waits for the stage (`full`, TMA
-//     transaction bytes) and for a free TMEM accumulator (`tempty`), issues
-//     the 18 MMAs, and commits them to `empty` (stage free) and `tfull`
-//     (accumulator ready);
+// Warp-specialised pipeline (the default).  Per CTA of 256 threads:
+//   warp 0 (one lane): TMA producer -- tile i's whole halo (18 x 10 pixels x
+//     32 channels) as ONE box with a 64-byte inner extent into staging buffer
+//     i % ST, once the transposers released it (mbarrier `sempty`); one
+//     64-byte row per pixel instead of four 16-byte ones;
+//   warps 6-7: transposers -- wait for the box (`sfull`, transaction bytes)
+//     and for a free plane buffer (`pempty`), copy the pixels' four 16-byte
+//     channel chunks into the four 8-channel planes the MMA descriptors view,
+//     make those writes visible to the tensor core (fence.proxy.async) and
+//     release the staging buffer (`sempty`) and publish the planes (`pfull`);
+//   warp 1 (one lane): MMA issuer -- waits for the planes (`pfull`) and a free
+//     TMEM accumulator (`tempty`), issues the 18 MMAs and commits them to
+//     `pempty` (planes free) and `tfull` (accumulator ready);
 //   warps 2-5: epilogue -- each reads its 32 TMEM lanes (warp w owns lanes
 //     32 (w % 4) ...) of the ready accumulator, releases it (`tempty`, one
 //     arrival per warp), then combines and stores its 32 pixels.
-// Loads run up to kWsStages tiles ahead and the MMAs of the next tile overlap
-// the epilogue of the current one; no CTA-wide barrier inside the tile loop.
-// Every wait is bounded (mbar_wait); a timeout sets *err, the roles stop, and
-// the copies and MMAs still in flight are waited for (bounded) before TMEM is
-// released.
+// No CTA-wide barrier inside the tile loop.  Every wait is bounded
+// (mbar_wait); a timeout sets *err, every role stops, and the copies and MMAs
+// still in flight are waited for (bounded) before TMEM is released.
 constexpr int kWsAcc = 2;
-constexpr int kWsThreads = 192;
-// shared memory of a CTA with ST halo stages (+ alignment slack); CTAs per SM
-// as many as fit 228 KB, at most 8 (64 TMEM columns each)
-template <int ST> constexpr int ws_smem() { return kWBytes + ST * kHaloBytes + 128; }
+constexpr int kWsThreads = 256;
+constexpr int kStageBytes = kHH * kHW * 64;      // 11,520: the halo as 64-byte pixels
+// shared memory of a CTA with ST stages (+ alignment slack); CTAs per SM as
+// many as fit 228 KB, at most 8 (64 TMEM columns each)
+template <int ST> constexpr int ws_smem() { return kWBytes + ST * (kStageBytes + kHaloBytes) + 128; }
 template <int ST> constexpr int ws_ctas_per_sm() { return 228 * 1024 / (ws_smem<ST>() + 1024) < 8 ? 228 * 1024 / (ws_smem<ST>() + 1024) : 8; }
 
-template <int MODE, int kWsStages>
+__device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+template <int MODE, int ST>
 __global__ void __launch_bounds__(kWsThreads)
 k_conv_ws(const __grid_constant__ CUtensorMap tin, int B, int H, int W, const bf16* __restrict__ wk,
           const void* __restrict__ aux, void* __restrict__ out, bf16* __restrict__ out16, int* __restrict__ err)
 {
     extern __shared__ unsigned char dsm_raw[];
     unsigned char* dsm = reinterpret_cast<unsigned char*>(((uintptr_t)dsm_raw + 127) & ~(uintptr_t)127);
-    unsigned char* wsm = dsm;                          // weights, kWBytes
-    unsigned char* halo = dsm + kWBytes;               // kWsStages x kHaloBytes
-    __shared__ __align__(8) uint64_t full[kWsStages], empty[kWsStages], tfull[kWsAcc], tempty[kWsAcc];
+    unsigned char* wsm = dsm;                                 // weights, kWBytes
+    unsigned char* stage = dsm + kWBytes;                     // ST x kStageBytes (TMA boxes)
+    unsigned char* planes = stage + ST * kStageBytes;         // ST x kHaloBytes (MMA operands)
+    __shared__ __align__(8) uint64_t sfull[ST], sempty[ST], pfull[ST], pempty[ST], tfull[kWsAcc], tempty[kWsAcc];
     __shared__ uint32_t tmem_sh;
     __shared__ volatile int s_stop;
-    __shared__ int s_loads, s_mmas;                    // issued counts, for the error path
+    __shared__ int s_loads, s_trans, s_mmas;                  // progress counts, for the error path
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     for (int i = tid; i < 32 * 36; i += kWsThreads) {
         const int co = i / 36, j = i % 36;
@@ -371,10 +381,13 @@ k_conv_ws(const __grid_constant__ CUtensorMap tin, int B, int H, int W, const bf
     if (tid == 32) {
         s_stop = 0;
         s_loads = 0;
+        s_trans = 0;
         s_mmas = 0;
-        for (int q = 0; q < kWsStages; q++) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[q])) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[q])) : "memory");
+        for (int q = 0; q < ST; q++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&sfull[q])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 2;" ::"r"(smem_u32(&sempty[q])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 2;" ::"r"(smem_u32(&pfull[q])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&pempty[q])) : "memory");
         }
         for (int q = 0; q < kWsAcc; q++) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&tfull[q])) : "memory");
@@ -397,28 +410,52 @@ k_conv_ws(const __grid_constant__ CUtensorMap tin, int B, int H, int W, const bf
     if (warp == 0) {
         if (lane == 0) {                               // TMA producer
             for (int i = 0; i < cnt && !s_stop; i++) {
-                const int q = i % kWsStages;
-                if (i >= kWsStages && !mbar_wait(smem_u32(&empty[q]), (uint32_t)((i / kWsStages - 1) & 1))) {
+                const int q = i % ST;
+                if (i >= ST && !mbar_wait(smem_u32(&sempty[q]), (uint32_t)((i / ST - 1) & 1))) {
                     s_stop = 1;
                     break;
                 }
                 const int t = tile_of(i);
                 const int b = t / per_img, rem = t - b * per_img;
                 const int y0 = (rem / tilesx) * kTH, x0 = (rem % tilesx) * kTW;
-                const uint32_t bar = smem_u32(&full[q]);
-                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(4 * kPlaneData)
+                const uint32_t bar = smem_u32(&sfull[q]);
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kStageBytes)
                              : "memory");
-                const uint32_t dst = smem_u32(halo + q * kHaloBytes);
-#pragma unroll
-                for (int p = 0; p < 4; p++) tma_plane(dst + p * kPlane, &tin, 8 * p, x0 - 1, y0 - 1, b, bar);
+                tma_plane(smem_u32(stage + q * kStageBytes), &tin, 0, x0 - 1, y0 - 1, b, bar);
                 s_loads = i + 1;
+            }
+        }
+    } else if (warp >= 6) {                            // transposers
+        const int tt = tid - 192;
+        for (int i = 0; i < cnt; i++) {
+            const int q = i % ST;
+            bool ok = !s_stop && mbar_wait(smem_u32(&sfull[q]), (uint32_t)((i / ST) & 1));
+            if (ok && i >= ST) ok = mbar_wait(smem_u32(&pempty[q]), (uint32_t)((i / ST - 1) & 1));
+            if (!__all_sync(0xffffffffu, ok)) {
+                if (lane == 0) s_stop = 1;
+                break;
+            }
+            const unsigned char* src = stage + q * kStageBytes;
+            unsigned char* dst = planes + q * kHaloBytes;
+            for (int m = tt; m < kHH * kHW * 4; m += 64) {
+                const int pix = m >> 2, part = m & 3;
+                *reinterpret_cast<uint4*>(dst + part * kPlane + pix * 16) =
+                    *reinterpret_cast<const uint4*>(src + pix * 64 + part * 16);
+            }
+            // the planes are read by the tensor core (async proxy)
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(smem_u32(&sempty[q]));
+                mbar_arrive(smem_u32(&pfull[q]));
+                if (warp == 6) s_trans = i + 1;
             }
         }
     } else if (warp == 1) {
         if (lane == 0) {                               // MMA issuer
             for (int i = 0; i < cnt && !s_stop; i++) {
-                const int q = i % kWsStages, a = i % kWsAcc;
-                if (!mbar_wait(smem_u32(&full[q]), (uint32_t)((i / kWsStages) & 1))) {
+                const int q = i % ST, a = i % kWsAcc;
+                if (!mbar_wait(smem_u32(&pfull[q]), (uint32_t)((i / ST) & 1))) {
                     s_stop = 1;
                     break;
                 }
@@ -427,7 +464,7 @@ k_conv_ws(const __grid_constant__ CUtensorMap tin, int B, int H, int W, const bf
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t hb = smem_u32(halo + q * kHaloBytes);
+                const uint32_t hb = smem_u32(planes + q * kHaloBytes);
 #pragma unroll
                 for (int tap = 0; tap < 9; tap++) {
                     const int dy = tap / 3, dx = tap % 3;
@@ -445,7 +482,7 @@ k_conv_ws(const __grid_constant__ CUtensorMap tin, int B, int H, int W, const bf
                     }
                 }
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                 smem_u32(&empty[q]))
+                                 smem_u32(&pempty[q]))
                              : "memory");
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                                  smem_u32(&tfull[a]))
@@ -479,8 +516,7 @@ k_conv_ws(const __grid_constant__ CUtensorMap tin, int B, int H, int W, const bf
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
-            if (lane == 0)
-                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[a])) : "memory");
+            if (lane == 0) mbar_arrive(smem_u32(&tempty[a]));
             const int t = tile_of(i);
             const int b = t / per_img, rem = t - b * per_img;
             const int gy = (rem / tilesx) * kTH + (m >> 3), gx = (rem % tilesx) * kTW + (m & 7);
@@ -491,8 +527,8 @@ k_conv_ws(const __grid_constant__ CUtensorMap tin, int B, int H, int W, const bf
     if (s_stop && tid == 32) {
         // report, then let the copies and MMAs still in flight finish (bounded) before TMEM is freed
         atomicOr(err, 1);
-        const int nl = s_loads, nm = s_mmas;
-        for (int k = nm; k < nl; k++) mbar_wait(smem_u32(&full[k % kWsStages]), (uint32_t)((k / kWsStages) & 1));
+        const int nl = s_loads, nt = s_trans, nm = s_mmas;
+        for (int k = nt; k < nl; k++) mbar_wait(smem_u32(&sfull[k % ST]), (uint32_t)((k / ST) & 1));
         if (nm > 0) mbar_wait(smem_u32(&tfull[(nm - 1) % kWsAcc]), (uint32_t)(((nm - 1) / kWsAcc) & 1));
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -520,12 +556,13 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
     return fn;
 }
 
-static CUtensorMap conv_input_map(int B, int H, int W, const __nv_bfloat16* in)
+// box_c: channels per box (32: the whole 64-byte pixel; 8: one plane)
+static CUtensorMap conv_input_map(int B, int H, int W, const __nv_bfloat16* in, int box_c)
 {
     CUtensorMap map;
     const cuuint64_t dims[4] = {32, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
     const cuuint64_t strides[3] = {64, (cuuint64_t)W * 64, (cuuint64_t)W * H * 64};
-    const cuuint32_t box[4] = {8, (cuuint32_t)kHW, (cuuint32_t)kHH, 1};
+    const cuuint32_t box[4] = {(cuuint32_t)box_c, (cuuint32_t)kHW, (cuuint32_t)kHH, 1};
     const cuuint32_t estride[4] = {1, 1, 1, 1};
     CUresult r = tensor_map_encoder()(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(in), dims,
                                       strides, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -537,8 +574,8 @@ static CUtensorMap conv_input_map(int B, int H, int W, const __nv_bfloat16* in)
 
 // JFEM_CNN_WS=0 selects the single-role kernel (k_conv_mid_tc) instead of the
 // warp-specialised pipeline (k_conv_ws); JFEM_CNN_WS_STAGES = 2, 3 or 4 sets
-// its halo stages (default kWsDefaultStages)
-constexpr int kWsDefaultStages = 4;
+// its stages (default kWsDefaultStages)
+constexpr int kWsDefaultStages = 2;
 static bool use_ws()
 {
     const char* e = getenv("JFEM_CNN_WS");
@@ -598,7 +635,7 @@ void conv_mid_tc(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* in, 
 {
     const int grid = conv_grid(B, H, W, in);
     if (grid <= 0) return;
-    const CUtensorMap map = conv_input_map(B, H, W, in);
+    const CUtensorMap map = conv_input_map(B, H, W, in, use_ws() ? 32 : 8);
     if (skip)
         launch_conv<kFwdSkip>(st, grid, map, B, H, W, wk, skip, out, nullptr, err);
     else
@@ -614,7 +651,7 @@ void conv_mid_tc_bwd(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* 
 {
     const int grid = conv_grid(B, H, W, gin);
     if (grid <= 0) return;
-    const CUtensorMap map = conv_input_map(B, H, W, gin);
+    const CUtensorMap map = conv_input_map(B, H, W, gin, use_ws() ? 32 : 8);
     if (mask)
         launch_conv<kBwdMask>(st, grid, map, B, H, W, wt, mask, out, out16, err);
     else

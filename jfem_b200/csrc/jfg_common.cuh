@@ -143,7 +143,13 @@ struct Matrix {
     // its values with one aligned vector load per offset.  The SELL layout is kept as
     // well (other kernels read it); products with a stencil copy of their
     // value type use this layout.
+    // The same point layout also serves the grid transfers between Q1 levels
+    // (st_kind 1: prolongation, fine rows; 2: restriction, coarse rows): the
+    // columns of a regular row are center(r) + offsets, center(r) computed
+    // from the row's grid position (strides st_S of the rows, st_S2 of the
+    // columns); st_K values per row (4 or 9).
     int st = 0;
+    int st_kind = 0, st_K = 9, st_S2 = 0;
     int st_S = 0, st_lo = 0, st_hi = 0, st_nirr = 0, st_ld = 0;
     int st_nb_reg = 0;                  // CTAs of the regular rows (a persistent grid over row pairs)
     int st_nb_irr = 0;                  // CTAs of the irregular rows
@@ -191,6 +197,10 @@ Matrix* assemble_tp(Context* c, const jfg_tp_desc& d, const double* h_kappa, con
                     int* h_node_of_grid, int* h_boundary);
 Matrix* assemble_th(Context* c, int cx, int cy, double nu, const double* h_force_qp, int lid, int pin,
                     double* h_rhs, int* h_boundary);
+// The transfer point layout (Matrix::st, kinds 1 / 2) of a prolongation or
+// restriction between Q1 grids with strides S (rows) and S2 (columns); a
+// no-op when it does not fit or after precision copies exist.
+void matrix_build_transfer_layout(Matrix* m, int kind, int S, int S2);
 void matrix_ensure_fp32(Matrix* m);
 void matrix_ensure_bf16(Matrix* m);
 void matrix_ensure_fp16(Matrix* m);

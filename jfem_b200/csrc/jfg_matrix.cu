@@ -198,35 +198,52 @@ __global__ void k_expand_rows(int rows, const int* ptr, int* ri)
     for (int k = ptr[r]; k < ptr[r + 1]; k++) ri[k] = r;
 }
 
-// stencil layout: a row is regular when it couples only to r + {-S-1..-S+1,
-// -1..1, S-1..S+1} and all nine of those columns exist
-__global__ void k_st_classify(int rows, int S, const int* __restrict__ ptr, const int* __restrict__ col,
-                              unsigned char* __restrict__ reg)
+// Point layouts (Matrix::st): row r is regular when its entries all sit at
+// center(r) + off_k for the layout's offsets and all those columns exist.
+//   kind 0 (9-point stencil):    center = r, offsets (a - 1) S + (b - 1), a, b in 0..2
+//   kind 1 (prolongation, rows = fine nodes with grid stride S, columns =
+//     coarse nodes with stride S2): center = (g / 2) S2 + h / 2 for
+//     (g, h) = (r / S, r % S), offsets {0, 1, S2, S2 + 1}
+//   kind 2 (restriction, rows = coarse nodes with stride S, columns = fine
+//     nodes with stride S2): center = 2 g S2 + 2 h, offsets (a - 1) S2 + (b - 1)
+__device__ __forceinline__ int pt_center(int kind, int S, int S2, int r)
+{
+    if (kind == 0) return r;
+    const int g = r / S, h = r - g * S;
+    return kind == 1 ? (g >> 1) * S2 + (h >> 1) : 2 * g * S2 + 2 * h;
+}
+// offset d -> slot (ascending column order), -1 when d is not an offset
+__device__ __forceinline__ int pt_slot(int kind, int S, int S2, int d)
+{
+    if (kind == 1) return d == 0 ? 0 : d == 1 ? 1 : d == S2 ? 2 : d == S2 + 1 ? 3 : -1;
+    const int X = kind == 0 ? S : S2;
+    if (d >= -1 && d <= 1) return d + 4;
+    if (d >= -X - 1 && d <= -X + 1) return d + X + 1;
+    if (d >= X - 1 && d <= X + 1) return d - X + 7;
+    return -1;
+}
+
+__global__ void k_st_classify(int rows, int cols, int kind, int S, int S2, const int* __restrict__ ptr,
+                              const int* __restrict__ col, unsigned char* __restrict__ reg)
 {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= rows) return;
-    bool ok = r - S - 1 >= 0 && r + S + 1 < rows;
-    for (int k = ptr[r]; ok && k < ptr[r + 1]; k++) {
-        const int d = col[k] - r;
-        const int a = d < 0 ? -d : d;
-        ok = a <= 1 || (a >= S - 1 && a <= S + 1);
-    }
+    const int c = pt_center(kind, S, S2, r);
+    const int X = kind == 0 ? S : S2;
+    const int lo = kind == 1 ? 0 : -X - 1, hi = kind == 1 ? S2 + 1 : X + 1;
+    bool ok = c + lo >= 0 && c + hi < cols;
+    for (int k = ptr[r]; ok && k < ptr[r + 1]; k++) ok = pt_slot(kind, S, S2, col[k] - c) >= 0;
     reg[r] = ok ? 1 : 0;
 }
 
-// offset d of a regular row -> slot 0..8 in ascending column order
-__device__ __forceinline__ int st_slot(int d, int S)
-{
-    return d <= -S + 1 ? d + S + 1 : (d >= S - 1 ? d - S + 7 : d + 4);
-}
-
-__global__ void k_st_fill(int lo, int nreg, int ld, int S, const int* __restrict__ ptr, const int* __restrict__ col,
-                          const double* __restrict__ val, double* __restrict__ st)
+__global__ void k_st_fill(int kind, int lo, int nreg, int ld, int S, int S2, const int* __restrict__ ptr,
+                          const int* __restrict__ col, const double* __restrict__ val, double* __restrict__ st)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nreg) return;
     const int r = lo + i;
-    for (int k = ptr[r]; k < ptr[r + 1]; k++) st[(int64_t)st_slot(col[k] - r, S) * ld + i] = val[k];
+    const int c = pt_center(kind, S, S2, r);
+    for (int k = ptr[r]; k < ptr[r + 1]; k++) st[(int64_t)pt_slot(kind, S, S2, col[k] - c) * ld + i] = val[k];
 }
 
 // CSR copy of the irregular rows (their entries in column order)
@@ -265,47 +282,54 @@ bool stencil_enabled()
     return !(e && e[0] == '0');
 }
 
-// Values-only 9-point layout (see Matrix::st).  The stride S is read off a
-// few middle rows (largest column offset - 1); the layout is kept when the
-// contiguous run of regular rows around the middle row leaves at most a
-// quarter of the rows outside it.
-static void build_stencil(Matrix* M, const std::vector<int>& len)
+// Point layout of M (see Matrix::st) for the rows whose entries fit it:
+// kind 0 detects the 9-point stencil's stride S off a few middle rows
+// (largest column offset - 1); kinds 1 and 2 (grid transfers) take S and S2
+// from the level matrices.  The layout is kept when the contiguous run of
+// regular rows around the middle row leaves at most a quarter of the rows
+// outside it.
+static void build_point_layout(Matrix* M, const std::vector<int>& len, int kind, int S, int S2)
 {
     const int n = M->rows;
-    if (n < 256 || M->rows != M->cols || !stencil_enabled()) return;
+    if (n < 256 || M->st || !stencil_enabled()) return;
+    if (kind == 0 && M->rows != M->cols) return;
     cudaStream_t s = M->ctx->stream;
-    std::vector<int> hp(n + 1);
-    JFG_CUDA(cudaMemcpyAsync(hp.data(), M->csr_ptr.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
-    JFG_CUDA(cudaStreamSynchronize(s));
-    int S = 0;
-    for (int j = 0; j < 16 && !S; j++) {
-        const int r = n / 2 + j;
-        const int a = hp[r], e = hp[r + 1];
-        if (e - a < 2 || e - a > 9) continue;
-        std::vector<int> c(e - a);
-        JFG_CUDA(cudaMemcpyAsync(c.data(), M->csr_col.p + a, sizeof(int) * (e - a), cudaMemcpyDeviceToHost, s));
+    if (kind == 0) {
+        std::vector<int> hp(n + 1);
+        JFG_CUDA(cudaMemcpyAsync(hp.data(), M->csr_ptr.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost, s));
         JFG_CUDA(cudaStreamSynchronize(s));
-        const int cand = c.back() - r - 1;
-        if (cand < 3) continue;
-        bool ok = true;
-        for (int v : c) {
-            const int d = std::abs(v - r);
-            ok = ok && (d <= 1 || (d >= cand - 1 && d <= cand + 1));
+        S = 0;
+        for (int j = 0; j < 16 && !S; j++) {
+            const int r = n / 2 + j;
+            const int a = hp[r], e = hp[r + 1];
+            if (e - a < 2 || e - a > 9) continue;
+            std::vector<int> c(e - a);
+            JFG_CUDA(cudaMemcpyAsync(c.data(), M->csr_col.p + a, sizeof(int) * (e - a), cudaMemcpyDeviceToHost, s));
+            JFG_CUDA(cudaStreamSynchronize(s));
+            const int cand = c.back() - r - 1;
+            if (cand < 3) continue;
+            bool ok = true;
+            for (int v : c) {
+                const int d = std::abs(v - r);
+                ok = ok && (d <= 1 || (d >= cand - 1 && d <= cand + 1));
+            }
+            if (ok) S = cand;
         }
-        if (ok) S = cand;
+        S2 = 0;
     }
-    if (!S) return;
+    if (S < 3 || (kind != 0 && S2 < 3)) return;
+    const int K = kind == 1 ? 4 : 9;
     DevBuf<unsigned char> reg;
     reg.alloc((size_t)n);
-    k_st_classify<<<nblk(n), 256, 0, s>>>(n, S, M->csr_ptr.p, M->csr_col.p, reg.p);
+    k_st_classify<<<nblk(n), 256, 0, s>>>(n, M->cols, kind, S, S2, M->csr_ptr.p, M->csr_col.p, reg.p);
     JFG_CUDA(cudaGetLastError());
     std::vector<unsigned char> hr(n);
     JFG_CUDA(cudaMemcpyAsync(hr.data(), reg.p, (size_t)n, cudaMemcpyDeviceToHost, s));
     JFG_CUDA(cudaStreamSynchronize(s));
-    // the stencil range: from the row after the last irregular row of the
-    // first half to the first irregular row of the second half (on 2-D grids
-    // numbered by first appearance the irregular rows are the first three and
-    // the last grid lines; the regular Dirichlet rows among them go to CSR)
+    // the range: from the row after the last irregular row of the first half
+    // to the first irregular row of the second half (on 2-D grids numbered by
+    // first appearance the irregular rows are the first and the last grid
+    // lines; the regular Dirichlet rows among them go to CSR)
     const int mid = n / 2;
     int lo = mid, hi = mid;
     while (lo > 0 && hr[lo - 1]) lo--;
@@ -322,31 +346,53 @@ static void build_stencil(Matrix* M, const std::vector<int>& len)
         }
     const int64_t irr_nnz = iptr.back();
     const int ld = (nreg + 7) / 8 * 8;
+    M->st_kind = kind;
+    M->st_K = K;
     M->st_S = S;
+    M->st_S2 = S2;
     M->st_lo = lo;
     M->st_hi = hi;
     M->st_nirr = nirr;
     M->st_ld = ld;
-    M->st_len = 9 * (int64_t)ld + irr_nnz;
+    M->st_len = (int64_t)K * ld + irr_nnz;
     M->st_val.alloc((size_t)M->st_len);
     M->st_irow.alloc(nirr ? (size_t)nirr : 1);
     M->st_iptr.alloc((size_t)nirr + 1);
     M->st_icol.alloc(irr_nnz ? (size_t)irr_nnz : 1);
-    JFG_CUDA(cudaMemsetAsync(M->st_val.p, 0, sizeof(double) * 9 * (size_t)ld, s));
-    k_st_fill<<<nblk(nreg), 256, 0, s>>>(lo, nreg, ld, S, M->csr_ptr.p, M->csr_col.p, M->csr_val.p, M->st_val.p);
+    JFG_CUDA(cudaMemsetAsync(M->st_val.p, 0, sizeof(double) * K * (size_t)ld, s));
+    k_st_fill<<<nblk(nreg), 256, 0, s>>>(kind, lo, nreg, ld, S, S2, M->csr_ptr.p, M->csr_col.p, M->csr_val.p,
+                                        M->st_val.p);
     JFG_CUDA(cudaGetLastError());
     if (nirr) {
         JFG_CUDA(cudaMemcpyAsync(M->st_irow.p, irow.data(), sizeof(int) * nirr, cudaMemcpyHostToDevice, s));
         JFG_CUDA(cudaMemcpyAsync(M->st_iptr.p, iptr.data(), sizeof(int) * (nirr + 1), cudaMemcpyHostToDevice, s));
         k_st_irregular<<<nblk(nirr), 256, 0, s>>>(nirr, M->st_irow.p, M->st_iptr.p, M->csr_ptr.p, M->csr_col.p,
-                                                 M->csr_val.p, M->st_icol.p, M->st_val.p + 9 * (int64_t)ld);
+                                                 M->csr_val.p, M->st_icol.p, M->st_val.p + (int64_t)K * ld);
         JFG_CUDA(cudaGetLastError());
     }
-    M->st_nb_reg = (int)nblk(nreg, kThreads * 2);          // one pair per thread (the launch caps the grid)
+    // the 9-point kernel takes rows in pairs (its launch caps the grid); the transfer kernel one row per thread
+    M->st_nb_reg = (int)nblk(nreg, kind == 0 ? kThreads * 2 : kThreads);
     M->st_nb_irr = (int)nblk(nirr, kThreads);
     M->nblocks = std::max(M->nblocks, M->st_nb_reg + M->st_nb_irr);
     JFG_CUDA(cudaStreamSynchronize(s));
     M->st = 1;
+}
+
+// Row lengths of a matrix's CSR on the host.
+static std::vector<int> row_lengths(const Matrix* M)
+{
+    std::vector<int> hp(M->rows + 1), len(M->rows + 1, 0);
+    JFG_CUDA(cudaMemcpyAsync(hp.data(), M->csr_ptr.p, sizeof(int) * (M->rows + 1), cudaMemcpyDeviceToHost,
+                             M->ctx->stream));
+    JFG_CUDA(cudaStreamSynchronize(M->ctx->stream));
+    for (int r = 0; r < M->rows; r++) len[r] = hp[r + 1] - hp[r];
+    return len;
+}
+
+void matrix_build_transfer_layout(Matrix* M, int kind, int S, int S2)
+{
+    if (M->st || M->csr_only || M->has32 || M->has16 || M->hash) return;   // precision copies follow the layout
+    build_point_layout(M, row_lengths(M), kind, S, S2);
 }
 
 // Builds CSR and SELL-32-sigma from merged, sorted, zero-free COO that is
@@ -466,7 +512,7 @@ static Matrix* build_from_sorted(Context* c, int rows, int cols, int64_t m, cons
         }
     }
     JFG_CUDA(cudaStreamSynchronize(s));
-    build_stencil(M, len);
+    build_point_layout(M, len, 0, 0, 0);
     return M;
 }
 
