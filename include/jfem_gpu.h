@@ -89,9 +89,13 @@ int jfg_spmv_lowp_dev(jfg_mat* m, int values, const float* d_x, float* d_y);
 /* The product layout the library picked for the matrix: *stencil = 1 when
  * the rows [lo, lo + regular_rows) use the values-only 9-point layout with
  * grid stride *stride (no column indices; the other_rows rows, with
- * other_nnz entries, keep a CSR copy), 0 for SELL-32 (then other_rows =
- * rows and other_nnz = nnz).  fp16_scale_inv: the factor of the FP16 copy's
- * row sums (0 before that copy exists).  Informational. */
+ * other_nnz entries, keep a CSR copy), 2 / 3 for the values-only layouts of
+ * a Q1 prolongation / restriction that a multigrid set-up gave the matrix
+ * (*stride: the stride of the grid of the rows), 0 for SELL-32 (then
+ * other_rows = rows and other_nnz = nnz).  fp16_scale_inv: the factor of the
+ * FP16 copy's row sums (0 before that copy exists).  Returns JFG_ERR_CUDA
+ * when a staged product of this matrix found its bulk copies incomplete
+ * after the bounded wait (the product's rows are then not written). */
 int jfg_matrix_layout(jfg_mat* m, int* stencil, int* stride, int* regular_rows, int* other_rows,
                       int64_t* other_nnz, double* fp16_scale_inv);
 /* Diagonal with duplicates summed.  Replaces Matrix.diag (Core/src/main/java/linalg/Matrix.java:157-175). */

@@ -272,12 +272,18 @@ int jfg_matrix_layout(jfg_mat* m, int* stencil, int* stride, int* regular_rows, 
 {
     if (!m) return JFG_ERR_BAD_ARG;
     const jfg::Matrix* M = m->m;
-    if (stencil) *stencil = M->st;
+    if (stencil) *stencil = M->st ? 1 + M->st_kind : 0;
     if (stride) *stride = M->st ? M->st_S : 0;
     if (regular_rows) *regular_rows = M->st ? M->st_hi - M->st_lo : 0;
     if (other_rows) *other_rows = M->st ? M->st_nirr : M->rows;
-    if (other_nnz) *other_nnz = M->st ? M->st_len - 9 * (int64_t)M->st_ld : M->nnz;
+    if (other_nnz) *other_nnz = M->st ? M->st_len - (int64_t)M->st_K * M->st_ld : M->nnz;
     if (fp16_scale_inv) *fp16_scale_inv = M->hash ? (double)M->hscale_inv : 0.0;
+    if (M->st) {
+        int e = 0;
+        if (cudaMemcpyAsync(&e, M->st_err.p, sizeof(int), cudaMemcpyDeviceToHost, M->ctx->stream) != cudaSuccess ||
+            cudaStreamSynchronize(M->ctx->stream) != cudaSuccess || e)
+            return JFG_ERR_CUDA;
+    }
     return JFG_OK;
 }
 

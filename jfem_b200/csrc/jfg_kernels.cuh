@@ -581,6 +581,226 @@ k_spmv_st(StArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi ep
 }
 
 // ---------------------------------------------------------------------------
+// staged point-layout SpMV (Matrix::st, all kinds): the value streams of a
+// tile of rows go to shared memory by bulk copies, the x gathers stay loads
+// ---------------------------------------------------------------------------
+struct PtArgs {
+    int S, S2, lo, nreg, ld, nirr, ntiles;
+    const int* irow;
+    const int* iptr;
+    const int* icol;
+    float vscale;          // FP16 values: factor of the row sums
+    int* err;              // set to 1 when a bulk copy does not complete
+};
+
+constexpr int kPtRows = 2 * kThreads;      // rows of one tile (two per thread)
+// stages of the value ring: 2-byte values three, FP32 / FP64 values two
+template <typename VT>
+__host__ __device__ constexpr int pt_stages() { return sizeof(VT) == 2 ? 3 : 2; }
+template <typename VT>
+constexpr int pt_smem(int K) { return pt_stages<VT>() * K * kPtRows * (int)sizeof(VT); }
+
+__device__ __forceinline__ uint32_t sh_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Bounded wait on an mbarrier phase (about half a second at most).
+__device__ __forceinline__ bool bulk_wait(uint32_t bar, uint32_t parity)
+{
+    for (int i = 0; i < (1 << 22); i++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (i > 16) __nanosleep(64);
+    }
+    return false;
+}
+__device__ __forceinline__ void bulk_arm(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// untiled bulk copy global -> shared (16-byte aligned addresses, size a multiple of 16)
+__device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(dst), "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// two consecutive values of one stream from shared memory
+__device__ __forceinline__ void sm_ld2(const double* p, double (&o)[2])
+{
+    const double2 v = *reinterpret_cast<const double2*>(p);
+    o[0] = v.x;
+    o[1] = v.y;
+}
+__device__ __forceinline__ void sm_ld2(const float* p, float (&o)[2])
+{
+    const float2 v = *reinterpret_cast<const float2*>(p);
+    o[0] = v.x;
+    o[1] = v.y;
+}
+template <typename H>
+__device__ __forceinline__ void sm_ld2(const H* p, float (&o)[2])
+{
+    o[0] = to_acc(p[0]);
+    o[1] = to_acc(p[1]);
+}
+
+// Staged point-layout SpMV.  A tile is kPtRows consecutive regular rows; its
+// K value streams (one per offset, kPtRows contiguous entries each) arrive in
+// shared memory by K bulk copies completing one mbarrier.  Thread 0 of a
+// persistent CTA issues the copies ST - 1 tiles ahead of the tile the CTA
+// sums, so the matrix stream is in flight without holding registers.  Each
+// thread sums two consecutive rows: the 9-point kind shares its three runs of
+// four x entries between the two rows, the transfer kinds gather per row.
+// Rows are summed in ascending column order from 0 with the same multiply-adds
+// as the SELL kernels (a stored zero adds exactly 0 for finite x): the result
+// equals theirs bit for bit.  The first CTAs of the grid take the irregular
+// rows from their CSR copy, one row per thread.  PF: the first tiles' copies
+// are issued before the wait for the preceding kernel (matrices that are not
+// written after set-up).  A tile whose copies do not complete within the
+// bounded wait sets *err; the CTA then waits (bounded) for the copies it has
+// issued and leaves.
+template <typename VT, typename XT, int NR, class Epi, class Fin, bool PF, int KIND>
+__global__ void __launch_bounds__(kThreads, sizeof(VT) == 8 ? 2 : kStCtasPerSm)
+k_spmv_pt(PtArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi epi, GridRed<NR, Fin> red,
+          const int* __restrict__ done)
+{
+    using AT = typename AccOf<VT>::T;
+    constexpr int K = KIND == 1 ? 4 : 9;
+    constexpr int ST = pt_stages<VT>();
+    constexpr int SE = K * kPtRows;                 // entries of one stage
+    extern __shared__ __align__(128) unsigned char pt_raw[];
+    VT* vs = reinterpret_cast<VT*>(pt_raw);
+    __shared__ __align__(8) uint64_t full[ST];
+    const int nb_irr = (m.nirr + kThreads - 1) / kThreads;
+    const bool regular = (int)blockIdx.x >= nb_irr;
+    const int G = (int)gridDim.x - nb_irr;
+    const int b = (int)blockIdx.x - nb_irr;
+    const int cnt = regular && b < m.ntiles ? (m.ntiles - 1 - b) / G + 1 : 0;
+    int issued = 0;                                 // tiles whose copies thread 0 has issued
+    auto issue = [&](int j) {
+        constexpr int E = 16 / (int)sizeof(VT);     // copy sizes: multiples of 16 bytes (within ld)
+        const int i0 = (b + j * G) * kPtRows;
+        const int rows = min(kPtRows, m.nreg - i0);
+        const uint32_t bytes = (uint32_t)((rows + E - 1) / E * E * (int)sizeof(VT));
+        const int s = j % ST;
+        const uint32_t bar = sh_addr(&full[s]);
+        bulk_arm(bar, (uint32_t)K * bytes);
+#pragma unroll
+        for (int k = 0; k < K; k++)
+            bulk_copy(sh_addr(vs + s * SE + k * kPtRows), val + (int64_t)k * m.ld + i0, bytes, bar);
+    };
+    if (cnt > 0) {
+        if (threadIdx.x == 0) {
+            for (int s = 0; s < ST; s++)
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sh_addr(&full[s])) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            if (PF)
+                for (; issued < min(ST, cnt); issued++) issue(issued);
+        }
+        __syncthreads();
+    }
+    pdl_wait();
+    if (done && *done) {
+        if (threadIdx.x == 0)
+            for (int j = 0; j < issued; j++) bulk_wait(sh_addr(&full[j]), 0);
+        return;
+    }
+    if (cnt > 0 && threadIdx.x == 0)
+        for (; issued < min(ST, cnt); issued++) issue(issued);
+    double acc[NR > 0 ? NR : 1];
+#pragma unroll
+    for (int q = 0; q < (NR > 0 ? NR : 1); q++) acc[q] = 0;
+    if (regular) {
+        const int l = 2 * (int)threadIdx.x;
+        for (int j = 0; j < cnt; j++) {
+            const int s = j % ST;
+            const bool ok = bulk_wait(sh_addr(&full[s]), (uint32_t)((j / ST) & 1));
+            // one vote: every thread leaves together, and every thread is past tile j - 1
+            if (!__syncthreads_and(ok)) {
+                if (threadIdx.x == 0) {
+                    atomicOr(m.err, 1);
+                    for (int q = j; q < issued; q++) bulk_wait(sh_addr(&full[q % ST]), (uint32_t)((q / ST) & 1));
+                }
+                return;
+            }
+            // tile j - 1 + ST into the stage tile j - 1 has left
+            if (threadIdx.x == 0 && j >= 1 && issued < cnt) {
+                issue(issued);
+                issued++;
+            }
+            const int i = (b + j * G) * kPtRows + l;
+            if (i >= m.nreg) continue;
+            const VT* vt = vs + s * SE + l;
+            AT v[K][2];
+#pragma unroll
+            for (int k = 0; k < K; k++) sm_ld2(vt + k * kPtRows, v[k]);
+            const bool two = i + 1 < m.nreg;
+            const int r0 = m.lo + i;
+            if constexpr (KIND == 0) {
+                AT xs[3][4];
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+                    const XT* xp = x + (r0 + (a - 1) * m.S - 1);
+#pragma unroll
+                    for (int e = 0; e < 3; e++) xs[a][e] = (AT)__ldg(xp + e);
+                    xs[a][3] = two ? (AT)__ldg(xp + 3) : (AT)0;
+                }
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    if (q == 1 && !two) break;
+                    AT sum = 0;
+#pragma unroll
+                    for (int k = 0; k < 9; k++) sum += v[k][q] * xs[k / 3][q + k % 3];
+                    if constexpr (std::is_same<VT, __half>::value) sum *= m.vscale;
+                    epi(r0 + q, sum, acc);
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    if (q == 1 && !two) break;
+                    const int r = r0 + q;
+                    const int g = r / m.S, h = r - g * m.S;
+                    AT sum = 0;
+                    if constexpr (KIND == 1) {
+                        const XT* xp = x + ((g >> 1) * m.S2 + (h >> 1));
+                        sum += v[0][q] * (AT)__ldg(xp);
+                        sum += v[1][q] * (AT)__ldg(xp + 1);
+                        sum += v[2][q] * (AT)__ldg(xp + m.S2);
+                        sum += v[3][q] * (AT)__ldg(xp + m.S2 + 1);
+                    } else {
+                        const XT* xp = x + (2 * g * m.S2 + 2 * h);
+#pragma unroll
+                        for (int k = 0; k < 9; k++) sum += v[k][q] * (AT)__ldg(xp + ((k / 3 - 1) * m.S2 + (k % 3 - 1)));
+                    }
+                    if constexpr (std::is_same<VT, __half>::value) sum *= m.vscale;
+                    epi(r, sum, acc);
+                }
+            }
+        }
+    } else {
+        const int g = (int)blockIdx.x * kThreads + (int)threadIdx.x;
+        if (g < m.nirr) {
+            const int r = m.irow[g];
+            const VT* iv = val + (int64_t)K * m.ld;
+            AT sum = 0;
+            for (int k = m.iptr[g]; k < m.iptr[g + 1]; k++) sum += to_acc(iv[k]) * (AT)__ldg(x + m.icol[k]);
+            if constexpr (std::is_same<VT, __half>::value) sum *= m.vscale;
+            epi(r, sum, acc);
+        }
+    }
+    pdl_launch_dependents();
+    if constexpr (NR > 0) red.reduce(acc);
+}
+
+// ---------------------------------------------------------------------------
 // grid-stride vector kernels: f(i, acc) per index, optional reduction
 // ---------------------------------------------------------------------------
 template <int NR, class F, class Fin>

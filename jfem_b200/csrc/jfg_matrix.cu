@@ -282,6 +282,14 @@ bool stencil_enabled()
     return !(e && e[0] == '0');
 }
 
+// JFEM_ST_STAGED=0 gives the 9-point layouts built afterwards the register
+// kernel k_spmv_st instead of the staged k_spmv_pt (read at each build)
+static bool st_staged_enabled()
+{
+    const char* e = getenv("JFEM_ST_STAGED");
+    return !(e && e[0] == '0');
+}
+
 // Point layout of M (see Matrix::st) for the rows whose entries fit it:
 // kind 0 detects the 9-point stencil's stride S off a few middle rows
 // (largest column offset - 1); kinds 1 and 2 (grid transfers) take S and S2
@@ -347,6 +355,9 @@ static void build_point_layout(Matrix* M, const std::vector<int>& len, int kind,
     const int64_t irr_nnz = iptr.back();
     const int ld = (nreg + 7) / 8 * 8;
     M->st_kind = kind;
+    M->st_staged = st_staged_enabled() ? 1 : 0;
+    M->st_err.alloc(1);
+    JFG_CUDA(cudaMemsetAsync(M->st_err.p, 0, sizeof(int), s));
     M->st_K = K;
     M->st_S = S;
     M->st_S2 = S2;

@@ -449,6 +449,14 @@ void MGImpl<T>::init(Context* ctx, int levels, Matrix* const* As, Matrix* const*
             JFG_CHECK(P[l]->rows == As[l + 1]->rows && P[l]->cols == As[l]->rows, JFG_ERR_BAD_ARG,
                       "prolongation shape does not match the level sizes");
             R[l] = matrix_transpose(P[l]);
+            // Q1 grids whose level matrices carry the 9-point layout with
+            // strides S (coarse) and 2 S - 1 (fine): values-only transfers
+            const Matrix* Ac = As[l];
+            const Matrix* Af = As[l + 1];
+            if (Ac->st && Af->st && Ac->st_kind == 0 && Af->st_kind == 0 && Af->st_S == 2 * Ac->st_S - 1) {
+                matrix_build_transfer_layout(P[l], 1, Af->st_S, Ac->st_S);
+                matrix_build_transfer_layout(R[l], 2, Ac->st_S, Af->st_S);
+            }
         }
         if (std::is_same<T, float>::value) {
             vbf16 = vfmt == 1 ? 1 : 0;

@@ -144,6 +144,42 @@ template <typename VT>
 constexpr int pipe_chunk() { return sizeof(VT) <= 2 ? 8 : 4; }
 constexpr int kPipeStages = 2;
 
+// The staged point-layout SpMV (k_spmv_pt) of a matrix with Matrix::st: a
+// persistent grid of as many regular CTAs as stay resident beside the CTAs of
+// the irregular rows (FP64 values: 2 CTAs per SM, others 4).
+template <typename VT, typename XT, int NR, class Epi, class Fin, bool PF, int KIND>
+void launch_pt_kind(cudaStream_t st, const Matrix* M, const VT* val, const XT* x, Epi epi, GridRed<NR, Fin> red,
+                    const int* done)
+{
+    const int nreg = M->st_hi - M->st_lo;
+    const int ntiles = (nreg + kPtRows - 1) / kPtRows;
+    const int cps = sizeof(VT) == 8 ? 2 : kStCtasPerSm;
+    const int nbr = std::max(1, std::min(ntiles, sm_count() * cps - M->st_nb_irr));
+    const int smem = pt_smem<VT>(KIND == 1 ? 4 : 9);
+    auto kern = k_spmv_pt<VT, XT, NR, Epi, Fin, PF, KIND>;
+    if (smem > 48 * 1024) {
+        static const bool set = [&] {
+            JFG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            return true;
+        }();
+        (void)set;
+    }
+    PtArgs a{M->st_S, M->st_S2, M->st_lo, nreg, M->st_ld, M->st_nirr, ntiles, M->st_irow.p, M->st_iptr.p,
+             M->st_icol.p, std::is_same<VT, __half>::value ? M->hscale_inv : 1.0f, M->st_err.p};
+    launch_ex(kern, dim3(nbr + M->st_nb_irr), dim3(kThreads), (size_t)smem, st, a, val, x, epi, red, done);
+}
+
+template <typename VT, typename XT, int NR, class Epi, class Fin, bool PF>
+void launch_pt(cudaStream_t st, const Matrix* M, const VT* val, const XT* x, Epi epi, GridRed<NR, Fin> red,
+               const int* done)
+{
+    switch (M->st_kind) {
+    case 1: launch_pt_kind<VT, XT, NR, Epi, Fin, PF, 1>(st, M, val, x, epi, red, done); break;
+    case 2: launch_pt_kind<VT, XT, NR, Epi, Fin, PF, 2>(st, M, val, x, epi, red, done); break;
+    default: launch_pt_kind<VT, XT, NR, Epi, Fin, PF, 0>(st, M, val, x, epi, red, done); break;
+    }
+}
+
 // PF: prefetch the matrix before the PDL wait (see k_spmv); only for
 // matrices that are not written after set-up.
 template <typename VT, typename XT, int NR, class Epi, class Fin = NoFin, bool PF = false>
@@ -152,7 +188,11 @@ void spmv_launch(cudaStream_t st, const Matrix* M, const VT* val, const XT* x, E
 {
     if (M->rows == 0) return;
     GridRed<NR, Fin> red{sc.partials, sc.counter, fin};
-    // the values-only stencil layout, when the matrix has one in this value type
+    // the values-only point layouts, when the matrix has one in this value type
+    if (M->st && val == LayoutVals<VT>::sell(M) && LayoutVals<VT>::st(M) && (M->st_staged || M->st_kind != 0)) {
+        launch_pt<VT, XT, NR, Epi, Fin, PF>(st, M, LayoutVals<VT>::st(M), x, epi, red, done);
+        return;
+    }
     if (M->st && val == LayoutVals<VT>::sell(M) && LayoutVals<VT>::st(M)) {
         // persistent: as many regular CTAs as stay resident next to the irregular ones
         // (FP64 values: up to 128 registers, 2 CTAs per SM)

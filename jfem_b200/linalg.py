@@ -319,14 +319,16 @@ class DeviceMatrix:
         return y
 
     def layout(self) -> dict:
-        """The product layout: {'stencil': bool, 'stride', 'regular_rows',
-        'other_rows', 'other_nnz', 'fp16_scale_inv'}."""
+        """The product layout: {'stencil': bool (the 9-point layout), 'kind'
+        ('sell', 'stencil', 'prolongation' or 'restriction'), 'stride',
+        'regular_rows', 'other_rows', 'other_nnz', 'fp16_scale_inv'}."""
         st, S, nreg, noth = C.c_int(), C.c_int(), C.c_int(), C.c_int()
         onnz = C.c_int64()
         hs = C.c_double()
         self.ctx.check(N.load().jfg_matrix_layout(self._h, C.byref(st), C.byref(S), C.byref(nreg), C.byref(noth),
                                                   C.byref(onnz), C.byref(hs)))
-        return {"stencil": bool(st.value), "stride": S.value, "regular_rows": nreg.value, "other_rows": noth.value,
+        return {"stencil": st.value == 1, "kind": ("sell", "stencil", "prolongation", "restriction")[st.value],
+                "stride": S.value, "regular_rows": nreg.value, "other_rows": noth.value,
                 "other_nnz": int(onnz.value), "fp16_scale_inv": hs.value}
 
     def time_spmv(self, precision=0, iters=50):

@@ -1,0 +1,92 @@
+"""The values-only point layouts and the staged product kernel.
+
+* 9-point layout of Q1 level matrices: the staged kernel (k_spmv_pt: value
+  streams by bulk copies into shared memory) and the register kernel
+  (k_spmv_st, JFEM_ST_STAGED=0) give the SELL kernels' bits (products in
+  FP64, FP32, BF16 and scaled FP16);
+* transfer layouts of Q1 prolongations (4 values per fine row) and
+  restrictions (9 values per coarse row), built by the multigrid set-up when
+  the level matrices carry the 9-point layout with strides S and 2 S - 1: the
+  V-cycle in every hierarchy precision equals the SELL-only V-cycle
+  (JFEM_STENCIL=0) bit for bit, and the prolongation's products equal the
+  oracle's COO scatter (SparseMatrix.mvMul / tvMul,
+  linalg/SparseMatrix.java:480-501) to 1e-12.
+"""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from jfem_b200 import JacobiSmoother, MGPreconditioner, problems
+from jfem_b200.linalg import DeviceMatrix
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def q1_512():
+    h, _ = problems.kappa_hierarchy(1, 4, 8, 0.05, 1.0, kseed=3)          # Q1 512^2, kappa-GRF
+    return h
+
+
+def _mg(h, ctx, precision):
+    L = len(h.systems)
+    mats = [DeviceMatrix(s.n, s.n, s.rows, s.cols, s.vals, ctx) for s in h.systems]
+    prol = [DeviceMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l], ctx) for l in range(L - 1)]
+    mg = MGPreconditioner(mats, prol, h.boundary, [None] + [JacobiSmoother(2, 2 / 3)] * (L - 1), cycles=1,
+                          use_fmg=False, precision=precision, ctx=ctx)
+    return mats, prol, mg
+
+
+@pytest.mark.parametrize("values", ["fp64", "fp32", "bf16", "fp16"])
+def test_staged_equals_register_stencil_kernel(ctx, q1_512, monkeypatch, values):
+    sy = q1_512.finest
+    A_pt = DeviceMatrix(sy.n, sy.n, sy.rows, sy.cols, sy.vals, ctx)
+    monkeypatch.setenv("JFEM_ST_STAGED", "0")
+    A_reg = DeviceMatrix(sy.n, sy.n, sy.rows, sy.cols, sy.vals, ctx)
+    monkeypatch.setenv("JFEM_STENCIL", "0")
+    A_sell = DeviceMatrix(sy.n, sy.n, sy.rows, sy.cols, sy.vals, ctx)
+    assert A_pt.layout()["kind"] == "stencil" and A_sell.layout()["kind"] == "sell"
+    x = np.random.default_rng(21).standard_normal(sy.n)
+    if values == "fp64":
+        ys = [A.spmv(x) for A in (A_pt, A_reg, A_sell)]
+        zs = [A.spmv_t(x) for A in (A_pt, A_reg, A_sell)]
+        assert np.array_equal(ys[0], ys[2]) and np.array_equal(ys[1], ys[2])
+        assert np.array_equal(zs[0], zs[2]) and np.array_equal(zs[1], zs[2])
+    else:
+        xd = torch.from_numpy(x.astype(np.float32)).cuda()
+        ys = [A.spmv_lowp_dev(xd, values).cpu().numpy() for A in (A_pt, A_reg, A_sell)]
+        assert np.array_equal(ys[0], ys[2]) and np.array_equal(ys[1], ys[2])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "mixed-bf16", "mixed-fp16"])
+def test_transfer_layouts_vcycle_bitwise(ctx, q1_512, monkeypatch, precision):
+    h = q1_512
+    b = h.finest.rhs
+    _, prol, mg = _mg(h, ctx, precision)
+    lay = prol[-1].layout()
+    assert lay["kind"] == "prolongation" and lay["stride"] == 513
+    assert lay["regular_rows"] > 0.99 * h.finest.n
+    v_pt = mg.vCycle(np.zeros(b.size), b)
+    monkeypatch.setenv("JFEM_STENCIL", "0")
+    _, prol0, mg0 = _mg(h, ctx, precision)
+    assert prol0[-1].layout()["kind"] == "sell"
+    v_sell = mg0.vCycle(np.zeros(b.size), b)
+    assert np.array_equal(v_pt, v_sell)
+
+
+def test_prolongation_layout_vs_oracle(ctx, q1_512):
+    h = q1_512
+    _, prol, _ = _mg(h, ctx, "fp64")
+    rng = np.random.default_rng(22)
+    for l in (len(prol) - 1, len(prol) - 3):
+        P = prol[l]
+        nf, nc = h.systems[l + 1].n, h.systems[l].n
+        assert P.layout()["kind"] == "prolongation"
+        ref = O.CooMatrix(nf, nc, *h.prolong[l])
+        x = rng.standard_normal(nc)
+        yr = ref.mvmul(x)
+        np.testing.assert_allclose(P.spmv(x), yr, rtol=1e-12, atol=1e-12 * np.abs(yr).max())
+        z = rng.standard_normal(nf)
+        zr = ref.tvmul(z)
+        np.testing.assert_allclose(P.spmv_t(z), zr, rtol=1e-12, atol=1e-12 * np.abs(zr).max())
