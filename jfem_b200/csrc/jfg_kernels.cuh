@@ -651,6 +651,50 @@ __device__ __forceinline__ void sm_ld2(const H* p, float (&o)[2])
     o[1] = to_acc(p[1]);
 }
 
+// The x entries that regular rows i and i + 1 of a point layout read (i
+// even; row i + 1 only when it is regular), in slot order: the 9-point kind
+// as three runs of four entries (grid lines below, at and above the rows,
+// shared by the two rows), the transfer kinds K entries per row.
+template <int KIND, typename AT, typename XT, int KX>
+__device__ __forceinline__ void pt_gather(const PtArgs& m, const XT* __restrict__ x, int i, AT (&xv)[KX])
+{
+    if (i >= m.nreg) return;
+    const bool two = i + 1 < m.nreg;
+    const int r0 = m.lo + i;
+    if constexpr (KIND == 0) {
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const XT* xp = x + (r0 + (a - 1) * m.S - 1);
+#pragma unroll
+            for (int e = 0; e < 3; e++) xv[4 * a + e] = (AT)__ldg(xp + e);
+            xv[4 * a + 3] = two ? (AT)__ldg(xp + 3) : (AT)0;
+        }
+    } else {
+        constexpr int K = KX / 2;
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+            if (q == 1 && !two) {
+#pragma unroll
+                for (int k = 0; k < K; k++) xv[K + k] = (AT)0;
+                break;
+            }
+            const int r = r0 + q;
+            const int g = r / m.S, h = r - g * m.S;
+            if constexpr (KIND == 1) {
+                const XT* xp = x + ((g >> 1) * m.S2 + (h >> 1));
+                xv[q * K + 0] = (AT)__ldg(xp);
+                xv[q * K + 1] = (AT)__ldg(xp + 1);
+                xv[q * K + 2] = (AT)__ldg(xp + m.S2);
+                xv[q * K + 3] = (AT)__ldg(xp + m.S2 + 1);
+            } else {
+                const XT* xp = x + (2 * g * m.S2 + 2 * h);
+#pragma unroll
+                for (int k = 0; k < 9; k++) xv[q * K + k] = (AT)__ldg(xp + ((k / 3 - 1) * m.S2 + (k % 3 - 1)));
+            }
+        }
+    }
+}
+
 // Staged point-layout SpMV.  A tile is kPtRows consecutive regular rows; its
 // K value streams (one per offset, kPtRows contiguous entries each) arrive in
 // shared memory by K bulk copies completing one mbarrier.  Thread 0 of a
@@ -720,6 +764,11 @@ k_spmv_pt(PtArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi ep
     for (int q = 0; q < (NR > 0 ? NR : 1); q++) acc[q] = 0;
     if (regular) {
         const int l = 2 * (int)threadIdx.x;
+        constexpr int KX = KIND == 0 ? 12 : 2 * K;
+        AT xv[KX];
+        // the x entries of a tile are gathered one tile ahead (their latency
+        // overlaps the sums of the tile before)
+        if (cnt > 0) pt_gather<KIND>(m, x, b * kPtRows + l, xv);
         for (int j = 0; j < cnt; j++) {
             const int s = j % ST;
             const bool ok = bulk_wait(sh_addr(&full[s]), (uint32_t)((j / ST) & 1));
@@ -737,52 +786,34 @@ k_spmv_pt(PtArgs m, const VT* __restrict__ val, const XT* __restrict__ x, Epi ep
                 issued++;
             }
             const int i = (b + j * G) * kPtRows + l;
-            if (i >= m.nreg) continue;
-            const VT* vt = vs + s * SE + l;
-            AT v[K][2];
+            AT xn[KX];
+            const bool more = j + 1 < cnt;
+            if (more) pt_gather<KIND>(m, x, i + G * kPtRows, xn);
+            if (i < m.nreg) {
+                const VT* vt = vs + s * SE + l;
+                AT v[K][2];
 #pragma unroll
-            for (int k = 0; k < K; k++) sm_ld2(vt + k * kPtRows, v[k]);
-            const bool two = i + 1 < m.nreg;
-            const int r0 = m.lo + i;
-            if constexpr (KIND == 0) {
-                AT xs[3][4];
-#pragma unroll
-                for (int a = 0; a < 3; a++) {
-                    const XT* xp = x + (r0 + (a - 1) * m.S - 1);
-#pragma unroll
-                    for (int e = 0; e < 3; e++) xs[a][e] = (AT)__ldg(xp + e);
-                    xs[a][3] = two ? (AT)__ldg(xp + 3) : (AT)0;
-                }
+                for (int k = 0; k < K; k++) sm_ld2(vt + k * kPtRows, v[k]);
+                const bool two = i + 1 < m.nreg;
+                const int r0 = m.lo + i;
 #pragma unroll
                 for (int q = 0; q < 2; q++) {
                     if (q == 1 && !two) break;
                     AT sum = 0;
+                    if constexpr (KIND == 0) {
 #pragma unroll
-                    for (int k = 0; k < 9; k++) sum += v[k][q] * xs[k / 3][q + k % 3];
+                        for (int k = 0; k < 9; k++) sum += v[k][q] * xv[(k / 3) * 4 + q + k % 3];
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < K; k++) sum += v[k][q] * xv[q * K + k];
+                    }
                     if constexpr (std::is_same<VT, __half>::value) sum *= m.vscale;
                     epi(r0 + q, sum, acc);
                 }
-            } else {
+            }
+            if (more) {
 #pragma unroll
-                for (int q = 0; q < 2; q++) {
-                    if (q == 1 && !two) break;
-                    const int r = r0 + q;
-                    const int g = r / m.S, h = r - g * m.S;
-                    AT sum = 0;
-                    if constexpr (KIND == 1) {
-                        const XT* xp = x + ((g >> 1) * m.S2 + (h >> 1));
-                        sum += v[0][q] * (AT)__ldg(xp);
-                        sum += v[1][q] * (AT)__ldg(xp + 1);
-                        sum += v[2][q] * (AT)__ldg(xp + m.S2);
-                        sum += v[3][q] * (AT)__ldg(xp + m.S2 + 1);
-                    } else {
-                        const XT* xp = x + (2 * g * m.S2 + 2 * h);
-#pragma unroll
-                        for (int k = 0; k < 9; k++) sum += v[k][q] * (AT)__ldg(xp + ((k / 3 - 1) * m.S2 + (k % 3 - 1)));
-                    }
-                    if constexpr (std::is_same<VT, __half>::value) sum *= m.vscale;
-                    epi(r, sum, acc);
-                }
+                for (int e = 0; e < KX; e++) xv[e] = xn[e];
             }
         }
     } else {

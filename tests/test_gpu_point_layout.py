@@ -66,7 +66,7 @@ def test_transfer_layouts_vcycle_bitwise(ctx, q1_512, monkeypatch, precision):
     _, prol, mg = _mg(h, ctx, precision)
     lay = prol[-1].layout()
     assert lay["kind"] == "prolongation" and lay["stride"] == 513
-    assert lay["regular_rows"] > 0.99 * h.finest.n
+    assert lay["regular_rows"] > 0.98 * h.finest.n
     v_pt = mg.vCycle(np.zeros(b.size), b)
     monkeypatch.setenv("JFEM_STENCIL", "0")
     _, prol0, mg0 = _mg(h, ctx, precision)
