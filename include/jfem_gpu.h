@@ -124,6 +124,13 @@ int jfg_matrix_galerkin(jfg_mat* r, jfg_mat* a, jfg_mat* p, jfg_mat** out);
  * the mean milliseconds per product.  x and y are library-owned device
  * vectors (x = 1).  Measurement helper, not part of the reference surface. */
 int jfg_spmv_time(jfg_mat* m, int precision, int iters, double* ms_per_spmv);
+/* Times products over `count` matrices of one context taken in turn, back to
+ * back on the context stream (rounds of count products, one event pair
+ * around all `iters` rounds after one untimed round); returns the mean
+ * milliseconds per product.  With matrices whose bytes together exceed the
+ * L2, every product reads its matrix from HBM with no flush between
+ * launches.  Measurement helper, not part of the reference surface. */
+int jfg_spmv_time_rotating(jfg_mat* const* ms, int count, int precision, int iters, double* ms_per_spmv);
 
 /* ---- smoothers ------------------------------------------------------- */
 typedef struct jfg_schwarz jfg_schwarz;

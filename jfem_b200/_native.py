@@ -32,7 +32,7 @@ EXPORTED = [
     "jfg_version",
     "jfg_kernel_launches",
     "jfg_matrix_from_coo", "jfg_matrix_free", "jfg_matrix_info", "jfg_spmv", "jfg_spmv_t", "jfg_spmv_dev",
-    "jfg_spmv_t_dev", "jfg_spmv_f32_dev", "jfg_spmv_lowp_dev", "jfg_matrix_layout", "jfg_matrix_diag", "jfg_spmv_time", "jfg_smooth",
+    "jfg_spmv_t_dev", "jfg_spmv_f32_dev", "jfg_spmv_lowp_dev", "jfg_matrix_layout", "jfg_matrix_diag", "jfg_spmv_time", "jfg_spmv_time_rotating", "jfg_smooth",
     "jfg_matrix_csr", "jfg_matrix_mmmul", "jfg_matrix_tmmul", "jfg_matrix_galerkin",
     "jfg_gs_create", "jfg_gs_free", "jfg_gs_info", "jfg_gs_ranks", "jfg_assemble_tp",
     "jfg_assemble_taylor_hood",
@@ -131,6 +131,7 @@ def load():
     L.jfg_matrix_layout.argtypes = [_P, _I, _I, _I, _I, C.POINTER(C.c_int64), _D]
     L.jfg_matrix_diag.argtypes = [_P, _D]
     L.jfg_spmv_time.argtypes = [_P, C.c_int, C.c_int, _D]
+    L.jfg_spmv_time_rotating.argtypes = [C.POINTER(_P), C.c_int, C.c_int, C.c_int, _D]
     L.jfg_matrix_csr.argtypes = [_P, _I, _I, _D]
     for f in ("jfg_matrix_mmmul", "jfg_matrix_tmmul"):
         getattr(L, f).argtypes = [_P, _P, C.POINTER(_P)]

@@ -465,6 +465,62 @@ int jfg_spmv_time(jfg_mat* m, int precision, int iters, double* ms)
     });
 }
 
+int jfg_spmv_time_rotating(jfg_mat* const* ms, int count, int precision, int iters, double* ms_per)
+{
+    if (!ms || count <= 0 || !ms[0] || !ms_per || iters <= 0) return JFG_ERR_BAD_ARG;
+    jfg_ctx* ctx = ms[0]->ctx;
+    for (int k = 0; k < count; k++)
+        if (!ms[k] || ms[k]->ctx != ctx) return JFG_ERR_BAD_ARG;
+    return guard(ctx, [&]() -> int {
+        cudaStream_t st = ctx->c.stream;
+        int nb = 0, rows = 0, cols = 0;
+        for (int k = 0; k < count; k++) {
+            nb = std::max(nb, ms[k]->m->nblocks);
+            rows = std::max(rows, ms[k]->m->rows);
+            cols = std::max(cols, ms[k]->m->cols);
+            if (precision) jfg::matrix_ensure_fp32(ms[k]->m);
+        }
+        jfg::Scratch sc = ctx_scratch(ctx, nb);
+        DevBuf<double> x64, y64;
+        DevBuf<float> x32, y32;
+        if (precision == 0) {
+            x64.alloc(cols);
+            y64.alloc(rows);
+            std::vector<double> ones(cols, 1.0);
+            JFG_CUDA(cudaMemcpyAsync(x64.p, ones.data(), sizeof(double) * cols, cudaMemcpyHostToDevice, st));
+        } else {
+            x32.alloc(cols);
+            y32.alloc(rows);
+            std::vector<float> ones(cols, 1.0f);
+            JFG_CUDA(cudaMemcpyAsync(x32.p, ones.data(), sizeof(float) * cols, cudaMemcpyHostToDevice, st));
+        }
+        auto round = [&]() {
+            for (int k = 0; k < count; k++) {
+                jfg::Matrix* M = ms[k]->m;
+                if (precision == 0)
+                    SpmvStore64::run(st, M, x64.p, y64.p, sc);
+                else
+                    jfg::spmv_launch<float, float, 0>(st, M, M->val32.p, x32.p, jfg::EpiStore<float>{y32.p}, sc,
+                                                      nullptr);
+            }
+        };
+        round();
+        cudaEvent_t e0, e1;
+        JFG_CUDA(cudaEventCreate(&e0));
+        JFG_CUDA(cudaEventCreate(&e1));
+        JFG_CUDA(cudaEventRecord(e0, st));
+        for (int i = 0; i < iters; i++) round();
+        JFG_CUDA(cudaEventRecord(e1, st));
+        JFG_CUDA(cudaEventSynchronize(e1));
+        float t = 0;
+        JFG_CUDA(cudaEventElapsedTime(&t, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *ms_per = (double)t / ((double)iters * count);
+        return JFG_OK;
+    });
+}
+
 // ---------------------------------------------------------------------------
 int jfg_smooth(jfg_mat* A, const jfg_smoother_desc* sm, const double* rhs, double* x)
 {

@@ -451,9 +451,12 @@ void MGImpl<T>::init(Context* ctx, int levels, Matrix* const* As, Matrix* const*
             R[l] = matrix_transpose(P[l]);
             // Q1 grids whose level matrices carry the 9-point layout with
             // strides S (coarse) and 2 S - 1 (fine): values-only transfers
+            // (JFEM_MG_TRANSFER=0 keeps them in SELL-32)
             const Matrix* Ac = As[l];
             const Matrix* Af = As[l + 1];
-            if (Ac->st && Af->st && Ac->st_kind == 0 && Af->st_kind == 0 && Af->st_S == 2 * Ac->st_S - 1) {
+            const char* et = getenv("JFEM_MG_TRANSFER");
+            if (!(et && et[0] == '0') && Ac->st && Af->st && Ac->st_kind == 0 && Af->st_kind == 0 &&
+                Af->st_S == 2 * Ac->st_S - 1) {
                 matrix_build_transfer_layout(P[l], 1, Af->st_S, Ac->st_S);
                 matrix_build_transfer_layout(R[l], 2, Ac->st_S, Af->st_S);
             }

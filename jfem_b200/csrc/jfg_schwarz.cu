@@ -328,95 +328,6 @@ __global__ void __launch_bounds__(kSchThreads, 5)
                          sr);
 }
 
-// A batch of up to kBatch patches of one colour that share one inverse (the
-// interior patches of a structured grid) in one CTA: the patch rows of b - A x
-// of every patch of the batch are gathered first (as patch_correct does),
-// then thread i walks row i of the shared inverse once and applies each
-// entry to every patch of the batch, so the inverse is streamed once per
-// batch instead of once per patch.  Each patch's sums run in patch_correct's
-// order with the same operations: the results equal the per-patch kernel's
-// bit for bit.  Patches of at most kBatchM DOFs (one row per thread).
-constexpr int kBatch = 8;
-constexpr int kBatchM = kSchThreads;
-
-template <typename T, typename IT>
-__global__ void __launch_bounds__(kSchThreads)
-    k_schwarz_batch(CsrView A, const int* __restrict__ bpat, const int* __restrict__ bptr,
-                    const int64_t* __restrict__ pptr, const int* __restrict__ dofs,
-                    const int64_t* __restrict__ inv_off, const IT* __restrict__ inv, const T* b, T* x, double om,
-                    double* lsol, int direct, const int* done)
-{
-    if (done && *done) return;
-    extern __shared__ __align__(16) unsigned char bsm[];
-    const int q0 = bptr[blockIdx.x];
-    const int cnt = bptr[blockIdx.x + 1] - q0;
-    const int p0 = bpat[q0];
-    const int m = (int)(pptr[p0 + 1] - pptr[p0]);
-    double* sr = reinterpret_cast<double*>(bsm);                    // cnt * m residual entries
-    int* sdof = reinterpret_cast<int*>(sr + kBatch * m);
-    int* srs = sdof + kBatch * m;
-    int* sre = srs + kBatch * m;
-    const int tid = threadIdx.x;
-    const int tot = cnt * m;
-    for (int t = tid; t < tot; t += blockDim.x) {
-        const int q = t / m, i = t - q * m;
-        const int g = dofs[pptr[bpat[q0 + q]] + i];
-        sdof[t] = g;
-        srs[t] = A.rp[g];
-        sre[t] = A.rp[g + 1];
-    }
-    __syncthreads();
-    const int sub = tid & (kRowLanes - 1);
-    const int per_pass = blockDim.x / kRowLanes;
-    for (int t0 = 0; t0 < tot; t0 += per_pass) {        // uniform trip count: the shuffles see full warps
-        const int t = t0 + tid / kRowLanes;
-        double acc = 0.0;
-        if (t < tot) {
-            const int k0 = srs[t] + sub, k1 = sre[t];
-            int c[kRowUnroll];
-            double v[kRowUnroll];
-#pragma unroll
-            for (int u = 0; u < kRowUnroll; u++) {
-                const int k = k0 + u * kRowLanes;
-                c[u] = k < k1 ? __ldg(A.col + k) : -1;
-                v[u] = k < k1 ? __ldg(A.val + k) : 0.0;
-            }
-#pragma unroll
-            for (int u = 0; u < kRowUnroll; u++)
-                if (c[u] >= 0) acc += v[u] * (double)x[c[u]];
-            for (int k = k0 + kRowUnroll * kRowLanes; k < k1; k += kRowLanes) acc += A.val[k] * (double)x[A.col[k]];
-        }
-#pragma unroll
-        for (int o = 1; o < kRowLanes; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (t < tot && sub == 0) sr[t] = (double)b[sdof[t]] - acc;
-    }
-    __syncthreads();
-    const IT* At = inv + inv_off[p0];                   // transposed: At[j * m + i] = inverse(i, j)
-    if (tid < m) {
-        const int i = tid;
-        double acc[kBatch];
-#pragma unroll
-        for (int q = 0; q < kBatch; q++) acc[q] = 0.0;
-#pragma unroll 4
-        for (int j = 0; j < m; j++) {
-            const double a = (double)__ldg(At + (size_t)j * m + i);
-#pragma unroll
-            for (int q = 0; q < kBatch; q++)
-                if (q < cnt) acc[q] += a * sr[q * m + j];
-        }
-#pragma unroll
-        for (int q = 0; q < kBatch; q++) {
-            if (q >= cnt) break;
-            if (direct) {
-                const int g = sdof[q * m + i];
-                x[g] = (T)((double)x[g] + acc[q] * om);
-            } else {
-                lsol[pptr[bpat[q0 + q]] + i] = acc[q];
-            }
-        }
-    }
-}
-
 // MultiplicativeSubspaceCorrection: the patches of plist one after another
 // in a single CTA (each step sees the previous steps' updates).
 template <typename T, typename IT>
@@ -494,45 +405,6 @@ __global__ void k_to_f32(int64_t n, const double* __restrict__ a, float* __restr
 CsrView csr_of(Matrix* A) { return CsrView{A->csr_ptr.p, A->csr_col.p, A->csr_val.p}; }
 
 }  // namespace
-
-// Groups each colour's patches (hc[start, start + count), ascending) by
-// shared inverse, first occurrence first and ascending within a group, and
-// cuts the groups into batches of at most kBatch patches.
-void SchwarzImpl::build_batches(std::vector<Colour*>& cols, const std::vector<int>& hc,
-                                const std::vector<int64_t>& hoff)
-{
-    std::vector<int> hb, hbp{0};
-    for (Colour* col : cols) {
-        col->b_start = (int)hbp.size() - 1;
-        std::vector<int64_t> keys;
-        std::map<int64_t, std::vector<int>> groups;
-        for (int q = 0; q < col->count; q++) {
-            const int p = hc[col->start + q];
-            auto it = groups.find(hoff[p]);
-            if (it == groups.end()) {
-                keys.push_back(hoff[p]);
-                groups[hoff[p]] = {p};
-            } else {
-                it->second.push_back(p);
-            }
-        }
-        for (int64_t k : keys) {
-            const std::vector<int>& g = groups[k];
-            for (size_t i = 0; i < g.size(); i += kBatch) {
-                const size_t e = std::min(g.size(), i + kBatch);
-                hb.insert(hb.end(), g.begin() + i, g.begin() + e);
-                hbp.push_back((int)hb.size());
-            }
-        }
-        col->b_count = (int)hbp.size() - 1 - col->b_start;
-    }
-    bpat.alloc(std::max<size_t>(hb.size(), 1));
-    bptr.alloc(hbp.size());
-    JFG_CUDA(cudaMemcpyAsync(bpat.p, hb.data(), sizeof(int) * hb.size(), cudaMemcpyHostToDevice, c->stream));
-    JFG_CUDA(cudaMemcpyAsync(bptr.p, hbp.data(), sizeof(int) * hbp.size(), cudaMemcpyHostToDevice, c->stream));
-    batch_smem = (size_t)kBatch * max_m * (sizeof(double) + 3 * sizeof(int));
-    batched = true;
-}
 
 void SchwarzImpl::build_scatter(Colour& col, const std::vector<int64_t>& hp, const std::vector<int>& hd,
                                 const std::vector<int>& patches, std::vector<int>& h_touched,
@@ -663,9 +535,6 @@ void SchwarzImpl::init(Context* ctx, Matrix* Am, int kind_, double omega_, int n
     std::vector<int> h_touched;
     std::vector<int64_t> h_tptr, h_slots;
     bool need_buffer = false;
-    // batches of patches that share an inverse (JFEM_SCHWARZ_BATCH=0: one CTA per patch)
-    const char* eb = getenv("JFEM_SCHWARZ_BATCH");
-    const bool batch_ok = !(eb && eb[0] == '0') && nunique < np && max_m <= kBatchM;
     if (kind == JFG_SCHWARZ_MULTIPLICATIVE) {
         std::vector<int> s(2 * (size_t)np);
         for (int p = 0; p < np; p++) {
@@ -716,11 +585,6 @@ void SchwarzImpl::init(Context* ctx, Matrix* Am, int kind_, double omega_, int n
                 need_buffer = true;
             }
         }
-        if (batch_ok) {
-            std::vector<Colour*> cols;
-            for (auto& col : colours) cols.push_back(&col);
-            build_batches(cols, hc, hoff2);
-        }
         // ColoredMultiplicativeSubspaceCorrection.solve starts with patch 0 alone
         int zero = 0;
         seq.alloc(1);
@@ -734,10 +598,6 @@ void SchwarzImpl::init(Context* ctx, Matrix* Am, int kind_, double omega_, int n
         JFG_CUDA(cudaMemcpyAsync(cpat.p, pl.data(), sizeof(int) * np, cudaMemcpyHostToDevice, st));
         build_scatter(all, hp, hd, pl, h_touched, h_tptr, h_slots);
         need_buffer = true;
-        if (batch_ok) {
-            std::vector<Colour*> cols{&all};
-            build_batches(cols, pl, hoff2);
-        }
     }
     if (need_buffer) {
         h_tptr.push_back((int64_t)h_slots.size());
@@ -779,20 +639,15 @@ void SchwarzImpl::colour_step(const Colour& col, const T* b, T* x, double om, co
     using IT = T;
     const IT* iv = static_cast<const IT*>(inv_of<T>(this));
     const bool additive = kind == JFG_SCHWARZ_ADDITIVE;
-    const bool direct = col.independent && !additive;
-    if (batched && col.b_count > 0)
-        k_schwarz_batch<T, IT><<<col.b_count, kSchThreads, batch_smem, st>>>(
-            csr_of(A), bpat.p, bptr.p + col.b_start, pptr.p, dofs.p, inv_off.p, iv, b, x, om,
-            direct ? nullptr : lsol.p, direct ? 1 : 0, done);
-    else
+    if (col.independent && !additive) {
         k_schwarz_patches<T, IT><<<col.count, kSchThreads, 0, st>>>(csr_of(A), cpat.p + col.start, pptr.p, dofs.p,
-                                                                    inv_off.p, iv, b, x, om,
-                                                                    direct ? nullptr : lsol.p, direct ? 1 : 0, done);
-    if (direct) {
+                                                                    inv_off.p, iv, b, x, om, nullptr, 1, done);
         JFG_CUDA(cudaGetLastError());
         note_launch();
         return;
     }
+    k_schwarz_patches<T, IT><<<col.count, kSchThreads, 0, st>>>(csr_of(A), cpat.p + col.start, pptr.p, dofs.p,
+                                                                inv_off.p, iv, b, x, om, lsol.p, 0, done);
     const int64_t nt = col.t_count;
     const unsigned grid = (unsigned)std::min<int64_t>((nt + 255) / 256, 148 * 16);
     if (nt > 0) {

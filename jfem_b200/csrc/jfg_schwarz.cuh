@@ -37,13 +37,7 @@ struct SchwarzImpl {
         int start = 0, count = 0;       // range of cpat
         bool independent = false;       // patches neither share nor couple DOFs: one fused kernel
         int64_t t_start = 0, t_count = 0;   // range of touched
-        int b_start = 0, b_count = 0;       // batches of patches sharing an inverse (range of bptr)
     };
-    // batches: the patches of batch k are bpat[bptr[k], bptr[k+1]) (up to 8, one
-    // inverse); built when inverses are shared and patches have <= 256 DOFs
-    bool batched = false;
-    size_t batch_smem = 0;
-    DevBuf<int> bpat, bptr;
     std::vector<Colour> colours;
     Colour all;                         // additive: every patch in order
 
@@ -66,7 +60,6 @@ struct SchwarzImpl {
 private:
     template <typename T>
     void colour_step(const Colour& col, const T* b, T* x, double om, const int* done, cudaStream_t st);
-    void build_batches(std::vector<Colour*>& cols, const std::vector<int>& hc, const std::vector<int64_t>& hoff);
     void build_scatter(Colour& col, const std::vector<int64_t>& hp, const std::vector<int>& hd,
                        const std::vector<int>& patches, std::vector<int>& h_touched, std::vector<int64_t>& h_tptr,
                        std::vector<int64_t>& h_slots);

@@ -331,6 +331,16 @@ class DeviceMatrix:
                 "stride": S.value, "regular_rows": nreg.value, "other_rows": noth.value,
                 "other_nnz": int(onnz.value), "fp16_scale_inv": hs.value}
 
+    @staticmethod
+    def time_spmv_rotating(mats, precision=0, iters=20):
+        """Milliseconds per product over the matrices taken in turn, back to
+        back (no L2 flush between launches: the matrices together should
+        exceed the L2)."""
+        arr = (C.c_void_p * len(mats))(*[m._h.value for m in mats])
+        ms = C.c_double()
+        mats[0].ctx.check(N.load().jfg_spmv_time_rotating(arr, len(mats), precision, iters, C.byref(ms)))
+        return ms.value
+
     def time_spmv(self, precision=0, iters=50):
         ms = C.c_double()
         self.ctx.check(N.load().jfg_spmv_time(self._h, precision, iters, C.byref(ms)))

@@ -213,28 +213,3 @@ def test_shared_inverses_for_identical_patches(ctx, monkeypatch):
     for i in (0, 9, 27, 63):
         assert np.array_equal(S1.localInverse(i), S2.localInverse(i))
 
-
-@pytest.mark.parametrize("corr", ["coloured", "additive"])
-def test_batched_patches_bitwise(ctx, monkeypatch, corr):
-    """Patches of one colour that share an inverse run in batches of up to 8
-    per CTA (the inverse streamed once per batch); JFEM_SCHWARZ_BATCH=0 gives
-    one CTA per patch.  Both orders of work give the same bits."""
-    sp, sy = fe_system(2, 24)
-    parts = (12, 12)
-    _, patches = cartesian_patch_dofs(sp, parts, 1)
-    cols = nine_colours(parts)
-
-    def make():
-        c = (ColoredMultiplicativeSubspaceCorrection(0.9) if corr == "coloured"
-             else AdditiveSubspaceCorrection(0.3))
-        return UpFrontSchwarz(dev(sy, ctx), patches, c, colours=cols if corr == "coloured" else None)
-
-    S1 = make()
-    monkeypatch.setenv("JFEM_SCHWARZ_BATCH", "0")
-    S0 = make()
-    x0 = np.random.default_rng(19).standard_normal(sy.n)
-    assert np.array_equal(S1.apply(x0, sy.rhs), S0.apply(x0, sy.rhs))
-    assert np.array_equal(S1.mvMul(sy.rhs), S0.mvMul(sy.rhs))
-    So = O.Schwarz(coo_oracle(sy), O.SCHWARZ_COLORED if corr == "coloured" else O.SCHWARZ_ADDITIVE, patches,
-                   0.9 if corr == "coloured" else 0.3, colours=cols if corr == "coloured" else None)
-    close(S1.apply(x0, sy.rhs), So.apply(x0, sy.rhs))
