@@ -287,8 +287,11 @@ __global__ void k_wgrad_mid_reduce(int nparts, const float* __restrict__ part, f
 __global__ void k_conv_in(int B, int H, int W, const float* __restrict__ x, const float* __restrict__ w1,
                           bf16* __restrict__ h1)
 {
-    __shared__ float ws[kC * 9];
-    for (int i = threadIdx.x; i < kC * 9; i += blockDim.x) ws[i] = w1[i];
+    // weights transposed to [tap][co]: each tap's 32 weights are eight
+    // float4 loads (uniform addresses: one broadcast each) instead of 32
+    // scalar loads; every output sums its taps in order as before
+    __shared__ __align__(16) float ws[9 * kC];
+    for (int i = threadIdx.x; i < kC * 9; i += blockDim.x) ws[(i % 9) * kC + i / 9] = w1[i];
     __syncthreads();
     const size_t npx = (size_t)B * H * W;
     for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < npx; p += (size_t)gridDim.x * blockDim.x) {
@@ -300,25 +303,37 @@ __global__ void k_conv_in(int B, int H, int W, const float* __restrict__ x, cons
             int gy = yy + tap / 3 - 1, gx = xx + tap % 3 - 1;
             in9[tap] = (gy >= 0 && gy < H && gx >= 0 && gx < W) ? x[(bb * H + gy) * W + gx] : 0.f;
         }
+        float s[kC];
+#pragma unroll
+        for (int co = 0; co < kC; co++) s[co] = 0.f;
+#pragma unroll
+        for (int tap = 0; tap < 9; tap++) {
+            const float4* w4 = reinterpret_cast<const float4*>(ws + tap * kC);
+#pragma unroll
+            for (int c4 = 0; c4 < kC / 4; c4++) {
+                const float4 w = w4[c4];
+                s[4 * c4 + 0] += w.x * in9[tap];
+                s[4 * c4 + 1] += w.y * in9[tap];
+                s[4 * c4 + 2] += w.z * in9[tap];
+                s[4 * c4 + 3] += w.w * in9[tap];
+            }
+        }
         __align__(16) bf16 o[kC];
 #pragma unroll
-        for (int co = 0; co < kC; co++) {
-            float s = 0.f;
-#pragma unroll
-            for (int tap = 0; tap < 9; tap++) s += ws[co * 9 + tap] * in9[tap];
-            o[co] = __float2bfloat16_rn(fmaxf(s, 0.f));
-        }
+        for (int co = 0; co < kC; co++) o[co] = __float2bfloat16_rn(fmaxf(s[co], 0.f));
 #pragma unroll
         for (int q = 0; q < 4; q++) reinterpret_cast<uint4*>(h1 + p * kC)[q] = reinterpret_cast<const uint4*>(o)[q];
     }
 }
 
-// last layer 32 -> 1: y = sum_tap sum_ci w6[ci][tap] h5[p + tap][ci]
+// last layer 32 -> 1: y = sum_tap sum_ci w6[ci][tap] h5[p + tap][ci]; the
+// weights transposed to [tap][ci] so that each group of eight channels takes
+// two float4 loads (uniform addresses), the sum order unchanged
 __global__ void k_conv_out(int B, int H, int W, const bf16* __restrict__ h5, const float* __restrict__ w6,
                            float* __restrict__ y)
 {
-    __shared__ float ws[kC * 9];
-    for (int i = threadIdx.x; i < kC * 9; i += blockDim.x) ws[i] = w6[i];
+    __shared__ __align__(16) float ws[9 * kC];
+    for (int i = threadIdx.x; i < kC * 9; i += blockDim.x) ws[(i % 9) * kC + i / 9] = w6[i];
     __syncthreads();
     const size_t npx = (size_t)B * H * W;
     for (size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x; p < npx; p += (size_t)gridDim.x * blockDim.x) {
@@ -329,15 +344,17 @@ __global__ void k_conv_out(int B, int H, int W, const bf16* __restrict__ h5, con
             int gy = yy + tap / 3 - 1, gx = xx + tap % 3 - 1;
             if (gy < 0 || gy >= H || gx < 0 || gx >= W) continue;
             const uint4* src = reinterpret_cast<const uint4*>(h5 + ((bb * H + gy) * W + gx) * kC);
+            const float4* w4 = reinterpret_cast<const float4*>(ws + tap * kC);
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 uint4 u = src[q];
+                const float4 wa = w4[2 * q], wb = w4[2 * q + 1];
+                const float wq[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
                 const __nv_bfloat162* h2 = reinterpret_cast<const __nv_bfloat162*>(&u);
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
                     float2 f = __bfloat1622float2(h2[e]);
-                    int ci = q * 8 + 2 * e;
-                    s += ws[ci * 9 + tap] * f.x + ws[(ci + 1) * 9 + tap] * f.y;
+                    s += wq[2 * e] * f.x + wq[2 * e + 1] * f.y;
                 }
             }
         }

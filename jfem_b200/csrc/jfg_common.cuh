@@ -149,7 +149,7 @@ struct Matrix {
     // from the row's grid position (strides st_S of the rows, st_S2 of the
     // columns); st_K values per row (4 or 9).
     int st = 0;
-    int st_staged = 1;            // the staged kernel (k_spmv_pt) for the 9-point kind; 0: k_spmv_st
+    int st_staged = 0;            // 1: the staged kernel (k_spmv_pt) for the 9-point kind; 0: k_spmv_st
     DevBuf<int> st_err;           // set by k_spmv_pt when a bulk copy does not complete
     int st_kind = 0, st_K = 9, st_S2 = 0;
     int st_S = 0, st_lo = 0, st_hi = 0, st_nirr = 0, st_ld = 0;

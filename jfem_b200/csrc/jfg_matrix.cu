@@ -282,12 +282,12 @@ bool stencil_enabled()
     return !(e && e[0] == '0');
 }
 
-// JFEM_ST_STAGED=0 gives the 9-point layouts built afterwards the register
-// kernel k_spmv_st instead of the staged k_spmv_pt (read at each build)
+// JFEM_ST_STAGED=1 gives the 9-point layouts built afterwards the staged
+// kernel k_spmv_pt instead of the register kernel k_spmv_st (read at each build)
 static bool st_staged_enabled()
 {
     const char* e = getenv("JFEM_ST_STAGED");
-    return !(e && e[0] == '0');
+    return e && e[0] == '1';
 }
 
 // Point layout of M (see Matrix::st) for the rows whose entries fit it:

@@ -188,12 +188,17 @@ void spmv_launch(cudaStream_t st, const Matrix* M, const VT* val, const XT* x, E
 {
     if (M->rows == 0) return;
     GridRed<NR, Fin> red{sc.partials, sc.counter, fin};
-    // the values-only point layouts, when the matrix has one in this value type
-    if (M->st && val == LayoutVals<VT>::sell(M) && LayoutVals<VT>::st(M) && (M->st_staged || M->st_kind != 0)) {
+    // the values-only point layouts, when the matrix has one in this value type:
+    // transfers (kinds 1, 2) by the staged kernel for 4- and 2-byte values
+    // (FP64 transfers measured faster in SELL-32), the 9-point kind by the
+    // register kernel k_spmv_st (measured faster than the staged one) unless
+    // the matrix was built with JFEM_ST_STAGED=1
+    const bool pt_layout = M->st && val == LayoutVals<VT>::sell(M) && LayoutVals<VT>::st(M);
+    if (pt_layout && ((M->st_kind != 0 && !std::is_same<VT, double>::value) || (M->st_kind == 0 && M->st_staged))) {
         launch_pt<VT, XT, NR, Epi, Fin, PF>(st, M, LayoutVals<VT>::st(M), x, epi, red, done);
         return;
     }
-    if (M->st && val == LayoutVals<VT>::sell(M) && LayoutVals<VT>::st(M)) {
+    if (pt_layout && M->st_kind == 0) {
         // persistent: as many regular CTAs as stay resident next to the irregular ones
         // (FP64 values: up to 128 registers, 2 CTAs per SM)
         const int nbr = std::max(1, std::min(M->st_nb_reg, sm_count() * (sizeof(VT) == 8 ? 2 : kStCtasPerSm) -

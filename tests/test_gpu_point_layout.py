@@ -1,9 +1,9 @@
 """The values-only point layouts and the staged product kernel.
 
-* 9-point layout of Q1 level matrices: the staged kernel (k_spmv_pt: value
-  streams by bulk copies into shared memory) and the register kernel
-  (k_spmv_st, JFEM_ST_STAGED=0) give the SELL kernels' bits (products in
-  FP64, FP32, BF16 and scaled FP16);
+* 9-point layout of Q1 level matrices: the register kernel (k_spmv_st, the
+  default) and the staged kernel (k_spmv_pt: value streams by bulk copies
+  into shared memory, JFEM_ST_STAGED=1) give the SELL kernels' bits
+  (products in FP64, FP32, BF16 and scaled FP16);
 * transfer layouts of Q1 prolongations (4 values per fine row) and
   restrictions (9 values per coarse row), built by the multigrid set-up when
   the level matrices carry the 9-point layout with strides S and 2 S - 1: the
@@ -41,6 +41,7 @@ def _mg(h, ctx, precision):
 @pytest.mark.parametrize("values", ["fp64", "fp32", "bf16", "fp16"])
 def test_staged_equals_register_stencil_kernel(ctx, q1_512, monkeypatch, values):
     sy = q1_512.finest
+    monkeypatch.setenv("JFEM_ST_STAGED", "1")
     A_pt = DeviceMatrix(sy.n, sy.n, sy.rows, sy.cols, sy.vals, ctx)
     monkeypatch.setenv("JFEM_ST_STAGED", "0")
     A_reg = DeviceMatrix(sy.n, sy.n, sy.rows, sy.cols, sy.vals, ctx)
@@ -80,8 +81,10 @@ def test_transfer_layouts_vcycle(ctx, q1_512, monkeypatch, precision):
     v_sell = mg0.vCycle(np.zeros(b.size), b)
     tol = 1e-12 if precision == "fp64" else 1e-5
     np.testing.assert_allclose(v_pt, v_sell, rtol=tol, atol=tol * np.abs(v_sell).max())
-    xc = np.random.default_rng(23).standard_normal(h.systems[-2].n)
-    assert np.array_equal(prol[-1].spmv(xc), prol0[-1].spmv(xc))
+    xc = torch.from_numpy(np.random.default_rng(23).standard_normal(h.systems[-2].n).astype(np.float32)).cuda()
+    for vals in ("fp32", "bf16", "fp16"):
+        assert np.array_equal(prol[-1].spmv_lowp_dev(xc, vals).cpu().numpy(),
+                              prol0[-1].spmv_lowp_dev(xc, vals).cpu().numpy())
     if precision == "fp64":
         L = len(h.systems)
         mats_o = [O.CooMatrix(s.n, s.n, s.rows, s.cols, s.vals) for s in h.systems]
@@ -93,9 +96,14 @@ def test_transfer_layouts_vcycle(ctx, q1_512, monkeypatch, precision):
 
 
 def test_prolongation_layout_vs_oracle(ctx, q1_512):
+    """FP64 products of the prolongations (SELL-32 for FP64 values) to
+    1e-12 and the FP32 products of the transfer layout within the classical
+    summation bound 2 (k + 1) u (|P| |x|) of the oracle's product of the same
+    FP32-rounded values and vector."""
     h = q1_512
-    _, prol, _ = _mg(h, ctx, "fp64")
+    _, prol, _ = _mg(h, ctx, "mixed")
     rng = np.random.default_rng(22)
+    u32 = 2.0 ** -24
     for l in (len(prol) - 1, len(prol) - 3):
         P = prol[l]
         nf, nc = h.systems[l + 1].n, h.systems[l].n
@@ -107,3 +115,10 @@ def test_prolongation_layout_vs_oracle(ctx, q1_512):
         z = rng.standard_normal(nf)
         zr = ref.tvmul(z)
         np.testing.assert_allclose(P.spmv_t(z), zr, rtol=1e-12, atol=1e-12 * np.abs(zr).max())
+        x32 = x.astype(np.float32)
+        y32 = P.spmv_lowp_dev(torch.from_numpy(x32).cuda(), "fp32").cpu().numpy().astype(np.float64)
+        r, c, v = h.prolong[l]
+        v32 = np.asarray(v).astype(np.float32).astype(np.float64)
+        exact = O.CooMatrix(nf, nc, r, c, v32).mvmul(x32.astype(np.float64))
+        absr = O.CooMatrix(nf, nc, r, c, np.abs(v32)).mvmul(np.abs(x32).astype(np.float64))
+        assert np.all(np.abs(y32 - exact) <= 2 * 5 * u32 * absr + 1e-30)
