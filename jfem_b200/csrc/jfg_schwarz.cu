@@ -259,6 +259,29 @@ __global__ void __launch_bounds__(kSchThreads)
 constexpr int kRowLanes = 4;     // lanes per residual row: 64 rows in flight per CTA
 constexpr int kRowUnroll = 8;    // entries per lane fetched before any product (rows <= 32 entries in one shot)
 
+// Row i of a patch inverse (stored transposed: At[j * m + i]) times the
+// residual r, summed in column order from 0.  The entries are loaded
+// kInvChunk at a time into registers before their multiply-adds, so the
+// loads of a chunk are in flight together.
+constexpr int kInvChunk = 16;
+
+template <typename IT>
+__device__ __forceinline__ double inv_row_dot(const IT* __restrict__ At, int m, int i, const double* r)
+{
+    double acc = 0.0;
+    for (int j0 = 0; j0 < m; j0 += kInvChunk) {
+        double a[kInvChunk];
+#pragma unroll
+        for (int u = 0; u < kInvChunk; u++) a[u] = j0 + u < m ? (double)__ldg(At + (size_t)(j0 + u) * m + i) : 0.0;
+#pragma unroll
+        for (int u = 0; u < kInvChunk; u++) {
+            if (j0 + u >= m) break;
+            acc += a[u] * r[j0 + u];
+        }
+    }
+    return acc;
+}
+
 template <typename T, typename IT>
 __device__ __forceinline__ void patch_correct(const CsrView& A, int p, const int64_t* __restrict__ pptr,
                                               const int* __restrict__ dofs, const int64_t* __restrict__ inv_off,
@@ -302,9 +325,7 @@ __device__ __forceinline__ void patch_correct(const CsrView& A, int p, const int
     __syncthreads();
     const IT* At = inv + inv_off[p];                    // transposed: At[j * m + i] = inverse(i, j)
     for (int i = tid; i < m; i += blockDim.x) {
-        double acc = 0.0;
-#pragma unroll 16
-        for (int j = 0; j < m; j++) acc += (double)__ldg(At + (size_t)j * m + i) * sr[j];
+        const double acc = inv_row_dot(At, m, i, sr);
         if (direct) {
             const int g = sdof[i];
             x[g] = (T)((double)x[g] + acc * om);
@@ -394,12 +415,18 @@ __global__ void __launch_bounds__(kSchThreads)
         double acc[kBatch];
 #pragma unroll
         for (int q = 0; q < kBatch; q++) acc[q] = 0.0;
-#pragma unroll 8
-        for (int j = 0; j < m; j++) {
-            const double a = (double)__ldg(At + (size_t)j * m + i);
+        for (int j0 = 0; j0 < m; j0 += kInvChunk) {
+            double a[kInvChunk];
 #pragma unroll
-            for (int q = 0; q < kBatch; q++)
-                if (q < cnt) acc[q] += a * sr[q][j];
+            for (int u = 0; u < kInvChunk; u++)
+                a[u] = j0 + u < m ? (double)__ldg(At + (size_t)(j0 + u) * m + i) : 0.0;
+#pragma unroll
+            for (int u = 0; u < kInvChunk; u++) {
+                if (j0 + u >= m) break;
+#pragma unroll
+                for (int q = 0; q < kBatch; q++)
+                    if (q < cnt) acc[q] += a[u] * sr[q][j0 + u];
+            }
         }
 #pragma unroll
         for (int q = 0; q < kBatch; q++) {
