@@ -661,8 +661,7 @@ def run_kappa(args):
             "gpu_launches": int(round(launches)),
             "roofline": {"bound": "hbm", "achieved": gbs32, "peak": peak, "unit": "GB/s", "frac": gbs32 / peak,
                          "traffic": None,
-                         "kernel": "k_spmv_pt<float> (values-only 9-point layout, value streams staged in "
-                                   "shared memory by bulk copies), finest level",
+                         "kernel": "k_spmv_st<float> (values-only 9-point layout), finest level",
                          "timing": "20 rounds of 4 back-to-back launches over 4 matrix copies, one event pair",
                          "peak_source": peak_src, "bytes_per_launch": b32, "ms_per_launch": ms_spmv32},
             "clocks": clk.summary(),
@@ -678,9 +677,12 @@ def run_kappa(args):
 
 
 # DRAM bytes (read + write) of one cold launch of the FP32 finest-level product
-# of the kappa workload, from an ncu capture of that launch (not measured by
-# this script); empty until captured.
-KAPPA_TRAFFIC = {}
+# of the kappa workload (k_spmv_st), from an ncu capture of that launch: a
+# constant of an earlier capture, not measured by this script.
+KAPPA_TRAFFIC = {"case": (1050625, 9410585), "bytes": 42063360,
+                 "source": "ncu capture of one cold k_spmv_st<float> launch on this matrix "
+                           "(dram__bytes_read.sum 42.058 MB + dram__bytes_write.sum 5 KB); a constant, "
+                           "not measured in this run"}
 
 
 def q2_extra(ctx, reps, stream, args):
@@ -1183,6 +1185,32 @@ def run_stokes(args):
                      "status": N.STATUS_NAMES[it.last.status],
                      "true_rel_residual": float(np.linalg.norm(r) / np.linalg.norm(b)), "setup_s": setup}
         del sol
+    # the reference's monolithic driver (Examples/src/StokesMGSchwarz.java):
+    # PGMRES with the MG of the whole Taylor-Hood system of every level (pinned
+    # first pressure unknown), coloured Schwarz smoothing (partitions
+    # 2 * 2^(l-1), overlap 2, 2 runs), FMG + 3 V-cycles per application
+    if os.environ.get("JFEM_BENCH_NO_MONOLITHIC") != "1":
+        from jfem_b200.stokes import MonolithicStokesMG
+        t1 = time.time()
+        mono = MonolithicStokesMG(ctx, cells=prob.spaces[-1].cx, coarse_cells=4, seed=0)
+        setup = time.time() - t1
+        bm = mono.rhs
+        tol_m = RTOL * float(np.linalg.norm(bm))
+        for _ in range(max(1, args.warmup)):
+            x, it = mono.solve(tol_m)
+        ts = []
+        for _ in range(max(1, args.steps // 3)):
+            t2 = time.perf_counter()
+            x, it = mono.solve(tol_m)
+            ts.append(time.perf_counter() - t2)
+        r = bm - mono.A.spmv(x)
+        out["monolithic_schwarz_mg"] = {
+            "time_s": min(ts), "iterations": it.iterations, "restarts": it.last.restarts,
+            "status": N.STATUS_NAMES[it.last.status], "true_rel_residual": float(np.linalg.norm(r) / np.linalg.norm(bm)),
+            "setup_s": setup, "dofs": int(mono.A.rows), "max_patch": max(sw.info()["max_patch"] for sw in mono.schwarz),
+            "mode": "PGMRES(50) + MG of the whole Taylor-Hood system (FMG + 3 V-cycles), coloured Schwarz "
+                    "2 runs, partitions 2*2^(l-1), overlap 2, pinned pressure (the reference's system)"}
+        del mono
     s = prob.system
     line = {"metric": "time-to-1e-8 residual (s), Stokes GMRES(50) + block-diagonal preconditioner",
             "value": out["schwarz_fp64"]["time_s"], "unit": "s", "n_gpus": 1, "steps": args.steps,

@@ -284,93 +284,96 @@ __global__ void k_wgrad_mid_reduce(int nparts, const float* __restrict__ part, f
 }
 
 // first layer 1 -> 32 with ReLU: h1 = relu(sum_tap w1[co][tap] x[p + tap])
-// First and last layers on CUDA cores, four lanes per pixel: lane q of a
-// pixel owns channels 8q .. 8q + 7 (one 16-byte chunk of the pixel's 64-byte
-// activation row), so a warp's loads and stores of activations cover eight
-// whole consecutive pixel rows (512 contiguous bytes) instead of touching a
-// 16-byte piece of 32 different rows.  Weights sit in shared memory as
-// [tap][channel] and are read as float4 vectors at uniform addresses.
+// First and last layers on CUDA cores.  A CTA row of the grid is one image
+// row (blockIdx.y = b * H + y); four lanes per pixel, lane q owning channels
+// 8q .. 8q + 7 (one 16-byte chunk of the pixel's 64-byte activation row), so
+// a warp's activation loads and stores cover eight whole consecutive pixel
+// rows.  No division per pixel, the nine taps unrolled with predicated
+// loads; weights in shared memory as [tap][channel], read as float4 vectors
+// at uniform addresses.
 constexpr int kLanesPerPx = 4;
+constexpr int kEdgePx = 256 / kLanesPerPx;        // pixels of one CTA (64 along x)
 
 // first layer 1 -> 32 with ReLU: h1[p][co] = relu(sum_tap w1[co][tap] x[p + tap]),
 // each output's taps summed in order
-__global__ void k_conv_in(int B, int H, int W, const float* __restrict__ x, const float* __restrict__ w1,
-                          bf16* __restrict__ h1)
+__global__ void __launch_bounds__(256)
+k_conv_in(int B, int H, int W, const float* __restrict__ x, const float* __restrict__ w1, bf16* __restrict__ h1)
 {
     __shared__ __align__(16) float ws[9 * kC];
     for (int i = threadIdx.x; i < kC * 9; i += blockDim.x) ws[(i % 9) * kC + i / 9] = w1[i];
     __syncthreads();
-    const int nt = B * H * W * kLanesPerPx;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
-        const int p = t / kLanesPerPx, q = t % kLanesPerPx;
-        const int xx = p % W, yy = (p / W) % H, bb = p / (H * W);
-        float in9[9];
+    const int row = blockIdx.y, yy = row % H;
+    const int xx = blockIdx.x * kEdgePx + (int)threadIdx.x / kLanesPerPx, q = threadIdx.x % kLanesPerPx;
+    if (xx >= W) return;
+    const float* xr = x + (size_t)row * W;
+    float in9[9];
 #pragma unroll
-        for (int tap = 0; tap < 9; tap++) {
-            const int gy = yy + tap / 3 - 1, gx = xx + tap % 3 - 1;
-            in9[tap] = (gy >= 0 && gy < H && gx >= 0 && gx < W) ? x[((size_t)bb * H + gy) * W + gx] : 0.f;
+    for (int dy = -1; dy <= 1; dy++) {
+        const bool okr = yy + dy >= 0 && yy + dy < H;
+#pragma unroll
+        for (int dx = -1; dx <= 1; dx++) {
+            const bool ok = okr && xx + dx >= 0 && xx + dx < W;
+            in9[(dy + 1) * 3 + dx + 1] = ok ? __ldg(xr + (ptrdiff_t)dy * W + xx + dx) : 0.f;
         }
-        float s[8];
-#pragma unroll
-        for (int c = 0; c < 8; c++) s[c] = 0.f;
-#pragma unroll
-        for (int tap = 0; tap < 9; tap++) {
-            const float4* w4 = reinterpret_cast<const float4*>(ws + tap * kC + 8 * q);
-            const float4 wa = w4[0], wb = w4[1];
-            s[0] += wa.x * in9[tap];
-            s[1] += wa.y * in9[tap];
-            s[2] += wa.z * in9[tap];
-            s[3] += wa.w * in9[tap];
-            s[4] += wb.x * in9[tap];
-            s[5] += wb.y * in9[tap];
-            s[6] += wb.z * in9[tap];
-            s[7] += wb.w * in9[tap];
-        }
-        __align__(16) bf16 o[8];
-#pragma unroll
-        for (int c = 0; c < 8; c++) o[c] = __float2bfloat16_rn(fmaxf(s[c], 0.f));
-        *reinterpret_cast<uint4*>(h1 + (size_t)p * kC + 8 * q) = *reinterpret_cast<const uint4*>(o);
     }
+    float s[8];
+#pragma unroll
+    for (int c = 0; c < 8; c++) s[c] = 0.f;
+#pragma unroll
+    for (int tap = 0; tap < 9; tap++) {
+        const float4* w4 = reinterpret_cast<const float4*>(ws + tap * kC + 8 * q);
+        const float4 wa = w4[0], wb = w4[1];
+        s[0] += wa.x * in9[tap];
+        s[1] += wa.y * in9[tap];
+        s[2] += wa.z * in9[tap];
+        s[3] += wa.w * in9[tap];
+        s[4] += wb.x * in9[tap];
+        s[5] += wb.y * in9[tap];
+        s[6] += wb.z * in9[tap];
+        s[7] += wb.w * in9[tap];
+    }
+    __align__(16) bf16 o[8];
+#pragma unroll
+    for (int c = 0; c < 8; c++) o[c] = __float2bfloat16_rn(fmaxf(s[c], 0.f));
+    *reinterpret_cast<uint4*>(h1 + ((size_t)row * W + xx) * kC + 8 * q) = *reinterpret_cast<const uint4*>(o);
 }
 
 // last layer 32 -> 1: y = sum_tap sum_ci w6[ci][tap] h5[p + tap][ci]; lane q
 // sums its eight channels over the taps, the four lanes' sums are added by
 // two shuffles (lanes (0+1) + (2+3))
-__global__ void k_conv_out(int B, int H, int W, const bf16* __restrict__ h5, const float* __restrict__ w6,
-                           float* __restrict__ y)
+__global__ void __launch_bounds__(256)
+k_conv_out(int B, int H, int W, const bf16* __restrict__ h5, const float* __restrict__ w6, float* __restrict__ y)
 {
     __shared__ __align__(16) float ws[9 * kC];
     for (int i = threadIdx.x; i < kC * 9; i += blockDim.x) ws[(i % 9) * kC + i / 9] = w6[i];
     __syncthreads();
-    const int nt = B * H * W * kLanesPerPx;
-    const int stride = gridDim.x * blockDim.x;
-    // the trip count is uniform across the CTA (full warps at the shuffles)
-    for (int t0 = blockIdx.x * blockDim.x; t0 < nt; t0 += stride) {
-        const int t = t0 + threadIdx.x;
-        const bool valid = t < nt;
-        const int p = valid ? t / kLanesPerPx : 0, q = t % kLanesPerPx;
-        const int xx = p % W, yy = (p / W) % H, bb = p / (H * W);
-        float s = 0.f;
-        if (valid) {
-            for (int tap = 0; tap < 9; tap++) {
-                const int gy = yy + tap / 3 - 1, gx = xx + tap % 3 - 1;
-                if (gy < 0 || gy >= H || gx < 0 || gx >= W) continue;
-                const uint4 u = *reinterpret_cast<const uint4*>(h5 + (((size_t)bb * H + gy) * W + gx) * kC + 8 * q);
-                const float4* w4 = reinterpret_cast<const float4*>(ws + tap * kC + 8 * q);
-                const float4 wa = w4[0], wb = w4[1];
-                const float wq[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
-                const __nv_bfloat162* h2 = reinterpret_cast<const __nv_bfloat162*>(&u);
+    const int row = blockIdx.y, yy = row % H;
+    const int xx = blockIdx.x * kEdgePx + (int)threadIdx.x / kLanesPerPx, q = threadIdx.x % kLanesPerPx;
+    const bool valid = xx < W;                      // every lane reaches the shuffles
+    const bf16* hr = h5 + ((size_t)row * W + xx) * kC + 8 * q;
+    float s = 0.f;
 #pragma unroll
-                for (int e = 0; e < 4; e++) {
-                    const float2 f = __bfloat1622float2(h2[e]);
-                    s += wq[2 * e] * f.x + wq[2 * e + 1] * f.y;
-                }
+    for (int dy = -1; dy <= 1; dy++) {
+        const bool okr = valid && yy + dy >= 0 && yy + dy < H;
+#pragma unroll
+        for (int dx = -1; dx <= 1; dx++) {
+            if (!(okr && xx + dx >= 0 && xx + dx < W)) continue;
+            const int tap = (dy + 1) * 3 + dx + 1;
+            const uint4 u = __ldg(reinterpret_cast<const uint4*>(hr + ((ptrdiff_t)dy * W + dx) * kC));
+            const float4* w4 = reinterpret_cast<const float4*>(ws + tap * kC + 8 * q);
+            const float4 wa = w4[0], wb = w4[1];
+            const float wq[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+            const __nv_bfloat162* h2 = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                const float2 f = __bfloat1622float2(h2[e]);
+                s += wq[2 * e] * f.x + wq[2 * e + 1] * f.y;
             }
         }
-        s += __shfl_xor_sync(0xffffffffu, s, 1);
-        s += __shfl_xor_sync(0xffffffffu, s, 2);
-        if (valid && q == 0) y[p] = s;
     }
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    if (valid && q == 0) y[(size_t)row * W + xx] = s;
 }
 
 // loss = mean (y - t)^2 (FP64 sum), dy = 2 (y - t) / N
@@ -624,11 +627,11 @@ bool use_tc()
 
 void cnn_forward(jfg_cnn* n, cudaStream_t st, int B, int H, int W, const float* x, float* y)
 {
-    size_t npx = (size_t)B * H * W;
     cnn_pack(n, st);
     const bf16* wk = n->wk.p;
-    JFG_CHECK(npx * kLanesPerPx < ((size_t)1 << 31), JFG_ERR_UNSUPPORTED, "image batch too large");
-    k_conv_in<<<grid1d(npx * kLanesPerPx), 256, 0, st>>>(B, H, W, x, n->w32.p + kLayerOff[0], n->h1.p);
+    JFG_CHECK((size_t)B * H < 65536, JFG_ERR_UNSUPPORTED, "image batch too large (B * H >= 65536 rows)");
+    const dim3 edge_grid((unsigned)((W + kEdgePx - 1) / kEdgePx), (unsigned)(B * H));
+    k_conv_in<<<edge_grid, 256, 0, st>>>(B, H, W, x, n->w32.p + kLayerOff[0], n->h1.p);
     JFG_CUDA(cudaGetLastError());
     if (use_tc()) {
         int* err = n->tc_err.p;
@@ -644,7 +647,7 @@ void cnn_forward(jfg_cnn* n, cudaStream_t st, int B, int H, int W, const float* 
         conv_mid<bf16, bf16, 1, true, false>(st, B, H, W, n->a4.p, wk + 3 * kMidParams, n->h3.p, nullptr,
                                              n->h5.p);
     }
-    k_conv_out<<<grid1d(npx * kLanesPerPx), 256, 0, st>>>(B, H, W, n->h5.p, n->w32.p + kLayerOff[5], y);
+    k_conv_out<<<edge_grid, 256, 0, st>>>(B, H, W, n->h5.p, n->w32.p + kLayerOff[5], y);
     JFG_CUDA(cudaGetLastError());
     note_launch(2);
 }

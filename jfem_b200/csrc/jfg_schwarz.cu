@@ -259,29 +259,6 @@ __global__ void __launch_bounds__(kSchThreads)
 constexpr int kRowLanes = 4;     // lanes per residual row: 64 rows in flight per CTA
 constexpr int kRowUnroll = 8;    // entries per lane fetched before any product (rows <= 32 entries in one shot)
 
-// Row i of a patch inverse (stored transposed: At[j * m + i]) times the
-// residual r, summed in column order from 0.  The entries are loaded
-// kInvChunk at a time into registers before their multiply-adds, so the
-// loads of a chunk are in flight together.
-constexpr int kInvChunk = 16;
-
-template <typename IT>
-__device__ __forceinline__ double inv_row_dot(const IT* __restrict__ At, int m, int i, const double* r)
-{
-    double acc = 0.0;
-    for (int j0 = 0; j0 < m; j0 += kInvChunk) {
-        double a[kInvChunk];
-#pragma unroll
-        for (int u = 0; u < kInvChunk; u++) a[u] = j0 + u < m ? (double)__ldg(At + (size_t)(j0 + u) * m + i) : 0.0;
-#pragma unroll
-        for (int u = 0; u < kInvChunk; u++) {
-            if (j0 + u >= m) break;
-            acc += a[u] * r[j0 + u];
-        }
-    }
-    return acc;
-}
-
 template <typename T, typename IT>
 __device__ __forceinline__ void patch_correct(const CsrView& A, int p, const int64_t* __restrict__ pptr,
                                               const int* __restrict__ dofs, const int64_t* __restrict__ inv_off,
@@ -325,7 +302,9 @@ __device__ __forceinline__ void patch_correct(const CsrView& A, int p, const int
     __syncthreads();
     const IT* At = inv + inv_off[p];                    // transposed: At[j * m + i] = inverse(i, j)
     for (int i = tid; i < m; i += blockDim.x) {
-        const double acc = inv_row_dot(At, m, i, sr);
+        double acc = 0.0;
+#pragma unroll 16
+        for (int j = 0; j < m; j++) acc += (double)__ldg(At + (size_t)j * m + i) * sr[j];
         if (direct) {
             const int g = sdof[i];
             x[g] = (T)((double)x[g] + acc * om);
@@ -356,6 +335,7 @@ __global__ void __launch_bounds__(kSchThreads, 5)
 // inverse, so the inverse is read once per batch.  Bit for bit the result of
 // k_schwarz_patches.
 constexpr int kBatch = 4;
+constexpr int kInvChunk = 8;               // inverse entries loaded ahead of their multiply-adds
 
 template <typename T>
 __global__ void __launch_bounds__(kSchThreads)
@@ -393,7 +373,7 @@ __global__ void __launch_bounds__(kSchThreads)
 // the same offsets.  Thread i sums row i of the inverse times each residual in
 // column order (patch_correct's order) and updates x.
 template <typename T, typename IT>
-__global__ void __launch_bounds__(kSchThreads)
+__global__ void __launch_bounds__(kSchThreads, 4)
     k_schwarz_inv_batch(const int* __restrict__ bpat, const int* __restrict__ bptr, const int* __restrict__ boff,
                         const int64_t* __restrict__ pptr, const int* __restrict__ rowdof,
                         const int64_t* __restrict__ inv_off, const IT* __restrict__ inv,
@@ -416,7 +396,7 @@ __global__ void __launch_bounds__(kSchThreads)
 #pragma unroll
         for (int q = 0; q < kBatch; q++) acc[q] = 0.0;
         for (int j0 = 0; j0 < m; j0 += kInvChunk) {
-            double a[kInvChunk];
+            double a[kInvChunk];                // the chunk's loads in flight together
 #pragma unroll
             for (int u = 0; u < kInvChunk; u++)
                 a[u] = j0 + u < m ? (double)__ldg(At + (size_t)(j0 + u) * m + i) : 0.0;

@@ -369,3 +369,98 @@ class StokesSolver:
         if s.pressure_fixed < 0:
             x[s.nv:] -= x[s.nv]          # the pinned system's pressure gauge
         return x, it
+
+
+# ---------------------------------------------------------------------------
+# Monolithic multigrid on the whole Taylor-Hood system (Examples/src/StokesMGSchwarz.java)
+# ---------------------------------------------------------------------------
+def pressure_prolongation(coarse: TaylorHoodSpace, fine: TaylorHoodSpace):
+    """Nodal Q1 interpolation of the pressure (COO rows, cols, vals; pressure
+    node numbering)."""
+    Px = prolongation_1d(1, coarse.cx)
+    Py = prolongation_1d(1, coarse.cy)
+    fx, cx_ = np.nonzero(Px)
+    fy, cy_ = np.nonzero(Py)
+    fxa, cxa = np.repeat(fx, fy.size), np.repeat(cx_, fy.size)
+    fya, cya = np.tile(fy, fx.size), np.tile(cy_, fx.size)
+    return (fxa * fine.pny + fya).astype(np.int32), (cxa * coarse.pny + cya).astype(np.int32), Px[fxa, cxa] * Py[fya, cya]
+
+
+def taylor_hood_prolongation(coarse: TaylorHoodSpace, fine: TaylorHoodSpace):
+    """Prolongation of the whole mixed space (MGPreconditionerSpace.createProlongationMatrix
+    on a TaylorHoodSpace): velocity by Q2 and pressure by Q1 nodal interpolation,
+    block diagonal (pressure unknowns after the velocity ones)."""
+    Rv, Cv, Vv = velocity_prolongation(coarse, fine)
+    Rp, Cp, Vp = pressure_prolongation(coarse, fine)
+    return (np.concatenate([Rv, Rp + fine.nv]).astype(np.int32), np.concatenate([Cv, Cp + coarse.nv]).astype(np.int32),
+            np.concatenate([Vv, Vp]))
+
+
+class MixedCells:
+    """The cell table of a Taylor-Hood space for the Cartesian patch builders:
+    cell_dofs[c] = the velocity unknowns (both components) and the pressure
+    unknowns with support on cell c (getShapeFunctionsWithSupportOnCell)."""
+
+    def __init__(self, th: TaylorHoodSpace):
+        self.cx, self.cy = th.cx, th.cy
+        self.cell_dofs = np.concatenate([th.cell_velocity_dofs, th.cell_pnodes + th.nv], axis=1)
+
+
+def mixed_zero_boundary(th: TaylorHoodSpace) -> np.ndarray:
+    """applyZeroBoundaryConditions of StokesMGSchwarz: the Dirichlet velocity
+    unknowns and the first pressure unknown."""
+    return np.concatenate([th.velocity_boundary(), [th.nv]]).astype(np.int32)
+
+
+def schwarz_partitions(level: int) -> tuple:
+    """createSmoothers of StokesMGSchwarz: 2 * 2^(level - 1) partitions per
+    direction on level >= 1 (2 * max(1, 2^(level-1)))."""
+    k = 2 * max(1, 2 ** (level - 1))
+    return (k, k)
+
+
+class MonolithicStokesMG:
+    """StokesMGSchwarz: multigrid on the whole Taylor-Hood system of every
+    level (velocity Dirichlet rows and the pinned first pressure unknown, as
+    createSystem writes them), Taylor-Hood prolongations, and on every level
+    above the coarsest a SchwarzSmoother(2, ColoredCartesianSchwarz(partitions
+    2 * 2^(l-1), overlap 2, DirectSolver, omega 1)) whose patches take every
+    velocity and pressure unknown with support on their cells; the
+    preconditioner is the reference's MG mvMul (FMG + `cycles` V-cycles).
+    solve() is PGMRES to the tolerance, as the driver solves."""
+
+    def __init__(self, ctx, cells: int = 64, coarse_cells: int = 4, nu: float = 1.0, seed: int = 0, runs: int = 2,
+                 overlap: int = 2, cycles: int = 3, use_fmg: bool = True, precision: str = "fp64"):
+        from .linalg import DeviceMatrix
+        from .multigrid import MGPreconditioner
+        from .schwarz import ColoredCartesianSchwarz, DirectSolver, SchwarzSmoother
+        levels = int(round(np.log2(cells // coarse_cells))) + 1
+        if coarse_cells << (levels - 1) != cells:
+            raise IllegalArgumentException("cells must be coarse_cells * 2^k")
+        self.ctx = ctx
+        self.spaces = [TaylorHoodSpace(coarse_cells << l, coarse_cells << l) for l in range(levels)]
+        force = fourier_force(seed=seed)
+        self.systems = [assemble_stokes(t, nu, force, pin_pressure=True) for t in self.spaces]
+        self.prolong = [taylor_hood_prolongation(self.spaces[l], self.spaces[l + 1]) for l in range(levels - 1)]
+        self.boundary = [mixed_zero_boundary(t) for t in self.spaces]
+        self.mats = [DeviceMatrix(s.n, s.n, s.rows, s.cols, s.vals, ctx) for s in self.systems]
+        self.prol = [DeviceMatrix(self.spaces[l + 1].n, self.spaces[l].n, *self.prolong[l], ctx)
+                     for l in range(levels - 1)]
+        self.schwarz, sms = [], [None]
+        for l in range(1, levels):
+            sw = ColoredCartesianSchwarz(self.mats[l], MixedCells(self.spaces[l]), schwarz_partitions(l), overlap,
+                                         DirectSolver(), 1.0)
+            self.schwarz.append(sw)
+            sms.append(SchwarzSmoother(runs, sw))
+        self.mg = MGPreconditioner(self.mats, self.prol, self.boundary, sms, cycles=cycles, use_fmg=use_fmg,
+                                   precision=precision, ctx=ctx)
+        self.A = self.mats[-1]
+        self.rhs = self.systems[-1].rhs
+
+    def solve(self, tol: float, restart: int = 50, max_restarts: int = 200):
+        from .linalg import IterativeSolver
+        it = IterativeSolver(ctx=self.ctx)
+        it.gm.ITERATIONS_BEFORE_RESTART = restart
+        it.gm.MAX_RESTARTS = max_restarts
+        x = it.solvePGMRES(self.A, self.mg, self.rhs, tol)
+        return x, it

@@ -78,3 +78,35 @@ def test_problem_levels():
     p = stokes_problem(16, 4)
     assert [t.cx for t in p.spaces] == [4, 8, 16]
     assert p.pressure_inverse.size == p.spaces[-1].np_ and p.pressure_inverse[0] == 1.0
+
+
+def test_taylor_hood_prolongation_and_patches():
+    """The whole-space prolongation interpolates a quadratic velocity and a
+    bilinear pressure exactly; the monolithic Schwarz patches take the
+    velocity and pressure unknowns of their cells (8 x 8 cells inside the
+    domain at partitions 2 * 2^(l-1), overlap 2) and the zero-boundary list is
+    the Dirichlet velocity plus the first pressure unknown."""
+    from jfem_b200.schwarz import cartesian_patch_dofs
+    from jfem_b200.stokes import (MixedCells, TaylorHoodSpace, mixed_zero_boundary, schwarz_partitions,
+                                  taylor_hood_prolongation)
+    c, f = TaylorHoodSpace(4, 4), TaylorHoodSpace(8, 8)
+    R, Cc, V = taylor_hood_prolongation(c, f)
+    P = sps.csr_matrix((V, (R, Cc)), shape=(f.n, c.n))
+
+    def field(th):
+        xv, yv = th.velocity_points()
+        g = np.arange(th.np_)
+        xp, yp = (g // th.pny) * th.hx, (g % th.pny) * th.hy
+        return np.concatenate([xv ** 2 - yv, 2 * xv * yv, 1 + xp - 3 * yp + xp * yp])
+
+    np.testing.assert_allclose(P @ field(c), field(f), atol=1e-13)
+    assert schwarz_partitions(1) == (2, 2) and schwarz_partitions(3) == (8, 8)
+    th = TaylorHoodSpace(16, 16)
+    _, patches = cartesian_patch_dofs(MixedCells(th), schwarz_partitions(2), 2)
+    assert len(patches) == 16
+    assert max(len(p) for p in patches) == 2 * 17 * 17 + 81
+    inner = patches[5]                                  # partition (1, 1): cells 2..9 x 2..9
+    assert len(inner) == 2 * 17 * 17 + 81 and np.all(np.diff(inner) > 0)
+    assert np.sum(inner >= th.nv) == 81
+    bd = mixed_zero_boundary(th)
+    assert bd[-1] == th.nv and np.array_equal(np.sort(bd[:-1]), np.sort(th.velocity_boundary()))
