@@ -328,95 +328,6 @@ __global__ void __launch_bounds__(kSchThreads, 5)
                          sr);
 }
 
-// Split colour step (independent colours): the patch rows of b - A x of every
-// patch of the colour by one wide launch (kRowLanes lanes per row, the
-// entries and the lane reduction exactly as patch_correct sums them), then
-// the patch inverses applied by CTAs of up to kBatch patches that share one
-// inverse, so the inverse is read once per batch.  Bit for bit the result of
-// k_schwarz_patches.
-constexpr int kBatch = 4;
-constexpr int kInvChunk = 8;               // inverse entries loaded ahead of their multiply-adds
-
-template <typename T>
-__global__ void __launch_bounds__(kSchThreads)
-    k_schwarz_resid(CsrView A, int nrows, const int* __restrict__ rowdof, const T* b, const T* x,
-                    double* __restrict__ rbuf, const int* done)
-{
-    if (done && *done) return;
-    const int t = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) / kRowLanes);
-    const int sub = threadIdx.x & (kRowLanes - 1);
-    double acc = 0.0;
-    int g = 0;
-    if (t < nrows) {
-        g = rowdof[t];
-        const int k0 = A.rp[g] + sub, k1 = A.rp[g + 1];
-        int c[kRowUnroll];
-        double v[kRowUnroll];
-#pragma unroll
-        for (int u = 0; u < kRowUnroll; u++) {
-            const int k = k0 + u * kRowLanes;
-            c[u] = k < k1 ? __ldg(A.col + k) : -1;
-            v[u] = k < k1 ? __ldg(A.val + k) : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < kRowUnroll; u++)
-            if (c[u] >= 0) acc += v[u] * (double)x[c[u]];
-        for (int k = k0 + kRowUnroll * kRowLanes; k < k1; k += kRowLanes) acc += A.val[k] * (double)x[A.col[k]];
-    }
-#pragma unroll
-    for (int o = 1; o < kRowLanes; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if (t < nrows && sub == 0) rbuf[t] = (double)b[g] - acc;
-}
-
-// Batch k: patches bpat[bptr[k], bptr[k+1]) (same inverse, same size m), the
-// residual of the q-th at rbuf + boff[bptr[k] + q], its DOFs at rowdof with
-// the same offsets.  Thread i sums row i of the inverse times each residual in
-// column order (patch_correct's order) and updates x.
-template <typename T, typename IT>
-__global__ void __launch_bounds__(kSchThreads, 4)
-    k_schwarz_inv_batch(const int* __restrict__ bpat, const int* __restrict__ bptr, const int* __restrict__ boff,
-                        const int64_t* __restrict__ pptr, const int* __restrict__ rowdof,
-                        const int64_t* __restrict__ inv_off, const IT* __restrict__ inv,
-                        const double* __restrict__ rbuf, T* x, double om, const int* done)
-{
-    if (done && *done) return;
-    __shared__ double sr[kBatch][kMaxPatch];
-    const int q0 = bptr[blockIdx.x];
-    const int cnt = bptr[blockIdx.x + 1] - q0;
-    const int p0 = bpat[q0];
-    const int m = (int)(pptr[p0 + 1] - pptr[p0]);
-    for (int q = 0; q < cnt; q++) {
-        const double* r = rbuf + boff[q0 + q];
-        for (int i = threadIdx.x; i < m; i += blockDim.x) sr[q][i] = r[i];
-    }
-    __syncthreads();
-    const IT* At = inv + inv_off[p0];                   // transposed: At[j * m + i] = inverse(i, j)
-    for (int i = threadIdx.x; i < m; i += blockDim.x) {
-        double acc[kBatch];
-#pragma unroll
-        for (int q = 0; q < kBatch; q++) acc[q] = 0.0;
-        for (int j0 = 0; j0 < m; j0 += kInvChunk) {
-            double a[kInvChunk];                // the chunk's loads in flight together
-#pragma unroll
-            for (int u = 0; u < kInvChunk; u++)
-                a[u] = j0 + u < m ? (double)__ldg(At + (size_t)(j0 + u) * m + i) : 0.0;
-#pragma unroll
-            for (int u = 0; u < kInvChunk; u++) {
-                if (j0 + u >= m) break;
-#pragma unroll
-                for (int q = 0; q < kBatch; q++)
-                    if (q < cnt) acc[q] += a[u] * sr[q][j0 + u];
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < kBatch; q++) {
-            if (q >= cnt) break;
-            const int g = rowdof[boff[q0 + q] + i];
-            x[g] = (T)((double)x[g] + acc[q] * om);
-        }
-    }
-}
-
 // MultiplicativeSubspaceCorrection: the patches of plist one after another
 // in a single CTA (each step sees the previous steps' updates).
 template <typename T, typename IT>
@@ -494,64 +405,6 @@ __global__ void k_to_f32(int64_t n, const double* __restrict__ a, float* __restr
 CsrView csr_of(Matrix* A) { return CsrView{A->csr_ptr.p, A->csr_col.p, A->csr_val.p}; }
 
 }  // namespace
-
-// Split-step tables of the independent colours: each colour's patch DOF
-// lists concatenated in the colour's patch order (rowdof), and its patches
-// grouped by shared inverse (first occurrence first, ascending inside a
-// group) into batches of at most kBatch with each patch's offset in rowdof.
-void SchwarzImpl::build_split(const std::vector<int64_t>& hp, const std::vector<int>& hd,
-                              const std::vector<int>& hc, const std::vector<int64_t>& hoff)
-{
-    std::vector<int> hr, hb, hbp{0}, hbo;
-    for (Colour& col : colours) {
-        if (!col.independent || col.count == 0) continue;
-        col.r_start = (int)hr.size();
-        std::map<int, int> where;                       // patch -> offset in rowdof
-        for (int q = 0; q < col.count; q++) {
-            const int p = hc[col.start + q];
-            where[p] = (int)hr.size();
-            hr.insert(hr.end(), hd.begin() + hp[p], hd.begin() + hp[p + 1]);
-        }
-        col.r_count = (int)hr.size() - col.r_start;
-        std::vector<int64_t> keys;
-        std::map<int64_t, std::vector<int>> groups;
-        for (int q = 0; q < col.count; q++) {
-            const int p = hc[col.start + q];
-            auto it = groups.find(hoff[p]);
-            if (it == groups.end()) {
-                keys.push_back(hoff[p]);
-                groups[hoff[p]] = {p};
-            } else {
-                it->second.push_back(p);
-            }
-        }
-        col.b_start = (int)hbp.size() - 1;
-        for (int64_t k : keys) {
-            const std::vector<int>& g = groups[k];
-            for (size_t i = 0; i < g.size(); i += kBatch) {
-                const size_t e = std::min(g.size(), i + kBatch);
-                for (size_t j = i; j < e; j++) {
-                    hb.push_back(g[j]);
-                    hbo.push_back(where[g[j]]);
-                }
-                hbp.push_back((int)hb.size());
-            }
-        }
-        col.b_count = (int)hbp.size() - 1 - col.b_start;
-    }
-    if (hr.empty()) return;
-    cudaStream_t st = c->stream;
-    rowdof.alloc(hr.size());
-    rbuf.alloc(hr.size());
-    bpat.alloc(hb.size());
-    boff.alloc(hbo.size());
-    bptr.alloc(hbp.size());
-    JFG_CUDA(cudaMemcpyAsync(rowdof.p, hr.data(), sizeof(int) * hr.size(), cudaMemcpyHostToDevice, st));
-    JFG_CUDA(cudaMemcpyAsync(bpat.p, hb.data(), sizeof(int) * hb.size(), cudaMemcpyHostToDevice, st));
-    JFG_CUDA(cudaMemcpyAsync(boff.p, hbo.data(), sizeof(int) * hbo.size(), cudaMemcpyHostToDevice, st));
-    JFG_CUDA(cudaMemcpyAsync(bptr.p, hbp.data(), sizeof(int) * hbp.size(), cudaMemcpyHostToDevice, st));
-    split = true;
-}
 
 void SchwarzImpl::build_scatter(Colour& col, const std::vector<int64_t>& hp, const std::vector<int>& hd,
                                 const std::vector<int>& patches, std::vector<int>& h_touched,
@@ -732,9 +585,6 @@ void SchwarzImpl::init(Context* ctx, Matrix* Am, int kind_, double omega_, int n
                 need_buffer = true;
             }
         }
-        // the split step for the independent colours (JFEM_SCHWARZ_SPLIT=0: one fused kernel per colour)
-        const char* es = getenv("JFEM_SCHWARZ_SPLIT");
-        if (!(es && es[0] == '0')) build_split(hp, hd, hc, hoff2);
         // ColoredMultiplicativeSubspaceCorrection.solve starts with patch 0 alone
         int zero = 0;
         seq.alloc(1);
@@ -789,17 +639,6 @@ void SchwarzImpl::colour_step(const Colour& col, const T* b, T* x, double om, co
     using IT = T;
     const IT* iv = static_cast<const IT*>(inv_of<T>(this));
     const bool additive = kind == JFG_SCHWARZ_ADDITIVE;
-    if (col.independent && !additive && split && col.r_count > 0) {
-        const unsigned g1 = (unsigned)(((int64_t)col.r_count * kRowLanes + kSchThreads - 1) / kSchThreads);
-        k_schwarz_resid<T><<<g1, kSchThreads, 0, st>>>(csr_of(A), col.r_count, rowdof.p + col.r_start, b, x,
-                                                       rbuf.p + col.r_start, done);
-        k_schwarz_inv_batch<T, IT><<<col.b_count, kSchThreads, 0, st>>>(bpat.p, bptr.p + col.b_start, boff.p,
-                                                                          pptr.p, rowdof.p, inv_off.p, iv, rbuf.p,
-                                                                          x, om, done);
-        JFG_CUDA(cudaGetLastError());
-        note_launch(2);
-        return;
-    }
     if (col.independent && !additive) {
         k_schwarz_patches<T, IT><<<col.count, kSchThreads, 0, st>>>(csr_of(A), cpat.p + col.start, pptr.p, dofs.p,
                                                                     inv_off.p, iv, b, x, om, nullptr, 1, done);

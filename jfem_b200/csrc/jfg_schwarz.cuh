@@ -37,13 +37,7 @@ struct SchwarzImpl {
         int start = 0, count = 0;       // range of cpat
         bool independent = false;       // patches neither share nor couple DOFs: one fused kernel
         int64_t t_start = 0, t_count = 0;   // range of touched
-        // split step (independent colours): the colour's patch rows are
-        // rowdof[r_start, r_start + r_count); its batches bptr[b_start, b_start + b_count]
-        int r_start = 0, r_count = 0, b_start = 0, b_count = 0;
     };
-    bool split = false;                 // independent colours take the split step
-    DevBuf<int> rowdof, bpat, bptr, boff;
-    DevBuf<double> rbuf;                // residual rows of one colour step
     std::vector<Colour> colours;
     Colour all;                         // additive: every patch in order
 
@@ -66,8 +60,6 @@ struct SchwarzImpl {
 private:
     template <typename T>
     void colour_step(const Colour& col, const T* b, T* x, double om, const int* done, cudaStream_t st);
-    void build_split(const std::vector<int64_t>& hp, const std::vector<int>& hd, const std::vector<int>& hc,
-                     const std::vector<int64_t>& hoff);
     void build_scatter(Colour& col, const std::vector<int64_t>& hp, const std::vector<int>& hd,
                        const std::vector<int>& patches, std::vector<int>& h_touched, std::vector<int64_t>& h_tptr,
                        std::vector<int64_t>& h_slots);

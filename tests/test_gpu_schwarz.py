@@ -214,21 +214,3 @@ def test_shared_inverses_for_identical_patches(ctx, monkeypatch):
         assert np.array_equal(S1.localInverse(i), S2.localInverse(i))
 
 
-
-def test_split_colour_step_bitwise(ctx, monkeypatch):
-    """Independent colours run as a residual launch over all patch rows of
-    the colour plus a launch applying each shared inverse to a batch of
-    patches; JFEM_SCHWARZ_SPLIT=0 fuses both into one CTA per patch.  The two
-    give the same bits (apply and mvMul)."""
-    sp, sy = fe_system(2, 24)
-    parts = (12, 12)
-    _, patches = cartesian_patch_dofs(sp, parts, 1)
-    cols = nine_colours(parts)
-    S1 = UpFrontSchwarz(dev(sy, ctx), patches, ColoredMultiplicativeSubspaceCorrection(0.9), colours=cols)
-    monkeypatch.setenv("JFEM_SCHWARZ_SPLIT", "0")
-    S0 = UpFrontSchwarz(dev(sy, ctx), patches, ColoredMultiplicativeSubspaceCorrection(0.9), colours=cols)
-    x0 = np.random.default_rng(19).standard_normal(sy.n)
-    assert np.array_equal(S1.apply(x0, sy.rhs), S0.apply(x0, sy.rhs))
-    assert np.array_equal(S1.mvMul(sy.rhs), S0.mvMul(sy.rhs))
-    So = O.Schwarz(coo_oracle(sy), O.SCHWARZ_COLORED, patches, 0.9, colours=cols)
-    close(S1.apply(x0, sy.rhs), So.apply(x0, sy.rhs))
