@@ -376,6 +376,38 @@ k_conv_out(int B, int H, int W, const bf16* __restrict__ h5, const float* __rest
     if (valid && q == 0) y[(size_t)row * W + xx] = s;
 }
 
+// y[p] = sum_t u[t][p + off_t] over the taps whose pixel lies in the image:
+// the output layer after the fused projection (kFwdProj) of the last 32 -> 32
+// layer.  One thread per pixel, one CTA row per image row.
+__global__ void __launch_bounds__(256)
+k_conv_taps(int B, int H, int W, const float* __restrict__ u, float* __restrict__ y)
+{
+    const int row = blockIdx.y, yy = row % H;
+    const int xx = blockIdx.x * 256 + (int)threadIdx.x;
+    if (xx >= W) return;
+    const size_t npx = (size_t)B * H * W;
+    const size_t p = (size_t)row * W + xx;
+    float s = 0.f;
+#pragma unroll
+    for (int dy = -1; dy <= 1; dy++) {
+        const bool okr = yy + dy >= 0 && yy + dy < H;
+#pragma unroll
+        for (int dx = -1; dx <= 1; dx++) {
+            if (!(okr && xx + dx >= 0 && xx + dx < W)) continue;
+            const int t = (dy + 1) * 3 + dx + 1;
+            s += __ldg(u + (size_t)t * npx + p + (ptrdiff_t)dy * W + dx);
+        }
+    }
+    y[p] = s;
+}
+
+// JFEM_CNN_PROJ=0 keeps the separate output layer in inference forwards
+bool cnn_proj_enabled()
+{
+    const char* e = getenv("JFEM_CNN_PROJ");
+    return !(e && e[0] == '0');
+}
+
 // loss = mean (y - t)^2 (FP64 sum), dy = 2 (y - t) / N
 struct VLoss {
     const float* y;
@@ -527,6 +559,9 @@ void conv_mid_tc(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* in, 
                  const __nv_bfloat16* skip, __nv_bfloat16* out, int* err);
 void conv_mid_tc_bwd(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* gin, const __nv_bfloat16* wt,
                      const __nv_bfloat16* mask, const float* skip, float* out, __nv_bfloat16* out16, int* err);
+bool conv_proj_available();
+void conv_mid_tc_proj(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* in, const __nv_bfloat16* wk,
+                      const __nv_bfloat16* skip, const float* w6, float* u, int* err);
 }  // namespace jfg
 
 // ---------------------------------------------------------------------------
@@ -544,6 +579,7 @@ struct jfg_cnn {
     jfg::DevBuf<float> w32, g32, m, v, part;
     jfg::DevBuf<__nv_bfloat16> wk, wt, h1, a2, h3, a4, h5;
     jfg::DevBuf<float> y, dy, gA, gB, gC;
+    jfg::DevBuf<float> u9;                   // nine tap planes of the fused output projection (inference)
     jfg::DevBuf<__nv_bfloat16> gB16, gC16;   // BF16 copies of gB / gC: inputs of the tensor-core input gradients
     jfg::DevBuf<double> loss;
     jfg::DevBuf<double> partials;
@@ -575,6 +611,7 @@ void cnn_reserve(jfg_cnn* n, size_t npx)
     n->gC.alloc(npx * kC);
     n->gB16.alloc(npx * kC);
     n->gC16.alloc(npx * kC);
+    n->u9.alloc(npx * 9);
     n->cap = npx;
 }
 
@@ -625,7 +662,10 @@ bool use_tc()
     return !(e && e[0] == '0');
 }
 
-void cnn_forward(jfg_cnn* n, cudaStream_t st, int B, int H, int W, const float* x, float* y)
+// keep_acts: training forwards keep every activation (h5 included) for the
+// backward pass; inference forwards (keep_acts = false) fuse the output layer
+// into the last tensor-core layer's epilogue (kFwdProj) when available.
+void cnn_forward(jfg_cnn* n, cudaStream_t st, int B, int H, int W, const float* x, float* y, bool keep_acts = true)
 {
     cnn_pack(n, st);
     const bf16* wk = n->wk.p;
@@ -638,6 +678,14 @@ void cnn_forward(jfg_cnn* n, cudaStream_t st, int B, int H, int W, const float* 
         conv_mid_tc(st, B, H, W, n->h1.p, wk + 0 * kMidParams, nullptr, n->a2.p, err);
         conv_mid_tc(st, B, H, W, n->a2.p, wk + 1 * kMidParams, n->h1.p, n->h3.p, err);
         conv_mid_tc(st, B, H, W, n->h3.p, wk + 2 * kMidParams, nullptr, n->a4.p, err);
+        if (!keep_acts && cnn_proj_enabled() && conv_proj_available()) {
+            conv_mid_tc_proj(st, B, H, W, n->a4.p, wk + 3 * kMidParams, n->h3.p, n->w32.p + kLayerOff[5], n->u9.p,
+                             err);
+            k_conv_taps<<<dim3((unsigned)((W + 255) / 256), (unsigned)(B * H)), 256, 0, st>>>(B, H, W, n->u9.p, y);
+            JFG_CUDA(cudaGetLastError());
+            note_launch(2);
+            return;
+        }
         conv_mid_tc(st, B, H, W, n->a4.p, wk + 3 * kMidParams, n->h3.p, n->h5.p, err);
     } else {
         conv_mid<bf16, bf16, 0, true, false>(st, B, H, W, n->h1.p, wk + 0 * kMidParams, nullptr, nullptr, n->a2.p);
@@ -802,7 +850,7 @@ int jfg_cnn_forward_dev(jfg_cnn* n, int B, int H, int W, const float* d_x, float
         JFG_CUDA(cudaSetDevice(jfg::ctx_device(n->ctx)));
         cudaStream_t st = jfg::ctx_stream(n->ctx);
         jfg::cnn_reserve(n, (size_t)B * H * W);
-        jfg::cnn_forward(n, st, B, H, W, d_x, d_y);
+        jfg::cnn_forward(n, st, B, H, W, d_x, d_y, false);
         jfg::cnn_check_tc(n, st);
         return JFG_OK;
     } catch (const jfg::Error& e) {
@@ -868,9 +916,9 @@ int jfg_cnn_time_forward(jfg_cnn* n, int B, int H, int W, int iters, double* ms_
         JFG_CUDA(cudaEventCreate(&e0));
         JFG_CUDA(cudaEventCreate(&e1));
         JFG_CUDA(cudaEventCreate(&e2));
-        jfg::cnn_forward(n, st, B, H, W, x.p, n->y.p);
+        jfg::cnn_forward(n, st, B, H, W, x.p, n->y.p, false);
         JFG_CUDA(cudaEventRecord(e0, st));
-        for (int i = 0; i < iters; i++) jfg::cnn_forward(n, st, B, H, W, x.p, n->y.p);
+        for (int i = 0; i < iters; i++) jfg::cnn_forward(n, st, B, H, W, x.p, n->y.p, false);
         JFG_CUDA(cudaEventRecord(e1, st));
         const bool tc = jfg::use_tc();
         for (int i = 0; i < iters; i++) {
@@ -994,7 +1042,7 @@ void mgcnn_apply(void* self, const double* v, double* z, const Scratch& sc, cons
     p->net->packed = true;
     JFG_CUDA(cudaGetLastError());
     note_launch(2);
-    cnn_forward(p->net, st, 1, p->H, p->W, p->img_in.p, p->img_out.p);
+    cnn_forward(p->net, st, 1, p->H, p->W, p->img_in.p, p->img_out.p, false);
     k_scatter_img<<<(npix + 255) / 256, 256, 0, st>>>(npix, p->dof.p, p->bd.p, p->img_out.p, p->scale.p,
                                                        p->out_scale, z);
     JFG_CUDA(cudaGetLastError());

@@ -93,6 +93,12 @@ __device__ __forceinline__ void tma_plane(uint32_t dst, const CUtensorMap* map, 
 //             copy: the TMA input of the following input-gradient convolution)
 //   kBwdSkip: out(f32) = acc + skip(f32)                     input gradient plus the skip path's
 constexpr int kFwd = 0, kFwdSkip = 1, kBwdMask = 2, kBwdSkip = 3;
+//   kFwdProj: the last 32 -> 32 layer (with skip) fused with the projection of
+//   the 32 -> 1 output layer: h = relu(acc + skip) rounded to BF16 (the values
+//   the output layer would read back), then u[t][p] = sum_c w6[c][t] h[c] for
+//   the nine taps t, written as nine FP32 planes; y = sum_t u[t][p + off_t]
+//   follows in a small kernel.  Warp-specialised kernel only.
+constexpr int kFwdProj = 4;
 
 // The epilogue of one output pixel: its 32 FP32 channel sums r (from TMEM)
 // combined and stored as MODE says; base = the pixel's first channel.
@@ -348,6 +354,34 @@ constexpr int kStageBytes = kHH * kHW * 64;      // 11,520: the halo as 64-byte 
 template <int ST> constexpr int ws_smem() { return kWBytes + ST * (kStageBytes + kHaloBytes) + 128; }
 template <int ST> constexpr int ws_ctas_per_sm() { return 228 * 1024 / (ws_smem<ST>() + 1024) < 8 ? 228 * 1024 / (ws_smem<ST>() + 1024) : 8; }
 
+// kFwdProj epilogue of one pixel (see kFwdProj); w6s is [tap][channel] FP32
+__device__ __forceinline__ void proj_store(const uint32_t (&r)[32], size_t pix, size_t npx,
+                                           const bf16* __restrict__ skip, const float* w6s, float* __restrict__ u)
+{
+    __align__(16) bf16 sv[32];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+        *reinterpret_cast<uint4*>(sv + 8 * q) = __ldg(reinterpret_cast<const uint4*>(skip + pix * 32 + 8 * q));
+    float h[32];
+#pragma unroll
+    for (int c = 0; c < 32; c++)
+        h[c] = __bfloat162float(__float2bfloat16_rn(fmaxf(__uint_as_float(r[c]) + __bfloat162float(sv[c]), 0.f)));
+#pragma unroll
+    for (int t = 0; t < 9; t++) {
+        const float4* w4 = reinterpret_cast<const float4*>(w6s + t * 32);
+        float acc = 0.f;
+#pragma unroll
+        for (int c4 = 0; c4 < 8; c4++) {
+            const float4 w = w4[c4];
+            acc += w.x * h[4 * c4];
+            acc += w.y * h[4 * c4 + 1];
+            acc += w.z * h[4 * c4 + 2];
+            acc += w.w * h[4 * c4 + 3];
+        }
+        u[(size_t)t * npx + pix] = acc;
+    }
+}
+
 __device__ __forceinline__ void mbar_arrive(uint32_t bar)
 {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
@@ -356,7 +390,8 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar)
 template <int MODE, int ST>
 __global__ void __launch_bounds__(kWsThreads)
 k_conv_ws(const __grid_constant__ CUtensorMap tin, int B, int H, int W, const bf16* __restrict__ wk,
-          const void* __restrict__ aux, void* __restrict__ out, bf16* __restrict__ out16, int* __restrict__ err)
+          const void* __restrict__ aux, void* __restrict__ out, bf16* __restrict__ out16, int* __restrict__ err,
+          const float* __restrict__ proj)
 {
     extern __shared__ unsigned char dsm_raw[];
     unsigned char* dsm = reinterpret_cast<unsigned char*>(((uintptr_t)dsm_raw + 127) & ~(uintptr_t)127);
@@ -373,6 +408,9 @@ k_conv_ws(const __grid_constant__ CUtensorMap tin, int B, int H, int W, const bf
         const uint4 v = *reinterpret_cast<const uint4*>(wk + co * 288 + j * 8);
         *reinterpret_cast<uint4*>(wsm + (co >> 3) * kWRowGroup + j * 128 + (co & 7) * 16) = v;
     }
+    __shared__ __align__(16) float w6s[MODE == kFwdProj ? 9 * 32 : 4];    // output-layer weights [tap][channel]
+    if constexpr (MODE == kFwdProj)
+        for (int i = tid; i < 9 * 32; i += kWsThreads) w6s[(i % 9) * 32 + i / 9] = proj[i];
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 64;" ::"r"(smem_u32(&tmem_sh))
                      : "memory");
@@ -520,7 +558,14 @@ k_conv_ws(const __grid_constant__ CUtensorMap tin, int B, int H, int W, const bf
             const int t = tile_of(i);
             const int b = t / per_img, rem = t - b * per_img;
             const int gy = (rem / tilesx) * kTH + (m >> 3), gx = (rem % tilesx) * kTW + (m & 7);
-            if (gy < H && gx < W) conv_store<MODE>(r, (((size_t)b * H + gy) * W + gx) * 32, aux, out, out16);
+            if (gy < H && gx < W) {
+                const size_t pix = ((size_t)b * H + gy) * W + gx;
+                if constexpr (MODE == kFwdProj)
+                    proj_store(r, pix, (size_t)B * H * W, static_cast<const bf16*>(aux), w6s,
+                               static_cast<float*>(out));
+                else
+                    conv_store<MODE>(r, pix * 32, aux, out, out16);
+            }
         }
     }
     __syncthreads();
@@ -600,14 +645,14 @@ static int conv_grid(int B, int H, int W, const void* in)
 
 template <int MODE, int ST>
 static void launch_ws(cudaStream_t st, int grid, const CUtensorMap& map, int B, int H, int W, const bf16* w,
-                      const void* aux, void* out, bf16* out16, int* err)
+                      const void* aux, void* out, bf16* out16, int* err, const float* proj = nullptr)
 {
     static bool attr = false;
     if (!attr) {
         JFG_CUDA(cudaFuncSetAttribute(k_conv_ws<MODE, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, ws_smem<ST>()));
         attr = true;
     }
-    k_conv_ws<MODE, ST><<<grid, kWsThreads, ws_smem<ST>(), st>>>(map, B, H, W, w, aux, out, out16, err);
+    k_conv_ws<MODE, ST><<<grid, kWsThreads, ws_smem<ST>(), st>>>(map, B, H, W, w, aux, out, out16, err, proj);
 }
 
 template <int MODE>
@@ -640,6 +685,29 @@ void conv_mid_tc(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* in, 
         launch_conv<kFwdSkip>(st, grid, map, B, H, W, wk, skip, out, nullptr, err);
     else
         launch_conv<kFwd>(st, grid, map, B, H, W, wk, nullptr, out, nullptr, err);
+}
+
+// The last 32 -> 32 layer with its skip input fused with the projection of
+// the 32 -> 1 output layer (kFwdProj): u receives nine FP32 planes of B*H*W
+// entries, u[t][p] = sum_c w6[c][t] relu(conv + skip)[p][c] (BF16-rounded
+// activations); w6 is FP32 [32 channels][9 taps].  Warp-specialised kernel
+// only (the caller checks conv_proj_available()).
+bool conv_proj_available() { return use_ws(); }
+
+void conv_mid_tc_proj(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* in, const __nv_bfloat16* wk,
+                      const __nv_bfloat16* skip, const float* w6, float* u, int* err)
+{
+    const int grid = conv_grid(B, H, W, in);
+    if (grid <= 0) return;
+    JFG_CHECK(use_ws(), JFG_ERR_UNSUPPORTED, "the fused output projection needs the warp-specialised convolution");
+    const CUtensorMap map = conv_input_map(B, H, W, in, 32);
+    switch (ws_stages()) {
+    case 2: launch_ws<kFwdProj, 2>(st, grid, map, B, H, W, wk, skip, u, nullptr, err, w6); break;
+    case 3: launch_ws<kFwdProj, 3>(st, grid, map, B, H, W, wk, skip, u, nullptr, err, w6); break;
+    default: launch_ws<kFwdProj, 4>(st, grid, map, B, H, W, wk, skip, u, nullptr, err, w6); break;
+    }
+    JFG_CUDA(cudaGetLastError());
+    note_launch();
 }
 
 // Input gradient of a 32 -> 32 layer on the tensor cores: conv3x3 of the

@@ -119,6 +119,7 @@ def test_warp_specialised_conv_equals_single_role(ctx, shape, monkeypatch):
     t = torch.from_numpy(rng.standard_normal(shape).astype(np.float32)).cuda()
     net = LearnedSmoother(ctx, w)
     monkeypatch.setenv("JFEM_CNN_TC", "1")
+    monkeypatch.setenv("JFEM_CNN_PROJ", "0")          # the separate output layer in both
     outs = []
     for ws in ("1", "0"):
         monkeypatch.setenv("JFEM_CNN_WS", ws)
@@ -128,3 +129,22 @@ def test_warp_specialised_conv_equals_single_role(ctx, shape, monkeypatch):
     assert np.all(np.isfinite(outs[0][0]))
     assert np.array_equal(outs[0][0], outs[1][0])
     assert np.array_equal(outs[0][1], outs[1][1])
+
+
+@pytest.mark.parametrize("shape", [(2, 45, 27), (1, 1025, 1025)])
+def test_fused_output_projection(ctx, shape, monkeypatch):
+    """Inference forwards fuse the 32 -> 1 output layer into the last tcgen05
+    layer's epilogue (nine per-pixel tap sums of the BF16 activations, then a
+    nine-tap gather): the same activations, FP32 sums in another order, so the
+    output equals the separate output layer's to FP32 rounding."""
+    rng = np.random.default_rng(14)
+    w = he_init(seed=9, gain_last=1.0)
+    x = torch.from_numpy(rng.standard_normal(shape).astype(np.float32)).cuda()
+    net = LearnedSmoother(ctx, w)
+    monkeypatch.setenv("JFEM_CNN_TC", "1")
+    y_f = net.forward(x).cpu().numpy()
+    monkeypatch.setenv("JFEM_CNN_PROJ", "0")
+    y_s = net.forward(x).cpu().numpy()
+    assert np.all(np.isfinite(y_f))
+    err = np.abs(y_f - y_s).max() / np.abs(y_s).max()
+    assert err < 1e-5, err
