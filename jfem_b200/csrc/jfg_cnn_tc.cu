@@ -584,6 +584,282 @@ k_conv_ws(const __grid_constant__ CUtensorMap tin, int B, int H, int W, const bf
     }
 }
 
+// ---------------------------------------------------------------------------
+// Strip convolution: the activations are the MMA's A operand in TMEM.
+//
+// A work item is a strip of 128 consecutive output pixels of a row (the
+// MMA's M: TMEM lane = x position) over a segment of rows.  Each input row
+// (130 pixels with the x halo) arrives in shared memory by four TMA boxes of
+// 8 channels (the canonical K-major planes of the tiled kernels), and one
+// thread copies it into TMEM three times, shifted by -1, 0, +1 pixels
+// (tcgen05.cp 128x256b: 128 lanes x 16 channels per copy), so that the tap
+// (dy, dx) of output row y reads input row y + dy - 1 at its dx copy.  The 18
+// MMAs of an output row (9 taps x K = 16 twice, N = 32) then read only the
+// weights from shared memory: 1 KB per MMA instead of 4 KB of A plus 1 KB of
+// B.  Rows live in a ring of five TMEM slots (48 columns each: 3 shifts x
+// 16); two 32-column accumulators let the epilogue of row j overlap the MMAs
+// of row j + 1.  The MMAs of every output pixel run in the tiled kernels'
+// order (taps in order, two K halves), so the results are theirs bit for
+// bit.  Roles: warp 0 TMA producer, warp 1 copy + MMA issuer, warps 2-5
+// epilogue (conv_store / proj_store of the tiled kernels).  Every wait is
+// bounded; a timeout sets *err and the CTA drains what it issued.
+// ---------------------------------------------------------------------------
+constexpr int kSW = 128;                         // output pixels of a strip row (M)
+constexpr int kSPx = kSW + 2;                    // input pixels of a row, x halo included
+constexpr int kSPlane = 2176;                    // plane stride: 130 x 16 B rounded up to 128
+constexpr int kSRowBytes = 4 * kSPlane;          // one input row in four 8-channel planes
+constexpr int kSRows = 4;                        // input rows in shared memory
+constexpr int kSSlots = 5;                       // input rows in TMEM
+constexpr int kSSlotCols = 48;                   // TMEM columns of a row: 3 shifts x 16
+constexpr int kSDcol = 256;                      // TMEM column of the two accumulators
+constexpr int kSThreads = 192;
+// one CTA per SM: the request is padded past half of the SM's shared memory,
+// so that no second CTA (which would wait for the 512 TMEM columns) is placed
+constexpr int kStripSmemUsed = kWBytes + kSRows * kSRowBytes + 128;
+constexpr int kStripSmem = kStripSmemUsed > 120 * 1024 ? kStripSmemUsed : 120 * 1024;
+
+struct StripGeo {
+    int B, H, W, nstrips, nsegs, rs;            // rs: output rows per segment
+};
+
+__device__ __forceinline__ void strip_item(const StripGeo& g, int t, int& b, int& sx, int& y0, int& y1)
+{
+    const int per_img = g.nstrips * g.nsegs;
+    b = t / per_img;
+    const int rem = t - b * per_img;
+    sx = rem / g.nsegs;
+    y0 = (rem - sx * g.nsegs) * g.rs;
+    y1 = min(g.H, y0 + g.rs);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kSThreads, 1)
+k_conv_strip(const __grid_constant__ CUtensorMap trow, StripGeo g, const bf16* __restrict__ wk,
+             const void* __restrict__ aux, void* __restrict__ out, bf16* __restrict__ out16, int* __restrict__ err,
+             const float* __restrict__ proj)
+{
+    extern __shared__ unsigned char dsm_raw[];
+    unsigned char* dsm = reinterpret_cast<unsigned char*>(((uintptr_t)dsm_raw + 127) & ~(uintptr_t)127);
+    unsigned char* wsm = dsm;                                  // weights, kWBytes
+    unsigned char* rows = dsm + kWBytes;                       // kSRows input rows
+    __shared__ __align__(8) uint64_t rfull[kSRows], rcp[kSRows], dfull[2], dempty[2];
+    __shared__ uint32_t tmem_sh;
+    __shared__ volatile int s_stop;
+    __shared__ int s_loads, s_copies, s_mmas;                  // progress counts, for the error path
+    __shared__ __align__(16) float w6s[MODE == kFwdProj ? 9 * 32 : 4];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int i = tid; i < 32 * 36; i += kSThreads) {
+        const int co = i / 36, j = i % 36;
+        const uint4 v = *reinterpret_cast<const uint4*>(wk + co * 288 + j * 8);
+        *reinterpret_cast<uint4*>(wsm + (co >> 3) * kWRowGroup + j * 128 + (co & 7) * 16) = v;
+    }
+    if constexpr (MODE == kFwdProj)
+        for (int i = tid; i < 9 * 32; i += kSThreads) w6s[(i % 9) * 32 + i / 9] = proj[i];
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&tmem_sh))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 32) {
+        s_stop = 0;
+        s_loads = 0;
+        s_copies = 0;
+        s_mmas = 0;
+        for (int q = 0; q < kSRows; q++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&rfull[q])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&rcp[q])) : "memory");
+        }
+        for (int q = 0; q < 2; q++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&dfull[q])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(smem_u32(&dempty[q])) : "memory");
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // weights: generic writes, async-proxy reads
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_sh;
+    const uint32_t wbase = smem_u32(wsm);
+    const uint32_t rbase = smem_u32(rows);
+    const int items = g.B * g.nstrips * g.nsegs;
+    const int cnt = (int)blockIdx.x < items ? (items - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+    if (warp == 0) {
+        if (lane == 0) {                               // TMA producer: the input rows of every item in order
+            int q = 0;
+            for (int i = 0; i < cnt && !s_stop; i++) {
+                int b, sx, y0, y1;
+                strip_item(g, (int)blockIdx.x + i * (int)gridDim.x, b, sx, y0, y1);
+                for (int yin = y0 - 1; yin <= y1 && !s_stop; yin++, q++) {
+                    const int sl = q % kSRows;
+                    if (q >= kSRows && !mbar_wait(smem_u32(&rcp[sl]), (uint32_t)((q / kSRows - 1) & 1))) {
+                        s_stop = 1;
+                        break;
+                    }
+                    const uint32_t bar = smem_u32(&rfull[sl]);
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                                 "r"(4 * kSPx * 16)
+                                 : "memory");
+#pragma unroll
+                    for (int c = 0; c < 4; c++)
+                        tma_plane(rbase + sl * kSRowBytes + c * kSPlane, &trow, 8 * c, sx * kSW - 1, yin, b, bar);
+                    s_loads = q + 1;
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            int q = 0;                                 // input rows copied into TMEM (CTA-wide sequence)
+            int j = 0;                                 // output rows issued
+            // input row qq: wait for its TMA boxes, copy it three times shifted
+            // into TMEM slot qq % kSSlots, commit the copies to rcp
+            auto copy_row = [&](int qq) -> bool {
+                const int sl = qq % kSRows;
+                if (!mbar_wait(smem_u32(&rfull[sl]), (uint32_t)((qq / kSRows) & 1))) return false;
+                const uint32_t src = rbase + sl * kSRowBytes;
+                const uint32_t dst = tmem + (uint32_t)((qq % kSSlots) * kSSlotCols);
+#pragma unroll
+                for (int dx = 0; dx < 3; dx++)
+#pragma unroll
+                    for (int kh = 0; kh < 2; kh++) {
+                        const uint64_t sd = umma_desc(src + 2 * kh * kSPlane + dx * 16, kSPlane, 128);
+                        asm volatile("tcgen05.cp.cta_group::1.128x256b [%0], %1;" ::"r"(dst + (uint32_t)(dx * 16 + kh * 8)),
+                                     "l"(sd)
+                                     : "memory");
+                    }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&rcp[sl]))
+                             : "memory");
+                s_copies = qq + 1;
+                return true;
+            };
+            auto copied = [&](int qq) {
+                return mbar_wait(smem_u32(&rcp[qq % kSRows]), (uint32_t)((qq / kSRows) & 1));
+            };
+            for (int i = 0; i < cnt && !s_stop; i++) {
+                int b, sx, y0, y1;
+                strip_item(g, (int)blockIdx.x + i * (int)gridDim.x, b, sx, y0, y1);
+                (void)b;
+                (void)sx;
+                const int q0 = q;                      // sequence number of input row y0 - 1
+                // the previous item's MMAs are complete before its TMEM rows are overwritten
+                if (j > 0 && !mbar_wait(smem_u32(&dfull[(j - 1) & 1]), (uint32_t)(((j - 1) >> 1) & 1))) {
+                    s_stop = 1;
+                    break;
+                }
+                bool ok = copy_row(q0) && copy_row(q0 + 1) && copy_row(q0 + 2);
+                q = q0 + 3;
+                for (int y = y0; ok && y < y1; y++, j++) {
+                    const int a = j & 1, r = y - y0;
+                    // the epilogue has read accumulator a (output row j - 2); with it the
+                    // MMAs of every row up to j - 2 are complete, so input row y - 3's
+                    // TMEM slot is free for input row y + 2
+                    if (j >= 2 && !mbar_wait(smem_u32(&dempty[a]), (uint32_t)(((j >> 1) - 1) & 1))) {
+                        ok = false;
+                        break;
+                    }
+                    if (y + 2 <= y1) {
+                        if (!copy_row(q0 + r + 3)) {
+                            ok = false;
+                            break;
+                        }
+                        q = q0 + r + 4;
+                    }
+                    if (!(copied(q0 + r) && copied(q0 + r + 1) && copied(q0 + r + 2))) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+                    for (int tap = 0; tap < 9; tap++) {
+                        const int dy = tap / 3, dx = tap % 3;
+                        const uint32_t arow = tmem + (uint32_t)(((q0 + r + dy) % kSSlots) * kSSlotCols + dx * 16);
+#pragma unroll
+                        for (int kh = 0; kh < 2; kh++) {
+                            const uint64_t db = umma_desc(wbase + (4 * tap + 2 * kh) * 128, 128, kWRowGroup);
+                            const uint32_t accum = (tap | kh) ? 1u : 0u;
+                            asm volatile(
+                                "{\n\t.reg .pred p;\n\t"
+                                "setp.ne.b32 p, %4, 0;\n\t"
+                                "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}"
+                                ::"r"(tmem + (uint32_t)(kSDcol + a * 32)), "r"(arow + (uint32_t)(kh * 8)), "l"(db),
+                                  "r"(kIdesc), "r"(accum)
+                                : "memory");
+                        }
+                    }
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                     smem_u32(&dfull[a]))
+                                 : "memory");
+                    s_mmas = j + 1;
+                }
+                if (!ok) {
+                    s_stop = 1;
+                    break;
+                }
+            }
+        }
+    } else {
+        const int lg = warp & 3;                       // TMEM lane group of this warp
+        int j = 0;
+        bool ok = true;
+        for (int i = 0; ok && i < cnt; i++) {
+            int b, sx, y0, y1;
+            strip_item(g, (int)blockIdx.x + i * (int)gridDim.x, b, sx, y0, y1);
+            for (int y = y0; y < y1; y++, j++) {
+                const int a = j & 1;
+                ok = !s_stop && mbar_wait(smem_u32(&dfull[a]), (uint32_t)((j >> 1) & 1));
+                if (!__all_sync(0xffffffffu, ok)) {
+                    if (lane == 0) s_stop = 1;
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                uint32_t r[32];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                    "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                    "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                      "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                      "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                      "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                    : "r"(tmem + ((uint32_t)(lg * 32) << 16) + (uint32_t)(kSDcol + a * 32))
+                    : "memory");
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) mbar_arrive(smem_u32(&dempty[a]));
+                const int x = sx * kSW + lg * 32 + lane;
+                if (x < g.W) {
+                    const size_t pix = ((size_t)b * g.H + y) * g.W + x;
+                    if constexpr (MODE == kFwdProj)
+                        proj_store(r, pix, (size_t)g.B * g.H * g.W, static_cast<const bf16*>(aux), w6s,
+                                   static_cast<float*>(out));
+                    else
+                        conv_store<MODE>(r, pix * 32, aux, out, out16);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (s_stop && tid == 32) {
+        // report, then let the loads, copies and MMAs still in flight finish (bounded) before TMEM is freed
+        atomicOr(err, 1);
+        const int nl = s_loads, nc = s_copies, nm = s_mmas;
+        for (int k = nc; k < nl; k++) mbar_wait(smem_u32(&rfull[k % kSRows]), (uint32_t)((k / kSRows) & 1));
+        if (nc > 0) mbar_wait(smem_u32(&rcp[(nc - 1) % kSRows]), (uint32_t)(((nc - 1) / kSRows) & 1));
+        if (nm > 0) mbar_wait(smem_u32(&dfull[(nm - 1) & 1]), (uint32_t)(((nm - 1) >> 1) & 1));
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+    }
+}
+
 }  // namespace
 
 // The driver's tensor-map encoder, fetched once through the runtime (no link
@@ -615,6 +891,70 @@ static CUtensorMap conv_input_map(int B, int H, int W, const __nv_bfloat16* in, 
                                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     JFG_CHECK(r == CUDA_SUCCESS, JFG_ERR_CUDA, "cuTensorMapEncodeTiled failed");
     return map;
+}
+
+// One input row of a strip: box of 8 channels x 130 pixels x 1 row (zero fill
+// outside the image: the x halo at the image edges and rows -1 and H).
+static CUtensorMap conv_row_map(int B, int H, int W, const __nv_bfloat16* in)
+{
+    CUtensorMap map;
+    const cuuint64_t dims[4] = {32, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
+    const cuuint64_t strides[3] = {64, (cuuint64_t)W * 64, (cuuint64_t)W * H * 64};
+    const cuuint32_t box[4] = {8, (cuuint32_t)kSPx, 1, 1};
+    const cuuint32_t estride[4] = {1, 1, 1, 1};
+    CUresult r = tensor_map_encoder()(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(in), dims,
+                                      strides, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    JFG_CHECK(r == CUDA_SUCCESS, JFG_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    return map;
+}
+
+// JFEM_CNN_STRIP=1 selects the strip kernel (k_conv_strip, activations in
+// TMEM) for the 32 -> 32 layers
+static bool use_strip()
+{
+    const char* e = getenv("JFEM_CNN_STRIP");
+    return e && e[0] == '1';
+}
+
+// Strip geometry: strips of 128 pixels, segments of rows sized so that the
+// items fill the SMs (one CTA per SM) in whole rounds: at most two items per
+// CTA when the image allows.
+static StripGeo strip_geo(int B, int H, int W)
+{
+    StripGeo g;
+    g.B = B;
+    g.H = H;
+    g.W = W;
+    g.nstrips = (W + kSW - 1) / kSW;
+    const int slots = 2 * sm_count();
+    int nsegs = std::max(1, slots / std::max(1, B * g.nstrips));
+    nsegs = std::min(nsegs, H);
+    g.rs = (H + nsegs - 1) / nsegs;
+    g.nsegs = (H + g.rs - 1) / g.rs;
+    return g;
+}
+
+template <int MODE>
+static void launch_strip(cudaStream_t st, int B, int H, int W, const bf16* in, const bf16* w, const void* aux,
+                         void* out, bf16* out16, int* err, const float* proj = nullptr)
+{
+    JFG_CHECK(((uintptr_t)in & 15) == 0, JFG_ERR_BAD_ARG, "convolution input not 16-byte aligned");
+    const StripGeo g = strip_geo(B, H, W);
+    const long long items = (long long)B * g.nstrips * g.nsegs;
+    JFG_CHECK(items < (1LL << 31), JFG_ERR_UNSUPPORTED, "image too large for the strip convolution");
+    const int grid = (int)std::min<long long>(items, sm_count());
+    if (grid <= 0) return;
+    static bool attr = false;
+    if (!attr) {
+        JFG_CUDA(cudaFuncSetAttribute(k_conv_strip<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, kStripSmem));
+        attr = true;
+    }
+    const CUtensorMap map = conv_row_map(B, H, W, in);
+    k_conv_strip<MODE><<<grid, kSThreads, kStripSmem, st>>>(map, g, w, aux, out, out16, err, proj);
+    JFG_CUDA(cudaGetLastError());
+    note_launch();
 }
 
 // JFEM_CNN_WS=0 selects the single-role kernel (k_conv_mid_tc) instead of the
@@ -678,6 +1018,13 @@ static void launch_conv(cudaStream_t st, int grid, const CUtensorMap& map, int B
 void conv_mid_tc(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* in, const __nv_bfloat16* wk,
                  const __nv_bfloat16* skip, __nv_bfloat16* out, int* err)
 {
+    if (use_strip()) {
+        if (skip)
+            launch_strip<kFwdSkip>(st, B, H, W, in, wk, skip, out, nullptr, err);
+        else
+            launch_strip<kFwd>(st, B, H, W, in, wk, nullptr, out, nullptr, err);
+        return;
+    }
     const int grid = conv_grid(B, H, W, in);
     if (grid <= 0) return;
     const CUtensorMap map = conv_input_map(B, H, W, in, use_ws() ? 32 : 8);
@@ -692,11 +1039,15 @@ void conv_mid_tc(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* in, 
 // entries, u[t][p] = sum_c w6[c][t] relu(conv + skip)[p][c] (BF16-rounded
 // activations); w6 is FP32 [32 channels][9 taps].  Warp-specialised kernel
 // only (the caller checks conv_proj_available()).
-bool conv_proj_available() { return use_ws(); }
+bool conv_proj_available() { return use_strip() || use_ws(); }
 
 void conv_mid_tc_proj(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* in, const __nv_bfloat16* wk,
                       const __nv_bfloat16* skip, const float* w6, float* u, int* err)
 {
+    if (use_strip()) {
+        launch_strip<kFwdProj>(st, B, H, W, in, wk, skip, u, nullptr, err, w6);
+        return;
+    }
     const int grid = conv_grid(B, H, W, in);
     if (grid <= 0) return;
     JFG_CHECK(use_ws(), JFG_ERR_UNSUPPORTED, "the fused output projection needs the warp-specialised convolution");
@@ -717,6 +1068,13 @@ void conv_mid_tc_proj(cudaStream_t st, int B, int H, int W, const __nv_bfloat16*
 void conv_mid_tc_bwd(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* gin, const __nv_bfloat16* wt,
                      const __nv_bfloat16* mask, const float* skip, float* out, __nv_bfloat16* out16, int* err)
 {
+    if (use_strip()) {
+        if (mask)
+            launch_strip<kBwdMask>(st, B, H, W, gin, wt, mask, out, out16, err);
+        else
+            launch_strip<kBwdSkip>(st, B, H, W, gin, wt, skip, out, nullptr, err);
+        return;
+    }
     const int grid = conv_grid(B, H, W, gin);
     if (grid <= 0) return;
     const CUtensorMap map = conv_input_map(B, H, W, gin, use_ws() ? 32 : 8);
