@@ -596,9 +596,9 @@ k_conv_ws(const __grid_constant__ CUtensorMap tin, int B, int H, int W, const bf
 // (dy, dx) of output row y reads input row y + dy - 1 at its dx copy.  The 18
 // MMAs of an output row (9 taps x K = 16 twice, N = 32) then read only the
 // weights from shared memory: 1 KB per MMA instead of 4 KB of A plus 1 KB of
-// B.  Rows live in a ring of five TMEM slots (48 columns each: 3 shifts x
+// B.  Rows live in a ring of four TMEM slots (48 columns each: 3 shifts x
 // 16); two 32-column accumulators let the epilogue of row j overlap the MMAs
-// of row j + 1.  The MMAs of every output pixel run in the tiled kernels'
+// of row j + 1; 256 TMEM columns per CTA, two CTAs per SM.  The MMAs of every output pixel run in the tiled kernels'
 // order (taps in order, two K halves), so the results are theirs bit for
 // bit.  Roles: warp 0 TMA producer, warp 1 copy + MMA issuer, warps 2-5
 // epilogue (conv_store / proj_store of the tiled kernels).  Every wait is
@@ -608,15 +608,18 @@ constexpr int kSW = 128;                         // output pixels of a strip row
 constexpr int kSPx = kSW + 2;                    // input pixels of a row, x halo included
 constexpr int kSPlane = 2176;                    // plane stride: 130 x 16 B rounded up to 128
 constexpr int kSRowBytes = 4 * kSPlane;          // one input row in four 8-channel planes
-constexpr int kSRows = 4;                        // input rows in shared memory
-constexpr int kSSlots = 5;                       // input rows in TMEM
+constexpr int kSRows = 6;                        // input rows in shared memory
+constexpr int kSSlots = 4;                       // input rows in TMEM
 constexpr int kSSlotCols = 48;                   // TMEM columns of a row: 3 shifts x 16
-constexpr int kSDcol = 256;                      // TMEM column of the two accumulators
+constexpr int kSDcol = kSSlots * kSSlotCols;     // TMEM column of the two accumulators (192)
+constexpr int kSTmemCols = 256;
+constexpr int kSCtasPerSm = 2;
 constexpr int kSThreads = 192;
-// one CTA per SM: the request is padded past half of the SM's shared memory,
-// so that no second CTA (which would wait for the 512 TMEM columns) is placed
+// two CTAs per SM (256 TMEM columns each): the request is padded past a third
+// of the SM's shared memory, so that no third CTA (which would wait for TMEM)
+// is placed
 constexpr int kStripSmemUsed = kWBytes + kSRows * kSRowBytes + 128;
-constexpr int kStripSmem = kStripSmemUsed > 120 * 1024 ? kStripSmemUsed : 120 * 1024;
+constexpr int kStripSmem = kStripSmemUsed > 80 * 1024 ? kStripSmemUsed : 80 * 1024;
 
 struct StripGeo {
     int B, H, W, nstrips, nsegs, rs;            // rs: output rows per segment
@@ -633,7 +636,7 @@ __device__ __forceinline__ void strip_item(const StripGeo& g, int t, int& b, int
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kSThreads, 1)
+__global__ void __launch_bounds__(kSThreads, kSCtasPerSm)
 k_conv_strip(const __grid_constant__ CUtensorMap trow, StripGeo g, const bf16* __restrict__ wk,
              const void* __restrict__ aux, void* __restrict__ out, bf16* __restrict__ out16, int* __restrict__ err,
              const float* __restrict__ proj)
@@ -656,7 +659,8 @@ k_conv_strip(const __grid_constant__ CUtensorMap trow, StripGeo g, const bf16* _
     if constexpr (MODE == kFwdProj)
         for (int i = tid; i < 9 * 32; i += kSThreads) w6s[(i % 9) * 32 + i / 9] = proj[i];
     if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&tmem_sh))
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_sh)),
+                     "n"(kSTmemCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -752,19 +756,10 @@ k_conv_strip(const __grid_constant__ CUtensorMap trow, StripGeo g, const bf16* _
                 q = q0 + 3;
                 for (int y = y0; ok && y < y1; y++, j++) {
                     const int a = j & 1, r = y - y0;
-                    // the epilogue has read accumulator a (output row j - 2); with it the
-                    // MMAs of every row up to j - 2 are complete, so input row y - 3's
-                    // TMEM slot is free for input row y + 2
+                    // the epilogue has read accumulator a (output row j - 2)
                     if (j >= 2 && !mbar_wait(smem_u32(&dempty[a]), (uint32_t)(((j >> 1) - 1) & 1))) {
                         ok = false;
                         break;
-                    }
-                    if (y + 2 <= y1) {
-                        if (!copy_row(q0 + r + 3)) {
-                            ok = false;
-                            break;
-                        }
-                        q = q0 + r + 4;
                     }
                     if (!(copied(q0 + r) && copied(q0 + r + 1) && copied(q0 + r + 2))) {
                         ok = false;
@@ -792,6 +787,20 @@ k_conv_strip(const __grid_constant__ CUtensorMap trow, StripGeo g, const bf16* _
                                      smem_u32(&dfull[a]))
                                  : "memory");
                     s_mmas = j + 1;
+                    // input row y + 2 goes into the slot of input row y - 2, which
+                    // output row j - 1 reads last: wait for that row's MMAs (row j's
+                    // are queued behind them), then copy
+                    if (y + 2 <= y1) {
+                        if (j >= 1 && !mbar_wait(smem_u32(&dfull[(j - 1) & 1]), (uint32_t)(((j - 1) >> 1) & 1))) {
+                            ok = false;
+                            break;
+                        }
+                        if (!copy_row(q0 + r + 3)) {
+                            ok = false;
+                            break;
+                        }
+                        q = q0 + r + 4;
+                    }
                 }
                 if (!ok) {
                     s_stop = 1;
@@ -856,7 +865,7 @@ k_conv_strip(const __grid_constant__ CUtensorMap trow, StripGeo g, const bf16* _
     __syncthreads();
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(kSTmemCols) : "memory");
     }
 }
 
@@ -944,7 +953,7 @@ static void launch_strip(cudaStream_t st, int B, int H, int W, const bf16* in, c
     const StripGeo g = strip_geo(B, H, W);
     const long long items = (long long)B * g.nstrips * g.nsegs;
     JFG_CHECK(items < (1LL << 31), JFG_ERR_UNSUPPORTED, "image too large for the strip convolution");
-    const int grid = (int)std::min<long long>(items, sm_count());
+    const int grid = (int)std::min<long long>(items, (long long)kSCtasPerSm * sm_count());
     if (grid <= 0) return;
     static bool attr = false;
     if (!attr) {
