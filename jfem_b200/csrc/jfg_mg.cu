@@ -68,6 +68,26 @@ __global__ void k_bc_defect(int naff, const int* __restrict__ row, const int* __
     d[r] = v[r] - s;
 }
 
+// k_bc_defect, and the first Jacobi sweep from zero of those rows:
+// y[r] = (dinv[r] * d[r]) * omega (the rest of y written by VCopyScaleMul)
+template <typename T>
+__global__ void k_bc_defect_scale(int naff, const int* __restrict__ row, const int* __restrict__ ptr,
+                                  const int* __restrict__ col, const T* __restrict__ val, const T* __restrict__ v,
+                                  T* __restrict__ d, const T* __restrict__ dinv, T* __restrict__ y, T omega,
+                                  const int* __restrict__ done)
+{
+    pdl_wait();
+    if (done && *done) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= naff) return;
+    int r = row[i];
+    T s = 0;
+    for (int k = ptr[i]; k < ptr[i + 1]; k++) s += val[k] * v[col[k]];
+    const T dr = v[r] - s;
+    d[r] = dr;
+    y[r] = (T)0 + (dinv[r] * dr) * omega;
+}
+
 // out[bd] += v[bd]   (initial.add(iterate), initial = boundary copy of v)
 template <typename T>
 __global__ void k_bc_add(int nb, const int* __restrict__ bd, const T* __restrict__ v, T* __restrict__ out,
@@ -512,7 +532,10 @@ void MGImpl<T>::init(Context* ctx, int levels, Matrix* const* As, Matrix* const*
         JFG_CUDA(cudaMemcpyAsync(hv.data(), Af->csr_val.p, sizeof(double) * Af->nnz, cudaMemcpyDeviceToHost, st));
         JFG_CUDA(cudaStreamSynchronize(st));
         std::vector<char> isbd(Af->rows, 0);
-        for (int i = 0; i < nbd_fine; i++) isbd[bdry[Lf][i]] = 1;
+        for (int i = 0; i < nbd_fine; i++) {
+            if (isbd[bdry[Lf][i]]) bd_unique = false;
+            isbd[bdry[Lf][i]] = 1;
+        }
         std::vector<int> arow, aptr{0}, acol;
         std::vector<T> aval;
         for (int rr = 0; rr < Af->rows; rr++) {
@@ -807,7 +830,13 @@ void MGImpl<T>::smooth(int l, const T* rhs, bool xzero, const Scratch& sc, const
         T* alt = t[l].p;
         for (int k = 0; k < d.runs; k++) {
             T* o = (k == d.runs - 1) ? dest : alt;
-            mg_spmv<T, 0>(*this, st, M, cur, EpiJacobi<T>{cur, rhs, dinv[l].p, o, om}, sc, done);
+            if (k == d.runs - 1 && bc_src && l == L - 1) {
+                mg_spmv<T, 0>(*this, st, M, cur, EpiJacobiBc<T>{cur, rhs, dinv[l].p, o, om, mask[l].p, bc_src}, sc,
+                              done);
+                bc_done = true;
+            } else {
+                mg_spmv<T, 0>(*this, st, M, cur, EpiJacobi<T>{cur, rhs, dinv[l].p, o, om}, sc, done);
+            }
             alt = cur;
             cur = o;
         }
@@ -985,11 +1014,28 @@ void MGImpl<T>::apply(const T* v, T* out, const Scratch& sc, const int* done, cu
 {
     int Lf = L - 1, m = n[Lf];
     T* defect = b[Lf].p;
-    vec_launch<0>(st, m, VCopy<T>{v, defect}, sc, done);
-    if (naff) {
-        launch_ex(k_bc_defect<T>, dim3(nb(naff)), dim3(256), 0, st, naff, (const int*)aff_row.p,
-                  (const int*)aff_ptr.p, (const int*)aff_col.p, (const T*)aff_val.p, v, defect, done);
+    // the defect copy fused with the finest level's first Jacobi sweep from zero
+    // (a plain V-cycle whose finest level is not the cluster tail)
+    const bool fuse_first = !use_fmg && !wcycle && L > 1 && cycles >= 1 && tail != Lf &&
+                            sm[Lf].kind == JFG_SMOOTH_JACOBI && sm[Lf].runs >= 1;
+    if (fuse_first) {
+        const T om = (T)sm[Lf].omega;
+        T* dst0 = (sm[Lf].runs % 2 == 1) ? x[Lf].p : t[Lf].p;
+        vec_launch<0>(st, m, VCopyScaleMul<T>{v, defect, dinv[Lf].p, dst0, om}, sc, done);
+        if (naff)
+            launch_ex(k_bc_defect_scale<T>, dim3(nb(naff)), dim3(256), 0, st, naff, (const int*)aff_row.p,
+                      (const int*)aff_ptr.p, (const int*)aff_col.p, (const T*)aff_val.p, v, defect,
+                      (const T*)dinv[Lf].p, dst0, om, done);
+    } else {
+        vec_launch<0>(st, m, VCopy<T>{v, defect}, sc, done);
+        if (naff) {
+            launch_ex(k_bc_defect<T>, dim3(nb(naff)), dim3(256), 0, st, naff, (const int*)aff_row.p,
+                      (const int*)aff_ptr.p, (const int*)aff_col.p, (const T*)aff_val.p, v, defect, done);
+        }
     }
+    // the boundary add folded into the last post-smoothing sweep when it writes out
+    bc_src = (nbd_fine && bd_unique) ? v : nullptr;
+    bc_done = false;
     bool xzero = true;
     if (use_fmg && L > 1) {
         fmg_into_top(defect, sc, done, st);
@@ -1004,18 +1050,24 @@ void MGImpl<T>::apply(const T* v, T* out, const Scratch& sc, const int* done, cu
     } else {
         // the last cycle's post-smoothing writes the result straight into out
         for (int cyc = 0; cyc < cycles; cyc++) {
+            // only the last cycle's post-smoothing writes out (bc_src applies there)
+            const T* keep = bc_src;
+            if (cyc != cycles - 1) bc_src = nullptr;
             if (wcycle)
                 wstep(Lf, defect, xzero, sc, done, st, cyc == cycles - 1 ? out : nullptr);
             else
-                vstep(Lf, defect, xzero, sc, done, st, false, cyc == cycles - 1 ? out : nullptr);
+                vstep(Lf, defect, xzero, sc, done, st, fuse_first && cyc == 0, cyc == cycles - 1 ? out : nullptr);
+            bc_src = keep;
             xzero = false;
         }
         if (xzero) vec_launch<0>(st, m, VZero<T>{x[Lf].p}, sc, done);
     }
     if (L == 1 || cycles == 0) vec_launch<0>(st, m, VCopy<T>{x[Lf].p, out}, sc, done);
-    if (nbd_fine) {
+    if (nbd_fine && !bc_done) {
         launch_ex(k_bc_add<T>, dim3(nb(nbd_fine)), dim3(256), 0, st, nbd_fine, (const int*)bd_fine.p, v, out, done);
     }
+    bc_src = nullptr;
+    bc_done = false;
 }
 
 template <typename T>

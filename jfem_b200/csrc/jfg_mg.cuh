@@ -51,6 +51,11 @@ struct MGImpl {
     // rows that have entries in boundary columns; those rows are kept as CSR.
     DevBuf<int> bd_fine;
     int nbd_fine = 0;
+    bool bd_unique = true;              // the finest boundary list names no unknown twice
+    // apply(): the last post-smoothing sweep adds bc_src at the finest boundary
+    // (instead of a separate k_bc_add launch); bc_done reports that it did
+    const T* bc_src = nullptr;
+    bool bc_done = false;
     DevBuf<int> aff_row, aff_ptr, aff_col;
     DevBuf<T> aff_val;
     int naff = 0;

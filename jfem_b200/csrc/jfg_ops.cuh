@@ -90,6 +90,23 @@ struct EpiJacobi {  // xn = x + (dinv * (b - A x)) * omega   (JacobiSmoother.jav
 };
 
 template <typename T>
+struct EpiJacobiBc {  // EpiJacobi, then xn += v on the boundary rows (the MG mvMul's initial.add(iterate))
+    const T* x;
+    const T* b;
+    const T* dinv;
+    T* xn;
+    T omega;
+    const unsigned char* mask;
+    const T* v;
+    template <typename AT, int K>
+    __device__ void operator()(int r, AT s, double (&)[K]) const
+    {
+        const T o = x[r] + (dinv[r] * (b[r] - (T)s)) * omega;
+        xn[r] = mask[r] ? v[r] + o : o;
+    }
+};
+
+template <typename T>
 struct EpiMasked {  // y = mask ? 0 : A x  (transfer followed by zero boundary values)
     const unsigned char* mask;
     T* y;
@@ -280,6 +297,20 @@ struct VScaleMul {  // y = (dinv * b) * omega      (first Jacobi sweep from a ze
     T* y;
     T omega;
     template <int K> __device__ void operator()(int i, double (&)[K]) const { y[i] = (T)0 + (dinv[i] * b[i]) * omega; }
+};
+template <typename T>
+struct VCopyScaleMul {  // d = v and y = (dinv * v) * omega: the defect copy fused with the first sweep from zero
+    const T* v;
+    T* d;
+    const T* dinv;
+    T* y;
+    T omega;
+    template <int K> __device__ void operator()(int i, double (&)[K]) const
+    {
+        const T vi = v[i];
+        d[i] = vi;
+        y[i] = (T)0 + (dinv[i] * vi) * omega;
+    }
 };
 template <typename A, typename B>
 struct VCast {  // b = (B) a
