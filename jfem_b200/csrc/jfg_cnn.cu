@@ -295,47 +295,69 @@ constexpr int kLanesPerPx = 4;
 constexpr int kEdgePx = 256 / kLanesPerPx;        // pixels of one CTA (64 along x)
 
 // first layer 1 -> 32 with ReLU: h1[p][co] = relu(sum_tap w1[co][tap] x[p + tap]),
-// each output's taps summed in order
+// each output's taps summed in order.  A thread keeps the 72 weights of its
+// eight channels in registers and walks kInRows rows down one column with a
+// sliding 3 x 3 input window (three new inputs per row), so the weights are
+// read from shared memory once per kInRows pixels.
+constexpr int kInRows = 8;
+
 __global__ void __launch_bounds__(256)
 k_conv_in(int B, int H, int W, const float* __restrict__ x, const float* __restrict__ w1, bf16* __restrict__ h1)
 {
     __shared__ __align__(16) float ws[9 * kC];
     for (int i = threadIdx.x; i < kC * 9; i += blockDim.x) ws[(i % 9) * kC + i / 9] = w1[i];
     __syncthreads();
-    const int row = blockIdx.y, yy = row % H;
     const int xx = blockIdx.x * kEdgePx + (int)threadIdx.x / kLanesPerPx, q = threadIdx.x % kLanesPerPx;
+    const int ry = (H + kInRows - 1) / kInRows;
+    const int bb = blockIdx.y / ry, y0 = (blockIdx.y - bb * ry) * kInRows;
     if (xx >= W) return;
-    const float* xr = x + (size_t)row * W;
-    float in9[9];
-#pragma unroll
-    for (int dy = -1; dy <= 1; dy++) {
-        const bool okr = yy + dy >= 0 && yy + dy < H;
-#pragma unroll
-        for (int dx = -1; dx <= 1; dx++) {
-            const bool ok = okr && xx + dx >= 0 && xx + dx < W;
-            in9[(dy + 1) * 3 + dx + 1] = ok ? __ldg(xr + (ptrdiff_t)dy * W + xx + dx) : 0.f;
-        }
-    }
-    float s[8];
-#pragma unroll
-    for (int c = 0; c < 8; c++) s[c] = 0.f;
+    float w[9][8];
 #pragma unroll
     for (int tap = 0; tap < 9; tap++) {
         const float4* w4 = reinterpret_cast<const float4*>(ws + tap * kC + 8 * q);
         const float4 wa = w4[0], wb = w4[1];
-        s[0] += wa.x * in9[tap];
-        s[1] += wa.y * in9[tap];
-        s[2] += wa.z * in9[tap];
-        s[3] += wa.w * in9[tap];
-        s[4] += wb.x * in9[tap];
-        s[5] += wb.y * in9[tap];
-        s[6] += wb.z * in9[tap];
-        s[7] += wb.w * in9[tap];
+        w[tap][0] = wa.x;
+        w[tap][1] = wa.y;
+        w[tap][2] = wa.z;
+        w[tap][3] = wa.w;
+        w[tap][4] = wb.x;
+        w[tap][5] = wb.y;
+        w[tap][6] = wb.z;
+        w[tap][7] = wb.w;
     }
-    __align__(16) bf16 o[8];
+    const float* xb = x + (size_t)bb * H * W;
+    auto row3 = [&](int yy, float (&v)[3]) {
+        const bool okr = yy >= 0 && yy < H;
 #pragma unroll
-    for (int c = 0; c < 8; c++) o[c] = __float2bfloat16_rn(fmaxf(s[c], 0.f));
-    *reinterpret_cast<uint4*>(h1 + ((size_t)row * W + xx) * kC + 8 * q) = *reinterpret_cast<const uint4*>(o);
+        for (int dx = -1; dx <= 1; dx++)
+            v[dx + 1] = okr && xx + dx >= 0 && xx + dx < W ? __ldg(xb + (size_t)yy * W + xx + dx) : 0.f;
+    };
+    float win[3][3];
+    row3(y0 - 1, win[0]);
+    row3(y0, win[1]);
+    const int y1 = min(H, y0 + kInRows);
+    for (int yy = y0; yy < y1; yy++) {
+        row3(yy + 1, win[2]);
+        float s[8];
+#pragma unroll
+        for (int c = 0; c < 8; c++) s[c] = 0.f;
+#pragma unroll
+        for (int tap = 0; tap < 9; tap++) {
+            const float in = win[tap / 3][tap % 3];
+#pragma unroll
+            for (int c = 0; c < 8; c++) s[c] += w[tap][c] * in;
+        }
+        __align__(16) bf16 o[8];
+#pragma unroll
+        for (int c = 0; c < 8; c++) o[c] = __float2bfloat16_rn(fmaxf(s[c], 0.f));
+        *reinterpret_cast<uint4*>(h1 + (((size_t)bb * H + yy) * W + xx) * kC + 8 * q) =
+            *reinterpret_cast<const uint4*>(o);
+#pragma unroll
+        for (int e = 0; e < 3; e++) {
+            win[0][e] = win[1][e];
+            win[1][e] = win[2][e];
+        }
+    }
 }
 
 // last layer 32 -> 1: y = sum_tap sum_ci w6[ci][tap] h5[p + tap][ci]; lane q
@@ -671,7 +693,8 @@ void cnn_forward(jfg_cnn* n, cudaStream_t st, int B, int H, int W, const float* 
     const bf16* wk = n->wk.p;
     JFG_CHECK((size_t)B * H < 65536, JFG_ERR_UNSUPPORTED, "image batch too large (B * H >= 65536 rows)");
     const dim3 edge_grid((unsigned)((W + kEdgePx - 1) / kEdgePx), (unsigned)(B * H));
-    k_conv_in<<<edge_grid, 256, 0, st>>>(B, H, W, x, n->w32.p + kLayerOff[0], n->h1.p);
+    const dim3 in_grid((unsigned)((W + kEdgePx - 1) / kEdgePx), (unsigned)(B * ((H + kInRows - 1) / kInRows)));
+    k_conv_in<<<in_grid, 256, 0, st>>>(B, H, W, x, n->w32.p + kLayerOff[0], n->h1.p);
     JFG_CUDA(cudaGetLastError());
     if (use_tc()) {
         int* err = n->tc_err.p;
