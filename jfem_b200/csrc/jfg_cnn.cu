@@ -584,6 +584,8 @@ void conv_mid_tc_bwd(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* 
 bool conv_proj_available();
 void conv_mid_tc_proj(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* in, const __nv_bfloat16* wk,
                       const __nv_bfloat16* skip, const float* w6, float* u, int* err);
+int wgrad_mid_tc(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* G16, const __nv_bfloat16* X,
+                 float* part, int max_parts, int* err);
 }  // namespace jfg
 
 // ---------------------------------------------------------------------------
@@ -666,11 +668,29 @@ void conv_mid(cudaStream_t st, int B, int H, int W, const InT* in, const bf16* w
     note_launch();
 }
 
-void wgrad_mid(jfg_cnn* n, cudaStream_t st, int B, int H, int W, const float* G, const bf16* X, float* dw)
+bool use_tc();
+
+// JFEM_CNN_WGRAD_TC=0 keeps the weight gradients on the mma.sync kernel
+// when the tensor-core path is on
+bool wgrad_tc_enabled()
 {
-    int ntiles = ((W + kTile - 1) / kTile) * ((H + kTile - 1) / kTile) * B;
-    int ctas = std::min(ntiles, kMidWgradCtas);
-    k_wgrad_mid<<<ctas, 288, 0, st>>>(B, H, W, G, X, n->part.p);
+    const char* e = getenv("JFEM_CNN_WGRAD_TC");
+    return !(e && e[0] == '0');
+}
+
+// G16: the BF16 copy of G (the tensor-core path reads it; the mma.sync kernel
+// rounds G to BF16 itself, so both contract the same values)
+void wgrad_mid(jfg_cnn* n, cudaStream_t st, int B, int H, int W, const float* G, const bf16* G16, const bf16* X,
+               float* dw)
+{
+    int ctas;
+    if (G16 && use_tc() && wgrad_tc_enabled()) {
+        ctas = wgrad_mid_tc(st, B, H, W, G16, X, n->part.p, kMidWgradCtas, n->tc_err.p);
+    } else {
+        int ntiles = ((W + kTile - 1) / kTile) * ((H + kTile - 1) / kTile) * B;
+        ctas = std::min(ntiles, kMidWgradCtas);
+        k_wgrad_mid<<<ctas, 288, 0, st>>>(B, H, W, G, X, n->part.p);
+    }
     k_wgrad_mid_reduce<<<(kMidParams + 255) / 256, 256, 0, st>>>(ctas, n->part.p, dw);
     JFG_CUDA(cudaGetLastError());
     note_launch(2);
@@ -744,26 +764,26 @@ void cnn_backward(jfg_cnn* n, cudaStream_t st, int B, int H, int W, const float*
     int* err = n->tc_err.p;
     k_relu_mask<<<grid1d(npx * kC), 256, 0, st>>>(npx * kC, n->gA.p, n->h5.p, n->gB.p, gB16);      // g5
     JFG_CUDA(cudaGetLastError());
-    wgrad_mid(n, st, B, H, W, n->gB.p, n->a4.p, g + kLayerOff[4]);                                  // dW5
+    wgrad_mid(n, st, B, H, W, n->gB.p, gB16, n->a4.p, g + kLayerOff[4]);                            // dW5
     if (tc)
         conv_mid_tc_bwd(st, B, H, W, gB16, wt + 3 * kMidParams, n->a4.p, nullptr, n->gC.p, n->gC16.p, err);
     else
         conv_mid<float, float, 0, false, true>(st, B, H, W, n->gB.p, wt + 3 * kMidParams, nullptr, n->a4.p,
                                                n->gC.p);                                            // g4
-    wgrad_mid(n, st, B, H, W, n->gC.p, n->h3.p, g + kLayerOff[3]);                                  // dW4
+    wgrad_mid(n, st, B, H, W, n->gC.p, tc ? n->gC16.p : nullptr, n->h3.p, g + kLayerOff[3]);     // dW4
     if (tc)
         conv_mid_tc_bwd(st, B, H, W, n->gC16.p, wt + 2 * kMidParams, nullptr, n->gB.p, n->gA.p, nullptr, err);
     else
         conv_mid<float, float, 2, false, false>(st, B, H, W, n->gC.p, wt + 2 * kMidParams, n->gB.p, nullptr,
                                                 n->gA.p);                                           // dh3
     k_relu_mask<<<grid1d(npx * kC), 256, 0, st>>>(npx * kC, n->gA.p, n->h3.p, n->gB.p, gB16);      // g3
-    wgrad_mid(n, st, B, H, W, n->gB.p, n->a2.p, g + kLayerOff[2]);                                  // dW3
+    wgrad_mid(n, st, B, H, W, n->gB.p, gB16, n->a2.p, g + kLayerOff[2]);                            // dW3
     if (tc)
         conv_mid_tc_bwd(st, B, H, W, gB16, wt + 1 * kMidParams, n->a2.p, nullptr, n->gC.p, n->gC16.p, err);
     else
         conv_mid<float, float, 0, false, true>(st, B, H, W, n->gB.p, wt + 1 * kMidParams, nullptr, n->a2.p,
                                                n->gC.p);                                            // g2
-    wgrad_mid(n, st, B, H, W, n->gC.p, n->h1.p, g + kLayerOff[1]);                                  // dW2
+    wgrad_mid(n, st, B, H, W, n->gC.p, tc ? n->gC16.p : nullptr, n->h1.p, g + kLayerOff[1]);     // dW2
     if (tc)
         conv_mid_tc_bwd(st, B, H, W, n->gC16.p, wt + 0 * kMidParams, nullptr, n->gB.p, n->gA.p, nullptr, err);
     else

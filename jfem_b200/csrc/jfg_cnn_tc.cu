@@ -869,6 +869,171 @@ k_conv_strip(const __grid_constant__ CUtensorMap trow, StripGeo g, const bf16* _
     }
 }
 
+// ---------------------------------------------------------------------------
+// Weight gradient of a 32 -> 32 layer on the tensor cores:
+//   dW[co][tap][ci] = sum_p G[p][co] X[p + tap][ci]
+// One MMA per tap and 16 pixels: D_tap (M = 128 rows, the first 32 = co;
+// N = 32 = ci) += A (G^T: rows co, K = 16 pixels) x B_tap (rows ci, K = the
+// same 16 pixels of X shifted by the tap).  Both operands are K-major
+// (channel-planar tiles in shared memory: core matrices of 8 channels x 8
+// pixels), so the pixels are the contraction: a tile of 8 x 32 output pixels
+// is 16 K-steps, its X halo (10 rows) is kept in three copies shifted by
+// dx - 1 pixels so that every tap's B is a descriptor view (the dy shift is
+// whole 32-pixel rows).  A's rows 32..127 are a zero region.  The nine
+// 32-column accumulators stay in TMEM over all tiles of the CTA; the epilogue
+// writes the CTA's partial dW (FP32, [co][tap * 32 + ci]) for the ordered
+// reduction of k_wgrad_mid_reduce.  Staging is done by all threads from the
+// BF16 images, one tile at a time (training-path kernel).
+// ---------------------------------------------------------------------------
+constexpr int kGTH = 8, kGTW = 32;               // output tile rows x columns (256 pixels)
+constexpr int kGChunks = kGTH * kGTW / 8;        // 32 chunks of 8 pixels
+constexpr int kGSbo = kGChunks * 128;            // A: bytes per 8-channel row group (4096)
+constexpr int kGABytes = 16 * kGSbo;             // 128 rows (32 real + 96 zero): 65,536
+constexpr int kXRows = kGTH + 2;                 // halo rows
+constexpr int kXChunks = kXRows * kGTW / 8;      // 40
+constexpr int kXSbo = kXChunks * 128;            // 5,120
+constexpr int kXCopyBytes = 4 * kXSbo;           // 20,480
+constexpr int kWgSmem = kGABytes + 3 * kXCopyBytes + 128;
+
+__device__ __forceinline__ uint4 ld_px(const bf16* __restrict__ img, int b, int H, int W, int y, int x)
+{
+    if (y < 0 || y >= H || x < 0 || x >= W) return make_uint4(0, 0, 0, 0);
+    return __ldg(reinterpret_cast<const uint4*>(img + (((size_t)b * H + y) * W + x) * 32));
+}
+
+// two pixels' 8 channels (a = pixel k, c = pixel k + 1, k even) into the
+// K-major core matrix rows: 8 words of (pixel k, pixel k + 1) per channel
+__device__ __forceinline__ void put_pair(unsigned char* dst, const uint4& a, const uint4& c)
+{
+    const uint32_t av[4] = {a.x, a.y, a.z, a.w}, cv[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        // channel 2j in the low halves, 2j + 1 in the high halves
+        *reinterpret_cast<uint32_t*>(dst + (2 * j) * 16) = (av[j] & 0xFFFFu) | (cv[j] << 16);
+        *reinterpret_cast<uint32_t*>(dst + (2 * j + 1) * 16) = (av[j] >> 16) | (cv[j] & 0xFFFF0000u);
+    }
+}
+
+__global__ void __launch_bounds__(256, 1)
+k_wgrad_tc(int B, int H, int W, const bf16* __restrict__ G, const bf16* __restrict__ X, float* __restrict__ part,
+           int* __restrict__ err)
+{
+    extern __shared__ unsigned char dsm_raw[];
+    unsigned char* dsm = reinterpret_cast<unsigned char*>(((uintptr_t)dsm_raw + 127) & ~(uintptr_t)127);
+    unsigned char* asm_ = dsm;                                    // A: G^T, 128 rows
+    unsigned char* xsm = dsm + kGABytes;                          // three shifted X copies
+    __shared__ __align__(8) uint64_t mdone;
+    __shared__ uint32_t tmem_sh;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int i = tid; i < kGABytes / 16; i += 256) reinterpret_cast<uint4*>(asm_)[i] = make_uint4(0, 0, 0, 0);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&tmem_sh))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 32) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mdone)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_sh;
+    const uint32_t abase = smem_u32(asm_), xbase = smem_u32(xsm);
+    const int tx = (W + kGTW - 1) / kGTW, ty = (H + kGTH - 1) / kGTH;
+    const int ntiles = tx * ty * B;
+    bool ok = true;
+    int it = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
+        const int b = t / (tx * ty), rem = t - b * (tx * ty);
+        const int y0 = (rem / tx) * kGTH, x0 = (rem % tx) * kGTW;
+        if (it > 0) {                                // the previous tile's MMAs have read the operands
+            const bool w = tid == 0 ? mbar_wait(smem_u32(&mdone), (uint32_t)((it - 1) & 1)) : true;
+            if (!__syncthreads_and(w)) {
+                ok = false;
+                break;
+            }
+        }
+        // G tile -> A rows 0..31: 128 pixel pairs x 4 channel groups
+        for (int i = tid; i < (kGTH * kGTW / 2) * 4; i += 256) {
+            const int pp = i >> 2, g = i & 3, k = 2 * pp;
+            const int r = k / kGTW, c = k % kGTW;
+            // the 8 channels of group g are the g-th 16 bytes of the pixel's 64
+            const uint4 a8 = ld_px(G + 8 * g, b, H, W, y0 + r, x0 + c);
+            const uint4 c8 = ld_px(G + 8 * g, b, H, W, y0 + r, x0 + c + 1);
+            put_pair(asm_ + g * kGSbo + (k / 8) * 128 + (k % 8) * 2, a8, c8);
+        }
+        // X halo -> three copies shifted by dx - 1: 10 rows x 16 pairs x 4 groups each
+        for (int i = tid; i < 3 * (kXRows * kGTW / 2) * 4; i += 256) {
+            const int g = i & 3, rest = i >> 2;
+            const int dx = rest / (kXRows * kGTW / 2), pp = rest % (kXRows * kGTW / 2), k = 2 * pp;
+            const int hr = k / kGTW, c = k % kGTW;
+            const uint4 a8 = ld_px(X + 8 * g, b, H, W, y0 + hr - 1, x0 + c + dx - 1);
+            const uint4 c8 = ld_px(X + 8 * g, b, H, W, y0 + hr - 1, x0 + c + dx);
+            put_pair(xsm + dx * kXCopyBytes + g * kXSbo + (k / 8) * 128 + (k % 8) * 2, a8, c8);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll 1
+            for (int sk = 0; sk < kGTH * kGTW / 16; sk++) {
+                const int r = sk >> 1, h = sk & 1;
+                const uint64_t da = umma_desc(abase + sk * 256, 128, kGSbo);
+#pragma unroll
+                for (int tap = 0; tap < 9; tap++) {
+                    const int dy = tap / 3, dx = tap % 3;
+                    const uint64_t db =
+                        umma_desc(xbase + dx * kXCopyBytes + ((r + dy) * (kGTW / 8) + 2 * h) * 128, 128, kXSbo);
+                    const uint32_t accum = (it > 0 || sk > 0) ? 1u : 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                        ::"r"(tmem + (uint32_t)(tap * 32)), "l"(da), "l"(db), "r"(kIdesc), "r"(accum)
+                        : "memory");
+                }
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&mdone))
+                         : "memory");
+        }
+    }
+    // all MMAs complete, then each CTA writes its partial dW from TMEM rows 0..31 (warp 0)
+    const bool w = (tid == 0 && ok && it > 0) ? mbar_wait(smem_u32(&mdone), (uint32_t)((it - 1) & 1)) : true;
+    ok = __syncthreads_and(ok && w);
+    if (!ok && tid == 0) atomicOr(err, 1);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (warp == 0) {
+        float* dst = part + (size_t)blockIdx.x * (32 * 288) + (size_t)lane * 288;
+#pragma unroll 1
+        for (int tap = 0; tap < 9; tap++) {
+            uint32_t r[32];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                  "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                  "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                : "r"(tmem + (uint32_t)(tap * 32))
+                : "memory");
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int ci = 0; ci < 32; ci++)
+                dst[tap * 32 + ci] = (it > 0 && ok) ? __uint_as_float(r[ci]) : 0.f;
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+    }
+}
+
 }  // namespace
 
 // The driver's tensor-map encoder, fetched once through the runtime (no link
@@ -1091,6 +1256,28 @@ void conv_mid_tc_bwd(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* 
         launch_conv<kBwdMask>(st, grid, map, B, H, W, wt, mask, out, out16, err);
     else
         launch_conv<kBwdSkip>(st, grid, map, B, H, W, wt, skip, out, nullptr, err);
+}
+
+// Per-CTA partial weight gradients of a 32 -> 32 layer on the tensor cores
+// (k_wgrad_tc) from the BF16 gradient image G16 and the BF16 layer input X:
+// part[cta][co * 288 + tap * 32 + ci]; returns the number of CTAs (at most
+// max_parts).  err is set to 1 if the MMA wait timed out.
+int wgrad_mid_tc(cudaStream_t st, int B, int H, int W, const __nv_bfloat16* G16, const __nv_bfloat16* X,
+                 float* part, int max_parts, int* err)
+{
+    const long long ntiles = (long long)((W + kGTW - 1) / kGTW) * ((H + kGTH - 1) / kGTH) * B;
+    JFG_CHECK(ntiles < (1LL << 31), JFG_ERR_UNSUPPORTED, "image too large for the tensor-core weight gradient");
+    const int ctas = (int)std::min<long long>(std::min<long long>(ntiles, sm_count()), max_parts);
+    if (ctas <= 0) return 0;
+    static bool attr = false;
+    if (!attr) {
+        JFG_CUDA(cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kWgSmem));
+        attr = true;
+    }
+    k_wgrad_tc<<<ctas, 256, kWgSmem, st>>>(B, H, W, G16, X, part, err);
+    JFG_CUDA(cudaGetLastError());
+    note_launch();
+    return ctas;
 }
 
 }  // namespace jfg

@@ -176,3 +176,31 @@ def test_strip_conv_equals_tiled(ctx, shape, monkeypatch):
     assert np.all(np.isfinite(outs[0][0]))
     for a, b in zip(outs[0], outs[1]):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("shape", [(2, 45, 27), (1, 257, 131), (3, 64, 64)])
+def test_tcgen05_weight_gradients_match_mma_sync(ctx, shape, monkeypatch):
+    """Weight gradients of the 32 -> 32 layers on the tensor cores (k_wgrad_tc:
+    G^T and the tap-shifted X as K-major channel-planar tiles, the pixels as
+    the contraction, nine TMEM accumulators per CTA) against the mma.sync
+    kernel on the same BF16 gradient images and activations: the same
+    products summed in another order, so they agree to FP32 rounding of the
+    sums."""
+    rng = np.random.default_rng(16)
+    w = he_init(seed=11, gain_last=1.0)
+    x = torch.from_numpy(rng.standard_normal(shape).astype(np.float32)).cuda()
+    t = torch.from_numpy(rng.standard_normal(shape).astype(np.float32)).cuda()
+    net = LearnedSmoother(ctx, w)
+    monkeypatch.setenv("JFEM_CNN_TC", "1")
+    l_tc, g_tc = net.loss_and_grad(x, t)
+    monkeypatch.setenv("JFEM_CNN_WGRAD_TC", "0")
+    l_ms, g_ms = net.loss_and_grad(x, t)
+    assert l_tc == l_ms
+    parts_tc, parts_ms = unpack(g_tc), unpack(g_ms)
+    for l in (1, 2, 3, 4):                       # the 32 -> 32 layers
+        a, b = parts_tc[l], parts_ms[l]
+        assert np.all(np.isfinite(a))
+        err = np.linalg.norm(a - b) / np.linalg.norm(b)
+        assert err < 1e-4, (l, err)
+    for l in (0, 5):                             # the edge layers are unchanged
+        assert np.array_equal(parts_tc[l], parts_ms[l])
