@@ -885,15 +885,16 @@ k_conv_strip(const __grid_constant__ CUtensorMap trow, StripGeo g, const bf16* _
 // reduction of k_wgrad_mid_reduce.  Staging is done by all threads from the
 // BF16 images, one tile at a time (training-path kernel).
 // ---------------------------------------------------------------------------
-constexpr int kGTH = 8, kGTW = 32;               // output tile rows x columns (256 pixels)
-constexpr int kGChunks = kGTH * kGTW / 8;        // 32 chunks of 8 pixels
-constexpr int kGSbo = kGChunks * 128;            // A: bytes per 8-channel row group (4096)
-constexpr int kGABytes = 16 * kGSbo;             // 128 rows (32 real + 96 zero): 65,536
+constexpr int kGTH = 8, kGTW = 16;               // output tile rows x columns (128 pixels)
+constexpr int kGChunks = kGTH * kGTW / 8;        // 16 chunks of 8 pixels
+constexpr int kGSbo = kGChunks * 128;            // A: bytes per 8-channel row group (2048)
+constexpr int kGABytes = 16 * kGSbo;             // 128 rows (32 real + 96 zero): 32,768
 constexpr int kXRows = kGTH + 2;                 // halo rows
-constexpr int kXChunks = kXRows * kGTW / 8;      // 40
-constexpr int kXSbo = kXChunks * 128;            // 5,120
-constexpr int kXCopyBytes = 4 * kXSbo;           // 20,480
-constexpr int kWgSmem = kGABytes + 3 * kXCopyBytes + 128;
+constexpr int kXChunks = kXRows * kGTW / 8;      // 20
+constexpr int kXSbo = kXChunks * 128;            // 2,560
+constexpr int kXCopyBytes = 4 * kXSbo;           // 10,240
+constexpr int kGStage = kGABytes + 3 * kXCopyBytes;   // 63,488: one tile's operands
+constexpr int kWgSmem = 2 * kGStage + 128;       // two stages: staging overlaps the MMAs
 
 __device__ __forceinline__ uint4 ld_px(const bf16* __restrict__ img, int b, int H, int W, int y, int x)
 {
@@ -920,26 +921,26 @@ k_wgrad_tc(int B, int H, int W, const bf16* __restrict__ G, const bf16* __restri
 {
     extern __shared__ unsigned char dsm_raw[];
     unsigned char* dsm = reinterpret_cast<unsigned char*>(((uintptr_t)dsm_raw + 127) & ~(uintptr_t)127);
-    unsigned char* asm_ = dsm;                                    // A: G^T, 128 rows
-    unsigned char* xsm = dsm + kGABytes;                          // three shifted X copies
-    __shared__ __align__(8) uint64_t mdone;
+    // stage s: A (G^T, 128 rows) at s * kGStage, then the three shifted X copies
+    __shared__ __align__(8) uint64_t mdone[2];
     __shared__ uint32_t tmem_sh;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    for (int i = tid; i < kGABytes / 16; i += 256) reinterpret_cast<uint4*>(asm_)[i] = make_uint4(0, 0, 0, 0);
+    for (int i = tid; i < 2 * kGStage / 16; i += 256) reinterpret_cast<uint4*>(dsm)[i] = make_uint4(0, 0, 0, 0);
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&tmem_sh))
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 32) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mdone)) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mdone[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mdone[1])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_sh;
-    const uint32_t abase = smem_u32(asm_), xbase = smem_u32(xsm);
+    const uint32_t sbase = smem_u32(dsm);
     const int tx = (W + kGTW - 1) / kGTW, ty = (H + kGTH - 1) / kGTH;
     const int ntiles = tx * ty * B;
     bool ok = true;
@@ -947,15 +948,18 @@ k_wgrad_tc(int B, int H, int W, const bf16* __restrict__ G, const bf16* __restri
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
         const int b = t / (tx * ty), rem = t - b * (tx * ty);
         const int y0 = (rem / tx) * kGTH, x0 = (rem % tx) * kGTW;
-        if (it > 0) {                                // the previous tile's MMAs have read the operands
-            const bool w = tid == 0 ? mbar_wait(smem_u32(&mdone), (uint32_t)((it - 1) & 1)) : true;
+        const int sg = it & 1;
+        unsigned char* asm_ = dsm + sg * kGStage;
+        unsigned char* xsm = asm_ + kGABytes;
+        if (it >= 2) {                               // tile it - 2's MMAs have read this stage
+            const bool w = tid == 0 ? mbar_wait(smem_u32(&mdone[sg]), (uint32_t)(((it >> 1) - 1) & 1)) : true;
             if (!__syncthreads_and(w)) {
                 ok = false;
                 break;
             }
         }
         // G tile -> A rows 0..31: 128 pixel pairs x 4 channel groups
-        for (int i = tid; i < (kGTH * kGTW / 2) * 4; i += 256) {
+        for (int i = tid; i < (kGTH * kGTW / 2) * 4; i += 256) {      // one item per thread
             const int pp = i >> 2, g = i & 3, k = 2 * pp;
             const int r = k / kGTW, c = k % kGTW;
             // the 8 channels of group g are the g-th 16 bytes of the pixel's 64
@@ -975,10 +979,11 @@ k_wgrad_tc(int B, int H, int W, const bf16* __restrict__ G, const bf16* __restri
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
+            const uint32_t abase = sbase + sg * kGStage, xbase = abase + kGABytes;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll 1
-            for (int sk = 0; sk < kGTH * kGTW / 16; sk++) {
-                const int r = sk >> 1, h = sk & 1;
+            for (int sk = 0; sk < kGTH * kGTW / 16; sk++) {         // one K-step per 16-pixel tile row
+                const int r = sk, h = 0;
                 const uint64_t da = umma_desc(abase + sk * 256, 128, kGSbo);
 #pragma unroll
                 for (int tap = 0; tap < 9; tap++) {
@@ -995,12 +1000,14 @@ k_wgrad_tc(int B, int H, int W, const bf16* __restrict__ G, const bf16* __restri
                 }
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_u32(&mdone))
+                             smem_u32(&mdone[sg]))
                          : "memory");
         }
     }
     // all MMAs complete, then each CTA writes its partial dW from TMEM rows 0..31 (warp 0)
-    const bool w = (tid == 0 && ok && it > 0) ? mbar_wait(smem_u32(&mdone), (uint32_t)((it - 1) & 1)) : true;
+    // commits complete in order: the last tile's covers every MMA
+    const bool w = (tid == 0 && ok && it > 0) ? mbar_wait(smem_u32(&mdone[(it - 1) & 1]), (uint32_t)(((it - 1) >> 1) & 1))
+                                              : true;
     ok = __syncthreads_and(ok && w);
     if (!ok && tid == 0) atomicOr(err, 1);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
