@@ -885,15 +885,20 @@ k_conv_strip(const __grid_constant__ CUtensorMap trow, StripGeo g, const bf16* _
 // reduction of k_wgrad_mid_reduce.  Staging is done by all threads from the
 // BF16 images, one tile at a time (training-path kernel).
 // ---------------------------------------------------------------------------
+// Core matrices are 128 bytes apart along K plus 16 bytes of padding (LBO =
+// 144) and the 8-channel row groups 32 bytes past a multiple of 128 (SBO), so
+// that the staging stores of a warp (4 channel groups x 2 chunks x 4 pixel
+// pairs, one channel row each) fall into 32 distinct banks.
 constexpr int kGTH = 8, kGTW = 16;               // output tile rows x columns (128 pixels)
+constexpr int kGLbo = 144;
 constexpr int kGChunks = kGTH * kGTW / 8;        // 16 chunks of 8 pixels
-constexpr int kGSbo = kGChunks * 128;            // A: bytes per 8-channel row group (2048)
-constexpr int kGABytes = 16 * kGSbo;             // 128 rows (32 real + 96 zero): 32,768
+constexpr int kGSbo = kGChunks * kGLbo + 32;     // A: bytes per 8-channel row group (2,336)
+constexpr int kGABytes = 16 * kGSbo;             // 128 rows (32 real + 96 zero): 37,376
 constexpr int kXRows = kGTH + 2;                 // halo rows
 constexpr int kXChunks = kXRows * kGTW / 8;      // 20
-constexpr int kXSbo = kXChunks * 128;            // 2,560
-constexpr int kXCopyBytes = 4 * kXSbo;           // 10,240
-constexpr int kGStage = kGABytes + 3 * kXCopyBytes;   // 63,488: one tile's operands
+constexpr int kXSbo = kXChunks * kGLbo + 96;     // 2,976
+constexpr int kXCopyBytes = 4 * kXSbo;           // 11,904
+constexpr int kGStage = kGABytes + 3 * kXCopyBytes;   // 73,088: one tile's operands
 constexpr int kWgSmem = 2 * kGStage + 128;       // two stages: staging overlaps the MMAs
 
 __device__ __forceinline__ uint4 ld_px(const bf16* __restrict__ img, int b, int H, int W, int y, int x)
@@ -965,7 +970,7 @@ k_wgrad_tc(int B, int H, int W, const bf16* __restrict__ G, const bf16* __restri
             // the 8 channels of group g are the g-th 16 bytes of the pixel's 64
             const uint4 a8 = ld_px(G + 8 * g, b, H, W, y0 + r, x0 + c);
             const uint4 c8 = ld_px(G + 8 * g, b, H, W, y0 + r, x0 + c + 1);
-            put_pair(asm_ + g * kGSbo + (k / 8) * 128 + (k % 8) * 2, a8, c8);
+            put_pair(asm_ + g * kGSbo + (k / 8) * kGLbo + (k % 8) * 2, a8, c8);
         }
         // X halo -> three copies shifted by dx - 1: 10 rows x 16 pairs x 4 groups each
         for (int i = tid; i < 3 * (kXRows * kGTW / 2) * 4; i += 256) {
@@ -974,7 +979,7 @@ k_wgrad_tc(int B, int H, int W, const bf16* __restrict__ G, const bf16* __restri
             const int hr = k / kGTW, c = k % kGTW;
             const uint4 a8 = ld_px(X + 8 * g, b, H, W, y0 + hr - 1, x0 + c + dx - 1);
             const uint4 c8 = ld_px(X + 8 * g, b, H, W, y0 + hr - 1, x0 + c + dx);
-            put_pair(xsm + dx * kXCopyBytes + g * kXSbo + (k / 8) * 128 + (k % 8) * 2, a8, c8);
+            put_pair(xsm + dx * kXCopyBytes + g * kXSbo + (k / 8) * kGLbo + (k % 8) * 2, a8, c8);
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
@@ -984,12 +989,12 @@ k_wgrad_tc(int B, int H, int W, const bf16* __restrict__ G, const bf16* __restri
 #pragma unroll 1
             for (int sk = 0; sk < kGTH * kGTW / 16; sk++) {         // one K-step per 16-pixel tile row
                 const int r = sk, h = 0;
-                const uint64_t da = umma_desc(abase + sk * 256, 128, kGSbo);
+                const uint64_t da = umma_desc(abase + sk * 2 * kGLbo, kGLbo, kGSbo);
 #pragma unroll
                 for (int tap = 0; tap < 9; tap++) {
                     const int dy = tap / 3, dx = tap % 3;
                     const uint64_t db =
-                        umma_desc(xbase + dx * kXCopyBytes + ((r + dy) * (kGTW / 8) + 2 * h) * 128, 128, kXSbo);
+                        umma_desc(xbase + dx * kXCopyBytes + ((r + dy) * (kGTW / 8) + 2 * h) * kGLbo, kGLbo, kXSbo);
                     const uint32_t accum = (it > 0 || sk > 0) ? 1u : 0u;
                     asm volatile(
                         "{\n\t.reg .pred p;\n\t"
