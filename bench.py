@@ -17,7 +17,7 @@ cells solved by a dense FP64 inverse.  Arms, each a whole solve to
 
 The working set (FP64 finest matrix, hierarchy, vectors) is larger than L2,
 so solves run back to back without a flush.  The Q2 512x512 -Lap u + 5u = f
-GMG-PCG (configs' multigrid case) is timed too and reported as extra keys.
+GMG-PCG (the Q2 multigrid case, 8 levels) is timed too and reported as extra keys.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
 
