@@ -158,7 +158,12 @@ struct EpiRestrictSweep {
 // the coarser level, coarse FP64 solve, prolongation + correction) is one
 // pass of each thread over its rows followed by a hardware cluster barrier
 // (barrier.cluster arrive.release / wait.acquire): no software spin-wait,
-// and no global-memory traffic inside the cycle.  The level entered from
+// and no global-memory traffic inside the cycle.  The coarsest levels, when
+// their rows fit next to the rest, are owned wholly by CTA 0 ("local"
+// levels): a phase whose own level and the level the next phase reads are
+// both local ends with a CTA barrier instead of a cluster barrier (the other
+// CTAs have no rows there), and every CTA still meets every cluster barrier,
+// so the sequence of cluster barriers is the same on all of them.  The level entered from
 // above reads its restricted right-hand side from global memory and the
 // result x of that level is written back at the end.  Row sums run in
 // ascending column order from 0 with fused multiply-adds, as in the
@@ -167,7 +172,8 @@ constexpr int kTailMaxLevels = 8;         // coarse level included
 constexpr int kTailMaxRowsPerCta = 4095;  // 12-bit local row of a packed column
 constexpr int kTailThreads = 1024;
 constexpr int kTailSmemBudget = 224 * 1024;
-constexpr int kTailMetaInts = 22;         // per level: A, R, P (5 each), dinv, mask, rows per CTA, x, t, b, r
+constexpr int kTailMetaInts = 23;         // per level: A, R, P (5 each), dinv, mask, rows per CTA, x, t, b, r, local
+constexpr int kTailLocalRows = 1100;      // largest level owned wholly by CTA 0 (if the shared memory allows)
 
 struct TailMat {
     int off_col, off_val;   // byte offsets of the column and value blocks in a CTA's shared memory
@@ -179,6 +185,7 @@ template <typename T>
 struct TailLevel {
     TailMat A, R, P;          // R: restriction into level l - 1, P: prolongation from level l - 1
     int Rl, n, runs;          // rows per CTA, rows, Jacobi sweeps
+    int local;                // every row on CTA 0 (Rl == n)
     int off_dinv, off_mask, off_x, off_t, off_b, off_r;
     T omega;
 };
@@ -261,6 +268,14 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
     extern __shared__ __align__(16) unsigned char sm[];
     cg::cluster_group cl = cg::this_cluster();
     const int c = (int)cl.block_rank();
+    // end of a phase: a CTA barrier when the phase's level and the level the
+    // next phase reads are both local (CTA 0 alone), else a cluster barrier
+    auto phase_end = [&](bool local) {
+        if (local)
+            __syncthreads();
+        else
+            cl.sync();
+    };
     // the matrices, diagonals and masks do not change after set-up: copy them
     // before waiting for the preceding kernel
     {
@@ -285,9 +300,10 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
         // the first sweep from the zero guess lands where the last one ends in x
         T* cur = vec((L.runs % 2 == 1) ? L.off_x : L.off_t);
         int cur_off = (L.runs % 2 == 1) ? L.off_x : L.off_t;
+        const bool loc = L.local != 0;
         if (l == P.top) {   // below the top the restriction phase did it
             tail_own(L.Rl, L.n, c, [&](int t) { cur[t] = (T)0 + (dinv[t] * b[t]) * om; });
-            cl.sync();
+            phase_end(loc);
         }
         for (int k = 1; k < L.runs; k++) {
             const int alt_off = cur_off == L.off_x ? L.off_t : L.off_x;
@@ -296,7 +312,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
             A.xoff = cur_off;
             const T* cu = cur;
             tail_spmv<T>(sm, A, c, [&](int t, T s) { alt[t] = cu[t] + (dinv[t] * (b[t] - s)) * om; });
-            cl.sync();
+            phase_end(loc);
             cur = alt;
             cur_off = alt_off;
         }
@@ -305,7 +321,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
             TailMat A = L.A;
             A.xoff = L.off_x;
             tail_spmv<T>(sm, A, c, [&](int t, T s) { r[t] = b[t] - s; });
-            cl.sync();
+            phase_end(loc);   // level l - 1 is local whenever level l is
         }
         {   // restriction into level l - 1 with zero boundary values (and its fused first sweep)
             const TailLevel<T>& Cl = P.lv[l - 1];
@@ -325,7 +341,10 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
             } else {
                 tail_spmv<T>(sm, R, c, [&](int t, T s) { bc[t] = mask[t] ? (T)0 : s; });
             }
-            cl.sync();
+            // a local level l - 1 is read next by CTA 0 alone; the other CTAs
+            // keep their r rows (read here remotely) until the next cluster
+            // barrier, which comes before any of them writes level l again
+            phase_end(Cl.local != 0);
         }
     }
     {   // coarsest level: x0 = Ainv * b0 in FP64, one warp per own row (the order of k_coarse_gemv)
@@ -345,7 +364,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
             s = warp_sum(s);
             if (lane == 0) x0[t] = (T)s;
         }
-        cl.sync();
+        phase_end(L0.local != 0 && (P.top < 1 || P.lv[1].local != 0));
     }
     for (int l = 1; l <= P.top; l++) {
         const TailLevel<T>& L = P.lv[l];
@@ -358,8 +377,11 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
             TailMat Pm = L.P;
             Pm.xoff = P.lv[l - 1].off_x;
             tail_spmv<T>(sm, Pm, c, [&](int t, T s) { x[t] = x[t] + (mask[t] ? (T)0 : s); });
-            cl.sync();
+            phase_end(L.local != 0);
         }
+        // the last phase of level l is read next by the prolongation into
+        // level l + 1 (or, at the top, by the copy-out of the own rows)
+        const bool loc_next = L.local != 0 && (l == P.top || P.lv[l + 1].local != 0);
         int cur_off = L.off_x;
         for (int k = 0; k < L.runs; k++) {
             const int alt_off = cur_off == L.off_x ? L.off_t : L.off_x;
@@ -368,14 +390,15 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_mg_tail(const __grid_consta
             TailMat A = L.A;
             A.xoff = cur_off;
             tail_spmv<T>(sm, A, c, [&](int t, T s) { alt[t] = cu[t] + (dinv[t] * (b[t] - s)) * om; });
-            cl.sync();
+            const bool last = k == L.runs - 1 && alt_off == L.off_x;
+            phase_end(last ? loc_next : L.local != 0);
             cur_off = alt_off;
         }
         if (cur_off != L.off_x) {
             const T* cu = vec(cur_off);
             T* x = vec(L.off_x);
             tail_own(L.Rl, L.n, c, [&](int t) { x[t] = cu[t]; });
-            cl.sync();
+            phase_end(loc_next);
         }
     }
     {   // the result of the top level back to global memory
@@ -657,7 +680,8 @@ void MGImpl<T>::build_tail()
     }
     std::vector<double> hdinv;
     auto al16 = [](size_t b) { return (b + 15) / 16 * 16; };
-    auto rows_per = [&](int l, int C) { return (n[l] + C - 1) / C; };
+    int loc_rows = 0;                                  // levels with at most this many rows are local (CTA 0)
+    auto rows_per = [&](int l, int C) { return n[l] <= loc_rows ? n[l] : (n[l] + C - 1) / C; };
     // byte sizes: constant package, then vectors
     auto sizes = [&](int top, int C, size_t& pkg, size_t& total) {
         pkg = 0;
@@ -691,6 +715,18 @@ void MGImpl<T>::build_tail()
         if (C) break;
     }
     if (top < 1 || !C) return;
+    {   // the largest set of coarsest levels that CTA 0 can own with the cluster still resident
+        const char* le = getenv("JFEM_MG_TAIL_LOCAL");
+        if (!(le && le[0] == '0')) {
+            for (int l = top; l >= 0; l--) {
+                if (n[l] > kTailLocalRows) continue;
+                loc_rows = n[l];
+                sizes(top, C, pkg_b, tot_b);
+                if (tot_b <= (size_t)kTailSmemBudget && tail_cluster_size<T>(tot_b) >= C) break;
+                loc_rows = 0;
+            }
+        }
+    }
     sizes(top, C, pkg_b, tot_b);
     // host copies of the diagonal inverses and masks
     std::vector<std::vector<T>> dv(top + 1);
@@ -756,6 +792,7 @@ void MGImpl<T>::build_tail()
             for (int t = 0; t < Rl && cc * Rl + t < n[l]; t++) pkg[cc * pkg_b + off + t] = mk[l][cc * Rl + t];
         off += al16((size_t)Rl);
         meta[17] = Rl;
+        meta[22] = n[l] <= loc_rows ? 1 : 0;
     }
     JFG_CHECK(off == pkg_b, JFG_ERR_CUDA, "tail package layout mismatch");
     for (int l = 0; l <= top; l++) {                      // vectors x, t, b, r
@@ -923,6 +960,7 @@ void MGImpl<T>::run_tail(bool first_sweep_done, const int* done, cudaStream_t st
         Lv.off_dinv = m[15];
         Lv.off_mask = m[16];
         Lv.Rl = m[17];
+        Lv.local = m[22];
         Lv.off_x = m[18];
         Lv.off_t = m[19];
         Lv.off_b = m[20];

@@ -98,6 +98,61 @@ def loss_and_grads(weights, x, t):
     return L, [dw1, dw2, dw3, dw4, dw5, dw6]
 
 
+def bf16(a):
+    """Round to the nearest BF16 value, ties to even (via FP32), as the GPU's
+    __float2bfloat16_rn does; returned as float64."""
+    f = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+    u = f.view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def forward_bf16(weights, x):
+    """The forward with the GPU's storage roundings (float64 arithmetic
+    otherwise): the 32 -> 32 layers read BF16 weights and BF16 input and skip
+    activations, every stored activation (h1, a2, h3, a4, h5) is BF16, the
+    1 -> 32 and 32 -> 1 layers use the FP32 master weights on the FP32 input
+    image and the BF16 h5."""
+    w1, w2, w3, w4, w5, w6 = weights
+    m2, m3, m4, m5 = (bf16(w) for w in (w2, w3, w4, w5))
+    h1 = bf16(relu(conv(x[..., None], w1)))
+    a2 = bf16(relu(conv(h1, m2)))
+    h3 = bf16(relu(h1 + conv(a2, m3)))
+    a4 = bf16(relu(conv(h3, m4)))
+    h5 = bf16(relu(h3 + conv(a4, m5)))
+    y = conv(h5, w6)[..., 0]
+    return y, (x, h1, a2, h3, a4, h5)
+
+
+def loss_and_grads_bf16(weights, x, t):
+    """loss_and_grads with the GPU backward's roundings: the gradient images
+    that enter a 32 -> 32 product (input gradient or weight gradient) are
+    rounded to BF16 (g5, g4, g3, g2), the products read the BF16 weights
+    (flipped for the input gradients) and the BF16 activations; the skip
+    gradients, the ReLU masks and the edge layers stay FP32."""
+    w1, w2, w3, w4, w5, w6 = weights
+    m2, m3, m4, m5 = (bf16(w) for w in (w2, w3, w4, w5))
+    y, (x, h1, a2, h3, a4, h5) = forward_bf16(weights, x)
+    npx = y.size
+    L = float(np.mean((y - t) ** 2))
+    dy = (2.0 / npx) * (y - t)
+    g6 = dy[..., None]
+    dw6 = conv_grad_weight(g6, h5)
+    g5 = conv_grad_input(g6, w6) * (h5 > 0)
+    b5 = bf16(g5)
+    dw5 = conv_grad_weight(b5, a4)
+    b4 = bf16(conv_grad_input(b5, m5) * (a4 > 0))
+    dw4 = conv_grad_weight(b4, h3)
+    g3 = (g5 + conv_grad_input(b4, m4)) * (h3 > 0)
+    b3 = bf16(g3)
+    dw3 = conv_grad_weight(b3, a2)
+    b2 = bf16(conv_grad_input(b3, m3) * (a2 > 0))
+    dw2 = conv_grad_weight(b2, h1)
+    g1 = (g3 + conv_grad_input(b2, m2)) * (h1 > 0)
+    dw1 = conv_grad_weight(g1, x[..., None])
+    return L, [dw1, dw2, dw3, dw4, dw5, dw6]
+
+
 def init_weights(C=32, seed=0):
     rng = np.random.default_rng(seed)
     out = []

@@ -44,6 +44,42 @@ def test_gradient_matches_oracle(ctx, shape):
         assert err < 6e-2, (l, err)
 
 
+@pytest.mark.parametrize("shape", [(1, 16, 16), (2, 19, 37), (3, 33, 8), (1, 130, 257)])
+def test_forward_matches_bf16_oracle(ctx, shape):
+    """The forward against the oracle that rounds where the GPU stores BF16
+    (weights of the 32 -> 32 layers, every stored activation): what is left
+    is FP32 summation order and the BF16 rounding flips it causes (measured
+    up to 5e-4 on these shapes, against 3e-2 for the unrounded oracle)."""
+    rng = np.random.default_rng(1)
+    w = he_init(seed=2, gain_last=1.0)
+    x = rng.standard_normal(shape).astype(np.float32)
+    net = LearnedSmoother(ctx, w)
+    y = net.forward(torch.from_numpy(x).cuda()).cpu().numpy()
+    yr, _ = CO.forward_bf16(unpack(w), x.astype(np.float64))
+    err = np.linalg.norm(y - yr) / np.linalg.norm(yr)
+    print(f"forward {shape}: rel err {err:.3e}")
+    assert err < 2e-3, err
+
+
+@pytest.mark.parametrize("shape", [(2, 16, 16), (1, 21, 18), (1, 67, 45)])
+def test_gradient_matches_bf16_oracle(ctx, shape):
+    """Loss and all six weight gradients against the oracle with the
+    backward's BF16 roundings (gradient images entering the 32 -> 32
+    products, BF16 weights and activations)."""
+    rng = np.random.default_rng(3)
+    w = he_init(seed=4, gain_last=1.0)
+    x = rng.standard_normal(shape).astype(np.float32)
+    t = rng.standard_normal(shape).astype(np.float32)
+    net = LearnedSmoother(ctx, w)
+    loss, g = net.loss_and_grad(torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda())
+    L, gr = CO.loss_and_grads_bf16(unpack(w), x.astype(np.float64), t.astype(np.float64))
+    errs = [np.linalg.norm(gg - rr) / np.linalg.norm(rr) for gg, rr in zip(unpack(g), gr)]
+    print(f"gradients {shape}: loss rel err {abs(loss - L) / L:.3e}, " + " ".join(f"{e:.3e}" for e in errs))
+    assert abs(loss - L) / L < 1e-3
+    for l, err in enumerate(errs):
+        assert err < 3e-3, (l, err)
+
+
 def test_training_reduces_loss(ctx):
     """A few hundred Adam steps fit a fixed linear target operator (a 3x3
     smoothing stencil) on random inputs."""

@@ -99,6 +99,37 @@ def test_vcycle_tail_matches_per_launch(ctx, monkeypatch, p, coarse, L, precisio
     np.testing.assert_allclose(v1, ref, rtol=1e-10, atol=1e-10 * np.abs(ref).max())
 
 
+@pytest.mark.parametrize("p,coarse,L", [(1, 4, 6), (1, 4, 4), (2, 2, 6)])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "mixed-bf16"])
+def test_vcycle_tail_local_levels_bit_identical(ctx, monkeypatch, p, coarse, L, precision):
+    """The coarsest levels of the V-cycle tail are owned wholly by one CTA of
+    the cluster (CTA barriers between their phases instead of cluster
+    barriers; JFEM_MG_TAIL_LOCAL=0 spreads them over the cluster like the
+    larger levels).  Every row is summed by the same thread code in the same
+    column order either way, so the V-cycle, the preconditioner and a PCG
+    solve are equal bit for bit, including hierarchies whose tail levels are
+    all local (Q1 4 levels)."""
+    from jfem_b200 import IterativeSolver
+    h = mg_levels(p, coarse, L, modes=8, seed=9)
+    b = h.finest.rhs
+    outs = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("JFEM_MG_TAIL_LOCAL", flag)
+        mats = [dev(s, ctx) for s in h.systems]
+        prol = [DeviceMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l], ctx) for l in range(L - 1)]
+        mg = MGPreconditioner(mats, prol, h.boundary, [None] + [JacobiSmoother(2, 2.0 / 3.0)] * (L - 1), cycles=1,
+                              use_fmg=False, precision=precision, ctx=ctx)
+        s = IterativeSolver(ctx=ctx)
+        s.precision = "fp64" if precision == "fp64" else "mixed-precond"
+        x = s.solvePCG(mats[-1], mg, b, 1e-9 * np.linalg.norm(b))
+        v = mg.vCycle(np.zeros(b.size), b)
+        w = mg.mvMul(b)
+        outs.append((v, w, x, s.iterations))
+    (v1, w1, x1, i1), (v0, w0, x0, i0) = outs
+    assert np.all(np.isfinite(v1))
+    assert np.array_equal(v1, v0) and np.array_equal(w1, w0) and np.array_equal(x1, x0) and i1 == i0
+
+
 @pytest.mark.parametrize("p,coarse,L", [(1, 4, 5), (2, 2, 4)])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_wcycle_and_mvmulw(ctx, p, coarse, L, precision):
