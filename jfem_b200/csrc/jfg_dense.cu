@@ -5,6 +5,22 @@
 // lowest index on ties), swaps rows and scales the column; a grid then applies
 // the rank-1 update to the trailing block.  Triangular solves run one CTA per
 // right-hand side, column-oriented.
+//
+// Matrices of more than kNb columns are factored in panels of kNb columns
+// (the same arithmetic in the same order, so the factors and pivots are those
+// of the column-by-column loop bit for bit):
+//   1. one CTA factors the panel (rows k0 .. n-1, one warp per row and one lane
+//      per panel column): pivot, swap inside the panel, scale, rank-1 update
+//      of the panel's remaining columns, for each of its kNb columns;
+//   2. the panel's row interchanges are applied to every other column, in
+//      order (one thread per column);
+//   3. U12 = L11^-1 A12 for the panel's rows right of it (one thread per
+//      column, L11 in shared memory; subtractions in ascending k);
+//   4. A22 -= L21 U12 by 64 x 64 tiles, each entry subtracting the kNb
+//      products in ascending k from its current value, one rounding each, as
+//      the rank-1 updates of the column loop do.
+// Four launches per kNb columns instead of two per column, and the trailing
+// block is read and written once per panel instead of once per column.
 #include "jfg_mg.cuh"
 
 namespace jfg {
@@ -60,7 +76,170 @@ __global__ void k_lu_update(int n, double* A, int k, const int* info)
     if (idx >= (int64_t)m * m) return;
     int i = k + 1 + (int)(idx / m);
     int j = k + 1 + (int)(idx % m);
-    A[(size_t)i * n + j] -= A[(size_t)i * n + k] * A[(size_t)k * n + j];
+    A[(size_t)i * n + j] = __fma_rn(-A[(size_t)i * n + k], A[(size_t)k * n + j], A[(size_t)i * n + j]);
+}
+
+constexpr int kNb = 32;          // panel width (one lane per panel column)
+constexpr int kPanelThreads = 512;
+constexpr int kPanelRows = 8;    // panel rows per warp in flight
+
+// Step 1: the panel of columns k0 .. k0 + nb - 1 (nb <= kNb), rows k0 .. n-1.
+__global__ void __launch_bounds__(kPanelThreads)
+k_lu_panel(int n, double* A, int* piv, int k0, int nb, int* info)
+{
+    __shared__ double best[kPanelThreads];
+    __shared__ int bidx[kPanelThreads];
+    __shared__ double urow[kNb];
+    if (*info) return;                         // an earlier panel was singular
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int k = k0; k < k0 + nb; k++) {
+        double b = -1.0;
+        int bi = k;
+        for (int i = k + threadIdx.x; i < n; i += blockDim.x) {
+            const double v = fabs(A[(size_t)i * n + k]);
+            if (v > b) { b = v; bi = i; }
+        }
+        best[threadIdx.x] = b;
+        bidx[threadIdx.x] = bi;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if (threadIdx.x < s) {
+                const double o = best[threadIdx.x + s];
+                const int oi = bidx[threadIdx.x + s];
+                if (o > best[threadIdx.x] || (o == best[threadIdx.x] && oi < bidx[threadIdx.x])) {
+                    best[threadIdx.x] = o;
+                    bidx[threadIdx.x] = oi;
+                }
+            }
+            __syncthreads();
+        }
+        const int p = bidx[0];
+        const bool ok = best[0] > 0.0;
+        if (threadIdx.x == 0) {
+            piv[k] = p;
+            if (!ok) *info = 1;
+        }
+        if (!ok) return;                       // the same decision on every thread
+        if (warp == 0 && lane < nb) {          // swap rows k and p inside the panel
+            const int c = k0 + lane;
+            const double t = A[(size_t)k * n + c];
+            const double u = A[(size_t)p * n + c];
+            A[(size_t)k * n + c] = u;
+            A[(size_t)p * n + c] = t;
+            urow[lane] = u;
+        }
+        __syncthreads();
+        const double inv = 1.0 / urow[k - k0];
+        const int lk = k - k0;
+        const bool upd = lane > lk && lane < nb;
+        const double uk = upd ? urow[lane] : 0.0;
+        // scale and rank-1 update of the panel rows below k: a warp takes
+        // kPanelRows rows at a time with all their loads issued first
+        for (int i0 = k + 1 + warp * kPanelRows; i0 < n; i0 += nw * kPanelRows) {
+            double av[kPanelRows], cv[kPanelRows];
+#pragma unroll
+            for (int u = 0; u < kPanelRows; u++) {
+                const int i = i0 + u;
+                av[u] = i < n ? A[(size_t)i * n + k] : 0.0;
+                cv[u] = (i < n && upd) ? A[(size_t)i * n + k0 + lane] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < kPanelRows; u++) {
+                const int i = i0 + u;
+                if (i < n) {
+                    const double l = av[u] * inv;
+                    if (lane == lk) A[(size_t)i * n + k] = l;
+                    if (upd) A[(size_t)i * n + k0 + lane] = __fma_rn(-l, uk, cv[u]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Step 2: the panel's interchanges on the columns outside it, in order.
+__global__ void k_lu_swap(int n, double* A, const int* piv, int k0, int nb, const int* info)
+{
+    if (*info) return;
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n - nb) return;
+    if (c >= k0) c += nb;
+    for (int k = k0; k < k0 + nb; k++) {
+        const int p = piv[k];
+        if (p != k) {
+            const double t = A[(size_t)k * n + c];
+            A[(size_t)k * n + c] = A[(size_t)p * n + c];
+            A[(size_t)p * n + c] = t;
+        }
+    }
+}
+
+// Step 3: rows k0 .. k0 + nb - 1 of the columns right of the panel,
+// U12 = L11^-1 A12 (unit lower L11).
+__global__ void k_lu_trsm(int n, double* A, int k0, int nb, const int* info)
+{
+    if (*info) return;
+    __shared__ double L[kNb][kNb + 1];
+    for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) L[t / nb][t % nb] = A[(size_t)(k0 + t / nb) * n + k0 + t % nb];
+    __syncthreads();
+    const int c = k0 + nb + blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    double x[kNb];
+#pragma unroll
+    for (int r = 0; r < kNb; r++)
+        if (r < nb) {
+            double v = A[(size_t)(k0 + r) * n + c];
+#pragma unroll
+            for (int q = 0; q < kNb; q++)
+                if (q < r) v = __fma_rn(-L[r][q], x[q], v);
+            x[r] = v;
+            A[(size_t)(k0 + r) * n + c] = v;
+        }
+}
+
+// Step 4: A22 -= L21 U12 on 64 x 64 tiles (256 threads, 4 x 4 entries each).
+constexpr int kGT = 64;
+__global__ void __launch_bounds__(256) k_lu_gemm(int n, double* A, int k0, int nb, const int* info)
+{
+    if (*info) return;
+    __shared__ double Ls[kNb][kGT + 1];    // L21 tile, transposed: Ls[q][row]
+    __shared__ double Us[kNb][kGT];        // U12 tile: Us[q][col]
+    const int s = k0 + nb;                 // first row / column of A22
+    const int r0 = s + blockIdx.y * kGT, c0 = s + blockIdx.x * kGT;
+    for (int t = threadIdx.x; t < kGT * kNb; t += blockDim.x) {
+        const int rr = t / kNb, q = t % kNb;
+        Ls[q][rr] = (q < nb && r0 + rr < n) ? A[(size_t)(r0 + rr) * n + k0 + q] : 0.0;
+        const int qq = t / kGT, cc = t % kGT;
+        Us[qq][cc] = (qq < nb && c0 + cc < n) ? A[(size_t)(k0 + qq) * n + c0 + cc] : 0.0;
+    }
+    __syncthreads();
+    const int tr = threadIdx.x / 16, tc = threadIdx.x % 16;   // rows tr + 16 a, columns tc + 16 b
+    double acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            const int r = r0 + tr + 16 * a, c = c0 + tc + 16 * b;
+            acc[a][b] = (r < n && c < n) ? A[(size_t)r * n + c] : 0.0;
+        }
+    for (int q = 0; q < nb; q++) {
+        double l[4], u[4];
+#pragma unroll
+        for (int a = 0; a < 4; a++) l[a] = Ls[q][tr + 16 * a];
+#pragma unroll
+        for (int b = 0; b < 4; b++) u[b] = Us[q][tc + 16 * b];
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int b = 0; b < 4; b++) acc[a][b] = __fma_rn(-l[a], u[b], acc[a][b]);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            const int r = r0 + tr + 16 * a, c = c0 + tc + 16 * b;
+            if (r < n && c < n) A[(size_t)r * n + c] = acc[a][b];
+        }
 }
 
 // One CTA per right-hand side column c: B[:, c] <- A^-1 B[:, c], with B
@@ -102,12 +281,29 @@ int lu_factor(Context* c, int n, double* A, int* piv, int* info)
 {
     cudaStream_t st = c->stream;
     JFG_CUDA(cudaMemsetAsync(info, 0, sizeof(int), st));
-    for (int k = 0; k < n; k++) {
-        k_lu_pivot<<<1, 1024, 0, st>>>(n, A, piv, k, info);
-        int m = n - k - 1;
-        if (m > 0) {
-            int64_t tot = (int64_t)m * m;
-            k_lu_update<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(n, A, k, info);
+    const char* e = getenv("JFEM_LU_BLOCKED");
+    if (n > kNb && !(e && e[0] == '0')) {
+        for (int k0 = 0; k0 < n; k0 += kNb) {
+            const int nb = std::min(kNb, n - k0);
+            k_lu_panel<<<1, kPanelThreads, 0, st>>>(n, A, piv, k0, nb, info);
+            if (n - nb > 0) k_lu_swap<<<(unsigned)((n - nb + 255) / 256), 256, 0, st>>>(n, A, piv, k0, nb, info);
+            const int m = n - k0 - nb;
+            if (m > 0) {
+                k_lu_trsm<<<(unsigned)((m + 127) / 128), 128, 0, st>>>(n, A, k0, nb, info);
+                const unsigned g = (unsigned)((m + kGT - 1) / kGT);
+                k_lu_gemm<<<dim3(g, g), 256, 0, st>>>(n, A, k0, nb, info);
+            }
+            JFG_CUDA(cudaGetLastError());
+            note_launch(m > 0 ? 4 : 2);
+        }
+    } else {
+        for (int k = 0; k < n; k++) {
+            k_lu_pivot<<<1, 1024, 0, st>>>(n, A, piv, k, info);
+            int m = n - k - 1;
+            if (m > 0) {
+                int64_t tot = (int64_t)m * m;
+                k_lu_update<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(n, A, k, info);
+            }
         }
     }
     JFG_CUDA(cudaGetLastError());

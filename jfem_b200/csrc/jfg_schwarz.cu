@@ -259,22 +259,15 @@ __global__ void __launch_bounds__(kSchThreads)
 constexpr int kRowLanes = 4;     // lanes per residual row: 64 rows in flight per CTA
 constexpr int kRowUnroll = 8;    // entries per lane fetched before any product (rows <= 32 entries in one shot)
 
-template <typename T, typename IT>
-__device__ __forceinline__ void patch_correct(const CsrView& A, int p, const int64_t* __restrict__ pptr,
-                                              const int* __restrict__ dofs, const int64_t* __restrict__ inv_off,
-                                              const IT* __restrict__ inv, const T* b, T* x, double om,
-                                              double* lsol, bool direct, int* sdof, int* srs, int* sre, double* sr)
+// sr[i] = b[sdof[i]] - (A x)[sdof[i]] for the m staged rows (row ranges in
+// srs / sre): kRowLanes lanes per row, lane `sub` summing the entries sub,
+// sub + kRowLanes, ... in order, then a butterfly over the lanes.  Every row
+// is summed the same way whatever the block size.
+template <typename T>
+__device__ __forceinline__ void residual_rows(const CsrView& A, int m, const int* sdof, const int* srs,
+                                              const int* sre, const T* b, const T* x, double* sr)
 {
     const int tid = threadIdx.x;
-    const int64_t off = pptr[p];
-    const int m = (int)(pptr[p + 1] - off);
-    for (int i = tid; i < m; i += blockDim.x) {
-        const int g = dofs[off + i];
-        sdof[i] = g;
-        srs[i] = A.rp[g];
-        sre[i] = A.rp[g + 1];
-    }
-    __syncthreads();
     const int sub = tid & (kRowLanes - 1);
     const int per_pass = blockDim.x / kRowLanes;
     for (int i0 = 0; i0 < m; i0 += per_pass) {          // uniform trip count: the shuffles see full warps
@@ -299,6 +292,25 @@ __device__ __forceinline__ void patch_correct(const CsrView& A, int p, const int
         for (int o = 1; o < kRowLanes; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if (i < m && sub == 0) sr[i] = (double)b[sdof[i]] - acc;
     }
+}
+
+template <typename T, typename IT>
+__device__ __forceinline__ void patch_correct(const CsrView& A, int p, const int64_t* __restrict__ pptr,
+                                              const int* __restrict__ dofs, const int64_t* __restrict__ inv_off,
+                                              const IT* __restrict__ inv, const T* b, T* x, double om,
+                                              double* lsol, bool direct, int* sdof, int* srs, int* sre, double* sr)
+{
+    const int tid = threadIdx.x;
+    const int64_t off = pptr[p];
+    const int m = (int)(pptr[p + 1] - off);
+    for (int i = tid; i < m; i += blockDim.x) {
+        const int g = dofs[off + i];
+        sdof[i] = g;
+        srs[i] = A.rp[g];
+        sre[i] = A.rp[g + 1];
+    }
+    __syncthreads();
+    residual_rows<T>(A, m, sdof, srs, sre, b, x, sr);
     __syncthreads();
     const IT* At = inv + inv_off[p];                    // transposed: At[j * m + i] = inverse(i, j)
     for (int i = tid; i < m; i += blockDim.x) {
@@ -326,6 +338,158 @@ __global__ void __launch_bounds__(kSchThreads, 5)
     __shared__ double sr[kMaxPatch];
     patch_correct<T, IT>(A, plist[blockIdx.x], pptr, dofs, inv_off, inv, b, x, om, lsol, direct != 0, sdof, srs, sre,
                          sr);
+}
+
+// Fast colour steps of independent colours (the fused direct step).  Both
+// kernels walk batches of up to kMaxBatch patches that share one inverse (the
+// interior patches of a structured grid; batch q holds the patches
+// bpat[bptr[q] .. bptr[q + 1])): the residual rows of all patches of a batch
+// are gathered together, then each inverse entry is read once and applied to
+// every patch of the batch.  Per patch the sums are those of patch_correct in
+// the same order, so the result is the same bit for bit.
+//   k_schwarz_batch (colours with many more patches than SMs, e.g. the finest
+//     level): two CTAs per SM, the inverse read from L2;
+//   k_schwarz_colour (the other colours, about one batch per SM): the batch's
+//     inverse is copied into shared memory by cp.async in the background of
+//     its DOF staging and residual rows, so the inverse product reads shared
+//     memory; a CTA with several batches reloads it only when the inverse
+//     changes (the batches are sorted by inverse).
+constexpr int kMaxBatch = 4;
+constexpr int kBatchThreads = 512;
+constexpr int kBatchRows = 1024;      // patch rows per batch of k_schwarz_batch
+constexpr int kColThreads = 1024;
+constexpr size_t kColSmemMax = 226 * 1024;
+
+template <typename T, typename IT>
+__global__ void __launch_bounds__(kBatchThreads, 2)
+    k_schwarz_batch(CsrView A, const int* __restrict__ bpat, const int* __restrict__ bptr,
+                    const int64_t* __restrict__ pptr, const int* __restrict__ dofs,
+                    const int64_t* __restrict__ inv_off, const IT* __restrict__ inv, const T* b, T* x, double om,
+                    const int* done)
+{
+    if (done && *done) return;
+    __shared__ int sdof[kBatchRows], srs[kBatchRows], sre[kBatchRows];
+    __shared__ double sr[kBatchRows];
+    const int tid = threadIdx.x;
+    const int q0 = bptr[blockIdx.x];
+    const int np_ = bptr[blockIdx.x + 1] - q0;
+    const int p0 = bpat[q0];
+    const int m = (int)(pptr[p0 + 1] - pptr[p0]);      // the same for every patch of the batch
+    const int rows = np_ * m;
+    for (int k = tid; k < rows; k += blockDim.x) {
+        const int pi = k / m, i = k - pi * m;
+        const int g = dofs[pptr[bpat[q0 + pi]] + i];
+        sdof[k] = g;
+        srs[k] = A.rp[g];
+        sre[k] = A.rp[g + 1];
+    }
+    __syncthreads();
+    residual_rows<T>(A, rows, sdof, srs, sre, b, x, sr);
+    __syncthreads();
+    const IT* At = inv + inv_off[p0];                   // transposed: At[j * m + i] = inverse(i, j)
+    for (int i = tid; i < m; i += blockDim.x) {
+        double acc[kMaxBatch];
+#pragma unroll
+        for (int q = 0; q < kMaxBatch; q++) acc[q] = 0.0;
+#pragma unroll 16
+        for (int j = 0; j < m; j++) {
+            const double a = (double)__ldg(At + (size_t)j * m + i);
+#pragma unroll
+            for (int q = 0; q < kMaxBatch; q++)
+                if (q < np_) acc[q] += a * sr[q * m + j];
+        }
+#pragma unroll
+        for (int q = 0; q < kMaxBatch; q++)
+            if (q < np_) {
+                const int g = sdof[q * m + i];
+                x[g] = (T)((double)x[g] + acc[q] * om);
+            }
+    }
+}
+
+__device__ __forceinline__ void cp_async_bytes(void* sdst, const void* gsrc, int bytes)
+{
+    if (bytes == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(sdst)), "l"(gsrc) : "memory");
+    else if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(sdst)), "l"(gsrc) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(sdst)), "l"(gsrc) : "memory");
+}
+
+// Dynamic shared memory of k_schwarz_colour: one inverse (mcap x mcap, IT),
+// then rows_cap ints x 3 and rows_cap doubles.
+template <typename IT>
+__host__ __device__ constexpr size_t col_smem_inv(int mcap) { return ((size_t)mcap * mcap * sizeof(IT) + 15) / 16 * 16; }
+__host__ __device__ constexpr size_t col_smem_rows(int rows_cap)
+{
+    return ((size_t)3 * rows_cap * sizeof(int) + 15) / 16 * 16 + (size_t)rows_cap * sizeof(double);
+}
+
+template <typename T, typename IT>
+__global__ void __launch_bounds__(kColThreads, 1)
+    k_schwarz_colour(CsrView A, const int* __restrict__ bpat, const int* __restrict__ bptr, int nbatch,
+                     const int64_t* __restrict__ pptr, const int* __restrict__ dofs,
+                     const int64_t* __restrict__ inv_off, const IT* __restrict__ inv, int mcap, int rows_cap,
+                     const T* b, T* x, double om, const int* done)
+{
+    if (done && *done) return;
+    extern __shared__ __align__(16) unsigned char col_smem[];
+    const int tid = threadIdx.x;
+    IT* sAt = reinterpret_cast<IT*>(col_smem);
+    const size_t inv_bytes = col_smem_inv<IT>(mcap);
+    int* sdof = reinterpret_cast<int*>(col_smem + inv_bytes);
+    int* srs = sdof + rows_cap;
+    int* sre = srs + rows_cap;
+    double* sr = reinterpret_cast<double*>(col_smem + inv_bytes + (((size_t)3 * rows_cap * sizeof(int) + 15) / 16 * 16));
+    int64_t loaded = -1;                                           // the inverse in shared memory
+    for (int qb = blockIdx.x; qb < nbatch; qb += gridDim.x) {     // the same trip count on every thread
+        const int q0 = bptr[qb];
+        const int np_ = bptr[qb + 1] - q0;
+        const int p0 = bpat[q0];
+        const int m = (int)(pptr[p0 + 1] - pptr[p0]);             // the same for every patch of the batch
+        const int rows = np_ * m;
+        const int64_t off = inv_off[p0];
+        if (off != loaded) {   // this batch's inverse into shared memory, in the background
+            const size_t bytes = (size_t)m * m * sizeof(IT);
+            const unsigned char* src = reinterpret_cast<const unsigned char*>(inv + off);
+            unsigned char* dst = reinterpret_cast<unsigned char*>(sAt);
+            const int g = ((reinterpret_cast<uintptr_t>(src) | bytes) & 15) == 0 ? 16 : (int)sizeof(IT);
+            for (size_t k = (size_t)tid * g; k < bytes; k += (size_t)blockDim.x * g) cp_async_bytes(dst + k, src + k, g);
+            loaded = off;
+        }
+        cp_async_commit();
+        for (int k = tid; k < rows; k += blockDim.x) {
+            const int pi = k / m, i = k - pi * m;
+            const int g = dofs[pptr[bpat[q0 + pi]] + i];
+            sdof[k] = g;
+            srs[k] = A.rp[g];
+            sre[k] = A.rp[g + 1];
+        }
+        __syncthreads();
+        residual_rows<T>(A, rows, sdof, srs, sre, b, x, sr);
+        cp_async_wait<0>();
+        __syncthreads();
+        for (int i = tid; i < m; i += blockDim.x) {               // sAt[j * m + i] = inverse(i, j)
+            double acc[kMaxBatch];
+#pragma unroll
+            for (int q = 0; q < kMaxBatch; q++) acc[q] = 0.0;
+#pragma unroll 16
+            for (int j = 0; j < m; j++) {
+                const double a = (double)sAt[(size_t)j * m + i];
+#pragma unroll
+                for (int q = 0; q < kMaxBatch; q++)
+                    if (q < np_) acc[q] += a * sr[q * m + j];
+            }
+#pragma unroll
+            for (int q = 0; q < kMaxBatch; q++)
+                if (q < np_) {
+                    const int g = sdof[q * m + i];
+                    x[g] = (T)((double)x[g] + acc[q] * om);
+                }
+        }
+        __syncthreads();   // the next batch overwrites the staged rows (and perhaps the inverse)
+    }
 }
 
 // MultiplicativeSubspaceCorrection: the patches of plist one after another
@@ -585,6 +749,55 @@ void SchwarzImpl::init(Context* ctx, Matrix* Am, int kind_, double omega_, int n
                 need_buffer = true;
             }
         }
+        // Independent colours run as batches of up to kMaxBatch patches that
+        // share one inverse: on k_schwarz_batch when the colour has many more
+        // patches than SMs, else on k_schwarz_colour (about one batch per SM,
+        // the inverse in shared memory); JFEM_SCHWARZ_FAST=0 keeps one CTA per
+        // patch reading the inverse from global memory.
+        const char* ef = getenv("JFEM_SCHWARZ_FAST");
+        fast = !(ef && ef[0] == '0');
+        int dev = 0, nsm = 148;
+        JFG_CUDA(cudaGetDevice(&dev));
+        JFG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        std::vector<int> h_bpat, h_bptr;
+        for (auto& col : colours) {
+            for (int q = 0; q < col.count; q++) {
+                const int pp = hc[col.start + q];
+                col.mcap = std::max<int>(col.mcap, (int)(hp[pp + 1] - hp[pp]));
+            }
+            if (!fast || !col.independent || col.count == 0) continue;
+            int pb = 0;
+            if ((col.count + kMaxBatch - 1) / kMaxBatch > nsm && kBatchRows / col.mcap >= 2) {
+                col.kern = 1;
+                pb = std::min(kMaxBatch, kBatchRows / col.mcap);
+            } else {
+                pb = std::min(kMaxBatch, (col.count + nsm - 1) / nsm);
+                col.rows_cap = pb * col.mcap;
+                // the FP32 copy of the inverses is half the size: the FP64 bound decides
+                if (col_smem_inv<double>(col.mcap) + col_smem_rows(col.rows_cap) > kColSmemMax) continue;
+                col.kern = 2;
+            }
+            std::vector<int> pl(hc.begin() + col.start, hc.begin() + col.start + col.count);
+            std::stable_sort(pl.begin(), pl.end(), [&](int a, int b2) { return hoff2[a] < hoff2[b2]; });
+            col.b_start = (int)h_bptr.size();
+            size_t q = 0;
+            while (q < pl.size()) {
+                size_t e = q + 1;
+                while (e < pl.size() && (int)(e - q) < pb && hoff2[pl[e]] == hoff2[pl[q]]) e++;
+                h_bptr.push_back((int)h_bpat.size());
+                h_bpat.insert(h_bpat.end(), pl.begin() + q, pl.begin() + e);
+                q = e;
+            }
+            col.b_count = (int)h_bptr.size() - col.b_start;
+            h_bptr.push_back((int)h_bpat.size());   // the end of the colour's last batch
+            col.grid = col.kern == 2 ? std::min(col.b_count, nsm) : col.b_count;
+        }
+        if (!h_bpat.empty()) {
+            bpat.alloc(h_bpat.size());
+            bptr.alloc(h_bptr.size());
+            JFG_CUDA(cudaMemcpyAsync(bpat.p, h_bpat.data(), sizeof(int) * h_bpat.size(), cudaMemcpyHostToDevice, st));
+            JFG_CUDA(cudaMemcpyAsync(bptr.p, h_bptr.data(), sizeof(int) * h_bptr.size(), cudaMemcpyHostToDevice, st));
+        }
         // ColoredMultiplicativeSubspaceCorrection.solve starts with patch 0 alone
         int zero = 0;
         seq.alloc(1);
@@ -640,8 +853,26 @@ void SchwarzImpl::colour_step(const Colour& col, const T* b, T* x, double om, co
     const IT* iv = static_cast<const IT*>(inv_of<T>(this));
     const bool additive = kind == JFG_SCHWARZ_ADDITIVE;
     if (col.independent && !additive) {
-        k_schwarz_patches<T, IT><<<col.count, kSchThreads, 0, st>>>(csr_of(A), cpat.p + col.start, pptr.p, dofs.p,
-                                                                    inv_off.p, iv, b, x, om, nullptr, 1, done);
+        if (col.kern == 1) {
+            k_schwarz_batch<T, IT><<<col.b_count, kBatchThreads, 0, st>>>(csr_of(A), bpat.p, bptr.p + col.b_start,
+                                                                          pptr.p, dofs.p, inv_off.p, iv, b, x, om,
+                                                                          done);
+        } else if (col.kern == 2) {
+            static bool attr = false;      // per instantiation
+            if (!attr) {
+                JFG_CUDA(cudaFuncSetAttribute(k_schwarz_colour<T, IT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)kColSmemMax));
+                attr = true;
+            }
+            const size_t smem = col_smem_inv<IT>(col.mcap) + col_smem_rows(col.rows_cap);
+            k_schwarz_colour<T, IT><<<col.grid, kColThreads, smem, st>>>(
+                csr_of(A), bpat.p, bptr.p + col.b_start, col.b_count, pptr.p, dofs.p, inv_off.p, iv, col.mcap,
+                col.rows_cap, b, x, om, done);
+        } else {
+            k_schwarz_patches<T, IT><<<col.count, kSchThreads, 0, st>>>(csr_of(A), cpat.p + col.start, pptr.p,
+                                                                        dofs.p, inv_off.p, iv, b, x, om, nullptr, 1,
+                                                                        done);
+        }
         JFG_CUDA(cudaGetLastError());
         note_launch();
         return;

@@ -21,6 +21,7 @@ struct SchwarzImpl {
     int max_m = 0;
     int64_t total_m = 0, total_inv = 0;
     int nunique = 0;                    // distinct patch operators (inverses stored)
+    bool fast = true;                   // batched / shared-memory colour-step kernels (JFEM_SCHWARZ_FAST)
     uint64_t uid = next_uid();
     DevBuf<int64_t> pptr, inv_off;      // patch p: dofs[pptr[p], pptr[p+1]), inverse at inv + inv_off[p]
     DevBuf<int> dofs;
@@ -33,10 +34,16 @@ struct SchwarzImpl {
     DevBuf<int64_t> slots;              // indices into lsol, in ascending patch order
     DevBuf<double> lsol;                // local solutions of the patches of one sweep step
     DevBuf<int> flag;
+    DevBuf<int> bpat, bptr;             // batches of patches sharing an inverse (colours with many patches)
     struct Colour {
         int start = 0, count = 0;       // range of cpat
         bool independent = false;       // patches neither share nor couple DOFs: one fused kernel
         int64_t t_start = 0, t_count = 0;   // range of touched
+        int mcap = 0;                   // largest patch of the colour
+        int b_start = 0, b_count = 0;   // batches bptr[b_start .. b_start + b_count] (0: one CTA per patch)
+        int kern = 0;                   // 0: one CTA per patch, 1: k_schwarz_batch, 2: k_schwarz_colour
+        int rows_cap = 0;               // patch rows per batch at most (k_schwarz_colour)
+        int grid = 0;                   // CTAs of the colour-step launch
     };
     std::vector<Colour> colours;
     Colour all;                         // additive: every patch in order

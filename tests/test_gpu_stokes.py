@@ -96,3 +96,24 @@ def test_jacobi_and_fp32_variants_converge(ctx):
         sol = StokesSolver(ctx, prob, **kw)
         x, it = sol.solve(tol)
         assert it.last.status == N.OK, kw
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+def test_fast_colour_steps_bit_identical(ctx, monkeypatch, fp32):
+    """The colour steps with many patches run as batches of patches sharing
+    one inverse (128^2 cells: ~455 patches per colour on the finest level),
+    those with few patches (the coarser levels) with the inverse copied into
+    shared memory; JFEM_SCHWARZ_FAST=0 runs one CTA per patch reading the
+    inverse from global memory.  Both sum every row and every inverse product
+    in the same order: the preconditioner is equal bit for bit, FP64 and with
+    the FP32 V-cycle (FP32 inverses)."""
+    prob = stokes_problem(128, 4, nu=1.0, seed=3, pin_pressure=False)
+    v = np.random.default_rng(4).standard_normal(prob.system.n)
+    outs = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("JFEM_SCHWARZ_FAST", flag)
+        sol = StokesSolver(ctx, prob, fp32_vcycle=fp32)
+        outs.append((sol.P.mvMul(v), sol.P.mvMul(2.0 * v)))
+        del sol
+    assert np.all(np.isfinite(outs[0][0]))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
