@@ -348,7 +348,8 @@ __global__ void __launch_bounds__(kSchThreads, 5)
 // every patch of the batch.  Per patch the sums are those of patch_correct in
 // the same order, so the result is the same bit for bit.
 //   k_schwarz_batch (colours with many more patches than SMs, e.g. the finest
-//     level): two CTAs per SM, the inverse read from L2;
+//     level): four CTAs of 256 threads per SM (measured best of 2-4 patches
+//     per batch x 256 / 512 threads), the inverse read from L2;
 //   k_schwarz_colour (the other colours, about one batch per SM): the batch's
 //     inverse is copied into shared memory by cp.async in the background of
 //     its DOF staging and residual rows, so the inverse product reads shared
@@ -360,8 +361,8 @@ constexpr int kBatchRows = 1024;      // patch rows per batch of k_schwarz_batch
 constexpr int kColThreads = 1024;
 constexpr size_t kColSmemMax = 226 * 1024;
 
-template <typename T, typename IT>
-__global__ void __launch_bounds__(kBatchThreads, 2)
+template <typename T, typename IT, int NT>
+__global__ void __launch_bounds__(NT, 1024 / NT)
     k_schwarz_batch(CsrView A, const int* __restrict__ bpat, const int* __restrict__ bptr,
                     const int64_t* __restrict__ pptr, const int* __restrict__ dofs,
                     const int64_t* __restrict__ inv_off, const IT* __restrict__ inv, const T* b, T* x, double om,
@@ -426,7 +427,9 @@ __host__ __device__ constexpr size_t col_smem_rows(int rows_cap)
     return ((size_t)3 * rows_cap * sizeof(int) + 15) / 16 * 16 + (size_t)rows_cap * sizeof(double);
 }
 
-template <typename T, typename IT>
+// SM = false (patches whose inverse does not fit shared memory): the inverse
+// is read from global memory, the rest is the same.
+template <typename T, typename IT, bool SM>
 __global__ void __launch_bounds__(kColThreads, 1)
     k_schwarz_colour(CsrView A, const int* __restrict__ bpat, const int* __restrict__ bptr, int nbatch,
                      const int64_t* __restrict__ pptr, const int* __restrict__ dofs,
@@ -437,7 +440,7 @@ __global__ void __launch_bounds__(kColThreads, 1)
     extern __shared__ __align__(16) unsigned char col_smem[];
     const int tid = threadIdx.x;
     IT* sAt = reinterpret_cast<IT*>(col_smem);
-    const size_t inv_bytes = col_smem_inv<IT>(mcap);
+    const size_t inv_bytes = SM ? col_smem_inv<IT>(mcap) : 0;
     int* sdof = reinterpret_cast<int*>(col_smem + inv_bytes);
     int* srs = sdof + rows_cap;
     int* sre = srs + rows_cap;
@@ -450,7 +453,7 @@ __global__ void __launch_bounds__(kColThreads, 1)
         const int m = (int)(pptr[p0 + 1] - pptr[p0]);             // the same for every patch of the batch
         const int rows = np_ * m;
         const int64_t off = inv_off[p0];
-        if (off != loaded) {   // this batch's inverse into shared memory, in the background
+        if (SM && off != loaded) {   // this batch's inverse into shared memory, in the background
             const size_t bytes = (size_t)m * m * sizeof(IT);
             const unsigned char* src = reinterpret_cast<const unsigned char*>(inv + off);
             unsigned char* dst = reinterpret_cast<unsigned char*>(sAt);
@@ -470,13 +473,14 @@ __global__ void __launch_bounds__(kColThreads, 1)
         residual_rows<T>(A, rows, sdof, srs, sre, b, x, sr);
         cp_async_wait<0>();
         __syncthreads();
+        const IT* Ag = inv + off;
         for (int i = tid; i < m; i += blockDim.x) {               // sAt[j * m + i] = inverse(i, j)
             double acc[kMaxBatch];
 #pragma unroll
             for (int q = 0; q < kMaxBatch; q++) acc[q] = 0.0;
 #pragma unroll 16
             for (int j = 0; j < m; j++) {
-                const double a = (double)sAt[(size_t)j * m + i];
+                const double a = SM ? (double)sAt[(size_t)j * m + i] : (double)__ldg(Ag + (size_t)j * m + i);
 #pragma unroll
                 for (int q = 0; q < kMaxBatch; q++)
                     if (q < np_) acc[q] += a * sr[q * m + j];
@@ -756,6 +760,11 @@ void SchwarzImpl::init(Context* ctx, Matrix* Am, int kind_, double omega_, int n
         // patch reading the inverse from global memory.
         const char* ef = getenv("JFEM_SCHWARZ_FAST");
         fast = !(ef && ef[0] == '0');
+        // launch shape of k_schwarz_batch: patches per batch (2..4) and threads per CTA (256 or 512)
+        const char* eb = getenv("JFEM_SCHWARZ_BATCH");
+        if (eb && eb[0] >= '2' && eb[0] <= '4') batch_max = eb[0] - '0';
+        const char* et = getenv("JFEM_SCHWARZ_BATCH_THREADS");
+        if (et && atoi(et) == 512) batch_threads = 512;
         int dev = 0, nsm = 148;
         JFG_CUDA(cudaGetDevice(&dev));
         JFG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -769,13 +778,17 @@ void SchwarzImpl::init(Context* ctx, Matrix* Am, int kind_, double omega_, int n
             int pb = 0;
             if ((col.count + kMaxBatch - 1) / kMaxBatch > nsm && kBatchRows / col.mcap >= 2) {
                 col.kern = 1;
-                pb = std::min(kMaxBatch, kBatchRows / col.mcap);
+                pb = std::min(batch_max, kBatchRows / col.mcap);
             } else {
                 pb = std::min(kMaxBatch, (col.count + nsm - 1) / nsm);
                 col.rows_cap = pb * col.mcap;
-                // the FP32 copy of the inverses is half the size: the FP64 bound decides
-                if (col_smem_inv<double>(col.mcap) + col_smem_rows(col.rows_cap) > kColSmemMax) continue;
-                col.kern = 2;
+                // the inverse in shared memory when it fits (the FP32 copy is half the
+                // size: the FP64 bound decides), else read from global memory
+                col.kern = col_smem_inv<double>(col.mcap) + col_smem_rows(col.rows_cap) <= kColSmemMax ? 2 : 3;
+                if (col_smem_rows(col.rows_cap) > kColSmemMax) {
+                    col.kern = 0;
+                    continue;
+                }
             }
             std::vector<int> pl(hc.begin() + col.start, hc.begin() + col.start + col.count);
             std::stable_sort(pl.begin(), pl.end(), [&](int a, int b2) { return hoff2[a] < hoff2[b2]; });
@@ -790,7 +803,7 @@ void SchwarzImpl::init(Context* ctx, Matrix* Am, int kind_, double omega_, int n
             }
             col.b_count = (int)h_bptr.size() - col.b_start;
             h_bptr.push_back((int)h_bpat.size());   // the end of the colour's last batch
-            col.grid = col.kern == 2 ? std::min(col.b_count, nsm) : col.b_count;
+            col.grid = col.kern >= 2 ? std::min(col.b_count, nsm) : col.b_count;
         }
         if (!h_bpat.empty()) {
             bpat.alloc(h_bpat.size());
@@ -854,18 +867,32 @@ void SchwarzImpl::colour_step(const Colour& col, const T* b, T* x, double om, co
     const bool additive = kind == JFG_SCHWARZ_ADDITIVE;
     if (col.independent && !additive) {
         if (col.kern == 1) {
-            k_schwarz_batch<T, IT><<<col.b_count, kBatchThreads, 0, st>>>(csr_of(A), bpat.p, bptr.p + col.b_start,
-                                                                          pptr.p, dofs.p, inv_off.p, iv, b, x, om,
-                                                                          done);
+            if (batch_threads == 256)
+                k_schwarz_batch<T, IT, 256><<<col.b_count, 256, 0, st>>>(csr_of(A), bpat.p, bptr.p + col.b_start,
+                                                                         pptr.p, dofs.p, inv_off.p, iv, b, x, om,
+                                                                         done);
+            else
+                k_schwarz_batch<T, IT, kBatchThreads><<<col.b_count, kBatchThreads, 0, st>>>(
+                    csr_of(A), bpat.p, bptr.p + col.b_start, pptr.p, dofs.p, inv_off.p, iv, b, x, om, done);
         } else if (col.kern == 2) {
             static bool attr = false;      // per instantiation
             if (!attr) {
-                JFG_CUDA(cudaFuncSetAttribute(k_schwarz_colour<T, IT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)kColSmemMax));
+                JFG_CUDA(cudaFuncSetAttribute(k_schwarz_colour<T, IT, true>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kColSmemMax));
                 attr = true;
             }
             const size_t smem = col_smem_inv<IT>(col.mcap) + col_smem_rows(col.rows_cap);
-            k_schwarz_colour<T, IT><<<col.grid, kColThreads, smem, st>>>(
+            k_schwarz_colour<T, IT, true><<<col.grid, kColThreads, smem, st>>>(
+                csr_of(A), bpat.p, bptr.p + col.b_start, col.b_count, pptr.p, dofs.p, inv_off.p, iv, col.mcap,
+                col.rows_cap, b, x, om, done);
+        } else if (col.kern == 3) {
+            static bool attr = false;      // per instantiation
+            if (!attr) {
+                JFG_CUDA(cudaFuncSetAttribute(k_schwarz_colour<T, IT, false>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kColSmemMax));
+                attr = true;
+            }
+            k_schwarz_colour<T, IT, false><<<col.grid, kColThreads, col_smem_rows(col.rows_cap), st>>>(
                 csr_of(A), bpat.p, bptr.p + col.b_start, col.b_count, pptr.p, dofs.p, inv_off.p, iv, col.mcap,
                 col.rows_cap, b, x, om, done);
         } else {

@@ -22,6 +22,8 @@ struct SchwarzImpl {
     int64_t total_m = 0, total_inv = 0;
     int nunique = 0;                    // distinct patch operators (inverses stored)
     bool fast = true;                   // batched / shared-memory colour-step kernels (JFEM_SCHWARZ_FAST)
+    int batch_max = 4;                  // patches per batch of k_schwarz_batch
+    int batch_threads = 256;            // its threads per CTA (4 CTAs per SM)
     uint64_t uid = next_uid();
     DevBuf<int64_t> pptr, inv_off;      // patch p: dofs[pptr[p], pptr[p+1]), inverse at inv + inv_off[p]
     DevBuf<int> dofs;
@@ -41,7 +43,8 @@ struct SchwarzImpl {
         int64_t t_start = 0, t_count = 0;   // range of touched
         int mcap = 0;                   // largest patch of the colour
         int b_start = 0, b_count = 0;   // batches bptr[b_start .. b_start + b_count] (0: one CTA per patch)
-        int kern = 0;                   // 0: one CTA per patch, 1: k_schwarz_batch, 2: k_schwarz_colour
+        int kern = 0;                   // 0: one CTA per patch, 1: k_schwarz_batch, 2 / 3: k_schwarz_colour
+                                        // with the inverse in shared / global memory
         int rows_cap = 0;               // patch rows per batch at most (k_schwarz_colour)
         int grid = 0;                   // CTAs of the colour-step launch
     };
