@@ -686,8 +686,9 @@ KAPPA_TRAFFIC = {"case": (1050625, 9410585), "bytes": 42063360,
 
 
 def q2_extra(ctx, reps, stream, args):
-    """The Q2 512x512 -Lap u + 5u = f GMG-PCG (FP64 and FP64 PCG + FP32
-    V-cycle, from e0), timed like the arms of the main line."""
+    """The Q2 512x512 -Lap u + 5u = f GMG-PCG (FP64, FP64 PCG + FP32
+    V-cycle, and FP64 PCG + V-cycle reading scaled-FP16 matrices, from e0),
+    timed like the arms of the main line."""
     import ctypes as C
     import torch
     from jfem_b200 import _native as N
@@ -698,6 +699,8 @@ def q2_extra(ctx, reps, stream, args):
     prol = [DeviceMatrix(h.systems[l + 1].n, h.systems[l].n, *h.prolong[l], ctx) for l in range(LEVELS - 1)]
     mg = MGPreconditioner(mats, prol, h.boundary, [None] + [JacobiSmoother(2, 2 / 3)] * (LEVELS - 1), cycles=1,
                           use_fmg=False, precision="mixed", ctx=ctx)
+    mg16 = MGPreconditioner(mats, prol, h.boundary, [None] + [JacobiSmoother(2, 2 / 3)] * (LEVELS - 1), cycles=1,
+                            use_fmg=False, precision="mixed-fp16", ctx=ctx)
     A = mats[-1]
     n = A.rows
     b = torch.from_numpy(h.finest.rhs).cuda()
@@ -707,7 +710,7 @@ def q2_extra(ctx, reps, stream, args):
     dx = torch.empty_like(e0)
     info = N.SolveInfo()
     res = {}
-    for name, prec in (("fp64", N.FP64), ("mixed", N.MIXED_PRECOND)):
+    for name, prec, pm in (("fp64", N.FP64, mg), ("mixed", N.MIXED_PRECOND, mg), ("fp16", N.MIXED_PRECOND, mg16)):
         def once():
             with torch.cuda.stream(stream):
                 dx.copy_(e0)
@@ -715,7 +718,7 @@ def q2_extra(ctx, reps, stream, args):
             N.load().jfg_solver_opts_default(C.byref(o))
             o.tol = tol
             o.precision = prec
-            ctx.check(N.load().jfg_solve_dev(ctx.handle, N.PCG, A.handle, N.PREC_MG, mg.handle,
+            ctx.check(N.load().jfg_solve_dev(ctx.handle, N.PCG, A.handle, N.PREC_MG, pm.handle,
                                              C.c_void_p(b.data_ptr()), C.c_void_p(dx.data_ptr()), C.byref(o),
                                              C.byref(info)))
         for _ in range(max(3, args.warmup)):
@@ -735,6 +738,7 @@ def q2_extra(ctx, reps, stream, args):
     ms32 = A.time_spmv(precision=1, iters=20)
     res["workload"] = WORKLOAD
     res["speedup_mixed_vs_fp64"] = res["fp64"]["time_s"] / res["mixed"]["time_s"]
+    res["speedup_fp16_vs_fp64"] = res["fp64"]["time_s"] / res["fp16"]["time_s"]
     res["spmv_fp32_gbs"] = spmv_bytes(n, A.nnz, 4, 4) / (ms32 * 1e-3) / 1e9
     return res
 
