@@ -38,7 +38,7 @@ from .linalg import (DenseMatrix, DeviceMatrix, IllegalArgumentException, Iterat
 
 __all__ = ["BlockSparseMatrix", "AbstractSchurSolver", "ExplicitSchurSolver", "IterativeExplicitSchur",
            "DirectSchur", "RichardsonExplicitSchur", "ImplicitSchurSolver", "IterativeImplicitSchur",
-           "SchurOperator"]
+           "SchurOperator", "BlockGaussSeidelSmoother"]
 
 
 def _coo_of(block):
@@ -438,3 +438,72 @@ class IterativeImplicitSchur(ImplicitSchurSolver):
 
     def solveSchur(self, A, b):
         return A.solvePGMRES(self.firstInverse, b, 1e-9, self.it)
+
+
+class BlockGaussSeidelSmoother:
+    """multigrid/BlockGaussseidelSmoother.java: block Gauss-Seidel over the
+    partition of a BlockSparseMatrix, omega = 1.  Each run (lines 33-66):
+    the strictly upper blocks applied to the iterate, then the blocks in
+    order, block i solved with the dense inverse of its diagonal block after
+    subtracting the strictly lower blocks times the blocks already solved.
+    The diagonal inverses come from the device LU (jfg_dense_inverse), an
+    uninvertible block is replaced by the identity as in
+    BlockSparseMatrix.getInvertedDiagonalMatrix (BlockSparseMatrix.java:194-220);
+    every block product is a device SpMV."""
+
+    omega = 1.0
+
+    def __init__(self, blockMatrix: BlockSparseMatrix, runs: int):
+        from .linalg import SingularMatrixException
+        self.runs = int(runs)
+        self.blockMatrix = blockMatrix
+        self.ctx = blockMatrix.ctx
+        self.starts = blockMatrix.getBlockStarts()
+        self.ends = blockMatrix.getBlockEnds()
+        nb = len(self.starts)
+        self._dinv = []
+        for i in range(nb):
+            r, c, v, (m, _) = blockMatrix.getBlockCoo(self.starts[i], self.starts[i])
+            d = np.zeros((m, m))
+            np.add.at(d, (r, c), v)
+            try:
+                inv = DenseMatrix(d, self.ctx).inverse()
+            except SingularMatrixException:
+                inv = np.eye(m)
+            ri, ci = np.nonzero(inv)
+            self._dinv.append(DeviceMatrix(m, m, ri, ci, inv[ri, ci], self.ctx))
+        # block (i, j) of the partition for every stored block off the diagonal
+        self._upper, self._lower = [], {}
+        for i in range(nb):
+            for j in range(nb):
+                if i != j and blockMatrix.hasBlock(self.starts[i], self.starts[j]):
+                    if i < j:
+                        self._upper.append((i, j))
+                    else:
+                        self._lower.setdefault(i, []).append(j)
+
+    def smooth(self, operator, rhs, iterate, verbose: bool = False, prefix: str = ""):
+        b = N.f64(rhs)
+        x = N.f64(iterate).copy()
+        n = self.blockMatrix.getVectorSize()
+        if b.shape != (n,) or x.shape != (n,):
+            raise IllegalArgumentException("Vectors are of different size")
+        bm, st, en = self.blockMatrix, self.starts, self.ends
+        if verbose:
+            print(prefix + " " + str(np.linalg.norm(operator.mvMul(x) - b)))
+        for _ in range(self.runs):
+            ux = np.zeros(n)
+            for (i, j) in self._upper:
+                ux[st[i]:en[i]] += bm.getBlockMatrix(i, j).spmv(x[st[j]:en[j]])
+            sub = b - ux * self.omega
+            x = np.zeros(n)
+            ret = []
+            for i in range(len(st)):
+                t = sub[st[i]:en[i]].copy()
+                for j in sorted(self._lower.get(i, [])):
+                    t -= bm.getBlockMatrix(i, j).spmv(ret[j]) * self.omega
+                ret.append(self._dinv[i].spmv(t))
+                x[st[i]:en[i]] += ret[i]
+            if verbose:
+                print(prefix + " " + str(np.linalg.norm(operator.mvMul(x) - b)))
+        return x
