@@ -505,9 +505,10 @@ __global__ void k_identity(int n, double* B)
     B[idx] = (idx / n == idx % n) ? 1.0 : 0.0;
 }
 
-// Whether a 16-CTA cluster of k_lu_panel_cl with `smem` bytes of dynamic
-// shared memory can be resident (asked once per size class).
-bool panel_cluster_ok(size_t smem)
+// Whether a 16-CTA cluster of k_lu_panel_cl with the largest dynamic shared
+// memory it is launched with (200 KB per CTA) can be resident; asked once per
+// process, on the first device that factors a large enough matrix.
+bool panel_cluster_ok()
 {
     static int cached = -1;
     if (cached >= 0) return cached == 1;
@@ -532,7 +533,6 @@ bool panel_cluster_ok(size_t smem)
     int nc = 0;
     if (cudaOccupancyMaxActiveClusters(&nc, k_lu_panel_cl, &cfg) == cudaSuccess && nc >= 1) cached = 1;
     cudaGetLastError();
-    (void)smem;
     return cached == 1;
 }
 
@@ -541,7 +541,7 @@ void launch_panel(int n, double* A, int* piv, int k0, int nb, int* info, cudaStr
     const int R = n - k0;
     const int rc = (R + kPcCtas - 1) / kPcCtas;
     const size_t smem = (size_t)rc * kPcStride * sizeof(double);
-    if (R >= 512 && smem <= 200 * 1024 && panel_cluster_ok(smem)) {
+    if (R >= 512 && smem <= 200 * 1024 && panel_cluster_ok()) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(kPcCtas);
         cfg.blockDim = dim3(kPcThreads);
