@@ -51,3 +51,20 @@ def test_one_block_is_a_direct_solve_and_smoothing_converges():
         e = np.sqrt((xs - x) @ D @ (xs - x))
         assert e < e_prev
         e_prev = e
+
+
+def test_uninvertible_block_becomes_identity():
+    """BlockSparseMatrix.getInvertedDiagonalMatrix (BlockSparseMatrix.java:194-220)
+    replaces a diagonal block it cannot invert by the identity: with a zero
+    (2, 2) block the second block of the result is its right-hand side minus
+    the lower block times the first block's solution."""
+    rng = np.random.default_rng(4)
+    A = rng.standard_normal((4, 4)) + 4 * np.eye(4)
+    B = rng.standard_normal((2, 4))
+    blocks = {(0, 0): A, (0, 1): B.T.copy(), (1, 0): B, (1, 1): np.zeros((2, 2))}
+    b = rng.standard_normal(6)
+    x0 = rng.standard_normal(6)
+    x = block_gauss_seidel(blocks, [0, 4], [4, 6], b, x0, 1)
+    x1 = np.linalg.solve(A, b[:4] - B.T @ x0[4:])
+    np.testing.assert_allclose(x[:4], x1, rtol=1e-12)
+    np.testing.assert_allclose(x[4:], b[4:] - B @ x1, rtol=1e-12)
