@@ -17,7 +17,39 @@ from .linalg import IllegalArgumentException, _as_device
 
 
 class DirectSolver:
-    """schwarz/DirectSolver.java: dense inverse of each local operator, cached."""
+    """schwarz/DirectSolver.java: dense inverse of each local operator, cached.
+
+    Inside the device Schwarz decompositions the inverses are built and kept
+    on the GPU (k_patch_inverse, one per distinct local operator).  As a
+    SystemSolver of its own, solve(system, rhs, patch) follows
+    DirectSolver.java:22-38: the first call for a patch inverts the given
+    local system (device LU, jfg_dense_inverse) and caches the inverse under
+    the patch number; every call returns inverse * rhs."""
+
+    def __init__(self):
+        self.inverses = {}
+
+    def solve(self, system, rhs, patch: int):
+        from .linalg import DenseMatrix
+        patch = int(patch)
+        if patch not in self.inverses:
+            ctx = getattr(system, "ctx", None)
+            if isinstance(system, DenseMatrix):
+                a = system.a
+            elif hasattr(system, "coo"):            # SparseMatrix / DeviceMatrix: duplicates summed
+                r, c, v = system.coo()
+                a = np.zeros((int(system.rows), int(system.cols)))
+                np.add.at(a, (np.asarray(r), np.asarray(c)), np.asarray(v, dtype=np.float64))
+            else:
+                a = np.asarray(system, dtype=np.float64)
+            if a.ndim != 2 or a.shape[0] != a.shape[1]:
+                raise IllegalArgumentException("the local system must be a square matrix")
+            self.inverses[patch] = DenseMatrix(a, ctx).inverse()
+        b = N.f64(rhs)
+        inv = self.inverses[patch]
+        if b.shape != (inv.shape[1],):
+            raise IllegalArgumentException("Vectors are of different size")
+        return inv @ b
 
 
 class MultiplicativeSubspaceCorrection:

@@ -74,3 +74,22 @@ def test_blocked_lu_bit_identical(ctx, monkeypatch, n):
     assert np.linalg.norm(a @ x - b) <= 1e-10 * np.linalg.norm(a) * np.linalg.norm(x) * n
     if n <= 1000:
         np.testing.assert_allclose(x, O.dense_solve(a, b), rtol=1e-7, atol=1e-9 * np.abs(x).max())
+
+
+def test_direct_solver_caches_patch_inverses(ctx):
+    """schwarz/DirectSolver.java:22-38 as a SystemSolver: the first solve for
+    a patch inverts the given local system (device LU) and caches it under
+    the patch number; later solves for that patch reuse the inverse, whatever
+    system they pass."""
+    from jfem_b200.schwarz import DirectSolver
+    rng = np.random.default_rng(9)
+    a = rng.standard_normal((12, 12)) + 12 * np.eye(12)
+    b = rng.standard_normal(12)
+    sp = SparseMatrix.from_coo(12, 12, *np.nonzero(a), a[np.nonzero(a)], ctx)
+    ds = DirectSolver()
+    np.testing.assert_allclose(ds.solve(sp, b, 3), np.linalg.solve(a, b), rtol=1e-12, atol=1e-13)
+    np.testing.assert_allclose(ds.solve(DenseMatrix(2 * a, ctx), b, 3), np.linalg.solve(a, b), rtol=1e-12,
+                               atol=1e-13)
+    np.testing.assert_allclose(ds.solve(DenseMatrix(2 * a, ctx), b, 4), np.linalg.solve(2 * a, b), rtol=1e-12,
+                               atol=1e-13)
+    assert sorted(ds.inverses) == [3, 4]
